@@ -1,0 +1,164 @@
+/*
+ * molsim_gpu.h -- C-ABI of the B200 force/energy path for MOLSIM.
+ *
+ * The library is a drop-in for MOLSIM's per-step force/energy routines of a
+ * monoatomic charged system.  The Fortran host keeps its own arrays and calls
+ * these entry points through an ISO_C_BINDING interface (the same mechanism
+ * MOLSIM already uses for FFTW, Src/energy.F90:100-110).  All arrays are
+ * plain host pointers; Fortran (3,N) real(8) arrays are passed as C [N][3]
+ * doubles.  Type indices, pair-table offsets and neighbour indices keep
+ * MOLSIM's 1-based values.
+ *
+ * Entry points and the MOLSIM routine each one replaces:
+ *   msg_create / msg_create_batch  -> set-up done by IOPotTwoBody+EwaldSetup
+ *                                     (Src/potential.F90:294-446,
+ *                                      Src/energy.F90:6601-7019) and IONList
+ *                                     (Src/nlist.F90:184-281)
+ *   msg_set_state / msg_get_state  -> the ro/rod/rodd globals (Src/mol.F90:1087-1098)
+ *   msg_build_nlist                -> SetVList -> SetVListMD (Src/nlist.F90:686-759)
+ *   msg_utotal                     -> UTotal (Src/energy.F90:280-434) with
+ *                                     UTwoBodyA, UEwald(SPM), UBond
+ *   msg_get_linacc                 -> GetLinAcc (Src/md.F90:601-617)
+ *   msg_velver                     -> MDDriver iSimulationStep: VelVer +
+ *                                     GetKinEnergy (Src/md.F90:154-168, 252-410)
+ *                                     followed by NList (Src/nlist.F90:597-621)
+ *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
+ *                                     (Src/bd.F90:53-59, 120-155) followed by NList
+ * Set-up helpers that restate MOLSIM's own set-up for callers without it:
+ *   msg_rcut_to_alpha              -> RcutToAlpha (Src/energy.F90:7090-7105)
+ *   msg_pot_tab                    -> PotTwoBodyTab1/2/3 with Pot_1_6_12
+ *                                     (Src/potential.F90:868-1258, 1349-1425)
+ *
+ * Status codes mirror MOLSIM's Stop() sites so the Fortran shim can stop with
+ * the same message.
+ */
+#ifndef MOLSIM_GPU_H
+#define MOLSIM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSG_OK               0
+#define MSG_ERR_TABLE_MIN    1  /* r2 < r2umin           (Src/energy.F90:478-479) */
+#define MSG_ERR_TABLE_RANGE  2  /* ibuf > nbuf           (Src/energy.F90:485)     */
+#define MSG_ERR_CAPACITY     3  /* nneighpn > maxnneigh  (Src/nlist.F90:752)      */
+#define MSG_ERR_CUDA         4  /* CUDA or cuFFT failure                          */
+#define MSG_ERR_TIMEOUT      5  /* a bounded device wait gave up                  */
+#define MSG_ERR_ARG          6  /* invalid argument                               */
+#define MSG_ERR_NONFINITE    7  /* a force or energy became NaN/Inf               */
+#define MSG_ERR_HARDCORE     8  /* r2 < r2atat (hard-core overlap, Src/energy.F90:476) */
+
+#define MSG_PREC_FP64        0  /* FP64 everywhere: the plain drop-in path          */
+#define MSG_PREC_MIXED       1  /* FP32 pair/grid forces, 64-bit fixed-point sums,
+                                   FP64 positions, integrator, energies, b^2 moduli */
+
+/* One system.  Mirrors the MolModule globals used on the path (Src/mol.F90). */
+typedef struct msg_params {
+    int32_t np;              /* particles (= atoms, monoatomic)                         */
+    int32_t npt;             /* particle types                                          */
+    double  boxlen[3];       /* periodic box, A (txbc='xyz')                            */
+    double  rcut;            /* real-space cutoff, A                                    */
+    double  drnlist;         /* Verlet skin, A                                          */
+    const int32_t *iptpn;    /* [np] type of each particle, 1-based                     */
+    const double  *az;       /* [np] charge, e                                          */
+    const double  *masspt;   /* [npt] mass, g/mol                                       */
+    const double  *ubuf;     /* pair table, 12 doubles per interval (Src/mol.F90:1120)  */
+    int32_t        nbuf;     /* doubles in ubuf                                         */
+    const int32_t *iubuflow; /* [natat] 1-based start of each type pair's table         */
+    const double  *r2umin;   /* [natat] lower table limit, A^2                          */
+    const double  *r2atat;   /* [natat] hard-core r^2 (0: none), A^2                    */
+    int32_t lewald;          /* 1: SPME reciprocal space                                */
+    int32_t order;           /* B-spline order                                          */
+    int32_t nmesh;           /* SPME grid edge (even)                                   */
+    int32_t lsurf;           /* 1: add the surface (dipole) term                        */
+    double  ualpha;          /* Ewald alpha, 1/A                                        */
+    double  epsi_four_pi;    /* Epsi0FourPi/relpermitt, kJ A / mol                      */
+    int32_t nbond;           /* bonds                                                   */
+    const int32_t *bond_ij;  /* [nbond][2] 1-based particle pairs                       */
+    const double  *bond_k;   /* [nbond] force constant divided by the power             */
+    const double  *bond_eq;  /* [nbond] equilibrium length, A                           */
+    const int32_t *bond_p;   /* [nbond] power                                           */
+    double  tstep;           /* time step, ps                                           */
+    const double  *bd_fac1;  /* [npt] BD drift factor (Src/bd.F90:138), may be NULL    */
+    const double  *bd_fac2;  /* [npt] BD noise factor (Src/bd.F90:139), may be NULL    */
+    int32_t maxnneigh;       /* row capacity hint for the neighbour list (0: automatic) */
+} msg_params;
+
+typedef struct msg_handle msg_handle;
+
+/* Energies of one system, MOLSIM's u%... fields (kJ/mol) and virial. */
+typedef struct msg_energy {
+    double utot;             /* u%tot                                   */
+    double utwob0;           /* u%twob(0) = sum over type pairs          */
+    double utwob[10];        /* u%twob(1..natat), natat <= 10 (npt <= 4) */
+    double urec;             /* u%rec (reciprocal + self + surface)      */
+    double ubond;            /* u%bond                                   */
+    double virial;           /* virial                                   */
+    double ekin;             /* kinetic energy after the step (MD)       */
+} msg_energy;
+
+/* Create a handle for one system on the current CUDA device. */
+int  msg_create(const msg_params *p, int32_t precision, msg_handle **out);
+/* Create a handle for nsys independent systems advanced together. */
+int  msg_create_batch(const msg_params *p, int32_t nsys, int32_t precision, msg_handle **out);
+void msg_destroy(msg_handle *h);
+const char *msg_last_error(const msg_handle *h);
+int32_t msg_nsys(const msg_handle *h);
+
+/* Positions ro, velocities rod, accelerations rodd of system isys, [np][3]; NULL skips. */
+int  msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd);
+int  msg_get_state(msg_handle *h, int32_t isys, double *ro, double *rod, double *rodd);
+
+/* Rebuild the Verlet list now (SetVListMD semantics: r2 < (rcut+drnlist)^2 with
+ * MOLSIM's PBCr2).  Optionally export it in MOLSIM's layout: nneighpn[np] and
+ * jpnlist[np][maxnneigh] with 1-based partners owned by the parity rule of
+ * Src/nlist.F90:741-744, ascending within each row.  *npair = half-list pairs. */
+int  msg_build_nlist(msg_handle *h, int32_t isys, int32_t *nneighpn, int32_t *jpnlist,
+                     int32_t maxnneigh, int64_t *npair);
+
+/* UTotal for every system; outputs for system isys: force (kJ/(mol A)),
+ * forceo (internal units), energies.  NULL outputs are skipped. */
+int  msg_utotal(msg_handle *h, int32_t isys, double *force, double *forceo, msg_energy *e);
+
+/* rodd = massip * forceo (GetLinAcc) from the last msg_utotal. */
+int  msg_get_linacc(msg_handle *h);
+
+/* nsteps velocity-Verlet steps of every system, entirely on the device.
+ * e (optional): [nsteps] energies of system isys after each step. */
+int  msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energy *e);
+
+/* nsteps Brownian-dynamics steps.  xi == NULL: FP32 normal noise from a
+ * Philox4x32-10 stream keyed by (seed, particle, step); otherwise xi holds
+ * caller noise for system isys, [nsteps][np][3] (for the drop-in, MOLSIM's
+ * GauRandom sequence).  xi_out (optional) receives the noise used. */
+int  msg_bd_step(msg_handle *h, int32_t nsteps, uint64_t seed, int32_t isys,
+                 const double *xi, double *xi_out, msg_energy *e);
+
+/* Number of list rebuilds since creation, for system isys. */
+int64_t msg_nrebuild(const msg_handle *h, int32_t isys);
+
+/* Set-up helpers (host only). */
+double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
+                         double boxlenshort, double rcut, int32_t *status);
+
+typedef struct msg_tab_params {
+    int32_t npt;
+    const double *zat, *sigat, *epsat;   /* [npt] */
+    double rcut, ualpha, epsi_four_pi;
+    int32_t lewald, lljcut;
+    double ljrcut, ljushift;
+    double r2uminin, utoltab, ftoltab, umaxtab, fmaxtab, rumaxfac;
+} msg_tab_params;
+
+/* Build MOLSIM's pair table.  Returns MSG_OK or MSG_ERR_CAPACITY (nbuf too
+ * small) or MSG_ERR_ARG (no convergence). */
+int  msg_pot_tab(const msg_tab_params *p, double *ubuf, int32_t nbuf, int32_t *iubuflow,
+                 int32_t *nugrid, double *r2umin, int32_t *nused);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

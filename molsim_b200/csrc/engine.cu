@@ -1,0 +1,909 @@
+// engine.cu -- the B200 force/energy engine behind the C-ABI of molsim_gpu.h.
+//
+// One handle owns every device buffer of its systems (concatenated), the pair
+// tables, the SPME grids with their cuFFT plans, and one CUDA stream.  A step
+// is a fixed sequence of kernels; each API call enqueues its steps and checks
+// the device error word once at the end.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/molsim_gpu.h"
+#include "common.cuh"
+#include "kernels_force.cuh"
+#include "kernels_md.cuh"
+#include "radix_sort.cuh"
+#include "setup.h"
+
+using namespace msg;
+
+namespace {
+
+struct CudaError {
+    int code;
+    std::string what;
+};
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) throw CudaError{MSG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+#define CKF(x)                                                                                 \
+    do {                                                                                       \
+        cufftResult r_ = (x);                                                                  \
+        if (r_ != CUFFT_SUCCESS) throw CudaError{MSG_ERR_CUDA, std::string(#x) + ": cufft error " + std::to_string((int)r_)}; \
+    } while (0)
+
+template <typename T>
+T *dalloc(size_t n)
+{
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    CK(cudaMemset(p, 0, n * sizeof(T)));
+    return static_cast<T *>(p);
+}
+
+template <typename T>
+void h2d(T *d, const T *h, size_t n, cudaStream_t st)
+{
+    if (n) CK(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+struct HostSys {
+    int n, off, npt, natat, order, s;
+    msg_params p;
+};
+
+struct FftClass {
+    int s, count;
+    long long grid_off, cgrid_off;
+    cufftHandle fwd = 0, bwd = 0;
+};
+
+}  // namespace
+
+struct msg_handle {
+    int nsys = 0, ntot = 0, prec = MSG_PREC_FP64, order = 4;
+    std::vector<SysDev> hs;
+    std::vector<int> hn;
+    std::string err;
+    cudaStream_t st = nullptr;
+    int dev = 0;
+    // particles (double-buffered where the rebuild permutes)
+    int cur = 0;
+    double4 *pos[2] = {}, *vel[2] = {}, *acc[2] = {}, *dsum[2] = {}, *fo[2] = {};
+    int *typ[2] = {}, *orig[2] = {};
+    int *cellid = nullptr, *inv = nullptr, *sysid = nullptr;
+    double4 *fsr = nullptr, *ftot = nullptr;
+    float4 *pos32 = nullptr;
+    // rebuild
+    uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *rhist = nullptr;
+    int ncell_tot = 0, cell_bits = 1;
+    int *cstart = nullptr, *cend = nullptr;
+    int *nbl = nullptr, *nnb = nullptr;
+    long long nbl_tot = 0;
+    // skin
+    double *r2o = nullptr, *skinout = nullptr;
+    SkinChunk *sc = nullptr;
+    unsigned *sysdone = nullptr;
+    int *flag = nullptr;
+    long long *nrebuild = nullptr;
+    // work lists
+    Tile *t128 = nullptr, *t32 = nullptr;
+    int nt128 = 0, nt32 = 0;
+    int4 *chunks = nullptr, *infl = nullptr;
+    int nchunk = 0, ninfl = 0;
+    double *ppart = nullptr, *fpart = nullptr, *ipart = nullptr, *psurf = nullptr;
+    double *esys = nullptr, *hist = nullptr;
+    int hist_cap = 0;
+    unsigned long long *stepctr = nullptr, *sstep = nullptr;
+    unsigned *rdone = nullptr;
+    ErrWord *errw = nullptr;
+    // tables
+    PairTab *ptab = nullptr;
+    int *ptmap = nullptr;
+    double *tz = nullptr, *tc = nullptr;
+    unsigned short *bst = nullptr;
+    double *massip = nullptr, *massp = nullptr, *fac1 = nullptr, *fac2 = nullptr;
+    int has_bd = 0;
+    // bonds
+    int *bptr = nullptr, *bpart = nullptr, *bpw = nullptr;
+    double *bk = nullptr, *beq = nullptr;
+    // SPME
+    int any_ewald = 0;
+    double *rgrid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
+    double2 *cgrid = nullptr;
+    long long grid_tot = 0, cgrid_tot = 0;
+    std::vector<FftClass> fft;
+    // staging
+    double *stage = nullptr;
+    size_t stage_n = 0;
+    double *xin = nullptr;
+    size_t xin_n = 0;
+    SysDev *dsys = nullptr;
+
+    ~msg_handle();
+    void build(const msg_params *p, int n, int prec);
+    void enqueue_rebuild();
+    void enqueue_forces(int mode);
+    void enqueue_reduce(bool record);
+    void enqueue_md_step(bool record);
+    void enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record);
+    void ensure_stage(size_t n);
+    int check();
+};
+
+static void free_all(msg_handle *h)
+{
+    void *ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->acc[0], h->acc[1], h->dsum[0], h->dsum[1],
+                    h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
+                    h->sysid, h->fsr, h->ftot, h->pos32, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
+                    h->cend, h->nbl, h->nnb, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
+                    h->t128, h->t32, h->chunks, h->infl, h->ppart, h->fpart, h->ipart, h->psurf, h->esys,
+                    h->hist, h->stepctr, h->sstep, h->rdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
+                    h->bst, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
+                    h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->stage, h->xin, h->dsys};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (auto &f : h->fft) {
+        if (f.fwd) cufftDestroy(f.fwd);
+        if (f.bwd) cufftDestroy(f.bwd);
+    }
+    h->fft.clear();
+    if (h->st) cudaStreamDestroy(h->st);
+    h->st = nullptr;
+}
+
+msg_handle::~msg_handle() { free_all(this); }
+
+void msg_handle::ensure_stage(size_t n)
+{
+    if (n <= stage_n) return;
+    if (stage) cudaFree(stage);
+    stage = dalloc<double>(n);
+    stage_n = n;
+}
+
+// ---------------------------------------------------------------------------
+// Set-up of all systems.
+// ---------------------------------------------------------------------------
+void msg_handle::build(const msg_params *P, int n, int precision)
+{
+    nsys = n;
+    prec = precision;
+    CK(cudaGetDevice(&dev));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    hs.resize(n);
+    hn.resize(n);
+    order = P[0].order;
+    std::vector<HostSys> H(n);
+    ntot = 0;
+    int type_tot = 0, pt_tot = 0, ptmap_tot = 0, cell_tot = 0, t128 = 0, t32 = 0, nch = 0, nif = 0;
+    long long nbl_acc = 0;
+    int ntab = 0;
+    size_t nbond_tot = 0;
+    for (int s = 0; s < n; ++s) {
+        const msg_params &p = P[s];
+        if (p.np < 1 || p.npt < 1 || p.npt > MAXT) throw CudaError{MSG_ERR_ARG, "np >= 1 and 1 <= npt <= 4 required"};
+        if (p.lewald && (p.order < 4 || p.order > 6 || p.nmesh < 4 || (p.nmesh & 1)))
+            throw CudaError{MSG_ERR_ARG, "SPME needs 4 <= order <= 6 and an even nmesh"};
+        if (p.lewald && p.order != order) throw CudaError{MSG_ERR_ARG, "all systems of a handle share one spline order"};
+        if (!p.iptpn || !p.az || !p.masspt || !p.ubuf || !p.iubuflow || !p.r2umin)
+            throw CudaError{MSG_ERR_ARG, "iptpn, az, masspt, ubuf, iubuflow and r2umin are required"};
+        SysDev &S = hs[s];
+        std::memset(&S, 0, sizeof(S));
+        S.n = p.np;
+        S.off = ntot;
+        S.npt = p.npt;
+        S.natat = p.npt * (p.npt + 1) / 2;
+        S.pt_off = pt_tot;
+        S.lewald = p.lewald ? 1 : 0;
+        S.lsurf = (p.lewald && p.lsurf) ? 1 : 0;
+        for (int d = 0; d < 3; ++d) {
+            S.box[d] = p.boxlen[d];
+            S.half[d] = p.boxlen[d] / 2.0;
+            S.boxi[d] = 1.0 / p.boxlen[d];
+        }
+        S.vol = p.boxlen[0] * p.boxlen[1] * p.boxlen[2];
+        S.rcut2 = p.rcut * p.rcut;
+        const double rl = p.rcut + p.drnlist;
+        S.rs2cut = rl * rl;
+        S.drnlist = p.drnlist;
+        for (int d = 0; d < 3; ++d) {
+            int nc = (int)std::floor(p.boxlen[d] / (rl * (1.0 + 1e-10)));
+            S.ncell[d] = std::max(1, nc);
+        }
+        S.cell_off = cell_tot;
+        cell_tot += S.ncell[0] * S.ncell[1] * S.ncell[2];
+        const double dens = p.np / S.vol;
+        const double vshell = 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl;
+        int cap = (int)std::ceil(2.0 * dens * vshell) + 64;
+        if (p.maxnneigh > 0) cap = std::max(cap, (int)p.maxnneigh);
+        cap = std::min(cap, ((p.np + 7) / 8) * 8);
+        cap = std::max(cap, 8);
+        S.cap = cap;
+        S.nbl_off = nbl_acc;
+        nbl_acc += (long long)cap * p.np;
+        S.s = p.lewald ? p.nmesh : 0;
+        S.order = p.order;
+        for (int d = 0; d < 3; ++d) S.dkdr[d] = p.lewald ? (double)p.nmesh / p.boxlen[d] : 0.0;
+        S.epsfp = p.epsi_four_pi;
+        S.alpha = p.ualpha;
+        double q2 = 0.0;
+        for (int i = 0; i < p.np; ++i) q2 += p.az[i] * p.az[i];
+        S.uself = -(p.ualpha / std::sqrt(3.1415926535897932) * q2);
+        S.dt = p.tstep;
+        S.type_off = type_tot;
+        S.ptmap_off = ptmap_tot;
+        S.tile128_off = t128;
+        S.ntile128 = (p.np + 127) / 128;
+        S.tile32_off = t32;
+        S.ntile32 = (p.np + 31) / 32;
+        S.chunk_off = nch;
+        S.nchunk = (p.np + SK_CHUNK - 1) / SK_CHUNK;
+        S.seed = (uint64_t)s * 0x9E3779B97F4A7C15ull;
+        t128 += S.ntile128;
+        t32 += S.ntile32;
+        nch += S.nchunk;
+        type_tot += p.npt;
+        pt_tot += S.natat;
+        ptmap_tot += p.npt * p.npt;
+        nbond_tot += (size_t)std::max(0, (int)p.nbond);
+        ntot += p.np;
+        hn[s] = p.np;
+        H[s].p = p;
+        if (p.bd_fac1 && p.bd_fac2) has_bd = 1;
+        if (p.lewald) any_ewald = 1;
+        (void)ntab;
+    }
+    ncell_tot = cell_tot;
+    cell_bits = 1;
+    while ((1u << cell_bits) <= (unsigned)cell_tot) ++cell_bits;
+    nbl_tot = nbl_acc;
+    nt128 = t128;
+    nt32 = t32;
+    nchunk = nch;
+
+    // --- SPME grids grouped by edge, one batched cuFFT plan pair per edge ---
+    if (any_ewald) {
+        std::map<int, std::vector<int>> bys;
+        for (int s = 0; s < n; ++s)
+            if (hs[s].lewald) bys[hs[s].s].push_back(s);
+        long long go = 0, co = 0, fo_acc = 0;
+        for (auto &kv : bys) {
+            const int e = kv.first;
+            FftClass fc;
+            fc.s = e;
+            fc.count = (int)kv.second.size();
+            fc.grid_off = go;
+            fc.cgrid_off = co;
+            for (int s : kv.second) {
+                hs[s].grid_off = go;
+                hs[s].cgrid_off = co;
+                go += (long long)e * e * e;
+                co += (long long)e * e * (e / 2 + 1);
+            }
+            fft.push_back(fc);
+        }
+        for (int s = 0; s < n; ++s)
+            if (hs[s].lewald) {
+                const int h = hs[s].s / 2 + 1;
+                hs[s].fac_off = fo_acc;
+                fo_acc += (long long)h * h * h;
+            }
+        grid_tot = go;
+        cgrid_tot = co;
+        rgrid = dalloc<double>(grid_tot);
+        cgrid = dalloc<double2>(cgrid_tot);
+        std::vector<double> hm(fo_acc), he(fo_acc), hv(fo_acc);
+        for (int s = 0; s < n; ++s)
+            if (hs[s].lewald)
+                spme_factors(hs[s].s, hs[s].order, hs[s].alpha, hs[s].box, hm.data() + hs[s].fac_off,
+                             he.data() + hs[s].fac_off, hv.data() + hs[s].fac_off);
+        mfac = dalloc<double>(fo_acc);
+        emf = dalloc<double>(fo_acc);
+        vmf = dalloc<double>(fo_acc);
+        CK(cudaMemcpy(mfac, hm.data(), fo_acc * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(emf, he.data(), fo_acc * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(vmf, hv.data(), fo_acc * sizeof(double), cudaMemcpyHostToDevice));
+        for (auto &fc : fft) {
+            int dims[3] = {fc.s, fc.s, fc.s};
+            const int rdist = fc.s * fc.s * fc.s, cdist = fc.s * fc.s * (fc.s / 2 + 1);
+            CKF(cufftPlanMany(&fc.fwd, 3, dims, nullptr, 1, rdist, nullptr, 1, cdist, CUFFT_D2Z, fc.count));
+            CKF(cufftPlanMany(&fc.bwd, 3, dims, nullptr, 1, cdist, nullptr, 1, rdist, CUFFT_Z2D, fc.count));
+            CKF(cufftSetStream(fc.fwd, st));
+            CKF(cufftSetStream(fc.bwd, st));
+        }
+        // influence work items
+        std::vector<int4> it;
+        for (int s = 0; s < n; ++s) {
+            if (!hs[s].lewald) continue;
+            const int e = hs[s].s;
+            const int nc = e * e * (e / 2 + 1);
+            hs[s].infl_off = (int)it.size();
+            for (int c = 0; c < nc; c += INFL_TILE) it.push_back(make_int4(s, c, std::min(nc, c + INFL_TILE), 0));
+            hs[s].ninfl = (int)it.size() - hs[s].infl_off;
+        }
+        ninfl = (int)it.size();
+        infl = dalloc<int4>(ninfl);
+        CK(cudaMemcpy(infl, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        ipart = dalloc<double>(2 * (size_t)ninfl);
+    }
+
+    // --- pair tables: per type pair, intervals from MOLSIM's ubuf ---
+    std::vector<PairTab> pt(pt_tot);
+    std::vector<int> pmap(std::max(1, ptmap_tot));
+    std::vector<double> vz, vc;
+    std::vector<unsigned short> vb;
+    std::vector<double> vmassip(type_tot), vmassp(type_tot), vf1(type_tot, 0.0), vf2(type_tot, 0.0);
+    for (int s = 0; s < n; ++s) {
+        const msg_params &p = P[s];
+        SysDev &S = hs[s];
+        int pidx = 0;
+        for (int it = 0; it < p.npt; ++it)
+            for (int jt = it; jt < p.npt; ++jt, ++pidx) {
+                pmap[S.ptmap_off + it * p.npt + jt] = S.pt_off + pidx;
+                pmap[S.ptmap_off + jt * p.npt + it] = S.pt_off + pidx;
+                PairTab &T = pt[S.pt_off + pidx];
+                T.k0 = (int)vz.size();
+                T.r2umin = p.r2umin[pidx];
+                T.r2atat = p.r2atat ? p.r2atat[pidx] : 0.0;
+                const int first = p.iubuflow[pidx] - 1;
+                if (first < 0 || first + 12 > p.nbuf) throw CudaError{MSG_ERR_ARG, "iubuflow outside ubuf"};
+                int k = 0;
+                for (;;) {
+                    const int b = first + 12 * k;
+                    if (b + 12 > p.nbuf) throw CudaError{MSG_ERR_ARG, "pair table does not reach r2umin"};
+                    vz.push_back(p.ubuf[b]);
+                    for (int c = 0; c < 12; ++c) vc.push_back(p.ubuf[b + c]);
+                    ++k;
+                    if (p.ubuf[b] <= T.r2umin) break;
+                }
+                T.nk = k;
+                // bucket starts
+                const double *z = vz.data() + T.k0;
+                T.z_hi = z[0];
+                T.z_lo = T.r2umin;
+                const double h = (T.z_hi > T.z_lo) ? (T.z_hi - T.z_lo) / MSG_NBUCKET : 1.0;
+                T.inv_h = 1.0 / h;
+                T.b0 = (int)vb.size();
+                for (int b = 0; b < MSG_NBUCKET; ++b) {
+                    const double zq = T.z_lo + (b + 2) * h;
+                    int kk = 0;
+                    while (kk < T.nk - 1 && zq < z[kk]) ++kk;
+                    vb.push_back((unsigned short)kk);
+                }
+            }
+        for (int t = 0; t < p.npt; ++t) {
+            vmassp[S.type_off + t] = p.masspt[t];
+            vmassip[S.type_off + t] = p.masspt[t] > 0.0 ? 1.0 / p.masspt[t] : 0.0;
+            if (p.bd_fac1) vf1[S.type_off + t] = p.bd_fac1[t];
+            if (p.bd_fac2) vf2[S.type_off + t] = p.bd_fac2[t];
+        }
+    }
+    ptab = dalloc<PairTab>(pt.size());
+    ptmap = dalloc<int>(pmap.size());
+    tz = dalloc<double>(vz.size());
+    tc = dalloc<double>(vc.size());
+    bst = dalloc<unsigned short>(vb.size());
+    massip = dalloc<double>(type_tot);
+    massp = dalloc<double>(type_tot);
+    fac1 = dalloc<double>(type_tot);
+    fac2 = dalloc<double>(type_tot);
+    CK(cudaMemcpy(ptab, pt.data(), pt.size() * sizeof(PairTab), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ptmap, pmap.data(), pmap.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(tz, vz.data(), vz.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(tc, vc.data(), vc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(bst, vb.data(), vb.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(massip, vmassip.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(massp, vmassp.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(fac1, vf1.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(fac2, vf2.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
+
+    // --- bonds: per-particle CSR in MOLSIM order (both ends) ---
+    {
+        std::vector<int> deg(ntot + 1, 0);
+        for (int s = 0; s < n; ++s) {
+            const msg_params &p = P[s];
+            for (int b = 0; b < p.nbond; ++b) {
+                const int a = p.bond_ij[2 * b] - 1, c = p.bond_ij[2 * b + 1] - 1;
+                if (a < 0 || c < 0 || a >= p.np || c >= p.np || a == c) throw CudaError{MSG_ERR_ARG, "bad bond"};
+                deg[hs[s].off + a + 1]++;
+                deg[hs[s].off + c + 1]++;
+            }
+        }
+        for (int i = 0; i < ntot; ++i) deg[i + 1] += deg[i];
+        std::vector<int> part(std::max(1, deg[ntot])), pw(std::max(1, deg[ntot]));
+        std::vector<double> kk(std::max(1, deg[ntot])), eq(std::max(1, deg[ntot]));
+        std::vector<int> fill(deg.begin(), deg.end() - 1);
+        for (int s = 0; s < n; ++s) {
+            const msg_params &p = P[s];
+            for (int b = 0; b < p.nbond; ++b) {
+                const int a = p.bond_ij[2 * b] - 1, c = p.bond_ij[2 * b + 1] - 1;
+                for (int e = 0; e < 2; ++e) {
+                    const int me = e ? c : a, other = e ? a : c;
+                    const int slot = fill[hs[s].off + me]++;
+                    part[slot] = other;
+                    pw[slot] = p.bond_p[b];
+                    kk[slot] = p.bond_k[b];
+                    eq[slot] = p.bond_eq[b];
+                }
+            }
+        }
+        bptr = dalloc<int>(ntot + 1);
+        bpart = dalloc<int>(part.size());
+        bpw = dalloc<int>(pw.size());
+        bk = dalloc<double>(kk.size());
+        beq = dalloc<double>(eq.size());
+        CK(cudaMemcpy(bptr, deg.data(), (ntot + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(bpart, part.data(), part.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(bpw, pw.data(), pw.size() * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(bk, kk.data(), kk.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(beq, eq.data(), eq.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+
+    // --- work lists ---
+    {
+        std::vector<Tile> a128, a32;
+        std::vector<int4> ch;
+        for (int s = 0; s < n; ++s) {
+            const SysDev &S = hs[s];
+            for (int i = 0; i < S.n; i += 128) a128.push_back(Tile{s, S.off + i, S.off + std::min(S.n, i + 128), 0});
+            for (int i = 0; i < S.n; i += 32) a32.push_back(Tile{s, S.off + i, S.off + std::min(S.n, i + 32), 0});
+            for (int i = 0; i < S.n; i += SK_CHUNK)
+                ch.push_back(make_int4(s, S.off + i, S.off + std::min(S.n, i + SK_CHUNK), 0));
+        }
+        this->t128 = dalloc<Tile>(a128.size());
+        this->t32 = dalloc<Tile>(a32.size());
+        chunks = dalloc<int4>(ch.size());
+        CK(cudaMemcpy(this->t128, a128.data(), a128.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(this->t32, a32.data(), a32.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+
+    // --- particles: MOLSIM order is the initial internal order ---
+    for (int b = 0; b < 2; ++b) {
+        pos[b] = dalloc<double4>(ntot);
+        vel[b] = dalloc<double4>(ntot);
+        acc[b] = dalloc<double4>(ntot);
+        dsum[b] = dalloc<double4>(ntot);
+        fo[b] = dalloc<double4>(ntot);
+        typ[b] = dalloc<int>(ntot);
+        orig[b] = dalloc<int>(ntot);
+    }
+    cellid = dalloc<int>(ntot);
+    inv = dalloc<int>(ntot);
+    sysid = dalloc<int>(ntot);
+    fsr = dalloc<double4>(ntot);
+    ftot = dalloc<double4>(ntot);
+    if (prec == MSG_PREC_MIXED) pos32 = dalloc<float4>(ntot);
+    {
+        std::vector<double4> hp(ntot);
+        std::vector<int> ht(ntot), ho(ntot), hsid(ntot);
+        for (int s = 0; s < n; ++s) {
+            const msg_params &p = P[s];
+            for (int i = 0; i < p.np; ++i) {
+                const int g = hs[s].off + i;
+                if (p.iptpn[i] < 1 || p.iptpn[i] > p.npt) throw CudaError{MSG_ERR_ARG, "iptpn out of range"};
+                hp[g] = make_double4(0.0, 0.0, 0.0, p.az[i]);
+                ht[g] = p.iptpn[i] - 1;
+                ho[g] = i;
+                hsid[g] = s;
+            }
+        }
+        CK(cudaMemcpy(pos[0], hp.data(), ntot * sizeof(double4), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(typ[0], ht.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(orig[0], ho.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        std::vector<int> idn(ntot);
+        for (int i = 0; i < ntot; ++i) idn[i] = i;
+        CK(cudaMemcpy(inv, idn.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(sysid, hsid.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        // until a system's first list build, its particles sit in its first cell
+        std::vector<int> hc(ntot);
+        for (int i = 0; i < ntot; ++i) hc[i] = hs[hsid[i]].cell_off;
+        CK(cudaMemcpy(cellid, hc.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    k0 = dalloc<uint32_t>(ntot);
+    v0 = dalloc<uint32_t>(ntot);
+    k1 = dalloc<uint32_t>(ntot);
+    v1 = dalloc<uint32_t>(ntot);
+    rhist = dalloc<uint32_t>((size_t)RS_BINS * ((ntot + RS_TILE - 1) / RS_TILE));
+    cstart = dalloc<int>(ncell_tot);
+    cend = dalloc<int>(ncell_tot);
+    nbl = dalloc<int>(nbl_tot);
+    nnb = dalloc<int>(ntot);
+    r2o = dalloc<double>(ntot);
+    skinout = dalloc<double>(2 * (size_t)n);
+    sc = dalloc<SkinChunk>(nchunk);
+    sysdone = dalloc<unsigned>(n);
+    flag = dalloc<int>(n);
+    nrebuild = dalloc<long long>(n);
+    ppart = dalloc<double>((size_t)nt32 * NPART_PAIR);
+    fpart = dalloc<double>((size_t)nt128 * NPART_FIN);
+    psurf = dalloc<double>((size_t)nt128 * 4);
+    esys = dalloc<double>((size_t)n * ESZ);
+    stepctr = dalloc<unsigned long long>(1);
+    sstep = dalloc<unsigned long long>(n);
+    rdone = dalloc<unsigned>(1);
+    errw = dalloc<ErrWord>(1);
+    if (!ipart) ipart = dalloc<double>(2);
+    dsys = dalloc<SysDev>(n);
+    CK(cudaMemcpy(dsys, hs.data(), n * sizeof(SysDev), cudaMemcpyHostToDevice));
+    CK(cudaDeviceSynchronize());
+}
+
+// ---------------------------------------------------------------------------
+// Kernel sequences.
+// ---------------------------------------------------------------------------
+void msg_handle::enqueue_rebuild()
+{
+    const int c = cur, o = 1 - cur;
+    k_rb_keys<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[c], orig[c], cellid, k0, v0);
+    const bool in1 = radix_sort_pairs(k0, v0, k1, v1, rhist, ntot, cell_bits, st);
+    const uint32_t *sk = in1 ? k1 : k0, *sv = in1 ? v1 : v0;
+    k_permute<<<nt128, 128, 0, st>>>(dsys, t128, flag, sk, sv, pos[c], pos[o], vel[c], vel[o], acc[c], acc[o],
+                                      dsum[c], dsum[o], fo[c], fo[o], typ[c], typ[o], orig[c], orig[o], cellid,
+                                      inv);
+    cur = o;
+    CK(cudaMemsetAsync(cstart, 0, sizeof(int) * ncell_tot, st));
+    CK(cudaMemsetAsync(cend, 0, sizeof(int) * ncell_tot, st));
+    k_cellrange<<<(ntot + 255) / 256, 256, 0, st>>>(cellid, sysid, flag, ntot, cstart, cend);
+    k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[cur], cellid, cstart, cend, nbl, nnb,
+                                                     ntot, errw);
+}
+
+template <int P>
+static void launch_spme(msg_handle *h)
+{
+    const int c = h->cur;
+    CK(cudaMemsetAsync(h->rgrid, 0, sizeof(double) * h->grid_tot, h->st));
+    k_spread_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->rgrid);
+    for (auto &f : h->fft)
+        CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
+    k_influence_fp64<<<h->ninfl, INFL_THREADS, 0, h->st>>>(h->dsys, h->infl, h->cgrid, h->mfac, h->emf, h->vmf,
+                                                          h->ipart);
+    for (auto &f : h->fft)
+        CKF(cufftExecZ2D(f.bwd, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off), h->rgrid + f.grid_off));
+}
+
+template <int P>
+static void launch_finalize(msg_handle *h, int mode)
+{
+    const int c = h->cur;
+    k_finalize_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->typ[c], h->orig[c], h->inv,
+                                                    h->rgrid, h->fsr, h->psurf, h->bptr, h->bpart, h->bk, h->beq,
+                                                    h->bpw, h->massip, h->massp, h->ftot, h->fo[c], h->vel[c],
+                                                    h->acc[c], h->fpart, mode, h->errw);
+}
+
+void msg_handle::enqueue_forces(int mode)
+{
+    const int c = cur;
+    k_pair_fp64<<<nt32, PAIR_THREADS, 0, st>>>(dsys, t32, pos[c], typ[c], nbl, nnb, ptmap, ptab, tz, tc, bst, fsr,
+                                               ppart, errw);
+    if (any_ewald) {
+        switch (order) {
+        case 4: launch_spme<4>(this); break;
+        case 5: launch_spme<5>(this); break;
+        default: launch_spme<6>(this); break;
+        }
+    }
+    switch (order) {
+    case 4: launch_finalize<4>(this, mode); break;
+    case 5: launch_finalize<5>(this, mode); break;
+    default: launch_finalize<6>(this, mode); break;
+    }
+}
+
+void msg_handle::enqueue_reduce(bool record)
+{
+    k_reduce<<<nsys, 256, 0, st>>>(dsys, ppart, ipart, fpart, psurf, esys, record ? hist : nullptr, hist_cap,
+                                   stepctr, sstep, rdone, nsys);
+}
+
+void msg_handle::enqueue_md_step(bool record)
+{
+    const int c = cur;
+    k_vv_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], vel[c], acc[c], dsum[c], orig[c], r2o, psurf, pos32);
+    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout);
+    enqueue_forces(1);
+    enqueue_reduce(record);
+    enqueue_rebuild();
+}
+
+void msg_handle::enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record)
+{
+    const int c = cur;
+    k_bd_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], fo[c], dsum[c], orig[c], typ[c], fac1, fac2, xin_step,
+                                    xout_step, seed, sstep, r2o, psurf, pos32);
+    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout);
+    enqueue_forces(0);
+    enqueue_reduce(record);
+    enqueue_rebuild();
+}
+
+int msg_handle::check()
+{
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    ErrWord e;
+    CK(cudaMemcpy(&e, errw, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e.code) {
+        static const char *names[] = {"ok", "r2 < r2umin (pair below the table minimum)", "table interval overrun",
+                                      "neighbour-list capacity exceeded", "cuda", "device timeout", "argument",
+                                      "non-finite force", "hard-core overlap"};
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s (system %d, particles %d, %d)",
+                      (e.code >= 0 && e.code <= 8) ? names[e.code] : "error", e.sys, e.i, e.j);
+        err = buf;
+        const int code = e.code;
+        CK(cudaMemset(errw, 0, sizeof(ErrWord)));
+        return code;
+    }
+    return MSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+#define API_BEGIN try {
+#define API_END                                       \
+    }                                                 \
+    catch (const CudaError &e) {                      \
+        if (h) h->err = e.what;                       \
+        return e.code;                                \
+    }
+
+static int create_impl(const msg_params *p, int32_t nsys, int32_t precision, msg_handle **out)
+{
+    if (!p || !out || nsys < 1 || (precision != MSG_PREC_FP64 && precision != MSG_PREC_MIXED)) return MSG_ERR_ARG;
+    msg_handle *h = new msg_handle();
+    try {
+        h->build(p, nsys, precision);
+        // initial neighbour lists: every system is rebuilt from its set-up order
+        std::vector<int> ones(nsys, 1);
+        CK(cudaMemcpy(h->flag, ones.data(), nsys * sizeof(int), cudaMemcpyHostToDevice));
+    } catch (const CudaError &e) {
+        std::fprintf(stderr, "msg_create: %s\n", e.what.c_str());
+        delete h;
+        *out = nullptr;
+        return e.code;
+    }
+    *out = h;
+    return MSG_OK;
+}
+
+extern "C" int msg_create(const msg_params *p, int32_t precision, msg_handle **out)
+{
+    return create_impl(p, 1, precision, out);
+}
+
+extern "C" int msg_create_batch(const msg_params *p, int32_t nsys, int32_t precision, msg_handle **out)
+{
+    return create_impl(p, nsys, precision, out);
+}
+
+extern "C" void msg_destroy(msg_handle *h) { delete h; }
+
+extern "C" const char *msg_last_error(const msg_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+extern "C" int32_t msg_nsys(const msg_handle *h) { return h ? h->nsys : 0; }
+
+extern "C" int msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    const SysDev &S = h->hs[isys];
+    h->ensure_stage(3 * (size_t)S.n);
+    const int c = h->cur, nb = (S.n + 255) / 256;
+    const double *src[3] = {ro, rod, rodd};
+    double4 *dst[3] = {h->pos[c], h->vel[c], h->acc[c]};
+    for (int k = 0; k < 3; ++k) {
+        if (!src[k]) continue;
+        h2d(h->stage, src[k], 3 * (size_t)S.n, h->st);
+        k_to_internal<<<nb, 256, 0, h->st>>>(h->stage, dst[k], h->inv, S.off, S.n, k == 0 ? 1 : 0);
+    }
+    if (ro) {
+        // positions changed: rebuild this system's list now (drosum is reset by the rebuild)
+        std::vector<int> f(h->nsys, 0);
+        f[isys] = 1;
+        h2d(h->flag, f.data(), h->nsys, h->st);
+        h->enqueue_rebuild();
+    }
+    return h->check();
+    API_END
+}
+
+extern "C" int msg_get_state(msg_handle *h, int32_t isys, double *ro, double *rod, double *rodd)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    const SysDev &S = h->hs[isys];
+    h->ensure_stage(3 * (size_t)S.n);
+    const int c = h->cur, nb = (S.n + 255) / 256;
+    double *dst[3] = {ro, rod, rodd};
+    const double4 *src[3] = {h->pos[c], h->vel[c], h->acc[c]};
+    for (int k = 0; k < 3; ++k) {
+        if (!dst[k]) continue;
+        k_to_molsim<<<nb, 256, 0, h->st>>>(src[k], h->stage, h->inv, S.off, S.n, 1.0);
+        CK(cudaMemcpyAsync(dst[k], h->stage, 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
+    }
+    return h->check();
+    API_END
+}
+
+extern "C" int msg_build_nlist(msg_handle *h, int32_t isys, int32_t *nneighpn, int32_t *jpnlist, int32_t maxnneigh,
+                               int64_t *npair)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    std::vector<int> f(h->nsys, 0);
+    f[isys] = 1;
+    h2d(h->flag, f.data(), h->nsys, h->st);
+    h->enqueue_rebuild();
+    int rc = h->check();
+    if (rc) return rc;
+    const SysDev &S = h->hs[isys];
+    if (npair) {
+        std::vector<int> nn(S.n);
+        CK(cudaMemcpy(nn.data(), h->nnb + S.off, S.n * sizeof(int), cudaMemcpyDeviceToHost));
+        long long tot = 0;
+        for (int v : nn) tot += v;
+        *npair = tot / 2;
+    }
+    if (nneighpn && jpnlist) {
+        if (maxnneigh < 1) return MSG_ERR_ARG;
+        int *dn = dalloc<int>(S.n);
+        int *dj = dalloc<int>((size_t)S.n * maxnneigh);
+        const int warps = 4;
+        k_export_nlist<<<(S.n + warps - 1) / warps, 32 * warps, warps * S.cap * sizeof(int), h->st>>>(
+            h->dsys, isys, h->nbl, h->nnb, h->orig[h->cur], dn, dj, maxnneigh, h->errw);
+        rc = h->check();
+        if (!rc) {
+            CK(cudaMemcpy(nneighpn, dn, S.n * sizeof(int), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(jpnlist, dj, (size_t)S.n * maxnneigh * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        cudaFree(dn);
+        cudaFree(dj);
+        return rc;
+    }
+    return MSG_OK;
+    API_END
+}
+
+static void fill_energy(const double *e, int natat, msg_energy *out)
+{
+    std::memset(out, 0, sizeof(*out));
+    out->utot = e[0];
+    out->utwob0 = e[1];
+    for (int p = 0; p < natat && p < 10; ++p) out->utwob[p] = e[2 + p];
+    out->urec = e[12];
+    out->ubond = e[13];
+    out->virial = e[14];
+    out->ekin = e[15];
+}
+
+extern "C" int msg_utotal(msg_handle *h, int32_t isys, double *force, double *forceo, msg_energy *e)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    h->enqueue_forces(0);
+    h->enqueue_reduce(false);
+    int rc = h->check();
+    if (rc) return rc;
+    const SysDev &S = h->hs[isys];
+    h->ensure_stage(3 * (size_t)S.n);
+    const int nb = (S.n + 255) / 256;
+    if (force) {
+        k_to_molsim<<<nb, 256, 0, h->st>>>(h->ftot, h->stage, h->inv, S.off, S.n, 1.0);
+        CK(cudaMemcpyAsync(force, h->stage, 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
+    }
+    if (forceo) {
+        k_to_molsim<<<nb, 256, 0, h->st>>>(h->fo[h->cur], h->stage, h->inv, S.off, S.n, 1.0);
+        CK(cudaMemcpyAsync(forceo, h->stage, 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
+    }
+    if (e) {
+        double he[ESZ];
+        CK(cudaMemcpyAsync(he, h->esys + (size_t)isys * ESZ, sizeof(he), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        fill_energy(he, S.natat, e);
+    }
+    return h->check();
+    API_END
+}
+
+extern "C" int msg_get_linacc(msg_handle *h)
+{
+    if (!h) return MSG_ERR_ARG;
+    API_BEGIN
+    const int c = h->cur;
+    k_linacc<<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->fo[c], h->typ[c], h->massip, h->acc[c]);
+    return h->check();
+    API_END
+}
+
+static void prepare_hist(msg_handle *h, int nsteps)
+{
+    if (nsteps > h->hist_cap) {
+        if (h->hist) cudaFree(h->hist);
+        h->hist = dalloc<double>((size_t)nsteps * h->nsys * ESZ);
+        h->hist_cap = nsteps;
+    }
+    CK(cudaMemsetAsync(h->stepctr, 0, sizeof(unsigned long long), h->st));
+}
+
+static void copy_hist(msg_handle *h, int nsteps, int isys, msg_energy *e)
+{
+    std::vector<double> buf((size_t)nsteps * h->nsys * ESZ);
+    CK(cudaMemcpyAsync(buf.data(), h->hist, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int k = 0; k < nsteps; ++k) fill_energy(&buf[((size_t)k * h->nsys + isys) * ESZ], h->hs[isys].natat, &e[k]);
+}
+
+extern "C" int msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energy *e)
+{
+    if (!h || nsteps < 0 || (e && (isys < 0 || isys >= h->nsys))) return MSG_ERR_ARG;
+    API_BEGIN
+    const bool rec = e != nullptr;
+    if (rec) prepare_hist(h, nsteps);
+    for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(rec);
+    int rc = h->check();
+    if (rc) return rc;
+    if (rec) copy_hist(h, nsteps, isys, e);
+    return MSG_OK;
+    API_END
+}
+
+extern "C" int msg_bd_step(msg_handle *h, int32_t nsteps, uint64_t seed, int32_t isys, const double *xi,
+                           double *xi_out, msg_energy *e)
+{
+    if (!h || nsteps < 0 || ((xi || xi_out || e) && (isys < 0 || isys >= h->nsys))) return MSG_ERR_ARG;
+    if (!h->has_bd) {
+        h->err = "bd_fac1/bd_fac2 were not given at creation";
+        return MSG_ERR_ARG;
+    }
+    API_BEGIN
+    const bool rec = e != nullptr;
+    if (rec) prepare_hist(h, nsteps);
+    const size_t per = 3 * (size_t)h->ntot;
+    if ((xi || xi_out) && per * std::max(1, nsteps) > h->xin_n) {
+        if (h->xin) cudaFree(h->xin);
+        h->xin_n = per * std::max(1, nsteps);
+        h->xin = dalloc<double>(h->xin_n);
+    }
+    const SysDev &S = h->hs[std::max(0, isys)];
+    if (xi) {
+        for (int k = 0; k < nsteps; ++k)
+            h2d(h->xin + k * per + 3 * (size_t)S.off, xi + (size_t)k * 3 * S.n, 3 * (size_t)S.n, h->st);
+    }
+    for (int k = 0; k < nsteps; ++k)
+        h->enqueue_bd_step(seed, xi ? h->xin + k * per : nullptr, xi_out ? h->xin + k * per : nullptr, rec);
+    int rc = h->check();
+    if (rc) return rc;
+    if (xi_out) {
+        std::vector<double> buf(per);
+        for (int k = 0; k < nsteps; ++k) {
+            CK(cudaMemcpy(buf.data(), h->xin + k * per, per * sizeof(double), cudaMemcpyDeviceToHost));
+            std::memcpy(xi_out + (size_t)k * 3 * S.n, buf.data() + 3 * (size_t)S.off, 3 * sizeof(double) * S.n);
+        }
+    }
+    if (rec) copy_hist(h, nsteps, isys, e);
+    return MSG_OK;
+    API_END
+}
+
+extern "C" int64_t msg_nrebuild(const msg_handle *h, int32_t isys)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return -1;
+    long long v = 0;
+    if (cudaMemcpy(&v, h->nrebuild + isys, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return v;
+}

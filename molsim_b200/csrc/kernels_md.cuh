@@ -1,0 +1,587 @@
+// kernels_md.cuh -- integrator, skin test, list rebuild and API-boundary kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace msg {
+
+// ---------------------------------------------------------------------------
+// Velocity Verlet, position half (Src/md.F90:286-298):
+//   drostep = dt*rod + (dt*dt/2)*rodd;  ro += drostep;  PBC(ro)
+// plus the drosum accumulation of NList (Src/nlist.F90:603-604), the skin
+// r^2 written in MOLSIM order, the surface-term partial sums and the FP32
+// position mirror.  Products and sums are rounded separately (no FMA) so
+// positions match MOLSIM's arithmetic.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_vv_pos(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                               double4 *__restrict__ pos, const double4 *__restrict__ vel,
+                                               const double4 *__restrict__ acc, double4 *__restrict__ dsum,
+                                               const int *__restrict__ orig, double *__restrict__ r2o,
+                                               double *__restrict__ psurf, float4 *__restrict__ pos32)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    const int i = T.i0 + threadIdx.x;
+    double qx = 0.0, qy = 0.0, qz = 0.0;
+    if (i < T.i1) {
+        const double dt = S.dt, fac = __dmul_rn(0.5, __dmul_rn(dt, dt));
+        double4 x = pos[i];
+        const double4 v = vel[i], a = acc[i];
+        double4 d = dsum[i];
+        const double sx = __dadd_rn(__dmul_rn(dt, v.x), __dmul_rn(fac, a.x));
+        const double sy = __dadd_rn(__dmul_rn(dt, v.y), __dmul_rn(fac, a.y));
+        const double sz = __dadd_rn(__dmul_rn(dt, v.z), __dmul_rn(fac, a.z));
+        x.x = pbc_wrap(__dadd_rn(x.x, sx), S.half[0], S.box[0], S.boxi[0]);
+        x.y = pbc_wrap(__dadd_rn(x.y, sy), S.half[1], S.box[1], S.boxi[1]);
+        x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
+        pos[i] = x;
+        d.x = __dadd_rn(d.x, sx);
+        d.y = __dadd_rn(d.y, sy);
+        d.z = __dadd_rn(d.z, sz);
+        dsum[i] = d;
+        r2o[S.off + orig[i]] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
+        if (pos32) pos32[i] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+        qx = x.w * x.x;
+        qy = x.w * x.y;
+        qz = x.w * x.z;
+    }
+    if (psurf && S.lsurf) {
+        __shared__ double red[3][4];
+        qx = warp_sum(qx);
+        qy = warp_sum(qy);
+        qz = warp_sum(qz);
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) { red[0][w] = qx; red[1][w] = qy; red[2][w] = qz; }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double s = 0.0;
+            for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
+            psurf[blockIdx.x * 4 + threadIdx.x] = s;
+        }
+    }
+}
+
+// Philox4x32-10 (Salmon et al., SC'11) counter-based generator.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+// Three FP32 standard normals for (seed, particle, step) by Box-Muller.
+__device__ __forceinline__ float3 gauss3(uint64_t seed, uint32_t particle, uint32_t step)
+{
+    const uint4 r = philox4x32_10(make_uint4(particle, step, 0x4d4f4c53u, 0u),
+                                  make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    const float inv = 2.3283064365386963e-10f;   // 2^-32
+    const float u1 = ((float)r.x + 1.0f) * inv, u2 = (float)r.y * inv;
+    const float u3 = ((float)r.z + 1.0f) * inv, u4 = (float)r.w * inv;
+    const float m1 = sqrtf(-2.0f * logf(u1)), m2 = sqrtf(-2.0f * logf(u3));
+    float s1, c1, s2, c2;
+    sincospif(2.0f * u2, &s1, &c1);
+    sincospif(2.0f * u4, &s2, &c2);
+    return make_float3(m1 * c1, m1 * s1, m2 * c2);
+}
+
+// Ermak-McCammon step (Src/bd.F90:142-152): drostep = fac1*forceo + fac2*xi,
+// ro += drostep, PBC.  xi is caller noise in MOLSIM order (xin) or Philox noise.
+__global__ void __launch_bounds__(128) k_bd_pos(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                               double4 *__restrict__ pos, const double4 *__restrict__ forceo,
+                                               double4 *__restrict__ dsum, const int *__restrict__ orig,
+                                               const int *__restrict__ typ, const double *__restrict__ fac1,
+                                               const double *__restrict__ fac2, const double *__restrict__ xin,
+                                               double *__restrict__ xout, uint64_t seed,
+                                               const unsigned long long *__restrict__ sstep,
+                                               double *__restrict__ r2o, double *__restrict__ psurf,
+                                               float4 *__restrict__ pos32)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    const int i = T.i0 + threadIdx.x;
+    double qx = 0.0, qy = 0.0, qz = 0.0;
+    if (i < T.i1) {
+        const int o = orig[i], t = S.type_off + typ[i];
+        const size_t g = (size_t)S.off + o;
+        double xi0, xi1, xi2;
+        if (xin) {
+            xi0 = xin[3 * g];
+            xi1 = xin[3 * g + 1];
+            xi2 = xin[3 * g + 2];
+        } else {
+            const float3 z = gauss3(seed ^ S.seed, (uint32_t)o, (uint32_t)sstep[T.sys]);
+            xi0 = z.x;
+            xi1 = z.y;
+            xi2 = z.z;
+        }
+        if (xout) {
+            xout[3 * g] = xi0;
+            xout[3 * g + 1] = xi1;
+            xout[3 * g + 2] = xi2;
+        }
+        const double f1 = fac1[t], f2 = fac2[t];
+        const double4 f = forceo[i];
+        double4 x = pos[i], d = dsum[i];
+        const double sx = __dadd_rn(__dmul_rn(f1, f.x), __dmul_rn(f2, xi0));
+        const double sy = __dadd_rn(__dmul_rn(f1, f.y), __dmul_rn(f2, xi1));
+        const double sz = __dadd_rn(__dmul_rn(f1, f.z), __dmul_rn(f2, xi2));
+        x.x = pbc_wrap(__dadd_rn(x.x, sx), S.half[0], S.box[0], S.boxi[0]);
+        x.y = pbc_wrap(__dadd_rn(x.y, sy), S.half[1], S.box[1], S.boxi[1]);
+        x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
+        pos[i] = x;
+        d.x = __dadd_rn(d.x, sx);
+        d.y = __dadd_rn(d.y, sy);
+        d.z = __dadd_rn(d.z, sz);
+        dsum[i] = d;
+        r2o[S.off + o] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
+        if (pos32) pos32[i] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
+        qx = x.w * x.x;
+        qy = x.w * x.y;
+        qz = x.w * x.z;
+    }
+    if (psurf && S.lsurf) {
+        __shared__ double red[3][4];
+        qx = warp_sum(qx);
+        qy = warp_sum(qy);
+        qz = warp_sum(qz);
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) { red[0][w] = qx; red[1][w] = qy; red[2][w] = qz; }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double s = 0.0;
+            for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
+            psurf[blockIdx.x * 4 + threadIdx.x] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Skin test of NList (Src/nlist.F90:600-613), reproduced exactly including its
+// running "second maximum": r2max2 only collects values that were not a new
+// running maximum when visited in MOLSIM order.  Chunks of 1024 MOLSIM indices
+// are summarised in parallel (block max B, non-record max A, the chunk's
+// record values); the last chunk of each system to finish combines them:
+// a chunk record R counts towards r2max2 iff R <= the prefix maximum P before
+// the chunk, so the chunk contributes max(A, max{R <= P}).
+// ---------------------------------------------------------------------------
+constexpr int SK_CHUNK = 1024, SK_THREADS = 256, SK_REC = 32;
+struct SkinChunk {
+    double bmax, amax;
+    int nrec, pad;
+    double rec[SK_REC];
+};
+
+// Block-wide exclusive prefix max over 256 threads (values >= 0).
+__device__ __forceinline__ double block_excl_max(double v, double *sm)
+{
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    double inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc = fmax(inc, y);
+    }
+    if (lane == 31) sm[w] = inc;
+    __syncthreads();
+    double pre = 0.0;
+    for (int k = 0; k < w; ++k) pre = fmax(pre, sm[k]);
+    double exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) exc = 0.0;
+    __syncthreads();
+    return fmax(pre, exc);
+}
+
+__device__ __forceinline__ double block_max(double v, double *sm)
+{
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    for (int k = 0; k < SK_THREADS / 32; ++k) r = fmax(r, sm[k]);
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ int block_excl_sum_int(int v, int *sm, int *total)
+{
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) sm[w] = inc;
+    __syncthreads();
+    int pre = 0, tot = 0;
+    for (int k = 0; k < SK_THREADS / 32; ++k) {
+        if (k < w) pre += sm[k];
+        tot += sm[k];
+    }
+    __syncthreads();
+    *total = tot;
+    return pre + inc - v;
+}
+
+// Contribution of one chunk to r2max2 given the prefix max P before it; all
+// threads of the block call this with the same arguments.
+__device__ double chunk_nonrecord_max(const double *r2, int o0, int o1, double P, double *smd)
+{
+    const int t = threadIdx.x;
+    double v[4], run = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int o = o0 + 4 * t + k;
+        v[k] = (o < o1) ? r2[o] : 0.0;
+    }
+    double tmax = fmax(fmax(v[0], v[1]), fmax(v[2], v[3]));
+    double pre = fmax(P, block_excl_max(tmax, smd));
+    double best = 0.0;
+    run = pre;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int o = o0 + 4 * t + k;
+        if (o < o1) {
+            if (v[k] > run) run = v[k];
+            else best = fmax(best, v[k]);
+        }
+    }
+    return block_max(best, smd);
+}
+
+__global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ sysv, const int4 *__restrict__ chunks,
+                                                    const double *__restrict__ r2o, SkinChunk *__restrict__ sc,
+                                                    unsigned *__restrict__ sysdone, int *__restrict__ flag,
+                                                    long long *__restrict__ nrebuild, double *__restrict__ skinout)
+{
+    __shared__ double smd[SK_THREADS / 32];
+    __shared__ int smi[SK_THREADS / 32];
+    __shared__ bool last;
+    const int4 C = chunks[blockIdx.x];   // sys, o0 (global), o1 (global), first chunk of system
+    const int s = C.x;
+    const SysDev &S = sysv[s];
+    const int t = threadIdx.x;
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int o = C.y + 4 * t + k;
+        v[k] = (o < C.z) ? r2o[o] : 0.0;
+    }
+    double tmax = fmax(fmax(v[0], v[1]), fmax(v[2], v[3]));
+    double run = block_excl_max(tmax, smd);
+    double amax = 0.0;
+    int nrec = 0;
+    double recv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int o = C.y + 4 * t + k;
+        if (o < C.z) {
+            if (v[k] > run) { run = v[k]; recv[nrec++] = v[k]; }
+            else amax = fmax(amax, v[k]);
+        }
+    }
+    int total;
+    const int roff = block_excl_sum_int(nrec, smi, &total);
+    SkinChunk &out = sc[blockIdx.x];
+    for (int k = 0; k < nrec; ++k)
+        if (roff + k < SK_REC) out.rec[roff + k] = recv[k];
+    const double bm = block_max(tmax, smd);
+    const double am = block_max(amax, smd);
+    if (t == 0) {
+        out.bmax = bm;
+        out.amax = am;
+        out.nrec = total;
+        __threadfence();
+        last = (atomicAdd(&sysdone[s], 1u) == (unsigned)(S.nchunk - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // Combine the system's chunks in MOLSIM order, 256 chunks per pass.
+    const int c0 = S.chunk_off;
+    double carry = 0.0, m2 = 0.0;
+    __shared__ int novf;
+    for (int cb = 0; cb < S.nchunk; cb += SK_THREADS) {
+        const int c = cb + t;
+        double bmx = 0.0;
+        if (c < S.nchunk) bmx = __ldcg(&sc[c0 + c].bmax);
+        const double P = fmax(carry, block_excl_max(bmx, smd));
+        double contrib = 0.0;
+        bool ovf = false;
+        if (c < S.nchunk) {
+            const int nr = __ldcg(&sc[c0 + c].nrec);
+            if (nr > SK_REC) {
+                ovf = true;
+            } else {
+                contrib = __ldcg(&sc[c0 + c].amax);
+                for (int k = 0; k < nr; ++k) {
+                    const double R = __ldcg(&sc[c0 + c].rec[k]);
+                    if (R <= P) contrib = fmax(contrib, R);
+                }
+            }
+        }
+        m2 = fmax(m2, block_max(contrib, smd));
+        // chunks with more records than stored are re-scanned by the whole block
+        if (t == 0) novf = 0;
+        __syncthreads();
+        if (ovf) atomicAdd(&novf, 1);
+        __syncthreads();
+        if (novf) {
+            for (int k = 0; k < SK_THREADS && cb + k < S.nchunk; ++k) {
+                __shared__ int isovf;
+                __shared__ double Pk;
+                if (t == k) { isovf = ovf ? 1 : 0; Pk = P; }
+                __syncthreads();
+                if (isovf) {
+                    const int o0 = S.off + (cb + k) * SK_CHUNK, o1 = min(S.off + S.n, o0 + SK_CHUNK);
+                    m2 = fmax(m2, chunk_nonrecord_max(r2o, o0, o1, Pk, smd));
+                }
+                __syncthreads();
+            }
+        }
+        carry = fmax(carry, block_max(bmx, smd));
+    }
+    if (t == 0) {
+        const int rebuild = (sqrt(carry) + sqrt(m2) > S.drnlist) ? 1 : 0;
+        flag[s] = rebuild;
+        if (rebuild) nrebuild[s] += 1;
+        if (skinout) { skinout[2 * s] = carry; skinout[2 * s + 1] = m2; }
+        sysdone[s] = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Verlet-cell rebuild.  Keys are global cell ids; rebuilt systems enter the
+// stable sort in MOLSIM order, other systems in their current order with their
+// current cell ids, so the sort leaves them in place.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int cell_coord(double x, double half, double boxi, int nc)
+{
+    int c = (int)floor((x + half) * boxi * (double)nc);
+    return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+}
+
+__global__ void __launch_bounds__(128) k_rb_keys(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                const int *__restrict__ flag, const double4 *__restrict__ pos,
+                                                const int *__restrict__ orig, const int *__restrict__ cellid,
+                                                uint32_t *__restrict__ key, uint32_t *__restrict__ val)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    const int i = T.i0 + threadIdx.x;
+    if (i >= T.i1) return;
+    if (flag[T.sys]) {
+        const double4 x = pos[i];
+        const int cx = cell_coord(x.x, S.half[0], S.boxi[0], S.ncell[0]);
+        const int cy = cell_coord(x.y, S.half[1], S.boxi[1], S.ncell[1]);
+        const int cz = cell_coord(x.z, S.half[2], S.boxi[2], S.ncell[2]);
+        const int q = S.off + orig[i];
+        key[q] = (uint32_t)(S.cell_off + (cz * S.ncell[1] + cy) * S.ncell[0] + cx);
+        val[q] = (uint32_t)i;
+    } else {
+        key[i] = (uint32_t)cellid[i];
+        val[i] = (uint32_t)i;
+    }
+}
+
+// Gather every per-particle array into the sorted order (double buffers).
+__global__ void __launch_bounds__(128) k_permute(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                const int *__restrict__ flag, const uint32_t *__restrict__ skey,
+                                                const uint32_t *__restrict__ sval,
+                                                const double4 *__restrict__ pos0, double4 *__restrict__ pos1,
+                                                const double4 *__restrict__ vel0, double4 *__restrict__ vel1,
+                                                const double4 *__restrict__ acc0, double4 *__restrict__ acc1,
+                                                const double4 *__restrict__ dsum0, double4 *__restrict__ dsum1,
+                                                const double4 *__restrict__ fo0, double4 *__restrict__ fo1,
+                                                const int *__restrict__ typ0, int *__restrict__ typ1,
+                                                const int *__restrict__ orig0, int *__restrict__ orig1,
+                                                int *__restrict__ cellid, int *__restrict__ inv)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    const int j = T.i0 + threadIdx.x;
+    if (j >= T.i1) return;
+    const int i = (int)sval[j];
+    const bool rb = flag[T.sys] != 0;
+    pos1[j] = pos0[i];
+    vel1[j] = vel0[i];
+    acc1[j] = acc0[i];
+    fo1[j] = fo0[i];
+    dsum1[j] = rb ? make_double4(0.0, 0.0, 0.0, 0.0) : dsum0[i];
+    typ1[j] = typ0[i];
+    const int o = orig0[i];
+    orig1[j] = o;
+    cellid[j] = (int)skey[j];
+    inv[S.off + o] = j;
+}
+
+__global__ void k_cellrange(const int *__restrict__ cellid, const int *__restrict__ sys,
+                            const int *__restrict__ flag, int n, int *__restrict__ cstart, int *__restrict__ cend)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n || !flag[sys[j]]) return;
+    const int c = cellid[j];
+    if (j == 0 || cellid[j - 1] != c) cstart[c] = j;
+    if (j == n - 1 || cellid[j + 1] != c) cend[c] = j + 1;
+}
+
+// Stencil of neighbour cells along one dimension: the three cells c-1, c, c+1
+// (periodic) when there are at least three, otherwise every cell once.
+__device__ __forceinline__ int stencil1(int c, int nc, int *out)
+{
+    if (nc >= 3) {
+        out[0] = (c + nc - 1) % nc;
+        out[1] = c;
+        out[2] = (c + 1) % nc;
+        return 3;
+    }
+    for (int k = 0; k < nc; ++k) out[k] = k;
+    return nc;
+}
+
+// Full Verlet list, one warp per particle: every j != i in the stencil with
+// r2 < (rcut+drnlist)^2 (SetVListMD's test, Src/nlist.F90:746-751), compacted
+// with a warp ballot.  Rows are ordered by stencil cell, then by MOLSIM index.
+__global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, const int *__restrict__ sys,
+                                              const int *__restrict__ flag, const double4 *__restrict__ pos,
+                                              const int *__restrict__ cellid, const int *__restrict__ cstart,
+                                              const int *__restrict__ cend, int *__restrict__ nbl,
+                                              int *__restrict__ nnb, int ntot, ErrWord *err)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= ntot) return;
+    const int s = sys[i];
+    if (!flag[s]) return;
+    const SysDev &S = sysv[s];
+    const double4 xi = pos[i];
+    const int c = cellid[i] - S.cell_off;
+    const int cx = c % S.ncell[0], cy = (c / S.ncell[0]) % S.ncell[1], cz = c / (S.ncell[0] * S.ncell[1]);
+    int sx[3], sy[3], sz[3];
+    const int nx = stencil1(cx, S.ncell[0], sx), ny = stencil1(cy, S.ncell[1], sy), nz = stencil1(cz, S.ncell[2], sz);
+    int *row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
+    int count = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int a = 0; a < nz; ++a)
+        for (int b = 0; b < ny; ++b)
+            for (int e = 0; e < nx; ++e) {
+                const int cc = S.cell_off + (sz[a] * S.ncell[1] + sy[b]) * S.ncell[0] + sx[e];
+                const int j0 = cstart[cc], j1 = cend[cc];
+                for (int jb = j0; jb < j1; jb += 32) {
+                    const int j = jb + lane;
+                    bool ok = false;
+                    if (j < j1 && j != i) {
+                        const double4 xj = pos[j];
+                        double dx = __dsub_rn(xi.x, xj.x), dy = __dsub_rn(xi.y, xj.y), dz = __dsub_rn(xi.z, xj.z);
+                        ok = pbcr2_exact(dx, dy, dz, S) < S.rs2cut;
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                    if (ok) {
+                        const int slot = count + __popc(bal & lt);
+                        if (slot < S.cap) row[slot] = j;
+                    }
+                    count += __popc(bal);
+                }
+            }
+    if (lane == 0) {
+        nnb[i] = min(count, S.cap);
+        if (count > S.cap) raise_error(err, 3, s, i, count);
+    }
+}
+
+// MOLSIM-layout export of one system's list: partners owned by the parity
+// rule of SetVListMD (Src/nlist.F90:741-744), 1-based, ascending per row.
+__global__ void k_export_nlist(const SysDev *__restrict__ sysv, int s, const int *__restrict__ nbl,
+                               const int *__restrict__ nnb, const int *__restrict__ orig,
+                               int *__restrict__ nneigh_out, int *__restrict__ jp_out, int maxn,
+                               ErrWord *err)
+{
+    extern __shared__ int buf[];
+    const SysDev &S = sysv[s];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int li = blockIdx.x * (blockDim.x >> 5) + w;
+    if (li >= S.n) return;
+    int *mine = buf + w * S.cap;
+    const int i = S.off + li;
+    const int ip = orig[i] + 1;
+    const int *row = nbl + S.nbl_off + (long long)li * S.cap;
+    const int n = nnb[i];
+    const unsigned lt = (1u << lane) - 1u;
+    int cnt = 0;
+    for (int kb = 0; kb < n; kb += 32) {
+        const int k = kb + lane;
+        int jp = 0;
+        bool ok = false;
+        if (k < n) {
+            jp = orig[row[k]] + 1;
+            const int itemp = (ip + jp) % 2;
+            ok = !((ip < jp && itemp == 0) || (ip > jp && itemp != 0));
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) mine[cnt + __popc(bal & lt)] = jp;
+        cnt += __popc(bal);
+    }
+    __syncwarp();
+    if (cnt > maxn) {
+        if (lane == 0) raise_error(err, 3, s, ip, cnt);
+        return;
+    }
+    for (int k = lane; k < cnt; k += 32) {
+        const int v = mine[k];
+        int r = 0;
+        for (int m = 0; m < cnt; ++m) r += (mine[m] < v);
+        jp_out[(long long)(ip - 1) * maxn + r] = v;
+    }
+    if (lane == 0) nneigh_out[ip - 1] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// API boundary: MOLSIM order <-> internal order.
+// ---------------------------------------------------------------------------
+__global__ void k_to_internal(const double *__restrict__ src, double4 *__restrict__ dst, const int *__restrict__ inv,
+                              int off, int n, int keep_w)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const int i = inv[off + o];
+    double4 v = dst[i];
+    v.x = src[3 * o];
+    v.y = src[3 * o + 1];
+    v.z = src[3 * o + 2];
+    if (!keep_w) v.w = 0.0;
+    dst[i] = v;
+}
+
+__global__ void k_to_molsim(const double4 *__restrict__ src, double *__restrict__ dst, const int *__restrict__ inv,
+                            int off, int n, double scale)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const double4 v = src[inv[off + o]];
+    dst[3 * o] = v.x * scale;
+    dst[3 * o + 1] = v.y * scale;
+    dst[3 * o + 2] = v.z * scale;
+}
+
+// rodd = massip * forceo (GetLinAcc, Src/md.F90:601-617)
+__global__ void k_linacc(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ fo,
+                         const int *__restrict__ typ, const double *__restrict__ massip, double4 *__restrict__ acc)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    const int i = T.i0 + threadIdx.x;
+    if (i >= T.i1) return;
+    const double mi = massip[S.type_off + typ[i]];
+    const double4 f = fo[i];
+    acc[i] = make_double4(mi * f.x, mi * f.y, mi * f.z, 0.0);
+}
+
+}  // namespace msg

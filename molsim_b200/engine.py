@@ -1,0 +1,202 @@
+"""Host-side mirror of MOLSIM's force/energy entry points over the C-ABI.
+
+The class `Engine` holds one library handle (one or many systems) and exposes
+the reference's routine names: `SetVList` (Src/nlist.F90:686), `UTotal`
+(Src/energy.F90:280), `GetLinAcc` (Src/md.F90:601), `VelVer` (Src/md.F90:252,
+with GetKinEnergy and NList after every step) and `BDStep` (Src/bd.F90:120,
+followed by UTotal and NList).  Errors raise `MolsimGpuError` carrying the
+status code of the Stop() site the reference would have hit.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import MsgEnergy, MsgParams, MsgTabParams, f64p, i32p
+
+
+class MolsimGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (status %d): %s" % (_lib.STATUS.get(code, "error"), code, msg))
+        self.code = code
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def rcut_to_alpha(uewaldtol, q2sum, epsi_four_pi, boxlenshort, rcut):
+    """RcutToAlpha (Src/energy.F90:7090-7105)."""
+    st = C.c_int32()
+    a = _lib.lib().msg_rcut_to_alpha(uewaldtol, q2sum, epsi_four_pi, boxlenshort, rcut, C.byref(st))
+    if st.value:
+        raise MolsimGpuError(st.value, "RcutToAlpha did not converge")
+    return a
+
+
+def pot_tab(sysd, ualpha, nbuf=100000):
+    """MOLSIM's pair table (PotTwoBodyTab1/2/3, Src/potential.F90:868-1135) for the (1,6,12)
+    potential of the system's types."""
+    npt = int(sysd["npt"])
+    natat = npt * (npt + 1) // 2
+    keep = [np.ascontiguousarray(sysd[k], np.float64) for k in ("zat", "sigat", "epsat")]
+    tp = MsgTabParams(npt, _p(keep[0], C.c_double), _p(keep[1], C.c_double), _p(keep[2], C.c_double),
+                      sysd["rcut"], ualpha, sysd["epsi_four_pi"], int(sysd["lewald"]), int(sysd["lljcut"]),
+                      sysd["ljrcut"], sysd["ljushift"], sysd["r2uminin"], sysd["utoltab"], sysd["ftoltab"],
+                      sysd["umaxtab"], sysd["fmaxtab"], sysd["rumaxfac"])
+    ubuf = np.zeros(nbuf)
+    iub = np.zeros(natat, np.int32)
+    nug = np.zeros(natat, np.int32)
+    r2umin = np.zeros(natat)
+    nused = C.c_int32()
+    rc = _lib.lib().msg_pot_tab(C.byref(tp), _p(ubuf, C.c_double), nbuf, _p(iub, C.c_int32), _p(nug, C.c_int32),
+                                _p(r2umin, C.c_double), C.byref(nused))
+    if rc:
+        raise MolsimGpuError(rc, "msg_pot_tab")
+    return dict(ubuf=ubuf[:nused.value].copy(), iubuflow=iub, nugrid=nug, r2umin=r2umin)
+
+
+def prepare(sysd):
+    """Derive alpha (IOPotTwoBody -> EwaldSetup, iewaldopt=3) and the pair table."""
+    q2sum = float(np.mean(np.asarray(sysd["az"], np.float64) ** 2))
+    alpha = rcut_to_alpha(sysd["uewaldtol"], q2sum, sysd["epsi_four_pi"], min(sysd["boxlen"]), sysd["rcut"])
+    tab = pot_tab(sysd, alpha)
+    natat = sysd["npt"] * (sysd["npt"] + 1) // 2
+    tab["r2atat"] = np.zeros(natat)
+    tab["ualpha"] = alpha
+    return tab
+
+
+class Engine:
+    """One library handle for `systems` (a list of system dicts, see systems.py) with their
+    tables (`tables[k]` from `prepare` or from a caller such as the oracle)."""
+
+    def __init__(self, systems, tables=None, precision="fp64", maxnneigh=0):
+        if isinstance(systems, dict):
+            systems = [systems]
+        if tables is None:
+            tables = [prepare(s) for s in systems]
+        elif isinstance(tables, dict):
+            tables = [tables]
+        self.systems = systems
+        self.tables = tables
+        self.nsys = len(systems)
+        self.natat = [s["npt"] * (s["npt"] + 1) // 2 for s in systems]
+        self._keep = []
+        arr = (MsgParams * self.nsys)()
+        for k, (s, t) in enumerate(zip(systems, tables)):
+            arr[k] = self._params(s, t, maxnneigh)
+        prec = _lib.MSG_PREC_MIXED if precision == "mixed" else _lib.MSG_PREC_FP64
+        h = C.c_void_p()
+        L = _lib.lib()
+        rc = L.msg_create_batch(arr, self.nsys, prec, C.byref(h)) if self.nsys > 1 else \
+            L.msg_create(arr, prec, C.byref(h))
+        if rc:
+            raise MolsimGpuError(rc, "msg_create failed")
+        self.h = h
+        for k, s in enumerate(systems):
+            self.set_state(k, s["ro"], s.get("rod"), s.get("rodd"))
+
+    def _params(self, s, t, maxnneigh):
+        k = {}
+        k["iptpn"] = np.ascontiguousarray(s["iptpn"], np.int32)
+        k["az"] = np.ascontiguousarray(s["az"], np.float64)
+        k["masspt"] = np.ascontiguousarray(s["masspt"], np.float64)
+        k["ubuf"] = np.ascontiguousarray(t["ubuf"], np.float64)
+        k["iubuflow"] = np.ascontiguousarray(t["iubuflow"], np.int32)
+        k["r2umin"] = np.ascontiguousarray(t["r2umin"], np.float64)
+        k["r2atat"] = np.ascontiguousarray(t.get("r2atat", np.zeros(len(t["r2umin"]))), np.float64)
+        k["bond_ij"] = np.ascontiguousarray(s.get("bond_ij", np.zeros((0, 2))), np.int32).reshape(-1)
+        k["bond_k"] = np.ascontiguousarray(s.get("bond_k", np.zeros(0)), np.float64)
+        k["bond_eq"] = np.ascontiguousarray(s.get("bond_eq", np.zeros(0)), np.float64)
+        k["bond_p"] = np.ascontiguousarray(s.get("bond_p", np.zeros(0)), np.int32)
+        fac = s.get("bd_fac")
+        if fac is not None:
+            k["fac1"] = np.ascontiguousarray(fac[0], np.float64)
+            k["fac2"] = np.ascontiguousarray(fac[1], np.float64)
+        self._keep.append(k)
+        null = C.POINTER(C.c_double)()
+        return MsgParams(int(s["np"]), int(s["npt"]), (C.c_double * 3)(*s["boxlen"]), s["rcut"], s["drnlist"],
+                         _p(k["iptpn"], C.c_int32), _p(k["az"], C.c_double), _p(k["masspt"], C.c_double),
+                         _p(k["ubuf"], C.c_double), len(k["ubuf"]), _p(k["iubuflow"], C.c_int32),
+                         _p(k["r2umin"], C.c_double), _p(k["r2atat"], C.c_double), int(s["lewald"]),
+                         int(s["order"]), int(s["nmesh"]), int(s["lsurf"]), t["ualpha"] if "ualpha" in t else s["ualpha"],
+                         s["epsi_four_pi"], len(k["bond_p"]), _p(k["bond_ij"], C.c_int32),
+                         _p(k["bond_k"], C.c_double), _p(k["bond_eq"], C.c_double), _p(k["bond_p"], C.c_int32),
+                         s["tstep"], _p(k["fac1"], C.c_double) if "fac1" in k else null,
+                         _p(k["fac2"], C.c_double) if "fac2" in k else null, int(maxnneigh))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            _lib.lib().msg_destroy(h)
+            self.h = None
+
+    def _check(self, rc):
+        if rc:
+            raise MolsimGpuError(rc, _lib.lib().msg_last_error(self.h).decode())
+
+    # --- state -------------------------------------------------------------
+    def set_state(self, isys, ro, rod=None, rodd=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (ro, rod, rodd)]
+        ptrs = [None if a is None else _p(a, C.c_double) for a in arrs]
+        self._check(_lib.lib().msg_set_state(self.h, isys, *ptrs))
+
+    def get_state(self, isys=0):
+        n = int(self.systems[isys]["np"])
+        out = [np.zeros((n, 3)) for _ in range(3)]
+        self._check(_lib.lib().msg_get_state(self.h, isys, *[_p(a, C.c_double) for a in out]))
+        return dict(ro=out[0], rod=out[1], rodd=out[2])
+
+    # --- MOLSIM entry points --------------------------------------------------
+    def SetVList(self, isys=0, export=True, maxnneigh=None):
+        """Rebuild now; return (nneighpn, jpnlist, npair) in MOLSIM's layout (1-based)."""
+        n = int(self.systems[isys]["np"])
+        npair = C.c_int64()
+        if not export:
+            self._check(_lib.lib().msg_build_nlist(self.h, isys, None, None, 0, C.byref(npair)))
+            return None, None, npair.value
+        maxn = int(maxnneigh or n)
+        nn = np.zeros(n, np.int32)
+        jp = np.zeros((n, maxn), np.int32)
+        self._check(_lib.lib().msg_build_nlist(self.h, isys, _p(nn, C.c_int32), _p(jp, C.c_int32), maxn,
+                                               C.byref(npair)))
+        return nn, jp, npair.value
+
+    def UTotal(self, isys=0):
+        n = int(self.systems[isys]["np"])
+        f = np.zeros((n, 3))
+        fo = np.zeros((n, 3))
+        e = MsgEnergy()
+        self._check(_lib.lib().msg_utotal(self.h, isys, _p(f, C.c_double), _p(fo, C.c_double), C.byref(e)))
+        d = e.as_dict(self.natat[isys])
+        d["force"] = f
+        d["forceo"] = fo
+        return d
+
+    def GetLinAcc(self):
+        self._check(_lib.lib().msg_get_linacc(self.h))
+
+    def VelVer(self, nsteps=1, isys=0, energies=True):
+        """nsteps of MDDriver(iSimulationStep) + NList for every system; energies of system isys."""
+        if not energies:
+            self._check(_lib.lib().msg_velver(self.h, nsteps, isys, None))
+            return None
+        e = (MsgEnergy * max(1, nsteps))()
+        self._check(_lib.lib().msg_velver(self.h, nsteps, isys, e))
+        return [e[k].as_dict(self.natat[isys]) for k in range(nsteps)]
+
+    def BDStep(self, nsteps=1, seed=0, isys=0, xi=None, return_noise=False, energies=True):
+        """nsteps of BDDriver(iSimulationStep) + NList.  xi: caller noise [nsteps][np][3]."""
+        n = int(self.systems[isys]["np"])
+        xin = None if xi is None else np.ascontiguousarray(xi, np.float64).reshape(nsteps, n, 3)
+        xout = np.zeros((nsteps, n, 3)) if return_noise else None
+        e = (MsgEnergy * max(1, nsteps))() if energies else None
+        self._check(_lib.lib().msg_bd_step(self.h, nsteps, seed, isys,
+                                           None if xin is None else _p(xin, C.c_double),
+                                           None if xout is None else _p(xout, C.c_double), e))
+        en = [e[k].as_dict(self.natat[isys]) for k in range(nsteps)] if energies else None
+        return (en, xout) if return_noise else en
+
+    def nrebuild(self, isys=0):
+        return _lib.lib().msg_nrebuild(self.h, isys)

@@ -1,0 +1,268 @@
+"""Seeded synthetic systems for the force/energy path.
+
+Each generator returns a plain dict describing one monoatomic charged system in
+MOLSIM's units (A, g/mol, ps, kJ/mol, K; Src/molsim.F90:786-805):
+
+    np, npt, boxlen[3], rcut, drnlist, iptpn[np] (1-based), az[np], masspt[npt],
+    zat/sigat/epsat[npt], temp, relpermitt, epsi_four_pi, uewaldtol, order, nmesh,
+    lewald, lsurf, tstep, bonds (bond_ij[nb][2] 1-based, bond_k (already divided by
+    the power, Src/potential.F90:3561), bond_eq, bond_p), ro[np][3], rod[np][3].
+
+The Ewald alpha and the pair table are derived from these by the library's own
+setup routines (`molsim_b200.setup`), exactly as MOLSIM derives them in
+IOPotTwoBody/EwaldSetup/PotTwoBodyTab1 from its namelists.
+"""
+import math
+
+import numpy as np
+
+# Src/mol.F90:60-80 and Src/molsim.F90:786-805
+PI = 3.1415926535897932
+AVNO = 6.02214179e23
+ECH = 1.602176487e-19
+GAS_CONSTANT = 8.314472
+EPSI0 = 8.854187817e-12
+SCLLEN, SCLMAS, SCLTIM, SCLENE, SCLDIF = 1.0e-10, 1.0e-03, 1.0e-12, 1.0e+03, 1.0e-09
+SCLVEL = SCLLEN / SCLTIM
+SCLFOR = SCLVEL / SCLTIM * SCLMAS
+EPSI0_FOUR_PI = ECH ** 2 / (4.0 * PI * EPSI0 * SCLLEN) * AVNO / SCLENE
+
+# nmlPotential defaults, Src/potential.F90:340-367.  utoltab/ftoltab and the
+# exponent of ljrcut are single-precision literals in the reference.
+F32_1EM5 = float(np.float32(1e-5))
+POT_DEFAULTS = dict(r2uminin=0.1, utoltab=F32_1EM5, ftoltab=F32_1EM5, umaxtab=20000.0,
+                    fmaxtab=20000.0, ljrcut=2.0 ** float(np.float32(1.0) / np.float32(6.0)),
+                    ljushift=1.0, rumaxfac=1.1)
+
+
+def kT(temp):
+    """k_B T in kJ/mol."""
+    return GAS_CONSTANT * temp / 1000.0
+
+
+def _min_image(d, box):
+    return d - box * np.round(d / box)
+
+
+def place_uniform(rng, n, box, mind, existing=None, exist_mind=None, batch=4096):
+    """Uniform positions in [-L/2, L/2)^3 with no pair closer than `mind` (and no
+    point closer than `exist_mind` to an `existing` point), by seeded rejection."""
+    from scipy.spatial import cKDTree
+
+    L = float(box)
+    pts = np.zeros((0, 3))
+    ex_tree = None
+    if existing is not None and len(existing):
+        ex_tree = cKDTree(np.mod(existing + L / 2, L), boxsize=L)
+    while len(pts) < n:
+        cand = rng.uniform(-L / 2, L / 2, size=(batch, 3))
+        cw = np.mod(cand + L / 2, L)
+        ok = np.ones(len(cand), bool)
+        if ex_tree is not None:
+            d, _ = ex_tree.query(cw, k=1)
+            ok &= d >= exist_mind
+        if len(pts):
+            t = cKDTree(np.mod(pts + L / 2, L), boxsize=L)
+            d, _ = t.query(cw, k=1)
+            ok &= d >= mind
+        cand, cw = cand[ok], cw[ok]
+        if len(cand) > 1:
+            t = cKDTree(cw, boxsize=L)
+            pairs = t.query_pairs(mind, output_type="ndarray")
+            if len(pairs):
+                drop = np.zeros(len(cand), bool)
+                for a, b in pairs:          # keep the earlier candidate of each close pair
+                    if not drop[a]:
+                        drop[b] = True
+                cand = cand[~drop]
+        pts = np.concatenate([pts, cand[: n - len(pts)]])
+    return pts
+
+
+def maxwell_velocities(rng, masses, temp):
+    """SetLinVel, Src/md.F90:802-822: v = sqrt(R T/(m sclmas sclvel^2)) * N(0,1)."""
+    fac = GAS_CONSTANT * temp / (SCLMAS * SCLVEL ** 2)
+    return rng.standard_normal((len(masses), 3)) * np.sqrt(fac / masses)[:, None]
+
+
+def _base(np_, npt, L, rcut, temp, relp, order, nmesh, tstep, drnlist=2.0, lsurf=False):
+    return dict(np=int(np_), npt=int(npt), boxlen=[float(L)] * 3, rcut=float(rcut),
+                drnlist=float(drnlist), temp=float(temp), relpermitt=float(relp),
+                epsi_four_pi=EPSI0_FOUR_PI / relp, uewaldtol=1e-5, order=int(order),
+                nmesh=int(nmesh), lewald=True, lsurf=bool(lsurf), lljcut=True, tstep=float(tstep),
+                nbond=0, bond_ij=np.zeros((0, 2), np.int32), bond_k=np.zeros(0),
+                bond_eq=np.zeros(0), bond_p=np.zeros(0, np.int32), **POT_DEFAULTS)
+
+
+def electrolyte(seed=0, n_pairs=500, L=100.0, temp=298.0, relp=78.4, sigma=4.0, mass=23.0,
+                rcut=30.0, nmesh=32, order=4, tstep=0.005, eps_kT=0.1):
+    """1:1 primitive-model electrolyte (500 + 500 ions, L=100 A, SPME 32^3 order 4, rc=30 A)."""
+    rng = np.random.default_rng(seed)
+    n = 2 * n_pairs
+    s = _base(n, 2, L, rcut, temp, relp, order, nmesh, tstep)
+    s["zat"] = np.array([1.0, -1.0])
+    s["sigat"] = np.array([sigma, sigma])
+    s["epsat"] = np.array([eps_kT * kT(temp)] * 2)
+    s["masspt"] = np.array([mass, mass])
+    s["iptpn"] = np.array([1] * n_pairs + [2] * n_pairs, np.int32)
+    s["az"] = s["zat"][s["iptpn"] - 1].copy()
+    s["ro"] = place_uniform(rng, n, L, 0.8 * sigma)
+    s["rod"] = maxwell_velocities(rng, s["masspt"][s["iptpn"] - 1], temp)
+    s["name"] = "electrolyte_%d" % n
+    return s
+
+
+def polyelectrolyte(seed=0, nchain=40, nbead=200, L=250.0, temp=298.0, relp=78.4, sigma=4.0,
+                    mass=23.0, rcut=25.0, nmesh=64, order=5, tstep=0.005, bond_kT=0.4, r0=5.0,
+                    eps_kT=0.1):
+    """40 chains x 200 beads (-1e) + 8000 counterions (+1e), L=250 A, SPME 64^3 order 5, rc=25 A.
+    Chains are random walks with 5 A steps rejecting overlaps below 0.8 sigma."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    nb = nchain * nbead
+    n = 2 * nb
+    s = _base(n, 2, L, rcut, temp, relp, order, nmesh, tstep)
+    s["zat"] = np.array([-1.0, 1.0])
+    s["sigat"] = np.array([sigma, sigma])
+    s["epsat"] = np.array([eps_kT * kT(temp)] * 2)
+    s["masspt"] = np.array([mass, mass])
+    s["iptpn"] = np.array([1] * nb + [2] * nb, np.int32)
+    s["az"] = s["zat"][s["iptpn"] - 1].copy()
+    mind = 0.8 * sigma
+    beads = []
+    for c in range(nchain):
+        for _attempt in range(1000):
+            chain = [rng.uniform(-L / 2, L / 2, 3)]
+            ok = True
+            prev = np.array(beads) if beads else None
+            tree = cKDTree(np.mod(prev + L / 2, L), boxsize=L) if prev is not None else None
+            while len(chain) < nbead and ok:
+                for _t in range(200):
+                    v = rng.standard_normal(3)
+                    p = chain[-1] + r0 * v / np.linalg.norm(v)
+                    p = _min_image(p, L)
+                    d_own = np.linalg.norm(_min_image(np.array(chain[:-1]) - p, L), axis=1) if len(chain) > 1 else np.array([1e9])
+                    if d_own.min() < mind:
+                        continue
+                    if tree is not None and tree.query(np.mod(p + L / 2, L))[0] < mind:
+                        continue
+                    chain.append(p)
+                    break
+                else:
+                    ok = False
+            if ok:
+                beads.extend(chain)
+                break
+        else:
+            raise RuntimeError("could not grow chain %d" % c)
+    beads = np.array(beads)
+    ions = place_uniform(rng, nb, L, mind, existing=beads, exist_mind=mind)
+    s["ro"] = np.concatenate([beads, ions])
+    s["rod"] = maxwell_velocities(rng, s["masspt"][s["iptpn"] - 1], temp)
+    bij = []
+    for c in range(nchain):
+        for k in range(nbead - 1):
+            bij.append((c * nbead + k + 1, c * nbead + k + 2))
+    s["bond_ij"] = np.array(bij, np.int32)
+    s["nbond"] = len(bij)
+    s["bond_p"] = np.full(len(bij), 2, np.int32)
+    s["bond_k"] = np.full(len(bij), bond_kT * kT(temp) / 2.0)   # k/p, Src/potential.F90:3561
+    s["bond_eq"] = np.full(len(bij), r0)
+    s["name"] = "polyelectrolyte_%d" % n
+    return s
+
+
+def colloid_bd(seed=0, n_macro=2000, z_macro=20.0, sigma_macro=40.0, n_salt_pairs=79000,
+               L=1200.0, temp=298.0, relp=78.4, sigma=4.0, rcut=30.0, nmesh=128, order=4,
+               tstep=1e-3, d_ion=1.0, d_macro=0.1, mass_ion=23.0, mass_macro=1.0e5, eps_kT=0.1):
+    """Charged colloids for Brownian dynamics: 2000 macroions (+20e, sigma 40 A), 40000
+    counterions (-1e) and 79000+79000 salt ions (sigma 4 A) in L=1200 A; SPME 128^3 order 4.
+    Types: 1 macroion, 2 anion (counterion and salt anion), 3 cation.  dcoeff in units of
+    1e-9 m^2/s (scldif)."""
+    rng = np.random.default_rng(seed)
+    n_ci = int(round(n_macro * z_macro))
+    n_an = n_ci + n_salt_pairs
+    n_cat = n_salt_pairs
+    n = n_macro + n_an + n_cat
+    s = _base(n, 3, L, rcut, temp, relp, order, nmesh, tstep)
+    s["zat"] = np.array([z_macro, -1.0, 1.0])
+    s["sigat"] = np.array([sigma_macro, sigma, sigma])
+    s["epsat"] = np.array([eps_kT * kT(temp)] * 3)
+    s["masspt"] = np.array([mass_macro, mass_ion, mass_ion])
+    s["dcoeff"] = np.array([d_macro, d_ion, d_ion])
+    s["iptpn"] = np.array([1] * n_macro + [2] * n_an + [3] * n_cat, np.int32)
+    s["az"] = s["zat"][s["iptpn"] - 1].copy()
+    macro = place_uniform(rng, n_macro, L, sigma_macro)
+    ions = place_uniform(rng, n_an + n_cat, L, 0.8 * sigma, existing=macro,
+                         exist_mind=0.5 * (sigma_macro + sigma), batch=32768)
+    s["ro"] = np.concatenate([macro, ions])
+    s["rod"] = np.zeros((n, 3))
+    s["name"] = "colloid_bd_%d" % n
+    return s
+
+
+def bd_factors(s):
+    """fac1/fac2 of BDStep, Src/bd.F90:135-140, per particle type."""
+    dt, T, D = s["tstep"], s["temp"], np.asarray(s["dcoeff"], np.float64)
+    fac1 = dt * SCLTIM * D * SCLDIF * SCLFOR / (GAS_CONSTANT * T * 1.0) / SCLLEN
+    fac2 = np.sqrt(2.0 * D * SCLDIF * dt * SCLTIM) / SCLLEN
+    return fac1, fac2
+
+
+def replica_electrolyte(rng, n, rho_red, temp, sigma=4.0, mass=23.0, order=4, nmesh=32,
+                        tstep=0.005, drnlist=2.0, eps_kT=0.1, relp=78.4):
+    """One member of the batched ensemble: N ions (N/2 of each sign) at reduced density
+    rho*sigma^3, temperature T; rc = min(30 A, L/2 - drnlist)."""
+    rho = rho_red / sigma ** 3
+    L = (n / rho) ** (1.0 / 3.0)
+    rcut = min(30.0, L / 2.0 - drnlist)
+    s = _base(n, 2, L, rcut, temp, relp, order, nmesh, tstep, drnlist=drnlist)
+    s["zat"] = np.array([1.0, -1.0])
+    s["sigat"] = np.array([sigma, sigma])
+    s["epsat"] = np.array([eps_kT * kT(temp)] * 2)
+    s["masspt"] = np.array([mass, mass])
+    s["iptpn"] = np.array([1] * (n // 2) + [2] * (n // 2), np.int32)
+    s["az"] = s["zat"][s["iptpn"] - 1].copy()
+    s["ro"] = place_uniform(rng, n, L, 0.8 * sigma)
+    s["rod"] = maxwell_velocities(rng, s["masspt"][s["iptpn"] - 1], temp)
+    s["name"] = "replica_%d" % n
+    return s
+
+
+def batched_ensemble(seed=0, nsys=512, nmin=200, nmax=4000):
+    """512 electrolytes with N ~ U{200..4000} (even), rho*sigma^3 ~ U[0.01, 0.3],
+    T ~ U[250, 400] K; the SPME grid edge is chosen later by the autotuner."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nsys):
+        n = 2 * int(rng.integers(nmin // 2, nmax // 2 + 1))
+        rho_red = float(rng.uniform(0.01, 0.3))
+        T = float(rng.uniform(250.0, 400.0))
+        out.append(replica_electrolyte(rng, n, rho_red, T))
+    return out
+
+
+def scaled_job(rng, n, kind):
+    """A serving job: the electrolyte generator at its density, or the polyelectrolyte
+    generator at its density with chains of up to 200 beads, scaled to N particles."""
+    if kind == "electrolyte":
+        L = 100.0 * (n / 1000.0) ** (1.0 / 3.0)
+        s = electrolyte(seed=int(rng.integers(1 << 30)), n_pairs=n // 2, L=L,
+                        rcut=min(30.0, L / 2 - 2.0), nmesh=_grid_for(L), order=4)
+    else:
+        nb = n // 2
+        nbead = min(200, max(2, nb))
+        nchain = max(1, nb // nbead)
+        nb = nchain * nbead
+        L = 250.0 * (2 * nb / 16000.0) ** (1.0 / 3.0)
+        s = polyelectrolyte(seed=int(rng.integers(1 << 30)), nchain=nchain, nbead=nbead, L=L,
+                            rcut=min(25.0, L / 2 - 2.0), nmesh=_grid_for(L), order=4)
+    return s
+
+
+def _grid_for(L, spacing=3.9):
+    for g in (16, 24, 32, 48, 64, 96, 128):
+        if L / g <= spacing:
+            return g
+    return 128

@@ -1,0 +1,1089 @@
+/*
+ * oracle.c -- FP64 CPU restatement of MOLSIM's serial force/energy hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see oracle.h).  Compiled with -O2
+ * -ffp-contract=off so that every a*b+c rounds twice, as the reference's
+ * gfortran/x86-64 build does.  Expressions keep the reference's evaluation
+ * order (Fortran evaluates a*b*c as (a*b)*c; x**2 as x*x).
+ */
+#include "oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* Src/mol.F90:60-80 */
+static const double Pi = 3.1415926535897932;
+static const double AvNo = 6.02214179e23;
+static const double ECh = 1.602176487e-19;
+static const double GasConstant = 8.314472;
+static const double Epsi0 = 8.854187817e-12;
+
+/* Default unit scales, Src/molsim.F90:786-795 */
+static const double scllen = 1.0e-10, sclmas = 1.0e-03, scltim = 1.0e-12, sclene = 1.0e+03;
+
+double or_gas_constant(void) { return GasConstant; }
+
+/* Epsi0FourPi = ECh**2/(FourPi*Epsi0*scllen)*AvNo/sclene, Src/molsim.F90:805 */
+double or_epsi0_four_pi(void)
+{
+    double FourPi = 4.0 * Pi;
+    return ECh * ECh / (FourPi * Epsi0 * scllen) * AvNo / sclene;
+}
+
+static double sclfor(void)
+{
+    double sclvel = scllen / scltim;
+    double sclacc = sclvel / scltim;
+    return sclacc * sclmas;
+}
+
+/* ------------------------------------------------------------------ */
+/* Erf2, Src/mollib.F90:215-274 (NAG Chebyshev form).                 */
+/* The reference's second branch starts from c(18), runs j=16..2 and  */
+/* finishes with c(j) where j==1 after the loop: c(17) is never used. */
+/* ------------------------------------------------------------------ */
+double or_erf2(double x)
+{
+    static const double c[19] = {0.0,
+        1.9449071068178803, 4.20186582324414e-2, -1.86866103976769e-2,
+        5.1281061839107e-3, -1.0683107461726e-3, 1.744737872522e-4,
+        -2.15642065714e-5, 1.7282657974e-6, -2.00479241e-8,
+        -1.64782105e-8, 2.0008475e-9, 2.57716e-11,
+        -3.06343e-11, 1.9158e-12, 3.703e-13,
+        -5.43e-14, -4.0e-15, 1.2e-15};
+    static const double d[18] = {0.0,
+        1.4831105640848036, -3.010710733865950e-1, 6.89948306898316e-2,
+        -1.39162712647222e-2, 2.4207995224335e-3, -3.658639685849e-4,
+        4.86209844323e-5, -5.7492565580e-6, 6.113243578e-7,
+        -5.89910153e-8, 5.2070091e-9, -4.232976e-10,
+        3.18811e-11, -2.2361e-12, 1.467e-13,
+        -9.0e-15, 5.0e-16};
+    const double sqrtpi = 1.7724538509055160, xup = 6.25;
+    const int ncfc = 18, ncfd = 17;
+    double xv = fabs(x), x2, bj = 0.0, bjp1, bjp2;
+    int j;
+    if (xv <= 2.0) {
+        x2 = x * x - 2.0;
+        bjp2 = 0.0;
+        bjp1 = d[ncfd];
+        for (j = ncfd - 1; j >= 2; --j) {
+            bj = x2 * bjp1 - bjp2 + d[j];
+            bjp2 = bjp1;
+            bjp1 = bj;
+        }
+        bj = x2 * bjp1 - bjp2 + d[1];
+        return 0.5 * (bj - bjp2) * x;
+    } else if (xv < xup) {
+        x2 = 2.0 - 20.0 / (xv + 3.0);
+        bjp2 = 0.0;
+        bjp1 = c[ncfc];
+        for (j = ncfd - 1; j >= 2; --j) {
+            bj = x2 * bjp1 - bjp2 + c[j];
+            bjp2 = bjp1;
+            bjp1 = bj;
+        }
+        /* Fortran loop variable after completion: j == 1 */
+        bj = x2 * bjp1 - bjp2 + c[1];
+        x2 = 0.5 * (bj - bjp2) / xv * exp(-x * x) / sqrtpi;
+        return (1.0 - x2) * (x >= 0.0 ? 1.0 : -1.0);
+    }
+    /* xv > xup (xv == xup exactly is left undefined by the reference) */
+    return x >= 0.0 ? 1.0 : -1.0;
+}
+
+/* CalcEwaldUfac, Src/potential.F90:2938-2960 */
+void or_ewald_ufac(double r1, double ualpha, double c[3])
+{
+    const double fac = 1.12837916709;
+    double ra = ualpha * r1;
+    double er = or_erf2(ra);
+    double ex = fac * exp(-(ra * ra));
+    c[0] = 1.0 - (er);
+    c[1] = 1.0 - (er - ra * ex);
+    c[2] = 1.0 - (er - ra * (1.0 + ra * ra) * ex);
+}
+
+/* CardinalBSpline, Src/mollib.F90:1629-1683 (values + first derivatives) */
+void or_cardinal_bspline(int order, double pos, int32_t *kmax, double *values, double *derivs)
+{
+    double lastvals[32];
+    int v = (int)floor(pos), n, i;
+    double x = pos - v, a;
+    *kmax = v;
+    for (i = 0; i < order; ++i) lastvals[i] = 0.0;
+    values[0] = x;
+    if (order > 1) {
+        values[1] = 1.0 - x;
+        for (n = 3; n <= order; ++n) {
+            for (i = 0; i < order; ++i) lastvals[i] = values[i];
+            values[0] = x * lastvals[0] / (n - 1);
+            for (i = 1; i <= n - 2; ++i) {
+                a = i + x;
+                values[i] = (a * lastvals[i] + (n - a) * lastvals[i - 1]) / (n - 1);
+            }
+            values[n - 1] = (1 - x) * lastvals[n - 2] / (n - 1);
+        }
+        n = order;
+        if (derivs) {
+            derivs[0] = lastvals[0];
+            for (i = 1; i <= n - 2; ++i) derivs[i] = lastvals[i] - lastvals[i - 1];
+            derivs[n - 1] = -lastvals[n - 2];
+        }
+    }
+}
+
+/* RcutToAlpha, Src/energy.F90:7090-7105 (charged system, lq2sum == 0) */
+double or_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
+                        double boxlenshort, double rcut, int32_t *status)
+{
+    double br = boxlenshort * rcut;
+    double y = (uewaldtol / (q2sum * epsi_four_pi)) * sqrt(2.0 * (br * br * br));
+    double xold = 1.0e-1, xnew = 0.0;
+    int i;
+    for (i = 1; i <= 40; ++i) {
+        xnew = (1.0 / rcut) * sqrt(-log(y * (xold * xold)));
+        if (fabs(xold - xnew) / xnew < 1.0e-6) break;
+        xold = xnew;
+    }
+    if (status) *status = (i > 40) ? 6 : 0;
+    return xnew;
+}
+
+/* EwaldErrorUReal, Src/potential.F90:2995-3018 (charges) */
+double or_ewald_error_ureal(double q2sum, double l, double alpha, double rcut, double unit)
+{
+    double fac = (alpha * rcut) * (alpha * rcut);
+    return unit * q2sum * sqrt(rcut / (2.0 * (l * l * l))) / fac * exp(-fac);
+}
+
+/* ------------------------------------------------------------------ */
+/* Pair potential table                                                */
+/* ------------------------------------------------------------------ */
+
+/* iptpt / iatat enumeration, Src/particle.F90:1528-1562 (1-based) */
+static int pair_index(int npt, int i, int j)
+{
+    int a = i < j ? i : j, b = i < j ? j : i, k = 0, ii, jj;
+    for (ii = 1; ii <= npt; ++ii)
+        for (jj = ii; jj <= npt; ++jj) {
+            ++k;
+            if (ii == a && jj == b) return k;
+        }
+    return 0;
+}
+
+/* x**6 as gfortran expands an integer power: (x*x*x)**2 */
+static double pow6(double x) { double x3 = x * x * x; return x3 * x3; }
+
+/* Pot_1_6_12 'calc', Src/potential.F90:1349-1425 (types are 1-based) */
+void or_pot_1_6_12(const or_tab_params *p, int iat, int jat, double r1,
+                   double *u0, double *u1, double *u2)
+{
+    double qq = p->zat[iat - 1] * p->zat[jat - 1] * p->epsi_four_pi;
+    double sig = 0.5 * (p->sigat[iat - 1] + p->sigat[jat - 1]);
+    double eps = sqrt(p->epsat[iat - 1] * p->epsat[jat - 1]);
+    double r1i = 1.0 / r1;
+    double fac = pow6(sig * r1i);
+    double c[3] = {1.0, 1.0, 1.0};
+    double us0, us1, us2;
+    if (p->lewald) or_ewald_ufac(r1, p->ualpha, c);
+    us0 = +4.0 * eps * (fac * fac - fac);
+    us1 = -(24.0 * eps * (2.0 * (fac * fac) - fac) * r1i);
+    us2 = +24.0 * eps * (26.0 * (fac * fac) - 7.0 * fac) * (r1i * r1i);
+    if (p->lljcut) {
+        if (r1 < p->ljrcut * sig) {
+            us0 = us0 + p->ljushift * eps;
+        } else {
+            us0 = 0.0; us1 = 0.0; us2 = 0.0;
+        }
+    }
+    *u0 = qq * c[0] * r1i + us0;
+    *u1 = -(qq * c[1] * (r1i * r1i)) + us1;
+    *u2 = 2.0 * qq * c[2] * (r1i * r1i * r1i) + us2;
+}
+
+/* SetUBuffer, Src/potential.F90:1139-1220 */
+static void set_ubuffer(double zlow, double u0low, double u1low, double u2low,
+                        double zupp, double u0upp, double u1upp, double u2upp, double *t)
+{
+    double dz1, dz2, dz3, rlow, rupp, w0low, w1low, w2low, w0upp, w1upp, w2upp, a, b, c;
+    int k;
+    if (u0low == 0.0 && u0upp == 0.0) {
+        t[0] = zlow;
+        for (k = 1; k < 12; ++k) t[k] = 0.0;
+        return;
+    }
+    rlow = sqrt(zlow);
+    rupp = sqrt(zupp);
+    dz1 = zupp - zlow;
+    dz2 = dz1 * dz1;
+    dz3 = dz2 * dz1;
+    w0low = u0low;
+    w0upp = u0upp;
+    w1low = 0.50 * u1low / rlow;
+    w1upp = 0.50 * u1upp / rupp;
+    w2low = 0.25 * (u2low - u1low / rlow) / zlow;
+    w2upp = 0.25 * (u2upp - u1upp / rupp) / zupp;
+    a = 6.0 * (w0upp - w0low - w1low * dz1 - 0.5 * w2low * dz2) / dz3;
+    b = 2.0 * (w1upp - w1low - w2low * dz1) / dz2;
+    c = (w2upp - w2low) / dz1;
+    t[0] = zlow;
+    t[1] = w0low;
+    t[2] = w1low;
+    t[3] = 0.5 * w2low;
+    t[4] = (10.0 * a - 12.0 * b + 3.0 * c) / (6.0);
+    t[5] = (-15.0 * a + 21.0 * b - 6.0 * c) / (6.0 * dz1);
+    t[6] = (2.0 * a - 3.0 * b + c) / (2.0 * dz2);
+    t[7] = -2.0 * t[2];
+    t[8] = -4.0 * t[3];
+    t[9] = -6.0 * t[4];
+    t[10] = -8.0 * t[5];
+    t[11] = -10.0 * t[6];
+}
+
+/* CheckUBuffer, Src/potential.F90:1224-1258 */
+static void check_ubuffer(const or_tab_params *p, int iat, int jat, double rlow, double rupp,
+                          const double *t, int *ok, int *repul)
+{
+    const int ncheck = 11;
+    double dr = (rupp - rlow) / (ncheck - 1), r1, dz, usum, fsum, u0, u1, u2;
+    int icheck;
+    *ok = 0;
+    *repul = 0;
+    for (icheck = 1; icheck <= ncheck; ++icheck) {
+        r1 = rlow + dr * (icheck - 1);
+        or_pot_1_6_12(p, iat, jat, r1, &u0, &u1, &u2);
+        dz = r1 * r1 - rlow * rlow;
+        usum = t[1] + dz * (t[2] + dz * (t[3] + dz * (t[4] + dz * (t[5] + dz * t[6]))));
+        fsum = t[7] + dz * (t[8] + dz * (t[9] + dz * (t[10] + dz * t[11])));
+        fsum = r1 * fsum;
+        if (fabs(usum - u0) > p->utoltab) return;
+        if (fabs(fsum + u1) > p->ftoltab) return;
+        if (fabs(usum) > p->umaxtab) *repul = 1;
+        if (fabs(fsum) > p->fmaxtab) *repul = 1;
+    }
+    *ok = 1;
+}
+
+/* PotTwoBodyTab3, Src/potential.F90:1054-1135.  ibuf is a 1-based cursor. */
+static int pot_tab3(const or_tab_params *p, int iat, int jat, int iatjat, int32_t *ibuf,
+                    double *ubuf, int32_t nbuf, int32_t *iubuflow, int32_t *nugrid,
+                    double *rumin, const double *rumax)
+{
+    const int mnugrid = 1200, ndr = 100;
+    const double drfac = 0.9;
+    double rlow = 0.0, rupp, zlow, zupp, dr, u0l, u1l, u2l, u0u, u1u, u2u, t[12];
+    int igrid, idr, ok = 0, repul = 0, k;
+    iubuflow[iatjat - 1] = *ibuf;
+    rupp = rumax[iatjat - 1];
+    dr = 0.5 * (rumax[iatjat - 1] - rumin[iatjat - 1]);
+    for (igrid = 1; igrid <= mnugrid; ++igrid) {
+        zupp = rupp * rupp;
+        for (idr = 1; idr <= ndr; ++idr) {
+            rlow = rupp - dr;
+            rlow = fmax(rumin[iatjat - 1], rlow);
+            zlow = rlow * rlow;
+            or_pot_1_6_12(p, iat, jat, rlow, &u0l, &u1l, &u2l);
+            or_pot_1_6_12(p, iat, jat, rupp, &u0u, &u1u, &u2u);
+            set_ubuffer(zlow, u0l, u1l, u2l, zupp, u0u, u1u, u2u, t);
+            check_ubuffer(p, iat, jat, rlow, rupp, t, &ok, &repul);
+            if (ok) {
+                rupp = rlow;
+                if (p->lljcut) dr = 2.0 * dr;
+                break;
+            }
+            dr = dr * drfac;
+        }
+        if (idr >= ndr + 1) return 6;
+        if (*ibuf + 11 > nbuf) return 2;
+        for (k = 0; k < 12; ++k) ubuf[*ibuf - 1 + k] = t[k];
+        *ibuf += 12;
+        if (repul) rumin[iatjat - 1] = rlow;
+        if (rlow <= rumin[iatjat - 1]) break;
+        if (repul) break;
+    }
+    if (igrid >= mnugrid + 1) return 6;
+    nugrid[iatjat - 1] = igrid;
+    return 0;
+}
+
+/* PotTwoBodyTab1 + PotTwoBodyTab2 + Pot_1_6_12 'init', Src/potential.F90:868-1050, 1370-1380 */
+int or_pot_tab(const or_tab_params *p, double *ubuf, int32_t nbuf,
+               int32_t *iubuflow, int32_t *nugrid, double *r2umin,
+               double *rumin, double *rumax, int32_t *nused)
+{
+    int npt = p->npt, ipt, jpt, rc;
+    int32_t ibuf = 1;
+    memset(ubuf, 0, sizeof(double) * (size_t)nbuf);
+    for (ipt = 1; ipt <= npt; ++ipt)
+        for (jpt = ipt; jpt <= npt; ++jpt) {
+            int ij = pair_index(npt, ipt, jpt);
+            double r2umax = (p->rumaxfac * (p->rcut + 0.0 + 0.0));
+            r2umax = r2umax * r2umax;
+            r2umin[ij - 1] = p->r2uminin;
+            rumax[ij - 1] = sqrt(r2umax);
+            rumin[ij - 1] = sqrt(r2umin[ij - 1]);
+            rc = pot_tab3(p, ipt, jpt, ij, &ibuf, ubuf, nbuf, iubuflow, nugrid, rumin, rumax);
+            if (rc) return rc;
+            r2umin[ij - 1] = rumin[ij - 1] * rumin[ij - 1];
+        }
+    if (nused) *nused = ibuf - 1;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* SPME setup, Src/energy.F90:6855-7019                                */
+/* ------------------------------------------------------------------ */
+void or_ewald_setup_spm(int s, int order, double ualpha, const double boxlen[3],
+                        double *meshfac, double *energyfac, double *virfac)
+{
+    const double TwoPi = 2.0 * Pi, FourPi = 4.0 * Pi;
+    double spl[32], b2[3][1024], vol, fac0, expfac, TwoPiBoxi[3];
+    int32_t z;
+    int i, m, k, nx, ny, nz, h = s / 2;
+    or_cardinal_bspline(order, 0.0, &z, spl, NULL);
+    for (i = 0; i < 3; ++i)
+        for (m = 0; m < s; ++m) {
+            double complex a = 0.0;
+            if ((order % 2 == 1) && (2 * m == s)) {
+                /* left unset by the reference; defined here as 0 (Nyquist plane dropped) */
+                b2[i][m] = 0.0;
+                continue;
+            }
+            for (k = 0; k <= order - 2; ++k) {
+                /* cmplx(0, x) without KIND is default (single precision) complex */
+                float ang = (float)(TwoPi * m * k / s);
+                float complex e = cexpf(I * ang);
+                a = a + spl[k + 1] * (double complex)e;
+            }
+            b2[i][m] = 1.0 / (creal(a) * creal(a) + cimag(a) * cimag(a));
+        }
+    vol = boxlen[0] * boxlen[1] * boxlen[2];
+    for (i = 0; i < 3; ++i) TwoPiBoxi[i] = TwoPi * (1.0 / boxlen[i]);
+    fac0 = FourPi / vol;
+    expfac = -1.0 / (4.0 * (ualpha * ualpha));
+    for (nz = 0; nz <= h; ++nz)
+        for (ny = 0; ny <= h; ++ny)
+            for (nx = 0; nx <= h; ++nx) {
+                size_t idx = (size_t)nx + (size_t)(h + 1) * ((size_t)ny + (size_t)(h + 1) * nz);
+                if (nx == 0 && ny == 0 && nz == 0) {
+                    meshfac[idx] = 0.0;
+                    energyfac[idx] = 0.0;
+                    virfac[idx] = 0.0;
+                } else {
+                    double kx = nx * TwoPiBoxi[0], ky = ny * TwoPiBoxi[1], kz = nz * TwoPiBoxi[2];
+                    double m2 = kx * kx + ky * ky + kz * kz;
+                    double c = exp(m2 * expfac) / m2;
+                    double mf = fac0 * c * b2[0][nx] * b2[1][ny] * b2[2][nz];
+                    meshfac[idx] = mf;
+                    if (nx == (s - nx) % s) mf = mf / 2;
+                    if (ny == (s - ny) % s) mf = mf / 2;
+                    if (nz == (s - nz) % s) mf = mf / 2;
+                    energyfac[idx] = mf;
+                    virfac[idx] = (1.0 + 2 * m2 * expfac) * mf;
+                }
+            }
+}
+
+/* ------------------------------------------------------------------ */
+/* FFT: recursive mixed-radix complex DFT (FFTW 3.3.4 is the reference */
+/* library; only its unnormalised conventions are restated here).     */
+/* ------------------------------------------------------------------ */
+/* x[k*stride], k<n; tw[e] = exp(sign*2*pi*i*e/N) for the top-level size N */
+static void fft1(double complex *x, int n, int stride, const double complex *tw, int N,
+                 double complex *tmp)
+{
+    int p, m, k, q, r;
+    if (n == 1) return;
+    for (p = 2; p <= n; ++p)
+        if (n % p == 0) break;
+    m = n / p;
+    for (r = 0; r < p; ++r)
+        for (k = 0; k < m; ++k) tmp[r * m + k] = x[(k * p + r) * stride];
+    for (r = 0; r < p; ++r) fft1(tmp + r * m, m, 1, tw, N, tmp + n);
+    for (k = 0; k < m; ++k)
+        for (q = 0; q < p; ++q) {
+            double complex acc = 0.0;
+            int kk = k + q * m;
+            for (r = 0; r < p; ++r) {
+                long e = ((long)r * kk) % n;
+                acc += tmp[r * m + k] * tw[e * (N / n)];
+            }
+            x[kk * stride] = acc;
+        }
+}
+
+static void fft3_complex(int s, double complex *a, int sign)
+{
+    double complex *tmp = malloc(sizeof(double complex) * (size_t)s * 4);
+    double complex *line = malloc(sizeof(double complex) * (size_t)s);
+    double complex *tw = malloc(sizeof(double complex) * (size_t)s);
+    int i, j, k;
+    for (i = 0; i < s; ++i) {
+        double ang = sign * 2.0 * Pi * (double)i / (double)s;
+        tw[i] = cos(ang) + I * sin(ang);
+    }
+    for (k = 0; k < s; ++k)          /* x lines */
+        for (j = 0; j < s; ++j) fft1(a + ((size_t)k * s + j) * s, s, 1, tw, s, tmp);
+    for (k = 0; k < s; ++k)          /* y lines */
+        for (i = 0; i < s; ++i) {
+            for (j = 0; j < s; ++j) line[j] = a[((size_t)k * s + j) * s + i];
+            fft1(line, s, 1, tw, s, tmp);
+            for (j = 0; j < s; ++j) a[((size_t)k * s + j) * s + i] = line[j];
+        }
+    for (j = 0; j < s; ++j)          /* z lines */
+        for (i = 0; i < s; ++i) {
+            for (k = 0; k < s; ++k) line[k] = a[((size_t)k * s + j) * s + i];
+            fft1(line, s, 1, tw, s, tmp);
+            for (k = 0; k < s; ++k) a[((size_t)k * s + j) * s + i] = line[k];
+        }
+    free(tw);
+    free(line);
+    free(tmp);
+}
+
+void or_fft3_r2c(int s, const double *in, double *out)
+{
+    size_t n = (size_t)s * s * s, i;
+    int h = s / 2 + 1, x, y, z;
+    double complex *a = malloc(sizeof(double complex) * n);
+    for (i = 0; i < n; ++i) a[i] = in[i];
+    fft3_complex(s, a, -1);
+    for (z = 0; z < s; ++z)
+        for (y = 0; y < s; ++y)
+            for (x = 0; x < h; ++x) {
+                double complex v = a[((size_t)z * s + y) * s + x];
+                size_t o = ((size_t)z * s + y) * h + x;
+                out[2 * o] = creal(v);
+                out[2 * o + 1] = cimag(v);
+            }
+    free(a);
+}
+
+void or_fft3_c2r(int s, const double *in, double *out)
+{
+    size_t n = (size_t)s * s * s, i;
+    int h = s / 2 + 1, x, y, z;
+    double complex *a = malloc(sizeof(double complex) * n);
+    for (z = 0; z < s; ++z)
+        for (y = 0; y < s; ++y)
+            for (x = 0; x < s; ++x) {
+                double complex v;
+                if (x < h) {
+                    size_t o = ((size_t)z * s + y) * h + x;
+                    v = in[2 * o] + I * in[2 * o + 1];
+                } else {
+                    int xs = s - x, ys = (s - y) % s, zs = (s - z) % s;
+                    size_t o = ((size_t)zs * s + ys) * h + xs;
+                    v = in[2 * o] - I * in[2 * o + 1];
+                }
+                a[((size_t)z * s + y) * s + x] = v;
+            }
+    fft3_complex(s, a, +1);
+    for (i = 0; i < n; ++i) out[i] = creal(a[i]);
+    free(a);
+}
+
+/* ------------------------------------------------------------------ */
+/* The system                                                          */
+/* ------------------------------------------------------------------ */
+struct or_sys {
+    int np, npt, natat;
+    double boxlen[3], boxlen2[3], boxleni[3], dpbc[3], vol;
+    double rcut, rcut2, drnlist;
+    int32_t *iptpn;
+    double *az, *massp, *massip;
+    double *ro, *rod, *rodd, *roddo, *drostep, *drosum, *force, *forceo;
+    double *ubuf; int nbuf; int32_t *iubuflow; double *r2umin, *r2atat;
+    int maxnneigh; int32_t *nneighpn, *jpnlist;
+    int lewald, order, s, lsurf; double ualpha, epsfp;
+    double *meshfac, *energyfac, *virfac, *qmesh, *fqmesh;
+    int nbond; int32_t *bond_ij; double *bond_k, *bond_eq; int32_t *bond_p;
+    double tstep;
+    int lcellbuild;
+};
+
+static void *dup(const void *p, size_t n)
+{
+    void *q = malloc(n ? n : 1);
+    if (p && n) memcpy(q, p, n);
+    else memset(q, 0, n ? n : 1);
+    return q;
+}
+
+or_sys *or_create(const or_params *p)
+{
+    or_sys *s = calloc(1, sizeof(or_sys));
+    int np = p->np, i, h;
+    s->np = np;
+    s->npt = p->npt;
+    s->natat = p->npt * (p->npt + 1) / 2;
+    /* SetBoxParam, Src/molaux.F90:325-336 (txbc='xyz') */
+    for (i = 0; i < 3; ++i) {
+        s->boxlen[i] = p->boxlen[i];
+        s->boxlen2[i] = p->boxlen[i] / 2.0;
+        s->boxleni[i] = 1.0 / p->boxlen[i];
+        s->dpbc[i] = p->boxlen[i];
+    }
+    s->vol = p->boxlen[0] * p->boxlen[1] * p->boxlen[2];
+    s->rcut = p->rcut;
+    s->rcut2 = p->rcut * p->rcut;
+    s->drnlist = p->drnlist;
+    s->iptpn = dup(p->iptpn, sizeof(int32_t) * np);
+    s->az = dup(p->az, sizeof(double) * np);
+    s->massp = malloc(sizeof(double) * np);
+    s->massip = malloc(sizeof(double) * np);
+    for (i = 0; i < np; ++i) {
+        double m = p->masspt[s->iptpn[i] - 1];
+        s->massp[i] = m;
+        s->massip[i] = m > 0.0 ? 1.0 / m : 0.0;
+    }
+    s->ro = calloc(3 * (size_t)np, sizeof(double));
+    s->rod = calloc(3 * (size_t)np, sizeof(double));
+    s->rodd = calloc(3 * (size_t)np, sizeof(double));
+    s->roddo = calloc(3 * (size_t)np, sizeof(double));
+    s->drostep = calloc(3 * (size_t)np, sizeof(double));
+    s->drosum = calloc(3 * (size_t)np, sizeof(double));
+    s->force = calloc(3 * (size_t)np, sizeof(double));
+    s->forceo = calloc(3 * (size_t)np, sizeof(double));
+    s->nbuf = p->nbuf;
+    s->ubuf = dup(p->ubuf, sizeof(double) * p->nbuf);
+    s->iubuflow = dup(p->iubuflow, sizeof(int32_t) * s->natat);
+    s->r2umin = dup(p->r2umin, sizeof(double) * s->natat);
+    s->r2atat = dup(p->r2atat, sizeof(double) * s->natat);
+    s->maxnneigh = p->maxnneigh;
+    s->nneighpn = calloc((size_t)np, sizeof(int32_t));
+    s->jpnlist = calloc((size_t)np * (size_t)p->maxnneigh, sizeof(int32_t));
+    s->lewald = p->lewald;
+    s->order = p->order;
+    s->s = p->nmesh;
+    s->lsurf = p->lsurf;
+    s->ualpha = p->ualpha;
+    s->epsfp = p->epsi_four_pi;
+    if (s->lewald) {
+        size_t n = (size_t)s->s * s->s * s->s;
+        h = s->s / 2 + 1;
+        s->meshfac = malloc(sizeof(double) * h * h * h);
+        s->energyfac = malloc(sizeof(double) * h * h * h);
+        s->virfac = malloc(sizeof(double) * h * h * h);
+        or_ewald_setup_spm(s->s, s->order, s->ualpha, s->boxlen, s->meshfac, s->energyfac, s->virfac);
+        s->qmesh = malloc(sizeof(double) * n);
+        s->fqmesh = malloc(sizeof(double) * 2 * (size_t)h * s->s * s->s);
+    }
+    s->nbond = p->nbond;
+    s->bond_ij = dup(p->bond_ij, sizeof(int32_t) * 2 * p->nbond);
+    s->bond_k = dup(p->bond_k, sizeof(double) * p->nbond);
+    s->bond_eq = dup(p->bond_eq, sizeof(double) * p->nbond);
+    s->bond_p = dup(p->bond_p, sizeof(int32_t) * p->nbond);
+    s->tstep = p->tstep;
+    s->lcellbuild = p->lcellbuild;
+    return s;
+}
+
+void or_destroy(or_sys *s)
+{
+    if (!s) return;
+    free(s->iptpn); free(s->az); free(s->massp); free(s->massip);
+    free(s->ro); free(s->rod); free(s->rodd); free(s->roddo); free(s->drostep); free(s->drosum);
+    free(s->force); free(s->forceo);
+    free(s->ubuf); free(s->iubuflow); free(s->r2umin); free(s->r2atat);
+    free(s->nneighpn); free(s->jpnlist);
+    free(s->meshfac); free(s->energyfac); free(s->virfac); free(s->qmesh); free(s->fqmesh);
+    free(s->bond_ij); free(s->bond_k); free(s->bond_eq); free(s->bond_p);
+    free(s);
+}
+
+void or_set_state(or_sys *s, const double *ro, const double *rod, const double *rodd)
+{
+    size_t n = 3 * (size_t)s->np * sizeof(double);
+    if (ro) memcpy(s->ro, ro, n);
+    if (rod) memcpy(s->rod, rod, n);
+    if (rodd) memcpy(s->rodd, rodd, n);
+}
+
+void or_get_state(const or_sys *s, double *ro, double *rod, double *rodd, double *drosum)
+{
+    size_t n = 3 * (size_t)s->np * sizeof(double);
+    if (ro) memcpy(ro, s->ro, n);
+    if (rod) memcpy(rod, s->rod, n);
+    if (rodd) memcpy(rodd, s->rodd, n);
+    if (drosum) memcpy(drosum, s->drosum, n);
+}
+
+void or_set_drosum(or_sys *s, const double *drosum)
+{
+    memcpy(s->drosum, drosum, 3 * (size_t)s->np * sizeof(double));
+}
+
+/* PBC (box), Src/molaux.F90:104-118: anint-wrap of one coordinate */
+static double pbc1(double d, double half, double len, double leni)
+{
+    if (fabs(d) > half) d = d - len * round(d * leni);
+    return d;
+}
+
+/* PBCr2 (box), Src/molaux.F90:149-161: single sign(dpbc,d) shift */
+static double pbcr2(const or_sys *s, double *dx, double *dy, double *dz)
+{
+    if (fabs(*dx) > s->boxlen2[0]) *dx = *dx - copysign(s->dpbc[0], *dx);
+    if (fabs(*dy) > s->boxlen2[1]) *dy = *dy - copysign(s->dpbc[1], *dy);
+    if (fabs(*dz) > s->boxlen2[2]) *dz = *dz - copysign(s->dpbc[2], *dz);
+    return *dx * *dx + *dy * *dy + *dz * *dz;
+}
+
+/* parity rule of SetVListMD, Src/nlist.F90:741-744 (1-based ip, jp) */
+static int owns(int ip, int jp)
+{
+    int itemp = (ip + jp) % 2;
+    if (ip < jp && itemp == 0) return 0;
+    if (ip > jp && itemp != 0) return 0;
+    return ip != jp;
+}
+
+/* SetVListMD, Src/nlist.F90:724-759 */
+static int set_vlist_md(or_sys *s)
+{
+    double rs2cut = (s->rcut + s->drnlist) * (s->rcut + s->drnlist);
+    int ip, jp, np = s->np;
+    for (ip = 1; ip <= np; ++ip) {
+        int32_t *row = s->jpnlist + (size_t)(ip - 1) * s->maxnneigh;
+        int nn = 0;
+        for (jp = 1; jp <= np; ++jp) {
+            double dx, dy, dz, r2;
+            if (!owns(ip, jp)) continue;
+            dx = s->ro[3 * (ip - 1)] - s->ro[3 * (jp - 1)];
+            dy = s->ro[3 * (ip - 1) + 1] - s->ro[3 * (jp - 1) + 1];
+            dz = s->ro[3 * (ip - 1) + 2] - s->ro[3 * (jp - 1) + 2];
+            r2 = pbcr2(s, &dx, &dy, &dz);
+            if (r2 < rs2cut) {
+                if (nn >= s->maxnneigh) return 3;
+                row[nn++] = jp;
+            }
+        }
+        s->nneighpn[ip - 1] = nn;
+    }
+    return 0;
+}
+
+static int cmp_i32(const void *a, const void *b)
+{
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* Same pair set and row order as SetVListMD, found through a cell grid
+ * (cell side >= rcut+drnlist) so that large N stays tractable; rows are
+ * sorted by jp, which is the order SetVListMD's jp loop produces. */
+static int set_vlist_cells(or_sys *s)
+{
+    double rl = s->rcut + s->drnlist, rs2cut = rl * rl;
+    int nc[3], d, np = s->np, ip, i;
+    for (d = 0; d < 3; ++d) {
+        nc[d] = (int)floor(s->boxlen[d] / rl);
+        if (nc[d] < 1) nc[d] = 1;
+    }
+    {
+        size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+        int32_t *head = malloc(sizeof(int32_t) * ncell), *next = malloc(sizeof(int32_t) * np);
+        int32_t *cell = malloc(sizeof(int32_t) * np);
+        for (i = 0; i < (int)ncell; ++i) head[i] = -1;
+        for (ip = np - 1; ip >= 0; --ip) {
+            int c[3];
+            for (d = 0; d < 3; ++d) {
+                int k = (int)floor((s->ro[3 * ip + d] + s->boxlen2[d]) * nc[d] / s->boxlen[d]);
+                if (k < 0) k = 0;
+                if (k >= nc[d]) k = nc[d] - 1;
+                c[d] = k;
+            }
+            cell[ip] = c[0] + nc[0] * (c[1] + nc[1] * c[2]);
+            next[ip] = head[cell[ip]];
+            head[cell[ip]] = ip;
+        }
+        for (ip = 0; ip < np; ++ip) {
+            int32_t *row = s->jpnlist + (size_t)ip * s->maxnneigh;
+            int nn = 0, cx = cell[ip] % nc[0], cy = (cell[ip] / nc[0]) % nc[1], cz = cell[ip] / (nc[0] * nc[1]);
+            int off[3][3], no[3], a, b, e;
+            for (d = 0; d < 3; ++d) {
+                int cc = d == 0 ? cx : (d == 1 ? cy : cz);
+                if (nc[d] >= 3) { no[d] = 3; off[d][0] = (cc + nc[d] - 1) % nc[d]; off[d][1] = cc; off[d][2] = (cc + 1) % nc[d]; }
+                else { no[d] = nc[d]; for (a = 0; a < nc[d]; ++a) off[d][a] = a; }
+            }
+            for (a = 0; a < no[2]; ++a)
+                for (b = 0; b < no[1]; ++b)
+                    for (e = 0; e < no[0]; ++e) {
+                        int32_t jp = head[off[0][e] + nc[0] * (off[1][b] + nc[1] * off[2][a])];
+                        for (; jp >= 0; jp = next[jp]) {
+                            double dx, dy, dz, r2;
+                            if (!owns(ip + 1, jp + 1)) continue;
+                            dx = s->ro[3 * ip] - s->ro[3 * jp];
+                            dy = s->ro[3 * ip + 1] - s->ro[3 * jp + 1];
+                            dz = s->ro[3 * ip + 2] - s->ro[3 * jp + 2];
+                            r2 = pbcr2(s, &dx, &dy, &dz);
+                            if (r2 < rs2cut) {
+                                if (nn >= s->maxnneigh) { free(head); free(next); free(cell); return 3; }
+                                row[nn++] = jp + 1;
+                            }
+                        }
+                    }
+            qsort(row, nn, sizeof(int32_t), cmp_i32);
+            s->nneighpn[ip] = nn;
+        }
+        free(head); free(next); free(cell);
+    }
+    return 0;
+}
+
+int or_set_vlist(or_sys *s) { return s->lcellbuild ? set_vlist_cells(s) : set_vlist_md(s); }
+
+void or_get_vlist(const or_sys *s, int32_t *nneighpn, int32_t *jpnlist)
+{
+    if (nneighpn) memcpy(nneighpn, s->nneighpn, sizeof(int32_t) * s->np);
+    if (jpnlist) memcpy(jpnlist, s->jpnlist, sizeof(int32_t) * (size_t)s->np * s->maxnneigh);
+}
+
+int64_t or_npair(const or_sys *s)
+{
+    int64_t n = 0;
+    int i;
+    for (i = 0; i < s->np; ++i) n += s->nneighpn[i];
+    return n;
+}
+
+/* UTwoBodyA, Src/energy.F90:445-544 (serial: iploc == ip) */
+static int utwobody_a(or_sys *s, double *utwob, double *virtwob)
+{
+    int ip, k, npt = s->npt;
+    double vir = 0.0;
+    for (k = 0; k <= s->natat; ++k) utwob[k] = 0.0;
+    for (ip = 1; ip <= s->np; ++ip) {
+        int ipt = s->iptpn[ip - 1];
+        const int32_t *row = s->jpnlist + (size_t)(ip - 1) * s->maxnneigh;
+        for (k = 0; k < s->nneighpn[ip - 1]; ++k) {
+            int jp = row[k], jpt = s->iptpn[jp - 1], iptjpt = pair_index(npt, ipt, jpt);
+            double dx = s->ro[3 * (ip - 1)] - s->ro[3 * (jp - 1)];
+            double dy = s->ro[3 * (ip - 1) + 1] - s->ro[3 * (jp - 1) + 1];
+            double dz = s->ro[3 * (ip - 1) + 2] - s->ro[3 * (jp - 1) + 2];
+            double r2 = pbcr2(s, &dx, &dy, &dz), usum, fsum = 0.0;
+            if (r2 > s->rcut2) continue;
+            if (r2 < s->r2atat[iptjpt - 1]) {
+                usum = 1e10;   /* hard-core overlap; the reference leaves fsum stale here */
+            } else if (r2 < s->r2umin[iptjpt - 1]) {
+                return 1;
+            } else {
+                int ibuf = s->iubuflow[iptjpt - 1];
+                const double *u;
+                for (;;) {
+                    if (r2 >= s->ubuf[ibuf - 1]) break;
+                    ibuf += 12;
+                    if (ibuf > s->nbuf) return 2;
+                }
+                u = s->ubuf + ibuf - 1;
+                {
+                    double d = r2 - u[0];
+                    usum = u[1] + d * (u[2] + d * (u[3] + d * (u[4] + d * (u[5] + d * u[6]))));
+                    fsum = u[7] + d * (u[8] + d * (u[9] + d * (u[10] + d * u[11])));
+                }
+            }
+            utwob[iptjpt] = utwob[iptjpt] + usum;
+            s->force[3 * (ip - 1)] += (fsum * dx);
+            s->force[3 * (ip - 1) + 1] += (fsum * dy);
+            s->force[3 * (ip - 1) + 2] += (fsum * dz);
+            s->force[3 * (jp - 1)] -= (fsum * dx);
+            s->force[3 * (jp - 1) + 1] -= (fsum * dy);
+            s->force[3 * (jp - 1) + 2] -= (fsum * dz);
+            vir = vir - (fsum * r2);
+        }
+    }
+    utwob[0] = 0.0;
+    for (k = 1; k <= s->natat; ++k) utwob[0] += utwob[k];
+    *virtwob = vir;
+    return 0;
+}
+
+/* UEwaldRecSPM + SPMFFTRec, Src/energy.F90:1207-1297, 6525-6587 */
+static void uewald_rec_spm(or_sys *s, double *urec, double *virrec)
+{
+    int S = s->s, order = s->order, h = S / 2, hp = S / 2 + 1, ia, m, ix, iy, iz;
+    size_t n = (size_t)S * S * S;
+    double dkdr[3], spline[3][32], deriv[3][32];
+    int32_t meshmax[3];
+    double uloc = 0.0, virloc = *virrec;
+    for (m = 0; m < 3; ++m) dkdr[m] = S / s->boxlen[m];
+    memset(s->qmesh, 0, sizeof(double) * n);
+    for (ia = 0; ia < s->np; ++ia) {
+        for (m = 0; m < 3; ++m) {
+            or_cardinal_bspline(order, dkdr[m] * s->ro[3 * ia + m], &meshmax[m], spline[m], deriv[m]);
+            meshmax[m] = (meshmax[m] + S) % S;
+        }
+        for (iz = 0; iz < order; ++iz) {
+            int nz = (S + meshmax[2] - iz) % S;
+            double qz = s->az[ia] * spline[2][iz];
+            for (iy = 0; iy < order; ++iy) {
+                int ny = (S + meshmax[1] - iy) % S;
+                double qyz = qz * spline[1][iy];
+                for (ix = 0; ix < order; ++ix) {
+                    int nx = (S + meshmax[0] - ix) % S;
+                    double q = qyz * spline[0][ix];
+                    s->qmesh[(size_t)nx + S * ((size_t)ny + (size_t)S * nz)] += q;
+                }
+            }
+        }
+    }
+    or_fft3_r2c(S, s->qmesh, s->fqmesh);
+    {
+        int nx, ny, nz;
+        for (nz = 0; nz <= h; ++nz) {
+            int nza = (S - nz) % S;
+            for (ny = 0; ny <= h; ++ny) {
+                int nya = (S - ny) % S;
+                for (nx = 0; nx <= h; ++nx) {
+                    size_t f = (size_t)nx + (size_t)hp * ((size_t)ny + (size_t)hp * nz);
+                    size_t i1 = (size_t)nx + (size_t)hp * ((size_t)ny + (size_t)S * nz);
+                    size_t i2 = (size_t)nx + (size_t)hp * ((size_t)ny + (size_t)S * nza);
+                    size_t i3 = (size_t)nx + (size_t)hp * ((size_t)nya + (size_t)S * nz);
+                    size_t i4 = (size_t)nx + (size_t)hp * ((size_t)nya + (size_t)S * nza);
+                    double *F = s->fqmesh;
+                    double v1r = F[2 * i1], v1i = F[2 * i1 + 1], v2r = F[2 * i2], v2i = F[2 * i2 + 1];
+                    double v3r = F[2 * i3], v3i = F[2 * i3 + 1], v4r = F[2 * i4], v4i = F[2 * i4 + 1];
+                    double Qsum = v1r * v1r + v1i * v1i + v2r * v2r + v2i * v2i
+                                + v3r * v3r + v3i * v3i + v4r * v4r + v4i * v4i;
+                    double mf = s->meshfac[f];
+                    uloc = uloc + Qsum * s->energyfac[f];
+                    virloc = virloc - Qsum * s->virfac[f];
+                    F[2 * i1] = v1r * mf; F[2 * i1 + 1] = v1i * mf;
+                    F[2 * i2] = v2r * mf; F[2 * i2 + 1] = v2i * mf;
+                    F[2 * i3] = v3r * mf; F[2 * i3 + 1] = v3i * mf;
+                    F[2 * i4] = v4r * mf; F[2 * i4 + 1] = v4i * mf;
+                }
+            }
+        }
+    }
+    or_fft3_c2r(S, s->fqmesh, s->qmesh);
+    for (ia = 0; ia < s->np; ++ia) {
+        double esum[3] = {0.0, 0.0, 0.0};
+        for (m = 0; m < 3; ++m) {
+            or_cardinal_bspline(order, dkdr[m] * s->ro[3 * ia + m], &meshmax[m], spline[m], deriv[m]);
+            meshmax[m] = (meshmax[m] + S) % S;
+        }
+        for (iz = 0; iz < order; ++iz) {
+            int nz = (S + meshmax[2] - iz) % S;
+            double splz = spline[2][iz], dsdz = deriv[2][iz];
+            for (iy = 0; iy < order; ++iy) {
+                int ny = (S + meshmax[1] - iy) % S;
+                double sply = spline[1][iy], dsdy = deriv[1][iy];
+                for (ix = 0; ix < order; ++ix) {
+                    int nx = (S + meshmax[0] - ix) % S;
+                    double splx = spline[0][ix], dsdx = deriv[0][ix];
+                    double Qval = s->qmesh[(size_t)nx + S * ((size_t)ny + (size_t)S * nz)];
+                    esum[0] = esum[0] + dsdx * sply * splz * Qval;
+                    esum[1] = esum[1] + splx * dsdy * splz * Qval;
+                    esum[2] = esum[2] + splx * sply * dsdz * Qval;
+                }
+            }
+        }
+        for (m = 0; m < 3; ++m)
+            s->force[3 * ia + m] = s->force[3 * ia + m] - s->az[ia] * esum[m] * dkdr[m] * s->epsfp;
+    }
+    *urec = uloc;
+    *virrec = virloc;
+}
+
+/* UEwald + UEwaldSelf + UEwaldSurf, Src/energy.F90:905-958, 1301-1371 (monoatomic) */
+static void uewald(or_sys *s, double *urec_out, double *utot, double *virial)
+{
+    double urec = 0.0, virrec = 0.0, q2 = 0.0;
+    int ia;
+    uewald_rec_spm(s, &urec, &virrec);
+    for (ia = 0; ia < s->np; ++ia) q2 += s->az[ia] * s->az[ia];
+    urec = urec - s->ualpha / sqrt(Pi) * q2;
+    if (s->lsurf) {
+        double fac = 2.0 * Pi / (3.0 * s->vol), sx = 0.0, sy = 0.0, sz = 0.0, term;
+        for (ia = 0; ia < s->np; ++ia) {
+            sx += s->az[ia] * s->ro[3 * ia];
+            sy += s->az[ia] * s->ro[3 * ia + 1];
+            sz += s->az[ia] * s->ro[3 * ia + 2];
+        }
+        term = fac * (sx * sx + sy * sy + sz * sz);
+        urec = urec + term;
+        for (ia = 0; ia < s->np; ++ia) {
+            s->force[3 * ia] = s->force[3 * ia] - s->epsfp * (2.0 * fac) * s->az[ia] * sx;
+            s->force[3 * ia + 1] = s->force[3 * ia + 1] - s->epsfp * (2.0 * fac) * s->az[ia] * sy;
+            s->force[3 * ia + 2] = s->force[3 * ia + 2] - s->epsfp * (2.0 * fac) * s->az[ia] * sz;
+        }
+        virrec = virrec - term;
+    }
+    urec = s->epsfp * urec;
+    *utot = *utot + urec;
+    *virial = *virial + s->epsfp * virrec;
+    *urec_out = urec;
+}
+
+/* UBond, Src/energy.F90:5335-5387 */
+static void ubond(or_sys *s, double *ub, double *utot, double *virial)
+{
+    double u = 0.0, vir = 0.0;
+    int b, k;
+    for (b = 0; b < s->nbond; ++b) {
+        int ip = s->bond_ij[2 * b] - 1, jp = s->bond_ij[2 * b + 1] - 1, pw = s->bond_p[b];
+        double dx = s->ro[3 * ip] - s->ro[3 * jp];
+        double dy = s->ro[3 * ip + 1] - s->ro[3 * jp + 1];
+        double dz = s->ro[3 * ip + 2] - s->ro[3 * jp + 2];
+        double r2 = pbcr2(s, &dx, &dy, &dz), r1 = sqrt(r2), term = r1 - s->bond_eq[b];
+        double tp = 1.0, fac;
+        for (k = 0; k < pw - 1; ++k) tp = tp * term;
+        fac = s->bond_k[b] * tp;
+        u = u + fac * term;
+        fac = -(pw * fac / r1);
+        s->force[3 * ip] += (fac * dx);
+        s->force[3 * ip + 1] += (fac * dy);
+        s->force[3 * ip + 2] += (fac * dz);
+        s->force[3 * jp] -= (fac * dx);
+        s->force[3 * jp + 1] -= (fac * dy);
+        s->force[3 * jp + 2] -= (fac * dz);
+        vir = vir - (fac * r2);
+    }
+    *ub = u;
+    *utot = *utot + u;
+    *virial = *virial + vir;
+}
+
+/* UTotal, Src/energy.F90:280-434 (monoatomic, charged, vlist) */
+int or_utotal(or_sys *s, double *force, double *forceo, double *u, double *virial)
+{
+    double utot = 0.0, vir = 0.0, virtwob = 0.0, urec = 0.0, ub = 0.0, fac;
+    double *utwob = malloc(sizeof(double) * (s->natat + 1));
+    int rc, i, k, n3 = 3 * s->np;
+    for (i = 0; i < n3; ++i) s->force[i] = 0.0;
+    rc = utwobody_a(s, utwob, &virtwob);
+    if (rc) { free(utwob); return rc; }
+    utot = utot + utwob[0];
+    vir = vir + virtwob;
+    if (s->lewald) uewald(s, &urec, &utot, &vir);
+    if (s->nbond > 0) ubond(s, &ub, &utot, &vir);
+    /* force -> internal units, forceo; virmolecule == 0 for monoatomic */
+    fac = (sclene / scllen) / sclfor();
+    if (force) memcpy(force, s->force, sizeof(double) * n3);
+    for (i = 0; i < n3; ++i) {
+        s->force[i] = s->force[i] * fac;
+        s->forceo[i] = 0.0 + s->force[i];
+    }
+    if (forceo) memcpy(forceo, s->forceo, sizeof(double) * n3);
+    if (u) {
+        u[0] = utot;
+        for (k = 0; k <= s->natat; ++k) u[1 + k] = utwob[k];
+        u[2 + s->natat] = urec;
+        u[3 + s->natat] = ub;
+    }
+    if (virial) *virial = vir;
+    free(utwob);
+    return 0;
+}
+
+/* NList iSimulationStep with inlist == 0, Src/nlist.F90:597-613 */
+int or_skin_test(or_sys *s, const double *drostep, double *max1, double *max2)
+{
+    double r2max1 = 0.0, r2max2 = 0.0;
+    int ip, m;
+    for (ip = 0; ip < s->np; ++ip) {
+        double r2;
+        for (m = 0; m < 3; ++m) s->drosum[3 * ip + m] = s->drosum[3 * ip + m] + drostep[3 * ip + m];
+        r2 = s->drosum[3 * ip] * s->drosum[3 * ip] + s->drosum[3 * ip + 1] * s->drosum[3 * ip + 1]
+           + s->drosum[3 * ip + 2] * s->drosum[3 * ip + 2];
+        if (r2 > r2max1) r2max1 = r2;
+        else if (r2 > r2max2) r2max2 = r2;
+    }
+    if (max1) *max1 = r2max1;
+    if (max2) *max2 = r2max2;
+    if (sqrt(r2max1) + sqrt(r2max2) > s->drnlist) {
+        memset(s->drosum, 0, sizeof(double) * 3 * s->np);
+        return 1;
+    }
+    return 0;
+}
+
+/* VelVer (linear) + GetLinAcc + GetKinEnergy + NList, Src/md.F90:252-410, 601-617, 1089-1112 */
+int or_velver_step(or_sys *s, double *ekin, int32_t *rebuilt)
+{
+    double dt = s->tstep, fac = 0.5 * (dt * dt), ek = 0.0;
+    int ip, m, rc, n3 = 3 * s->np;
+    for (ip = 0; ip < s->np; ++ip) {
+        for (m = 0; m < 3; ++m) {
+            int i = 3 * ip + m;
+            s->drostep[i] = dt * s->rod[i] + fac * s->rodd[i];
+            s->ro[i] = s->ro[i] + s->drostep[i];
+        }
+        for (m = 0; m < 3; ++m)
+            s->ro[3 * ip + m] = pbc1(s->ro[3 * ip + m], s->boxlen2[m], s->dpbc[m], s->boxleni[m]);
+    }
+    rc = or_utotal(s, NULL, NULL, NULL, NULL);
+    if (rc) return rc;
+    for (m = 0; m < n3; ++m) s->roddo[m] = s->rodd[m];
+    for (ip = 0; ip < s->np; ++ip)
+        for (m = 0; m < 3; ++m) s->rodd[3 * ip + m] = s->massip[ip] * s->forceo[3 * ip + m];
+    for (m = 0; m < n3; ++m) s->rod[m] = s->rod[m] + 0.5 * dt * (s->rodd[m] + s->roddo[m]);
+    for (ip = 0; ip < s->np; ++ip) {
+        const double *v = s->rod + 3 * ip;
+        ek = ek + 0.5 * s->massp[ip] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    }
+    {
+        double sclvel = scllen / scltim;
+        ek = ek * sclmas * (sclvel * sclvel) / sclene;
+    }
+    if (ekin) *ekin = ek;
+    if (or_skin_test(s, s->drostep, NULL, NULL)) {
+        if (rebuilt) *rebuilt = 1;
+        return or_set_vlist(s);
+    }
+    if (rebuilt) *rebuilt = 0;
+    return 0;
+}
+
+/* BDDriver iSimulationStep: BDStep then UTotal, then NList; Src/bd.F90:53-59, 120-155 */
+int or_bd_step(or_sys *s, const double *xi, const double *fac1, const double *fac2, int32_t *rebuilt)
+{
+    int ip, m, rc;
+    for (ip = 0; ip < s->np; ++ip) {
+        int ipt = s->iptpn[ip] - 1;
+        for (m = 0; m < 3; ++m) {
+            int i = 3 * ip + m;
+            s->drostep[i] = fac1[ipt] * s->forceo[i] + fac2[ipt] * xi[i];
+            s->ro[i] = s->ro[i] + s->drostep[i];
+        }
+        for (m = 0; m < 3; ++m)
+            s->ro[3 * ip + m] = pbc1(s->ro[3 * ip + m], s->boxlen2[m], s->dpbc[m], s->boxleni[m]);
+    }
+    rc = or_utotal(s, NULL, NULL, NULL, NULL);
+    if (rc) return rc;
+    if (or_skin_test(s, s->drostep, NULL, NULL)) {
+        if (rebuilt) *rebuilt = 1;
+        return or_set_vlist(s);
+    }
+    if (rebuilt) *rebuilt = 0;
+    return 0;
+}
+
+/* GauRandom, Src/mollib.F90:2739-2766 (polar Box-Muller over a 31-bit LCG) */
+double or_gau_random(int32_t *iseed, int32_t *flag, double *save)
+{
+    const int32_t k = 16087;
+    const double f = 1.0 / 2147483648.0;
+    double rx, ry, r, fac;
+    if (*flag) {
+        for (;;) {
+            *iseed = (int32_t)(((uint32_t)*iseed * (uint32_t)k) & 0x7fffffffu);
+            rx = 2.0 * (f * *iseed - 0.5);
+            *iseed = (int32_t)(((uint32_t)*iseed * (uint32_t)k) & 0x7fffffffu);
+            ry = 2.0 * (f * *iseed - 0.5);
+            r = rx * rx + ry * ry;
+            if (r < 1.0) break;
+        }
+        fac = sqrt(-2.0 * log(r) / r);
+        *save = ry * fac;
+        *flag = 0;
+        return rx * fac;
+    }
+    *flag = 1;
+    return *save;
+}

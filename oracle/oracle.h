@@ -1,0 +1,140 @@
+/*
+ * oracle.h -- FP64 CPU restatement of MOLSIM's serial force/energy hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA path is
+ * compared against.  Only the tests, the smoke check and the CPU-baseline leg
+ * of the benchmark may load it; the product library never links or calls it.
+ *
+ * Every routine names the MOLSIM (TomHoefken/molsim) source it restates,
+ * as Src/<file>:<line>.  Arrays follow MOLSIM's layout: Fortran (3,N) is
+ * C [N][3]; particle types, pair-table offsets and neighbour indices are
+ * 1-based exactly as in MOLSIM's globals (Src/mol.F90:1087-1135).
+ *
+ * Parity status: the reference is Fortran and no Fortran compiler exists in
+ * this build environment, so these routines are pinned against the
+ * reference's own in-code self checks (CheckUBuffer tolerances, TestCellList
+ * completeness, TestEwaldSPM-style SPME-vs-converged checks, standard Ewald)
+ * and against analytic known answers, not against outputs of the compiled
+ * reference.
+ */
+#ifndef MOLSIM_ORACLE_H
+#define MOLSIM_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- physical constants and units, Src/mol.F90:60-80, Src/molsim.F90:786-805 ---- */
+double or_epsi0_four_pi(void);          /* e^2/(4 pi eps0 A) N_A / 1e3  [kJ A / mol] */
+double or_gas_constant(void);           /* J/(mol K) */
+
+/* ---- scalar numerics ---- */
+double or_erf2(double x);                                   /* Src/mollib.F90:215-274 */
+void   or_ewald_ufac(double r1, double ualpha, double c[3]);/* Src/potential.F90:2938-2960 */
+void   or_cardinal_bspline(int order, double pos, int32_t *kmax,
+                           double *values, double *derivs);  /* Src/mollib.F90:1629-1683 */
+double or_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
+                        double boxlenshort, double rcut, int32_t *status); /* Src/energy.F90:7090-7105 */
+double or_ewald_error_ureal(double q2sum, double l, double alpha, double rcut,
+                            double unit);                   /* Src/potential.F90:2995-3018 */
+
+/* ---- pair potential (1,6,12) and its table, Src/potential.F90:868-1258, 1349-1425 ---- */
+typedef struct or_tab_params {
+    int32_t npt;             /* particle (= atom) types */
+    const double *zat;       /* [npt] charge, e */
+    const double *sigat;     /* [npt] LJ sigma, A */
+    const double *epsat;     /* [npt] LJ epsilon, kJ/mol */
+    double rcut;             /* A */
+    double ualpha;           /* Ewald alpha, 1/A */
+    double epsi_four_pi;     /* Epsi0FourPi / relpermitt */
+    int32_t lewald;          /* erfc-screened Coulomb */
+    int32_t lljcut;          /* cut-and-shift LJ at ljrcut*sigma */
+    double ljrcut;
+    double ljushift;
+    double r2uminin;
+    double utoltab, ftoltab, umaxtab, fmaxtab;
+    double rumaxfac;
+} or_tab_params;
+
+/* Potential value and r-derivatives u0, u1=du/dr, u2=d2u/dr2 (Pot_1_6_12 'calc'). */
+void or_pot_1_6_12(const or_tab_params *p, int iat, int jat, double r1,
+                   double *u0, double *u1, double *u2);
+
+/* Build the full table (PotTwoBodyTab1/2/3 + SetUBuffer + CheckUBuffer).
+ * ubuf capacity nbuf doubles; iubuflow/nugrid/r2umin/rumin/rumax sized natat.
+ * Returns 0, or 2 when nbuf is too small, or 6 when dr/igrid did not converge. */
+int or_pot_tab(const or_tab_params *p, double *ubuf, int32_t nbuf,
+               int32_t *iubuflow, int32_t *nugrid, double *r2umin,
+               double *rumin, double *rumax, int32_t *nused);
+
+/* ---- SPME setup, Src/energy.F90:6855-7019 ---- */
+void or_ewald_setup_spm(int s, int order, double ualpha, const double boxlen[3],
+                        double *meshfac, double *energyfac, double *virfac);
+
+/* ---- FFT with FFTW's unnormalised r2c (e^-i) / c2r (e^+i) conventions ----
+ * real grid [s][s][s] (x fastest) <-> complex [s][s][s/2+1] interleaved re,im */
+void or_fft3_r2c(int s, const double *in, double *out);
+void or_fft3_c2r(int s, const double *in, double *out);
+
+/* ---- the simulated system (mirrors the MolModule globals used on the path) ---- */
+typedef struct or_params {
+    int32_t np, npt;
+    double boxlen[3];
+    double rcut, drnlist;
+    const int32_t *iptpn;    /* [np] 1-based type */
+    const double *az;        /* [np] charge, e */
+    const double *masspt;    /* [npt] mass, g/mol */
+    const double *ubuf; int32_t nbuf;
+    const int32_t *iubuflow; /* [natat] 1-based */
+    const double *r2umin;    /* [natat] */
+    const double *r2atat;    /* [natat] */
+    int32_t lewald, order, nmesh, lsurf;
+    double ualpha, epsi_four_pi;
+    int32_t nbond;
+    const int32_t *bond_ij;  /* [nbond][2] 1-based, in chain order */
+    const double *bond_k;    /* [nbond] force constant already divided by power */
+    const double *bond_eq;   /* [nbond] */
+    const int32_t *bond_p;   /* [nbond] power */
+    double tstep;
+    int32_t maxnneigh;       /* row capacity of jpnlist */
+    int32_t lcellbuild;      /* 1: build the Verlet list through cells (same pair set) */
+} or_params;
+
+typedef struct or_sys or_sys;
+
+or_sys *or_create(const or_params *p);
+void    or_destroy(or_sys *s);
+void    or_set_state(or_sys *s, const double *ro, const double *rod, const double *rodd);
+void    or_get_state(const or_sys *s, double *ro, double *rod, double *rodd, double *drosum);
+void    or_set_drosum(or_sys *s, const double *drosum);
+
+int  or_set_vlist(or_sys *s);                            /* SetVListMD, Src/nlist.F90:724-759 */
+void or_get_vlist(const or_sys *s, int32_t *nneighpn, int32_t *jpnlist);
+int64_t or_npair(const or_sys *s);
+
+/* UTotal.  u = [tot, twob(0..nptpt), rec, bond]; virial scalar.
+ * force is in kJ/(mol A) (MOLSIM `force`), forceo in internal units (`forceo`). */
+int  or_utotal(or_sys *s, double *force, double *forceo, double *u, double *virial);
+
+/* One velocity-Verlet step (VelVer linear part, GetKinEnergy, NList skin test).
+ * Returns status; *rebuilt=1 when the list was rebuilt after the step. */
+int  or_velver_step(or_sys *s, double *ekin, int32_t *rebuilt);
+
+/* One Ermak-McCammon step (BDStep, UTotal, NList skin test) with caller noise
+ * xi[np][3]; fac1/fac2 per type. */
+int  or_bd_step(or_sys *s, const double *xi, const double *fac1, const double *fac2,
+                int32_t *rebuilt);
+
+/* MOLSIM's GauRandom with its SAVEd spare carried in (flag, save). */
+double or_gau_random(int32_t *iseed, int32_t *flag, double *save);
+
+/* The reference's own rebuild test (NList iSimulationStep branch) on a given
+ * drostep; updates drosum, returns 1 when a rebuild is due. */
+int  or_skin_test(or_sys *s, const double *drostep, double *max1, double *max2);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,66 @@
+"""Shared helpers of the tests: systems with their tables, and comparison metrics."""
+import functools
+
+import numpy as np
+
+import pyoracle as O
+from molsim_b200 import systems as S
+
+
+def oracle_table(s):
+    """Alpha and pair table from the oracle (RcutToAlpha + PotTwoBodyTab1)."""
+    q2 = float(np.mean(np.asarray(s["az"]) ** 2))
+    alpha = O.rcut_to_alpha(s["uewaldtol"], q2, s["epsi_four_pi"], min(s["boxlen"]), s["rcut"])
+    pot = dict(npt=s["npt"], zat=s["zat"], sigat=s["sigat"], epsat=s["epsat"], rcut=s["rcut"], ualpha=alpha,
+               epsi_four_pi=s["epsi_four_pi"], lewald=int(s["lewald"]), lljcut=int(s["lljcut"]),
+               **{k: s[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab",
+                                    "fmaxtab", "rumaxfac")})
+    t = O.pot_tab(pot)
+    t["ualpha"] = alpha
+    t["r2atat"] = np.zeros(len(t["r2umin"]))
+    return t
+
+
+def oracle_system(s, t, cell=False, maxnneigh=None):
+    d = dict(s)
+    d["ualpha"] = t["ualpha"]
+    return O.System(d, t, maxnneigh=maxnneigh or s["np"], lcellbuild=cell)
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+@functools.lru_cache(maxsize=None)
+def electrolyte_small(n_pairs=64, L=40.0, seed=1, lsurf=False):
+    s = S.electrolyte(seed=seed, n_pairs=n_pairs, L=L, rcut=min(18.0, L / 2 - 2.0), nmesh=16)
+    s["lsurf"] = lsurf
+    return s
+
+
+@functools.lru_cache(maxsize=None)
+def config0():
+    return S.electrolyte(0)
+
+
+@functools.lru_cache(maxsize=None)
+def config1():
+    return S.polyelectrolyte(0)
+
+
+@functools.lru_cache(maxsize=None)
+def pe_small():
+    return S.polyelectrolyte(seed=3, nchain=4, nbead=50, L=80.0, rcut=20.0, nmesh=32, order=5)
+
+
+@functools.lru_cache(maxsize=None)
+def colloid_small():
+    s = S.colloid_bd(seed=2, n_macro=8, n_salt_pairs=400, L=200.0, nmesh=32)
+    s["bd_fac"] = S.bd_factors(s)
+    return s

@@ -1,0 +1,135 @@
+"""GPU parity of the FP64 drop-in path against the FP64 oracle, through the C-ABI.
+
+Bars (from the task's correctness contract):
+  * neighbour-pair set bit-exact (MOLSIM layout: nneighpn and sorted jpnlist rows);
+  * forces within 1e-5 relative RMS (the FP64 path lands near 1e-12);
+  * total energy, its terms and the virial within 1e-7 relative.
+"""
+import numpy as np
+import pytest
+
+import helpers as Hp
+from molsim_b200 import Engine
+from molsim_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5
+ENERGY_TOL = 1e-7
+
+
+def _pair(s, **kw):
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t, cell=s["np"] > 20000)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    g = Engine(s, t, **kw)
+    return t, o, g
+
+
+def _check_nlist(o, g, n):
+    nn_o, jp_o = o.get_vlist()
+    nn_g, jp_g, npair = g.SetVList(0, export=True, maxnneigh=o.maxnneigh)
+    assert npair == int(nn_o.sum())
+    assert np.array_equal(nn_o, nn_g)
+    for ip in range(n):
+        k = nn_o[ip]
+        assert np.array_equal(jp_o[ip, :k], jp_g[ip, :k]), ip
+
+
+def _check_utotal(o, g, ftol=FORCE_TOL, etol=ENERGY_TOL):
+    ro = o.utotal()
+    rg = g.UTotal()
+    assert Hp.rel_rms(rg["force"], ro["force"]) < ftol
+    assert Hp.rel_rms(rg["forceo"], ro["forceo"]) < ftol
+    for k in ("utot", "urec", "virial"):
+        assert Hp.rel(rg[k], ro[k]) < etol, (k, rg[k], ro[k])
+    for p, v in enumerate(ro["utwob"]):
+        assert abs(rg["utwob"][p] - v) <= etol * max(abs(ro["utot"]), abs(v)), (p, rg["utwob"][p], v)
+    if ro["ubond"] != 0.0:
+        assert Hp.rel(rg["ubond"], ro["ubond"]) < etol
+    return ro, rg
+
+
+@pytest.mark.parametrize("lsurf", [False, True])
+def test_small_electrolyte_nlist_and_utotal(lsurf):
+    s = dict(Hp.electrolyte_small(lsurf=lsurf))
+    t, o, g = _pair(s)
+    _check_nlist(o, g, s["np"])
+    ro, rg = _check_utotal(o, g)
+    assert Hp.rel_rms(rg["force"], ro["force"]) < 1e-10
+
+
+def test_config0_electrolyte():
+    s = Hp.config0()
+    t, o, g = _pair(s)
+    _check_nlist(o, g, s["np"])
+    _check_utotal(o, g)
+
+
+def test_config1_polyelectrolyte():
+    s = Hp.config1()
+    t, o, g = _pair(s)
+    _check_nlist(o, g, s["np"])
+    ro, rg = _check_utotal(o, g)
+    assert ro["ubond"] > 0.0
+
+
+def test_velver_short_trajectory():
+    """Ten velocity-Verlet steps (with NList skin tests) against the oracle."""
+    s = dict(Hp.pe_small())
+    s["tstep"] = 0.01
+    t, o, g = _pair(s)
+    o.utotal()
+    st = o.get_state()
+    rodd = np.zeros_like(st["ro"])
+    # GetLinAcc on both sides from the same forces
+    g.UTotal()
+    g.GetLinAcc()
+    rodd = g.get_state()["rodd"]
+    o.set_state(st["ro"], st["rod"], rodd)
+    eg = g.VelVer(10)
+    for k in range(10):
+        ek, _ = o.velver_step()
+        assert Hp.rel(eg[k]["ekin"], ek) < 1e-9
+    sg, so = g.get_state(), o.get_state()
+    d = sg["ro"] - so["ro"]
+    box = s["boxlen"][0]
+    d -= box * np.round(d / box)
+    assert np.abs(d).max() < 1e-9
+    assert Hp.rel_rms(sg["rod"], so["rod"]) < 1e-9
+
+
+def test_bd_with_injected_noise():
+    """Brownian dynamics with the caller's noise (the drop-in mode): five steps."""
+    s = dict(Hp.colloid_small())
+    t, o, g = _pair(s)
+    o.utotal()
+    g.UTotal()
+    rng = np.random.default_rng(7)
+    xi = rng.standard_normal((5, s["np"], 3))
+    fac1, fac2 = s["bd_fac"]
+    eg = g.BDStep(5, xi=xi)
+    for k in range(5):
+        o.bd_step(xi[k], fac1, fac2)
+    sg, so = g.get_state(), o.get_state()
+    d = sg["ro"] - so["ro"]
+    box = s["boxlen"][0]
+    d -= box * np.round(d / box)
+    assert np.abs(d).max() < 1e-9
+    rg, ro = g.UTotal(), o.utotal()
+    assert Hp.rel_rms(rg["force"], ro["force"]) < FORCE_TOL
+    assert Hp.rel(eg[-1]["utot"], ro["utot"]) < ENERGY_TOL
+
+
+def test_batch_equals_alone():
+    """Systems advanced together in one handle give the results they give alone."""
+    sys_list = [dict(Hp.electrolyte_small()), dict(Hp.pe_small())]
+    sys_list[1]["order"] = 4
+    tabs = [Hp.oracle_table(s) for s in sys_list]
+    gb = Engine(sys_list, tabs)
+    for k, (s, t) in enumerate(zip(sys_list, tabs)):
+        ga = Engine(s, t)
+        ra, rb = ga.UTotal(), gb.UTotal(k)
+        assert Hp.rel_rms(rb["force"], ra["force"]) < 1e-12
+        assert Hp.rel(rb["utot"], ra["utot"]) < 1e-12

@@ -1,0 +1,67 @@
+"""CPU checks of the product library: it loads without a GPU, exports every
+entry point declared in include/*.h, and its host set-up routines reproduce
+the oracle's (RcutToAlpha, the pair table)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+import helpers as Hp
+import pyoracle as O
+from molsim_b200 import _lib, pot_tab, rcut_to_alpha
+from molsim_b200 import systems as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if f.endswith(".h"):
+            txt = open(os.path.join(inc, f)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names |= set(re.findall(r"\b(msg_[a-z0-9_]+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = C.CDLL(_lib.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(L, n), n
+    assert names <= set(_lib.SIGNATURES)
+
+
+def test_rcut_to_alpha_matches_oracle():
+    for L_, rc, tol in ((100.0, 30.0, 1e-5), (250.0, 25.0, 1e-5), (1200.0, 30.0, 1e-5), (40.0, 18.0, 1e-4)):
+        epsfp = S.EPSI0_FOUR_PI / 78.4
+        a = rcut_to_alpha(tol, 1.0, epsfp, L_, rc)
+        b = O.rcut_to_alpha(tol, 1.0, epsfp, L_, rc)
+        assert a == b
+        # the Kolafa-Perram estimate at that alpha gives back the tolerance
+        est = O.lib().or_ewald_error_ureal(1.0, L_, a, rc, epsfp)
+        assert abs(est / tol - 1) < 1e-4
+
+
+def test_pot_tab_matches_oracle_bitwise():
+    for s in (Hp.config0(), Hp.colloid_small(), Hp.electrolyte_small()):
+        t = Hp.oracle_table(s)
+        p = pot_tab(s, t["ualpha"])
+        assert np.array_equal(p["iubuflow"], t["iubuflow"])
+        assert np.array_equal(p["nugrid"], t["nugrid"])
+        assert np.array_equal(p["ubuf"], t["ubuf"])
+        assert np.array_equal(p["r2umin"], t["r2umin"])
+
+
+def test_engine_fails_loudly_without_library(monkeypatch, tmp_path):
+    monkeypatch.setattr(_lib, "_LIB", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
+    try:
+        _lib.lib()
+    except RuntimeError as e:
+        assert "not built" in str(e)
+    else:
+        raise AssertionError("loading a missing library must fail")
