@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Throughput of MOLSIM's per-step force/energy path on B200.
+
+Workload (one GPU): the polyelectrolyte solution -- 40 chains x 200 beads
+(-1e, sigma 4 A, harmonic bonds k = 0.4 kT/A^2, r0 = 5 A) plus 8000 counterions,
+16000 particles in a 250 A box; SPME 64^3, order 5, rc = 25 A; tabulated LJ +
+Coulomb; velocity Verlet, dt = 0.005 ps.  A step is one MD step (VelVer + UTotal
++ NList skin test / rebuild).  Synthetic, seeded inputs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank advances its own replica (seed = rank): the path does
+not shard, so N>1 runs N independent replicas ("weak" scaling, no collective
+on the data path).  `--impl reference` times MOLSIM's serial algorithm (the
+FP64 CPU restatement in oracle/, compiled -O2) on the host cores, one replica
+per core.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+WORKLOAD = "polyelectrolyte_16000"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_workload(seed):
+    from molsim_b200 import systems as S
+    return S.polyelectrolyte(seed=seed)
+
+
+# --------------------------------------------------------------------------
+# CPU reference: the oracle, one replica per process
+# --------------------------------------------------------------------------
+def _oracle_worker(args):
+    seed, steps, warm = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle as O
+    from molsim_b200 import systems as S
+    s = S.polyelectrolyte(seed=seed)
+    q2 = float(np.mean(s["az"] ** 2))
+    alpha = O.rcut_to_alpha(s["uewaldtol"], q2, s["epsi_four_pi"], min(s["boxlen"]), s["rcut"])
+    pot = dict(npt=s["npt"], zat=s["zat"], sigat=s["sigat"], epsat=s["epsat"], rcut=s["rcut"], ualpha=alpha,
+               epsi_four_pi=s["epsi_four_pi"], lewald=1, lljcut=1,
+               **{k: s[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab", "fmaxtab",
+                                    "rumaxfac")})
+    t = O.pot_tab(pot)
+    t["r2atat"] = np.zeros(3)
+    d = dict(s)
+    d["ualpha"] = alpha
+    o = O.System(d, t, maxnneigh=512, lcellbuild=True)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    o.utotal()
+    st = o.get_state()
+    fo = o.utotal()["forceo"]
+    o.set_state(st["ro"], st["rod"], fo / s["masspt"][s["iptpn"] - 1][:, None])
+    for _ in range(warm):
+        o.velver_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.velver_step()
+    return s["np"] * steps, time.perf_counter() - t0
+
+
+def cpu_reference(steps, warm, procs):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_oracle_worker, [(1000 + k, steps, warm) for k in range(procs)])
+    # all replicas run concurrently: aggregate = sum of work / longest replica time
+    work = sum(r[0] for r in res)
+    tmax = max(r[1] for r in res)
+    return work / tmax, tmax
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    steps = max(1, min(a.steps, 20))
+    warm = max(0, min(a.warmup, 2))
+    value, tmax = cpu_reference(steps, warm, procs)
+    sample = "%d concurrent replicas x %d velocity-Verlet steps of the 16000-particle polyelectrolyte" % (procs, steps)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": 1000.0 * tmax / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": 16000, "spme": "64^3 order 5", "rcut_A": 25.0,
+                       "integrator": "velocity Verlet", "replicas": procs},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU
+# --------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_profile_traffic():
+    """Per-launch DRAM bytes of the pair kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "pair_kernel_polyelectrolyte_16000.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def run_gpu(a):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from molsim_b200 import Engine, _lib
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    s = make_workload(seed=rank)
+    n = int(s["np"])
+    eng = Engine(s, precision=a.precision)
+    eng.UTotal()
+    eng.GetLinAcc()
+    _, _, npair = eng.SetVList(0, export=False)
+    ext = torch.cuda.ExternalStream(eng.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
+    L = _lib.lib()
+
+    def step_async(k):
+        rc = L.msg_velver_async(eng.h, k)
+        if rc:
+            raise RuntimeError(L.msg_last_error(eng.h).decode())
+
+    # warm-up (also captures the step graph)
+    for _ in range(max(3, a.warmup)):
+        with torch.cuda.stream(ext):
+            flush.zero_()
+        step_async(1)
+    eng.VelVer(1, energies=False)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K steps, L2 flushed before each, device time per step ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    clocks = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = eng.launch_count()
+    for k in range(a.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()
+            starts[k].record(ext)
+        step_async(1)
+        with torch.cuda.stream(ext):
+            ends[k].record(ext)
+    torch.cuda.synchronize()
+    launches = eng.launch_count() - l0
+    clk = clocks.stop()
+    t_ms = sum(st.elapsed_time(en) for st, en in zip(starts, ends))
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+        t_ms = float(tt.item())
+    value = n * a.steps * world / (t_ms / 1000.0)
+
+    # ---- per-kernel device times: the same K steps with the library's CUDA-event timers ----
+    eng.set_timing(True)
+    for k in range(a.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()
+        eng.VelVer(1, energies=False)
+    kt = eng.kernel_times()
+    eng.set_timing(False)
+    total_k = sum(v[0] for v in kt.values()) or 1.0
+    breakdown = {k: {"ms_per_launch": (v[0] / v[1]) if v[1] else 0.0, "share": v[0] / total_k}
+                 for k, v in kt.items() if v[1]}
+
+    # ---- end to end through the C-ABI with host buffers (the drop-in call pattern) ----
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    st0 = eng.get_state(0)
+    ro, rod, rodd = pinned((n, 3)), pinned((n, 3)), pinned((n, 3))
+    ro[:], rod[:], rodd[:] = st0["ro"], st0["rod"], st0["rodd"]
+    e = _lib.MsgEnergy()
+    f64 = C.POINTER(C.c_double)
+    pr = [x.ctypes.data_as(f64) for x in (ro, rod, rodd)]
+    ke = max(10, a.steps // 2)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        assert L.msg_put_state(eng.h, 0, pr[0], pr[1], pr[2], 1) == 0
+        assert L.msg_velver(eng.h, 1, 0, C.byref(e)) == 0
+        assert L.msg_get_state(eng.h, 0, pr[0], pr[1], pr[2]) == 0
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = n * ke * world / t_e2e
+
+    # ---- roofline of the pair kernel ----
+    s_pos = 32 if a.precision == "fp64" else 16
+    s_f = 24
+    b_pair = n * (s_pos + s_f) + 4 * npair
+    t_pair = breakdown.get("pair", {}).get("ms_per_launch", 0.0) / 1000.0
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = b_pair / t_pair / 1e9 if t_pair > 0 else 0.0
+    traffic = read_profile_traffic()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu_steps = 3
+        v, tmax = cpu_reference(cpu_steps, 1, 1)
+        cpu = {"value": v, "unit": METRIC, "cores": 1, "kind": "port",
+               "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
+                         "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
+
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32+i64",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "particles": n, "half_list_pairs": int(npair),
+                       "spme": "64^3 order 5", "rcut_A": 25.0, "skin_A": 2.0, "precision": a.precision,
+                       "integrator": "velocity Verlet", "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
+                    "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
+            "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": b_pair,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
+                         else "fallback 6650 GB/s"},
+            "kernels": breakdown, "gpu_launches": int(launches), "clocks": clk,
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_gpu(a)
+
+
+if __name__ == "__main__":
+    main()

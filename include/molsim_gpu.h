@@ -130,6 +130,11 @@ int  msg_get_linacc(msg_handle *h);
  * e (optional): [nsteps] energies of system isys after each step. */
 int  msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energy *e);
 
+/* As msg_velver without energies, but returns once the steps are enqueued on
+ * the handle's stream (msg_stream); device errors surface at the next
+ * synchronous call. */
+int  msg_velver_async(msg_handle *h, int32_t nsteps);
+
 /* nsteps Brownian-dynamics steps.  xi == NULL: FP32 normal noise from a
  * Philox4x32-10 stream keyed by (seed, particle, step); otherwise xi holds
  * caller noise for system isys, [nsteps][np][3] (for the drop-in, MOLSIM's
@@ -139,6 +144,21 @@ int  msg_bd_step(msg_handle *h, int32_t nsteps, uint64_t seed, int32_t isys,
 
 /* Number of list rebuilds since creation, for system isys. */
 int64_t msg_nrebuild(const msg_handle *h, int32_t isys);
+
+/* Like msg_set_state; keep_list != 0 states that ro continues the trajectory the
+ * device holds (e.g. it came back from msg_get_state), so the Verlet list and
+ * the skin accumulator drosum stay valid and no rebuild is forced. */
+int  msg_put_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd,
+                   int32_t keep_list);
+
+/* Instrumentation: the handle's CUDA stream (cudaStream_t), kernel launches
+ * issued so far, and per-kernel CUDA-event timers (enabled by msg_set_timing). */
+void   *msg_stream(const msg_handle *h);
+int64_t msg_launch_count(const msg_handle *h);
+int     msg_set_timing(msg_handle *h, int32_t on);
+/* Timer k (0 <= k < msg_ntimers()): name, summed device milliseconds, launches. */
+int32_t msg_ntimers(void);
+int     msg_kernel_time(const msg_handle *h, int32_t k, const char **name, double *total_ms, int64_t *launches);
 
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,

@@ -57,8 +57,15 @@ SIGNATURES = {
     "msg_utotal": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_get_linacc": (C.c_int, [C.c_void_p]),
     "msg_velver": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MsgEnergy)]),
+    "msg_velver_async": (C.c_int, [C.c_void_p, C.c_int32]),
     "msg_bd_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_uint64, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_nrebuild": (C.c_int64, [C.c_void_p, C.c_int32]),
+    "msg_put_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p, C.c_int32]),
+    "msg_stream": (C.c_void_p, [C.c_void_p]),
+    "msg_launch_count": (C.c_int64, [C.c_void_p]),
+    "msg_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "msg_ntimers": (C.c_int32, []),
+    "msg_kernel_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_char_p), f64p, C.POINTER(C.c_int64)]),
     "msg_rcut_to_alpha": (C.c_double, [C.c_double] * 5 + [i32p]),
     "msg_pot_tab": (C.c_int, [C.POINTER(MsgTabParams), f64p, C.c_int32, i32p, i32p, f64p, i32p]),
 }

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -62,6 +63,10 @@ struct HostSys {
     msg_params p;
 };
 
+enum { TM_POS, TM_SKIN, TM_PAIR, TM_SPREAD, TM_FFT, TM_INFL, TM_FINAL, TM_REDUCE, TM_REBUILD, TM_N };
+const char *const kTimerNames[TM_N] = {"position_update", "skin_test", "pair", "spread", "fft",
+                                        "influence", "gather_finalize", "reduce", "rebuild"};
+
 struct FftClass {
     int s, count;
     long long grid_off, cgrid_off;
@@ -88,7 +93,7 @@ struct msg_handle {
     uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *rhist = nullptr;
     int ncell_tot = 0, cell_bits = 1;
     int *cstart = nullptr, *cend = nullptr;
-    int *nbl = nullptr, *nnb = nullptr;
+    int *nbl = nullptr, *nnb = nullptr, *nmaxrow = nullptr;
     long long nbl_tot = 0;
     // skin
     double *r2o = nullptr, *skinout = nullptr;
@@ -129,16 +134,91 @@ struct msg_handle {
     double *xin = nullptr;
     size_t xin_n = 0;
     SysDev *dsys = nullptr;
+    // instrumentation
+    long long launches = 0;
+    bool timing = false;
+    std::vector<cudaEvent_t> evpool;
+    std::vector<int> pend_k;
+    std::vector<cudaEvent_t> pend_a, pend_b;
+    cudaEvent_t open_ev[TM_N] = {};
+    double tm_ms[TM_N] = {};
+    long long tm_n[TM_N] = {};
 
     ~msg_handle();
+    cudaEvent_t get_event()
+    {
+        cudaEvent_t e;
+        if (!evpool.empty()) {
+            e = evpool.back();
+            evpool.pop_back();
+        } else {
+            CK(cudaEventCreate(&e));
+        }
+        return e;
+    }
+    bool capturing = false;
+    void rec_event(cudaEvent_t e)
+    {
+        // under stream capture an external record node keeps the timestamp in the graph
+        CK(cudaEventRecordWithFlags(e, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    }
+    void tbeg(int k)
+    {
+        if (!timing) return;
+        open_ev[k] = get_event();
+        rec_event(open_ev[k]);
+    }
+    void tend(int k)
+    {
+        if (!timing) return;
+        cudaEvent_t b = get_event();
+        rec_event(b);
+        pend_k.push_back(k);
+        pend_a.push_back(open_ev[k]);
+        pend_b.push_back(b);
+    }
+    void flush_timers()
+    {
+        for (size_t q = 0; q < pend_k.size(); ++q) {
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, pend_a[q], pend_b[q]));
+            tm_ms[pend_k[q]] += ms;
+            tm_n[pend_k[q]] += 1;
+            evpool.push_back(pend_a[q]);
+            evpool.push_back(pend_b[q]);
+        }
+        pend_k.clear();
+        pend_a.clear();
+        pend_b.clear();
+    }
     void build(const msg_params *p, int n, int prec);
     void enqueue_rebuild();
     void enqueue_forces(int mode);
     void enqueue_reduce(bool record);
     void enqueue_md_step(bool record);
     void enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record);
+    // CUDA graph of one step; the rebuild sits in an IF node opened by k_skin
+    cudaGraphConditionalHandle cond = 0;
+    int use_cond = 0;
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        int kind = -1;            // 0 MD, 1 BD (Philox noise)
+        bool record = false, timing = false;
+        uint64_t seed = 0;
+        double *hist = nullptr;
+        int hist_cap = 0;
+        long long launches = 0;
+        std::vector<int> tk;
+        std::vector<cudaEvent_t> ta, tb;
+    } graph;
+    bool use_graphs = true;
+    void drop_graph();
+    void ensure_graph(int kind, bool record, uint64_t seed);
+    void launch_graph();
     void ensure_stage(size_t n);
     int check();
+    bool grow_lists();
+    int rebuild_checked(const std::vector<int> &flags);
 };
 
 static void free_all(msg_handle *h)
@@ -146,7 +226,7 @@ static void free_all(msg_handle *h)
     void *ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->acc[0], h->acc[1], h->dsum[0], h->dsum[1],
                     h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
                     h->sysid, h->fsr, h->ftot, h->pos32, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
-                    h->cend, h->nbl, h->nnb, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
+                    h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
                     h->t128, h->t32, h->chunks, h->infl, h->ppart, h->fpart, h->ipart, h->psurf, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
@@ -158,11 +238,19 @@ static void free_all(msg_handle *h)
         if (f.bwd) cufftDestroy(f.bwd);
     }
     h->fft.clear();
+    for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->pend_a) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->pend_b) cudaEventDestroy(e);
+    h->evpool.clear();
     if (h->st) cudaStreamDestroy(h->st);
     h->st = nullptr;
 }
 
-msg_handle::~msg_handle() { free_all(this); }
+msg_handle::~msg_handle()
+{
+    drop_graph();
+    free_all(this);
+}
 
 void msg_handle::ensure_stage(size_t n)
 {
@@ -186,9 +274,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     order = P[0].order;
     std::vector<HostSys> H(n);
     ntot = 0;
-    int type_tot = 0, pt_tot = 0, ptmap_tot = 0, cell_tot = 0, t128 = 0, t32 = 0, nch = 0, nif = 0;
+    int type_tot = 0, pt_tot = 0, ptmap_tot = 0, cell_tot = 0, t128 = 0, t32 = 0, nch = 0;
     long long nbl_acc = 0;
-    int ntab = 0;
     size_t nbond_tot = 0;
     for (int s = 0; s < n; ++s) {
         const msg_params &p = P[s];
@@ -262,7 +349,6 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         H[s].p = p;
         if (p.bd_fac1 && p.bd_fac2) has_bd = 1;
         if (p.lewald) any_ewald = 1;
-        (void)ntab;
     }
     ncell_tot = cell_tot;
     cell_bits = 1;
@@ -520,6 +606,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     cend = dalloc<int>(ncell_tot);
     nbl = dalloc<int>(nbl_tot);
     nnb = dalloc<int>(ntot);
+    nmaxrow = dalloc<int>(n);
     r2o = dalloc<double>(ntot);
     skinout = dalloc<double>(2 * (size_t)n);
     sc = dalloc<SkinChunk>(nchunk);
@@ -545,50 +632,67 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 // ---------------------------------------------------------------------------
 void msg_handle::enqueue_rebuild()
 {
-    const int c = cur, o = 1 - cur;
-    k_rb_keys<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[c], orig[c], cellid, k0, v0);
+    // cur stays 0: rebuilt systems are permuted into the [1] buffers and copied home
+    tbeg(TM_REBUILD);
+    k_rb_keys<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], orig[0], cellid, k0, v0);
     const bool in1 = radix_sort_pairs(k0, v0, k1, v1, rhist, ntot, cell_bits, st);
     const uint32_t *sk = in1 ? k1 : k0, *sv = in1 ? v1 : v0;
-    k_permute<<<nt128, 128, 0, st>>>(dsys, t128, flag, sk, sv, pos[c], pos[o], vel[c], vel[o], acc[c], acc[o],
-                                      dsum[c], dsum[o], fo[c], fo[o], typ[c], typ[o], orig[c], orig[o], cellid,
-                                      inv);
-    cur = o;
-    CK(cudaMemsetAsync(cstart, 0, sizeof(int) * ncell_tot, st));
-    CK(cudaMemsetAsync(cend, 0, sizeof(int) * ncell_tot, st));
+    k_permute<<<nt128, 128, 0, st>>>(dsys, t128, flag, sk, sv, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1],
+                                      fo[0], fo[1], typ[0], typ[1], orig[0], orig[1], cellid, inv);
+    k_copyback<<<nt128, 128, 0, st>>>(t128, flag, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1], fo[0], fo[1],
+                                       typ[0], typ[1], orig[0], orig[1], dsum[0]);
+    k_clear_cells<<<(ncell_tot + 255) / 256, 256, 0, st>>>(cstart, cend, ncell_tot);
     k_cellrange<<<(ntot + 255) / 256, 256, 0, st>>>(cellid, sysid, flag, ntot, cstart, cend);
-    k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[cur], cellid, cstart, cend, nbl, nnb,
-                                                     ntot, errw);
+    k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[0], cellid, cstart, cend, nbl, nnb,
+                                                     ntot, nmaxrow, errw);
+    tend(TM_REBUILD);
+    launches += 6 + 3 * ((cell_bits + 7) / 8);
 }
 
 template <int P>
 static void launch_spme(msg_handle *h)
 {
     const int c = h->cur;
+    h->tbeg(TM_SPREAD);
     CK(cudaMemsetAsync(h->rgrid, 0, sizeof(double) * h->grid_tot, h->st));
-    k_spread_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->rgrid);
+    k_spread_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->rgrid, h->psurf);
+    h->tend(TM_SPREAD);
+    h->tbeg(TM_FFT);
     for (auto &f : h->fft)
         CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
+    h->tend(TM_FFT);
+    h->tbeg(TM_INFL);
     k_influence_fp64<<<h->ninfl, INFL_THREADS, 0, h->st>>>(h->dsys, h->infl, h->cgrid, h->mfac, h->emf, h->vmf,
                                                           h->ipart);
+    h->tend(TM_INFL);
+    h->tbeg(TM_FFT);
     for (auto &f : h->fft)
         CKF(cufftExecZ2D(f.bwd, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off), h->rgrid + f.grid_off));
+    h->tend(TM_FFT);
+    h->launches += 2;
 }
 
 template <int P>
 static void launch_finalize(msg_handle *h, int mode)
 {
     const int c = h->cur;
+    h->tbeg(TM_FINAL);
+    h->launches += 1;
     k_finalize_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->typ[c], h->orig[c], h->inv,
                                                     h->rgrid, h->fsr, h->psurf, h->bptr, h->bpart, h->bk, h->beq,
                                                     h->bpw, h->massip, h->massp, h->ftot, h->fo[c], h->vel[c],
                                                     h->acc[c], h->fpart, mode, h->errw);
+    h->tend(TM_FINAL);
 }
 
 void msg_handle::enqueue_forces(int mode)
 {
     const int c = cur;
+    tbeg(TM_PAIR);
     k_pair_fp64<<<nt32, PAIR_THREADS, 0, st>>>(dsys, t32, pos[c], typ[c], nbl, nnb, ptmap, ptab, tz, tc, bst, fsr,
                                                ppart, errw);
+    tend(TM_PAIR);
+    launches += 1;
     if (any_ewald) {
         switch (order) {
         case 4: launch_spme<4>(this); break;
@@ -605,35 +709,200 @@ void msg_handle::enqueue_forces(int mode)
 
 void msg_handle::enqueue_reduce(bool record)
 {
+    tbeg(TM_REDUCE);
     k_reduce<<<nsys, 256, 0, st>>>(dsys, ppart, ipart, fpart, psurf, esys, record ? hist : nullptr, hist_cap,
                                    stepctr, sstep, rdone, nsys);
+    tend(TM_REDUCE);
+    launches += 1;
 }
 
 void msg_handle::enqueue_md_step(bool record)
 {
     const int c = cur;
-    k_vv_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], vel[c], acc[c], dsum[c], orig[c], r2o, psurf, pos32);
-    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout);
+    tbeg(TM_POS);
+    k_vv_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], vel[c], acc[c], dsum[c], orig[c], r2o, nullptr, pos32);
+    tend(TM_POS);
+    tbeg(TM_SKIN);
+    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
+    tend(TM_SKIN);
+    launches += 2;
     enqueue_forces(1);
     enqueue_reduce(record);
-    enqueue_rebuild();
+    if (!use_cond) enqueue_rebuild();
 }
 
 void msg_handle::enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record)
 {
     const int c = cur;
+    tbeg(TM_POS);
     k_bd_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], fo[c], dsum[c], orig[c], typ[c], fac1, fac2, xin_step,
-                                    xout_step, seed, sstep, r2o, psurf, pos32);
-    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout);
+                                    xout_step, seed, sstep, r2o, nullptr, pos32);
+    tend(TM_POS);
+    tbeg(TM_SKIN);
+    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
+    tend(TM_SKIN);
+    launches += 2;
     enqueue_forces(0);
     enqueue_reduce(record);
+    if (!use_cond) enqueue_rebuild();
+}
+
+// Row capacity follows the longest row seen (x1.5 + 32).  When a system's rows
+// outgrow it, every list is re-laid out and rebuilt.  Returns true on growth.
+bool msg_handle::grow_lists()
+{
+    std::vector<int> mx(nsys);
+    CK(cudaMemcpy(mx.data(), nmaxrow, nsys * sizeof(int), cudaMemcpyDeviceToHost));
+    bool grow = false;
+    std::vector<int> cap(nsys);
+    for (int s = 0; s < nsys; ++s) {
+        int need = (int)std::ceil(1.5 * mx[s]) + 32;
+        need = std::min(((need + 7) / 8) * 8, std::max(8, ((hs[s].n + 7) / 8) * 8));
+        cap[s] = hs[s].cap;
+        if (need > hs[s].cap) {
+            cap[s] = need;
+            grow = true;
+        }
+    }
+    if (!grow) return false;
+    drop_graph();
+    long long acc = 0;
+    for (int s = 0; s < nsys; ++s) {
+        hs[s].cap = cap[s];
+        hs[s].nbl_off = acc;
+        acc += (long long)cap[s] * hs[s].n;
+    }
+    CK(cudaStreamSynchronize(st));
+    CK(cudaFree(nbl));
+    nbl = dalloc<int>(acc);
+    nbl_tot = acc;
+    CK(cudaMemcpy(dsys, hs.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice));
+    return true;
+}
+
+// Rebuild the flagged systems; on a capacity overflow grow the rows and rebuild all.
+int msg_handle::rebuild_checked(const std::vector<int> &flags)
+{
+    h2d(flag, flags.data(), nsys, st);
     enqueue_rebuild();
+    int rc = check();
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        if (rc != MSG_OK && rc != MSG_ERR_CAPACITY) return rc;
+        if (!grow_lists()) return rc;
+        std::vector<int> all(nsys, 1);
+        h2d(flag, all.data(), nsys, st);
+        enqueue_rebuild();
+        rc = check();
+    }
+    return rc;
+}
+
+void msg_handle::drop_graph()
+{
+    if (graph.exec) cudaGraphExecDestroy(graph.exec);
+    for (cudaEvent_t e : graph.ta) cudaEventDestroy(e);
+    for (cudaEvent_t e : graph.tb) cudaEventDestroy(e);
+    graph = StepGraph();
+}
+
+void msg_handle::ensure_graph(int kind, bool record, uint64_t seed)
+{
+    if (graph.exec && graph.kind == kind && graph.record == record && graph.timing == timing &&
+        (kind == 0 || graph.seed == seed) && graph.hist == (record ? hist : nullptr) &&
+        graph.hist_cap == (record ? hist_cap : 0))
+        return;
+    drop_graph();
+    CK(cudaStreamSynchronize(st));
+    flush_timers();
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0u, cudaGraphCondAssignDefault));
+    const long long l0 = launches;
+    const size_t p0 = pend_k.size();
+    CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    use_cond = 1;
+    if (kind == 0)
+        enqueue_md_step(record);
+    else
+        enqueue_bd_step(seed, nullptr, nullptr, record);
+    use_cond = 0;
+    // the rebuild: an IF node after everything captured so far
+    tbeg(TM_REBUILD);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    CK(cudaGraphAddNode(&cn, g, deps, nd, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+    cudaEvent_t rb_begin = timing ? open_ev[TM_REBUILD] : nullptr;
+    if (timing) {
+        cudaEvent_t b = get_event();
+        rec_event(b);
+        pend_k.push_back(TM_REBUILD);
+        pend_a.push_back(rb_begin);
+        pend_b.push_back(b);
+    }
+    CK(cudaStreamEndCapture(st, &g));
+    capturing = false;
+    // capture the rebuild into the body graph (timers off inside: the IF node is timed as a whole)
+    const bool tsave = timing;
+    timing = false;
+    CK(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_rebuild();
+    cudaGraph_t bdone;
+    CK(cudaStreamEndCapture(st, &bdone));
+    timing = tsave;
+    CK(cudaGraphInstantiate(&graph.exec, g, 0));
+    CK(cudaGraphDestroy(g));
+    graph.kind = kind;
+    graph.record = record;
+    graph.timing = timing;
+    graph.seed = seed;
+    graph.hist = record ? hist : nullptr;
+    graph.hist_cap = record ? hist_cap : 0;
+    graph.launches = launches - l0;
+    launches = l0;
+    // events captured as graph nodes stay with the graph and are read after each launch
+    for (size_t q = p0; q < pend_k.size(); ++q) {
+        graph.tk.push_back(pend_k[q]);
+        graph.ta.push_back(pend_a[q]);
+        graph.tb.push_back(pend_b[q]);
+    }
+    pend_k.resize(p0);
+    pend_a.resize(p0);
+    pend_b.resize(p0);
+}
+
+void msg_handle::launch_graph()
+{
+    CK(cudaGraphLaunch(graph.exec, st));
+    launches += graph.launches;
+    if (graph.timing) {
+        // the graph's event nodes are re-recorded by every launch: read them now
+        CK(cudaStreamSynchronize(st));
+        for (size_t q = 0; q < graph.tk.size(); ++q) {
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, graph.ta[q], graph.tb[q]));
+            tm_ms[graph.tk[q]] += ms;
+            tm_n[graph.tk[q]] += 1;
+        }
+    }
 }
 
 int msg_handle::check()
 {
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
+    flush_timers();
     ErrWord e;
     CK(cudaMemcpy(&e, errw, sizeof(e), cudaMemcpyDeviceToHost));
     if (e.code) {
@@ -666,6 +935,8 @@ static int create_impl(const msg_params *p, int32_t nsys, int32_t precision, msg
 {
     if (!p || !out || nsys < 1 || (precision != MSG_PREC_FP64 && precision != MSG_PREC_MIXED)) return MSG_ERR_ARG;
     msg_handle *h = new msg_handle();
+    // MSG_NO_GRAPHS=1 launches every kernel directly instead of replaying a CUDA graph
+    if (const char *ng = std::getenv("MSG_NO_GRAPHS")) h->use_graphs = !(ng[0] == '1');
     try {
         h->build(p, nsys, precision);
         // initial neighbour lists: every system is rebuilt from its set-up order
@@ -697,10 +968,9 @@ extern "C" const char *msg_last_error(const msg_handle *h) { return h ? h->err.c
 
 extern "C" int32_t msg_nsys(const msg_handle *h) { return h ? h->nsys : 0; }
 
-extern "C" int msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd)
+static int put_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd,
+                     bool keep_list)
 {
-    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
-    API_BEGIN
     const SysDev &S = h->hs[isys];
     h->ensure_stage(3 * (size_t)S.n);
     const int c = h->cur, nb = (S.n + 255) / 256;
@@ -710,15 +980,31 @@ extern "C" int msg_set_state(msg_handle *h, int32_t isys, const double *ro, cons
         if (!src[k]) continue;
         h2d(h->stage, src[k], 3 * (size_t)S.n, h->st);
         k_to_internal<<<nb, 256, 0, h->st>>>(h->stage, dst[k], h->inv, S.off, S.n, k == 0 ? 1 : 0);
+        h->launches += 1;
     }
-    if (ro) {
-        // positions changed: rebuild this system's list now (drosum is reset by the rebuild)
+    if (ro && !keep_list) {
+        // new positions: rebuild this system's list now (the rebuild resets drosum)
         std::vector<int> f(h->nsys, 0);
         f[isys] = 1;
-        h2d(h->flag, f.data(), h->nsys, h->st);
-        h->enqueue_rebuild();
+        return h->rebuild_checked(f);
     }
     return h->check();
+}
+
+extern "C" int msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    return put_state(h, isys, ro, rod, rodd, false);
+    API_END
+}
+
+extern "C" int msg_put_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd,
+                             int32_t keep_list)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    return put_state(h, isys, ro, rod, rodd, keep_list != 0);
     API_END
 }
 
@@ -734,6 +1020,7 @@ extern "C" int msg_get_state(msg_handle *h, int32_t isys, double *ro, double *ro
     for (int k = 0; k < 3; ++k) {
         if (!dst[k]) continue;
         k_to_molsim<<<nb, 256, 0, h->st>>>(src[k], h->stage, h->inv, S.off, S.n, 1.0);
+        h->launches += 1;
         CK(cudaMemcpyAsync(dst[k], h->stage, 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
     }
     return h->check();
@@ -747,9 +1034,7 @@ extern "C" int msg_build_nlist(msg_handle *h, int32_t isys, int32_t *nneighpn, i
     API_BEGIN
     std::vector<int> f(h->nsys, 0);
     f[isys] = 1;
-    h2d(h->flag, f.data(), h->nsys, h->st);
-    h->enqueue_rebuild();
-    int rc = h->check();
+    int rc = h->rebuild_checked(f);
     if (rc) return rc;
     const SysDev &S = h->hs[isys];
     if (npair) {
@@ -854,10 +1139,35 @@ extern "C" int msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energ
     API_BEGIN
     const bool rec = e != nullptr;
     if (rec) prepare_hist(h, nsteps);
-    for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(rec);
+    if (h->use_graphs && nsteps > 0) {
+        h->ensure_graph(0, rec, 0);
+        for (int k = 0; k < nsteps; ++k) h->launch_graph();
+    } else {
+        for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(rec);
+    }
     int rc = h->check();
     if (rc) return rc;
     if (rec) copy_hist(h, nsteps, isys, e);
+    if (h->grow_lists()) {
+        std::vector<int> all(h->nsys, 1);
+        return h->rebuild_checked(all);
+    }
+    return MSG_OK;
+    API_END
+}
+
+extern "C" int msg_velver_async(msg_handle *h, int32_t nsteps)
+{
+    if (!h || nsteps < 0) return MSG_ERR_ARG;
+    API_BEGIN
+    if (h->timing) return MSG_ERR_ARG;   // timers need the synchronous call
+    if (h->use_graphs && nsteps > 0) {
+        h->ensure_graph(0, false, 0);
+        for (int k = 0; k < nsteps; ++k) h->launch_graph();
+    } else {
+        for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(false);
+    }
+    CK(cudaGetLastError());
     return MSG_OK;
     API_END
 }
@@ -884,8 +1194,13 @@ extern "C" int msg_bd_step(msg_handle *h, int32_t nsteps, uint64_t seed, int32_t
         for (int k = 0; k < nsteps; ++k)
             h2d(h->xin + k * per + 3 * (size_t)S.off, xi + (size_t)k * 3 * S.n, 3 * (size_t)S.n, h->st);
     }
-    for (int k = 0; k < nsteps; ++k)
-        h->enqueue_bd_step(seed, xi ? h->xin + k * per : nullptr, xi_out ? h->xin + k * per : nullptr, rec);
+    if (h->use_graphs && !xi && !xi_out && nsteps > 0) {
+        h->ensure_graph(1, rec, seed);
+        for (int k = 0; k < nsteps; ++k) h->launch_graph();
+    } else {
+        for (int k = 0; k < nsteps; ++k)
+            h->enqueue_bd_step(seed, xi ? h->xin + k * per : nullptr, xi_out ? h->xin + k * per : nullptr, rec);
+    }
     int rc = h->check();
     if (rc) return rc;
     if (xi_out) {
@@ -906,4 +1221,31 @@ extern "C" int64_t msg_nrebuild(const msg_handle *h, int32_t isys)
     long long v = 0;
     if (cudaMemcpy(&v, h->nrebuild + isys, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     return v;
+}
+
+extern "C" void *msg_stream(const msg_handle *h) { return h ? (void *)h->st : nullptr; }
+
+extern "C" int64_t msg_launch_count(const msg_handle *h) { return h ? h->launches : -1; }
+
+extern "C" int msg_set_timing(msg_handle *h, int32_t on)
+{
+    if (!h) return MSG_ERR_ARG;
+    h->timing = on != 0;
+    if (h->graph.exec && h->graph.timing != h->timing) h->drop_graph();
+    for (int k = 0; k < TM_N; ++k) {
+        h->tm_ms[k] = 0.0;
+        h->tm_n[k] = 0;
+    }
+    return MSG_OK;
+}
+
+extern "C" int32_t msg_ntimers(void) { return TM_N; }
+
+extern "C" int msg_kernel_time(const msg_handle *h, int32_t k, const char **name, double *total_ms, int64_t *launches)
+{
+    if (!h || k < 0 || k >= TM_N) return MSG_ERR_ARG;
+    if (name) *name = kTimerNames[k];
+    if (total_ms) *total_ms = h->tm_ms[k];
+    if (launches) *launches = h->tm_n[k];
+    return MSG_OK;
 }

@@ -121,45 +121,69 @@ __global__ void __launch_bounds__(PAIR_THREADS) k_pair_fp64(
 // ---------------------------------------------------------------------------
 // SPME charge spreading (Src/energy.F90:1226-1245): Q(k - i) += q*Mx*My*Mz.
 // ---------------------------------------------------------------------------
+// Also writes the per-tile dipole sums sum(q r) of the surface term
+// (UEwaldSurf, Src/energy.F90:1354-1357) from the same final positions.
+__device__ __forceinline__ void tile_dipole(const SysDev &S, double qx, double qy, double qz,
+                                            double *__restrict__ psurf)
+{
+    __shared__ double red[3][4];
+    qx = warp_sum(qx);
+    qy = warp_sum(qy);
+    qz = warp_sum(qz);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { red[0][w] = qx; red[1][w] = qy; red[2][w] = qz; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double s = 0.0;
+        for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
+        psurf[blockIdx.x * 4 + threadIdx.x] = s;
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(128) k_spread_fp64(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                                    const double4 *__restrict__ pos, double *__restrict__ grid)
+                                                    const double4 *__restrict__ pos, double *__restrict__ grid,
+                                                    double *__restrict__ psurf)
 {
     const Tile T = tiles[blockIdx.x];
     const SysDev &S = sysv[T.sys];
+    if (!S.lewald) return;
     const int i = T.i0 + threadIdx.x;
-    if (i >= T.i1 || !S.lewald) return;
-    const double4 x = pos[i];
-    const int s = S.s;
-    double th[3][P], dth[3][P];
-    int km[3];
-    const double xc[3] = {x.x, x.y, x.z};
+    double4 x = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (i < T.i1) {
+        x = pos[i];
+        const int s = S.s;
+        double th[3][P], dth[3][P];
+        int km[3];
+        const double xc[3] = {x.x, x.y, x.z};
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        int k = bspline<P>(S.dkdr[m] * xc[m], th[m], dth[m]);
-        k %= s;
-        km[m] = k < 0 ? k + s : k;
-    }
-    double *G = grid + S.grid_off;
+        for (int m = 0; m < 3; ++m) {
+            int k = bspline<P>(S.dkdr[m] * xc[m], th[m], dth[m]);
+            k %= s;
+            km[m] = k < 0 ? k + s : k;
+        }
+        double *G = grid + S.grid_off;
 #pragma unroll
-    for (int iz = 0; iz < P; ++iz) {
-        int nz = km[2] - iz;
-        nz += (nz < 0) ? s : 0;
-        const double qz = x.w * th[2][iz];
+        for (int iz = 0; iz < P; ++iz) {
+            int nz = km[2] - iz;
+            nz += (nz < 0) ? s : 0;
+            const double qz = x.w * th[2][iz];
 #pragma unroll
-        for (int iy = 0; iy < P; ++iy) {
-            int ny = km[1] - iy;
-            ny += (ny < 0) ? s : 0;
-            const double qyz = qz * th[1][iy];
-            double *rowp = G + ((size_t)nz * s + ny) * s;
+            for (int iy = 0; iy < P; ++iy) {
+                int ny = km[1] - iy;
+                ny += (ny < 0) ? s : 0;
+                const double qyz = qz * th[1][iy];
+                double *rowp = G + ((size_t)nz * s + ny) * s;
 #pragma unroll
-            for (int ix = 0; ix < P; ++ix) {
-                int nx = km[0] - ix;
-                nx += (nx < 0) ? s : 0;
-                atomicAdd(rowp + nx, qyz * th[0][ix]);
+                for (int ix = 0; ix < P; ++ix) {
+                    int nx = km[0] - ix;
+                    nx += (nx < 0) ? s : 0;
+                    atomicAdd(rowp + nx, qyz * th[0][ix]);
+                }
             }
         }
     }
+    if (S.lsurf) tile_dipole(S, x.w * x.x, x.w * x.y, x.w * x.z, psurf);
 }
 
 // ---------------------------------------------------------------------------

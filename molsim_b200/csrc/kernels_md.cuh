@@ -260,7 +260,8 @@ __device__ double chunk_nonrecord_max(const double *r2, int o0, int o1, double P
 __global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ sysv, const int4 *__restrict__ chunks,
                                                     const double *__restrict__ r2o, SkinChunk *__restrict__ sc,
                                                     unsigned *__restrict__ sysdone, int *__restrict__ flag,
-                                                    long long *__restrict__ nrebuild, double *__restrict__ skinout)
+                                                    long long *__restrict__ nrebuild, double *__restrict__ skinout,
+                                                    cudaGraphConditionalHandle cond, int use_cond)
 {
     __shared__ double smd[SK_THREADS / 32];
     __shared__ int smi[SK_THREADS / 32];
@@ -352,7 +353,11 @@ __global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ 
     if (t == 0) {
         const int rebuild = (sqrt(carry) + sqrt(m2) > S.drnlist) ? 1 : 0;
         flag[s] = rebuild;
-        if (rebuild) nrebuild[s] += 1;
+        if (rebuild) {
+            nrebuild[s] += 1;
+            // inside a CUDA graph: open the conditional rebuild node of this step
+            if (use_cond) cudaGraphSetConditional(cond, 1u);
+        }
         if (skinout) { skinout[2 * s] = carry; skinout[2 * s + 1] = m2; }
         sysdone[s] = 0u;
     }
@@ -392,35 +397,67 @@ __global__ void __launch_bounds__(128) k_rb_keys(const SysDev *__restrict__ sysv
     }
 }
 
-// Gather every per-particle array into the sorted order (double buffers).
+// Gather the per-particle arrays of rebuilt systems into the sorted order
+// (into scratch buffers; k_copyback moves them home).  Systems that are not
+// rebuilt keep their order, so their particles are not touched.
 __global__ void __launch_bounds__(128) k_permute(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
                                                 const int *__restrict__ flag, const uint32_t *__restrict__ skey,
                                                 const uint32_t *__restrict__ sval,
                                                 const double4 *__restrict__ pos0, double4 *__restrict__ pos1,
                                                 const double4 *__restrict__ vel0, double4 *__restrict__ vel1,
                                                 const double4 *__restrict__ acc0, double4 *__restrict__ acc1,
-                                                const double4 *__restrict__ dsum0, double4 *__restrict__ dsum1,
                                                 const double4 *__restrict__ fo0, double4 *__restrict__ fo1,
                                                 const int *__restrict__ typ0, int *__restrict__ typ1,
                                                 const int *__restrict__ orig0, int *__restrict__ orig1,
                                                 int *__restrict__ cellid, int *__restrict__ inv)
 {
     const Tile T = tiles[blockIdx.x];
+    if (!flag[T.sys]) return;
     const SysDev &S = sysv[T.sys];
     const int j = T.i0 + threadIdx.x;
     if (j >= T.i1) return;
     const int i = (int)sval[j];
-    const bool rb = flag[T.sys] != 0;
     pos1[j] = pos0[i];
     vel1[j] = vel0[i];
     acc1[j] = acc0[i];
     fo1[j] = fo0[i];
-    dsum1[j] = rb ? make_double4(0.0, 0.0, 0.0, 0.0) : dsum0[i];
     typ1[j] = typ0[i];
     const int o = orig0[i];
     orig1[j] = o;
     cellid[j] = (int)skey[j];
     inv[S.off + o] = j;
+}
+
+// Home the permuted arrays and reset drosum (NList: drosum = Zero at a rebuild).
+__global__ void __launch_bounds__(128) k_copyback(const Tile *__restrict__ tiles, const int *__restrict__ flag,
+                                                 double4 *__restrict__ pos0, const double4 *__restrict__ pos1,
+                                                 double4 *__restrict__ vel0, const double4 *__restrict__ vel1,
+                                                 double4 *__restrict__ acc0, const double4 *__restrict__ acc1,
+                                                 double4 *__restrict__ fo0, const double4 *__restrict__ fo1,
+                                                 int *__restrict__ typ0, const int *__restrict__ typ1,
+                                                 int *__restrict__ orig0, const int *__restrict__ orig1,
+                                                 double4 *__restrict__ dsum)
+{
+    const Tile T = tiles[blockIdx.x];
+    if (!flag[T.sys]) return;
+    const int j = T.i0 + threadIdx.x;
+    if (j >= T.i1) return;
+    pos0[j] = pos1[j];
+    vel0[j] = vel1[j];
+    acc0[j] = acc1[j];
+    fo0[j] = fo1[j];
+    typ0[j] = typ1[j];
+    orig0[j] = orig1[j];
+    dsum[j] = make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+__global__ void k_clear_cells(int *__restrict__ cstart, int *__restrict__ cend, int n)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) {
+        cstart[c] = 0;
+        cend[c] = 0;
+    }
 }
 
 __global__ void k_cellrange(const int *__restrict__ cellid, const int *__restrict__ sys,
@@ -454,7 +491,8 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
                                               const int *__restrict__ flag, const double4 *__restrict__ pos,
                                               const int *__restrict__ cellid, const int *__restrict__ cstart,
                                               const int *__restrict__ cend, int *__restrict__ nbl,
-                                              int *__restrict__ nnb, int ntot, ErrWord *err)
+                                              int *__restrict__ nnb, int ntot, int *__restrict__ nmaxrow,
+                                              ErrWord *err)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -493,6 +531,7 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
             }
     if (lane == 0) {
         nnb[i] = min(count, S.cap);
+        atomicMax(nmaxrow + s, count);
         if (count > S.cap) raise_error(err, 3, s, i, count);
     }
 }

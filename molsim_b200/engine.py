@@ -200,3 +200,30 @@ class Engine:
 
     def nrebuild(self, isys=0):
         return _lib.lib().msg_nrebuild(self.h, isys)
+
+    def put_state(self, isys, ro, rod=None, rodd=None, keep_list=True):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (ro, rod, rodd)]
+        ptrs = [None if a is None else _p(a, C.c_double) for a in arrs]
+        self._check(_lib.lib().msg_put_state(self.h, isys, *ptrs, 1 if keep_list else 0))
+
+    # --- instrumentation ---------------------------------------------------
+    def stream(self):
+        return _lib.lib().msg_stream(self.h)
+
+    def launch_count(self):
+        return _lib.lib().msg_launch_count(self.h)
+
+    def set_timing(self, on=True):
+        self._check(_lib.lib().msg_set_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        """{timer name: (total device ms, launches)} since the last set_timing."""
+        L = _lib.lib()
+        out = {}
+        for k in range(L.msg_ntimers()):
+            name = C.c_char_p()
+            ms = C.c_double()
+            n = C.c_int64()
+            self._check(L.msg_kernel_time(self.h, k, C.byref(name), C.byref(ms), C.byref(n)))
+            out[name.value.decode()] = (ms.value, n.value)
+        return out

@@ -133,3 +133,44 @@ def test_batch_equals_alone():
         ra, rb = ga.UTotal(), gb.UTotal(k)
         assert Hp.rel_rms(rb["force"], ra["force"]) < 1e-12
         assert Hp.rel(rb["utot"], ra["utot"]) < 1e-12
+
+
+def test_graph_replay_matches_direct_launches(monkeypatch):
+    """The CUDA-graph step (rebuild in a conditional node) equals the directly launched step."""
+    s = dict(Hp.pe_small())
+    s["tstep"] = 0.02
+    s["drnlist"] = 0.6
+    t = Hp.oracle_table(s)
+    ga = Engine(s, t)
+    monkeypatch.setenv("MSG_NO_GRAPHS", "1")
+    gb = Engine(s, t)
+    monkeypatch.delenv("MSG_NO_GRAPHS")
+    for g in (ga, gb):
+        g.UTotal()
+        g.GetLinAcc()
+    ea, eb = ga.VelVer(40), gb.VelVer(40)
+    assert ga.nrebuild() == gb.nrebuild() > 1
+    for x, y in zip(ea, eb):
+        assert Hp.rel(x["utot"], y["utot"]) < 1e-10
+    sa, sb = ga.get_state(), gb.get_state()
+    assert np.abs(sa["ro"] - sb["ro"]).max() < 1e-9
+
+
+def test_rebuild_schedule_matches_oracle():
+    """The skin test (with MOLSIM's running second maximum) triggers the same rebuilds."""
+    s = dict(Hp.pe_small())
+    s["tstep"] = 0.02
+    s["drnlist"] = 0.6
+    t, o, g = _pair(s)
+    g.UTotal()
+    g.GetLinAcc()
+    st = g.get_state()
+    o.set_state(st["ro"], st["rod"], st["rodd"])
+    o.utotal()
+    nb0 = g.nrebuild()
+    for k in range(25):
+        _, rb = o.velver_step()
+        g.VelVer(1, energies=False)
+        nb = g.nrebuild()
+        assert (nb - nb0) == int(rb), k
+        nb0 = nb
