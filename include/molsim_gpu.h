@@ -160,6 +160,27 @@ int     msg_set_timing(msg_handle *h, int32_t on);
 int32_t msg_ntimers(void);
 int     msg_kernel_time(const msg_handle *h, int32_t k, const char **name, double *total_ms, int64_t *launches);
 
+/* UTwoBodyA's pair force, energy and virial on the caller's own MOLSIM arrays,
+ * allocating nothing.  No counterpart in the reference: it serves callers that
+ * cannot call cudaMalloc (a host whose device memory all comes from its own
+ * pool or a framework allocator, or a memory budget that forbids a library to
+ * grow).  All arrays are device-accessible memory the caller owns: ro [np][3],
+ * iptpn [np] (1-based), nneighpn [np] and jpnlist [np][maxnneigh] (MOLSIM's
+ * half list, 1-based partners), ubuf [nbuf]; force [np][3] is overwritten in
+ * kJ/(mol A) (MOLSIM `force` before UTotal's unit scaling), utwob
+ * [natat+1] receives u%twob(0..natat), virial [1] the pair virial.  boxlen,
+ * iubuflow, r2umin and r2atat (may be NULL) are host arrays.  The only scratch
+ * is a fixed static device array (about 88 KiB per GPU, held until exit), so
+ * np <= 262144; larger np returns MSG_ERR_ARG.  The first call on a device
+ * looks up that array's address: make it before any stream capture.  Calls
+ * share the array; calls that overlap on the GPU race.  The call waits for
+ * its work on `stream` (a cudaStream_t, NULL for the default stream). */
+int  msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen[3], double rcut, const double *ro,
+                          const int32_t *iptpn, const int32_t *nneighpn, const int32_t *jpnlist,
+                          int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
+                          const double *r2umin, const double *r2atat, double *force, double *utwob,
+                          double *virial, void *stream);
+
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
                          double boxlenshort, double rcut, int32_t *status);

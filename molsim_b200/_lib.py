@@ -66,6 +66,9 @@ SIGNATURES = {
     "msg_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "msg_ntimers": (C.c_int32, []),
     "msg_kernel_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_char_p), f64p, C.POINTER(C.c_int64)]),
+    "msg_utwobody_noalloc": (C.c_int, [C.c_int32, C.c_int32, f64p, C.c_double, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, i32p, f64p,
+                                       f64p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "msg_rcut_to_alpha": (C.c_double, [C.c_double] * 5 + [i32p]),
     "msg_pot_tab": (C.c_int, [C.POINTER(MsgTabParams), f64p, C.c_int32, i32p, i32p, f64p, i32p]),
 }
