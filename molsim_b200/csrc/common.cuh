@@ -17,7 +17,7 @@
 
 #define MSG_MAX_NATAT 10
 #define MSG_MAX_ORDER 8
-#define MSG_NBUCKET 2048
+#define MSG_NBUCKET 1024
 
 namespace msg {
 
@@ -49,11 +49,17 @@ struct SysDev {
     double dt;
     int bond_off;               // CSR offset of this system's per-particle bond rows
     int tile128_off, ntile128;  // tiles of 128 particles
-    int tile32_off, ntile32;    // tiles of 32 particles
     int chunk_off, nchunk;      // skin chunks of 1024 MOLSIM indices
     int infl_off, ninfl;        // influence work items
     int type_off;               // first entry of this system's per-type arrays
     int ptmap_off;              // first entry of this system's npt*npt type-pair map
+    int tab_k0, tab_nk, tab_b0; // this system's slice of the concatenated table (intervals, buckets)
+    int tab_smem;               // 1: the slice fits the pair kernel's shared-memory table
+    double r2umin_max;          // largest r2umin / r2atat over the type pairs: pairs at or above
+    double r2atat_max;          //   these need no per-pair lower-limit check
+    double fxs[3];              // 2^32 / box: fixed-point coordinate scale of the mixed mirror
+    float fxi[3];               // box / 2^32
+    float pad3;
     uint64_t seed;              // Philox key of this system's Brownian noise
     unsigned long long pad2;
 };
@@ -68,6 +74,41 @@ struct PairTab {
 };
 
 struct Tile { int sys, i0, i1, pad; };
+
+// Mixed-precision position mirror: box coordinates as 32-bit fixed point
+// (2^32 units per box length, wrapping), charge bits in .w.  The difference
+// of two such coordinates is exact and wraps to the minimum image.
+__device__ __forceinline__ int fx_coord(double x, double scale)
+{
+    return (int)(unsigned)(unsigned long long)__double2ll_rn(x * scale);
+}
+__device__ __forceinline__ int4 fx_pos(const double4 &x, const SysDev &S)
+{
+    return make_int4(fx_coord(x.x, S.fxs[0]), fx_coord(x.y, S.fxs[1]), fx_coord(x.z, S.fxs[2]),
+                     __float_as_int((float)x.w));
+}
+
+// Per-system accumulators of one step, 64-bit fixed point (2^-32 units), added
+// with integer atomics: the sums do not depend on the order blocks finish.
+enum {
+    EA_UTWOB = 0,      // 10 slots: u%twob per type pair
+    EA_VIRPAIR = 10,
+    EA_UREC = 11,      // reciprocal-space energy and virial before the self term
+    EA_VIRREC = 12,
+    EA_UBOND = 13,
+    EA_VIRBOND = 14,
+    EA_EKIN = 15,      // sum of m v^2 / 2 in internal units
+    EA_DIP = 16,       // 3 slots: sum of q r for the surface term
+    EA_N = 20
+};
+constexpr double kEFix = 4294967296.0;
+constexpr double kEFixInv = 1.0 / 4294967296.0;
+
+__device__ __forceinline__ void acc_add(long long *a, double v)
+{
+    atomicAdd(reinterpret_cast<unsigned long long *>(a), (unsigned long long)__double2ll_rn(v * kEFix));
+}
+__device__ __forceinline__ double acc_get(const long long *a) { return (double)__ldcg(a) * kEFixInv; }
 
 // Error word: code, system, and two particle indices of the first error seen.
 struct ErrWord { int code, sys, i, j; };
@@ -120,15 +161,12 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 // Cardinal B-spline values and first derivatives (Src/mollib.F90:1629-1683):
-// values[i] = M_P(x+i), derivs[i] = M_{P-1}(x+i) - M_{P-1}(x+i-1), x = pos - floor(pos).
-// Returns kmax = floor(pos).
+// values[i] = M_P(x+i), derivs[i] = M_{P-1}(x+i) - M_{P-1}(x+i-1) for the
+// fractional position x in [0, 1).
 template <int P, typename R>
-__device__ __forceinline__ int bspline(R pos, R *values, R *derivs)
+__device__ __forceinline__ void bspline_frac(R x, R *values, R *derivs)
 {
     R lastv[P];
-    R fl = floor(pos);
-    int v = (int)fl;
-    R x = pos - fl;
 #pragma unroll
     for (int i = 0; i < P; ++i) lastv[i] = R(0);
     values[0] = x;
@@ -150,7 +188,17 @@ __device__ __forceinline__ int bspline(R pos, R *values, R *derivs)
 #pragma unroll
     for (int i = 1; i <= P - 2; ++i) derivs[i] = lastv[i] - lastv[i - 1];
     derivs[P - 1] = -lastv[P - 2];
-    return v;
+}
+
+// Splines at the mesh coordinate u = dkdr * r; returns kmax = floor(u) wrapped
+// into [0, s).  The fraction is formed in FP64 and then rounded to R.
+template <int P, typename R>
+__device__ __forceinline__ int bspline_at(double u, int s, R *values, R *derivs)
+{
+    const double fl = floor(u);
+    bspline_frac<P, R>((R)(u - fl), values, derivs);
+    int k = (int)fl % s;
+    return k < 0 ? k + s : k;
 }
 
 }  // namespace msg

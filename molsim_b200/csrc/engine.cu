@@ -63,9 +63,9 @@ struct HostSys {
     msg_params p;
 };
 
-enum { TM_POS, TM_SKIN, TM_PAIR, TM_SPREAD, TM_FFT, TM_INFL, TM_FINAL, TM_REDUCE, TM_REBUILD, TM_N };
-const char *const kTimerNames[TM_N] = {"position_update", "skin_test", "pair", "spread", "fft",
-                                        "influence", "gather_finalize", "reduce", "rebuild"};
+enum { TM_POS, TM_PAIR, TM_SPREAD, TM_FFT, TM_INFL, TM_FINAL, TM_REBUILD, TM_N };
+const char *const kTimerNames[TM_N] = {"position_update_skin", "pair", "spread", "fft", "influence",
+                                        "gather_finalize", "rebuild"};
 
 struct FftClass {
     int s, count;
@@ -88,7 +88,7 @@ struct msg_handle {
     int *typ[2] = {}, *orig[2] = {};
     int *cellid = nullptr, *inv = nullptr, *sysid = nullptr;
     double4 *fsr = nullptr, *ftot = nullptr;
-    float4 *pos32 = nullptr;
+    int4 *posfx = nullptr;
     // rebuild
     uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *rhist = nullptr;
     int ncell_tot = 0, cell_bits = 1;
@@ -102,20 +102,24 @@ struct msg_handle {
     int *flag = nullptr;
     long long *nrebuild = nullptr;
     // work lists
-    Tile *t128 = nullptr, *t32 = nullptr;
-    int nt128 = 0, nt32 = 0;
+    Tile *t128 = nullptr;
+    PairTask *ptask = nullptr;
+    int nt128 = 0, nptask = 0, max_npt = 1;
     int4 *chunks = nullptr, *infl = nullptr;
     int nchunk = 0, ninfl = 0;
-    double *ppart = nullptr, *fpart = nullptr, *ipart = nullptr, *psurf = nullptr;
+    long long *eacc = nullptr;
+    int pair_grid = 0;
+    size_t pair_smem = 0;
     double *esys = nullptr, *hist = nullptr;
     int hist_cap = 0;
     unsigned long long *stepctr = nullptr, *sstep = nullptr;
-    unsigned *rdone = nullptr;
+    unsigned *rdone = nullptr, *fdone = nullptr;
     ErrWord *errw = nullptr;
     // tables
     PairTab *ptab = nullptr;
     int *ptmap = nullptr;
     double *tz = nullptr, *tc = nullptr;
+    float *tz32 = nullptr, *tc32 = nullptr;
     unsigned short *bst = nullptr;
     double *massip = nullptr, *massp = nullptr, *fac1 = nullptr, *fac2 = nullptr;
     int has_bd = 0;
@@ -126,6 +130,9 @@ struct msg_handle {
     int any_ewald = 0;
     double *rgrid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
     double2 *cgrid = nullptr;
+    float *rgrid32 = nullptr;
+    float2 *cgrid32 = nullptr;
+    unsigned long long *igrid = nullptr;
     long long grid_tot = 0, cgrid_tot = 0;
     std::vector<FftClass> fft;
     // staging
@@ -193,8 +200,7 @@ struct msg_handle {
     }
     void build(const msg_params *p, int n, int prec);
     void enqueue_rebuild();
-    void enqueue_forces(int mode);
-    void enqueue_reduce(bool record);
+    void enqueue_forces(int mode, bool record);
     void enqueue_md_step(bool record);
     void enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record);
     // CUDA graph of one step; the rebuild sits in an IF node opened by k_skin
@@ -225,12 +231,12 @@ static void free_all(msg_handle *h)
 {
     void *ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->acc[0], h->acc[1], h->dsum[0], h->dsum[1],
                     h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
-                    h->sysid, h->fsr, h->ftot, h->pos32, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
+                    h->sysid, h->fsr, h->ftot, h->posfx, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
                     h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
-                    h->t128, h->t32, h->chunks, h->infl, h->ppart, h->fpart, h->ipart, h->psurf, h->esys,
-                    h->hist, h->stepctr, h->sstep, h->rdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
-                    h->bst, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
-                    h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->stage, h->xin, h->dsys};
+                    h->t128, h->ptask, h->chunks, h->infl, h->eacc, h->esys,
+                    h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
+                    h->bst, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
+                    h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (auto &f : h->fft) {
@@ -274,7 +280,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     order = P[0].order;
     std::vector<HostSys> H(n);
     ntot = 0;
-    int type_tot = 0, pt_tot = 0, ptmap_tot = 0, cell_tot = 0, t128 = 0, t32 = 0, nch = 0;
+    int type_tot = 0, pt_tot = 0, ptmap_tot = 0, cell_tot = 0, t128 = 0, nch = 0;
     long long nbl_acc = 0;
     size_t nbond_tot = 0;
     for (int s = 0; s < n; ++s) {
@@ -300,6 +306,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             S.boxi[d] = 1.0 / p.boxlen[d];
         }
         S.vol = p.boxlen[0] * p.boxlen[1] * p.boxlen[2];
+        for (int d = 0; d < 3; ++d) {
+            S.fxs[d] = 4294967296.0 / p.boxlen[d];
+            S.fxi[d] = (float)(p.boxlen[d] / 4294967296.0);
+        }
         S.rcut2 = p.rcut * p.rcut;
         const double rl = p.rcut + p.drnlist;
         S.rs2cut = rl * rl;
@@ -316,6 +326,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         if (p.maxnneigh > 0) cap = std::max(cap, (int)p.maxnneigh);
         cap = std::min(cap, ((p.np + 7) / 8) * 8);
         cap = std::max(cap, 8);
+        // rows start on 32-byte boundaries: the pair kernel reads them 16 bytes at a time
+        cap = ((cap + 7) / 8) * 8;
         S.cap = cap;
         S.nbl_off = nbl_acc;
         nbl_acc += (long long)cap * p.np;
@@ -332,13 +344,11 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         S.ptmap_off = ptmap_tot;
         S.tile128_off = t128;
         S.ntile128 = (p.np + 127) / 128;
-        S.tile32_off = t32;
-        S.ntile32 = (p.np + 31) / 32;
         S.chunk_off = nch;
         S.nchunk = (p.np + SK_CHUNK - 1) / SK_CHUNK;
         S.seed = (uint64_t)s * 0x9E3779B97F4A7C15ull;
         t128 += S.ntile128;
-        t32 += S.ntile32;
+        max_npt = std::max(max_npt, (int)p.npt);
         nch += S.nchunk;
         type_tot += p.npt;
         pt_tot += S.natat;
@@ -355,7 +365,6 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     while ((1u << cell_bits) <= (unsigned)cell_tot) ++cell_bits;
     nbl_tot = nbl_acc;
     nt128 = t128;
-    nt32 = t32;
     nchunk = nch;
 
     // --- SPME grids grouped by edge, one batched cuFFT plan pair per edge ---
@@ -387,8 +396,14 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             }
         grid_tot = go;
         cgrid_tot = co;
-        rgrid = dalloc<double>(grid_tot);
-        cgrid = dalloc<double2>(cgrid_tot);
+        if (prec == MSG_PREC_MIXED) {
+            igrid = dalloc<unsigned long long>(grid_tot);
+            rgrid32 = dalloc<float>(grid_tot);
+            cgrid32 = dalloc<float2>(cgrid_tot);
+        } else {
+            rgrid = dalloc<double>(grid_tot);
+            cgrid = dalloc<double2>(cgrid_tot);
+        }
         std::vector<double> hm(fo_acc), he(fo_acc), hv(fo_acc);
         for (int s = 0; s < n; ++s)
             if (hs[s].lewald)
@@ -403,8 +418,11 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         for (auto &fc : fft) {
             int dims[3] = {fc.s, fc.s, fc.s};
             const int rdist = fc.s * fc.s * fc.s, cdist = fc.s * fc.s * (fc.s / 2 + 1);
-            CKF(cufftPlanMany(&fc.fwd, 3, dims, nullptr, 1, rdist, nullptr, 1, cdist, CUFFT_D2Z, fc.count));
-            CKF(cufftPlanMany(&fc.bwd, 3, dims, nullptr, 1, cdist, nullptr, 1, rdist, CUFFT_Z2D, fc.count));
+            const bool f32 = prec == MSG_PREC_MIXED;
+            CKF(cufftPlanMany(&fc.fwd, 3, dims, nullptr, 1, rdist, nullptr, 1, cdist, f32 ? CUFFT_R2C : CUFFT_D2Z,
+                              fc.count));
+            CKF(cufftPlanMany(&fc.bwd, 3, dims, nullptr, 1, cdist, nullptr, 1, rdist, f32 ? CUFFT_C2R : CUFFT_Z2D,
+                              fc.count));
             CKF(cufftSetStream(fc.fwd, st));
             CKF(cufftSetStream(fc.bwd, st));
         }
@@ -421,7 +439,6 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         ninfl = (int)it.size();
         infl = dalloc<int4>(ninfl);
         CK(cudaMemcpy(infl, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice));
-        ipart = dalloc<double>(2 * (size_t)ninfl);
     }
 
     // --- pair tables: per type pair, intervals from MOLSIM's ubuf ---
@@ -468,6 +485,21 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                     vb.push_back((unsigned short)kk);
                 }
             }
+        S.tab_k0 = pt[S.pt_off].k0;
+        S.tab_b0 = pt[S.pt_off].b0;
+        S.tab_nk = (int)vz.size() - S.tab_k0;
+        {
+            const size_t bytes = (prec == MSG_PREC_MIXED) ? pair_smem_bytes<float>(S.tab_nk, S.natat * MSG_NBUCKET)
+                                                          : pair_smem_bytes<double>(S.tab_nk, S.natat * MSG_NBUCKET);
+            S.tab_smem = bytes <= 96 * 1024 ? 1 : 0;
+            if (S.tab_smem) pair_smem = std::max(pair_smem, bytes);
+        }
+        S.r2umin_max = 0.0;
+        S.r2atat_max = 0.0;
+        for (int q = 0; q < S.natat; ++q) {
+            S.r2umin_max = std::max(S.r2umin_max, pt[S.pt_off + q].r2umin);
+            S.r2atat_max = std::max(S.r2atat_max, pt[S.pt_off + q].r2atat);
+        }
         for (int t = 0; t < p.npt; ++t) {
             vmassp[S.type_off + t] = p.masspt[t];
             vmassip[S.type_off + t] = p.masspt[t] > 0.0 ? 1.0 / p.masspt[t] : 0.0;
@@ -489,6 +521,13 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     CK(cudaMemcpy(tz, vz.data(), vz.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(tc, vc.data(), vc.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(bst, vb.data(), vb.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    {
+        std::vector<float> fz(vz.begin(), vz.end()), fc(vc.begin(), vc.end());
+        tz32 = dalloc<float>(fz.size());
+        tc32 = dalloc<float>(fc.size());
+        CK(cudaMemcpy(tz32, fz.data(), fz.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(tc32, fc.data(), fc.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     CK(cudaMemcpy(massip, vmassip.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(massp, vmassp.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(fac1, vf1.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
@@ -538,20 +577,31 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 
     // --- work lists ---
     {
-        std::vector<Tile> a128, a32;
+        std::vector<Tile> a128;
+        std::vector<PairTask> pt16;
         std::vector<int4> ch;
         for (int s = 0; s < n; ++s) {
             const SysDev &S = hs[s];
             for (int i = 0; i < S.n; i += 128) a128.push_back(Tile{s, S.off + i, S.off + std::min(S.n, i + 128), 0});
-            for (int i = 0; i < S.n; i += 32) a32.push_back(Tile{s, S.off + i, S.off + std::min(S.n, i + 32), 0});
+            // lanes per particle: about four row entries per lane (expected full-list row)
+            const double rl = std::sqrt(S.rs2cut);
+            const double nrow = S.n / S.vol * 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl;
+            int G = 4;
+            while (G < 32 && 2 * G <= nrow / 4.0) G *= 2;
+            const int per = 32 / G;
+            const size_t first = pt16.size();
+            for (int i = 0; i < S.n; i += per)
+                pt16.push_back(PairTask{s, S.off + i, S.off + std::min(S.n, i + per), G, 0, 0, 0, 0});
+            for (size_t q = first; q < pt16.size(); ++q) pt16[q].send = (int)pt16.size();
             for (int i = 0; i < S.n; i += SK_CHUNK)
                 ch.push_back(make_int4(s, S.off + i, S.off + std::min(S.n, i + SK_CHUNK), 0));
         }
+        nptask = (int)pt16.size();
         this->t128 = dalloc<Tile>(a128.size());
-        this->t32 = dalloc<Tile>(a32.size());
+        ptask = dalloc<PairTask>(pt16.size());
         chunks = dalloc<int4>(ch.size());
         CK(cudaMemcpy(this->t128, a128.data(), a128.size() * sizeof(Tile), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(this->t32, a32.data(), a32.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ptask, pt16.data(), pt16.size() * sizeof(PairTask), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
     }
 
@@ -570,7 +620,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     sysid = dalloc<int>(ntot);
     fsr = dalloc<double4>(ntot);
     ftot = dalloc<double4>(ntot);
-    if (prec == MSG_PREC_MIXED) pos32 = dalloc<float4>(ntot);
+    posfx = dalloc<int4>(ntot);
     {
         std::vector<double4> hp(ntot);
         std::vector<int> ht(ntot), ho(ntot), hsid(ntot);
@@ -613,17 +663,32 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     sysdone = dalloc<unsigned>(n);
     flag = dalloc<int>(n);
     nrebuild = dalloc<long long>(n);
-    ppart = dalloc<double>((size_t)nt32 * NPART_PAIR);
-    fpart = dalloc<double>((size_t)nt128 * NPART_FIN);
-    psurf = dalloc<double>((size_t)nt128 * 4);
+    eacc = dalloc<long long>((size_t)n * EA_N);
     esys = dalloc<double>((size_t)n * ESZ);
     stepctr = dalloc<unsigned long long>(1);
     sstep = dalloc<unsigned long long>(n);
     rdone = dalloc<unsigned>(1);
+    fdone = dalloc<unsigned>(n);
     errw = dalloc<ErrWord>(1);
-    if (!ipart) ipart = dalloc<double>(2);
     dsys = dalloc<SysDev>(n);
     CK(cudaMemcpy(dsys, hs.data(), n * sizeof(SysDev), cudaMemcpyHostToDevice));
+    {
+        // persistent pair grid: as many blocks as fit the SMs at once
+        int nsm = 0, per = 0;
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+#define MSG_PAIR_CFG(PRC, NTV)                                                                           \
+    do {                                                                                                \
+        CK(cudaFuncSetAttribute(k_pair<PRC, NTV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));      \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pair<PRC, NTV>, PAIR_BLOCK, pair_smem)); \
+    } while (0)
+        if (prec == MSG_PREC_MIXED) {
+            if (max_npt <= 2) MSG_PAIR_CFG(PrecM, 2); else MSG_PAIR_CFG(PrecM, 4);
+        } else {
+            if (max_npt <= 2) MSG_PAIR_CFG(PrecD, 2); else MSG_PAIR_CFG(PrecD, 4);
+        }
+#undef MSG_PAIR_CFG
+        pair_grid = std::max(1, std::min(nptask, nsm * std::max(1, per)));
+    }
     CK(cudaDeviceSynchronize());
 }
 
@@ -643,107 +708,133 @@ void msg_handle::enqueue_rebuild()
                                        typ[0], typ[1], orig[0], orig[1], dsum[0]);
     k_clear_cells<<<(ncell_tot + 255) / 256, 256, 0, st>>>(cstart, cend, ncell_tot);
     k_cellrange<<<(ntot + 255) / 256, 256, 0, st>>>(cellid, sysid, flag, ntot, cstart, cend);
-    k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[0], cellid, cstart, cend, nbl, nnb,
-                                                     ntot, nmaxrow, errw);
+    k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[0], typ[0], cellid, cstart, cend, nbl,
+                                                     nnb, ntot, nmaxrow, errw);
+    // positions were permuted: refresh the FP32 mirror of rebuilt systems
+    k_mirror<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], posfx);
     tend(TM_REBUILD);
-    launches += 6 + 3 * ((cell_bits + 7) / 8);
+    launches += 7 + 3 * ((cell_bits + 7) / 8);
 }
 
-template <int P>
+template <int P, class PR>
 static void launch_spme(msg_handle *h)
 {
-    const int c = h->cur;
     h->tbeg(TM_SPREAD);
-    CK(cudaMemsetAsync(h->rgrid, 0, sizeof(double) * h->grid_tot, h->st));
-    k_spread_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->rgrid, h->psurf);
+    if (!PR::mixed) CK(cudaMemsetAsync(h->rgrid, 0, sizeof(double) * h->grid_tot, h->st));
+    k_spread<P, PR><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->rgrid, h->igrid,
+                                                  h->eacc);
+    h->launches += 1;
+    if (PR::mixed) {
+        k_grid_to_f32<<<(unsigned)((h->grid_tot + 255) / 256), 256, 0, h->st>>>(h->igrid, h->rgrid32, h->grid_tot);
+        h->launches += 1;
+    }
     h->tend(TM_SPREAD);
     h->tbeg(TM_FFT);
-    for (auto &f : h->fft)
-        CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
+    for (auto &f : h->fft) {
+        if (PR::mixed)
+            CKF(cufftExecR2C(f.fwd, h->rgrid32 + f.grid_off, reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off)));
+        else
+            CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off,
+                             reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
+    }
     h->tend(TM_FFT);
     h->tbeg(TM_INFL);
-    k_influence_fp64<<<h->ninfl, INFL_THREADS, 0, h->st>>>(h->dsys, h->infl, h->cgrid, h->mfac, h->emf, h->vmf,
-                                                          h->ipart);
+    k_influence<PR><<<h->ninfl, INFL_THREADS, 0, h->st>>>(h->dsys, h->infl, h->cgrid, h->cgrid32, h->mfac, h->emf,
+                                                          h->vmf, h->eacc);
+    h->launches += 1;
     h->tend(TM_INFL);
     h->tbeg(TM_FFT);
-    for (auto &f : h->fft)
-        CKF(cufftExecZ2D(f.bwd, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off), h->rgrid + f.grid_off));
+    for (auto &f : h->fft) {
+        if (PR::mixed)
+            CKF(cufftExecC2R(f.bwd, reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off), h->rgrid32 + f.grid_off));
+        else
+            CKF(cufftExecZ2D(f.bwd, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off),
+                             h->rgrid + f.grid_off));
+    }
     h->tend(TM_FFT);
-    h->launches += 2;
 }
 
-template <int P>
-static void launch_finalize(msg_handle *h, int mode)
+template <int P, class PR>
+static void launch_finalize(msg_handle *h, int mode, bool record)
 {
-    const int c = h->cur;
+    FinOut fo;
+    fo.esys = h->esys;
+    fo.hist = record ? h->hist : nullptr;
+    fo.hist_cap = h->hist_cap;
+    fo.nsys = h->nsys;
+    fo.stepctr = h->stepctr;
+    fo.sstep = h->sstep;
+    fo.fdone = h->fdone;
+    fo.alldone = h->rdone;
     h->tbeg(TM_FINAL);
     h->launches += 1;
-    k_finalize_fp64<P><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[c], h->typ[c], h->orig[c], h->inv,
-                                                    h->rgrid, h->fsr, h->psurf, h->bptr, h->bpart, h->bk, h->beq,
-                                                    h->bpw, h->massip, h->massp, h->ftot, h->fo[c], h->vel[c],
-                                                    h->acc[c], h->fpart, mode, h->errw);
+    k_finalize<P, PR><<<h->nt128, FIN_THREADS, 0, h->st>>>(
+        h->dsys, h->t128, h->pos[0], h->typ[0], h->orig[0], h->inv, h->rgrid, h->rgrid32, h->fsr,
+        h->eacc, h->bptr, h->bpart, h->bk, h->beq, h->bpw, h->massip, h->massp, h->ftot, h->fo[0], h->vel[0],
+        h->acc[0], mode, fo, h->errw);
     h->tend(TM_FINAL);
 }
 
-void msg_handle::enqueue_forces(int mode)
+template <class PR>
+static void launch_forces(msg_handle *h, int mode, bool record)
 {
-    const int c = cur;
-    tbeg(TM_PAIR);
-    k_pair_fp64<<<nt32, PAIR_THREADS, 0, st>>>(dsys, t32, pos[c], typ[c], nbl, nnb, ptmap, ptab, tz, tc, bst, fsr,
-                                               ppart, errw);
-    tend(TM_PAIR);
-    launches += 1;
-    if (any_ewald) {
-        switch (order) {
-        case 4: launch_spme<4>(this); break;
-        case 5: launch_spme<5>(this); break;
-        default: launch_spme<6>(this); break;
+    h->tbeg(TM_PAIR);
+    const typename PR::V4 *pp =
+        reinterpret_cast<const typename PR::V4 *>(PR::mixed ? (const void *)h->posfx : (const void *)h->pos[0]);
+    const typename PR::R *tzp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tz32 : (const void *)h->tz);
+    const typename PR::R *tcp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tc32 : (const void *)h->tc);
+    if (h->max_npt <= 2)
+        k_pair<PR, 2><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
+                                                              h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
+                                                              h->eacc, h->errw);
+    else
+        k_pair<PR, 4><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
+                                                              h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
+                                                              h->eacc, h->errw);
+    h->tend(TM_PAIR);
+    h->launches += 1;
+    if (h->any_ewald) {
+        switch (h->order) {
+        case 4: launch_spme<4, PR>(h); break;
+        case 5: launch_spme<5, PR>(h); break;
+        default: launch_spme<6, PR>(h); break;
         }
     }
-    switch (order) {
-    case 4: launch_finalize<4>(this, mode); break;
-    case 5: launch_finalize<5>(this, mode); break;
-    default: launch_finalize<6>(this, mode); break;
+    switch (h->order) {
+    case 4: launch_finalize<4, PR>(h, mode, record); break;
+    case 5: launch_finalize<5, PR>(h, mode, record); break;
+    default: launch_finalize<6, PR>(h, mode, record); break;
     }
 }
 
-void msg_handle::enqueue_reduce(bool record)
+void msg_handle::enqueue_forces(int mode, bool record)
 {
-    tbeg(TM_REDUCE);
-    k_reduce<<<nsys, 256, 0, st>>>(dsys, ppart, ipart, fpart, psurf, esys, record ? hist : nullptr, hist_cap,
-                                   stepctr, sstep, rdone, nsys);
-    tend(TM_REDUCE);
-    launches += 1;
+    if (prec == MSG_PREC_MIXED)
+        launch_forces<PrecM>(this, mode, record);
+    else
+        launch_forces<PrecD>(this, mode, record);
 }
 
 void msg_handle::enqueue_md_step(bool record)
 {
-    const int c = cur;
     tbeg(TM_POS);
-    k_vv_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], vel[c], acc[c], dsum[c], orig[c], r2o, nullptr, pos32);
+    k_vv_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, inv, pos[0], vel[0], acc[0], dsum[0], posfx, r2o, sc,
+                                             sysdone, flag, nrebuild, skinout, cond, use_cond);
     tend(TM_POS);
-    tbeg(TM_SKIN);
-    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
-    tend(TM_SKIN);
-    launches += 2;
-    enqueue_forces(1);
-    enqueue_reduce(record);
+    launches += 1;
+    enqueue_forces(1, record);
     if (!use_cond) enqueue_rebuild();
 }
 
 void msg_handle::enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record)
 {
-    const int c = cur;
     tbeg(TM_POS);
-    k_bd_pos<<<nt128, 128, 0, st>>>(dsys, t128, pos[c], fo[c], dsum[c], orig[c], typ[c], fac1, fac2, xin_step,
-                                    xout_step, seed, sstep, r2o, nullptr, pos32);
+    k_bd_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, inv, pos[0], fo[0], dsum[0], typ[0], fac1, fac2, xin_step,
+                                             xout_step, seed, sstep, posfx, r2o, sc, sysdone, flag, nrebuild, skinout,
+                                             cond, use_cond);
     tend(TM_POS);
-    tbeg(TM_SKIN);
-    k_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
-    tend(TM_SKIN);
-    launches += 2;
-    enqueue_forces(0);
-    enqueue_reduce(record);
+    launches += 1;
+    enqueue_forces(0, record);
     if (!use_cond) enqueue_rebuild();
 }
 
@@ -915,6 +1006,11 @@ int msg_handle::check()
         err = buf;
         const int code = e.code;
         CK(cudaMemset(errw, 0, sizeof(ErrWord)));
+        // an aborted step may leave partial sums and counters behind
+        CK(cudaMemset(eacc, 0, sizeof(long long) * nsys * EA_N));
+        CK(cudaMemset(fdone, 0, sizeof(unsigned) * nsys));
+        CK(cudaMemset(sysdone, 0, sizeof(unsigned) * nsys));
+        CK(cudaMemset(rdone, 0, sizeof(unsigned)));
         return code;
     }
     return MSG_OK;
@@ -980,6 +1076,10 @@ static int put_state(msg_handle *h, int32_t isys, const double *ro, const double
         if (!src[k]) continue;
         h2d(h->stage, src[k], 3 * (size_t)S.n, h->st);
         k_to_internal<<<nb, 256, 0, h->st>>>(h->stage, dst[k], h->inv, S.off, S.n, k == 0 ? 1 : 0);
+        h->launches += 1;
+    }
+    if (ro) {
+        k_mirror_range<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->posfx);
         h->launches += 1;
     }
     if (ro && !keep_list) {
@@ -1080,8 +1180,7 @@ extern "C" int msg_utotal(msg_handle *h, int32_t isys, double *force, double *fo
 {
     if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
     API_BEGIN
-    h->enqueue_forces(0);
-    h->enqueue_reduce(false);
+    h->enqueue_forces(0, false);
     int rc = h->check();
     if (rc) return rc;
     const SysDev &S = h->hs[isys];

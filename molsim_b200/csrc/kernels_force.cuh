@@ -1,130 +1,18 @@
-// kernels_force.cuh -- pair table force, SPME and per-step reductions.
+// kernels_force.cuh -- SPME (spread, influence, gather) and the per-step finalize.
 #pragma once
 
 #include "common.cuh"
+#include "kernels_pair.cuh"
 
 namespace msg {
 
-constexpr int PAIR_G = 8;                 // lanes per particle in the pair kernel
-constexpr int PAIR_THREADS = 256;         // 32 particles per block (tile of 32)
-constexpr int NPART_PAIR = MSG_MAX_NATAT + 1;
-constexpr int MAXT = 4;                   // particle types per system (natat <= 10)
+constexpr double kGridFix = 1099511627776.0;       // 2^40: fixed-point scale of the mixed charge grid
+constexpr double kGridFixInv = 1.0 / 1099511627776.0;
 
-// Interval of MOLSIM's table (Src/energy.F90:481-486).  The reference walks
-// ibuf upwards from iubuflow while r2 < zlow; the walk here starts at a bucket
-// entry bstart[b] chosen on the host to lie at or before the interval the full
-// walk would find, and then performs the same comparisons, so it ends on the
-// same interval.
-template <typename Z>
-__device__ __forceinline__ int table_interval(const PairTab &P, const Z *__restrict__ tz,
-                                              const unsigned short *__restrict__ bst, Z r2, bool &bad)
-{
-    int k = 0;
-    if (r2 < (Z)P.z_hi) {
-        int b = (int)((r2 - (Z)P.z_lo) * (Z)P.inv_h);
-        b = b < 0 ? 0 : (b >= MSG_NBUCKET ? MSG_NBUCKET - 1 : b);
-        k = bst[P.b0 + b];
-    }
-    const Z *z = tz + P.k0;
-    while (r2 < __ldg(z + k)) {
-        if (++k >= P.nk) { bad = true; k = P.nk - 1; break; }
-    }
-    return k;
-}
-
-// ---------------------------------------------------------------------------
-// UTwoBodyA (Src/energy.F90:445-544) over a full Verlet list, FP64.
-// PAIR_G lanes per particle; forces of particle i are summed in registers in
-// a fixed order (no atomics).  Each pair's energy and virial are counted once
-// (i < j); per-tile partial sums go to ppart[tile][type pair | virial].
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(PAIR_THREADS) k_pair_fp64(
-    const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
-    const int *__restrict__ typ, const int *__restrict__ nbl, const int *__restrict__ nnb,
-    const int *__restrict__ ptmap, const PairTab *__restrict__ ptab, const double *__restrict__ tz,
-    const double *__restrict__ tc, const unsigned short *__restrict__ bst, double4 *__restrict__ fsr,
-    double *__restrict__ ppart, ErrWord *err)
-{
-    __shared__ double red[PAIR_THREADS / PAIR_G][NPART_PAIR];
-    const Tile T = tiles[blockIdx.x];
-    const SysDev &S = sysv[T.sys];
-    const int li = threadIdx.x / PAIR_G, g = threadIdx.x % PAIR_G;
-    const int i = T.i0 + li;
-    double fx = 0.0, fy = 0.0, fz = 0.0, vir = 0.0;
-    double ut[MAXT] = {0.0, 0.0, 0.0, 0.0};
-    int ti = 0;
-    if (i < T.i1) {
-        const double4 xi = pos[i];
-        ti = typ[i];
-        const int n = nnb[i];
-        const int *row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
-        for (int k = g; k < n; k += PAIR_G) {
-            const int j = __ldg(row + k);
-            const double4 xj = pos[j];
-            double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const double r2 = pbcr2_exact(dx, dy, dz, S);
-            if (r2 > S.rcut2) continue;
-            const int tj = typ[j];
-            const PairTab &P = ptab[pair_of(ptmap, S, ti, tj)];
-            double usum, fsum;
-            if (r2 < P.r2atat) {
-                usum = 1e10;   // hard-core overlap (the reference leaves fsum stale here)
-                fsum = 0.0;
-            } else if (r2 < P.r2umin) {
-                raise_error(err, 1, T.sys, i, j);
-                continue;
-            } else {
-                bool bad = false;
-                const int kk = table_interval(P, tz, bst, r2, bad);
-                if (bad) raise_error(err, 2, T.sys, i, j);
-                const double *c = tc + (size_t)(P.k0 + kk) * 12;
-                const double d = r2 - c[0];
-                usum = c[1] + d * (c[2] + d * (c[3] + d * (c[4] + d * (c[5] + d * c[6]))));
-                fsum = c[7] + d * (c[8] + d * (c[9] + d * (c[10] + d * c[11])));
-            }
-            fx += fsum * dx;
-            fy += fsum * dy;
-            fz += fsum * dz;
-            if (i < j) {
-#pragma unroll
-                for (int t = 0; t < MAXT; ++t) ut[t] += (tj == t) ? usum : 0.0;
-                vir -= fsum * r2;
-            }
-        }
-    }
-#pragma unroll
-    for (int o = PAIR_G / 2; o > 0; o >>= 1) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, o);
-        fy += __shfl_xor_sync(0xffffffffu, fy, o);
-        fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        vir += __shfl_xor_sync(0xffffffffu, vir, o);
-#pragma unroll
-        for (int t = 0; t < MAXT; ++t) ut[t] += __shfl_xor_sync(0xffffffffu, ut[t], o);
-    }
-    if (g == 0) {
-        if (i < T.i1) fsr[i] = make_double4(fx, fy, fz, 0.0);
-#pragma unroll
-        for (int p = 0; p < NPART_PAIR; ++p) red[li][p] = 0.0;
-        if (i < T.i1) {
-            for (int t = 0; t < S.npt; ++t) red[li][pair_of(ptmap, S, ti, t) - S.pt_off] += ut[t];
-            red[li][MSG_MAX_NATAT] = vir;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < NPART_PAIR) {
-        double s = 0.0;
-        for (int l = 0; l < PAIR_THREADS / PAIR_G; ++l) s += red[l][threadIdx.x];
-        ppart[(size_t)blockIdx.x * NPART_PAIR + threadIdx.x] = s;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// SPME charge spreading (Src/energy.F90:1226-1245): Q(k - i) += q*Mx*My*Mz.
-// ---------------------------------------------------------------------------
-// Also writes the per-tile dipole sums sum(q r) of the surface term
-// (UEwaldSurf, Src/energy.F90:1354-1357) from the same final positions.
-__device__ __forceinline__ void tile_dipole(const SysDev &S, double qx, double qy, double qz,
-                                            double *__restrict__ psurf)
+// Block dipole sums sum(q r) of the surface term (UEwaldSurf,
+// Src/energy.F90:1354-1357) from the final positions of the step, added to the
+// system's fixed-point accumulators.
+__device__ __forceinline__ void block_dipole(double qx, double qy, double qz, long long *__restrict__ ea)
 {
     __shared__ double red[3][4];
     qx = warp_sum(qx);
@@ -136,15 +24,22 @@ __device__ __forceinline__ void tile_dipole(const SysDev &S, double qx, double q
     if (threadIdx.x < 3) {
         double s = 0.0;
         for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
-        psurf[blockIdx.x * 4 + threadIdx.x] = s;
+        acc_add(ea + EA_DIP + threadIdx.x, s);
     }
 }
 
-template <int P>
-__global__ void __launch_bounds__(128) k_spread_fp64(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                                    const double4 *__restrict__ pos, double *__restrict__ grid,
-                                                    double *__restrict__ psurf)
+// ---------------------------------------------------------------------------
+// SPME charge spreading (Src/energy.F90:1226-1245): Q(k - i) += q*Mx*My*Mz.
+// PrecD: FP64 atomics into the FP64 grid.  PrecM: FP32 splines, each
+// contribution rounded to 2^-40 and added as a 64-bit integer, so the grid is
+// the same whatever order the atomics land in.
+// ---------------------------------------------------------------------------
+template <int P, class PR>
+__global__ void __launch_bounds__(128) k_spread(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                               const double4 *__restrict__ pos, double *__restrict__ grid, unsigned long long *__restrict__ igrid,
+                                               long long *__restrict__ eacc)
 {
+    using R = typename PR::R;
     const Tile T = tiles[blockIdx.x];
     const SysDev &S = sysv[T.sys];
     if (!S.lewald) return;
@@ -152,38 +47,49 @@ __global__ void __launch_bounds__(128) k_spread_fp64(const SysDev *__restrict__ 
     double4 x = make_double4(0.0, 0.0, 0.0, 0.0);
     if (i < T.i1) {
         x = pos[i];
-        const int s = S.s;
-        double th[3][P], dth[3][P];
-        int km[3];
         const double xc[3] = {x.x, x.y, x.z};
+        const int s = S.s;
+        R th[3][P], dth[3][P];
+        int km[3];
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-            int k = bspline<P>(S.dkdr[m] * xc[m], th[m], dth[m]);
-            k %= s;
-            km[m] = k < 0 ? k + s : k;
-        }
-        double *G = grid + S.grid_off;
+        for (int m = 0; m < 3; ++m) km[m] = bspline_at<P, R>(S.dkdr[m] * xc[m], s, th[m], dth[m]);
+        const R q = (R)x.w;
 #pragma unroll
         for (int iz = 0; iz < P; ++iz) {
             int nz = km[2] - iz;
             nz += (nz < 0) ? s : 0;
-            const double qz = x.w * th[2][iz];
+            const R qz = q * th[2][iz];
 #pragma unroll
             for (int iy = 0; iy < P; ++iy) {
                 int ny = km[1] - iy;
                 ny += (ny < 0) ? s : 0;
-                const double qyz = qz * th[1][iy];
-                double *rowp = G + ((size_t)nz * s + ny) * s;
+                const R qyz = qz * th[1][iy];
+                const size_t rowo = S.grid_off + ((size_t)nz * s + ny) * s;
 #pragma unroll
                 for (int ix = 0; ix < P; ++ix) {
                     int nx = km[0] - ix;
                     nx += (nx < 0) ? s : 0;
-                    atomicAdd(rowp + nx, qyz * th[0][ix]);
+                    if (PR::mixed)
+                        atomicAdd(igrid + rowo + nx,
+                                  (unsigned long long)__double2ll_rn((double)(qyz * th[0][ix]) * kGridFix));
+                    else
+                        atomicAdd(grid + rowo + nx, (double)(qyz * th[0][ix]));
                 }
             }
         }
     }
-    if (S.lsurf) tile_dipole(S, x.w * x.x, x.w * x.y, x.w * x.z, psurf);
+    if (S.lsurf) block_dipole(x.w * x.x, x.w * x.y, x.w * x.z, eacc + (size_t)T.sys * EA_N);
+}
+
+// Mixed path: fixed-point grid -> FP32 grid for the FP32 FFT, clearing the
+// fixed-point grid for the next step.
+__global__ void k_grid_to_f32(unsigned long long *__restrict__ igrid, float *__restrict__ g, long long n)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        g[k] = (float)((double)(long long)igrid[k] * kGridFixInv);
+        igrid[k] = 0ull;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -192,32 +98,41 @@ __global__ void __launch_bounds__(128) k_spread_fp64(const SysDev *__restrict__ 
 // W -= |F|^2 * vmf, where emf/vmf carry the reference's halving at kx=0, s/2
 // and the mirror double counts in y and z are already resolved.
 // ---------------------------------------------------------------------------
-constexpr int INFL_THREADS = 256, INFL_ITEMS = 4;
-constexpr int INFL_TILE = INFL_THREADS * INFL_ITEMS;
+constexpr int INFL_THREADS = 256;
+constexpr int INFL_TILE = 512;
 
-__global__ void __launch_bounds__(INFL_THREADS) k_influence_fp64(
-    const SysDev *__restrict__ sysv, const int4 *__restrict__ items, double2 *__restrict__ cg,
-    const double *__restrict__ mfac, const double *__restrict__ emf, const double *__restrict__ vmf,
-    double *__restrict__ ipart)
+template <class PR>
+__global__ void __launch_bounds__(INFL_THREADS) k_influence(const SysDev *__restrict__ sysv, const int4 *__restrict__ items,
+                                                           double2 *__restrict__ cg, float2 *__restrict__ cg32,
+                                                           const double *__restrict__ mfac, const double *__restrict__ emf,
+                                                           const double *__restrict__ vmf, long long *__restrict__ eacc)
 {
     __shared__ double red[2][INFL_THREADS / 32];
     const int4 W = items[blockIdx.x];   // sys, first complex index, end
     const SysDev &S = sysv[W.x];
     const int s = S.s, h = s / 2 + 1;
     double e = 0.0, v = 0.0;
-    double2 *F = cg + S.cgrid_off;
     for (int c = W.y + threadIdx.x; c < W.z; c += INFL_THREADS) {
         const int kx = c % h, r = c / h, ky = r % s, kz = r / s;
         const int fy = ky <= s / 2 ? ky : s - ky, fz = kz <= s / 2 ? kz : s - kz;
         const size_t f = S.fac_off + kx + (size_t)h * (fy + (size_t)h * fz);
-        double2 q = F[c];
-        const double q2 = q.x * q.x + q.y * q.y;
+        const double m = mfac[f];
+        double q2;
+        if (PR::mixed) {
+            float2 q = cg32[S.cgrid_off + c];
+            q2 = (double)(q.x * q.x + q.y * q.y);
+            q.x *= (float)m;
+            q.y *= (float)m;
+            cg32[S.cgrid_off + c] = q;
+        } else {
+            double2 q = cg[S.cgrid_off + c];
+            q2 = q.x * q.x + q.y * q.y;
+            q.x *= m;
+            q.y *= m;
+            cg[S.cgrid_off + c] = q;
+        }
         e += q2 * emf[f];
         v -= q2 * vmf[f];
-        const double m = mfac[f];
-        q.x *= m;
-        q.y *= m;
-        F[c] = q;
     }
     e = warp_sum(e);
     v = warp_sum(v);
@@ -227,7 +142,7 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence_fp64(
     if (threadIdx.x < 2) {
         double sacc = 0.0;
         for (int k = 0; k < INFL_THREADS / 32; ++k) sacc += red[threadIdx.x][k];
-        ipart[(size_t)blockIdx.x * 2 + threadIdx.x] = sacc;
+        acc_add(eacc + (size_t)W.x * EA_N + EA_UREC + threadIdx.x, sacc);
     }
 }
 
@@ -236,33 +151,45 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence_fp64(
 // (Src/energy.F90:1349-1371), bonds (UBond, Src/energy.F90:5335-5387), the
 // UTotal unit conversion into forceo (Src/energy.F90:405-419) and, for MD,
 // the velocity half of VelVer with GetLinAcc (Src/md.F90:349-358, 601-617)
-// and the kinetic-energy partial sum of GetKinEnergy.
+// and GetKinEnergy's partial sum.  The last block of each system then sums
+// the system's partials in a fixed order into its energy record
+// (UTotal/UEwald bookkeeping, Src/energy.F90:395-430, 948-952):
+//   0 utot, 1 utwob(0), 2..11 utwob(1..10), 12 urec, 13 ubond, 14 virial, 15 ekin
 // mode 0: forces only; 1: + velocity Verlet update.
 // ---------------------------------------------------------------------------
 constexpr int NPART_FIN = 4;    // ubond, virbond, ekin, spare
+constexpr int ESZ = 16;
+constexpr int FIN_THREADS = 128;
 
-template <int P>
-__global__ void __launch_bounds__(128) k_finalize_fp64(
+struct FinOut {
+    double *esys, *hist;
+    int hist_cap, nsys;
+    unsigned long long *stepctr, *sstep;
+    unsigned *fdone, *alldone;
+};
+
+template <int P, class PR>
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
-    const int *__restrict__ typ, const int *__restrict__ orig, const int *__restrict__ inv,
-    const double *__restrict__ grid, const double4 *__restrict__ fsr, const double *__restrict__ psurf,
-    const int *__restrict__ bptr, const int *__restrict__ bpart, const double *__restrict__ bk,
-    const double *__restrict__ beq, const int *__restrict__ bpw, const double *__restrict__ massip,
-    const double *__restrict__ massp, double4 *__restrict__ ftot, double4 *__restrict__ forceo,
-    double4 *__restrict__ vel, double4 *__restrict__ acc, double *__restrict__ fpart, int mode,
+    const int *__restrict__ typ, const int *__restrict__ orig,
+    const int *__restrict__ inv, const double *__restrict__ grid, const float *__restrict__ grid32,
+    const double4 *__restrict__ fsr, long long *__restrict__ eacc, const int *__restrict__ bptr,
+    const int *__restrict__ bpart,
+    const double *__restrict__ bk, const double *__restrict__ beq, const int *__restrict__ bpw,
+    const double *__restrict__ massip, const double *__restrict__ massp, double4 *__restrict__ ftot,
+    double4 *__restrict__ forceo, double4 *__restrict__ vel, double4 *__restrict__ acc, int mode, FinOut out,
     ErrWord *err)
 {
+    using R = typename PR::R;
     __shared__ double sq[3];
-    __shared__ double red[3][4];
+    __shared__ double red[3][FIN_THREADS / 32];
+    __shared__ bool last;
     const Tile T = tiles[blockIdx.x];
     const SysDev &S = sysv[T.sys];
     const int i = T.i0 + threadIdx.x;
+    long long *ea = eacc + (size_t)T.sys * EA_N;
     if (S.lsurf) {
-        if (threadIdx.x < 3) {
-            double a = 0.0;
-            for (int k = 0; k < S.ntile128; ++k) a += psurf[(size_t)(S.tile128_off + k) * 4 + threadIdx.x];
-            sq[threadIdx.x] = a;
-        }
+        if (threadIdx.x < 3) sq[threadIdx.x] = acc_get(ea + EA_DIP + threadIdx.x);
         __syncthreads();
     }
     double ub = 0.0, vb = 0.0, ek = 0.0;
@@ -272,17 +199,12 @@ __global__ void __launch_bounds__(128) k_finalize_fp64(
         double Fx = f0.x, Fy = f0.y, Fz = f0.z;
         if (S.lewald) {
             const int s = S.s;
-            double th[3][P], dth[3][P];
-            int km[3];
             const double xc[3] = {x.x, x.y, x.z};
+            R th[3][P], dth[3][P];
+            int km[3];
 #pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                int k = bspline<P>(S.dkdr[m] * xc[m], th[m], dth[m]);
-                k %= s;
-                km[m] = k < 0 ? k + s : k;
-            }
-            const double *G = grid + S.grid_off;
-            double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+            for (int m = 0; m < 3; ++m) km[m] = bspline_at<P, R>(S.dkdr[m] * xc[m], s, th[m], dth[m]);
+            R e0 = 0, e1 = 0, e2 = 0;
 #pragma unroll
             for (int iz = 0; iz < P; ++iz) {
                 int nz = km[2] - iz;
@@ -291,21 +213,21 @@ __global__ void __launch_bounds__(128) k_finalize_fp64(
                 for (int iy = 0; iy < P; ++iy) {
                     int ny = km[1] - iy;
                     ny += (ny < 0) ? s : 0;
-                    const double *rowp = G + ((size_t)nz * s + ny) * s;
+                    const size_t rowo = S.grid_off + ((size_t)nz * s + ny) * s;
 #pragma unroll
                     for (int ix = 0; ix < P; ++ix) {
                         int nx = km[0] - ix;
                         nx += (nx < 0) ? s : 0;
-                        const double Q = rowp[nx];
+                        const R Q = PR::mixed ? (R)grid32[rowo + nx] : (R)grid[rowo + nx];
                         e0 += dth[0][ix] * th[1][iy] * th[2][iz] * Q;
                         e1 += th[0][ix] * dth[1][iy] * th[2][iz] * Q;
                         e2 += th[0][ix] * th[1][iy] * dth[2][iz] * Q;
                     }
                 }
             }
-            Fx -= x.w * e0 * S.dkdr[0] * S.epsfp;
-            Fy -= x.w * e1 * S.dkdr[1] * S.epsfp;
-            Fz -= x.w * e2 * S.dkdr[2] * S.epsfp;
+            Fx -= x.w * (double)e0 * S.dkdr[0] * S.epsfp;
+            Fy -= x.w * (double)e1 * S.dkdr[1] * S.epsfp;
+            Fz -= x.w * (double)e2 * S.dkdr[2] * S.epsfp;
             if (S.lsurf) {
                 const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
                 Fx -= S.epsfp * (2.0 * fac) * x.w * sq[0];
@@ -362,107 +284,56 @@ __global__ void __launch_bounds__(128) k_finalize_fp64(
     __syncthreads();
     if (threadIdx.x < 3) {
         double a = 0.0;
-        for (int k = 0; k < 4; ++k) a += red[threadIdx.x][k];
-        fpart[(size_t)blockIdx.x * NPART_FIN + threadIdx.x] = a;
+        for (int k = 0; k < FIN_THREADS / 32; ++k) a += red[threadIdx.x][k];
+        acc_add(ea + EA_UBOND + threadIdx.x, a);
     }
-}
-
-// ---------------------------------------------------------------------------
-// Per-system totals (UTotal/UEwald bookkeeping, Src/energy.F90:395-430, 948-952),
-// summed in a fixed order.  Record layout (ESZ doubles):
-//   0 utot, 1 utwob(0), 2..11 utwob(1..10), 12 urec, 13 ubond, 14 virial, 15 ekin
-// ---------------------------------------------------------------------------
-constexpr int ESZ = 16;
-
-__device__ double block_sum_fixed(double v, double *sm)
-{
-    v = warp_sum(v);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) sm[w] = v;
+    // ---- the last block of the system forms the system's totals ----
+    __threadfence();
     __syncthreads();
-    double r = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sm[k];
+    if (threadIdx.x == 0) last = (atomicAdd(&out.fdone[T.sys], 1u) == (unsigned)(S.ntile128 - 1));
     __syncthreads();
-    return r;
-}
-
-__global__ void __launch_bounds__(256) k_reduce(const SysDev *__restrict__ sysv, const double *__restrict__ ppart,
-                                               const double *__restrict__ ipart, const double *__restrict__ fpart,
-                                               const double *__restrict__ psurf, double *__restrict__ esys,
-                                               double *__restrict__ hist, int hist_cap,
-                                               unsigned long long *__restrict__ stepctr,
-                                               unsigned long long *__restrict__ sstep,
-                                               unsigned *__restrict__ done, int nsys)
-{
-    __shared__ double sm[8];
-    __shared__ unsigned long long step;
-    const int s = blockIdx.x;
-    const SysDev &S = sysv[s];
-    if (threadIdx.x == 0) step = *stepctr;
-    double acc[NPART_PAIR];
-    for (int p = 0; p < NPART_PAIR; ++p) {
-        double a = 0.0;
-        for (int k = threadIdx.x; k < S.ntile32; k += blockDim.x)
-            a += ppart[(size_t)(S.tile32_off + k) * NPART_PAIR + p];
-        acc[p] = block_sum_fixed(a, sm);
-    }
-    double fin[3];
-    for (int p = 0; p < 3; ++p) {
-        double a = 0.0;
-        for (int k = threadIdx.x; k < S.ntile128; k += blockDim.x)
-            a += fpart[(size_t)(S.tile128_off + k) * NPART_FIN + p];
-        fin[p] = block_sum_fixed(a, sm);
-    }
-    double rec[2] = {0.0, 0.0};
-    if (S.lewald) {
-        for (int p = 0; p < 2; ++p) {
-            double a = 0.0;
-            for (int k = threadIdx.x; k < S.ninfl; k += blockDim.x) a += ipart[(size_t)(S.infl_off + k) * 2 + p];
-            rec[p] = block_sum_fixed(a, sm);
-        }
-    }
-    double sq[3] = {0.0, 0.0, 0.0};
-    if (S.lsurf) {
-        for (int p = 0; p < 3; ++p) {
-            double a = 0.0;
-            for (int k = threadIdx.x; k < S.ntile128; k += blockDim.x) a += psurf[(size_t)(S.tile128_off + k) * 4 + p];
-            sq[p] = block_sum_fixed(a, sm);
-        }
-    }
+    if (!last) return;
+    __threadfence();
     if (threadIdx.x == 0) {
+        double a[EA_N];
+        for (int p = 0; p < EA_N; ++p) a[p] = acc_get(ea + p);
+        for (int p = 0; p < EA_N; ++p) ea[p] = 0;   // ready for the next step
+        const unsigned long long step = *((volatile unsigned long long *)out.stepctr);
         double e[ESZ];
         for (int k = 0; k < ESZ; ++k) e[k] = 0.0;
         double u0 = 0.0;
         for (int p = 0; p < S.natat; ++p) {
-            e[2 + p] = acc[p];
-            u0 += acc[p];
+            e[2 + p] = a[EA_UTWOB + p];
+            u0 += a[EA_UTWOB + p];
         }
         e[1] = u0;
         double urec = 0.0, virrec = 0.0;
         if (S.lewald) {
-            urec = rec[0] + S.uself;
-            virrec = rec[1];
+            urec = a[EA_UREC] + S.uself;
+            virrec = a[EA_VIRREC];
             if (S.lsurf) {
                 const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
-                const double term = fac * (sq[0] * sq[0] + sq[1] * sq[1] + sq[2] * sq[2]);
+                const double term =
+                    fac * (a[EA_DIP] * a[EA_DIP] + a[EA_DIP + 1] * a[EA_DIP + 1] + a[EA_DIP + 2] * a[EA_DIP + 2]);
                 urec += term;
                 virrec -= term;
             }
             urec *= S.epsfp;
         }
         e[12] = urec;
-        e[13] = fin[0];
-        e[0] = u0 + urec + fin[0];
-        e[14] = acc[MSG_MAX_NATAT] + S.epsfp * virrec + fin[1];
-        e[15] = fin[2] * kEkinFac;
-        for (int k = 0; k < ESZ; ++k) esys[(size_t)s * ESZ + k] = e[k];
-        sstep[s] += 1;
-        if (hist && step < (unsigned long long)hist_cap)
-            for (int k = 0; k < ESZ; ++k) hist[((size_t)step * nsys + s) * ESZ + k] = e[k];
+        e[13] = a[EA_UBOND];
+        e[0] = u0 + urec + a[EA_UBOND];
+        e[14] = a[EA_VIRPAIR] + S.epsfp * virrec + a[EA_VIRBOND];
+        e[15] = a[EA_EKIN] * kEkinFac;
+        for (int k = 0; k < ESZ; ++k) out.esys[(size_t)T.sys * ESZ + k] = e[k];
+        if (out.hist && step < (unsigned long long)out.hist_cap)
+            for (int k = 0; k < ESZ; ++k) out.hist[((size_t)step * out.nsys + T.sys) * ESZ + k] = e[k];
+        out.sstep[T.sys] += 1;
+        out.fdone[T.sys] = 0u;
         __threadfence();
-        if (atomicAdd(done, 1u) == (unsigned)(nsys - 1)) {
-            *done = 0u;
-            *stepctr = step + 1;
+        if (atomicAdd(out.alldone, 1u) == (unsigned)(out.nsys - 1)) {
+            *out.alldone = 0u;
+            *out.stepctr = step + 1;
         }
     }
 }

@@ -5,62 +5,6 @@
 
 namespace msg {
 
-// ---------------------------------------------------------------------------
-// Velocity Verlet, position half (Src/md.F90:286-298):
-//   drostep = dt*rod + (dt*dt/2)*rodd;  ro += drostep;  PBC(ro)
-// plus the drosum accumulation of NList (Src/nlist.F90:603-604), the skin
-// r^2 written in MOLSIM order, the surface-term partial sums and the FP32
-// position mirror.  Products and sums are rounded separately (no FMA) so
-// positions match MOLSIM's arithmetic.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_vv_pos(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                               double4 *__restrict__ pos, const double4 *__restrict__ vel,
-                                               const double4 *__restrict__ acc, double4 *__restrict__ dsum,
-                                               const int *__restrict__ orig, double *__restrict__ r2o,
-                                               double *__restrict__ psurf, float4 *__restrict__ pos32)
-{
-    const Tile T = tiles[blockIdx.x];
-    const SysDev &S = sysv[T.sys];
-    const int i = T.i0 + threadIdx.x;
-    double qx = 0.0, qy = 0.0, qz = 0.0;
-    if (i < T.i1) {
-        const double dt = S.dt, fac = __dmul_rn(0.5, __dmul_rn(dt, dt));
-        double4 x = pos[i];
-        const double4 v = vel[i], a = acc[i];
-        double4 d = dsum[i];
-        const double sx = __dadd_rn(__dmul_rn(dt, v.x), __dmul_rn(fac, a.x));
-        const double sy = __dadd_rn(__dmul_rn(dt, v.y), __dmul_rn(fac, a.y));
-        const double sz = __dadd_rn(__dmul_rn(dt, v.z), __dmul_rn(fac, a.z));
-        x.x = pbc_wrap(__dadd_rn(x.x, sx), S.half[0], S.box[0], S.boxi[0]);
-        x.y = pbc_wrap(__dadd_rn(x.y, sy), S.half[1], S.box[1], S.boxi[1]);
-        x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
-        pos[i] = x;
-        d.x = __dadd_rn(d.x, sx);
-        d.y = __dadd_rn(d.y, sy);
-        d.z = __dadd_rn(d.z, sz);
-        dsum[i] = d;
-        r2o[S.off + orig[i]] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
-        if (pos32) pos32[i] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
-        qx = x.w * x.x;
-        qy = x.w * x.y;
-        qz = x.w * x.z;
-    }
-    if (psurf && S.lsurf) {
-        __shared__ double red[3][4];
-        qx = warp_sum(qx);
-        qy = warp_sum(qy);
-        qz = warp_sum(qz);
-        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) { red[0][w] = qx; red[1][w] = qy; red[2][w] = qz; }
-        __syncthreads();
-        if (threadIdx.x < 3) {
-            double s = 0.0;
-            for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
-            psurf[blockIdx.x * 4 + threadIdx.x] = s;
-        }
-    }
-}
-
 // Philox4x32-10 (Salmon et al., SC'11) counter-based generator.
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 {
@@ -89,77 +33,6 @@ __device__ __forceinline__ float3 gauss3(uint64_t seed, uint32_t particle, uint3
     sincospif(2.0f * u2, &s1, &c1);
     sincospif(2.0f * u4, &s2, &c2);
     return make_float3(m1 * c1, m1 * s1, m2 * c2);
-}
-
-// Ermak-McCammon step (Src/bd.F90:142-152): drostep = fac1*forceo + fac2*xi,
-// ro += drostep, PBC.  xi is caller noise in MOLSIM order (xin) or Philox noise.
-__global__ void __launch_bounds__(128) k_bd_pos(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                               double4 *__restrict__ pos, const double4 *__restrict__ forceo,
-                                               double4 *__restrict__ dsum, const int *__restrict__ orig,
-                                               const int *__restrict__ typ, const double *__restrict__ fac1,
-                                               const double *__restrict__ fac2, const double *__restrict__ xin,
-                                               double *__restrict__ xout, uint64_t seed,
-                                               const unsigned long long *__restrict__ sstep,
-                                               double *__restrict__ r2o, double *__restrict__ psurf,
-                                               float4 *__restrict__ pos32)
-{
-    const Tile T = tiles[blockIdx.x];
-    const SysDev &S = sysv[T.sys];
-    const int i = T.i0 + threadIdx.x;
-    double qx = 0.0, qy = 0.0, qz = 0.0;
-    if (i < T.i1) {
-        const int o = orig[i], t = S.type_off + typ[i];
-        const size_t g = (size_t)S.off + o;
-        double xi0, xi1, xi2;
-        if (xin) {
-            xi0 = xin[3 * g];
-            xi1 = xin[3 * g + 1];
-            xi2 = xin[3 * g + 2];
-        } else {
-            const float3 z = gauss3(seed ^ S.seed, (uint32_t)o, (uint32_t)sstep[T.sys]);
-            xi0 = z.x;
-            xi1 = z.y;
-            xi2 = z.z;
-        }
-        if (xout) {
-            xout[3 * g] = xi0;
-            xout[3 * g + 1] = xi1;
-            xout[3 * g + 2] = xi2;
-        }
-        const double f1 = fac1[t], f2 = fac2[t];
-        const double4 f = forceo[i];
-        double4 x = pos[i], d = dsum[i];
-        const double sx = __dadd_rn(__dmul_rn(f1, f.x), __dmul_rn(f2, xi0));
-        const double sy = __dadd_rn(__dmul_rn(f1, f.y), __dmul_rn(f2, xi1));
-        const double sz = __dadd_rn(__dmul_rn(f1, f.z), __dmul_rn(f2, xi2));
-        x.x = pbc_wrap(__dadd_rn(x.x, sx), S.half[0], S.box[0], S.boxi[0]);
-        x.y = pbc_wrap(__dadd_rn(x.y, sy), S.half[1], S.box[1], S.boxi[1]);
-        x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
-        pos[i] = x;
-        d.x = __dadd_rn(d.x, sx);
-        d.y = __dadd_rn(d.y, sy);
-        d.z = __dadd_rn(d.z, sz);
-        dsum[i] = d;
-        r2o[S.off + o] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
-        if (pos32) pos32[i] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
-        qx = x.w * x.x;
-        qy = x.w * x.y;
-        qz = x.w * x.z;
-    }
-    if (psurf && S.lsurf) {
-        __shared__ double red[3][4];
-        qx = warp_sum(qx);
-        qy = warp_sum(qy);
-        qz = warp_sum(qz);
-        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) { red[0][w] = qx; red[1][w] = qy; red[2][w] = qz; }
-        __syncthreads();
-        if (threadIdx.x < 3) {
-            double s = 0.0;
-            for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
-            psurf[blockIdx.x * 4 + threadIdx.x] = s;
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -257,25 +130,19 @@ __device__ double chunk_nonrecord_max(const double *r2, int o0, int o1, double P
     return block_max(best, smd);
 }
 
-__global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ sysv, const int4 *__restrict__ chunks,
-                                                    const double *__restrict__ r2o, SkinChunk *__restrict__ sc,
-                                                    unsigned *__restrict__ sysdone, int *__restrict__ flag,
-                                                    long long *__restrict__ nrebuild, double *__restrict__ skinout,
-                                                    cudaGraphConditionalHandle cond, int use_cond)
+// Chunk summary of four consecutive MOLSIM-order skin values per thread, and,
+// in the last chunk of the system to finish, the combination in MOLSIM order
+// and the rebuild decision (NList, Src/nlist.F90:600-613).
+__device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[4], int o0, int o1,
+                           const double *__restrict__ r2o, SkinChunk *__restrict__ sc,
+                           unsigned *__restrict__ sysdone, int *__restrict__ flag,
+                           long long *__restrict__ nrebuild, double *__restrict__ skinout,
+                           cudaGraphConditionalHandle cond, int use_cond)
 {
     __shared__ double smd[SK_THREADS / 32];
     __shared__ int smi[SK_THREADS / 32];
     __shared__ bool last;
-    const int4 C = chunks[blockIdx.x];   // sys, o0 (global), o1 (global), first chunk of system
-    const int s = C.x;
-    const SysDev &S = sysv[s];
     const int t = threadIdx.x;
-    double v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int o = C.y + 4 * t + k;
-        v[k] = (o < C.z) ? r2o[o] : 0.0;
-    }
     double tmax = fmax(fmax(v[0], v[1]), fmax(v[2], v[3]));
     double run = block_excl_max(tmax, smd);
     double amax = 0.0;
@@ -283,15 +150,15 @@ __global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ 
     double recv[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        int o = C.y + 4 * t + k;
-        if (o < C.z) {
+        const int o = o0 + 4 * t + k;
+        if (o < o1) {
             if (v[k] > run) { run = v[k]; recv[nrec++] = v[k]; }
             else amax = fmax(amax, v[k]);
         }
     }
     int total;
     const int roff = block_excl_sum_int(nrec, smi, &total);
-    SkinChunk &out = sc[blockIdx.x];
+    SkinChunk &out = sc[chunk];
     for (int k = 0; k < nrec; ++k)
         if (roff + k < SK_REC) out.rec[roff + k] = recv[k];
     const double bm = block_max(tmax, smd);
@@ -342,8 +209,8 @@ __global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ 
                 if (t == k) { isovf = ovf ? 1 : 0; Pk = P; }
                 __syncthreads();
                 if (isovf) {
-                    const int o0 = S.off + (cb + k) * SK_CHUNK, o1 = min(S.off + S.n, o0 + SK_CHUNK);
-                    m2 = fmax(m2, chunk_nonrecord_max(r2o, o0, o1, Pk, smd));
+                    const int q0 = S.off + (cb + k) * SK_CHUNK, q1 = min(S.off + S.n, q0 + SK_CHUNK);
+                    m2 = fmax(m2, chunk_nonrecord_max(r2o, q0, q1, Pk, smd));
                 }
                 __syncthreads();
             }
@@ -361,6 +228,115 @@ __global__ void __launch_bounds__(SK_THREADS) k_skin(const SysDev *__restrict__ 
         if (skinout) { skinout[2 * s] = carry; skinout[2 * s + 1] = m2; }
         sysdone[s] = 0u;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Velocity Verlet, position half (Src/md.F90:286-298) fused with NList's skin
+// test: drostep = dt*rod + (dt*dt/2)*rodd; ro += drostep; PBC(ro);
+// drosum += drostep (Src/nlist.F90:603-604).  Each block is one skin chunk of
+// 1024 consecutive MOLSIM indices, so the skin values arrive in MOLSIM order;
+// particles are reached through inv[].  Products and sums round separately
+// (no FMA) so positions follow MOLSIM's arithmetic.  Also refreshes the FP32
+// position mirror used by the mixed-precision kernels.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(SK_THREADS) k_vv_skin(
+    const SysDev *__restrict__ sysv, const int4 *__restrict__ chunks, const int *__restrict__ inv,
+    double4 *__restrict__ pos, const double4 *__restrict__ vel, const double4 *__restrict__ acc,
+    double4 *__restrict__ dsum, int4 *__restrict__ posfx, double *__restrict__ r2o, SkinChunk *__restrict__ sc,
+    unsigned *__restrict__ sysdone, int *__restrict__ flag, long long *__restrict__ nrebuild,
+    double *__restrict__ skinout, cudaGraphConditionalHandle cond, int use_cond)
+{
+    const int4 C = chunks[blockIdx.x];
+    const SysDev &S = sysv[C.x];
+    const double dt = S.dt, fac = __dmul_rn(0.5, __dmul_rn(dt, dt));
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int o = C.y + 4 * threadIdx.x + k;
+        v[k] = 0.0;
+        if (o < C.z) {
+            const int i = inv[o];
+            double4 x = pos[i];
+            const double4 u = vel[i], a = acc[i];
+            double4 d = dsum[i];
+            const double sx = __dadd_rn(__dmul_rn(dt, u.x), __dmul_rn(fac, a.x));
+            const double sy = __dadd_rn(__dmul_rn(dt, u.y), __dmul_rn(fac, a.y));
+            const double sz = __dadd_rn(__dmul_rn(dt, u.z), __dmul_rn(fac, a.z));
+            x.x = pbc_wrap(__dadd_rn(x.x, sx), S.half[0], S.box[0], S.boxi[0]);
+            x.y = pbc_wrap(__dadd_rn(x.y, sy), S.half[1], S.box[1], S.boxi[1]);
+            x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
+            pos[i] = x;
+            if (posfx) posfx[i] = fx_pos(x, S);
+            d.x = __dadd_rn(d.x, sx);
+            d.y = __dadd_rn(d.y, sy);
+            d.z = __dadd_rn(d.z, sz);
+            dsum[i] = d;
+            v[k] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
+            r2o[o] = v[k];
+        }
+    }
+    skin_chunk(S, C.x, blockIdx.x, v, C.y, C.z, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
+}
+
+// Ermak-McCammon step (Src/bd.F90:142-152) fused with the skin test:
+// drostep = fac1*forceo + fac2*xi, ro += drostep, PBC.  xi is caller noise in
+// MOLSIM order (xin) or FP32 Philox noise keyed by (seed, particle, step).
+__global__ void __launch_bounds__(SK_THREADS) k_bd_skin(
+    const SysDev *__restrict__ sysv, const int4 *__restrict__ chunks, const int *__restrict__ inv,
+    double4 *__restrict__ pos, const double4 *__restrict__ forceo, double4 *__restrict__ dsum,
+    const int *__restrict__ typ, const double *__restrict__ fac1, const double *__restrict__ fac2,
+    const double *__restrict__ xin, double *__restrict__ xout, uint64_t seed,
+    const unsigned long long *__restrict__ sstep, int4 *__restrict__ posfx, double *__restrict__ r2o,
+    SkinChunk *__restrict__ sc, unsigned *__restrict__ sysdone, int *__restrict__ flag,
+    long long *__restrict__ nrebuild, double *__restrict__ skinout, cudaGraphConditionalHandle cond,
+    int use_cond)
+{
+    const int4 C = chunks[blockIdx.x];
+    const SysDev &S = sysv[C.x];
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int o = C.y + 4 * threadIdx.x + k;
+        v[k] = 0.0;
+        if (o < C.z) {
+            const int i = inv[o];
+            const int t = S.type_off + typ[i];
+            double xi0, xi1, xi2;
+            if (xin) {
+                xi0 = xin[3 * (size_t)o];
+                xi1 = xin[3 * (size_t)o + 1];
+                xi2 = xin[3 * (size_t)o + 2];
+            } else {
+                const float3 z = gauss3(seed ^ S.seed, (uint32_t)(o - S.off), (uint32_t)sstep[C.x]);
+                xi0 = z.x;
+                xi1 = z.y;
+                xi2 = z.z;
+            }
+            if (xout) {
+                xout[3 * (size_t)o] = xi0;
+                xout[3 * (size_t)o + 1] = xi1;
+                xout[3 * (size_t)o + 2] = xi2;
+            }
+            const double f1 = fac1[t], f2 = fac2[t];
+            const double4 f = forceo[i];
+            double4 x = pos[i], d = dsum[i];
+            const double sx = __dadd_rn(__dmul_rn(f1, f.x), __dmul_rn(f2, xi0));
+            const double sy = __dadd_rn(__dmul_rn(f1, f.y), __dmul_rn(f2, xi1));
+            const double sz = __dadd_rn(__dmul_rn(f1, f.z), __dmul_rn(f2, xi2));
+            x.x = pbc_wrap(__dadd_rn(x.x, sx), S.half[0], S.box[0], S.boxi[0]);
+            x.y = pbc_wrap(__dadd_rn(x.y, sy), S.half[1], S.box[1], S.boxi[1]);
+            x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
+            pos[i] = x;
+            if (posfx) posfx[i] = fx_pos(x, S);
+            d.x = __dadd_rn(d.x, sx);
+            d.y = __dadd_rn(d.y, sy);
+            d.z = __dadd_rn(d.z, sz);
+            dsum[i] = d;
+            v[k] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
+            r2o[o] = v[k];
+        }
+    }
+    skin_chunk(S, C.x, blockIdx.x, v, C.y, C.z, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
 }
 
 // ---------------------------------------------------------------------------
@@ -451,6 +427,27 @@ __global__ void __launch_bounds__(128) k_copyback(const Tile *__restrict__ tiles
     dsum[j] = make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
+// Fixed-point position mirror of rebuilt systems after their permutation.
+__global__ void __launch_bounds__(128) k_mirror(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                               const int *__restrict__ flag, const double4 *__restrict__ pos,
+                                               int4 *__restrict__ posfx)
+{
+    const Tile T = tiles[blockIdx.x];
+    if (!flag[T.sys]) return;
+    const int j = T.i0 + threadIdx.x;
+    if (j >= T.i1) return;
+    posfx[j] = fx_pos(pos[j], sysv[T.sys]);
+}
+
+__global__ void k_mirror_range(const SysDev *__restrict__ sysv, int sys, const double4 *__restrict__ pos,
+                               int4 *__restrict__ posfx)
+{
+    const SysDev &S = sysv[sys];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= S.n) return;
+    posfx[S.off + j] = fx_pos(pos[S.off + j], S);
+}
+
 __global__ void k_clear_cells(int *__restrict__ cstart, int *__restrict__ cend, int n)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -489,6 +486,7 @@ __device__ __forceinline__ int stencil1(int c, int nc, int *out)
 // with a warp ballot.  Rows are ordered by stencil cell, then by MOLSIM index.
 __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, const int *__restrict__ sys,
                                               const int *__restrict__ flag, const double4 *__restrict__ pos,
+                                              const int *__restrict__ typ,
                                               const int *__restrict__ cellid, const int *__restrict__ cstart,
                                               const int *__restrict__ cend, int *__restrict__ nbl,
                                               int *__restrict__ nnb, int ntot, int *__restrict__ nmaxrow,
@@ -524,7 +522,8 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
                     const unsigned bal = __ballot_sync(0xffffffffu, ok);
                     if (ok) {
                         const int slot = count + __popc(bal & lt);
-                        if (slot < S.cap) row[slot] = j;
+                        // entry: partner index, partner type in bits 28-29
+                        if (slot < S.cap) row[slot] = j | (typ[j] << 28);
                     }
                     count += __popc(bal);
                 }
@@ -560,7 +559,7 @@ __global__ void k_export_nlist(const SysDev *__restrict__ sysv, int s, const int
         int jp = 0;
         bool ok = false;
         if (k < n) {
-            jp = orig[row[k]] + 1;
+            jp = orig[row[k] & ((1 << 28) - 1)] + 1;
             const int itemp = (ip + jp) % 2;
             ok = !((ip < jp && itemp == 0) || (ip > jp && itemp != 0));
         }

@@ -1,0 +1,344 @@
+// kernels_pair.cuh -- UTwoBodyA (Src/energy.F90:445-544) over the full Verlet list.
+//
+// One particle per group of G lanes; the lanes stride over the particle's
+// row, so a row is read with coalesced 64-byte segments and every pair is
+// evaluated by both of its particles (forces need no atomics and are summed in
+// a fixed order).  Each pair's energy and virial are counted once (i < j).
+// List entries carry the partner's type in bits 28-29, so the type-pair record
+// is found without a load of the partner's type.  A block owns a contiguous
+// range of warp tasks (32/G particles each, G lanes per particle chosen per
+// system from the row length), keeps the current system's table (coefficient
+// rows and bucket starts) in shared memory, and its warps pull tasks from a
+// shared counter, so no barrier waits on a long row.  The G lanes of a particle read
+// consecutive row entries -- consecutive particles of one cell, so the
+// position gathers coalesce -- and in FP32 each lane carries two such entries
+// in lockstep, so their loads and polynomial chains overlap.
+// Each particle's energy and virial are rounded once to 64-bit fixed point and
+// summed as integers, so the totals do not depend on the task layout.
+//
+// Two precisions share the kernel:
+//   PrecD  positions double4, table FP64, forces summed in FP64 registers;
+//   PrecM  positions as 32-bit fixed-point box coordinates (exact, wrapping
+//          differences converted to FP32), table and pair forces FP32; each
+//          lane's FP64 partial force is rounded to 64-bit fixed point
+//          (2^-32 kJ/(mol A)) and the lanes are combined as integers, so the
+//          result does not depend on the combination order.
+// Energies and virial are summed in FP64 within a block and added to the
+// system's 64-bit fixed-point accumulators (order-independent) in both.
+#pragma once
+
+#include "common.cuh"
+
+namespace msg {
+
+constexpr int PAIR_BLOCK = 256;
+constexpr int MAXT = 4;
+constexpr int NBL_JMASK = (1 << 28) - 1;
+constexpr double kFixScale = 4294967296.0;          // 2^32
+constexpr double kFixInv = 1.0 / 4294967296.0;
+
+struct PrecD {
+    using R = double;
+    using V4 = double4;
+    static constexpr bool mixed = false;
+};
+struct PrecM {
+    using R = float;
+    using V4 = int4;   // fixed-point box coordinates (fx_pos)
+    static constexpr bool mixed = true;
+};
+
+// Interval of MOLSIM's table (Src/energy.F90:481-486): the reference walks
+// ibuf upwards from iubuflow while r2 < zlow.  pair_eval starts the walk at a
+// bucket entry chosen on the host to lie at or before the interval the full
+// walk finds, then makes the same comparisons, so it ends on the same interval.
+__device__ __forceinline__ double pbc_shift(double d, double half, double box)
+{
+    return (fabs(d) > half) ? d - copysign(box, d) : d;
+}
+
+// Warp tasks: 32/G consecutive particles of one system, G lanes each.  send is
+// the index one past the last task of the same system (a task run).
+struct PairTask { int sys, i0, i1, g, send, pad0, pad1, pad2; };
+
+// Coefficient row of 12 values ([0] = zlow of the interval,
+// Src/potential.F90:1192-1207) read with 16-byte loads.
+template <typename R> struct Row12;
+template <> struct Row12<double> {
+    double c[12];
+    __device__ __forceinline__ void load(const double *p)
+    {
+        const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const double2 v = q[k];
+            c[2 * k] = v.x;
+            c[2 * k + 1] = v.y;
+        }
+    }
+};
+template <> struct Row12<float> {
+    float c[12];
+    __device__ __forceinline__ void load(const float *p)
+    {
+        const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float4 v = q[k];
+            c[4 * k] = v.x;
+            c[4 * k + 1] = v.y;
+            c[4 * k + 2] = v.z;
+            c[4 * k + 3] = v.w;
+        }
+    }
+};
+
+// Shared-memory image of a system's table: coefficient rows, then bucket
+// starts.  Sized on the host (pair_smem_bytes); systems whose table does not
+// fit read it from global memory through the same generic pointers.
+template <typename R>
+__host__ __device__ inline size_t pair_smem_bytes(int nk, int nbucket)
+{
+    return (size_t)nk * 12 * sizeof(R) + (size_t)nbucket * sizeof(unsigned short);
+}
+
+// Lanes per batch: B row segments per lane are in flight together.
+template <class PR> struct PairBatch { static constexpr int B = PR::mixed ? 2 : 1; };
+
+// NT: particle types per system accounted in registers (2 or 4).
+// Block b owns warp tasks [b*ntasks/nb, (b+1)*ntasks/nb); it walks them in runs of
+// one system: load that system's table into shared memory, let its warps pull
+// tasks from a shared counter, and meet at a barrier only where the run ends.
+template <class PR, int NT>
+__global__ void __launch_bounds__(PAIR_BLOCK, 2) k_pair(
+    const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, int ntasks,
+    const typename PR::V4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
+    const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
+    const typename PR::R *__restrict__ tz, const typename PR::R *__restrict__ tc,
+    const unsigned short *__restrict__ bst, double4 *__restrict__ fsr, long long *__restrict__ eacc, ErrWord *err)
+{
+    using R = typename PR::R;
+    using V4 = typename PR::V4;
+    constexpr int B = PairBatch<PR>::B;
+    (void)tz;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ PairTab sP[MSG_MAX_NATAT];
+    __shared__ int sMap[MAXT * MAXT];
+    __shared__ int sNext;
+    const int lane = threadIdx.x & 31;
+    const int t0 = (int)(((long long)blockIdx.x * ntasks) / gridDim.x);
+    const int t1 = (int)(((long long)(blockIdx.x + 1) * ntasks) / gridDim.x);
+    // energies by (particle type, partner type) in 64-bit fixed point: each particle's
+    // contribution is rounded once, so the sums do not depend on which warp took which task
+    long long ue[NT * NT];
+    long long vir = 0;
+#pragma unroll
+    for (int q = 0; q < NT * NT; ++q) ue[q] = 0;
+    int loaded = -1;
+    const R *Tc = nullptr;
+    const unsigned short *Tb = nullptr;
+    int kbase = 0, bbase = 0;
+    for (int rs = t0; rs < t1;) {
+        const PairTask W0 = tasks[rs];
+        const int re = min(t1, W0.send);
+        __syncthreads();                      // previous run's warps are done with sNext / the table
+        if (W0.sys != loaded) {
+            const SysDev &Sn = sysv[W0.sys];
+            if (threadIdx.x < Sn.natat) sP[threadIdx.x] = ptab[Sn.pt_off + threadIdx.x];
+            if (threadIdx.x < Sn.npt * Sn.npt) sMap[threadIdx.x] = ptmap[Sn.ptmap_off + threadIdx.x] - Sn.pt_off;
+            kbase = Sn.tab_k0;
+            bbase = Sn.tab_b0;
+            if (Sn.tab_smem) {
+                R *sc = reinterpret_cast<R *>(dyn);
+                unsigned short *sb = reinterpret_cast<unsigned short *>(sc + (size_t)12 * Sn.tab_nk);
+                const int nc = 12 * Sn.tab_nk, nb = Sn.natat * MSG_NBUCKET;
+                for (int k = threadIdx.x; k < nc; k += PAIR_BLOCK) sc[k] = tc[(size_t)12 * Sn.tab_k0 + k];
+                for (int k = threadIdx.x; k < nb; k += PAIR_BLOCK) sb[k] = bst[Sn.tab_b0 + k];
+                Tc = sc;
+                Tb = sb;
+            } else {
+                Tc = tc + (size_t)12 * Sn.tab_k0;
+                Tb = bst + Sn.tab_b0;
+            }
+            loaded = W0.sys;
+        }
+        if (threadIdx.x == 0) sNext = rs;
+        __syncthreads();
+        const SysDev &S = sysv[W0.sys];
+        const R rcut2 = (R)S.rcut2;
+        const R lowmax = (R)fmax(S.r2umin_max, S.r2atat_max);
+        for (;;) {
+            int task = 0;
+            if (lane == 0) task = atomicAdd(&sNext, 1);
+            task = __shfl_sync(0xffffffffu, task, 0);
+            if (task >= re) break;
+            const PairTask W = tasks[task];
+            const int G = W.g;
+            const int g = lane & (G - 1);
+            const int i = W.i0 + lane / G;
+            const bool act = i < W.i1;
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            double ut[NT];                                   // energy by partner type
+            double vi = 0.0;
+#pragma unroll
+            for (int t = 0; t < NT; ++t) ut[t] = 0.0;
+            int ti = 0, n = 0;
+            V4 xi;
+            const int *row = nbl;
+            if (act) {
+                xi = pos[i];
+                ti = typ[i];
+                n = nnb[i];
+                row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
+            }
+            for (int kb = g; kb < n; kb += B * G) {
+                // B row entries G apart per lane: the particle's G lanes read consecutive entries
+                int ee[B];
+                bool ok[B];
+                V4 xj[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    ok[u] = kb + u * G < n;
+                    ee[u] = ok[u] ? __ldg(row + kb + u * G) : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < B; ++u) xj[u] = pos[ok[u] ? (ee[u] & NBL_JMASK) : i];
+                R dx[B], dy[B], dz[B], r2[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    if constexpr (PR::mixed) {
+                        // exact integer difference, wrapped to the minimum image
+                        dx[u] = (float)(int)((unsigned)xi.x - (unsigned)xj[u].x) * S.fxi[0];
+                        dy[u] = (float)(int)((unsigned)xi.y - (unsigned)xj[u].y) * S.fxi[1];
+                        dz[u] = (float)(int)((unsigned)xi.z - (unsigned)xj[u].z) * S.fxi[2];
+                        r2[u] = dx[u] * dx[u] + dy[u] * dy[u] + dz[u] * dz[u];
+                    } else {
+                        dx[u] = pbc_shift(xi.x - xj[u].x, S.half[0], S.box[0]);
+                        dy[u] = pbc_shift(xi.y - xj[u].y, S.half[1], S.box[1]);
+                        dz[u] = pbc_shift(xi.z - xj[u].z, S.half[2], S.box[2]);
+                        // the reference's rounding: ((dx*dx)+(dy*dy))+(dz*dz), no FMA
+                        r2[u] = __dadd_rn(__dadd_rn(__dmul_rn(dx[u], dx[u]), __dmul_rn(dy[u], dy[u])),
+                                          __dmul_rn(dz[u], dz[u]));
+                    }
+                    ok[u] = ok[u] && !(r2[u] > rcut2);
+                }
+                int tj[B], kk[B], pi[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    tj[u] = (unsigned)ee[u] >> 28;
+                    pi[u] = sMap[ti * S.npt + (ok[u] ? tj[u] : 0)];
+                    const PairTab &P = sP[pi[u]];
+                    const float r2f = (float)r2[u];
+                    int k = 0;
+                    if (r2f < (float)P.z_hi) {
+                        int bk = (int)((r2f - (float)P.z_lo) * (float)P.inv_h);
+                        bk = bk < 0 ? 0 : (bk >= MSG_NBUCKET ? MSG_NBUCKET - 1 : bk);
+                        k = Tb[P.b0 - bbase + bk];
+                    }
+                    kk[u] = k;
+                }
+                Row12<R> c[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) c[u].load(Tc + (size_t)(sP[pi[u]].k0 - kbase + kk[u]) * 12);
+                R usum[B], fsum[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    if (ok[u] && (r2[u] < lowmax || r2[u] < c[u].c[0])) {
+                        // rare: below the type pair's lower limits, or the walk goes past the bucket start
+                        const PairTab &Q = sP[pi[u]];
+                        if (r2[u] < (R)Q.r2atat) {
+                            // hard-core overlap: u = 1e10, f = 0 (the reference leaves fsum stale here)
+                            c[u].c[0] = r2[u];
+                            c[u].c[1] = (R)1e10;
+#pragma unroll
+                            for (int q = 2; q < 12; ++q) c[u].c[q] = (R)0;
+                        } else if (r2[u] < (R)Q.r2umin) {
+                            raise_error(err, 1, W.sys, i, ee[u] & NBL_JMASK);
+                            ok[u] = false;
+                        } else {
+                            while (r2[u] < c[u].c[0]) {
+                                if (++kk[u] >= Q.nk) {
+                                    raise_error(err, 2, W.sys, i, ee[u] & NBL_JMASK);
+                                    kk[u] = Q.nk - 1;
+                                    c[u].load(Tc + (size_t)(Q.k0 - kbase + kk[u]) * 12);
+                                    break;
+                                }
+                                c[u].load(Tc + (size_t)(Q.k0 - kbase + kk[u]) * 12);
+                            }
+                        }
+                    }
+                    const R d = r2[u] - c[u].c[0];
+                    usum[u] = c[u].c[1] + d * (c[u].c[2] + d * (c[u].c[3] + d * (c[u].c[4] + d * (c[u].c[5] +
+                              d * c[u].c[6]))));
+                    fsum[u] = c[u].c[7] + d * (c[u].c[8] + d * (c[u].c[9] + d * (c[u].c[10] + d * c[u].c[11])));
+                }
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    if (!ok[u]) continue;
+                    const int j = ee[u] & NBL_JMASK;
+                    fx += (double)(fsum[u] * dx[u]);
+                    fy += (double)(fsum[u] * dy[u]);
+                    fz += (double)(fsum[u] * dz[u]);
+                    if (i < j) {
+#pragma unroll
+                        for (int t = 0; t < NT; ++t) ut[t] += (tj[u] == t) ? (double)usum[u] : 0.0;
+                        vi -= (double)fsum[u] * (double)r2[u];
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                const long long v = __double2ll_rn(ut[t] * kEFix);
+#pragma unroll
+                for (int q = 0; q < NT; ++q) ue[q * NT + t] += (q == ti) ? v : 0;
+            }
+            vir += __double2ll_rn(vi * kEFix);
+            // reduce the particle's force over its G lanes; in FP32 mode each lane's FP64
+            // partial is rounded to 64-bit fixed point first, so the combination is exact
+            if constexpr (PR::mixed) {
+                long long ax = __double2ll_rn(fx * kFixScale), ay = __double2ll_rn(fy * kFixScale),
+                          az = __double2ll_rn(fz * kFixScale);
+                for (int o = G >> 1; o > 0; o >>= 1) {
+                    ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                    ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                    az += __shfl_xor_sync(0xffffffffu, az, o);
+                }
+                if (act && g == 0)
+                    fsr[i] = make_double4((double)ax * kFixInv, (double)ay * kFixInv, (double)az * kFixInv, 0.0);
+            } else {
+                for (int o = G >> 1; o > 0; o >>= 1) {
+                    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                }
+                if (act && g == 0) fsr[i] = make_double4(fx, fy, fz, 0.0);
+            }
+        }
+        // the run's energies: per warp, integer sums into the system's accumulators
+#pragma unroll
+        for (int q = 0; q < NT * NT; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ue[q] += __shfl_xor_sync(0xffffffffu, ue[q], o);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vir += __shfl_xor_sync(0xffffffffu, vir, o);
+        long long *ea = eacc + (size_t)W0.sys * EA_N;
+        if (lane < S.npt * S.npt) {
+            const int ti = lane / S.npt, tj = lane % S.npt;
+            // (ti, tj) and (tj, ti) are one type pair: take ti <= tj and add both halves
+            if (ti <= tj) {
+                long long v = 0;
+#pragma unroll
+                for (int q = 0; q < NT * NT; ++q)
+                    v += (q == ti * NT + tj || (ti != tj && q == tj * NT + ti)) ? ue[q] : 0;
+                if (v) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_UTWOB + sMap[lane]), (unsigned long long)v);
+            }
+        }
+        if (lane == 31 && vir) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_VIRPAIR), (unsigned long long)vir);
+#pragma unroll
+        for (int q = 0; q < NT * NT; ++q) ue[q] = 0;
+        vir = 0;
+        rs = re;
+    }
+}
+
+}  // namespace msg

@@ -59,7 +59,8 @@ def pot_tab(sysd, ualpha, nbuf=100000):
 def prepare(sysd):
     """Derive alpha (IOPotTwoBody -> EwaldSetup, iewaldopt=3) and the pair table."""
     q2sum = float(np.mean(np.asarray(sysd["az"], np.float64) ** 2))
-    alpha = rcut_to_alpha(sysd["uewaldtol"], q2sum, sysd["epsi_four_pi"], min(sysd["boxlen"]), sysd["rcut"])
+    alpha = rcut_to_alpha(sysd["uewaldtol"], q2sum, sysd["epsi_four_pi"], min(sysd["boxlen"]), sysd["rcut"]) \
+        if sysd["lewald"] else 0.0
     tab = pot_tab(sysd, alpha)
     natat = sysd["npt"] * (sysd["npt"] + 1) // 2
     tab["r2atat"] = np.zeros(natat)

@@ -276,6 +276,10 @@ class System:
             raise RuntimeError("BDStep failed: %d" % rc)
         return bool(rb.value)
 
+    def set_drosum(self, drosum):
+        d = np.ascontiguousarray(drosum, np.float64)
+        lib().or_set_drosum(self.h, _p(d, C.c_double))
+
     def skin_test(self, drostep):
         d = np.ascontiguousarray(drostep, np.float64)
         m1 = C.c_double()

@@ -10,7 +10,8 @@ from molsim_b200 import systems as S
 def oracle_table(s):
     """Alpha and pair table from the oracle (RcutToAlpha + PotTwoBodyTab1)."""
     q2 = float(np.mean(np.asarray(s["az"]) ** 2))
-    alpha = O.rcut_to_alpha(s["uewaldtol"], q2, s["epsi_four_pi"], min(s["boxlen"]), s["rcut"])
+    alpha = O.rcut_to_alpha(s["uewaldtol"], q2, s["epsi_four_pi"], min(s["boxlen"]), s["rcut"]) \
+        if s["lewald"] else 0.0
     pot = dict(npt=s["npt"], zat=s["zat"], sigat=s["sigat"], epsat=s["epsat"], rcut=s["rcut"], ualpha=alpha,
                epsi_four_pi=s["epsi_four_pi"], lewald=int(s["lewald"]), lljcut=int(s["lljcut"]),
                **{k: s[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab",
