@@ -38,7 +38,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--replicas", type=int, default=16,
+                    help="replicas of the workload in one handle for the batched figure (0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -211,6 +213,30 @@ def run_gpu(a):
         if rc:
             raise RuntimeError(L.msg_last_error(eng.h).decode())
 
+    def timed_steps(e, K):
+        """K steps, L2 flushed before each, device time summed over the steps (ms)."""
+        Lx = _lib.lib()
+        extx = torch.cuda.ExternalStream(e.stream())
+        for _ in range(max(3, a.warmup)):
+            with torch.cuda.stream(extx):
+                flush.zero_()
+            if Lx.msg_velver_async(e.h, 1):
+                raise RuntimeError(Lx.msg_last_error(e.h).decode())
+        e.VelVer(1, energies=False)
+        torch.cuda.synchronize()
+        st = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        en = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        for k in range(K):
+            with torch.cuda.stream(extx):
+                flush.zero_()
+                st[k].record(extx)
+            if Lx.msg_velver_async(e.h, 1):
+                raise RuntimeError(Lx.msg_last_error(e.h).decode())
+            with torch.cuda.stream(extx):
+                en[k].record(extx)
+        torch.cuda.synchronize()
+        return sum(x.elapsed_time(y) for x, y in zip(st, en))
+
     # warm-up (also captures the step graph)
     for _ in range(max(3, a.warmup)):
         with torch.cuda.stream(ext):
@@ -228,6 +254,7 @@ def run_gpu(a):
     torch.cuda.synchronize()
     clocks.start()
     l0 = eng.launch_count()
+    nb0 = eng.nrebuild(0)
     for k in range(a.steps):
         with torch.cuda.stream(ext):
             flush.zero_()
@@ -237,6 +264,7 @@ def run_gpu(a):
             ends[k].record(ext)
     torch.cuda.synchronize()
     launches = eng.launch_count() - l0
+    rebuilds = eng.nrebuild(0) - nb0
     clk = clocks.stop()
     t_ms = sum(st.elapsed_time(en) for st, en in zip(starts, ends))
     if world > 1:
@@ -245,6 +273,27 @@ def run_gpu(a):
         torch.distributed.barrier()
         t_ms = float(tt.item())
     value = n * a.steps * world / (t_ms / 1000.0)
+
+    # ---- the plain FP64 path on the same system (the drop-in and the comparison base) ----
+    fp64_value = None
+    if a.precision != "fp64":
+        e64 = Engine(s, precision="fp64")
+        e64.UTotal()
+        e64.GetLinAcc()
+        fp64_value = n * a.steps / (timed_steps(e64, a.steps) / 1000.0)
+        del e64
+    # ---- batched: replicas of the workload advanced together in one handle ----
+    batched = None
+    if a.replicas > 1:
+        eb = Engine([dict(s) for _ in range(a.replicas)], precision=a.precision)
+        eb.UTotal(0)
+        eb.GetLinAcc()
+        kb = max(10, a.steps // 4)
+        tb = timed_steps(eb, kb)
+        batched = {"replicas": a.replicas, "value": n * a.replicas * kb / (tb / 1000.0), "unit": METRIC,
+                   "steps": kb, "ms_per_step": tb / kb,
+                   "vs_fp64_single": (n * a.replicas * kb / (tb / 1000.0)) / fp64_value if fp64_value else None}
+        del eb
 
     # ---- per-kernel device times: the same K steps with the library's CUDA-event timers ----
     eng.set_timing(True)
@@ -267,7 +316,7 @@ def run_gpu(a):
     e = _lib.MsgEnergy()
     f64 = C.POINTER(C.c_double)
     pr = [x.ctypes.data_as(f64) for x in (ro, rod, rodd)]
-    ke = max(10, a.steps // 2)
+    ke = max(10, a.steps // 2) if not a.no_e2e else 1
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -315,7 +364,9 @@ def run_gpu(a):
             "config": {"workload": WORKLOAD, "particles": n, "half_list_pairs": int(npair),
                        "spme": "64^3 order 5", "rcut_A": 25.0, "skin_A": 2.0, "precision": a.precision,
                        "integrator": "velocity Verlet", "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "flushed (256 MB write) before every timed step"},
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "rebuilds_in_timed_steps": int(rebuilds)},
+            "fp64_value": fp64_value, "batched": batched,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

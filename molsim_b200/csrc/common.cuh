@@ -71,6 +71,8 @@ struct PairTab {
     int pad;
     double z_lo, z_hi, inv_h;   // bucket grid over [z_lo, z_hi)
     double r2umin, r2atat;
+    float fz_lo, fz_hi, finv_h; // the bucket grid in FP32 (the bucket index is formed in FP32)
+    float pad2;
 };
 
 struct Tile { int sys, i0, i1, pad; };

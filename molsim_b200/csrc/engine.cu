@@ -477,6 +477,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                 T.z_lo = T.r2umin;
                 const double h = (T.z_hi > T.z_lo) ? (T.z_hi - T.z_lo) / MSG_NBUCKET : 1.0;
                 T.inv_h = 1.0 / h;
+                T.fz_lo = (float)T.z_lo;
+                T.fz_hi = (float)T.z_hi;
+                T.finv_h = (float)T.inv_h;
                 T.b0 = (int)vb.size();
                 for (int b = 0; b < MSG_NBUCKET; ++b) {
                     const double zq = T.z_lo + (b + 2) * h;

@@ -20,9 +20,9 @@
 //   PrecD  positions double4, table FP64, forces summed in FP64 registers;
 //   PrecM  positions as 32-bit fixed-point box coordinates (exact, wrapping
 //          differences converted to FP32), table and pair forces FP32; each
-//          lane's FP64 partial force is rounded to 64-bit fixed point
-//          (2^-32 kJ/(mol A)) and the lanes are combined as integers, so the
-//          result does not depend on the combination order.
+//          lane's partial force (a few pair terms, FP32) is rounded to 64-bit
+//          fixed point (2^-32 kJ/(mol A)) and the lanes are combined as
+//          integers, so the result does not depend on the combination order.
 // Energies and virial are summed in FP64 within a block and added to the
 // system's 64-bit fixed-point accumulators (order-independent) in both.
 #pragma once
@@ -103,14 +103,20 @@ __host__ __device__ inline size_t pair_smem_bytes(int nk, int nbucket)
 }
 
 // Lanes per batch: B row segments per lane are in flight together.
-template <class PR> struct PairBatch { static constexpr int B = PR::mixed ? 2 : 1; };
+#ifndef MSG_PAIR_B32
+#define MSG_PAIR_B32 2
+#endif
+#ifndef MSG_PAIR_MINB
+#define MSG_PAIR_MINB 2
+#endif
+template <class PR> struct PairBatch { static constexpr int B = PR::mixed ? MSG_PAIR_B32 : 1; };
 
 // NT: particle types per system accounted in registers (2 or 4).
 // Block b owns warp tasks [b*ntasks/nb, (b+1)*ntasks/nb); it walks them in runs of
 // one system: load that system's table into shared memory, let its warps pull
 // tasks from a shared counter, and meet at a barrier only where the run ends.
 template <class PR, int NT>
-__global__ void __launch_bounds__(PAIR_BLOCK, 2) k_pair(
+__global__ void __launch_bounds__(PAIR_BLOCK, MSG_PAIR_MINB) k_pair(
     const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, int ntasks,
     const typename PR::V4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
     const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
@@ -177,11 +183,13 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 2) k_pair(
             const int g = lane & (G - 1);
             const int i = W.i0 + lane / G;
             const bool act = i < W.i1;
-            double fx = 0.0, fy = 0.0, fz = 0.0;
-            double ut[NT];                                   // energy by partner type
-            double vi = 0.0;
+            // lane partial sums in R: a lane adds only a few pair terms before the
+            // particle's sums are rounded to 64-bit fixed point
+            R fx = 0, fy = 0, fz = 0;
+            R ut[NT];                                        // energy by partner type
+            R vi = 0;
 #pragma unroll
-            for (int t = 0; t < NT; ++t) ut[t] = 0.0;
+            for (int t = 0; t < NT; ++t) ut[t] = 0;
             int ti = 0, n = 0;
             V4 xi;
             const int *row = nbl;
@@ -230,8 +238,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 2) k_pair(
                     const PairTab &P = sP[pi[u]];
                     const float r2f = (float)r2[u];
                     int k = 0;
-                    if (r2f < (float)P.z_hi) {
-                        int bk = (int)((r2f - (float)P.z_lo) * (float)P.inv_h);
+                    if (r2f < P.fz_hi) {
+                        int bk = (int)((r2f - P.fz_lo) * P.finv_h);
                         bk = bk < 0 ? 0 : (bk >= MSG_NBUCKET ? MSG_NBUCKET - 1 : bk);
                         k = Tb[P.b0 - bbase + bk];
                     }
@@ -276,28 +284,28 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 2) k_pair(
                 for (int u = 0; u < B; ++u) {
                     if (!ok[u]) continue;
                     const int j = ee[u] & NBL_JMASK;
-                    fx += (double)(fsum[u] * dx[u]);
-                    fy += (double)(fsum[u] * dy[u]);
-                    fz += (double)(fsum[u] * dz[u]);
+                    fx += fsum[u] * dx[u];
+                    fy += fsum[u] * dy[u];
+                    fz += fsum[u] * dz[u];
                     if (i < j) {
 #pragma unroll
-                        for (int t = 0; t < NT; ++t) ut[t] += (tj[u] == t) ? (double)usum[u] : 0.0;
-                        vi -= (double)fsum[u] * (double)r2[u];
+                        for (int t = 0; t < NT; ++t) ut[t] += (tj[u] == t) ? usum[u] : (R)0;
+                        vi -= fsum[u] * r2[u];
                     }
                 }
             }
 #pragma unroll
             for (int t = 0; t < NT; ++t) {
-                const long long v = __double2ll_rn(ut[t] * kEFix);
+                const long long v = __double2ll_rn((double)ut[t] * kEFix);
 #pragma unroll
                 for (int q = 0; q < NT; ++q) ue[q * NT + t] += (q == ti) ? v : 0;
             }
-            vir += __double2ll_rn(vi * kEFix);
+            vir += __double2ll_rn((double)vi * kEFix);
             // reduce the particle's force over its G lanes; in FP32 mode each lane's FP64
             // partial is rounded to 64-bit fixed point first, so the combination is exact
             if constexpr (PR::mixed) {
-                long long ax = __double2ll_rn(fx * kFixScale), ay = __double2ll_rn(fy * kFixScale),
-                          az = __double2ll_rn(fz * kFixScale);
+                long long ax = __double2ll_rn((double)fx * kFixScale), ay = __double2ll_rn((double)fy * kFixScale),
+                          az = __double2ll_rn((double)fz * kFixScale);
                 for (int o = G >> 1; o > 0; o >>= 1) {
                     ax += __shfl_xor_sync(0xffffffffu, ax, o);
                     ay += __shfl_xor_sync(0xffffffffu, ay, o);
@@ -311,7 +319,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, 2) k_pair(
                     fy += __shfl_xor_sync(0xffffffffu, fy, o);
                     fz += __shfl_xor_sync(0xffffffffu, fz, o);
                 }
-                if (act && g == 0) fsr[i] = make_double4(fx, fy, fz, 0.0);
+                if (act && g == 0) fsr[i] = make_double4((double)fx, (double)fy, (double)fz, 0.0);
             }
         }
         // the run's energies: per warp, integer sums into the system's accumulators
