@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--replicas", type=int, default=16,
                     help="replicas of the workload in one handle for the batched figure (0: skip)")
+    ap.add_argument("--serve-jobs", type=int, default=200,
+                    help="jobs in the serving stream (Poisson arrivals at 200/s; 0: skip)")
+    ap.add_argument("--serve-budget-gib", type=float, default=4.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -181,6 +184,46 @@ def read_profile_traffic():
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
+
+
+def run_serving(a):
+    """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
+    half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
+    admitted by device-memory budget into concurrent cohorts.  Beside it: a sample of
+    the same jobs run alone, one after another, on the plain FP64 path."""
+    import torch
+
+    from molsim_b200 import Engine
+    from molsim_b200.serve import Server, poisson_stream
+
+    jobs = poisson_stream(seed=11, rate=200.0, njobs=a.serve_jobs, nmin=100, nmax=20000, nsteps=1000)
+    # load the library and fill the cuFFT plan cache outside the measured stream
+    warm = poisson_stream(seed=12, rate=1e6, njobs=4, nmin=100, nmax=400, nsteps=20)
+    Server(1 << 30, precision="mixed", chunk=10).run(warm, realtime=False)
+    srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50)
+    torch.cuda.synchronize()
+    m = srv.run(jobs)
+    # the plain FP64 path, each job alone: a sample across sizes, 200 steps each
+    smp = sorted(jobs, key=lambda j: j.n)[:: max(1, len(jobs) // 12)][:12]
+    work = tsum = 0.0
+    ks = 200
+    for j in smp:
+        e = Engine(j.system, j.table, precision="fp64")
+        e.UTotal()
+        e.GetLinAcc()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.VelVer(ks, energies=False)
+        torch.cuda.synchronize()
+        tsum += (time.perf_counter() - t0) * j.nsteps / ks
+        work += j.n * j.nsteps
+        del e
+    alone = work / tsum if tsum else None
+    m.update({"unit": METRIC, "jobs_per_s_offered": 200.0, "nsteps_per_job": 1000,
+              "precision": "mixed", "fp64_alone_value": alone,
+              "fp64_alone_sample": "%d jobs across the size range, %d steps each, scaled to 1000" % (len(smp), ks),
+              "vs_fp64_alone": (m["value"] / alone) if alone else None})
+    return m
 
 
 def run_gpu(a):
@@ -353,6 +396,10 @@ def run_gpu(a):
                "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
                          "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
 
+    serving = None
+    if rank == 0 and world == 1 and a.serve_jobs > 0:
+        serving = run_serving(a)
+
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank != 0:
@@ -366,7 +413,7 @@ def run_gpu(a):
                        "integrator": "velocity Verlet", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "flushed (256 MB write) before every timed step",
                        "rebuilds_in_timed_steps": int(rebuilds)},
-            "fp64_value": fp64_value, "batched": batched,
+            "fp64_value": fp64_value, "batched": batched, "serving": serving,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

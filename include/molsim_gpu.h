@@ -151,6 +151,28 @@ int64_t msg_nrebuild(const msg_handle *h, int32_t isys);
 int  msg_put_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd,
                    int32_t keep_list);
 
+/* --- Serving support (no counterpart in the reference, which runs one system
+ * per process).  A serving loop keeps several handles resident, each on its
+ * own stream, and advances them concurrently.  Handles allocate and free
+ * device memory stream-ordered from the device's pool and take their cuFFT
+ * plans from a process-wide cache, so creating or destroying one does not
+ * wait for the others' work. */
+
+/* Device bytes a handle for these systems would allocate (a dry set-up that
+ * allocates nothing; cuFFT work areas by cufftEstimateMany). */
+int  msg_estimate_bytes(const msg_params *p, int32_t nsys, int32_t precision, int64_t *bytes);
+/* Device bytes the handle holds now (its buffers and cuFFT work area). */
+int64_t msg_device_bytes(const msg_handle *h);
+/* Number of msg_velver_async batches of this handle still running on the
+ * device (0: idle and the device error word is clean).  A negative value is
+ * minus a status code (a device error raised by the finished steps). */
+int  msg_pending(msg_handle *h);
+/* Energies of system isys after the last step enqueued (waits for the stream). */
+int  msg_get_energy(msg_handle *h, int32_t isys, msg_energy *e);
+/* Destroy idle cached cuFFT plans and return unused pool memory to the device
+ * (may wait for the device). */
+int  msg_trim_caches(void);
+
 /* Instrumentation: the handle's CUDA stream (cudaStream_t), kernel launches
  * issued so far, and per-kernel CUDA-event timers (enabled by msg_set_timing). */
 void   *msg_stream(const msg_handle *h);

@@ -61,6 +61,11 @@ SIGNATURES = {
     "msg_bd_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_uint64, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_nrebuild": (C.c_int64, [C.c_void_p, C.c_int32]),
     "msg_put_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p, C.c_int32]),
+    "msg_estimate_bytes": (C.c_int, [C.POINTER(MsgParams), C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
+    "msg_device_bytes": (C.c_int64, [C.c_void_p]),
+    "msg_pending": (C.c_int, [C.c_void_p]),
+    "msg_get_energy": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(MsgEnergy)]),
+    "msg_trim_caches": (C.c_int, []),
     "msg_stream": (C.c_void_p, [C.c_void_p]),
     "msg_launch_count": (C.c_int64, [C.c_void_p]),
     "msg_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),

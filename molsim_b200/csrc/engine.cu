@@ -12,6 +12,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -43,16 +45,6 @@ struct CudaError {
     } while (0)
 
 template <typename T>
-T *dalloc(size_t n)
-{
-    void *p = nullptr;
-    if (n == 0) n = 1;
-    CK(cudaMalloc(&p, n * sizeof(T)));
-    CK(cudaMemset(p, 0, n * sizeof(T)));
-    return static_cast<T *>(p);
-}
-
-template <typename T>
 void h2d(T *d, const T *h, size_t n, cudaStream_t st)
 {
     if (n) CK(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -67,10 +59,48 @@ enum { TM_POS, TM_PAIR, TM_SPREAD, TM_FFT, TM_INFL, TM_FINAL, TM_REBUILD, TM_N }
 const char *const kTimerNames[TM_N] = {"position_update_skin", "pair", "spread", "fft", "influence",
                                         "gather_finalize", "rebuild"};
 
+// cuFFT plans are cached process-wide by (edge, batch, type, direction) and
+// run on a work area that the owning handle allocates stream-ordered, so
+// creating or destroying a handle never frees device memory through cuFFT
+// (a free would wait for every stream of the device).  A grid class of
+// `count` systems runs as power-of-two sub-batches, which bounds the number
+// of distinct plans.
+struct PlanKey {
+    int s, count, f32, fwd;
+    bool operator<(const PlanKey &o) const
+    {
+        return s != o.s ? s < o.s : count != o.count ? count < o.count : f32 != o.f32 ? f32 < o.f32 : fwd < o.fwd;
+    }
+};
+std::mutex g_plan_mu;
+std::map<PlanKey, std::vector<std::pair<cufftHandle, size_t>>> g_plan_idle;
+
+cufftResult make_plan(const PlanKey &k, cufftHandle *out, size_t *ws)
+{
+    int dims[3] = {k.s, k.s, k.s};
+    const int rdist = k.s * k.s * k.s, cdist = k.s * k.s * (k.s / 2 + 1);
+    const cufftType t = k.fwd ? (k.f32 ? CUFFT_R2C : CUFFT_D2Z) : (k.f32 ? CUFFT_C2R : CUFFT_Z2D);
+    cufftResult r = cufftCreate(out);
+    if (r != CUFFT_SUCCESS) return r;
+    r = cufftSetAutoAllocation(*out, 0);
+    if (r == CUFFT_SUCCESS)
+        r = k.fwd ? cufftMakePlanMany(*out, 3, dims, nullptr, 1, rdist, nullptr, 1, cdist, t, k.count, ws)
+                  : cufftMakePlanMany(*out, 3, dims, nullptr, 1, cdist, nullptr, 1, rdist, t, k.count, ws);
+    if (r != CUFFT_SUCCESS) cufftDestroy(*out);
+    return r;
+}
+
+struct FftPart {
+    int count;
+    long long grid_off, cgrid_off;
+    cufftHandle fwd = 0, bwd = 0;
+    size_t ws_fwd = 0, ws_bwd = 0;
+};
+
 struct FftClass {
     int s, count;
     long long grid_off, cgrid_off;
-    cufftHandle fwd = 0, bwd = 0;
+    std::vector<FftPart> parts;
 };
 
 }  // namespace
@@ -150,6 +180,53 @@ struct msg_handle {
     cudaEvent_t open_ev[TM_N] = {};
     double tm_ms[TM_N] = {};
     long long tm_n[TM_N] = {};
+
+    // device memory: stream-ordered from the device's pool; a dry build only counts bytes
+    // systems whose positions were given: only these have lists to rebuild after a re-layout
+    std::vector<int> placed;
+    bool dry = false;
+    long long bytes_live = 0;
+    size_t alloc_log = 0;       // MSG_ALLOC_LOG=<bytes>: report allocations at least that large
+    std::unordered_map<void *, size_t> sizes;
+    void *fftwork = nullptr;
+    std::vector<cudaEvent_t> inflight;   // one event per asynchronous step batch
+    template <typename T>
+    T *dalloc(size_t n)
+    {
+        if (n == 0) n = 1;
+        const size_t b = ((n * sizeof(T) + 511) / 512) * 512;
+        bytes_live += (long long)b;
+        if (alloc_log && b >= alloc_log) std::fprintf(stderr, "msg alloc %zu bytes\n", b);
+        if (dry) return reinterpret_cast<T *>((uintptr_t)512);
+        void *p = nullptr;
+        CK(cudaMallocAsync(&p, b, st));
+        CK(cudaMemsetAsync(p, 0, b, st));
+        sizes[p] = b;
+        return static_cast<T *>(p);
+    }
+    void dfree(void *p)
+    {
+        if (!p || dry) return;
+        auto it = sizes.find(p);
+        if (it != sizes.end()) {
+            bytes_live -= (long long)it->second;
+            sizes.erase(it);
+        }
+        cudaFreeAsync(p, st);
+    }
+    void up(void *d, const void *hsrc, size_t bytes)
+    {
+        if (dry || !bytes) return;
+        CK(cudaMemcpyAsync(d, hsrc, bytes, cudaMemcpyHostToDevice, st));
+    }
+    void down(void *hdst, const void *d, size_t bytes)
+    {
+        if (!bytes) return;
+        CK(cudaMemcpyAsync(hdst, d, bytes, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    void plan_fft();
+    void release_fft();
 
     ~msg_handle();
     cudaEvent_t get_event()
@@ -237,13 +314,13 @@ static void free_all(msg_handle *h)
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys};
-    for (void *p : ptrs)
-        if (p) cudaFree(p);
-    for (auto &f : h->fft) {
-        if (f.fwd) cufftDestroy(f.fwd);
-        if (f.bwd) cufftDestroy(f.bwd);
+    if (!h->dry && h->st) {
+        for (void *p : ptrs) h->dfree(p);
+        h->dfree(h->fftwork);
     }
-    h->fft.clear();
+    h->release_fft();
+    for (cudaEvent_t e : h->inflight) cudaEventDestroy(e);
+    h->inflight.clear();
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->pend_a) cudaEventDestroy(e);
     for (cudaEvent_t e : h->pend_b) cudaEventDestroy(e);
@@ -261,7 +338,7 @@ msg_handle::~msg_handle()
 void msg_handle::ensure_stage(size_t n)
 {
     if (n <= stage_n) return;
-    if (stage) cudaFree(stage);
+    if (stage) dfree(stage);
     stage = dalloc<double>(n);
     stage_n = n;
 }
@@ -273,10 +350,13 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 {
     nsys = n;
     prec = precision;
-    CK(cudaGetDevice(&dev));
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (!dry) {
+        CK(cudaGetDevice(&dev));
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    }
     hs.resize(n);
     hn.resize(n);
+    placed.assign(n, 0);
     order = P[0].order;
     std::vector<HostSys> H(n);
     ntot = 0;
@@ -412,20 +492,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         mfac = dalloc<double>(fo_acc);
         emf = dalloc<double>(fo_acc);
         vmf = dalloc<double>(fo_acc);
-        CK(cudaMemcpy(mfac, hm.data(), fo_acc * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(emf, he.data(), fo_acc * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(vmf, hv.data(), fo_acc * sizeof(double), cudaMemcpyHostToDevice));
-        for (auto &fc : fft) {
-            int dims[3] = {fc.s, fc.s, fc.s};
-            const int rdist = fc.s * fc.s * fc.s, cdist = fc.s * fc.s * (fc.s / 2 + 1);
-            const bool f32 = prec == MSG_PREC_MIXED;
-            CKF(cufftPlanMany(&fc.fwd, 3, dims, nullptr, 1, rdist, nullptr, 1, cdist, f32 ? CUFFT_R2C : CUFFT_D2Z,
-                              fc.count));
-            CKF(cufftPlanMany(&fc.bwd, 3, dims, nullptr, 1, cdist, nullptr, 1, rdist, f32 ? CUFFT_C2R : CUFFT_Z2D,
-                              fc.count));
-            CKF(cufftSetStream(fc.fwd, st));
-            CKF(cufftSetStream(fc.bwd, st));
-        }
+        up(mfac, hm.data(), fo_acc * sizeof(double));
+        up(emf, he.data(), fo_acc * sizeof(double));
+        up(vmf, hv.data(), fo_acc * sizeof(double));
+        plan_fft();
         // influence work items
         std::vector<int4> it;
         for (int s = 0; s < n; ++s) {
@@ -438,7 +508,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         }
         ninfl = (int)it.size();
         infl = dalloc<int4>(ninfl);
-        CK(cudaMemcpy(infl, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        up(infl, it.data(), it.size() * sizeof(int4));
     }
 
     // --- pair tables: per type pair, intervals from MOLSIM's ubuf ---
@@ -519,22 +589,22 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     massp = dalloc<double>(type_tot);
     fac1 = dalloc<double>(type_tot);
     fac2 = dalloc<double>(type_tot);
-    CK(cudaMemcpy(ptab, pt.data(), pt.size() * sizeof(PairTab), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ptmap, pmap.data(), pmap.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(tz, vz.data(), vz.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(tc, vc.data(), vc.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(bst, vb.data(), vb.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    up(ptab, pt.data(), pt.size() * sizeof(PairTab));
+    up(ptmap, pmap.data(), pmap.size() * sizeof(int));
+    up(tz, vz.data(), vz.size() * sizeof(double));
+    up(tc, vc.data(), vc.size() * sizeof(double));
+    up(bst, vb.data(), vb.size() * sizeof(unsigned short));
     {
         std::vector<float> fz(vz.begin(), vz.end()), fc(vc.begin(), vc.end());
         tz32 = dalloc<float>(fz.size());
         tc32 = dalloc<float>(fc.size());
-        CK(cudaMemcpy(tz32, fz.data(), fz.size() * sizeof(float), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(tc32, fc.data(), fc.size() * sizeof(float), cudaMemcpyHostToDevice));
+        up(tz32, fz.data(), fz.size() * sizeof(float));
+        up(tc32, fc.data(), fc.size() * sizeof(float));
     }
-    CK(cudaMemcpy(massip, vmassip.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(massp, vmassp.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(fac1, vf1.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(fac2, vf2.data(), type_tot * sizeof(double), cudaMemcpyHostToDevice));
+    up(massip, vmassip.data(), type_tot * sizeof(double));
+    up(massp, vmassp.data(), type_tot * sizeof(double));
+    up(fac1, vf1.data(), type_tot * sizeof(double));
+    up(fac2, vf2.data(), type_tot * sizeof(double));
 
     // --- bonds: per-particle CSR in MOLSIM order (both ends) ---
     {
@@ -571,11 +641,11 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         bpw = dalloc<int>(pw.size());
         bk = dalloc<double>(kk.size());
         beq = dalloc<double>(eq.size());
-        CK(cudaMemcpy(bptr, deg.data(), (ntot + 1) * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(bpart, part.data(), part.size() * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(bpw, pw.data(), pw.size() * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(bk, kk.data(), kk.size() * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(beq, eq.data(), eq.size() * sizeof(double), cudaMemcpyHostToDevice));
+        up(bptr, deg.data(), (ntot + 1) * sizeof(int));
+        up(bpart, part.data(), part.size() * sizeof(int));
+        up(bpw, pw.data(), pw.size() * sizeof(int));
+        up(bk, kk.data(), kk.size() * sizeof(double));
+        up(beq, eq.data(), eq.size() * sizeof(double));
     }
 
     // --- work lists ---
@@ -603,9 +673,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         this->t128 = dalloc<Tile>(a128.size());
         ptask = dalloc<PairTask>(pt16.size());
         chunks = dalloc<int4>(ch.size());
-        CK(cudaMemcpy(this->t128, a128.data(), a128.size() * sizeof(Tile), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ptask, pt16.data(), pt16.size() * sizeof(PairTask), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(chunks, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        up(this->t128, a128.data(), a128.size() * sizeof(Tile));
+        up(ptask, pt16.data(), pt16.size() * sizeof(PairTask));
+        up(chunks, ch.data(), ch.size() * sizeof(int4));
     }
 
     // --- particles: MOLSIM order is the initial internal order ---
@@ -638,17 +708,17 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                 hsid[g] = s;
             }
         }
-        CK(cudaMemcpy(pos[0], hp.data(), ntot * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(typ[0], ht.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(orig[0], ho.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        up(pos[0], hp.data(), ntot * sizeof(double4));
+        up(typ[0], ht.data(), ntot * sizeof(int));
+        up(orig[0], ho.data(), ntot * sizeof(int));
         std::vector<int> idn(ntot);
         for (int i = 0; i < ntot; ++i) idn[i] = i;
-        CK(cudaMemcpy(inv, idn.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(sysid, hsid.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        up(inv, idn.data(), ntot * sizeof(int));
+        up(sysid, hsid.data(), ntot * sizeof(int));
         // until a system's first list build, its particles sit in its first cell
         std::vector<int> hc(ntot);
         for (int i = 0; i < ntot; ++i) hc[i] = hs[hsid[i]].cell_off;
-        CK(cudaMemcpy(cellid, hc.data(), ntot * sizeof(int), cudaMemcpyHostToDevice));
+        up(cellid, hc.data(), ntot * sizeof(int));
     }
     k0 = dalloc<uint32_t>(ntot);
     v0 = dalloc<uint32_t>(ntot);
@@ -674,8 +744,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     fdone = dalloc<unsigned>(n);
     errw = dalloc<ErrWord>(1);
     dsys = dalloc<SysDev>(n);
-    CK(cudaMemcpy(dsys, hs.data(), n * sizeof(SysDev), cudaMemcpyHostToDevice));
-    {
+    up(dsys, hs.data(), n * sizeof(SysDev));
+    if (!dry) {
         // persistent pair grid: as many blocks as fit the SMs at once
         int nsm = 0, per = 0;
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -692,7 +762,78 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 #undef MSG_PAIR_CFG
         pair_grid = std::max(1, std::min(nptask, nsm * std::max(1, per)));
     }
-    CK(cudaDeviceSynchronize());
+    if (!dry) CK(cudaStreamSynchronize(st));
+}
+
+// Split each grid class into power-of-two sub-batches and take their plans
+// from the cache; one work area (the largest any plan asks for) serves them
+// all, since a handle runs its transforms one after another on its stream.
+void msg_handle::plan_fft()
+{
+    const int f32 = prec == MSG_PREC_MIXED ? 1 : 0;
+    size_t need = 0;
+    for (auto &fc : fft) {
+        long long go = fc.grid_off, co = fc.cgrid_off;
+        const long long rs = (long long)fc.s * fc.s * fc.s, cs = (long long)fc.s * fc.s * (fc.s / 2 + 1);
+        for (int bit = 30; bit >= 0; --bit) {
+            const int c = 1 << bit;
+            if (!(fc.count & c)) continue;
+            FftPart part;
+            part.count = c;
+            part.grid_off = go;
+            part.cgrid_off = co;
+            go += rs * c;
+            co += cs * c;
+            for (int dir = 1; dir >= 0; --dir) {
+                const PlanKey key{fc.s, c, f32, dir};
+                cufftHandle hp = 0;
+                size_t ws = 0;
+                if (dry) {
+                    int dims[3] = {fc.s, fc.s, fc.s};
+                    const cufftType t = dir ? (f32 ? CUFFT_R2C : CUFFT_D2Z) : (f32 ? CUFFT_C2R : CUFFT_Z2D);
+                    // without a device cuFFT cannot estimate: assume one complex grid per transform
+                    if (cufftEstimateMany(3, dims, nullptr, 1, dir ? (int)rs : (int)cs, nullptr, 1,
+                                          dir ? (int)cs : (int)rs, t, c, &ws) != CUFFT_SUCCESS)
+                        ws = (size_t)c * (size_t)cs * (f32 ? sizeof(float2) : sizeof(double2));
+                } else {
+                    {
+                        std::lock_guard<std::mutex> lk(g_plan_mu);
+                        auto &v = g_plan_idle[key];
+                        if (!v.empty()) {
+                            hp = v.back().first;
+                            ws = v.back().second;
+                            v.pop_back();
+                        }
+                    }
+                    if (!hp) CKF(make_plan(key, &hp, &ws));
+                }
+                (dir ? part.fwd : part.bwd) = hp;
+                (dir ? part.ws_fwd : part.ws_bwd) = ws;
+                need = std::max(need, ws);
+            }
+            fc.parts.push_back(part);
+        }
+    }
+    fftwork = dalloc<unsigned char>(std::max<size_t>(need, 1));
+    if (dry) return;
+    for (auto &fc : fft)
+        for (auto &pt : fc.parts)
+            for (cufftHandle hp : {pt.fwd, pt.bwd}) {
+                CKF(cufftSetWorkArea(hp, fftwork));
+                CKF(cufftSetStream(hp, st));
+            }
+}
+
+void msg_handle::release_fft()
+{
+    const int f32 = prec == MSG_PREC_MIXED ? 1 : 0;
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    for (auto &fc : fft)
+        for (auto &pt : fc.parts) {
+            if (pt.fwd) g_plan_idle[PlanKey{fc.s, pt.count, f32, 1}].push_back({pt.fwd, pt.ws_fwd});
+            if (pt.bwd) g_plan_idle[PlanKey{fc.s, pt.count, f32, 0}].push_back({pt.bwd, pt.ws_bwd});
+        }
+    fft.clear();
 }
 
 // ---------------------------------------------------------------------------
@@ -733,13 +874,15 @@ static void launch_spme(msg_handle *h)
     }
     h->tend(TM_SPREAD);
     h->tbeg(TM_FFT);
-    for (auto &f : h->fft) {
-        if (PR::mixed)
-            CKF(cufftExecR2C(f.fwd, h->rgrid32 + f.grid_off, reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off)));
-        else
-            CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off,
-                             reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
-    }
+    for (auto &fc : h->fft)
+        for (auto &f : fc.parts) {
+            if (PR::mixed)
+                CKF(cufftExecR2C(f.fwd, h->rgrid32 + f.grid_off,
+                                 reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off)));
+            else
+                CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off,
+                                 reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
+        }
     h->tend(TM_FFT);
     h->tbeg(TM_INFL);
     k_influence<PR><<<h->ninfl, INFL_THREADS, 0, h->st>>>(h->dsys, h->infl, h->cgrid, h->cgrid32, h->mfac, h->emf,
@@ -747,13 +890,15 @@ static void launch_spme(msg_handle *h)
     h->launches += 1;
     h->tend(TM_INFL);
     h->tbeg(TM_FFT);
-    for (auto &f : h->fft) {
-        if (PR::mixed)
-            CKF(cufftExecC2R(f.bwd, reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off), h->rgrid32 + f.grid_off));
-        else
-            CKF(cufftExecZ2D(f.bwd, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off),
-                             h->rgrid + f.grid_off));
-    }
+    for (auto &fc : h->fft)
+        for (auto &f : fc.parts) {
+            if (PR::mixed)
+                CKF(cufftExecC2R(f.bwd, reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off),
+                                 h->rgrid32 + f.grid_off));
+            else
+                CKF(cufftExecZ2D(f.bwd, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off),
+                                 h->rgrid + f.grid_off));
+        }
     h->tend(TM_FFT);
 }
 
@@ -846,13 +991,16 @@ void msg_handle::enqueue_bd_step(uint64_t seed, const double *xin_step, double *
 bool msg_handle::grow_lists()
 {
     std::vector<int> mx(nsys);
-    CK(cudaMemcpy(mx.data(), nmaxrow, nsys * sizeof(int), cudaMemcpyDeviceToHost));
+    down(mx.data(), nmaxrow, nsys * sizeof(int));
     bool grow = false;
     std::vector<int> cap(nsys);
     for (int s = 0; s < nsys; ++s) {
         int need = (int)std::ceil(1.5 * mx[s]) + 32;
         need = std::min(((need + 7) / 8) * 8, std::max(8, ((hs[s].n + 7) / 8) * 8));
         cap[s] = hs[s].cap;
+        if (alloc_log && need > hs[s].cap)
+            std::fprintf(stderr, "msg grow system %d: n %d longest row %d cap %d -> %d\n", s, hs[s].n, mx[s],
+                         hs[s].cap, need);
         if (need > hs[s].cap) {
             cap[s] = need;
             grow = true;
@@ -867,10 +1015,10 @@ bool msg_handle::grow_lists()
         acc += (long long)cap[s] * hs[s].n;
     }
     CK(cudaStreamSynchronize(st));
-    CK(cudaFree(nbl));
+    dfree(nbl);
     nbl = dalloc<int>(acc);
     nbl_tot = acc;
-    CK(cudaMemcpy(dsys, hs.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice));
+    up(dsys, hs.data(), nsys * sizeof(SysDev));
     return true;
 }
 
@@ -883,7 +1031,7 @@ int msg_handle::rebuild_checked(const std::vector<int> &flags)
     for (int attempt = 0; attempt < 3; ++attempt) {
         if (rc != MSG_OK && rc != MSG_ERR_CAPACITY) return rc;
         if (!grow_lists()) return rc;
-        std::vector<int> all(nsys, 1);
+        std::vector<int> all(placed.begin(), placed.end());
         h2d(flag, all.data(), nsys, st);
         enqueue_rebuild();
         rc = check();
@@ -998,7 +1146,7 @@ int msg_handle::check()
     CK(cudaGetLastError());
     flush_timers();
     ErrWord e;
-    CK(cudaMemcpy(&e, errw, sizeof(e), cudaMemcpyDeviceToHost));
+    down(&e, errw, sizeof(e));
     if (e.code) {
         static const char *names[] = {"ok", "r2 < r2umin (pair below the table minimum)", "table interval overrun",
                                       "neighbour-list capacity exceeded", "cuda", "device timeout", "argument",
@@ -1008,12 +1156,13 @@ int msg_handle::check()
                       (e.code >= 0 && e.code <= 8) ? names[e.code] : "error", e.sys, e.i, e.j);
         err = buf;
         const int code = e.code;
-        CK(cudaMemset(errw, 0, sizeof(ErrWord)));
+        CK(cudaMemsetAsync(errw, 0, sizeof(ErrWord), st));
         // an aborted step may leave partial sums and counters behind
-        CK(cudaMemset(eacc, 0, sizeof(long long) * nsys * EA_N));
-        CK(cudaMemset(fdone, 0, sizeof(unsigned) * nsys));
-        CK(cudaMemset(sysdone, 0, sizeof(unsigned) * nsys));
-        CK(cudaMemset(rdone, 0, sizeof(unsigned)));
+        CK(cudaMemsetAsync(eacc, 0, sizeof(long long) * nsys * EA_N, st));
+        CK(cudaMemsetAsync(fdone, 0, sizeof(unsigned) * nsys, st));
+        CK(cudaMemsetAsync(sysdone, 0, sizeof(unsigned) * nsys, st));
+        CK(cudaMemsetAsync(rdone, 0, sizeof(unsigned), st));
+        CK(cudaStreamSynchronize(st));
         return code;
     }
     return MSG_OK;
@@ -1030,17 +1179,34 @@ int msg_handle::check()
         return e.code;                                \
     }
 
+// The device's default memory pool keeps freed blocks for reuse instead of
+// returning them at every synchronisation (a process-local attribute).
+static void keep_pool_blocks()
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    });
+}
+
 static int create_impl(const msg_params *p, int32_t nsys, int32_t precision, msg_handle **out)
 {
     if (!p || !out || nsys < 1 || (precision != MSG_PREC_FP64 && precision != MSG_PREC_MIXED)) return MSG_ERR_ARG;
+    keep_pool_blocks();
     msg_handle *h = new msg_handle();
+    if (const char *al = std::getenv("MSG_ALLOC_LOG")) h->alloc_log = (size_t)std::atoll(al);
     // MSG_NO_GRAPHS=1 launches every kernel directly instead of replaying a CUDA graph
     if (const char *ng = std::getenv("MSG_NO_GRAPHS")) h->use_graphs = !(ng[0] == '1');
     try {
         h->build(p, nsys, precision);
         // initial neighbour lists: every system is rebuilt from its set-up order
         std::vector<int> ones(nsys, 1);
-        CK(cudaMemcpy(h->flag, ones.data(), nsys * sizeof(int), cudaMemcpyHostToDevice));
+        h->up(h->flag, ones.data(), nsys * sizeof(int));
     } catch (const CudaError &e) {
         std::fprintf(stderr, "msg_create: %s\n", e.what.c_str());
         delete h;
@@ -1063,6 +1229,41 @@ extern "C" int msg_create_batch(const msg_params *p, int32_t nsys, int32_t preci
 
 extern "C" void msg_destroy(msg_handle *h) { delete h; }
 
+extern "C" int msg_estimate_bytes(const msg_params *p, int32_t nsys, int32_t precision, int64_t *bytes)
+{
+    if (!p || !bytes || nsys < 1 || (precision != MSG_PREC_FP64 && precision != MSG_PREC_MIXED)) return MSG_ERR_ARG;
+    msg_handle *h = new msg_handle();
+    h->dry = true;
+    if (const char *al = std::getenv("MSG_ALLOC_LOG")) h->alloc_log = (size_t)std::atoll(al);
+    int rc = MSG_OK;
+    try {
+        h->build(p, nsys, precision);
+        *bytes = h->bytes_live;
+    } catch (const CudaError &e) {
+        if (h->alloc_log) std::fprintf(stderr, "msg_estimate_bytes: %s\n", e.what.c_str());
+        rc = e.code;
+    }
+    delete h;
+    return rc;
+}
+
+extern "C" int64_t msg_device_bytes(const msg_handle *h) { return h ? h->bytes_live : -1; }
+
+extern "C" int msg_trim_caches(void)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        for (auto &kv : g_plan_idle)
+            for (auto &pw : kv.second) cufftDestroy(pw.first);
+        g_plan_idle.clear();
+    }
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess)
+        return MSG_ERR_CUDA;
+    return cudaMemPoolTrimTo(pool, 0) == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
+}
+
 extern "C" const char *msg_last_error(const msg_handle *h) { return h ? h->err.c_str() : "null handle"; }
 
 extern "C" int32_t msg_nsys(const msg_handle *h) { return h ? h->nsys : 0; }
@@ -1084,6 +1285,7 @@ static int put_state(msg_handle *h, int32_t isys, const double *ro, const double
     if (ro) {
         k_mirror_range<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->posfx);
         h->launches += 1;
+        h->placed[isys] = 1;
     }
     if (ro && !keep_list) {
         // new positions: rebuild this system's list now (the rebuild resets drosum)
@@ -1142,25 +1344,25 @@ extern "C" int msg_build_nlist(msg_handle *h, int32_t isys, int32_t *nneighpn, i
     const SysDev &S = h->hs[isys];
     if (npair) {
         std::vector<int> nn(S.n);
-        CK(cudaMemcpy(nn.data(), h->nnb + S.off, S.n * sizeof(int), cudaMemcpyDeviceToHost));
+        h->down(nn.data(), h->nnb + S.off, S.n * sizeof(int));
         long long tot = 0;
         for (int v : nn) tot += v;
         *npair = tot / 2;
     }
     if (nneighpn && jpnlist) {
         if (maxnneigh < 1) return MSG_ERR_ARG;
-        int *dn = dalloc<int>(S.n);
-        int *dj = dalloc<int>((size_t)S.n * maxnneigh);
+        int *dn = h->dalloc<int>(S.n);
+        int *dj = h->dalloc<int>((size_t)S.n * maxnneigh);
         const int warps = 4;
         k_export_nlist<<<(S.n + warps - 1) / warps, 32 * warps, warps * S.cap * sizeof(int), h->st>>>(
             h->dsys, isys, h->nbl, h->nnb, h->orig[h->cur], dn, dj, maxnneigh, h->errw);
         rc = h->check();
         if (!rc) {
-            CK(cudaMemcpy(nneighpn, dn, S.n * sizeof(int), cudaMemcpyDeviceToHost));
-            CK(cudaMemcpy(jpnlist, dj, (size_t)S.n * maxnneigh * sizeof(int), cudaMemcpyDeviceToHost));
+            h->down(nneighpn, dn, S.n * sizeof(int));
+            h->down(jpnlist, dj, (size_t)S.n * maxnneigh * sizeof(int));
         }
-        cudaFree(dn);
-        cudaFree(dj);
+        h->dfree(dn);
+        h->dfree(dj);
         return rc;
     }
     return MSG_OK;
@@ -1220,8 +1422,8 @@ extern "C" int msg_get_linacc(msg_handle *h)
 static void prepare_hist(msg_handle *h, int nsteps)
 {
     if (nsteps > h->hist_cap) {
-        if (h->hist) cudaFree(h->hist);
-        h->hist = dalloc<double>((size_t)nsteps * h->nsys * ESZ);
+        if (h->hist) h->dfree(h->hist);
+        h->hist = h->dalloc<double>((size_t)nsteps * h->nsys * ESZ);
         h->hist_cap = nsteps;
     }
     CK(cudaMemsetAsync(h->stepctr, 0, sizeof(unsigned long long), h->st));
@@ -1251,7 +1453,7 @@ extern "C" int msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energ
     if (rc) return rc;
     if (rec) copy_hist(h, nsteps, isys, e);
     if (h->grow_lists()) {
-        std::vector<int> all(h->nsys, 1);
+        std::vector<int> all(h->placed.begin(), h->placed.end());
         return h->rebuild_checked(all);
     }
     return MSG_OK;
@@ -1269,8 +1471,47 @@ extern "C" int msg_velver_async(msg_handle *h, int32_t nsteps)
     } else {
         for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(false);
     }
+    cudaEvent_t ev = h->get_event();
+    CK(cudaEventRecord(ev, h->st));
+    h->inflight.push_back(ev);
     CK(cudaGetLastError());
     return MSG_OK;
+    API_END
+}
+
+extern "C" int msg_pending(msg_handle *h)
+{
+    if (!h) return -MSG_ERR_ARG;
+    try {
+        size_t done = 0;
+        while (done < h->inflight.size()) {
+            const cudaError_t q = cudaEventQuery(h->inflight[done]);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) {
+                h->err = std::string("msg_pending: ") + cudaGetErrorString(q);
+                return -MSG_ERR_CUDA;
+            }
+            h->evpool.push_back(h->inflight[done]);
+            ++done;
+        }
+        h->inflight.erase(h->inflight.begin(), h->inflight.begin() + done);
+        if (!h->inflight.empty()) return (int)h->inflight.size();
+        const int rc = h->check();
+        return rc ? -rc : 0;
+    } catch (const CudaError &e) {
+        h->err = e.what;
+        return -e.code;
+    }
+}
+
+extern "C" int msg_get_energy(msg_handle *h, int32_t isys, msg_energy *e)
+{
+    if (!h || !e || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    double he[ESZ];
+    h->down(he, h->esys + (size_t)isys * ESZ, sizeof(he));
+    fill_energy(he, h->hs[isys].natat, e);
+    return h->check();
     API_END
 }
 
@@ -1287,9 +1528,9 @@ extern "C" int msg_bd_step(msg_handle *h, int32_t nsteps, uint64_t seed, int32_t
     if (rec) prepare_hist(h, nsteps);
     const size_t per = 3 * (size_t)h->ntot;
     if ((xi || xi_out) && per * std::max(1, nsteps) > h->xin_n) {
-        if (h->xin) cudaFree(h->xin);
+        if (h->xin) h->dfree(h->xin);
         h->xin_n = per * std::max(1, nsteps);
-        h->xin = dalloc<double>(h->xin_n);
+        h->xin = h->dalloc<double>(h->xin_n);
     }
     const SysDev &S = h->hs[std::max(0, isys)];
     if (xi) {
@@ -1308,7 +1549,7 @@ extern "C" int msg_bd_step(msg_handle *h, int32_t nsteps, uint64_t seed, int32_t
     if (xi_out) {
         std::vector<double> buf(per);
         for (int k = 0; k < nsteps; ++k) {
-            CK(cudaMemcpy(buf.data(), h->xin + k * per, per * sizeof(double), cudaMemcpyDeviceToHost));
+            h->down(buf.data(), h->xin + k * per, per * sizeof(double));
             std::memcpy(xi_out + (size_t)k * 3 * S.n, buf.data() + 3 * (size_t)S.off, 3 * sizeof(double) * S.n);
         }
     }
@@ -1321,7 +1562,9 @@ extern "C" int64_t msg_nrebuild(const msg_handle *h, int32_t isys)
 {
     if (!h || isys < 0 || isys >= h->nsys) return -1;
     long long v = 0;
-    if (cudaMemcpy(&v, h->nrebuild + isys, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (cudaMemcpyAsync(&v, h->nrebuild + isys, sizeof(v), cudaMemcpyDeviceToHost, h->st) != cudaSuccess ||
+        cudaStreamSynchronize(h->st) != cudaSuccess)
+        return -1;
     return v;
 }
 

@@ -68,6 +68,28 @@ def prepare(sysd):
     return tab
 
 
+def params_array(systems, tables, maxnneigh=0):
+    """msg_params for the systems (and the arrays they point into, which must outlive the call)."""
+    keep = []
+    arr = (MsgParams * len(systems))()
+    for k, (s, t) in enumerate(zip(systems, tables)):
+        arr[k] = Engine._params_for(s, t, maxnneigh, keep)
+    return arr, keep
+
+
+def estimate_bytes(systems, tables, precision="mixed"):
+    """Device bytes a handle for these systems would hold (msg_estimate_bytes)."""
+    if isinstance(systems, dict):
+        systems, tables = [systems], [tables]
+    arr, _keep = params_array(systems, tables)
+    out = C.c_int64()
+    prec = _lib.MSG_PREC_MIXED if precision == "mixed" else _lib.MSG_PREC_FP64
+    rc = _lib.lib().msg_estimate_bytes(arr, len(systems), prec, C.byref(out))
+    if rc:
+        raise MolsimGpuError(rc, "msg_estimate_bytes")
+    return int(out.value)
+
+
 class Engine:
     """One library handle for `systems` (a list of system dicts, see systems.py) with their
     tables (`tables[k]` from `prepare` or from a caller such as the oracle)."""
@@ -99,6 +121,10 @@ class Engine:
             self.set_state(k, s["ro"], s.get("rod"), s.get("rodd"))
 
     def _params(self, s, t, maxnneigh):
+        return Engine._params_for(s, t, maxnneigh, self._keep)
+
+    @staticmethod
+    def _params_for(s, t, maxnneigh, keep):
         k = {}
         k["iptpn"] = np.ascontiguousarray(s["iptpn"], np.int32)
         k["az"] = np.ascontiguousarray(s["az"], np.float64)
@@ -115,7 +141,7 @@ class Engine:
         if fac is not None:
             k["fac1"] = np.ascontiguousarray(fac[0], np.float64)
             k["fac2"] = np.ascontiguousarray(fac[1], np.float64)
-        self._keep.append(k)
+        keep.append(k)
         null = C.POINTER(C.c_double)()
         return MsgParams(int(s["np"]), int(s["npt"]), (C.c_double * 3)(*s["boxlen"]), s["rcut"], s["drnlist"],
                          _p(k["iptpn"], C.c_int32), _p(k["az"], C.c_double), _p(k["masspt"], C.c_double),
@@ -206,6 +232,26 @@ class Engine:
         arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (ro, rod, rodd)]
         ptrs = [None if a is None else _p(a, C.c_double) for a in arrs]
         self._check(_lib.lib().msg_put_state(self.h, isys, *ptrs, 1 if keep_list else 0))
+
+    # --- serving support -----------------------------------------------------
+    def velver_async(self, nsteps):
+        """Enqueue nsteps MD steps of every system and return at once."""
+        self._check(_lib.lib().msg_velver_async(self.h, nsteps))
+
+    def pending(self):
+        """Asynchronous step batches still on the device; raises on a device error."""
+        r = _lib.lib().msg_pending(self.h)
+        if r < 0:
+            raise MolsimGpuError(-r, _lib.lib().msg_last_error(self.h).decode())
+        return r
+
+    def energy(self, isys=0):
+        e = MsgEnergy()
+        self._check(_lib.lib().msg_get_energy(self.h, isys, C.byref(e)))
+        return e.as_dict(self.natat[isys])
+
+    def device_bytes(self):
+        return int(_lib.lib().msg_device_bytes(self.h))
 
     # --- instrumentation ---------------------------------------------------
     def stream(self):

@@ -137,6 +137,8 @@ def polyelectrolyte(seed=0, nchain=40, nbead=200, L=250.0, temp=298.0, relp=78.4
             ok = True
             prev = np.array(beads) if beads else None
             tree = cKDTree(np.mod(prev + L / 2, L), boxsize=L) if prev is not None else None
+            if tree is not None and tree.query(np.mod(chain[0] + L / 2, L))[0] < mind:
+                continue                 # the chain's first bead overlaps an earlier chain
             while len(chain) < nbead and ok:
                 for _t in range(200):
                     v = rng.standard_normal(3)
@@ -243,13 +245,13 @@ def batched_ensemble(seed=0, nsys=512, nmin=200, nmax=4000):
     return out
 
 
-def scaled_job(rng, n, kind):
+def scaled_job(rng, n, kind, order=4):
     """A serving job: the electrolyte generator at its density, or the polyelectrolyte
     generator at its density with chains of up to 200 beads, scaled to N particles."""
     if kind == "electrolyte":
         L = 100.0 * (n / 1000.0) ** (1.0 / 3.0)
         s = electrolyte(seed=int(rng.integers(1 << 30)), n_pairs=n // 2, L=L,
-                        rcut=min(30.0, L / 2 - 2.0), nmesh=_grid_for(L), order=4)
+                        rcut=min(30.0, L / 2 - 2.0), nmesh=_grid_for(L), order=order)
     else:
         nb = n // 2
         nbead = min(200, max(2, nb))
@@ -257,7 +259,7 @@ def scaled_job(rng, n, kind):
         nb = nchain * nbead
         L = 250.0 * (2 * nb / 16000.0) ** (1.0 / 3.0)
         s = polyelectrolyte(seed=int(rng.integers(1 << 30)), nchain=nchain, nbead=nbead, L=L,
-                            rcut=min(25.0, L / 2 - 2.0), nmesh=_grid_for(L), order=4)
+                            rcut=min(25.0, L / 2 - 2.0), nmesh=_grid_for(L), order=order)
     return s
 
 
