@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--replicas", type=int, default=16,
                     help="replicas of the workload in one handle for the batched figure (0: skip)")
+    ap.add_argument("--ensemble", type=int, default=512,
+                    help="systems in the batched ensemble (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=200,
                     help="jobs in the serving stream (Poisson arrivals at 200/s; 0: skip)")
     ap.add_argument("--serve-budget-gib", type=float, default=4.0)
@@ -186,6 +188,81 @@ def read_profile_traffic():
     return float(m.group(1)) if m else None
 
 
+def timed_md_steps(e, K, flush, warmup):
+    """K MD steps of every system of engine e, L2 flushed before each; device time
+    summed over the steps (ms), CUDA events on the engine's stream."""
+    import torch
+
+    from molsim_b200 import _lib
+
+    Lx = _lib.lib()
+    extx = torch.cuda.ExternalStream(e.stream())
+    for _ in range(max(3, warmup)):
+        with torch.cuda.stream(extx):
+            flush.zero_()
+        if Lx.msg_velver_async(e.h, 1):
+            raise RuntimeError(Lx.msg_last_error(e.h).decode())
+    e.VelVer(1, energies=False)
+    torch.cuda.synchronize()
+    st = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    en = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    for k in range(K):
+        with torch.cuda.stream(extx):
+            flush.zero_()
+            st[k].record(extx)
+        if Lx.msg_velver_async(e.h, 1):
+            raise RuntimeError(Lx.msg_last_error(e.h).decode())
+        with torch.cuda.stream(extx):
+            en[k].record(extx)
+    torch.cuda.synchronize()
+    return sum(x.elapsed_time(y) for x, y in zip(st, en))
+
+
+def run_ensemble(a, flush):
+    """The batched ensemble: electrolytes with N ~ U{200..4000}, rho*sigma^3 ~ U[0.01, 0.3],
+    T ~ U[250, 400] K, SPME order 4 with the grid edge of each system chosen by the
+    autotuner from {16, 24, 32, 48}; all systems in one handle, one CUDA-graph replay
+    per step.  Mixed precision, beside the same ensemble on the FP64 path."""
+    import torch
+
+    from molsim_b200 import Engine, prepare
+    from molsim_b200.autotune import apply_grids, tune_grids, tune_pair_lanes
+    from molsim_b200.systems import batched_ensemble
+
+    t0 = time.perf_counter()
+    systems = batched_ensemble(seed=0, nsys=a.ensemble)
+    tables = [prepare(s) for s in systems]
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    edges, rep = tune_grids(systems, tables)
+    t_tune = time.perf_counter() - t0
+    sy = apply_grids(systems, edges)
+    ntot = sum(int(s["np"]) for s in sy)
+    eng = Engine(sy, tables, precision="mixed")
+    eng.UTotal(0)
+    eng.GetLinAcc()
+    best, lane_ms = tune_pair_lanes(eng)
+    K = max(10, a.steps // 4)
+    ms = timed_md_steps(eng, K, flush, a.warmup)
+    value = ntot * K / (ms / 1000.0)
+    del eng
+    e64 = Engine(sy, tables, precision="fp64")
+    e64.UTotal(0)
+    e64.GetLinAcc()
+    ms64 = timed_md_steps(e64, K, flush, a.warmup)
+    del e64
+    torch.cuda.synchronize()
+    hist = {g: edges.count(g) for g in sorted(set(edges))}
+    return {"systems": len(sy), "particles": ntot, "value": value, "unit": METRIC, "steps": K,
+            "ms_per_step": ms / K, "precision": "mixed", "fp64_batched_value": ntot * K / (ms64 / 1000.0),
+            "vs_fp64_batched": ms64 / ms,
+            "autotune": {"grid_edges": hist, "target_met": int(sum(r["met"] for r in rep)),
+                         "rule": "cheapest edge with measured reciprocal RMS force error <= Kolafa-Perram "
+                                 "real-space estimate (reference 96^3 order 6)",
+                         "pair_lane_shift": best, "pair_lane_ms_per_step": lane_ms, "tune_s": t_tune},
+            "generate_s": t_gen}
+
+
 def run_serving(a):
     """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
     half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
@@ -257,28 +334,7 @@ def run_gpu(a):
             raise RuntimeError(L.msg_last_error(eng.h).decode())
 
     def timed_steps(e, K):
-        """K steps, L2 flushed before each, device time summed over the steps (ms)."""
-        Lx = _lib.lib()
-        extx = torch.cuda.ExternalStream(e.stream())
-        for _ in range(max(3, a.warmup)):
-            with torch.cuda.stream(extx):
-                flush.zero_()
-            if Lx.msg_velver_async(e.h, 1):
-                raise RuntimeError(Lx.msg_last_error(e.h).decode())
-        e.VelVer(1, energies=False)
-        torch.cuda.synchronize()
-        st = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-        en = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-        for k in range(K):
-            with torch.cuda.stream(extx):
-                flush.zero_()
-                st[k].record(extx)
-            if Lx.msg_velver_async(e.h, 1):
-                raise RuntimeError(Lx.msg_last_error(e.h).decode())
-            with torch.cuda.stream(extx):
-                en[k].record(extx)
-        torch.cuda.synchronize()
-        return sum(x.elapsed_time(y) for x, y in zip(st, en))
+        return timed_md_steps(e, K, flush, a.warmup)
 
     # warm-up (also captures the step graph)
     for _ in range(max(3, a.warmup)):
@@ -396,7 +452,9 @@ def run_gpu(a):
                "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
                          "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
 
-    serving = None
+    ensemble = serving = None
+    if rank == 0 and world == 1 and a.ensemble > 0:
+        ensemble = run_ensemble(a, flush)
     if rank == 0 and world == 1 and a.serve_jobs > 0:
         serving = run_serving(a)
 
@@ -413,7 +471,7 @@ def run_gpu(a):
                        "integrator": "velocity Verlet", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "flushed (256 MB write) before every timed step",
                        "rebuilds_in_timed_steps": int(rebuilds)},
-            "fp64_value": fp64_value, "batched": batched, "serving": serving,
+            "fp64_value": fp64_value, "batched": batched, "ensemble": ensemble, "serving": serving,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

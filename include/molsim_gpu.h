@@ -123,6 +123,18 @@ int  msg_build_nlist(msg_handle *h, int32_t isys, int32_t *nneighpn, int32_t *jp
  * forceo (internal units), energies.  NULL outputs are skipped. */
 int  msg_utotal(msg_handle *h, int32_t isys, double *force, double *forceo, msg_energy *e);
 
+/* The forces of system isys from the last force evaluation of the handle
+ * (msg_utotal or a step), without recomputing them.  NULL outputs are skipped. */
+int  msg_get_forces(msg_handle *h, int32_t isys, double *force, double *forceo);
+
+/* Tuning knobs (no counterpart in the reference).  MSG_TUNE_PAIR_LANES: lanes
+ * per particle in the pair kernel scaled by 2^value (-4..4) from the default
+ * chosen by the expected row length.  FP64 results move by FP64 rounding only;
+ * mixed results by FP32 rounding (a lane's partial sum is regrouped), and stay
+ * deterministic for each setting. */
+#define MSG_TUNE_PAIR_LANES 1
+int  msg_tune(msg_handle *h, int32_t key, int32_t value);
+
 /* rodd = massip * forceo (GetLinAcc) from the last msg_utotal. */
 int  msg_get_linacc(msg_handle *h);
 

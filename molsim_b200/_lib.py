@@ -12,6 +12,7 @@ f64p = C.POINTER(C.c_double)
 MSG_OK = 0
 MSG_PREC_FP64 = 0
 MSG_PREC_MIXED = 1
+MSG_TUNE_PAIR_LANES = 1
 STATUS = {0: "ok", 1: "r2 < r2umin", 2: "table interval overrun", 3: "neighbour capacity exceeded",
           4: "CUDA error", 5: "device timeout", 6: "invalid argument", 7: "non-finite force",
           8: "hard-core overlap"}
@@ -56,6 +57,8 @@ SIGNATURES = {
     "msg_build_nlist": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(C.c_int64)]),
     "msg_utotal": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_get_linacc": (C.c_int, [C.c_void_p]),
+    "msg_get_forces": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p]),
+    "msg_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "msg_velver": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MsgEnergy)]),
     "msg_velver_async": (C.c_int, [C.c_void_p, C.c_int32]),
     "msg_bd_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_uint64, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),

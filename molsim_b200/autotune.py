@@ -1,0 +1,112 @@
+"""Autotuner for batched ensembles: SPME grid per system and pair-kernel lanes.
+
+SPME grid (per system).  MOLSIM takes the grid edge from the input
+(nmesh, Src/energy.F90:6855-7019) and alpha from the real-space tolerance
+(RcutToAlpha, Src/energy.F90:7090-7105).  For an ensemble of systems of
+different sizes and densities the edge is chosen here instead: for each system,
+the cheapest edge among the candidates whose reciprocal-space force error does
+not exceed the real-space truncation error at the system's alpha and cutoff.
+
+* The reciprocal-space error is MEASURED: forces of every system with each
+  candidate edge (FP64 path, same alpha and table) against a reference solve
+  on a fine grid at spline order 6.  Real-space, self and bonded terms are the
+  same in both, so the difference is the reciprocal-space error alone.
+* The real-space error is the Kolafa-Perram estimate (J. Kolafa, J. W. Perram,
+  Mol. Simul. 9 (1992) 351): for random charges the RMS force error of
+  truncating erfc(alpha r)/r at rc is
+      dF = 2 sqrt(<q^2>) sqrt(sum_j q_j^2 / (rc V)) exp(-alpha^2 rc^2) * EpsiFourPi
+  (kJ/(mol A)), from integrating the squared large-r erfc force over the
+  particles beyond rc.
+* A system no candidate satisfies gets the largest candidate.
+
+Pair lanes (per handle).  The pair kernel gives each particle G lanes, G set
+from the expected row length; the tuner times a few steps for G scaled by
+2^shift and keeps the fastest.  In FP64 the results do not depend on G beyond
+FP64 rounding; in mixed precision a lane adds its few pair terms in FP32
+before rounding them to fixed point, so G moves results by FP32 rounding
+(relative 1e-7 level) while each setting stays deterministic and independent
+of which other systems share the handle.  Timing advances the systems by
+len(shifts) * (steps + 2) MD steps.
+"""
+import time
+
+import numpy as np
+
+CANDIDATES = (16, 24, 32, 48)
+
+
+def kolafa_perram_force_error(system, alpha):
+    q = np.asarray(system["az"], np.float64)
+    vol = float(np.prod(system["boxlen"]))
+    rc = float(system["rcut"])
+    return 2.0 * np.sqrt(np.mean(q * q)) * np.sqrt(np.sum(q * q) / (rc * vol)) * \
+        np.exp(-(alpha * rc) ** 2) * float(system["epsi_four_pi"])
+
+
+def _forces(systems, tables, nmesh, order, chunk):
+    """FP64 forces of every system with the given grid edge(s) and order."""
+    from .engine import Engine
+
+    out = []
+    for a in range(0, len(systems), chunk):
+        sub = []
+        for k in range(a, min(len(systems), a + chunk)):
+            d = dict(systems[k])
+            d["nmesh"] = int(nmesh[k] if np.ndim(nmesh) else nmesh)
+            d["order"] = int(order)
+            sub.append(d)
+        e = Engine(sub, tables[a:a + len(sub)], precision="fp64")
+        e.UTotal(0)
+        out.extend(e.forces(k)[0] for k in range(len(sub)))
+        del e
+    return out
+
+
+def tune_grids(systems, tables, candidates=CANDIDATES, order=4, ref_mesh=None, ref_order=6, chunk=128):
+    """Grid edge per system.  Returns (edges, report) where report[k] holds the
+    measured RMS reciprocal error per candidate and the real-space target."""
+    cands = sorted(candidates)
+    if ref_mesh is None:
+        ref_mesh = 2 * cands[-1]
+    ref = _forces(systems, tables, ref_mesh, ref_order, chunk)
+    err = {c: [] for c in cands}
+    for c in cands:
+        fc = _forces(systems, tables, c, order, chunk)
+        for k in range(len(systems)):
+            err[c].append(float(np.sqrt(np.mean(np.sum((fc[k] - ref[k]) ** 2, axis=1)))))
+    edges, report = [], []
+    for k, s in enumerate(systems):
+        target = kolafa_perram_force_error(s, tables[k]["ualpha"])
+        pick = next((c for c in cands if err[c][k] <= target), cands[-1])
+        edges.append(pick)
+        report.append(dict(target=target, met=err[pick][k] <= target, err={c: err[c][k] for c in cands}))
+    return edges, report
+
+
+def apply_grids(systems, edges, order=4):
+    out = []
+    for s, g in zip(systems, edges):
+        d = dict(s)
+        d["nmesh"] = int(g)
+        d["order"] = int(order)
+        out.append(d)
+    return out
+
+
+def tune_pair_lanes(engine, shifts=(-1, 0, 1), steps=10):
+    """Time `steps` MD steps per lane scaling; leave the engine on the fastest.
+    Returns (best shift, {shift: ms per step})."""
+    import torch
+
+    times = {}
+    for sh in shifts:
+        engine.tune_pair_lanes(sh)
+        engine.VelVer(2, energies=False)           # capture the graph for this layout
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        engine.VelVer(steps, energies=False)
+        torch.cuda.synchronize()
+        times[sh] = 1000.0 * (time.perf_counter() - t0) / steps
+    best = min(times, key=times.get)
+    engine.tune_pair_lanes(best)
+    return best, times

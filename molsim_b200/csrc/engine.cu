@@ -227,6 +227,9 @@ struct msg_handle {
     }
     void plan_fft();
     void release_fft();
+    int pair_blocks_max = 1, pair_shift = 0;
+    std::vector<PairTask> make_pair_tasks(int shift) const;
+    void set_pair_lanes(int shift);
 
     ~msg_handle();
     cudaEvent_t get_event()
@@ -656,19 +659,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         for (int s = 0; s < n; ++s) {
             const SysDev &S = hs[s];
             for (int i = 0; i < S.n; i += 128) a128.push_back(Tile{s, S.off + i, S.off + std::min(S.n, i + 128), 0});
-            // lanes per particle: about four row entries per lane (expected full-list row)
-            const double rl = std::sqrt(S.rs2cut);
-            const double nrow = S.n / S.vol * 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl;
-            int G = 4;
-            while (G < 32 && 2 * G <= nrow / 4.0) G *= 2;
-            const int per = 32 / G;
-            const size_t first = pt16.size();
-            for (int i = 0; i < S.n; i += per)
-                pt16.push_back(PairTask{s, S.off + i, S.off + std::min(S.n, i + per), G, 0, 0, 0, 0});
-            for (size_t q = first; q < pt16.size(); ++q) pt16[q].send = (int)pt16.size();
             for (int i = 0; i < S.n; i += SK_CHUNK)
                 ch.push_back(make_int4(s, S.off + i, S.off + std::min(S.n, i + SK_CHUNK), 0));
         }
+        pt16 = make_pair_tasks(0);
         nptask = (int)pt16.size();
         this->t128 = dalloc<Tile>(a128.size());
         ptask = dalloc<PairTask>(pt16.size());
@@ -760,9 +754,48 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             if (max_npt <= 2) MSG_PAIR_CFG(PrecD, 2); else MSG_PAIR_CFG(PrecD, 4);
         }
 #undef MSG_PAIR_CFG
-        pair_grid = std::max(1, std::min(nptask, nsm * std::max(1, per)));
+        pair_blocks_max = nsm * std::max(1, per);
+        pair_grid = std::max(1, std::min(nptask, pair_blocks_max));
     }
     if (!dry) CK(cudaStreamSynchronize(st));
+}
+
+// Warp tasks of the pair kernel: 32/G consecutive particles of one system, G
+// lanes per particle.  G follows the expected full-list row (about four row
+// entries per lane), scaled by 2^shift (the pair-lane tuning knob), 2..32.
+std::vector<PairTask> msg_handle::make_pair_tasks(int shift) const
+{
+    std::vector<PairTask> pt;
+    for (int s = 0; s < nsys; ++s) {
+        const SysDev &S = hs[s];
+        const double rl = std::sqrt(S.rs2cut);
+        const double nrow = S.n / S.vol * 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl;
+        int G = 4;
+        while (G < 32 && 2 * G <= nrow / 4.0) G *= 2;
+        for (int k = 0; k < shift && G < 32; ++k) G *= 2;
+        for (int k = 0; k > shift && G > 2; --k) G /= 2;
+        const int per = 32 / G;
+        const size_t first = pt.size();
+        for (int i = 0; i < S.n; i += per)
+            pt.push_back(PairTask{s, S.off + i, S.off + std::min(S.n, i + per), G, 0, 0, 0, 0});
+        for (size_t q = first; q < pt.size(); ++q) pt[q].send = (int)pt.size();
+    }
+    return pt;
+}
+
+void msg_handle::set_pair_lanes(int shift)
+{
+    if (shift == pair_shift) return;
+    drop_graph();
+    CK(cudaStreamSynchronize(st));
+    std::vector<PairTask> pt = make_pair_tasks(shift);
+    dfree(ptask);
+    ptask = dalloc<PairTask>(pt.size());
+    up(ptask, pt.data(), pt.size() * sizeof(PairTask));
+    nptask = (int)pt.size();
+    pair_grid = std::max(1, std::min(nptask, pair_blocks_max));
+    pair_shift = shift;
+    CK(cudaStreamSynchronize(st));
 }
 
 // Split each grid class into power-of-two sub-batches and take their plans
@@ -1406,6 +1439,38 @@ extern "C" int msg_utotal(msg_handle *h, int32_t isys, double *force, double *fo
         fill_energy(he, S.natat, e);
     }
     return h->check();
+    API_END
+}
+
+extern "C" int msg_get_forces(msg_handle *h, int32_t isys, double *force, double *forceo)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    const SysDev &S = h->hs[isys];
+    h->ensure_stage(3 * (size_t)S.n);
+    const int nb = (S.n + 255) / 256;
+    if (force) {
+        k_to_molsim<<<nb, 256, 0, h->st>>>(h->ftot, h->stage, h->inv, S.off, S.n, 1.0);
+        h->down(force, h->stage, 3 * sizeof(double) * S.n);
+    }
+    if (forceo) {
+        k_to_molsim<<<nb, 256, 0, h->st>>>(h->fo[h->cur], h->stage, h->inv, S.off, S.n, 1.0);
+        h->down(forceo, h->stage, 3 * sizeof(double) * S.n);
+    }
+    return h->check();
+    API_END
+}
+
+extern "C" int msg_tune(msg_handle *h, int32_t key, int32_t value)
+{
+    if (!h) return MSG_ERR_ARG;
+    API_BEGIN
+    if (key == MSG_TUNE_PAIR_LANES) {
+        if (value < -4 || value > 4) return MSG_ERR_ARG;
+        h->set_pair_lanes(value);
+        return MSG_OK;
+    }
+    return MSG_ERR_ARG;
     API_END
 }
 

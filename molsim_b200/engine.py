@@ -201,6 +201,18 @@ class Engine:
         d["forceo"] = fo
         return d
 
+    def forces(self, isys=0):
+        """(force, forceo) of system isys from the last force evaluation, no recomputation."""
+        n = int(self.systems[isys]["np"])
+        f = np.zeros((n, 3))
+        fo = np.zeros((n, 3))
+        self._check(_lib.lib().msg_get_forces(self.h, isys, _p(f, C.c_double), _p(fo, C.c_double)))
+        return f, fo
+
+    def tune_pair_lanes(self, shift):
+        """Lanes per particle in the pair kernel scaled by 2**shift (results move by rounding only)."""
+        self._check(_lib.lib().msg_tune(self.h, _lib.MSG_TUNE_PAIR_LANES, int(shift)))
+
     def GetLinAcc(self):
         self._check(_lib.lib().msg_get_linacc(self.h))
 

@@ -1,0 +1,71 @@
+"""Autotuner: SPME grid choice per system and the pair-lane knob."""
+import numpy as np
+import pytest
+
+from molsim_b200 import autotune as A
+
+
+def test_kolafa_perram_unit_charges():
+    s = dict(az=np.array([1.0, -1.0] * 500), boxlen=[100.0] * 3, rcut=30.0, epsi_four_pi=17.72)
+    a = 0.0876
+    want = 2.0 * np.sqrt(1000 / (30.0 * 1e6)) * np.exp(-(a * 30.0) ** 2) * 17.72
+    assert A.kolafa_perram_force_error(s, a) == pytest.approx(want, rel=1e-14)
+
+
+def _ensemble(n=6, seed=2):
+    from molsim_b200 import prepare
+    from molsim_b200.systems import replica_electrolyte
+
+    rng = np.random.default_rng(seed)
+    sy = [replica_electrolyte(rng, 2 * int(rng.integers(100, 600)), float(rng.uniform(0.01, 0.3)),
+                              float(rng.uniform(250, 400))) for _ in range(n)]
+    return sy, [prepare(s) for s in sy]
+
+
+@pytest.mark.gpu
+def test_grid_choice_meets_real_space_target_or_is_largest():
+    sy, tb = _ensemble()
+    edges, rep = A.tune_grids(sy, tb)
+    for g, r in zip(edges, rep):
+        assert g in A.CANDIDATES
+        if r["met"]:
+            assert r["err"][g] <= r["target"]
+            # no cheaper candidate meets it
+            assert all(r["err"][c] > r["target"] for c in A.CANDIDATES if c < g)
+        else:
+            assert g == max(A.CANDIDATES)
+        errs = [r["err"][c] for c in sorted(A.CANDIDATES)]
+        assert all(x > y for x, y in zip(errs, errs[1:])), errs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_pair_lanes_keep_results_within_tolerance(precision):
+    """The lane count regroups the FP32 partial sums a lane adds before its
+    fixed-point round, so mixed results move by FP32 rounding only (force
+    relative RMS <= 1e-6, energies <= 1e-6 of the total); each setting is itself
+    deterministic.  FP64: forces 1e-12; energies and virial 1e-9 of the total,
+    the 2^-32 kJ/mol quantum of each lane's fixed-point energy."""
+    from molsim_b200 import Engine
+
+    sy, tb = _ensemble(n=4, seed=4)
+    e = Engine(sy, tb, precision=precision)
+    tol = 1e-6 if precision == "mixed" else 1e-12
+    etol = 1e-6 if precision == "mixed" else 1e-9
+    base = None
+    for sh in (0, -1, 1, 2, 0):
+        e.tune_pair_lanes(sh)
+        e.UTotal(0)
+        f = [e.forces(k)[0] for k in range(len(sy))]
+        en = [e.energy(k) for k in range(len(sy))]
+        if base is None:
+            base = (f, en)
+            continue
+        for a, b in zip(f, base[0]):
+            assert np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)) <= tol
+            if sh == 0:
+                assert np.array_equal(a, b)           # same setting: same bits
+        for a, b in zip(en, base[1]):
+            scale = abs(b["utot"]) + abs(b["urec"]) + abs(b["utwob"][0])
+            for key in ("utot", "urec", "virial"):
+                assert abs(a[key] - b[key]) <= etol * max(scale, abs(b[key]))
