@@ -280,6 +280,7 @@ def run_serving(a):
     srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50)
     torch.cuda.synchronize()
     m = srv.run(jobs)
+    m.pop("latencies", None)
     # the plain FP64 path, each job alone: a sample across sizes, 200 steps each
     smp = sorted(jobs, key=lambda j: j.n)[:: max(1, len(jobs) // 12)][:12]
     work = tsum = 0.0

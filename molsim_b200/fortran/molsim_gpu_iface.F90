@@ -1,0 +1,155 @@
+! molsim_gpu_iface.F90 -- Fortran 2003 ISO_C_BINDING interface to libmolsim_gpu.so
+!
+! Binds the C-ABI of include/molsim_gpu.h for MOLSIM's Fortran host, the same
+! way MOLSIM binds FFTW (use, intrinsic :: iso_c_binding; Src/energy.F90:100-110).
+! Fortran (3,N) real(8) arrays are passed as they are (column-major (3,N) is
+! C [N][3]); type, table and neighbour indices keep MOLSIM's 1-based values.
+!
+! Build: gfortran -c molsim_gpu_iface.F90, link molsim_ser with
+!        -L<dir> -lmolsim_gpu -Wl,-rpath,<dir>
+! This file was not compiled in this repository's build (no Fortran compiler
+! in the build image); the C side it binds is tested through the same
+! entry points from Python.
+
+module MolsimGpu
+
+   use, intrinsic :: iso_c_binding
+   implicit none
+
+   integer(c_int32_t), parameter :: MSG_OK = 0, MSG_ERR_TABLE_MIN = 1, MSG_ERR_TABLE_RANGE = 2, &
+                                    MSG_ERR_CAPACITY = 3, MSG_ERR_CUDA = 4, MSG_ERR_TIMEOUT = 5, &
+                                    MSG_ERR_ARG = 6, MSG_ERR_NONFINITE = 7, MSG_ERR_HARDCORE = 8
+   integer(c_int32_t), parameter :: MSG_PREC_FP64 = 0, MSG_PREC_MIXED = 1
+
+   ! struct msg_params (field order and types as in molsim_gpu.h)
+   type, bind(c) :: msg_params
+      integer(c_int32_t) :: np, npt
+      real(c_double)     :: boxlen(3)
+      real(c_double)     :: rcut, drnlist
+      type(c_ptr)        :: iptpn, az, masspt, ubuf
+      integer(c_int32_t) :: nbuf
+      type(c_ptr)        :: iubuflow, r2umin, r2atat
+      integer(c_int32_t) :: lewald, order, nmesh, lsurf
+      real(c_double)     :: ualpha, epsi_four_pi
+      integer(c_int32_t) :: nbond
+      type(c_ptr)        :: bond_ij, bond_k, bond_eq, bond_p
+      real(c_double)     :: tstep
+      type(c_ptr)        :: bd_fac1, bd_fac2
+      integer(c_int32_t) :: maxnneigh
+   end type msg_params
+
+   ! struct msg_energy
+   type, bind(c) :: msg_energy
+      real(c_double) :: utot, utwob0, utwob(10), urec, ubond, virial, ekin
+   end type msg_energy
+
+   interface
+      integer(c_int) function msg_create(p, precision, h) bind(c, name='msg_create')
+         import :: c_int, c_int32_t, c_ptr, msg_params
+         type(msg_params), intent(in)         :: p
+         integer(c_int32_t), value            :: precision
+         type(c_ptr), intent(out)             :: h
+      end function msg_create
+
+      subroutine msg_destroy(h) bind(c, name='msg_destroy')
+         import :: c_ptr
+         type(c_ptr), value :: h
+      end subroutine msg_destroy
+
+      type(c_ptr) function msg_last_error(h) bind(c, name='msg_last_error')
+         import :: c_ptr
+         type(c_ptr), value :: h
+      end function msg_last_error
+
+      integer(c_int) function msg_set_state(h, isys, ro, rod, rodd) bind(c, name='msg_set_state')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: ro, rod, rodd
+      end function msg_set_state
+
+      integer(c_int) function msg_get_state(h, isys, ro, rod, rodd) bind(c, name='msg_get_state')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: ro, rod, rodd
+      end function msg_get_state
+
+      integer(c_int) function msg_build_nlist(h, isys, nneighpn, jpnlist, maxnneigh, npair) &
+            bind(c, name='msg_build_nlist')
+         import :: c_int, c_int32_t, c_int64_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: nneighpn, jpnlist
+         integer(c_int32_t), value :: maxnneigh
+         integer(c_int64_t), intent(out) :: npair
+      end function msg_build_nlist
+
+      integer(c_int) function msg_utotal(h, isys, force, forceo, e) bind(c, name='msg_utotal')
+         import :: c_int, c_int32_t, c_ptr, msg_energy
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: force, forceo
+         type(msg_energy), intent(out) :: e
+      end function msg_utotal
+
+      integer(c_int) function msg_get_linacc(h) bind(c, name='msg_get_linacc')
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function msg_get_linacc
+
+      integer(c_int) function msg_velver(h, nsteps, isys, e) bind(c, name='msg_velver')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: nsteps, isys
+         type(c_ptr), value        :: e          ! msg_energy(nsteps) or c_null_ptr
+      end function msg_velver
+
+      integer(c_int) function msg_bd_step(h, nsteps, seed, isys, xi, xi_out, e) bind(c, name='msg_bd_step')
+         import :: c_int, c_int32_t, c_int64_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: nsteps
+         integer(c_int64_t), value :: seed
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: xi, xi_out, e
+      end function msg_bd_step
+
+      integer(c_int) function msg_put_state(h, isys, ro, rod, rodd, keep_list) bind(c, name='msg_put_state')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: ro, rod, rodd
+         integer(c_int32_t), value :: keep_list
+      end function msg_put_state
+
+      integer(c_int64_t) function msg_nrebuild(h, isys) bind(c, name='msg_nrebuild')
+         import :: c_int32_t, c_int64_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+      end function msg_nrebuild
+
+      real(c_double) function msg_rcut_to_alpha(uewaldtol, q2sum, epsi_four_pi, boxlenshort, rcut, status) &
+            bind(c, name='msg_rcut_to_alpha')
+         import :: c_double, c_int32_t
+         real(c_double), value :: uewaldtol, q2sum, epsi_four_pi, boxlenshort, rcut
+         integer(c_int32_t), intent(out) :: status
+      end function msg_rcut_to_alpha
+   end interface
+
+contains
+
+   ! The message of the last error of handle h as a Fortran string.
+   function MsgError(h) result(txt)
+      type(c_ptr), intent(in) :: h
+      character(len=256) :: txt
+      character(kind=c_char), pointer :: s(:)
+      integer :: i
+      txt = ''
+      call c_f_pointer(msg_last_error(h), s, [256])
+      do i = 1, 256
+         if (s(i) == c_null_char) exit
+         txt(i:i) = s(i)
+      end do
+   end function MsgError
+
+end module MolsimGpu

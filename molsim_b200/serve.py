@@ -227,6 +227,7 @@ class Server:
                     mean_s=float(lat.mean()), makespan_s=span, particle_steps=work,
                     value=work / span, cohorts=self.ncohorts,
                     mean_cohort_jobs=float(np.mean(self.cohort_sizes)) if self.cohort_sizes else 0.0,
+                    latencies=[float(x) for x in lat] if ok else [],
                     max_concurrent_cohorts=self.max_concurrent, peak_reserved_bytes=self.peak_used,
                     peak_device_bytes=self.peak_device, budget_bytes=self.budget)
 

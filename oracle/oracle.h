@@ -10,12 +10,14 @@
  * C [N][3]; particle types, pair-table offsets and neighbour indices are
  * 1-based exactly as in MOLSIM's globals (Src/mol.F90:1087-1135).
  *
- * Parity status: the reference is Fortran and no Fortran compiler exists in
- * this build environment, so these routines are pinned against the
+ * Parity status: PARITY UNPINNED against the reference itself.  The
+ * reference is Fortran, ships no golden vectors for this path, and no Fortran
+ * compiler exists in this build environment, so no output of the compiled
+ * reference is available.  These routines are checked instead against the
  * reference's own in-code self checks (CheckUBuffer tolerances, TestCellList
  * completeness, TestEwaldSPM-style SPME-vs-converged checks, standard Ewald)
- * and against analytic known answers, not against outputs of the compiled
- * reference.
+ * and against analytic known answers (isolated ion pair, harmonic bond,
+ * rock-salt Madelung constant, NumPy FFT conventions).
  */
 #ifndef MOLSIM_ORACLE_H
 #define MOLSIM_ORACLE_H

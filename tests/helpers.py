@@ -65,3 +65,12 @@ def colloid_small():
     s = S.colloid_bd(seed=2, n_macro=8, n_salt_pairs=400, L=200.0, nmesh=32)
     s["bd_fac"] = S.bd_factors(s)
     return s
+
+
+@functools.lru_cache(maxsize=None)
+def config2():
+    """200,000-particle charged-colloid BD system (2000 macroions +20e, 40000 counterions,
+    79000 salt pairs, L = 1200 A, SPME 128^3 order 4, rc = 30 A)."""
+    s = S.colloid_bd(seed=0)
+    s["bd_fac"] = S.bd_factors(s)
+    return s

@@ -63,8 +63,10 @@ def test_pair_lanes_keep_results_within_tolerance(precision):
             continue
         for a, b in zip(f, base[0]):
             assert np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)) <= tol
-            if sh == 0:
-                assert np.array_equal(a, b)           # same setting: same bits
+            if sh == 0 and precision == "mixed":
+                # same setting: same bits (the FP64 charge grid uses FP64 atomics, so FP64
+                # repeats only to rounding)
+                assert np.array_equal(a, b)
         for a, b in zip(en, base[1]):
             scale = abs(b["utot"]) + abs(b["urec"]) + abs(b["utwob"][0])
             for key in ("utot", "urec", "virial"):

@@ -229,3 +229,43 @@ def test_mixed_velver_tracks_fp64():
     em, ed = gm.VelVer(20), gd.VelVer(20)
     for x, y in zip(em, ed):
         assert Hp.rel(x["utot"], y["utot"]) < 1e-5
+
+
+def _check_nlist_fast(o, g, n):
+    """As _check_nlist, vectorised for large systems."""
+    nn_o, jp_o = o.get_vlist()
+    nn_g, jp_g, npair = g.SetVList(0, export=True, maxnneigh=o.maxnneigh)
+    assert npair == int(nn_o.sum())
+    assert np.array_equal(nn_o, nn_g)
+    mask = np.arange(jp_o.shape[1])[None, :] < nn_o[:, None]
+    assert np.array_equal(np.where(mask, jp_o, 0), np.where(mask, jp_g, 0))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config2_colloid_bd_full_size(precision):
+    """The 200,000-particle Brownian-dynamics config at full size against the oracle with
+    its cell-list build: pair set bit-exact, UTotal, and two BD steps with injected noise."""
+    s = Hp.config2()
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t, cell=True, maxnneigh=256)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    g = Engine(s, t, precision=precision, maxnneigh=256)
+    _check_nlist_fast(o, g, s["np"])
+    ro = o.utotal()
+    rg = g.UTotal()
+    assert Hp.rel_rms(rg["force"], ro["force"]) < FORCE_TOL
+    etol = ENERGY_TOL if precision == "fp64" else 1e-6
+    scale = abs(ro["utot"]) + abs(ro["urec"]) + abs(ro["utwob"][0])
+    for k in ("utot", "urec", "virial"):
+        assert abs(rg[k] - ro[k]) <= etol * max(abs(ro[k]), scale if precision == "mixed" else 0.0), k
+    rng = np.random.default_rng(11)
+    xi = rng.standard_normal((2, s["np"], 3))
+    fac1, fac2 = s["bd_fac"]
+    g.BDStep(2, xi=xi, energies=False)
+    for k in range(2):
+        o.bd_step(xi[k], fac1, fac2)
+    d = g.get_state()["ro"] - o.get_state()["ro"]
+    box = s["boxlen"][0]
+    d -= box * np.round(d / box)
+    assert np.abs(d).max() < (1e-9 if precision == "fp64" else 1e-5)
