@@ -133,6 +133,13 @@ int  msg_get_forces(msg_handle *h, int32_t isys, double *force, double *forceo);
  * mixed results by FP32 rounding (a lane's partial sum is regrouped), and stay
  * deterministic for each setting. */
 #define MSG_TUNE_PAIR_LANES 1
+/* MSG_TUNE_PAIR_KERNEL (mixed path): 1 (default) the lean FP32 pair kernel that
+ * splits each pair's energy between its two ends, 0 the kernel shared with the
+ * FP64 path; both within the mixed-precision tolerance of the FP64 result. */
+#define MSG_TUNE_PAIR_KERNEL 2
+/* MSG_TUNE_PAIR_UNROLL (lean kernel): row entries each lane keeps in flight,
+ * 1, 2 (default) or 4.  Results do not depend on it. */
+#define MSG_TUNE_PAIR_UNROLL 3
 int  msg_tune(msg_handle *h, int32_t key, int32_t value);
 
 /* rodd = massip * forceo (GetLinAcc) from the last msg_utotal. */

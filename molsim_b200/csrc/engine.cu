@@ -150,7 +150,10 @@ struct msg_handle {
     int *ptmap = nullptr;
     double *tz = nullptr, *tc = nullptr;
     float *tz32 = nullptr, *tc32 = nullptr;
-    unsigned short *bst = nullptr;
+    unsigned short *bst = nullptr, *bsa = nullptr;   // bucket starts: per type pair / absolute row
+    int pair_lean = 1;                                // mixed path: k_pair_m (1) or k_pair (0)
+    int pair_unroll = 2;                              // k_pair_m: row entries in flight per lane
+    int nsm = 148;
     double *massip = nullptr, *massp = nullptr, *fac1 = nullptr, *fac2 = nullptr;
     int has_bd = 0;
     // bonds
@@ -227,9 +230,10 @@ struct msg_handle {
     }
     void plan_fft();
     void release_fft();
-    int pair_blocks_max = 1, pair_shift = 0;
+    int pair_blocks_max = 1, pair_blocks_lean = 1, pair_shift = 0;
     std::vector<PairTask> make_pair_tasks(int shift) const;
     void set_pair_lanes(int shift);
+    void set_lean_grid(int nsm);
 
     ~msg_handle();
     cudaEvent_t get_event()
@@ -315,7 +319,7 @@ static void free_all(msg_handle *h)
                     h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
                     h->t128, h->ptask, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
-                    h->bst, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
+                    h->bst, h->bsa, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
@@ -562,6 +566,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                 }
             }
         S.tab_k0 = pt[S.pt_off].k0;
+        if ((int)vz.size() - S.tab_k0 > 65535) throw CudaError{MSG_ERR_ARG, "more than 65535 table intervals in one system"};
         S.tab_b0 = pt[S.pt_off].b0;
         S.tab_nk = (int)vz.size() - S.tab_k0;
         {
@@ -588,6 +593,18 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     tz = dalloc<double>(vz.size());
     tc = dalloc<double>(vc.size());
     bst = dalloc<unsigned short>(vb.size());
+    bsa = dalloc<unsigned short>(vb.size());
+    {
+        // absolute bucket starts: the row within the system's table
+        std::vector<unsigned short> va(vb.size());
+        for (int s = 0; s < n; ++s)
+            for (int q = 0; q < hs[s].natat; ++q) {
+                const PairTab &T = pt[hs[s].pt_off + q];
+                for (int b = 0; b < MSG_NBUCKET; ++b)
+                    va[T.b0 + b] = (unsigned short)(vb[T.b0 + b] + (T.k0 - hs[s].tab_k0));
+            }
+        up(bsa, va.data(), va.size() * sizeof(unsigned short));
+    }
     massip = dalloc<double>(type_tot);
     massp = dalloc<double>(type_tot);
     fac1 = dalloc<double>(type_tot);
@@ -741,7 +758,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     up(dsys, hs.data(), n * sizeof(SysDev));
     if (!dry) {
         // persistent pair grid: as many blocks as fit the SMs at once
-        int nsm = 0, per = 0;
+        int per = 0;
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
 #define MSG_PAIR_CFG(PRC, NTV)                                                                           \
     do {                                                                                                \
@@ -750,14 +767,35 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     } while (0)
         if (prec == MSG_PREC_MIXED) {
             if (max_npt <= 2) MSG_PAIR_CFG(PrecM, 2); else MSG_PAIR_CFG(PrecM, 4);
+            set_lean_grid(nsm);
         } else {
             if (max_npt <= 2) MSG_PAIR_CFG(PrecD, 2); else MSG_PAIR_CFG(PrecD, 4);
         }
 #undef MSG_PAIR_CFG
         pair_blocks_max = nsm * std::max(1, per);
+        if (prec != MSG_PREC_MIXED) pair_blocks_lean = pair_blocks_max;
         pair_grid = std::max(1, std::min(nptask, pair_blocks_max));
     }
     if (!dry) CK(cudaStreamSynchronize(st));
+}
+
+// Persistent grid of the lean pair kernel for its current unroll: as many
+// blocks as fit the SMs at once.
+void msg_handle::set_lean_grid(int nsm)
+{
+    int perm = 0;
+#define MSG_LEAN_OCC(NTV, UV)                                                                                \
+    do {                                                                                                     \
+        CK(cudaFuncSetAttribute(k_pair_m<NTV, UV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024)); \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perm, k_pair_m<NTV, UV>, PAIR_BLOCK, pair_smem));  \
+    } while (0)
+    if (max_npt <= 2) {
+        if (pair_unroll == 1) MSG_LEAN_OCC(2, 1); else if (pair_unroll == 2) MSG_LEAN_OCC(2, 2); else MSG_LEAN_OCC(2, 4);
+    } else {
+        if (pair_unroll == 1) MSG_LEAN_OCC(4, 1); else if (pair_unroll == 2) MSG_LEAN_OCC(4, 2); else MSG_LEAN_OCC(4, 4);
+    }
+#undef MSG_LEAN_OCC
+    pair_blocks_lean = nsm * std::max(1, perm);
 }
 
 // Warp tasks of the pair kernel: 32/G consecutive particles of one system, G
@@ -964,7 +1002,20 @@ static void launch_forces(msg_handle *h, int mode, bool record)
         reinterpret_cast<const typename PR::V4 *>(PR::mixed ? (const void *)h->posfx : (const void *)h->pos[0]);
     const typename PR::R *tzp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tz32 : (const void *)h->tz);
     const typename PR::R *tcp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tc32 : (const void *)h->tc);
-    if (h->max_npt <= 2)
+    if (PR::mixed && h->pair_lean) {
+        const int grid = std::max(1, std::min(h->nptask, h->pair_blocks_lean));
+#define MSG_LEAN(NTV, UV)                                                                                   \
+    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, h->posfx,     \
+                                                                 h->typ[0], h->nbl, h->nnb, h->ptmap,      \
+                                                                 h->ptab, h->tc32, h->bsa, h->fsr, h->eacc, \
+                                                                 h->errw)
+        if (h->max_npt <= 2) {
+            if (h->pair_unroll == 1) MSG_LEAN(2, 1); else if (h->pair_unroll == 2) MSG_LEAN(2, 2); else MSG_LEAN(2, 4);
+        } else {
+            if (h->pair_unroll == 1) MSG_LEAN(4, 1); else if (h->pair_unroll == 2) MSG_LEAN(4, 2); else MSG_LEAN(4, 4);
+        }
+#undef MSG_LEAN
+    } else if (h->max_npt <= 2)
         k_pair<PR, 2><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
                                                               h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
                                                               h->eacc, h->errw);
@@ -1468,6 +1519,23 @@ extern "C" int msg_tune(msg_handle *h, int32_t key, int32_t value)
     if (key == MSG_TUNE_PAIR_LANES) {
         if (value < -4 || value > 4) return MSG_ERR_ARG;
         h->set_pair_lanes(value);
+        return MSG_OK;
+    }
+    if (key == MSG_TUNE_PAIR_UNROLL) {
+        if (value != 1 && value != 2 && value != 4) return MSG_ERR_ARG;
+        if (h->pair_unroll != value) {
+            h->drop_graph();
+            h->pair_unroll = value;
+            if (h->prec == MSG_PREC_MIXED) h->set_lean_grid(h->nsm);
+        }
+        return MSG_OK;
+    }
+    if (key == MSG_TUNE_PAIR_KERNEL) {
+        if (value != 0 && value != 1) return MSG_ERR_ARG;
+        if (h->pair_lean != value) {
+            h->drop_graph();
+            h->pair_lean = value;
+        }
         return MSG_OK;
     }
     return MSG_ERR_ARG;

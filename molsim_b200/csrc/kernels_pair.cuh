@@ -109,6 +109,9 @@ __host__ __device__ inline size_t pair_smem_bytes(int nk, int nbucket)
 #ifndef MSG_PAIR_MINB
 #define MSG_PAIR_MINB 2
 #endif
+#ifndef MSG_PAIR_MINB_M
+#define MSG_PAIR_MINB_M 3
+#endif
 template <class PR> struct PairBatch { static constexpr int B = PR::mixed ? MSG_PAIR_B32 : 1; };
 
 // NT: particle types per system accounted in registers (2 or 4).
@@ -344,6 +347,224 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MSG_PAIR_MINB) k_pair(
         if (lane == 31 && vir) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_VIRPAIR), (unsigned long long)vir);
 #pragma unroll
         for (int q = 0; q < NT * NT; ++q) ue[q] = 0;
+        vir = 0;
+        rs = re;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Lean FP32 pair kernel of the mixed-precision path.
+//
+// Same work split as k_pair (G lanes per particle over the full list, tasks
+// pulled from a shared counter, the system's table in shared memory), with
+// less work and more memory parallelism per list entry:
+//   * one shared record per (particle type, partner type): the FP32 bucket
+//     grid (z_lo, 1/h) and the bucket base, read with one 16-byte load;
+//   * bucket starts hold the absolute row of the system's table, so the row
+//     address is one multiply-add (`bsa`, built on the host);
+//   * above the table top the clamped last bucket already names the first
+//     interval, so there is no separate upper-range test;
+//   * every pair is seen from both ends; each end adds half of the pair's
+//     energy and virial, so there is no ownership test per entry;
+//   * each lane loads U row entries, then their U partner positions, before
+//     it uses any of them, so U gathers per lane are in flight together.
+// The interval found is the one MOLSIM's walk ends on (Src/energy.F90:481-486),
+// as in k_pair.
+// ---------------------------------------------------------------------------
+
+// Unordered type pair (a <= b) of NT types -> 0 .. NT(NT+1)/2-1, a-major.
+template <int NT>
+__host__ __device__ constexpr int tpair(int a, int b) { return a * (2 * NT - a + 1) / 2 + (b - a); }
+
+template <int NT, int U>
+__global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MINB_M : 2) k_pair_m(
+    const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, int ntasks,
+    const int4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
+    const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
+    const float *__restrict__ tc, const unsigned short *__restrict__ bsa, double4 *__restrict__ fsr,
+    long long *__restrict__ eacc, ErrWord *err)
+{
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ PairTab sP[MSG_MAX_NATAT];
+    __shared__ float4 sT[MAXT * MAXT];        // (z_lo, 1/h, unused, bucket base as int bits)
+    __shared__ int sMap[MAXT * MAXT];
+    __shared__ int sNext;
+    const int lane = threadIdx.x & 31;
+    const int t0 = (int)(((long long)blockIdx.x * ntasks) / gridDim.x);
+    const int t1 = (int)(((long long)(blockIdx.x + 1) * ntasks) / gridDim.x);
+    // energies by unordered type pair and the virial, 64-bit fixed point per lane
+    constexpr int NQ = tpair<NT>(NT - 1, NT - 1) + 1;
+    long long ue[NQ];
+    long long vir = 0;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) ue[q] = 0;
+    int loaded = -1;
+    const float *Tc = nullptr;
+    const unsigned short *Tb = nullptr;
+    int kbase = 0;
+    for (int rs = t0; rs < t1;) {
+        const PairTask W0 = tasks[rs];
+        const int re = min(t1, W0.send);
+        __syncthreads();
+        if (W0.sys != loaded) {
+            const SysDev &Sn = sysv[W0.sys];
+            if (threadIdx.x < Sn.natat) sP[threadIdx.x] = ptab[Sn.pt_off + threadIdx.x];
+            if (threadIdx.x < Sn.npt * Sn.npt) {
+                const int q = ptmap[Sn.ptmap_off + threadIdx.x] - Sn.pt_off;
+                sMap[threadIdx.x] = q;
+                const PairTab &P = ptab[Sn.pt_off + q];
+                const int a = threadIdx.x / Sn.npt, b = threadIdx.x % Sn.npt;
+                sT[a * MAXT + b] = make_float4(P.fz_lo, P.finv_h, 0.0f, __int_as_float(q * MSG_NBUCKET));
+            }
+            kbase = Sn.tab_k0;
+            if (Sn.tab_smem) {
+                float *sc = reinterpret_cast<float *>(dyn);
+                unsigned short *sb = reinterpret_cast<unsigned short *>(sc + (size_t)12 * Sn.tab_nk);
+                const int nc = 12 * Sn.tab_nk, nb = Sn.natat * MSG_NBUCKET;
+                for (int k = threadIdx.x; k < nc; k += PAIR_BLOCK) sc[k] = tc[(size_t)12 * Sn.tab_k0 + k];
+                for (int k = threadIdx.x; k < nb; k += PAIR_BLOCK) sb[k] = bsa[Sn.tab_b0 + k];
+                Tc = sc;
+                Tb = sb;
+            } else {
+                Tc = tc + (size_t)12 * Sn.tab_k0;
+                Tb = bsa + Sn.tab_b0;
+            }
+            loaded = W0.sys;
+        }
+        if (threadIdx.x == 0) sNext = rs;
+        __syncthreads();
+        const SysDev &S = sysv[W0.sys];
+        const float rcut2 = (float)S.rcut2;
+        const float lowmax = (float)fmax(S.r2umin_max, S.r2atat_max);
+        const float sx = S.fxi[0], sy = S.fxi[1], sz = S.fxi[2];
+        for (;;) {
+            int task = 0;
+            if (lane == 0) task = atomicAdd(&sNext, 1);
+            task = __shfl_sync(0xffffffffu, task, 0);
+            if (task >= re) break;
+            const PairTask W = tasks[task];
+            const int G = W.g;
+            const int g = lane & (G - 1);
+            const int i = W.i0 + lane / G;
+            const bool act = i < W.i1;
+            float fx = 0.0f, fy = 0.0f, fz = 0.0f, vi = 0.0f;
+            float ut[NT];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) ut[t] = 0.0f;
+            int ti = 0, n = 0;
+            int4 xi = make_int4(0, 0, 0, 0);
+            const int *row = nbl;
+            if (act) {
+                xi = pos[i];
+                ti = typ[i];
+                n = nnb[i];
+                row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
+            }
+            const float4 *sTi = sT + ti * MAXT;
+            // U row entries per lane in flight: their indices, then their partners' positions,
+            // are loaded before any of them is used
+            for (int kb = g; kb < n; kb += U * G) {
+                int ee[U];
+                int4 xj[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) ee[u] = (kb + u * G < n) ? __ldg(row + kb + u * G) : -1;
+#pragma unroll
+                for (int u = 0; u < U; ++u) xj[u] = pos[ee[u] >= 0 ? (ee[u] & NBL_JMASK) : i];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (ee[u] < 0) continue;
+                    const int e = ee[u];
+                    const int j = e & NBL_JMASK;
+                    const int tj = (unsigned)e >> 28;
+                    // exact integer difference, wrapped to the minimum image
+                    const float dx = (float)(int)((unsigned)xi.x - (unsigned)xj[u].x) * sx;
+                    const float dy = (float)(int)((unsigned)xi.y - (unsigned)xj[u].y) * sy;
+                    const float dz = (float)(int)((unsigned)xi.z - (unsigned)xj[u].z) * sz;
+                    const float r2 = dx * dx + dy * dy + dz * dz;
+                    if (r2 > rcut2) continue;
+                    const float4 T = sTi[tj];
+                    int bk = __float2int_rz((r2 - T.x) * T.y);
+                    bk = min(max(bk, 0), MSG_NBUCKET - 1);
+                    int kk = Tb[__float_as_int(T.w) + bk];
+                    Row12<float> c;
+                    c.load(Tc + (size_t)kk * 12);
+                    bool ok = true;
+                    if (r2 < lowmax || r2 < c.c[0]) {
+                        // rare: below the type pair's lower limits, or the walk goes past the bucket start
+                        const PairTab &Q = sP[sMap[ti * S.npt + tj]];
+                        const int kend = Q.k0 - kbase + Q.nk;
+                        if (r2 < (float)Q.r2atat) {
+                            // hard-core overlap: u = 1e10, f = 0 (the reference leaves fsum stale here)
+                            c.c[0] = r2;
+                            c.c[1] = 1e10f;
+#pragma unroll
+                            for (int q = 2; q < 12; ++q) c.c[q] = 0.0f;
+                        } else if (r2 < (float)Q.r2umin) {
+                            raise_error(err, 1, W.sys, i, j);
+                            ok = false;
+                        } else {
+                            while (r2 < c.c[0]) {
+                                if (++kk >= kend) {
+                                    raise_error(err, 2, W.sys, i, j);
+                                    kk = kend - 1;
+                                    c.load(Tc + (size_t)kk * 12);
+                                    break;
+                                }
+                                c.load(Tc + (size_t)kk * 12);
+                            }
+                        }
+                    }
+                    if (!ok) continue;
+                    const float d = r2 - c.c[0];
+                    const float uu = c.c[1] + d * (c.c[2] + d * (c.c[3] + d * (c.c[4] + d * (c.c[5] + d * c.c[6]))));
+                    const float f = c.c[7] + d * (c.c[8] + d * (c.c[9] + d * (c.c[10] + d * c.c[11])));
+                    fx += f * dx;
+                    fy += f * dy;
+                    fz += f * dz;
+#pragma unroll
+                    for (int t = 0; t < NT; ++t) ut[t] += (tj == t) ? uu : 0.0f;
+                    vi -= f * r2;
+                }
+            }
+            // each pair was seen from both ends: each end keeps half of its energy and virial
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                const long long v = __double2ll_rn((double)ut[t] * (0.5 * kEFix));
+#pragma unroll
+                for (int a = 0; a < NT; ++a) ue[tpair<NT>(min(a, t), max(a, t))] += (a == ti) ? v : 0;
+            }
+            vir += __double2ll_rn((double)vi * (0.5 * kEFix));
+            long long ax = __float2ll_rn(fx * 4294967296.0f), ay = __float2ll_rn(fy * 4294967296.0f),
+                      az = __float2ll_rn(fz * 4294967296.0f);
+            for (int o = G >> 1; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                az += __shfl_xor_sync(0xffffffffu, az, o);
+            }
+            if (act && g == 0)
+                fsr[i] = make_double4((double)ax * kFixInv, (double)ay * kFixInv, (double)az * kFixInv, 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ue[q] += __shfl_xor_sync(0xffffffffu, ue[q], o);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vir += __shfl_xor_sync(0xffffffffu, vir, o);
+        long long *ea = eacc + (size_t)W0.sys * EA_N;
+        if (lane < S.npt * S.npt) {
+            const int ta = lane / S.npt, tb = lane % S.npt;
+            if (ta <= tb) {
+                long long v = 0;
+#pragma unroll
+                for (int a = 0; a < NT; ++a)
+#pragma unroll
+                    for (int b = a; b < NT; ++b) v += (a == ta && b == tb) ? ue[tpair<NT>(a, b)] : 0;
+                if (v) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_UTWOB + sMap[lane]), (unsigned long long)v);
+            }
+        }
+        if (lane == 31 && vir) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_VIRPAIR), (unsigned long long)vir);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) ue[q] = 0;
         vir = 0;
         rs = re;
     }

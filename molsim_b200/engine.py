@@ -156,7 +156,10 @@ class Engine:
     def __del__(self):
         h = getattr(self, "h", None)
         if h is not None and h.value:
-            _lib.lib().msg_destroy(h)
+            try:
+                _lib.lib().msg_destroy(h)
+            except TypeError:           # interpreter shutdown: the module globals are gone
+                pass
             self.h = None
 
     def _check(self, rc):
