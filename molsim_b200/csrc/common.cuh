@@ -55,6 +55,7 @@ struct SysDev {
     int ptmap_off;              // first entry of this system's npt*npt type-pair map
     int tab_k0, tab_nk, tab_b0; // this system's slice of the concatenated table (intervals, buckets)
     int tab_smem;               // 1: the slice fits the pair kernel's shared-memory table
+    int tab_smem_m;             // 1: the slice fits the lean FP32 pair kernel's shared-memory table
     double r2umin_max;          // largest r2umin / r2atat over the type pairs: pairs at or above
     double r2atat_max;          //   these need no per-pair lower-limit check
     double fxs[3];              // 2^32 / box: fixed-point coordinate scale of the mixed mirror

@@ -150,7 +150,9 @@ struct msg_handle {
     int *ptmap = nullptr;
     double *tz = nullptr, *tc = nullptr;
     float *tz32 = nullptr, *tc32 = nullptr;
-    unsigned short *bst = nullptr, *bsa = nullptr;   // bucket starts: per type pair / absolute row
+    unsigned short *bst = nullptr;                    // bucket starts per type pair
+    int2 *bkz = nullptr;                              // lean kernel buckets: (absolute row, its z_low)
+    size_t pair_smem_m = 0;
     int pair_lean = 1;                                // mixed path: k_pair_m (1) or k_pair (0)
     int pair_unroll = 2;                              // k_pair_m: row entries in flight per lane
     int nsm = 148;
@@ -319,7 +321,7 @@ static void free_all(msg_handle *h)
                     h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
                     h->t128, h->ptask, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
-                    h->bst, h->bsa, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
+                    h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
@@ -574,6 +576,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                                                           : pair_smem_bytes<double>(S.tab_nk, S.natat * MSG_NBUCKET);
             S.tab_smem = bytes <= 96 * 1024 ? 1 : 0;
             if (S.tab_smem) pair_smem = std::max(pair_smem, bytes);
+            const size_t bm = lean_smem_bytes(S.tab_nk, S.natat * MSG_NBUCKET);
+            S.tab_smem_m = bm <= 96 * 1024 ? 1 : 0;
+            if (S.tab_smem_m) pair_smem_m = std::max(pair_smem_m, bm);
         }
         S.r2umin_max = 0.0;
         S.r2atat_max = 0.0;
@@ -593,17 +598,29 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     tz = dalloc<double>(vz.size());
     tc = dalloc<double>(vc.size());
     bst = dalloc<unsigned short>(vb.size());
-    bsa = dalloc<unsigned short>(vb.size());
+    bkz = dalloc<int2>(vb.size());
     {
-        // absolute bucket starts: the row within the system's table
-        std::vector<unsigned short> va(vb.size());
+        // lean-kernel buckets: the interval that holds the bucket's top (with 1% of a bucket
+        // of slack for the FP32 bucket index), as a row of the system's table, and that
+        // interval's z_low in FP32.  A pair below that z_low lies in the next interval unless
+        // two interval bounds fall inside one bucket, where the kernel walks as MOLSIM does.
+        std::vector<int2> va(vb.size());
         for (int s = 0; s < n; ++s)
             for (int q = 0; q < hs[s].natat; ++q) {
                 const PairTab &T = pt[hs[s].pt_off + q];
-                for (int b = 0; b < MSG_NBUCKET; ++b)
-                    va[T.b0 + b] = (unsigned short)(vb[T.b0 + b] + (T.k0 - hs[s].tab_k0));
+                const double *z = vz.data() + T.k0;
+                const double h = (T.z_hi > T.z_lo) ? (T.z_hi - T.z_lo) / MSG_NBUCKET : 1.0;
+                for (int b = 0; b < MSG_NBUCKET; ++b) {
+                    const double zq = T.z_lo + (b + 1.01) * h;
+                    int kk = 0;
+                    while (kk < T.nk - 1 && zq < z[kk]) ++kk;
+                    float zf = (float)z[kk];
+                    int zi;
+                    std::memcpy(&zi, &zf, sizeof(zi));
+                    va[T.b0 + b] = make_int2(kk + (T.k0 - hs[s].tab_k0), zi);
+                }
             }
-        up(bsa, va.data(), va.size() * sizeof(unsigned short));
+        up(bkz, va.data(), va.size() * sizeof(int2));
     }
     massip = dalloc<double>(type_tot);
     massp = dalloc<double>(type_tot);
@@ -787,7 +804,7 @@ void msg_handle::set_lean_grid(int nsm)
 #define MSG_LEAN_OCC(NTV, UV)                                                                                \
     do {                                                                                                     \
         CK(cudaFuncSetAttribute(k_pair_m<NTV, UV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024)); \
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perm, k_pair_m<NTV, UV>, PAIR_BLOCK, pair_smem));  \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perm, k_pair_m<NTV, UV>, PAIR_BLOCK, pair_smem_m)); \
     } while (0)
     if (max_npt <= 2) {
         if (pair_unroll == 1) MSG_LEAN_OCC(2, 1); else if (pair_unroll == 2) MSG_LEAN_OCC(2, 2); else MSG_LEAN_OCC(2, 4);
@@ -1005,10 +1022,10 @@ static void launch_forces(msg_handle *h, int mode, bool record)
     if (PR::mixed && h->pair_lean) {
         const int grid = std::max(1, std::min(h->nptask, h->pair_blocks_lean));
 #define MSG_LEAN(NTV, UV)                                                                                   \
-    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, h->posfx,     \
-                                                                 h->typ[0], h->nbl, h->nnb, h->ptmap,      \
-                                                                 h->ptab, h->tc32, h->bsa, h->fsr, h->eacc, \
-                                                                 h->errw)
+    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem_m, h->st>>>(h->dsys, h->ptask, h->nptask, h->posfx,   \
+                                                                   h->typ[0], h->nbl, h->nnb, h->ptmap,    \
+                                                                   h->ptab, h->tc32, h->bkz, h->fsr,       \
+                                                                   h->eacc, h->errw)
         if (h->max_npt <= 2) {
             if (h->pair_unroll == 1) MSG_LEAN(2, 1); else if (h->pair_unroll == 2) MSG_LEAN(2, 2); else MSG_LEAN(2, 4);
         } else {

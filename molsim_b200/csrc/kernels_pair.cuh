@@ -102,6 +102,13 @@ __host__ __device__ inline size_t pair_smem_bytes(int nk, int nbucket)
     return (size_t)nk * 12 * sizeof(R) + (size_t)nbucket * sizeof(unsigned short);
 }
 
+// Shared-memory image of a system's table for k_pair_m: FP32 coefficient rows,
+// then (row, z_low) buckets.
+__host__ __device__ inline size_t lean_smem_bytes(int nk, int nbucket)
+{
+    return (size_t)nk * 12 * sizeof(float) + (size_t)nbucket * sizeof(int2);
+}
+
 // Lanes per batch: B row segments per lane are in flight together.
 #ifndef MSG_PAIR_B32
 #define MSG_PAIR_B32 2
@@ -360,8 +367,11 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MSG_PAIR_MINB) k_pair(
 // less work and more memory parallelism per list entry:
 //   * one shared record per (particle type, partner type): the FP32 bucket
 //     grid (z_lo, 1/h) and the bucket base, read with one 16-byte load;
-//   * bucket starts hold the absolute row of the system's table, so the row
-//     address is one multiply-add (`bsa`, built on the host);
+//   * a bucket holds the interval containing its top, as a row of the system's
+//     table, and that interval's z_low; a pair below that z_low takes the next
+//     row.  Intervals are wider than buckets except at the shortest distances,
+//     so this compare replaces MOLSIM's walk for all but about 2e-4 of the
+//     pairs, which still walk (`bkz`, built on the host);
 //   * above the table top the clamped last bucket already names the first
 //     interval, so there is no separate upper-range test;
 //   * every pair is seen from both ends; each end adds half of the pair's
@@ -381,12 +391,12 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
     const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, int ntasks,
     const int4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
     const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
-    const float *__restrict__ tc, const unsigned short *__restrict__ bsa, double4 *__restrict__ fsr,
+    const float *__restrict__ tc, const int2 *__restrict__ bkz, double4 *__restrict__ fsr,
     long long *__restrict__ eacc, ErrWord *err)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ PairTab sP[MSG_MAX_NATAT];
-    __shared__ float4 sT[MAXT * MAXT];        // (z_lo, 1/h, unused, bucket base as int bits)
+    __shared__ float4 sT[MAXT * MAXT];        // (z_lo, 1/h, end row, bucket base), the last two as int bits
     __shared__ int sMap[MAXT * MAXT];
     __shared__ int sNext;
     const int lane = threadIdx.x & 31;
@@ -400,7 +410,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
     for (int q = 0; q < NQ; ++q) ue[q] = 0;
     int loaded = -1;
     const float *Tc = nullptr;
-    const unsigned short *Tb = nullptr;
+    const int2 *Tb = nullptr;
     int kbase = 0;
     for (int rs = t0; rs < t1;) {
         const PairTask W0 = tasks[rs];
@@ -414,20 +424,21 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
                 sMap[threadIdx.x] = q;
                 const PairTab &P = ptab[Sn.pt_off + q];
                 const int a = threadIdx.x / Sn.npt, b = threadIdx.x % Sn.npt;
-                sT[a * MAXT + b] = make_float4(P.fz_lo, P.finv_h, 0.0f, __int_as_float(q * MSG_NBUCKET));
+                sT[a * MAXT + b] = make_float4(P.fz_lo, P.finv_h, __int_as_float(P.k0 - Sn.tab_k0 + P.nk),
+                                               __int_as_float(q * MSG_NBUCKET));
             }
             kbase = Sn.tab_k0;
-            if (Sn.tab_smem) {
+            if (Sn.tab_smem_m) {
                 float *sc = reinterpret_cast<float *>(dyn);
-                unsigned short *sb = reinterpret_cast<unsigned short *>(sc + (size_t)12 * Sn.tab_nk);
+                int2 *sb = reinterpret_cast<int2 *>(sc + (size_t)12 * Sn.tab_nk);
                 const int nc = 12 * Sn.tab_nk, nb = Sn.natat * MSG_NBUCKET;
                 for (int k = threadIdx.x; k < nc; k += PAIR_BLOCK) sc[k] = tc[(size_t)12 * Sn.tab_k0 + k];
-                for (int k = threadIdx.x; k < nb; k += PAIR_BLOCK) sb[k] = bsa[Sn.tab_b0 + k];
+                for (int k = threadIdx.x; k < nb; k += PAIR_BLOCK) sb[k] = bkz[Sn.tab_b0 + k];
                 Tc = sc;
                 Tb = sb;
             } else {
                 Tc = tc + (size_t)12 * Sn.tab_k0;
-                Tb = bsa + Sn.tab_b0;
+                Tb = bkz + Sn.tab_b0;
             }
             loaded = W0.sys;
         }
@@ -485,7 +496,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
                     const float4 T = sTi[tj];
                     int bk = __float2int_rz((r2 - T.x) * T.y);
                     bk = min(max(bk, 0), MSG_NBUCKET - 1);
-                    int kk = Tb[__float_as_int(T.w) + bk];
+                    const int2 B = Tb[__float_as_int(T.w) + bk];
+                    int kk = min(B.x + (r2 < __int_as_float(B.y) ? 1 : 0), __float_as_int(T.z) - 1);
                     Row12<float> c;
                     c.load(Tc + (size_t)kk * 12);
                     bool ok = true;
