@@ -953,7 +953,7 @@ static void launch_spme(msg_handle *h)
 {
     h->tbeg(TM_SPREAD);
     if (!PR::mixed) CK(cudaMemsetAsync(h->rgrid, 0, sizeof(double) * h->grid_tot, h->st));
-    k_spread<P, PR><<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->rgrid, h->igrid,
+    k_spread<P, PR><<<h->nt128 * (128 / SPREAD_PART), SPREAD_THREADS, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->rgrid, h->igrid,
                                                   h->eacc);
     h->launches += 1;
     if (PR::mixed) {

@@ -14,16 +14,16 @@ constexpr double kGridFixInv = 1.0 / 1099511627776.0;
 // system's fixed-point accumulators.
 __device__ __forceinline__ void block_dipole(double qx, double qy, double qz, long long *__restrict__ ea)
 {
-    __shared__ double red[3][4];
+    __shared__ double red[3][32];
     qx = warp_sum(qx);
     qy = warp_sum(qy);
     qz = warp_sum(qz);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     if (lane == 0) { red[0][w] = qx; red[1][w] = qy; red[2][w] = qz; }
     __syncthreads();
     if (threadIdx.x < 3) {
         double s = 0.0;
-        for (int k = 0; k < 4; ++k) s += red[threadIdx.x][k];
+        for (int k = 0; k < nw; ++k) s += red[threadIdx.x][k];
         acc_add(ea + EA_DIP + threadIdx.x, s);
     }
 }
@@ -33,50 +33,57 @@ __device__ __forceinline__ void block_dipole(double qx, double qy, double qz, lo
 // PrecD: FP64 atomics into the FP64 grid.  PrecM: FP32 splines, each
 // contribution rounded to 2^-40 and added as a 64-bit integer, so the grid is
 // the same whatever order the atomics land in.
+// A block takes SPREAD_PART particles: one thread per particle forms the
+// splines into shared memory, then the block walks the particles' P^3
+// contributions x-fastest, so the lanes of a warp add into runs of P
+// consecutive grid points (fewer L2 sectors per atomic instruction than one
+// particle per lane).
 // ---------------------------------------------------------------------------
+constexpr int SPREAD_PART = 32;
+constexpr int SPREAD_THREADS = 128;
+
 template <int P, class PR>
-__global__ void __launch_bounds__(128) k_spread(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                               const double4 *__restrict__ pos, double *__restrict__ grid, unsigned long long *__restrict__ igrid,
-                                               long long *__restrict__ eacc)
+__global__ void __launch_bounds__(SPREAD_THREADS) k_spread(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                           const double4 *__restrict__ pos, double *__restrict__ grid,
+                                                           unsigned long long *__restrict__ igrid, long long *__restrict__ eacc)
 {
     using R = typename PR::R;
-    const Tile T = tiles[blockIdx.x];
+    __shared__ R sth[SPREAD_PART][3][P];
+    __shared__ int skm[SPREAD_PART][3];
+    __shared__ R sq[SPREAD_PART];
+    const Tile T = tiles[blockIdx.x / (128 / SPREAD_PART)];
     const SysDev &S = sysv[T.sys];
     if (!S.lewald) return;
-    const int i = T.i0 + threadIdx.x;
+    const int p0 = T.i0 + (int)(blockIdx.x % (128 / SPREAD_PART)) * SPREAD_PART;
+    const int np = max(0, min(SPREAD_PART, T.i1 - p0));
+    const int s = S.s;
     double4 x = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (i < T.i1) {
-        x = pos[i];
+    if ((int)threadIdx.x < np) {
+        x = pos[p0 + threadIdx.x];
         const double xc[3] = {x.x, x.y, x.z};
-        const int s = S.s;
         R th[3][P], dth[3][P];
-        int km[3];
 #pragma unroll
-        for (int m = 0; m < 3; ++m) km[m] = bspline_at<P, R>(S.dkdr[m] * xc[m], s, th[m], dth[m]);
-        const R q = (R)x.w;
+        for (int m = 0; m < 3; ++m) {
+            skm[threadIdx.x][m] = bspline_at<P, R>(S.dkdr[m] * xc[m], s, th[m], dth[m]);
 #pragma unroll
-        for (int iz = 0; iz < P; ++iz) {
-            int nz = km[2] - iz;
-            nz += (nz < 0) ? s : 0;
-            const R qz = q * th[2][iz];
-#pragma unroll
-            for (int iy = 0; iy < P; ++iy) {
-                int ny = km[1] - iy;
-                ny += (ny < 0) ? s : 0;
-                const R qyz = qz * th[1][iy];
-                const size_t rowo = S.grid_off + ((size_t)nz * s + ny) * s;
-#pragma unroll
-                for (int ix = 0; ix < P; ++ix) {
-                    int nx = km[0] - ix;
-                    nx += (nx < 0) ? s : 0;
-                    if (PR::mixed)
-                        atomicAdd(igrid + rowo + nx,
-                                  (unsigned long long)__double2ll_rn((double)(qyz * th[0][ix]) * kGridFix));
-                    else
-                        atomicAdd(grid + rowo + nx, (double)(qyz * th[0][ix]));
-                }
-            }
+            for (int k = 0; k < P; ++k) sth[threadIdx.x][m][k] = th[m][k];
         }
+        sq[threadIdx.x] = (R)x.w;
+    }
+    __syncthreads();
+    const int ncon = np * P * P * P;
+    for (int c = threadIdx.x; c < ncon; c += SPREAD_THREADS) {
+        const int ix = c % P, r1 = c / P, iy = r1 % P, r2 = r1 / P, iz = r2 % P, pp = r2 / P;
+        int nx = skm[pp][0] - ix, ny = skm[pp][1] - iy, nz = skm[pp][2] - iz;
+        nx += (nx < 0) ? s : 0;
+        ny += (ny < 0) ? s : 0;
+        nz += (nz < 0) ? s : 0;
+        const R v = sq[pp] * sth[pp][2][iz] * sth[pp][1][iy] * sth[pp][0][ix];
+        const size_t at = S.grid_off + ((size_t)nz * s + ny) * s + nx;
+        if (PR::mixed)
+            atomicAdd(igrid + at, (unsigned long long)__double2ll_rn((double)v * kGridFix));
+        else
+            atomicAdd(grid + at, (double)v);
     }
     if (S.lsurf) block_dipole(x.w * x.x, x.w * x.y, x.w * x.z, eacc + (size_t)T.sys * EA_N);
 }
@@ -159,7 +166,8 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence(const SysDev *__rest
 // ---------------------------------------------------------------------------
 constexpr int NPART_FIN = 4;    // ubond, virbond, ekin, spare
 constexpr int ESZ = 16;
-constexpr int FIN_THREADS = 128;
+constexpr int FIN_LANES = 4;                      // lanes per particle in the grid gather
+constexpr int FIN_THREADS = 128 * FIN_LANES;      // one 128-particle tile per block
 
 struct FinOut {
     double *esys, *hist;
@@ -186,17 +194,34 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     __shared__ bool last;
     const Tile T = tiles[blockIdx.x];
     const SysDev &S = sysv[T.sys];
-    const int i = T.i0 + threadIdx.x;
+    // FIN_LANES lanes per particle share the gather; the group's first lane does the rest
+    const int g = threadIdx.x & (FIN_LANES - 1);
+    const int i = T.i0 + (int)threadIdx.x / FIN_LANES;
     long long *ea = eacc + (size_t)T.sys * EA_N;
     if (S.lsurf) {
         if (threadIdx.x < 3) sq[threadIdx.x] = acc_get(ea + EA_DIP + threadIdx.x);
         __syncthreads();
     }
     double ub = 0.0, vb = 0.0, ek = 0.0;
+    R e0 = 0, e1 = 0, e2 = 0;
+    double4 x = make_double4(0.0, 0.0, 0.0, 0.0);
+    // the particle's own loads go out before the gather so that their latencies overlap
+    double4 f0 = make_double4(0.0, 0.0, 0.0, 0.0), vold = f0, aold = f0;
+    int o = 0, tyi = 0, bb0 = 0, bb1 = 0;
     if (i < T.i1) {
-        const double4 x = pos[i];
-        const double4 f0 = fsr[i];
-        double Fx = f0.x, Fy = f0.y, Fz = f0.z;
+        x = pos[i];
+        o = orig[i];
+        if (g == 0) {
+            f0 = fsr[i];
+            if (mode == 1) {
+                tyi = typ[i];
+                vold = vel[i];
+                aold = acc[i];
+            }
+        } else {
+            bb0 = bptr[S.off + o];
+            bb1 = bptr[S.off + o + 1];
+        }
         if (S.lewald) {
             const int s = S.s;
             const double xc[3] = {x.x, x.y, x.z};
@@ -204,41 +229,42 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
             int km[3];
 #pragma unroll
             for (int m = 0; m < 3; ++m) km[m] = bspline_at<P, R>(S.dkdr[m] * xc[m], s, th[m], dth[m]);
-            R e0 = 0, e1 = 0, e2 = 0;
-#pragma unroll
-            for (int iz = 0; iz < P; ++iz) {
+            // the P*P (iy, iz) grid lines of the particle, dealt round the group's lanes
+            for (int l = g; l < P * P; l += FIN_LANES) {
+                const int iy = l % P, iz = l / P;
                 int nz = km[2] - iz;
                 nz += (nz < 0) ? s : 0;
+                int ny = km[1] - iy;
+                ny += (ny < 0) ? s : 0;
+                R tz = th[2][0], dtz = dth[2][0], ty = th[1][0], dty = dth[1][0];
 #pragma unroll
-                for (int iy = 0; iy < P; ++iy) {
-                    int ny = km[1] - iy;
-                    ny += (ny < 0) ? s : 0;
-                    const size_t rowo = S.grid_off + ((size_t)nz * s + ny) * s;
-#pragma unroll
-                    for (int ix = 0; ix < P; ++ix) {
-                        int nx = km[0] - ix;
-                        nx += (nx < 0) ? s : 0;
-                        const R Q = PR::mixed ? (R)grid32[rowo + nx] : (R)grid[rowo + nx];
-                        e0 += dth[0][ix] * th[1][iy] * th[2][iz] * Q;
-                        e1 += th[0][ix] * dth[1][iy] * th[2][iz] * Q;
-                        e2 += th[0][ix] * th[1][iy] * dth[2][iz] * Q;
-                    }
+                for (int k = 1; k < P; ++k) {
+                    tz = (iz == k) ? th[2][k] : tz;
+                    dtz = (iz == k) ? dth[2][k] : dtz;
+                    ty = (iy == k) ? th[1][k] : ty;
+                    dty = (iy == k) ? dth[1][k] : dty;
                 }
-            }
-            Fx -= x.w * (double)e0 * S.dkdr[0] * S.epsfp;
-            Fy -= x.w * (double)e1 * S.dkdr[1] * S.epsfp;
-            Fz -= x.w * (double)e2 * S.dkdr[2] * S.epsfp;
-            if (S.lsurf) {
-                const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
-                Fx -= S.epsfp * (2.0 * fac) * x.w * sq[0];
-                Fy -= S.epsfp * (2.0 * fac) * x.w * sq[1];
-                Fz -= S.epsfp * (2.0 * fac) * x.w * sq[2];
+                const size_t rowo = S.grid_off + ((size_t)nz * s + ny) * s;
+                R a0 = 0, a1 = 0;
+#pragma unroll
+                for (int ix = 0; ix < P; ++ix) {
+                    int nx = km[0] - ix;
+                    nx += (nx < 0) ? s : 0;
+                    const R Q = PR::mixed ? (R)grid32[rowo + nx] : (R)grid[rowo + nx];
+                    a0 += dth[0][ix] * Q;
+                    a1 += th[0][ix] * Q;
+                }
+                e0 += a0 * ty * tz;
+                e1 += a1 * dty * tz;
+                e2 += a1 * ty * dtz;
             }
         }
-        // bonds of this particle (both ends of a bond compute it; counted once)
-        const int o = orig[i];
-        const int b1 = bptr[S.off + o + 1];
-        for (int b = bptr[S.off + o]; b < b1; ++b) {
+    }
+    // bonds of this particle (UBond), dealt round lanes 1.. of the group; both ends of a
+    // bond compute its force, its energy and virial are counted once (o < po)
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    if (i < T.i1 && g > 0) {
+        for (int b = bb0 + g - 1; b < bb1; b += FIN_LANES - 1) {
             const int po = bpart[b];
             const double4 xj = pos[inv[S.off + po]];
             double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
@@ -250,24 +276,50 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
             double fac = bk[b] * tp;
             const double u = fac * term;
             fac = -(pw * fac / r1);
-            Fx += fac * dx;
-            Fy += fac * dy;
-            Fz += fac * dz;
+            bx += fac * dx;
+            by += fac * dy;
+            bz += fac * dz;
             if (o < po) {
                 ub += u;
                 vb -= fac * r2;
             }
         }
+    }
+#pragma unroll
+    for (int m = FIN_LANES >> 1; m > 0; m >>= 1) {
+        e0 += __shfl_xor_sync(0xffffffffu, e0, m);
+        e1 += __shfl_xor_sync(0xffffffffu, e1, m);
+        e2 += __shfl_xor_sync(0xffffffffu, e2, m);
+        bx += __shfl_xor_sync(0xffffffffu, bx, m);
+        by += __shfl_xor_sync(0xffffffffu, by, m);
+        bz += __shfl_xor_sync(0xffffffffu, bz, m);
+    }
+    if (i < T.i1 && g == 0) {
+        double Fx = f0.x, Fy = f0.y, Fz = f0.z;
+        if (S.lewald) {
+            Fx -= x.w * (double)e0 * S.dkdr[0] * S.epsfp;
+            Fy -= x.w * (double)e1 * S.dkdr[1] * S.epsfp;
+            Fz -= x.w * (double)e2 * S.dkdr[2] * S.epsfp;
+            if (S.lsurf) {
+                const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
+                Fx -= S.epsfp * (2.0 * fac) * x.w * sq[0];
+                Fy -= S.epsfp * (2.0 * fac) * x.w * sq[1];
+                Fz -= S.epsfp * (2.0 * fac) * x.w * sq[2];
+            }
+        }
+        Fx += bx;
+        Fy += by;
+        Fz += bz;
         if (!isfinite(Fx) || !isfinite(Fy) || !isfinite(Fz)) raise_error(err, 7, T.sys, i, 0);
         ftot[i] = make_double4(Fx, Fy, Fz, 0.0);
         const double4 fo = make_double4(Fx * kForceFac, Fy * kForceFac, Fz * kForceFac, 0.0);
         forceo[i] = fo;
         if (mode == 1) {
-            const int t = S.type_off + typ[i];
+            const int t = S.type_off + tyi;
             const double mi = massip[t], hdt = 0.5 * S.dt;
-            const double4 ao = acc[i];
+            const double4 ao = aold;
             const double4 an = make_double4(mi * fo.x, mi * fo.y, mi * fo.z, 0.0);
-            double4 v = vel[i];
+            double4 v = vold;
             v.x = __dadd_rn(v.x, __dmul_rn(hdt, __dadd_rn(an.x, ao.x)));
             v.y = __dadd_rn(v.y, __dmul_rn(hdt, __dadd_rn(an.y, ao.y)));
             v.z = __dadd_rn(v.z, __dmul_rn(hdt, __dadd_rn(an.z, ao.z)));

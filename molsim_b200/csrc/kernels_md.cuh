@@ -44,14 +44,16 @@ __device__ __forceinline__ float3 gauss3(uint64_t seed, uint32_t particle, uint3
 // a chunk record R counts towards r2max2 iff R <= the prefix maximum P before
 // the chunk, so the chunk contributes max(A, max{R <= P}).
 // ---------------------------------------------------------------------------
-constexpr int SK_CHUNK = 1024, SK_THREADS = 256, SK_REC = 32;
+// 128 MOLSIM indices per chunk, one per thread: a 16000-particle system spreads
+// over 125 blocks.
+constexpr int SK_THREADS = 128, SK_PER = 1, SK_CHUNK = SK_THREADS * SK_PER, SK_REC = 32;
 struct SkinChunk {
     double bmax, amax;
     int nrec, pad;
     double rec[SK_REC];
 };
 
-// Block-wide exclusive prefix max over 256 threads (values >= 0).
+// Block-wide exclusive prefix max over the block's threads (values >= 0).
 __device__ __forceinline__ double block_excl_max(double v, double *sm)
 {
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
@@ -109,19 +111,19 @@ __device__ __forceinline__ int block_excl_sum_int(int v, int *sm, int *total)
 __device__ double chunk_nonrecord_max(const double *r2, int o0, int o1, double P, double *smd)
 {
     const int t = threadIdx.x;
-    double v[4], run = 0.0;
+    double v[SK_PER], run = 0.0, tmax = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int o = o0 + 4 * t + k;
+    for (int k = 0; k < SK_PER; ++k) {
+        int o = o0 + SK_PER * t + k;
         v[k] = (o < o1) ? r2[o] : 0.0;
+        tmax = fmax(tmax, v[k]);
     }
-    double tmax = fmax(fmax(v[0], v[1]), fmax(v[2], v[3]));
     double pre = fmax(P, block_excl_max(tmax, smd));
     double best = 0.0;
     run = pre;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int o = o0 + 4 * t + k;
+    for (int k = 0; k < SK_PER; ++k) {
+        int o = o0 + SK_PER * t + k;
         if (o < o1) {
             if (v[k] > run) run = v[k];
             else best = fmax(best, v[k]);
@@ -130,10 +132,10 @@ __device__ double chunk_nonrecord_max(const double *r2, int o0, int o1, double P
     return block_max(best, smd);
 }
 
-// Chunk summary of four consecutive MOLSIM-order skin values per thread, and,
+// Chunk summary of SK_PER consecutive MOLSIM-order skin values per thread, and,
 // in the last chunk of the system to finish, the combination in MOLSIM order
 // and the rebuild decision (NList, Src/nlist.F90:600-613).
-__device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[4], int o0, int o1,
+__device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[SK_PER], int o0, int o1,
                            const double *__restrict__ r2o, SkinChunk *__restrict__ sc,
                            unsigned *__restrict__ sysdone, int *__restrict__ flag,
                            long long *__restrict__ nrebuild, double *__restrict__ skinout,
@@ -143,14 +145,16 @@ __device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[4],
     __shared__ int smi[SK_THREADS / 32];
     __shared__ bool last;
     const int t = threadIdx.x;
-    double tmax = fmax(fmax(v[0], v[1]), fmax(v[2], v[3]));
+    double tmax = 0.0;
+#pragma unroll
+    for (int k = 0; k < SK_PER; ++k) tmax = fmax(tmax, v[k]);
     double run = block_excl_max(tmax, smd);
     double amax = 0.0;
     int nrec = 0;
-    double recv[4];
+    double recv[SK_PER];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int o = o0 + 4 * t + k;
+    for (int k = 0; k < SK_PER; ++k) {
+        const int o = o0 + SK_PER * t + k;
         if (o < o1) {
             if (v[k] > run) { run = v[k]; recv[nrec++] = v[k]; }
             else amax = fmax(amax, v[k]);
@@ -173,7 +177,7 @@ __device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[4],
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // Combine the system's chunks in MOLSIM order, 256 chunks per pass.
+    // Combine the system's chunks in MOLSIM order, SK_THREADS chunks per pass.
     const int c0 = S.chunk_off;
     double carry = 0.0, m2 = 0.0;
     __shared__ int novf;
@@ -234,7 +238,7 @@ __device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[4],
 // Velocity Verlet, position half (Src/md.F90:286-298) fused with NList's skin
 // test: drostep = dt*rod + (dt*dt/2)*rodd; ro += drostep; PBC(ro);
 // drosum += drostep (Src/nlist.F90:603-604).  Each block is one skin chunk of
-// 1024 consecutive MOLSIM indices, so the skin values arrive in MOLSIM order;
+// SK_CHUNK consecutive MOLSIM indices, so the skin values arrive in MOLSIM order;
 // particles are reached through inv[].  Products and sums round separately
 // (no FMA) so positions follow MOLSIM's arithmetic.  Also refreshes the FP32
 // position mirror used by the mixed-precision kernels.
@@ -249,10 +253,10 @@ __global__ void __launch_bounds__(SK_THREADS) k_vv_skin(
     const int4 C = chunks[blockIdx.x];
     const SysDev &S = sysv[C.x];
     const double dt = S.dt, fac = __dmul_rn(0.5, __dmul_rn(dt, dt));
-    double v[4];
+    double v[SK_PER];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int o = C.y + 4 * threadIdx.x + k;
+    for (int k = 0; k < SK_PER; ++k) {
+        const int o = C.y + SK_PER * threadIdx.x + k;
         v[k] = 0.0;
         if (o < C.z) {
             const int i = inv[o];
@@ -293,10 +297,10 @@ __global__ void __launch_bounds__(SK_THREADS) k_bd_skin(
 {
     const int4 C = chunks[blockIdx.x];
     const SysDev &S = sysv[C.x];
-    double v[4];
+    double v[SK_PER];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int o = C.y + 4 * threadIdx.x + k;
+    for (int k = 0; k < SK_PER; ++k) {
+        const int o = C.y + SK_PER * threadIdx.x + k;
         v[k] = 0.0;
         if (o < C.z) {
             const int i = inv[o];
