@@ -140,6 +140,13 @@ int  msg_get_forces(msg_handle *h, int32_t isys, double *force, double *forceo);
 /* MSG_TUNE_PAIR_UNROLL (lean kernel): row entries each lane keeps in flight,
  * 1, 2 (default) or 4.  Results do not depend on it. */
 #define MSG_TUNE_PAIR_UNROLL 3
+/* MSG_TUNE_OVERLAP: 1 (default) runs the pair kernel on a second stream beside
+ * the SPME chain, 0 runs them one after the other.  MSG_TUNE_PAIR_BLOCKS: pair
+ * blocks per SM of the lean kernel (0, the default: as many as fit, or 2 when
+ * the pair kernel runs beside the SPME chain).  Neither
+ * changes results. */
+#define MSG_TUNE_OVERLAP 4
+#define MSG_TUNE_PAIR_BLOCKS 5
 int  msg_tune(msg_handle *h, int32_t key, int32_t value);
 
 /* rodd = massip * forceo (GetLinAcc) from the last msg_utotal. */

@@ -111,6 +111,11 @@ struct msg_handle {
     std::vector<int> hn;
     std::string err;
     cudaStream_t st = nullptr;
+    // second stream of the step: the pair kernel runs there beside the SPME chain
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int overlap = 1;                 // pair kernel concurrent with spread/FFT/influence
+    int pair_per_sm = 0;             // pair blocks per SM (0: as many as fit; 2 when overlapped)
     int dev = 0;
     // particles (double-buffered where the rebuild permutes)
     int cur = 0;
@@ -334,8 +339,12 @@ static void free_all(msg_handle *h)
     for (cudaEvent_t e : h->pend_a) cudaEventDestroy(e);
     for (cudaEvent_t e : h->pend_b) cudaEventDestroy(e);
     h->evpool.clear();
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->st2) cudaStreamDestroy(h->st2);
     if (h->st) cudaStreamDestroy(h->st);
-    h->st = nullptr;
+    h->st = h->st2 = nullptr;
+    h->ev_fork = h->ev_join = nullptr;
 }
 
 msg_handle::~msg_handle()
@@ -362,6 +371,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     if (!dry) {
         CK(cudaGetDevice(&dev));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     }
     hs.resize(n);
     hn.resize(n);
@@ -1014,15 +1026,29 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
 template <class PR>
 static void launch_forces(msg_handle *h, int mode, bool record)
 {
+    // The pair kernel and the SPME chain (spread, FFT, influence, FFT) read
+    // different inputs and add into different accumulators: the pair kernel runs
+    // on a second stream beside the chain and finalize waits for both.  (Per-kernel
+    // timers need one stream, so timing serialises them.)
+    const bool par = h->overlap && h->any_ewald && !h->timing;
+    cudaStream_t ps = h->st;
+    if (par) {
+        CK(cudaEventRecord(h->ev_fork, h->st));
+        CK(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
+        ps = h->st2;
+    }
     h->tbeg(TM_PAIR);
     const typename PR::V4 *pp =
         reinterpret_cast<const typename PR::V4 *>(PR::mixed ? (const void *)h->posfx : (const void *)h->pos[0]);
     const typename PR::R *tzp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tz32 : (const void *)h->tz);
     const typename PR::R *tcp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tc32 : (const void *)h->tc);
     if (PR::mixed && h->pair_lean) {
-        const int grid = std::max(1, std::min(h->nptask, h->pair_blocks_lean));
+        // beside the SPME chain the pair kernel leaves room on each SM for the chain's blocks
+        const int per_sm = h->pair_per_sm > 0 ? h->pair_per_sm : (par ? 2 : 0);
+        const int cap = per_sm > 0 ? std::min(h->pair_blocks_lean, h->nsm * per_sm) : h->pair_blocks_lean;
+        const int grid = std::max(1, std::min(h->nptask, cap));
 #define MSG_LEAN(NTV, UV)                                                                                   \
-    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem_m, h->st>>>(h->dsys, h->ptask, h->nptask, h->posfx,   \
+    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem_m, ps>>>(h->dsys, h->ptask, h->nptask, h->posfx,      \
                                                                    h->typ[0], h->nbl, h->nnb, h->ptmap,    \
                                                                    h->ptab, h->tc32, h->bkz, h->fsr,       \
                                                                    h->eacc, h->errw)
@@ -1033,11 +1059,11 @@ static void launch_forces(msg_handle *h, int mode, bool record)
         }
 #undef MSG_LEAN
     } else if (h->max_npt <= 2)
-        k_pair<PR, 2><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
+        k_pair<PR, 2><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, ps>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
                                                               h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
                                                               h->eacc, h->errw);
     else
-        k_pair<PR, 4><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, h->st>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
+        k_pair<PR, 4><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, ps>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
                                                               h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
                                                               h->eacc, h->errw);
     h->tend(TM_PAIR);
@@ -1048,6 +1074,10 @@ static void launch_forces(msg_handle *h, int mode, bool record)
         case 5: launch_spme<5, PR>(h); break;
         default: launch_spme<6, PR>(h); break;
         }
+    }
+    if (par) {
+        CK(cudaEventRecord(h->ev_join, h->st2));
+        CK(cudaStreamWaitEvent(h->st, h->ev_join, 0));
     }
     switch (h->order) {
     case 4: launch_finalize<4, PR>(h, mode, record); break;
@@ -1544,6 +1574,22 @@ extern "C" int msg_tune(msg_handle *h, int32_t key, int32_t value)
             h->drop_graph();
             h->pair_unroll = value;
             if (h->prec == MSG_PREC_MIXED) h->set_lean_grid(h->nsm);
+        }
+        return MSG_OK;
+    }
+    if (key == MSG_TUNE_OVERLAP) {
+        if (value != 0 && value != 1) return MSG_ERR_ARG;
+        if (h->overlap != value) {
+            h->drop_graph();
+            h->overlap = value;
+        }
+        return MSG_OK;
+    }
+    if (key == MSG_TUNE_PAIR_BLOCKS) {
+        if (value < 0 || value > 32) return MSG_ERR_ARG;
+        if (h->pair_per_sm != value) {
+            h->drop_graph();
+            h->pair_per_sm = value;
         }
         return MSG_OK;
     }
