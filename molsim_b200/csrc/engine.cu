@@ -943,21 +943,19 @@ void msg_handle::enqueue_rebuild()
 {
     // cur stays 0: rebuilt systems are permuted into the [1] buffers and copied home
     tbeg(TM_REBUILD);
-    k_rb_keys<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], orig[0], cellid, k0, v0);
-    const bool in1 = radix_sort_pairs(k0, v0, k1, v1, rhist, ntot, cell_bits, st);
+    k_rb_keys<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], orig[0], cellid, k0, v0, cstart, cend, ncell_tot);
+    int nsort = 0;
+    const bool in1 = radix_sort_pairs(k0, v0, k1, v1, rhist, ntot, cell_bits, st, &nsort);
     const uint32_t *sk = in1 ? k1 : k0, *sv = in1 ? v1 : v0;
     k_permute<<<nt128, 128, 0, st>>>(dsys, t128, flag, sk, sv, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1],
-                                      fo[0], fo[1], typ[0], typ[1], orig[0], orig[1], cellid, inv);
-    k_copyback<<<nt128, 128, 0, st>>>(t128, flag, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1], fo[0], fo[1],
-                                       typ[0], typ[1], orig[0], orig[1], dsum[0]);
-    k_clear_cells<<<(ncell_tot + 255) / 256, 256, 0, st>>>(cstart, cend, ncell_tot);
-    k_cellrange<<<(ntot + 255) / 256, 256, 0, st>>>(cellid, sysid, flag, ntot, cstart, cend);
+                                      fo[0], fo[1], typ[0], typ[1], orig[0], orig[1], cellid, inv, cstart, cend,
+                                      ntot);
+    k_copyback<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1], fo[0],
+                                       fo[1], typ[0], typ[1], orig[0], orig[1], dsum[0], posfx);
     k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[0], typ[0], cellid, cstart, cend, nbl,
                                                      nnb, ntot, nmaxrow, errw);
-    // positions were permuted: refresh the FP32 mirror of rebuilt systems
-    k_mirror<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], posfx);
     tend(TM_REBUILD);
-    launches += 7 + 3 * ((cell_bits + 7) / 8);
+    launches += 4 + nsort;
 }
 
 template <int P, class PR>

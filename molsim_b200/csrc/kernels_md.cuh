@@ -354,11 +354,17 @@ __device__ __forceinline__ int cell_coord(double x, double half, double boxi, in
     return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
 }
 
+// Also empties every cell range (k_permute refills those of rebuilt systems).
 __global__ void __launch_bounds__(128) k_rb_keys(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
                                                 const int *__restrict__ flag, const double4 *__restrict__ pos,
                                                 const int *__restrict__ orig, const int *__restrict__ cellid,
-                                                uint32_t *__restrict__ key, uint32_t *__restrict__ val)
+                                                uint32_t *__restrict__ key, uint32_t *__restrict__ val,
+                                                int *__restrict__ cstart, int *__restrict__ cend, int ncell)
 {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        cstart[c] = 0;
+        cend[c] = 0;
+    }
     const Tile T = tiles[blockIdx.x];
     const SysDev &S = sysv[T.sys];
     const int i = T.i0 + threadIdx.x;
@@ -378,8 +384,9 @@ __global__ void __launch_bounds__(128) k_rb_keys(const SysDev *__restrict__ sysv
 }
 
 // Gather the per-particle arrays of rebuilt systems into the sorted order
-// (into scratch buffers; k_copyback moves them home).  Systems that are not
-// rebuilt keep their order, so their particles are not touched.
+// (into scratch buffers; k_copyback moves them home) and mark where each of
+// their cells starts and ends in it.  Systems that are not rebuilt keep their
+// order, so their particles are not touched.
 __global__ void __launch_bounds__(128) k_permute(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
                                                 const int *__restrict__ flag, const uint32_t *__restrict__ skey,
                                                 const uint32_t *__restrict__ sval,
@@ -389,13 +396,17 @@ __global__ void __launch_bounds__(128) k_permute(const SysDev *__restrict__ sysv
                                                 const double4 *__restrict__ fo0, double4 *__restrict__ fo1,
                                                 const int *__restrict__ typ0, int *__restrict__ typ1,
                                                 const int *__restrict__ orig0, int *__restrict__ orig1,
-                                                int *__restrict__ cellid, int *__restrict__ inv)
+                                                int *__restrict__ cellid, int *__restrict__ inv,
+                                                int *__restrict__ cstart, int *__restrict__ cend, int n)
 {
     const Tile T = tiles[blockIdx.x];
     if (!flag[T.sys]) return;
     const SysDev &S = sysv[T.sys];
     const int j = T.i0 + threadIdx.x;
     if (j >= T.i1) return;
+    const int c = (int)skey[j];
+    if (j == 0 || (int)skey[j - 1] != c) cstart[c] = j;
+    if (j == n - 1 || (int)skey[j + 1] != c) cend[c] = j + 1;
     const int i = (int)sval[j];
     pos1[j] = pos0[i];
     vel1[j] = vel0[i];
@@ -408,39 +419,31 @@ __global__ void __launch_bounds__(128) k_permute(const SysDev *__restrict__ sysv
     inv[S.off + o] = j;
 }
 
-// Home the permuted arrays and reset drosum (NList: drosum = Zero at a rebuild).
-__global__ void __launch_bounds__(128) k_copyback(const Tile *__restrict__ tiles, const int *__restrict__ flag,
+// Home the permuted arrays, reset drosum (NList: drosum = Zero at a rebuild)
+// and refresh the fixed-point mirror of the moved positions.
+__global__ void __launch_bounds__(128) k_copyback(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                 const int *__restrict__ flag,
                                                  double4 *__restrict__ pos0, const double4 *__restrict__ pos1,
                                                  double4 *__restrict__ vel0, const double4 *__restrict__ vel1,
                                                  double4 *__restrict__ acc0, const double4 *__restrict__ acc1,
                                                  double4 *__restrict__ fo0, const double4 *__restrict__ fo1,
                                                  int *__restrict__ typ0, const int *__restrict__ typ1,
                                                  int *__restrict__ orig0, const int *__restrict__ orig1,
-                                                 double4 *__restrict__ dsum)
+                                                 double4 *__restrict__ dsum, int4 *__restrict__ posfx)
 {
     const Tile T = tiles[blockIdx.x];
     if (!flag[T.sys]) return;
     const int j = T.i0 + threadIdx.x;
     if (j >= T.i1) return;
-    pos0[j] = pos1[j];
+    const double4 x = pos1[j];
+    pos0[j] = x;
+    posfx[j] = fx_pos(x, sysv[T.sys]);
     vel0[j] = vel1[j];
     acc0[j] = acc1[j];
     fo0[j] = fo1[j];
     typ0[j] = typ1[j];
     orig0[j] = orig1[j];
     dsum[j] = make_double4(0.0, 0.0, 0.0, 0.0);
-}
-
-// Fixed-point position mirror of rebuilt systems after their permutation.
-__global__ void __launch_bounds__(128) k_mirror(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                               const int *__restrict__ flag, const double4 *__restrict__ pos,
-                                               int4 *__restrict__ posfx)
-{
-    const Tile T = tiles[blockIdx.x];
-    if (!flag[T.sys]) return;
-    const int j = T.i0 + threadIdx.x;
-    if (j >= T.i1) return;
-    posfx[j] = fx_pos(pos[j], sysv[T.sys]);
 }
 
 __global__ void k_mirror_range(const SysDev *__restrict__ sysv, int sys, const double4 *__restrict__ pos,
@@ -450,25 +453,6 @@ __global__ void k_mirror_range(const SysDev *__restrict__ sysv, int sys, const d
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= S.n) return;
     posfx[S.off + j] = fx_pos(pos[S.off + j], S);
-}
-
-__global__ void k_clear_cells(int *__restrict__ cstart, int *__restrict__ cend, int n)
-{
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n) {
-        cstart[c] = 0;
-        cend[c] = 0;
-    }
-}
-
-__global__ void k_cellrange(const int *__restrict__ cellid, const int *__restrict__ sys,
-                            const int *__restrict__ flag, int n, int *__restrict__ cstart, int *__restrict__ cend)
-{
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n || !flag[sys[j]]) return;
-    const int c = cellid[j];
-    if (j == 0 || cellid[j - 1] != c) cstart[c] = j;
-    if (j == n - 1 || cellid[j + 1] != c) cend[c] = j + 1;
 }
 
 // Stencil of neighbour cells along one dimension: the three cells c-1, c, c+1

@@ -20,20 +20,21 @@ constexpr int RS_TILE = RS_THREADS * RS_ROUNDS;
 constexpr int RS_BINS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
 
+template <int NB>
 __global__ void __launch_bounds__(RS_THREADS) rs_hist(const uint32_t *__restrict__ keys, int n,
                                                       int shift, uint32_t *__restrict__ hist)
 {
-    __shared__ uint32_t cnt[RS_BINS];
-    cnt[threadIdx.x] = 0;
+    __shared__ uint32_t cnt[NB];
+    for (int b = threadIdx.x; b < NB; b += RS_THREADS) cnt[b] = 0;
     __syncthreads();
     const int base = blockIdx.x * RS_TILE;
 #pragma unroll
     for (int k = 0; k < RS_ROUNDS; ++k) {
         int idx = base + k * RS_THREADS + threadIdx.x;
-        if (idx < n) atomicAdd(&cnt[(keys[idx] >> shift) & (RS_BINS - 1)], 1u);
+        if (idx < n) atomicAdd(&cnt[(keys[idx] >> shift) & (NB - 1)], 1u);
     }
     __syncthreads();
-    hist[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
+    for (int b = threadIdx.x; b < NB; b += RS_THREADS) hist[b * gridDim.x + blockIdx.x] = cnt[b];
 }
 
 // Exclusive scan of len entries in place, one block of 1024 threads.
@@ -43,7 +44,14 @@ __global__ void __launch_bounds__(1024) rs_scan(uint32_t *__restrict__ a, int le
     const int t = threadIdx.x, per = (len + 1023) / 1024;
     const int b = t * per, e = min(len, b + per);
     uint32_t s = 0;
-    for (int i = b; i < e; ++i) s += a[i];
+    // eight independent loads in flight per thread
+    for (int i0 = b; i0 < e; i0 += 8) {
+        uint32_t x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = (i0 + k < e) ? a[i0 + k] : 0u;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += x[k];
+    }
     // inclusive warp scan of the per-thread sums
     uint32_t v = s;
     const int lane = t & 31, w = t >> 5;
@@ -65,25 +73,33 @@ __global__ void __launch_bounds__(1024) rs_scan(uint32_t *__restrict__ a, int le
     }
     __syncthreads();
     uint32_t run = v - s + (w > 0 ? wsum[w - 1] : 0u);
-    for (int i = b; i < e; ++i) {
-        uint32_t x = a[i];
-        a[i] = run;
-        run += x;
+    for (int i0 = b; i0 < e; i0 += 8) {
+        uint32_t x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = (i0 + k < e) ? a[i0 + k] : 0u;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (i0 + k < e) a[i0 + k] = run;
+            run += x[k];
+        }
     }
 }
 
+template <int NB>
 __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t *__restrict__ kin,
                                                          const uint32_t *__restrict__ vin,
                                                          uint32_t *__restrict__ kout,
                                                          uint32_t *__restrict__ vout, int n, int shift,
                                                          const uint32_t *__restrict__ offs)
 {
-    __shared__ uint32_t base[RS_BINS];
-    __shared__ uint32_t wcnt[RS_WARPS][RS_BINS];
+    __shared__ uint32_t base[NB];
+    __shared__ uint32_t wcnt[RS_WARPS][NB];
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-    base[t] = offs[t * gridDim.x + blockIdx.x];
+    for (int b = t; b < NB; b += RS_THREADS) {
+        base[b] = offs[b * gridDim.x + blockIdx.x];
 #pragma unroll
-    for (int ww = 0; ww < RS_WARPS; ++ww) wcnt[ww][t] = 0;
+        for (int ww = 0; ww < RS_WARPS; ++ww) wcnt[ww][b] = 0;
+    }
     __syncthreads();
     const int blockbase = blockIdx.x * RS_TILE;
     const unsigned lt = (1u << lane) - 1u;
@@ -93,7 +109,7 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t *__restr
         const bool valid = idx < n;
         const uint32_t key = valid ? kin[idx] : 0u;
         const uint32_t val = valid ? vin[idx] : 0u;
-        const uint32_t d = valid ? ((key >> shift) & (RS_BINS - 1)) : (uint32_t)RS_BINS;
+        const uint32_t d = valid ? ((key >> shift) & (NB - 1)) : (uint32_t)NB;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const int lrank = __popc(peers & lt);
         if (valid && lane == __ffs(peers) - 1) wcnt[w][d] = (uint32_t)__popc(peers);
@@ -106,32 +122,37 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t *__restr
             vout[pos] = val;
         }
         __syncthreads();
-        uint32_t tot = 0;
+        for (int b = t; b < NB; b += RS_THREADS) {
+            uint32_t tot = 0;
 #pragma unroll
-        for (int ww = 0; ww < RS_WARPS; ++ww) {
-            tot += wcnt[ww][t];
-            wcnt[ww][t] = 0;
+            for (int ww = 0; ww < RS_WARPS; ++ww) {
+                tot += wcnt[ww][b];
+                wcnt[ww][b] = 0;
+            }
+            base[b] += tot;
         }
-        base[t] += tot;
         __syncthreads();
     }
 }
 
-// Sort n pairs by the low `bits` bits of the key.  k0/v0 hold the input; k1/v1
-// are scratch of the same size; hist needs 256*ceil(n/1024) entries.  Returns
-// true when the sorted data ended in (k1, v1), false when in (k0, v0).
+// Sort n pairs by the low `bits` bits of the key in 8-bit passes.  k0/v0 hold
+// the input; k1/v1 are scratch of the same size; hist needs 256*ceil(n/1024)
+// entries.  Returns true when the sorted data ended in (k1, v1), false when in
+// (k0, v0).  Sets *launches.
 inline bool radix_sort_pairs(uint32_t *k0, uint32_t *v0, uint32_t *k1, uint32_t *v1, uint32_t *hist,
-                             int n, int bits, cudaStream_t st)
+                             int n, int bits, cudaStream_t st, int *launches = nullptr)
 {
     const int nb = (n + RS_TILE - 1) / RS_TILE;
-    bool flip = false;
+    if (launches) *launches = 0;
     if (n <= 0) return false;
+    bool flip = false;
     for (int shift = 0; shift < bits; shift += 8) {
         uint32_t *ki = flip ? k1 : k0, *vi = flip ? v1 : v0;
         uint32_t *ko = flip ? k0 : k1, *vo = flip ? v0 : v1;
-        rs_hist<<<nb, RS_THREADS, 0, st>>>(ki, n, shift, hist);
+        rs_hist<RS_BINS><<<nb, RS_THREADS, 0, st>>>(ki, n, shift, hist);
         rs_scan<<<1, 1024, 0, st>>>(hist, RS_BINS * nb);
-        rs_scatter<<<nb, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n, shift, hist);
+        rs_scatter<RS_BINS><<<nb, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n, shift, hist);
+        if (launches) *launches += 3;
         flip = !flip;
     }
     return flip;
