@@ -162,7 +162,7 @@ struct msg_handle {
     int pair_unroll = 2;                              // k_pair_m: row entries in flight per lane
     int nsm = 148;
     double *massip = nullptr, *massp = nullptr, *fac1 = nullptr, *fac2 = nullptr;
-    int has_bd = 0;
+    int has_bd = 0, has_bonds = 0;
     // bonds
     int *bptr = nullptr, *bpart = nullptr, *bpw = nullptr;
     double *bk = nullptr, *beq = nullptr;
@@ -455,6 +455,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         pt_tot += S.natat;
         ptmap_tot += p.npt * p.npt;
         nbond_tot += (size_t)std::max(0, (int)p.nbond);
+        if (p.nbond > 0) has_bonds = 1;
         ntot += p.np;
         hn[s] = p.np;
         H[s].p = p;
@@ -1064,6 +1065,11 @@ static void launch_forces(msg_handle *h, int mode, bool record)
         k_pair<PR, 4><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, ps>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
                                                               h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
                                                               h->eacc, h->errw);
+    if (h->has_bonds) {
+        k_bonds<<<h->nt128, 128, 0, ps>>>(h->dsys, h->t128, h->pos[0], h->orig[0], h->inv, h->bptr, h->bpart, h->bk,
+                                          h->beq, h->bpw, h->fsr, h->eacc);
+        h->launches += 1;
+    }
     h->tend(TM_PAIR);
     h->launches += 1;
     if (h->any_ewald) {

@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence(const SysDev *__rest
 
 // ---------------------------------------------------------------------------
 // Finalize: SPME force gather (Src/energy.F90:1258-1285), surface term
-// (Src/energy.F90:1349-1371), bonds (UBond, Src/energy.F90:5335-5387), the
+// (Src/energy.F90:1349-1371) on top of the pair and bond forces, the
 // UTotal unit conversion into forceo (Src/energy.F90:405-419) and, for MD,
 // the velocity half of VelVer with GetLinAcc (Src/md.F90:349-358, 601-617)
 // and GetKinEnergy's partial sum.  The last block of each system then sums
@@ -164,6 +164,71 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence(const SysDev *__rest
 //   0 utot, 1 utwob(0), 2..11 utwob(1..10), 12 urec, 13 ubond, 14 virial, 15 ekin
 // mode 0: forces only; 1: + velocity Verlet update.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// UBond (Src/energy.F90:5335-5387): u += k'(r - r0)^p, F = -p k'(r - r0)^(p-1)/r d.
+// Runs after the pair kernel on its stream, beside the SPME chain: each
+// particle adds the forces of its bonds (both ends of a bond compute it) to
+// its short-range force; a bond's energy and virial count once (o < po).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_bonds(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                              const double4 *__restrict__ pos, const int *__restrict__ orig,
+                                              const int *__restrict__ inv, const int *__restrict__ bptr,
+                                              const int *__restrict__ bpart, const double *__restrict__ bk,
+                                              const double *__restrict__ beq, const int *__restrict__ bpw,
+                                              double4 *__restrict__ fsr, long long *__restrict__ eacc)
+{
+    __shared__ double red[2][4];
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    const int i = T.i0 + threadIdx.x;
+    double ub = 0.0, vb = 0.0;
+    if (i < T.i1) {
+        const int o = orig[i];
+        const int b0 = bptr[S.off + o], b1 = bptr[S.off + o + 1];
+        if (b1 > b0) {
+            const double4 x = pos[i];
+            double bx = 0.0, by = 0.0, bz = 0.0;
+            for (int b = b0; b < b1; ++b) {
+                const int po = bpart[b];
+                const double4 xj = pos[inv[S.off + po]];
+                double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
+                const double r2 = pbcr2_exact(dx, dy, dz, S), r1 = sqrt(r2);
+                const double term = r1 - beq[b];
+                const int pw = bpw[b];
+                double tp = 1.0;
+                for (int k = 0; k < pw - 1; ++k) tp *= term;
+                double fac = bk[b] * tp;
+                const double u = fac * term;
+                fac = -(pw * fac / r1);
+                bx += fac * dx;
+                by += fac * dy;
+                bz += fac * dz;
+                if (o < po) {
+                    ub += u;
+                    vb -= fac * r2;
+                }
+            }
+            double4 f = fsr[i];
+            f.x += bx;
+            f.y += by;
+            f.z += bz;
+            fsr[i] = f;
+        }
+    }
+    ub = warp_sum(ub);
+    vb = warp_sum(vb);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[0][w] = ub;
+        red[1][w] = vb;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        const double a = red[threadIdx.x][0] + red[threadIdx.x][1] + red[threadIdx.x][2] + red[threadIdx.x][3];
+        if (a != 0.0) acc_add(eacc + (size_t)T.sys * EA_N + EA_UBOND + threadIdx.x, a);
+    }
+}
+
 constexpr int NPART_FIN = 4;    // ubond, virbond, ekin, spare
 constexpr int ESZ = 16;
 constexpr int FIN_LANES = 4;                      // lanes per particle in the grid gather
@@ -207,10 +272,9 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     double4 x = make_double4(0.0, 0.0, 0.0, 0.0);
     // the particle's own loads go out before the gather so that their latencies overlap
     double4 f0 = make_double4(0.0, 0.0, 0.0, 0.0), vold = f0, aold = f0;
-    int o = 0, tyi = 0, bb0 = 0, bb1 = 0;
+    int tyi = 0;
     if (i < T.i1) {
         x = pos[i];
-        o = orig[i];
         if (g == 0) {
             f0 = fsr[i];
             if (mode == 1) {
@@ -218,9 +282,6 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 vold = vel[i];
                 aold = acc[i];
             }
-        } else {
-            bb0 = bptr[S.off + o];
-            bb1 = bptr[S.off + o + 1];
         }
         if (S.lewald) {
             const int s = S.s;
@@ -260,39 +321,11 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
             }
         }
     }
-    // bonds of this particle (UBond), dealt round lanes 1.. of the group; both ends of a
-    // bond compute its force, its energy and virial are counted once (o < po)
-    double bx = 0.0, by = 0.0, bz = 0.0;
-    if (i < T.i1 && g > 0) {
-        for (int b = bb0 + g - 1; b < bb1; b += FIN_LANES - 1) {
-            const int po = bpart[b];
-            const double4 xj = pos[inv[S.off + po]];
-            double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
-            const double r2 = pbcr2_exact(dx, dy, dz, S), r1 = sqrt(r2);
-            const double term = r1 - beq[b];
-            const int pw = bpw[b];
-            double tp = 1.0;
-            for (int k = 0; k < pw - 1; ++k) tp *= term;
-            double fac = bk[b] * tp;
-            const double u = fac * term;
-            fac = -(pw * fac / r1);
-            bx += fac * dx;
-            by += fac * dy;
-            bz += fac * dz;
-            if (o < po) {
-                ub += u;
-                vb -= fac * r2;
-            }
-        }
-    }
 #pragma unroll
     for (int m = FIN_LANES >> 1; m > 0; m >>= 1) {
         e0 += __shfl_xor_sync(0xffffffffu, e0, m);
         e1 += __shfl_xor_sync(0xffffffffu, e1, m);
         e2 += __shfl_xor_sync(0xffffffffu, e2, m);
-        bx += __shfl_xor_sync(0xffffffffu, bx, m);
-        by += __shfl_xor_sync(0xffffffffu, by, m);
-        bz += __shfl_xor_sync(0xffffffffu, bz, m);
     }
     if (i < T.i1 && g == 0) {
         double Fx = f0.x, Fy = f0.y, Fz = f0.z;
@@ -307,9 +340,6 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 Fz -= S.epsfp * (2.0 * fac) * x.w * sq[2];
             }
         }
-        Fx += bx;
-        Fy += by;
-        Fz += bz;
         if (!isfinite(Fx) || !isfinite(Fy) || !isfinite(Fz)) raise_error(err, 7, T.sys, i, 0);
         ftot[i] = make_double4(Fx, Fy, Fz, 0.0);
         const double4 fo = make_double4(Fx * kForceFac, Fy * kForceFac, Fz * kForceFac, 0.0);
