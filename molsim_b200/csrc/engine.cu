@@ -139,6 +139,8 @@ struct msg_handle {
     // work lists
     Tile *t128 = nullptr;
     PairTask *ptask = nullptr;
+    int2 *psrange = nullptr;          // lean pair kernel: each system's tasks [first, end)
+    int *psched = nullptr;            // its per-system task counters and finished-block counter
     int nt128 = 0, nptask = 0, max_npt = 1;
     int4 *chunks = nullptr, *infl = nullptr;
     int nchunk = 0, ninfl = 0;
@@ -239,6 +241,7 @@ struct msg_handle {
     void release_fft();
     int pair_blocks_max = 1, pair_blocks_lean = 1, pair_shift = 0;
     std::vector<PairTask> make_pair_tasks(int shift) const;
+    void set_pair_chunks(const std::vector<PairTask> &pt, bool replace);
     void set_pair_lanes(int shift);
     void set_lean_grid(int nsm);
 
@@ -324,7 +327,7 @@ static void free_all(msg_handle *h)
                     h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
                     h->sysid, h->fsr, h->ftot, h->posfx, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
                     h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
-                    h->t128, h->ptask, h->chunks, h->infl, h->eacc, h->esys,
+                    h->t128, h->ptask, h->psrange, h->psched, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys};
@@ -711,6 +714,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         }
         pt16 = make_pair_tasks(0);
         nptask = (int)pt16.size();
+        set_pair_chunks(pt16, false);
+        psched = dalloc<int>(n + 1);
         this->t128 = dalloc<Tile>(a128.size());
         ptask = dalloc<PairTask>(pt16.size());
         chunks = dalloc<int4>(ch.size());
@@ -851,6 +856,20 @@ std::vector<PairTask> msg_handle::make_pair_tasks(int shift) const
     return pt;
 }
 
+// Each system's task range for the lean pair kernel's per-system counters.
+void msg_handle::set_pair_chunks(const std::vector<PairTask> &pt, bool replace)
+{
+    std::vector<int2> r(nsys, make_int2(0, 0));
+    for (size_t a = 0; a < pt.size();) {
+        const int end = pt[a].send;
+        r[pt[a].sys] = make_int2((int)a, end);
+        a = (size_t)end;
+    }
+    if (replace) dfree(psrange);
+    psrange = dalloc<int2>(nsys);
+    up(psrange, r.data(), r.size() * sizeof(int2));
+}
+
 void msg_handle::set_pair_lanes(int shift)
 {
     if (shift == pair_shift) return;
@@ -861,6 +880,7 @@ void msg_handle::set_pair_lanes(int shift)
     ptask = dalloc<PairTask>(pt.size());
     up(ptask, pt.data(), pt.size() * sizeof(PairTask));
     nptask = (int)pt.size();
+    set_pair_chunks(pt, true);
     pair_grid = std::max(1, std::min(nptask, pair_blocks_max));
     pair_shift = shift;
     CK(cudaStreamSynchronize(st));
@@ -1047,7 +1067,8 @@ static void launch_forces(msg_handle *h, int mode, bool record)
         const int cap = per_sm > 0 ? std::min(h->pair_blocks_lean, h->nsm * per_sm) : h->pair_blocks_lean;
         const int grid = std::max(1, std::min(h->nptask, cap));
 #define MSG_LEAN(NTV, UV)                                                                                   \
-    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem_m, ps>>>(h->dsys, h->ptask, h->nptask, h->posfx,      \
+    k_pair_m<NTV, UV><<<grid, PAIR_BLOCK, h->pair_smem_m, ps>>>(h->dsys, h->ptask, h->psrange, h->nsys,        \
+                                                                h->nptask, h->psched, h->posfx,           \
                                                                    h->typ[0], h->nbl, h->nnb, h->ptmap,    \
                                                                    h->ptab, h->tc32, h->bkz, h->fsr,       \
                                                                    h->eacc, h->errw)
@@ -1297,6 +1318,7 @@ int msg_handle::check()
         CK(cudaMemsetAsync(fdone, 0, sizeof(unsigned) * nsys, st));
         CK(cudaMemsetAsync(sysdone, 0, sizeof(unsigned) * nsys, st));
         CK(cudaMemsetAsync(rdone, 0, sizeof(unsigned), st));
+        CK(cudaMemsetAsync(psched, 0, (nsys + 1) * sizeof(int), st));
         CK(cudaStreamSynchronize(st));
         return code;
     }

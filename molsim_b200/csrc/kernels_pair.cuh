@@ -377,7 +377,12 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MSG_PAIR_MINB) k_pair(
 //   * every pair is seen from both ends; each end adds half of the pair's
 //     energy and virial, so there is no ownership test per entry;
 //   * each lane loads U row entries, then their U partner positions, before
-//     it uses any of them, so U gathers per lane are in flight together.
+//     it uses any of them, so U gathers per lane are in flight together;
+//   * each system has a global task counter; a block starts at the system that
+//     holds its share of the tasks, its warps pull tasks from that counter
+//     until it runs dry, then the block moves on to the next system (the
+//     table is reloaded only then), so blocks that draw cheap tasks take more
+//     of them; the last block to finish resets the counters for the next launch.
 // The interval found is the one MOLSIM's walk ends on (Src/energy.F90:481-486),
 // as in k_pair.
 // ---------------------------------------------------------------------------
@@ -388,7 +393,8 @@ __host__ __device__ constexpr int tpair(int a, int b) { return a * (2 * NT - a +
 
 template <int NT, int U>
 __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MINB_M : 2) k_pair_m(
-    const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, int ntasks,
+    const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, const int2 *__restrict__ srange,
+    int nsys, int ntasks, int *__restrict__ sched,
     const int4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
     const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
     const float *__restrict__ tc, const int2 *__restrict__ bkz, double4 *__restrict__ fsr,
@@ -398,10 +404,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
     __shared__ PairTab sP[MSG_MAX_NATAT];
     __shared__ float4 sT[MAXT * MAXT];        // (z_lo, 1/h, end row, bucket base), the last two as int bits
     __shared__ int sMap[MAXT * MAXT];
-    __shared__ int sNext;
+    __shared__ int sNpt, sDrained;
     const int lane = threadIdx.x & 31;
-    const int t0 = (int)(((long long)blockIdx.x * ntasks) / gridDim.x);
-    const int t1 = (int)(((long long)(blockIdx.x + 1) * ntasks) / gridDim.x);
     // energies by unordered type pair and the virial, 64-bit fixed point per lane
     constexpr int NQ = tpair<NT>(NT - 1, NT - 1) + 1;
     long long ue[NQ];
@@ -412,11 +416,54 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
     const float *Tc = nullptr;
     const int2 *Tb = nullptr;
     int kbase = 0;
-    for (int rs = t0; rs < t1;) {
-        const PairTask W0 = tasks[rs];
-        const int re = min(t1, W0.send);
+    // the lanes' energy sums belong to system `held`; they go to its accumulators
+    // (one warp-wide sum per lane group) when the block moves to another system
+    int held = -1;
+    auto flush = [&](int sys) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ue[q] += __shfl_xor_sync(0xffffffffu, ue[q], o);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vir += __shfl_xor_sync(0xffffffffu, vir, o);
+        long long *ea = eacc + (size_t)sys * EA_N;
+        const int npt = sNpt;
+        if (lane < npt * npt) {
+            const int ta = lane / npt, tb = lane % npt;
+            if (ta <= tb) {
+                long long v = 0;
+#pragma unroll
+                for (int a = 0; a < NT; ++a)
+#pragma unroll
+                    for (int b = a; b < NT; ++b) v += (a == ta && b == tb) ? ue[tpair<NT>(a, b)] : 0;
+                if (v) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_UTWOB + sMap[lane]), (unsigned long long)v);
+            }
+        }
+        if (lane == 31 && vir) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_VIRPAIR), (unsigned long long)vir);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) ue[q] = 0;
+        vir = 0;
+    };
+    // the system holding this block's share of the tasks
+    int s0 = 0;
+    {
+        const int p = (int)(((long long)blockIdx.x * ntasks) / gridDim.x);
+        while (s0 + 1 < nsys && srange[s0].y <= p) ++s0;
+    }
+    for (int visit = 0; visit < nsys; ++visit) {
+        const int sys = (s0 + visit) % nsys;
+        const int2 R = srange[sys];           // the system's tasks [R.x, R.y)
+        if (R.y <= R.x) continue;
+        __syncthreads();                      // every warp is done with the previous system
+        // skip a system other blocks have drained already (one read, shared by the block)
+        if (threadIdx.x == 0) sDrained = atomicAdd(&sched[sys], 0) >= R.y - R.x;
         __syncthreads();
-        if (W0.sys != loaded) {
+        if (sDrained) continue;
+        if (held >= 0) flush(held);
+        held = sys;
+        if (sys != loaded) {
+            __syncthreads();                  // every warp has flushed with the old type map
+            const PairTask W0 = tasks[R.x];
             const SysDev &Sn = sysv[W0.sys];
             if (threadIdx.x < Sn.natat) sP[threadIdx.x] = ptab[Sn.pt_off + threadIdx.x];
             if (threadIdx.x < Sn.npt * Sn.npt) {
@@ -440,19 +487,21 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
                 Tc = tc + (size_t)12 * Sn.tab_k0;
                 Tb = bkz + Sn.tab_b0;
             }
+            if (threadIdx.x == 0) sNpt = Sn.npt;
             loaded = W0.sys;
         }
-        if (threadIdx.x == 0) sNext = rs;
         __syncthreads();
-        const SysDev &S = sysv[W0.sys];
+        const SysDev &S = sysv[sys];
         const float rcut2 = (float)S.rcut2;
         const float lowmax = (float)fmax(S.r2umin_max, S.r2atat_max);
         const float sx = S.fxi[0], sy = S.fxi[1], sz = S.fxi[2];
+        // the next task's index is fetched while this one runs, hiding the atomic's latency
+        int nxt = 0;
+        if (lane == 0) nxt = R.x + atomicAdd(&sched[sys], 1);
         for (;;) {
-            int task = 0;
-            if (lane == 0) task = atomicAdd(&sNext, 1);
-            task = __shfl_sync(0xffffffffu, task, 0);
-            if (task >= re) break;
+            const int task = __shfl_sync(0xffffffffu, nxt, 0);
+            if (task >= R.y) break;
+            if (lane == 0) nxt = R.x + atomicAdd(&sched[sys], 1);
             const PairTask W = tasks[task];
             const int G = W.g;
             const int g = lane & (G - 1);
@@ -556,29 +605,19 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MIN
             if (act && g == 0)
                 fsr[i] = make_double4((double)ax * kFixInv, (double)ay * kFixInv, (double)az * kFixInv, 0.0);
         }
-#pragma unroll
-        for (int q = 0; q < NQ; ++q)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) ue[q] += __shfl_xor_sync(0xffffffffu, ue[q], o);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) vir += __shfl_xor_sync(0xffffffffu, vir, o);
-        long long *ea = eacc + (size_t)W0.sys * EA_N;
-        if (lane < S.npt * S.npt) {
-            const int ta = lane / S.npt, tb = lane % S.npt;
-            if (ta <= tb) {
-                long long v = 0;
-#pragma unroll
-                for (int a = 0; a < NT; ++a)
-#pragma unroll
-                    for (int b = a; b < NT; ++b) v += (a == ta && b == tb) ? ue[tpair<NT>(a, b)] : 0;
-                if (v) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_UTWOB + sMap[lane]), (unsigned long long)v);
-            }
-        }
-        if (lane == 31 && vir) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_VIRPAIR), (unsigned long long)vir);
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) ue[q] = 0;
-        vir = 0;
-        rs = re;
+    }
+    if (held >= 0) flush(held);
+    // the last block to finish resets the task counters for the next launch
+    __shared__ bool lastb;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        lastb = atomicAdd(&sched[nsys], 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (lastb) {
+        for (int k = threadIdx.x; k <= nsys; k += blockDim.x) sched[k] = 0;
+        __threadfence();
     }
 }
 
