@@ -39,7 +39,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--replicas", type=int, default=16,
+    ap.add_argument("--replicas", type=int, default=32,
                     help="replicas of the workload in one handle for the batched figure (0: skip)")
     ap.add_argument("--ensemble", type=int, default=512,
                     help="systems in the batched ensemble (0: skip)")
