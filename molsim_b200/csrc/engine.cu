@@ -133,7 +133,6 @@ struct msg_handle {
     // skin
     double *r2o = nullptr, *skinout = nullptr;
     SkinChunk *sc = nullptr;
-    unsigned *sysdone = nullptr;
     int *flag = nullptr;
     long long *nrebuild = nullptr;
     // work lists
@@ -294,7 +293,7 @@ struct msg_handle {
     }
     void build(const msg_params *p, int n, int prec);
     void enqueue_rebuild();
-    void enqueue_forces(int mode, bool record);
+    void enqueue_forces(int mode, bool record, bool skin = false);
     void enqueue_md_step(bool record);
     void enqueue_bd_step(uint64_t seed, const double *xin_step, double *xout_step, bool record);
     // CUDA graph of one step; the rebuild sits in an IF node opened by k_skin
@@ -326,7 +325,7 @@ static void free_all(msg_handle *h)
     void *ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->acc[0], h->acc[1], h->dsum[0], h->dsum[1],
                     h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
                     h->sysid, h->fsr, h->ftot, h->posfx, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
-                    h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->sysdone, h->flag, h->nrebuild,
+                    h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->flag, h->nrebuild,
                     h->t128, h->ptask, h->psrange, h->psched, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
@@ -779,7 +778,6 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     r2o = dalloc<double>(ntot);
     skinout = dalloc<double>(2 * (size_t)n);
     sc = dalloc<SkinChunk>(nchunk);
-    sysdone = dalloc<unsigned>(n);
     flag = dalloc<int>(n);
     nrebuild = dalloc<long long>(n);
     eacc = dalloc<long long>((size_t)n * EA_N);
@@ -1043,7 +1041,7 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
 }
 
 template <class PR>
-static void launch_forces(msg_handle *h, int mode, bool record)
+static void launch_forces(msg_handle *h, int mode, bool record, bool skin)
 {
     // The pair kernel and the SPME chain (spread, FFT, influence, FFT) read
     // different inputs and add into different accumulators: the pair kernel runs
@@ -1055,6 +1053,12 @@ static void launch_forces(msg_handle *h, int mode, bool record)
         CK(cudaEventRecord(h->ev_fork, h->st));
         CK(cudaStreamWaitEvent(h->st2, h->ev_fork, 0));
         ps = h->st2;
+    }
+    if (skin) {
+        // the skin test's combine: needed only by the rebuild at the end of the step
+        k_skin_combine<<<h->nsys, SK_THREADS, 0, ps>>>(h->dsys, h->r2o, h->sc, h->flag, h->nrebuild, h->skinout,
+                                                       h->cond, h->use_cond);
+        h->launches += 1;
     }
     h->tbeg(TM_PAIR);
     const typename PR::V4 *pp =
@@ -1111,22 +1115,21 @@ static void launch_forces(msg_handle *h, int mode, bool record)
     }
 }
 
-void msg_handle::enqueue_forces(int mode, bool record)
+void msg_handle::enqueue_forces(int mode, bool record, bool skin)
 {
     if (prec == MSG_PREC_MIXED)
-        launch_forces<PrecM>(this, mode, record);
+        launch_forces<PrecM>(this, mode, record, skin);
     else
-        launch_forces<PrecD>(this, mode, record);
+        launch_forces<PrecD>(this, mode, record, skin);
 }
 
 void msg_handle::enqueue_md_step(bool record)
 {
     tbeg(TM_POS);
-    k_vv_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, inv, pos[0], vel[0], acc[0], dsum[0], posfx, r2o, sc,
-                                             sysdone, flag, nrebuild, skinout, cond, use_cond);
+    k_vv_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, inv, pos[0], vel[0], acc[0], dsum[0], posfx, r2o, sc);
     tend(TM_POS);
     launches += 1;
-    enqueue_forces(1, record);
+    enqueue_forces(1, record, true);
     if (!use_cond) enqueue_rebuild();
 }
 
@@ -1134,11 +1137,10 @@ void msg_handle::enqueue_bd_step(uint64_t seed, const double *xin_step, double *
 {
     tbeg(TM_POS);
     k_bd_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, inv, pos[0], fo[0], dsum[0], typ[0], fac1, fac2, xin_step,
-                                             xout_step, seed, sstep, posfx, r2o, sc, sysdone, flag, nrebuild, skinout,
-                                             cond, use_cond);
+                                             xout_step, seed, sstep, posfx, r2o, sc);
     tend(TM_POS);
     launches += 1;
-    enqueue_forces(0, record);
+    enqueue_forces(0, record, true);
     if (!use_cond) enqueue_rebuild();
 }
 
@@ -1316,7 +1318,6 @@ int msg_handle::check()
         // an aborted step may leave partial sums and counters behind
         CK(cudaMemsetAsync(eacc, 0, sizeof(long long) * nsys * EA_N, st));
         CK(cudaMemsetAsync(fdone, 0, sizeof(unsigned) * nsys, st));
-        CK(cudaMemsetAsync(sysdone, 0, sizeof(unsigned) * nsys, st));
         CK(cudaMemsetAsync(rdone, 0, sizeof(unsigned), st));
         CK(cudaMemsetAsync(psched, 0, (nsys + 1) * sizeof(int), st));
         CK(cudaStreamSynchronize(st));

@@ -132,18 +132,11 @@ __device__ double chunk_nonrecord_max(const double *r2, int o0, int o1, double P
     return block_max(best, smd);
 }
 
-// Chunk summary of SK_PER consecutive MOLSIM-order skin values per thread, and,
-// in the last chunk of the system to finish, the combination in MOLSIM order
-// and the rebuild decision (NList, Src/nlist.F90:600-613).
-__device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[SK_PER], int o0, int o1,
-                           const double *__restrict__ r2o, SkinChunk *__restrict__ sc,
-                           unsigned *__restrict__ sysdone, int *__restrict__ flag,
-                           long long *__restrict__ nrebuild, double *__restrict__ skinout,
-                           cudaGraphConditionalHandle cond, int use_cond)
+// Chunk summary of SK_PER consecutive MOLSIM-order skin values per thread.
+__device__ void skin_chunk(int chunk, const double v[SK_PER], int o0, int o1, SkinChunk *__restrict__ sc)
 {
     __shared__ double smd[SK_THREADS / 32];
     __shared__ int smi[SK_THREADS / 32];
-    __shared__ bool last;
     const int t = threadIdx.x;
     double tmax = 0.0;
 #pragma unroll
@@ -171,12 +164,21 @@ __device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[SK_
         out.bmax = bm;
         out.amax = am;
         out.nrec = total;
-        __threadfence();
-        last = (atomicAdd(&sysdone[s], 1u) == (unsigned)(S.nchunk - 1));
     }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
+}
+
+// The combination of a system's chunk summaries in MOLSIM order and the rebuild
+// decision (NList, Src/nlist.F90:600-613): one block per system, launched after
+// the position update.  Only the rebuild at the end of the step needs it, so in
+// the step graph it runs beside the force computation.
+__global__ void __launch_bounds__(SK_THREADS) k_skin_combine(
+    const SysDev *__restrict__ sysv, const double *__restrict__ r2o, const SkinChunk *__restrict__ sc,
+    int *__restrict__ flag, long long *__restrict__ nrebuild, double *__restrict__ skinout,
+    cudaGraphConditionalHandle cond, int use_cond)
+{
+    __shared__ double smd[SK_THREADS / 32];
+    const int s = blockIdx.x, t = threadIdx.x;
+    const SysDev &S = sysv[s];
     // Combine the system's chunks in MOLSIM order, SK_THREADS chunks per pass.
     const int c0 = S.chunk_off;
     double carry = 0.0, m2 = 0.0;
@@ -230,7 +232,6 @@ __device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[SK_
             if (use_cond) cudaGraphSetConditional(cond, 1u);
         }
         if (skinout) { skinout[2 * s] = carry; skinout[2 * s + 1] = m2; }
-        sysdone[s] = 0u;
     }
 }
 
@@ -246,9 +247,7 @@ __device__ void skin_chunk(const SysDev &S, int s, int chunk, const double v[SK_
 __global__ void __launch_bounds__(SK_THREADS) k_vv_skin(
     const SysDev *__restrict__ sysv, const int4 *__restrict__ chunks, const int *__restrict__ inv,
     double4 *__restrict__ pos, const double4 *__restrict__ vel, const double4 *__restrict__ acc,
-    double4 *__restrict__ dsum, int4 *__restrict__ posfx, double *__restrict__ r2o, SkinChunk *__restrict__ sc,
-    unsigned *__restrict__ sysdone, int *__restrict__ flag, long long *__restrict__ nrebuild,
-    double *__restrict__ skinout, cudaGraphConditionalHandle cond, int use_cond)
+    double4 *__restrict__ dsum, int4 *__restrict__ posfx, double *__restrict__ r2o, SkinChunk *__restrict__ sc)
 {
     const int4 C = chunks[blockIdx.x];
     const SysDev &S = sysv[C.x];
@@ -279,7 +278,7 @@ __global__ void __launch_bounds__(SK_THREADS) k_vv_skin(
             r2o[o] = v[k];
         }
     }
-    skin_chunk(S, C.x, blockIdx.x, v, C.y, C.z, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
+    skin_chunk(blockIdx.x, v, C.y, C.z, sc);
 }
 
 // Ermak-McCammon step (Src/bd.F90:142-152) fused with the skin test:
@@ -291,9 +290,7 @@ __global__ void __launch_bounds__(SK_THREADS) k_bd_skin(
     const int *__restrict__ typ, const double *__restrict__ fac1, const double *__restrict__ fac2,
     const double *__restrict__ xin, double *__restrict__ xout, uint64_t seed,
     const unsigned long long *__restrict__ sstep, int4 *__restrict__ posfx, double *__restrict__ r2o,
-    SkinChunk *__restrict__ sc, unsigned *__restrict__ sysdone, int *__restrict__ flag,
-    long long *__restrict__ nrebuild, double *__restrict__ skinout, cudaGraphConditionalHandle cond,
-    int use_cond)
+    SkinChunk *__restrict__ sc)
 {
     const int4 C = chunks[blockIdx.x];
     const SysDev &S = sysv[C.x];
@@ -340,7 +337,7 @@ __global__ void __launch_bounds__(SK_THREADS) k_bd_skin(
             r2o[o] = v[k];
         }
     }
-    skin_chunk(S, C.x, blockIdx.x, v, C.y, C.z, r2o, sc, sysdone, flag, nrebuild, skinout, cond, use_cond);
+    skin_chunk(blockIdx.x, v, C.y, C.z, sc);
 }
 
 // ---------------------------------------------------------------------------
