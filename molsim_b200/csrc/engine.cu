@@ -72,6 +72,34 @@ struct PlanKey {
         return s != o.s ? s < o.s : count != o.count ? count < o.count : f32 != o.f32 ? f32 < o.f32 : fwd < o.fwd;
     }
 };
+// Small pinned host blocks for the per-call device-to-host reads (error word,
+// longest rows, energy history): with the reads in pinned memory an API call
+// waits for its stream once.  The blocks are pooled for the process and never
+// freed, because freeing pinned memory would wait for the whole device.
+constexpr size_t kPinBytes = 64 * 1024;
+std::mutex g_pin_mu;
+std::vector<void *> g_pin_free;
+
+void *pin_acquire()
+{
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (!g_pin_free.empty()) {
+        void *p = g_pin_free.back();
+        g_pin_free.pop_back();
+        return p;
+    }
+    void *p = nullptr;
+    if (cudaMallocHost(&p, kPinBytes) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void pin_release(void *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
+}
+
 std::mutex g_plan_mu;
 std::map<PlanKey, std::vector<std::pair<cufftHandle, size_t>>> g_plan_idle;
 
@@ -238,6 +266,15 @@ struct msg_handle {
     }
     void plan_fft();
     void release_fft();
+    // pinned block: [0, 256) error word, [256, 256 + 4 nsys) longest rows, then energy history
+    unsigned char *pin = nullptr;
+    ErrWord *pin_err() { return reinterpret_cast<ErrWord *>(pin); }
+    int *pin_rows() { return (pin && 256 + 4 * (size_t)nsys <= kPinBytes / 2) ? reinterpret_cast<int *>(pin + 256) : nullptr; }
+    double *pin_hist(size_t n)
+    {
+        const size_t off = ((256 + 4 * (size_t)nsys + 15) / 16) * 16;
+        return (pin && off + n * sizeof(double) <= kPinBytes) ? reinterpret_cast<double *>(pin + off) : nullptr;
+    }
     int pair_blocks_max = 1, pair_blocks_lean = 1, pair_shift = 0;
     std::vector<PairTask> make_pair_tasks(int shift) const;
     void set_pair_chunks(const std::vector<PairTask> &pt, bool replace);
@@ -316,7 +353,7 @@ struct msg_handle {
     void launch_graph();
     void ensure_stage(size_t n);
     int check();
-    bool grow_lists();
+    bool grow_lists(const int *mx_host = nullptr);
     int rebuild_checked(const std::vector<int> &flags);
 };
 
@@ -335,6 +372,8 @@ static void free_all(msg_handle *h)
         h->dfree(h->fftwork);
     }
     h->release_fft();
+    pin_release(h->pin);
+    h->pin = nullptr;
     for (cudaEvent_t e : h->inflight) cudaEventDestroy(e);
     h->inflight.clear();
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
@@ -374,6 +413,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         CK(cudaGetDevice(&dev));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        pin = static_cast<unsigned char *>(pin_acquire());
         CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     }
@@ -1146,10 +1186,13 @@ void msg_handle::enqueue_bd_step(uint64_t seed, const double *xin_step, double *
 
 // Row capacity follows the longest row seen (x1.5 + 32).  When a system's rows
 // outgrow it, every list is re-laid out and rebuilt.  Returns true on growth.
-bool msg_handle::grow_lists()
+bool msg_handle::grow_lists(const int *mx_host)
 {
     std::vector<int> mx(nsys);
-    down(mx.data(), nmaxrow, nsys * sizeof(int));
+    if (mx_host)
+        std::memcpy(mx.data(), mx_host, nsys * sizeof(int));
+    else
+        down(mx.data(), nmaxrow, nsys * sizeof(int));
     bool grow = false;
     std::vector<int> cap(nsys);
     for (int s = 0; s < nsys; ++s) {
@@ -1300,11 +1343,18 @@ void msg_handle::launch_graph()
 
 int msg_handle::check()
 {
-    CK(cudaStreamSynchronize(st));
+    ErrWord e;
+    if (pin) {
+        // the error word rides with whatever reads the caller queued: one wait
+        CK(cudaMemcpyAsync(pin_err(), errw, sizeof(ErrWord), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        e = *pin_err();
+    } else {
+        CK(cudaStreamSynchronize(st));
+        down(&e, errw, sizeof(e));
+    }
     CK(cudaGetLastError());
     flush_timers();
-    ErrWord e;
-    down(&e, errw, sizeof(e));
     if (e.code) {
         static const char *names[] = {"ok", "r2 < r2umin (pair below the table minimum)", "table interval overrun",
                                       "neighbour-list capacity exceeded", "cuda", "device timeout", "argument",
@@ -1430,21 +1480,23 @@ static int put_state(msg_handle *h, int32_t isys, const double *ro, const double
                      bool keep_list)
 {
     const SysDev &S = h->hs[isys];
-    h->ensure_stage(3 * (size_t)S.n);
+    // one staging region per array, so the copies and conversions do not wait on each other
+    h->ensure_stage(9 * (size_t)S.n);
     const int c = h->cur, nb = (S.n + 255) / 256;
     const double *src[3] = {ro, rod, rodd};
-    double4 *dst[3] = {h->pos[c], h->vel[c], h->acc[c]};
+    const double *stg[3] = {nullptr, nullptr, nullptr};
     for (int k = 0; k < 3; ++k) {
         if (!src[k]) continue;
-        h2d(h->stage, src[k], 3 * (size_t)S.n, h->st);
-        k_to_internal<<<nb, 256, 0, h->st>>>(h->stage, dst[k], h->inv, S.off, S.n, k == 0 ? 1 : 0);
+        double *p = h->stage + 3 * (size_t)S.n * k;
+        h2d(p, src[k], 3 * (size_t)S.n, h->st);
+        stg[k] = p;
+    }
+    if (ro || rod || rodd) {
+        k_state_in<<<nb, 256, 0, h->st>>>(h->dsys, isys, stg[0], stg[1], stg[2], h->pos[c], h->vel[c], h->acc[c],
+                                          h->posfx, h->inv);
         h->launches += 1;
     }
-    if (ro) {
-        k_mirror_range<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->posfx);
-        h->launches += 1;
-        h->placed[isys] = 1;
-    }
+    if (ro) h->placed[isys] = 1;
     if (ro && !keep_list) {
         // new positions: rebuild this system's list now (the rebuild resets drosum)
         std::vector<int> f(h->nsys, 0);
@@ -1476,16 +1528,19 @@ extern "C" int msg_get_state(msg_handle *h, int32_t isys, double *ro, double *ro
     if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
     API_BEGIN
     const SysDev &S = h->hs[isys];
-    h->ensure_stage(3 * (size_t)S.n);
+    h->ensure_stage(9 * (size_t)S.n);
     const int c = h->cur, nb = (S.n + 255) / 256;
     double *dst[3] = {ro, rod, rodd};
-    const double4 *src[3] = {h->pos[c], h->vel[c], h->acc[c]};
-    for (int k = 0; k < 3; ++k) {
-        if (!dst[k]) continue;
-        k_to_molsim<<<nb, 256, 0, h->st>>>(src[k], h->stage, h->inv, S.off, S.n, 1.0);
+    double *stg[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; ++k)
+        if (dst[k]) stg[k] = h->stage + 3 * (size_t)S.n * k;
+    if (ro || rod || rodd) {
+        k_state_out<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->vel[c], h->acc[c], stg[0], stg[1], stg[2],
+                                           h->inv);
         h->launches += 1;
-        CK(cudaMemcpyAsync(dst[k], h->stage, 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
     }
+    for (int k = 0; k < 3; ++k)
+        if (dst[k]) CK(cudaMemcpyAsync(dst[k], stg[k], 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
     return h->check();
     API_END
 }
@@ -1672,10 +1727,21 @@ extern "C" int msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energ
     } else {
         for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(rec);
     }
+    // the longest rows and the energy history come back with the error word: one wait
+    int *prow = h->pin_rows();
+    if (prow) CK(cudaMemcpyAsync(prow, h->nmaxrow, h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    const size_t nh = (size_t)nsteps * h->nsys * ESZ;
+    double *ph = rec ? h->pin_hist(nh) : nullptr;
+    if (ph) CK(cudaMemcpyAsync(ph, h->hist, nh * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     int rc = h->check();
     if (rc) return rc;
-    if (rec) copy_hist(h, nsteps, isys, e);
-    if (h->grow_lists()) {
+    if (rec) {
+        if (ph)
+            for (int k = 0; k < nsteps; ++k) fill_energy(&ph[((size_t)k * h->nsys + isys) * ESZ], h->hs[isys].natat, &e[k]);
+        else
+            copy_hist(h, nsteps, isys, e);
+    }
+    if (h->grow_lists(prow)) {
         std::vector<int> all(h->placed.begin(), h->placed.end());
         return h->rebuild_checked(all);
     }

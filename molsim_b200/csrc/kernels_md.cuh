@@ -443,15 +443,6 @@ __global__ void __launch_bounds__(128) k_copyback(const SysDev *__restrict__ sys
     dsum[j] = make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
-__global__ void k_mirror_range(const SysDev *__restrict__ sysv, int sys, const double4 *__restrict__ pos,
-                               int4 *__restrict__ posfx)
-{
-    const SysDev &S = sysv[sys];
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= S.n) return;
-    posfx[S.off + j] = fx_pos(pos[S.off + j], S);
-}
-
 // Stencil of neighbour cells along one dimension: the three cells c-1, c, c+1
 // (periodic) when there are at least three, otherwise every cell once.
 __device__ __forceinline__ int stencil1(int c, int nc, int *out)
@@ -569,20 +560,6 @@ __global__ void k_export_nlist(const SysDev *__restrict__ sysv, int s, const int
 // ---------------------------------------------------------------------------
 // API boundary: MOLSIM order <-> internal order.
 // ---------------------------------------------------------------------------
-__global__ void k_to_internal(const double *__restrict__ src, double4 *__restrict__ dst, const int *__restrict__ inv,
-                              int off, int n, int keep_w)
-{
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n) return;
-    const int i = inv[off + o];
-    double4 v = dst[i];
-    v.x = src[3 * o];
-    v.y = src[3 * o + 1];
-    v.z = src[3 * o + 2];
-    if (!keep_w) v.w = 0.0;
-    dst[i] = v;
-}
-
 __global__ void k_to_molsim(const double4 *__restrict__ src, double *__restrict__ dst, const int *__restrict__ inv,
                             int off, int n, double scale)
 {
@@ -592,6 +569,52 @@ __global__ void k_to_molsim(const double4 *__restrict__ src, double *__restrict_
     dst[3 * o] = v.x * scale;
     dst[3 * o + 1] = v.y * scale;
     dst[3 * o + 2] = v.z * scale;
+}
+
+// Positions, velocities and accelerations of one system from MOLSIM layout
+// (three staged [n][3] arrays; a null one is skipped) into the internal
+// order, with the fixed-point mirror of the positions: one launch per state.
+__global__ void k_state_in(const SysDev *__restrict__ sysv, int sys, const double *__restrict__ sro,
+                           const double *__restrict__ srod, const double *__restrict__ srodd,
+                           double4 *__restrict__ pos, double4 *__restrict__ vel, double4 *__restrict__ acc,
+                           int4 *__restrict__ posfx, const int *__restrict__ inv)
+{
+    const SysDev &S = sysv[sys];
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= S.n) return;
+    const int i = inv[S.off + o];
+    if (sro) {
+        double4 v = pos[i];                       // .w holds the charge
+        v.x = sro[3 * o];
+        v.y = sro[3 * o + 1];
+        v.z = sro[3 * o + 2];
+        pos[i] = v;
+        posfx[i] = fx_pos(v, S);
+    }
+    if (srod) vel[i] = make_double4(srod[3 * o], srod[3 * o + 1], srod[3 * o + 2], 0.0);
+    if (srodd) acc[i] = make_double4(srodd[3 * o], srodd[3 * o + 1], srodd[3 * o + 2], 0.0);
+}
+
+// The reverse: internal order -> three MOLSIM-layout staging arrays.
+__global__ void k_state_out(const SysDev *__restrict__ sysv, int sys, const double4 *__restrict__ pos,
+                            const double4 *__restrict__ vel, const double4 *__restrict__ acc,
+                            double *__restrict__ dro, double *__restrict__ drod, double *__restrict__ drodd,
+                            const int *__restrict__ inv)
+{
+    const SysDev &S = sysv[sys];
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= S.n) return;
+    const int i = inv[S.off + o];
+    const double4 *src[3] = {pos, vel, acc};
+    double *dst[3] = {dro, drod, drodd};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (!dst[k]) continue;
+        const double4 v = src[k][i];
+        dst[k][3 * o] = v.x;
+        dst[k][3 * o + 1] = v.y;
+        dst[k][3 * o + 2] = v.z;
+    }
 }
 
 // rodd = massip * forceo (GetLinAcc, Src/md.F90:601-617)
