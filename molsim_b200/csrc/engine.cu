@@ -1074,9 +1074,8 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
     h->tbeg(TM_FINAL);
     h->launches += 1;
     k_finalize<P, PR><<<h->nt128, FIN_THREADS, 0, h->st>>>(
-        h->dsys, h->t128, h->pos[0], h->typ[0], h->orig[0], h->inv, h->rgrid, h->rgrid32, h->fsr,
-        h->eacc, h->bptr, h->bpart, h->bk, h->beq, h->bpw, h->massip, h->massp, h->ftot, h->fo[0], h->vel[0],
-        h->acc[0], mode, fo, h->errw);
+        h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->eacc, h->massip, h->massp,
+        h->ftot, h->fo[0], h->vel[0], h->acc[0], mode, fo, h->errw);
     h->tend(TM_FINAL);
 }
 

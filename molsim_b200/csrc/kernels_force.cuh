@@ -244,11 +244,8 @@ struct FinOut {
 template <int P, class PR>
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
-    const int *__restrict__ typ, const int *__restrict__ orig,
-    const int *__restrict__ inv, const double *__restrict__ grid, const float *__restrict__ grid32,
-    const double4 *__restrict__ fsr, long long *__restrict__ eacc, const int *__restrict__ bptr,
-    const int *__restrict__ bpart,
-    const double *__restrict__ bk, const double *__restrict__ beq, const int *__restrict__ bpw,
+    const int *__restrict__ typ, const double *__restrict__ grid, const float *__restrict__ grid32,
+    const double4 *__restrict__ fsr, long long *__restrict__ eacc,
     const double *__restrict__ massip, const double *__restrict__ massp, double4 *__restrict__ ftot,
     double4 *__restrict__ forceo, double4 *__restrict__ vel, double4 *__restrict__ acc, int mode, FinOut out,
     ErrWord *err)

@@ -71,3 +71,32 @@ def test_pair_lanes_keep_results_within_tolerance(precision):
             scale = abs(b["utot"]) + abs(b["urec"]) + abs(b["utwob"][0])
             for key in ("utot", "urec", "virial"):
                 assert abs(a[key] - b[key]) <= etol * max(scale, abs(b[key]))
+
+
+@pytest.mark.gpu
+def test_scheduling_knobs_keep_mixed_results_bitwise():
+    """The pair/SPME overlap, the pair blocks per SM and the unroll only change how
+    work is scheduled: mixed-precision forces, energies and a short trajectory stay
+    bit-identical."""
+    from molsim_b200 import Engine, _lib
+
+    sy, tb = _ensemble(n=3, seed=6)
+    L = _lib.lib()
+
+    def run(overlap, blocks, unroll):
+        e = Engine(sy, tb, precision="mixed")
+        assert L.msg_tune(e.h, _lib.MSG_TUNE_OVERLAP, overlap) == 0
+        assert L.msg_tune(e.h, _lib.MSG_TUNE_PAIR_BLOCKS, blocks) == 0
+        assert L.msg_tune(e.h, _lib.MSG_TUNE_PAIR_UNROLL, unroll) == 0
+        e.UTotal(0)
+        e.GetLinAcc()
+        e.VelVer(12, energies=False)
+        return [e.get_state(k)["ro"] for k in range(len(sy))], [e.energy(k) for k in range(len(sy))]
+
+    ref = run(1, 0, 2)
+    for knobs in ((0, 0, 2), (1, 1, 1), (1, 3, 4)):
+        got = run(*knobs)
+        for a, b in zip(got[0], ref[0]):
+            assert np.array_equal(a, b), knobs
+        for a, b in zip(got[1], ref[1]):
+            assert a == b, knobs
