@@ -38,11 +38,11 @@ __device__ __forceinline__ float3 gauss3(uint64_t seed, uint32_t particle, uint3
 // ---------------------------------------------------------------------------
 // Skin test of NList (Src/nlist.F90:600-613), reproduced exactly including its
 // running "second maximum": r2max2 only collects values that were not a new
-// running maximum when visited in MOLSIM order.  Chunks of 1024 MOLSIM indices
-// are summarised in parallel (block max B, non-record max A, the chunk's
-// record values); the last chunk of each system to finish combines them:
-// a chunk record R counts towards r2max2 iff R <= the prefix maximum P before
-// the chunk, so the chunk contributes max(A, max{R <= P}).
+// running maximum when visited in MOLSIM order.  Chunks of SK_CHUNK MOLSIM
+// indices are summarised in parallel by the position update (block max B,
+// non-record max A, the chunk's record values); k_skin_combine then walks a
+// system's chunks in order: a chunk record R counts towards r2max2 iff R <= the
+// prefix maximum P before the chunk, so the chunk contributes max(A, max{R <= P}).
 // ---------------------------------------------------------------------------
 // 128 MOLSIM indices per chunk, one per thread: a 16000-particle system spreads
 // over 125 blocks.
