@@ -242,7 +242,7 @@ def run_ensemble(a, flush):
     import torch
 
     from molsim_b200 import Engine, prepare
-    from molsim_b200.autotune import apply_grids, tune_grids, tune_pair_lanes
+    from molsim_b200.autotune import apply_grids, tune_grids, tune_pair_kernel
     from molsim_b200.systems import batched_ensemble
 
     t0 = time.perf_counter()
@@ -257,7 +257,7 @@ def run_ensemble(a, flush):
     eng = Engine(sy, tables, precision="mixed")
     eng.UTotal(0)
     eng.GetLinAcc()
-    best, lane_ms = tune_pair_lanes(eng)
+    best, lane_ms = tune_pair_kernel(eng)
     K = max(10, a.steps // 4)
     ms = timed_md_steps(eng, K, flush, a.warmup)
     value = ntot * K / (ms / 1000.0)
@@ -275,7 +275,7 @@ def run_ensemble(a, flush):
             "autotune": {"grid_edges": hist, "target_met": int(sum(r["met"] for r in rep)),
                          "rule": "cheapest edge with measured reciprocal RMS force error <= Kolafa-Perram "
                                  "real-space estimate (reference 96^3 order 6)",
-                         "pair_lane_shift": best, "pair_lane_ms_per_step": lane_ms, "tune_s": t_tune},
+                         "pair_kernel": best, "pair_kernel_ms_per_step": lane_ms, "tune_s": t_tune},
             "generate_s": t_gen}
 
 
@@ -340,6 +340,10 @@ def run_gpu(a):
     eng = Engine(s, precision=a.precision)
     eng.UTotal()
     eng.GetLinAcc()
+    tuned = None
+    if a.precision == "mixed":
+        from molsim_b200.autotune import tune_pair_kernel
+        tuned, _ = tune_pair_kernel(eng, steps=20)
     _, _, npair = eng.SetVList(0, export=False)
     ext = torch.cuda.ExternalStream(eng.stream())
     flush = L2Flush()
@@ -404,9 +408,13 @@ def run_gpu(a):
         eb = Engine([dict(s) for _ in range(a.replicas)], precision=a.precision)
         eb.UTotal(0)
         eb.GetLinAcc()
+        tuned_b = None
+        if a.precision == "mixed":
+            from molsim_b200.autotune import tune_pair_kernel
+            tuned_b, _ = tune_pair_kernel(eb, steps=5)
         kb = max(10, a.steps // 4)
         tb = timed_steps(eb, kb)
-        batched = {"replicas": a.replicas, "value": n * a.replicas * kb / (tb / 1000.0), "unit": METRIC,
+        batched = {"replicas": a.replicas, "pair_kernel": tuned_b, "value": n * a.replicas * kb / (tb / 1000.0), "unit": METRIC,
                    "steps": kb, "ms_per_step": tb / kb,
                    "vs_fp64_single": (n * a.replicas * kb / (tb / 1000.0)) / fp64_value if fp64_value else None}
         del eb
@@ -487,7 +495,7 @@ def run_gpu(a):
                        "spme": "64^3 order 5", "rcut_A": 25.0, "skin_A": 2.0, "precision": a.precision,
                        "integrator": "velocity Verlet", "parallelism": "replicas" if world > 1 else "single",
                        "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
-                       "rebuilds_in_timed_steps": int(rebuilds)},
+                       "rebuilds_in_timed_steps": int(rebuilds), "pair_kernel": tuned},
             "fp64_value": fp64_value, "batched": batched, "ensemble": ensemble, "serving": serving,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},

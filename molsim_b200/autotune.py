@@ -19,9 +19,11 @@ not exceed the real-space truncation error at the system's alpha and cutoff.
   particles beyond rc.
 * A system no candidate satisfies gets the largest candidate.
 
-Pair lanes (per handle).  The pair kernel gives each particle G lanes, G set
-from the expected row length; the tuner times a few steps for G scaled by
-2^shift and keeps the fastest.  In FP64 the results do not depend on G beyond
+Pair kernel shape (per handle).  The pair kernel gives each particle G lanes,
+G set from the expected row length; the tuner times a few steps for G scaled
+by 2^shift, for 1, 2 or 4 row entries in flight per lane, and for all SMs or
+2 blocks per SM (room for the SPME chain running beside it), and keeps the
+fastest.  In FP64 the results do not depend on G beyond
 FP64 rounding; in mixed precision a lane adds its few pair terms in FP32
 before rounding them to fixed point, so G moves results by FP32 rounding
 (relative 1e-7 level) while each setting stays deterministic and independent
@@ -93,20 +95,58 @@ def apply_grids(systems, edges, order=4):
     return out
 
 
+def _time_steps(engine, steps):
+    import torch
+
+    engine.VelVer(2, energies=False)               # capture the graph for this layout
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    engine.VelVer(steps, energies=False)
+    torch.cuda.synchronize()
+    return 1000.0 * (time.perf_counter() - t0) / steps
+
+
 def tune_pair_lanes(engine, shifts=(-1, 0, 1), steps=10):
     """Time `steps` MD steps per lane scaling; leave the engine on the fastest.
     Returns (best shift, {shift: ms per step})."""
-    import torch
-
     times = {}
     for sh in shifts:
         engine.tune_pair_lanes(sh)
-        engine.VelVer(2, energies=False)           # capture the graph for this layout
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        engine.VelVer(steps, energies=False)
-        torch.cuda.synchronize()
-        times[sh] = 1000.0 * (time.perf_counter() - t0) / steps
+        times[sh] = _time_steps(engine, steps)
     best = min(times, key=times.get)
     engine.tune_pair_lanes(best)
     return best, times
+
+
+def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2)):
+    """Shape of the pair kernel for this handle, by timing MD steps: lanes per particle
+    (2^shift times the default), row entries in flight per lane (unroll), and pair blocks
+    per SM (0: as many as fit; 2: room for the SPME chain beside it), one knob at a time
+    from the defaults.  Leaves the engine on the best; returns ({knob: value}, {setting:
+    ms per step}).  Mixed precision only (the knobs belong to its pair kernel)."""
+    from . import _lib
+
+    L = _lib.lib()
+
+    def setk(key, val):
+        if L.msg_tune(engine.h, key, int(val)):
+            raise RuntimeError("msg_tune(%d, %d) failed" % (key, val))
+
+    best = {"shift": 0, "unroll": 2, "blocks": 0}
+    log = {}
+    for name, vals, key in (("shift", shifts, None), ("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
+                            ("blocks", blocks, _lib.MSG_TUNE_PAIR_BLOCKS)):
+        res = {}
+        for v in vals:
+            if key is None:
+                engine.tune_pair_lanes(v)
+            else:
+                setk(key, v)
+            res[v] = _time_steps(engine, steps)
+            log["%s=%s" % (name, v)] = res[v]
+        best[name] = min(res, key=res.get)
+        if key is None:
+            engine.tune_pair_lanes(best[name])
+        else:
+            setk(key, best[name])
+    return best, log

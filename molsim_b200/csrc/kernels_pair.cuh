@@ -391,8 +391,10 @@ __global__ void __launch_bounds__(PAIR_BLOCK, MSG_PAIR_MINB) k_pair(
 template <int NT>
 __host__ __device__ constexpr int tpair(int a, int b) { return a * (2 * NT - a + 1) / 2 + (b - a); }
 
+// Register budget with two particle types: one entry in flight per lane (U = 1) leaves room
+// for 4 blocks of 256 per SM, two entries for 3; otherwise 2 blocks.
 template <int NT, int U>
-__global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? MSG_PAIR_MINB_M : 2) k_pair_m(
+__global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U == 1 ? 4 : (U == 2 ? MSG_PAIR_MINB_M : 2)) : 2) k_pair_m(
     const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, const int2 *__restrict__ srange,
     int nsys, int ntasks, int *__restrict__ sched,
     const int4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
