@@ -1,9 +1,10 @@
 // engine.cu -- the B200 force/energy engine behind the C-ABI of molsim_gpu.h.
 //
 // One handle owns every device buffer of its systems (concatenated), the pair
-// tables, the SPME grids with their cuFFT plans, and one CUDA stream.  A step
-// is a fixed sequence of kernels; each API call enqueues its steps and checks
-// the device error word once at the end.
+// tables, the SPME grids with their cuFFT plans, and two CUDA streams: a step
+// is a fixed graph of kernels whose pair/bond branch runs on the second stream
+// beside the SPME chain.  Each API call enqueues its steps and waits for the
+// handle's stream once at the end, reading the device error word back then.
 #include <cufft.h>
 
 #include <algorithm>

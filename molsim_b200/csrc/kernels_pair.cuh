@@ -1,5 +1,8 @@
 // kernels_pair.cuh -- UTwoBodyA (Src/energy.F90:445-544) over the full Verlet list.
 //
+// k_pair (below) serves the FP64 path (and the mixed path on request); the
+// mixed path runs k_pair_m, further down, by default.
+//
 // One particle per group of G lanes; the lanes stride over the particle's
 // row, so a row is read with coalesced 64-byte segments and every pair is
 // evaluated by both of its particles (forces need no atomics and are summed in
