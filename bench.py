@@ -446,9 +446,8 @@ def run_gpu(a):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(ke):
-        assert L.msg_put_state(eng.h, 0, pr[0], pr[1], pr[2], 1) == 0
-        assert L.msg_velver(eng.h, 1, 0, C.byref(e)) == 0
-        assert L.msg_get_state(eng.h, 0, pr[0], pr[1], pr[2]) == 0
+        # the drop-in step with host-held state: send, step, return (msg_velver_host)
+        assert L.msg_velver_host(eng.h, 0, 1, pr[0], pr[1], pr[2], C.byref(e)) == 0
     t_e2e = time.perf_counter() - t0
     if world > 1:
         tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)

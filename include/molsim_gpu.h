@@ -156,6 +156,16 @@ int  msg_get_linacc(msg_handle *h);
  * e (optional): [nsteps] energies of system isys after each step. */
 int  msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energy *e);
 
+/* The drop-in step with host-held state: ro, rod, rodd of system isys (the
+ * host's arrays, [np][3], continuing the device's trajectory as with
+ * msg_put_state(keep_list = 1)) go to the device, nsteps of MDDriver run, and
+ * the new state comes back into the same arrays, with the energies of each
+ * step in e (optional, [nsteps]).  Same result as msg_put_state + msg_velver +
+ * msg_get_state, with one wait for the device instead of three.  NULL arrays
+ * are neither sent nor returned. */
+int  msg_velver_host(msg_handle *h, int32_t isys, int32_t nsteps, double *ro, double *rod, double *rodd,
+                     msg_energy *e);
+
 /* As msg_velver without energies, but returns once the steps are enqueued on
  * the handle's stream (msg_stream); device errors surface at the next
  * synchronous call. */

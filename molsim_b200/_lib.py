@@ -65,6 +65,7 @@ SIGNATURES = {
     "msg_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "msg_velver": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MsgEnergy)]),
     "msg_velver_async": (C.c_int, [C.c_void_p, C.c_int32]),
+    "msg_velver_host": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, f64p, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_bd_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_uint64, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_nrebuild": (C.c_int64, [C.c_void_p, C.c_int32]),
     "msg_put_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p, C.c_int32]),

@@ -1476,8 +1476,10 @@ extern "C" const char *msg_last_error(const msg_handle *h) { return h ? h->err.c
 
 extern "C" int32_t msg_nsys(const msg_handle *h) { return h ? h->nsys : 0; }
 
-static int put_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd,
-                     bool keep_list)
+// Host state of system isys (MOLSIM layout, NULL arrays skipped) onto the
+// device, stream-ordered: copies through one staging region per array, then one
+// conversion kernel.
+static void upload_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd)
 {
     const SysDev &S = h->hs[isys];
     // one staging region per array, so the copies and conversions do not wait on each other
@@ -1497,6 +1499,31 @@ static int put_state(msg_handle *h, int32_t isys, const double *ro, const double
         h->launches += 1;
     }
     if (ro) h->placed[isys] = 1;
+}
+
+// The reverse, into host arrays; complete once the stream reaches it.
+static void download_state(msg_handle *h, int32_t isys, double *ro, double *rod, double *rodd)
+{
+    const SysDev &S = h->hs[isys];
+    h->ensure_stage(9 * (size_t)S.n);
+    const int c = h->cur, nb = (S.n + 255) / 256;
+    double *dst[3] = {ro, rod, rodd};
+    double *stg[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; ++k)
+        if (dst[k]) stg[k] = h->stage + 3 * (size_t)S.n * k;
+    if (ro || rod || rodd) {
+        k_state_out<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->vel[c], h->acc[c], stg[0], stg[1], stg[2],
+                                           h->inv);
+        h->launches += 1;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (dst[k]) CK(cudaMemcpyAsync(dst[k], stg[k], 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
+}
+
+static int put_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd,
+                     bool keep_list)
+{
+    upload_state(h, isys, ro, rod, rodd);
     if (ro && !keep_list) {
         // new positions: rebuild this system's list now (the rebuild resets drosum)
         std::vector<int> f(h->nsys, 0);
@@ -1527,20 +1554,7 @@ extern "C" int msg_get_state(msg_handle *h, int32_t isys, double *ro, double *ro
 {
     if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
     API_BEGIN
-    const SysDev &S = h->hs[isys];
-    h->ensure_stage(9 * (size_t)S.n);
-    const int c = h->cur, nb = (S.n + 255) / 256;
-    double *dst[3] = {ro, rod, rodd};
-    double *stg[3] = {nullptr, nullptr, nullptr};
-    for (int k = 0; k < 3; ++k)
-        if (dst[k]) stg[k] = h->stage + 3 * (size_t)S.n * k;
-    if (ro || rod || rodd) {
-        k_state_out<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->vel[c], h->acc[c], stg[0], stg[1], stg[2],
-                                           h->inv);
-        h->launches += 1;
-    }
-    for (int k = 0; k < 3; ++k)
-        if (dst[k]) CK(cudaMemcpyAsync(dst[k], stg[k], 3 * sizeof(double) * S.n, cudaMemcpyDeviceToHost, h->st));
+    download_state(h, isys, ro, rod, rodd);
     return h->check();
     API_END
 }
@@ -1728,6 +1742,43 @@ extern "C" int msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energ
         for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(rec);
     }
     // the longest rows and the energy history come back with the error word: one wait
+    int *prow = h->pin_rows();
+    if (prow) CK(cudaMemcpyAsync(prow, h->nmaxrow, h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    const size_t nh = (size_t)nsteps * h->nsys * ESZ;
+    double *ph = rec ? h->pin_hist(nh) : nullptr;
+    if (ph) CK(cudaMemcpyAsync(ph, h->hist, nh * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    int rc = h->check();
+    if (rc) return rc;
+    if (rec) {
+        if (ph)
+            for (int k = 0; k < nsteps; ++k) fill_energy(&ph[((size_t)k * h->nsys + isys) * ESZ], h->hs[isys].natat, &e[k]);
+        else
+            copy_hist(h, nsteps, isys, e);
+    }
+    if (h->grow_lists(prow)) {
+        std::vector<int> all(h->placed.begin(), h->placed.end());
+        return h->rebuild_checked(all);
+    }
+    return MSG_OK;
+    API_END
+}
+
+extern "C" int msg_velver_host(msg_handle *h, int32_t isys, int32_t nsteps, double *ro, double *rod, double *rodd,
+                               msg_energy *e)
+{
+    if (!h || isys < 0 || isys >= h->nsys || nsteps < 0) return MSG_ERR_ARG;
+    API_BEGIN
+    // the host arrays continue the device's trajectory: the list and drosum stay valid
+    upload_state(h, isys, ro, rod, rodd);
+    const bool rec = e != nullptr;
+    if (rec) prepare_hist(h, nsteps);
+    if (h->use_graphs && nsteps > 0) {
+        h->ensure_graph(0, rec, 0);
+        for (int k = 0; k < nsteps; ++k) h->launch_graph();
+    } else {
+        for (int k = 0; k < nsteps; ++k) h->enqueue_md_step(rec);
+    }
+    download_state(h, isys, ro, rod, rodd);
     int *prow = h->pin_rows();
     if (prow) CK(cudaMemcpyAsync(prow, h->nmaxrow, h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->st));
     const size_t nh = (size_t)nsteps * h->nsys * ESZ;

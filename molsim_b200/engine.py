@@ -240,6 +240,17 @@ class Engine:
         en = [e[k].as_dict(self.natat[isys]) for k in range(nsteps)] if energies else None
         return (en, xout) if return_noise else en
 
+    def VelVerHost(self, state, nsteps=1, isys=0, energies=True):
+        """nsteps of MDDriver with host-held state: state = dict(ro, rod, rodd) ([np][3]
+        float64 arrays, continuing the device's trajectory) is sent, stepped and overwritten
+        with the new state, in one call (msg_velver_host)."""
+        arrs = [np.ascontiguousarray(state[k], np.float64) for k in ("ro", "rod", "rodd")]
+        e = (MsgEnergy * max(1, nsteps))() if energies else None
+        self._check(_lib.lib().msg_velver_host(self.h, isys, nsteps, *[_p(a, C.c_double) for a in arrs], e))
+        for k, a in zip(("ro", "rod", "rodd"), arrs):
+            state[k] = a
+        return [e[k].as_dict(self.natat[isys]) for k in range(nsteps)] if energies else None
+
     def nrebuild(self, isys=0):
         return _lib.lib().msg_nrebuild(self.h, isys)
 

@@ -269,3 +269,36 @@ def test_config2_colloid_bd_full_size(precision):
     box = s["boxlen"][0]
     d -= box * np.round(d / box)
     assert np.abs(d).max() < (1e-9 if precision == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_velver_host_equals_put_step_get(precision):
+    """msg_velver_host (state in, steps, state out in one call) gives what
+    msg_put_state + msg_velver + msg_get_state give: bit for bit in the mixed path;
+    to FP64 rounding in the FP64 path (its charge grid is summed with FP64 atomics)."""
+    s = dict(Hp.pe_small())
+    t = Hp.oracle_table(s)
+    a = Engine(s, t, precision=precision)
+    b = Engine(s, t, precision=precision)
+    for g in (a, b):
+        g.UTotal()
+        g.GetLinAcc()
+    sa = a.get_state()
+    sb = b.get_state()
+    for _ in range(3):
+        a.put_state(0, sa["ro"], sa["rod"], sa["rodd"], keep_list=True)
+        ea = a.VelVer(2)
+        sa = a.get_state()
+        eb = b.VelVerHost(sb, nsteps=2)
+    box = s["boxlen"][0]
+    for k in ("ro", "rod", "rodd"):
+        if precision == "mixed":
+            assert np.array_equal(sa[k], sb[k]), k
+        else:
+            d = sa[k] - sb[k]
+            if k == "ro":
+                d -= box * np.round(d / box)
+            assert np.abs(d).max() <= 1e-10 * max(1.0, np.abs(sa[k]).max()), k
+    for x, y in zip(ea, eb):
+        for k in ("utot", "virial", "ekin"):
+            assert x[k] == y[k] if precision == "mixed" else abs(x[k] - y[k]) <= 1e-9 * abs(x[k]), k
