@@ -105,6 +105,13 @@ module MolsimGpu
          type(c_ptr), value        :: e          ! msg_energy(nsteps) or c_null_ptr
       end function msg_velver
 
+      integer(c_int) function msg_velver_host(h, isys, nsteps, ro, rod, rodd, e) bind(c, name='msg_velver_host')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys, nsteps
+         type(c_ptr), value        :: ro, rod, rodd, e   ! (3,np) real(8) each; e: msg_energy(nsteps) or c_null_ptr
+      end function msg_velver_host
+
       integer(c_int) function msg_bd_step(h, nsteps, seed, isys, xi, xi_out, e) bind(c, name='msg_bd_step')
          import :: c_int, c_int32_t, c_int64_t, c_ptr
          type(c_ptr), value        :: h
