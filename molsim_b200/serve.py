@@ -179,7 +179,11 @@ class Server:
                 ids = set(id(j) for j in take)
                 queue = [j for j in queue if id(j) not in ids]
                 tadm = self.clock() - t0
-                c = self.backend(take, self.precision, self.chunk)
+                try:
+                    c = self.backend(take, self.precision, self.chunk)
+                except Exception as exc:          # set-up failed: these jobs fail, the server goes on
+                    self._fail(take, exc, self.clock() - t0, finished)
+                    continue
                 c.cid = self.ncohorts
                 c.reserved = max(tot, getattr(c, "nbytes", 0))
                 self.device_now += getattr(c, "nbytes", 0)
@@ -197,7 +201,16 @@ class Server:
             still = []
             progressed = False
             for c in running:
-                if c.pump():
+                try:
+                    complete = c.pump()
+                except Exception as exc:          # a device error in this cohort: fail its jobs
+                    self._fail(c.jobs, exc, self.clock() - t0, finished)
+                    c.close()
+                    self.used -= c.reserved
+                    self.device_now -= getattr(c, "nbytes", 0)
+                    progressed = True
+                    continue
+                if complete:
                     res = c.harvest()
                     tdone = self.clock() - t0
                     for j, r in zip(c.jobs, res):
@@ -214,6 +227,13 @@ class Server:
             if not progressed and poll_s:
                 time.sleep(poll_s)
         return self.metrics(finished)
+
+    @staticmethod
+    def _fail(jobs, exc, now, finished):
+        for j in jobs:
+            j.error = "%s: %s" % (type(exc).__name__, exc)
+            j.done = now
+            finished.append(j)
 
     def metrics(self, finished):
         ok = [j for j in finished if not j.error]

@@ -161,3 +161,22 @@ def test_estimate_bytes_bounds_the_handle():
     got = e.device_bytes()
     # the real handle may only differ by its cuFFT work area (estimated) and list growth
     assert 0.8 * est <= got <= 1.25 * est, (est, got)
+
+
+class FailingCohort(FakeCohort):
+    """A cohort whose device work fails (e.g. a pair below the table minimum)."""
+
+    def pump(self):
+        if any(j.n == 666 for j in self.jobs):
+            raise RuntimeError("r2 < r2umin (status 1)")
+        return super().pump()
+
+
+def test_device_error_fails_the_cohort_and_the_server_goes_on():
+    jobs = _jobs([(100, 10, 0.0, 10), (666, 10, 0.001, 10), (100, 10, 0.05, 10), (200, 10, 0.06, 10)])
+    srv = Server(1000, backend=FailingCohort, clock=TickClock(), estimate=lambda j: j.nbytes,
+                 max_cohorts=4, max_jobs=1, chunk=5)
+    m = srv.run(jobs, poll_s=0)
+    assert m["failed"] == 1 and "r2umin" in jobs[1].error
+    assert all(j.result for j in jobs if j.jid != 1)
+    assert srv.used == 0
