@@ -43,6 +43,7 @@ def parse():
                     help="replicas of the workload in one handle for the batched figure (0: skip)")
     ap.add_argument("--ensemble", type=int, default=512,
                     help="systems in the batched ensemble (0: skip)")
+    ap.add_argument("--bd", type=int, default=1, help="time the 200,000-particle BD system (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=200,
                     help="jobs in the serving stream (Poisson arrivals at 200/s; 0: skip)")
     ap.add_argument("--serve-budget-gib", type=float, default=4.0)
@@ -279,6 +280,49 @@ def run_ensemble(a, flush):
             "generate_s": t_gen}
 
 
+def run_bd(a, flush):
+    """The 200,000-particle charged-colloid Brownian dynamics (2000 macroions +20e, 40000
+    counterions, 79000 salt pairs; L = 1200 A; SPME 128^3 order 4; rc = 30 A; Ermak-McCammon,
+    dt = 1e-3 ps, FP32 Philox noise): device time per BD step, L2 flushed before each, mixed
+    precision beside the FP64 path."""
+    import torch
+
+    from molsim_b200 import Engine, _lib
+    from molsim_b200 import systems as S
+
+    s = S.colloid_bd(seed=0)
+    s["bd_fac"] = S.bd_factors(s)
+    n = int(s["np"])
+    L = _lib.lib()
+    out = {"particles": n, "spme": "128^3 order 4", "rcut_A": 30.0, "unit": METRIC}
+    for prec in ("mixed", "fp64"):
+        e = Engine(s, precision=prec)
+        e.UTotal()
+        ext = torch.cuda.ExternalStream(e.stream())
+        K = max(10, a.steps // 10)
+        for _ in range(3):
+            e.BDStep(1, seed=7, energies=False)
+        torch.cuda.synchronize()
+        st = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        en = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        for k in range(K):
+            with torch.cuda.stream(ext):
+                flush()
+                st[k].record(ext)
+            if L.msg_bd_step(e.h, 1, 7, 0, None, None, None):
+                raise RuntimeError(L.msg_last_error(e.h).decode())
+            with torch.cuda.stream(ext):
+                en[k].record(ext)
+        torch.cuda.synchronize()
+        ms = sum(x.elapsed_time(y) for x, y in zip(st, en))
+        out["value" if prec == "mixed" else "fp64_value"] = n * K / (ms / 1000.0)
+        out["ms_per_step" if prec == "mixed" else "fp64_ms_per_step"] = ms / K
+        out["steps"] = K
+        del e
+    out["vs_fp64"] = out["value"] / out["fp64_value"]
+    return out
+
+
 def run_serving(a):
     """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
     half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
@@ -476,7 +520,9 @@ def run_gpu(a):
                "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
                          "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
 
-    ensemble = serving = None
+    ensemble = serving = bd = None
+    if rank == 0 and world == 1 and a.bd:
+        bd = run_bd(a, flush)
     if rank == 0 and world == 1 and a.ensemble > 0:
         ensemble = run_ensemble(a, flush)
     if rank == 0 and world == 1 and a.serve_jobs > 0:
@@ -496,6 +542,7 @@ def run_gpu(a):
                        "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
                        "rebuilds_in_timed_steps": int(rebuilds), "pair_kernel": tuned},
             "fp64_value": fp64_value, "batched": batched, "ensemble": ensemble, "serving": serving,
+            "bd_200k": bd,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
