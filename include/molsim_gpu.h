@@ -162,7 +162,10 @@ int  msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energy *e);
  * the new state comes back into the same arrays, with the energies of each
  * step in e (optional, [nsteps]).  Same result as msg_put_state + msg_velver +
  * msg_get_state, with one wait for the device instead of three.  NULL arrays
- * are neither sent nor returned. */
+ * are neither sent nor returned.  With nsteps = 1 and page-locked arrays
+ * (cudaHostAlloc / cudaMallocHost, or cudaHostRegister with
+ * cudaHostRegisterMapped where the device uses the host address) the exchange
+ * runs in place inside the step's CUDA graph, without copies. */
 int  msg_velver_host(msg_handle *h, int32_t isys, int32_t nsteps, double *ro, double *rod, double *rodd,
                      msg_energy *e);
 

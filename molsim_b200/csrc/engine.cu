@@ -5,6 +5,7 @@
 // is a fixed graph of kernels whose pair/bond branch runs on the second stream
 // beside the SPME chain.  Each API call enqueues its steps and waits for the
 // handle's stream once at the end, reading the device error word back then.
+#include <cuda.h>
 #include <cufft.h>
 
 #include <algorithm>
@@ -143,6 +144,11 @@ struct msg_handle {
     // second stream of the step: the pair kernel runs there beside the SPME chain
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // third stream of the host-exchange graph: positions go back to the host while the forces run
+    cudaStream_t st3 = nullptr;
+    cudaEvent_t ev_io0 = nullptr, ev_io1 = nullptr;
+    double *io_ro = nullptr;         // mapped host positions written right after the position update
+    int io_ro_sys = -1;
     int overlap = 1;                 // pair kernel concurrent with spread/FFT/influence
     int pair_per_sm = 0;             // pair blocks per SM (0: as many as fit; 2 when overlapped)
     int dev = 0;
@@ -269,6 +275,12 @@ struct msg_handle {
     void release_fft();
     // pinned block: [0, 256) error word, [256, 256 + 4 nsys) longest rows, then energy history
     unsigned char *pin = nullptr;
+    unsigned char *dpin = nullptr;   // the block's mapped device address (null: not mapped)
+    template <class T>
+    T *map_host(T *p) const
+    {
+        return p ? reinterpret_cast<T *>(dpin + (reinterpret_cast<unsigned char *>(p) - pin)) : nullptr;
+    }
     ErrWord *pin_err() { return reinterpret_cast<ErrWord *>(pin); }
     int *pin_rows() { return (pin && 256 + 4 * (size_t)nsys <= kPinBytes / 2) ? reinterpret_cast<int *>(pin + 256) : nullptr; }
     double *pin_hist(size_t n)
@@ -347,13 +359,21 @@ struct msg_handle {
         long long launches = 0;
         std::vector<int> tk;
         std::vector<cudaEvent_t> ta, tb;
-    } graph;
+        // host exchange captured with the step (msg_velver_host on page-locked arrays)
+        int io_sys = -1;
+        double *io[3] = {nullptr, nullptr, nullptr};
+    } graph, iograph;
     bool use_graphs = true;
     void drop_graph();
+    void drop_one(StepGraph &gr);
     void ensure_graph(int kind, bool record, uint64_t seed);
+    void build_graph(StepGraph &gr, int kind, bool record, uint64_t seed, int io_sys, double *const io[3]);
+    void ensure_io_graph(bool record, int io_sys, double *const io[3]);
     void launch_graph();
+    void launch_one(StepGraph &gr);
     void ensure_stage(size_t n);
     int check();
+    int check_word(const ErrWord &e);
     bool grow_lists(const int *mx_host = nullptr);
     int rebuild_checked(const std::vector<int> &flags);
 };
@@ -375,6 +395,7 @@ static void free_all(msg_handle *h)
     h->release_fft();
     pin_release(h->pin);
     h->pin = nullptr;
+    h->dpin = nullptr;
     for (cudaEvent_t e : h->inflight) cudaEventDestroy(e);
     h->inflight.clear();
     for (cudaEvent_t e : h->evpool) cudaEventDestroy(e);
@@ -383,10 +404,13 @@ static void free_all(msg_handle *h)
     h->evpool.clear();
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_io0) cudaEventDestroy(h->ev_io0);
+    if (h->ev_io1) cudaEventDestroy(h->ev_io1);
+    if (h->st3) cudaStreamDestroy(h->st3);
     if (h->st2) cudaStreamDestroy(h->st2);
     if (h->st) cudaStreamDestroy(h->st);
-    h->st = h->st2 = nullptr;
-    h->ev_fork = h->ev_join = nullptr;
+    h->st = h->st2 = h->st3 = nullptr;
+    h->ev_fork = h->ev_join = h->ev_io0 = h->ev_io1 = nullptr;
 }
 
 msg_handle::~msg_handle()
@@ -415,8 +439,16 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
         pin = static_cast<unsigned char *>(pin_acquire());
+        void *dp = nullptr;
+        if (pin && cudaHostGetDevicePointer(&dp, pin, 0) == cudaSuccess)
+            dpin = static_cast<unsigned char *>(dp);
+        else
+            cudaGetLastError();
         CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        CK(cudaStreamCreateWithFlags(&st3, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_io0, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_io1, cudaEventDisableTiming));
     }
     hs.resize(n);
     hn.resize(n);
@@ -1169,6 +1201,15 @@ void msg_handle::enqueue_md_step(bool record)
     k_vv_skin<<<nchunk, SK_THREADS, 0, st>>>(dsys, chunks, inv, pos[0], vel[0], acc[0], dsum[0], posfx, r2o, sc);
     tend(TM_POS);
     launches += 1;
+    if (io_ro) {
+        // the new positions are final: send them to the host beside the force work
+        CK(cudaEventRecord(ev_io0, st));
+        CK(cudaStreamWaitEvent(st3, ev_io0, 0));
+        const int nb = (hs[io_ro_sys].n + STATE_BLOCK - 1) / STATE_BLOCK;
+        k_state_out<<<nb, STATE_BLOCK, 0, st3>>>(dsys, io_ro_sys, pos[0], vel[0], acc[0], io_ro, nullptr, nullptr, inv);
+        launches += 1;
+        CK(cudaEventRecord(ev_io1, st3));
+    }
     enqueue_forces(1, record, true);
     if (!use_cond) enqueue_rebuild();
 }
@@ -1240,12 +1281,18 @@ int msg_handle::rebuild_checked(const std::vector<int> &flags)
     return rc;
 }
 
+void msg_handle::drop_one(StepGraph &gr)
+{
+    if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    for (cudaEvent_t e : gr.ta) cudaEventDestroy(e);
+    for (cudaEvent_t e : gr.tb) cudaEventDestroy(e);
+    gr = StepGraph();
+}
+
 void msg_handle::drop_graph()
 {
-    if (graph.exec) cudaGraphExecDestroy(graph.exec);
-    for (cudaEvent_t e : graph.ta) cudaEventDestroy(e);
-    for (cudaEvent_t e : graph.tb) cudaEventDestroy(e);
-    graph = StepGraph();
+    drop_one(graph);
+    drop_one(iograph);
 }
 
 void msg_handle::ensure_graph(int kind, bool record, uint64_t seed)
@@ -1254,7 +1301,26 @@ void msg_handle::ensure_graph(int kind, bool record, uint64_t seed)
         (kind == 0 || graph.seed == seed) && graph.hist == (record ? hist : nullptr) &&
         graph.hist_cap == (record ? hist_cap : 0))
         return;
-    drop_graph();
+    drop_one(graph);
+    double *none[3] = {nullptr, nullptr, nullptr};
+    build_graph(graph, kind, record, seed, -1, none);
+}
+
+// One MD step with the host exchange of msg_velver_host on page-locked arrays:
+// the conversion kernels read and write the caller's arrays in place, and the
+// read-backs follow the rebuild node -- one launch, one wait.
+void msg_handle::ensure_io_graph(bool record, int io_sys, double *const io[3])
+{
+    if (iograph.exec && iograph.record == record && iograph.io_sys == io_sys && iograph.io[0] == io[0] &&
+        iograph.io[1] == io[1] && iograph.io[2] == io[2] && iograph.hist == (record ? hist : nullptr) &&
+        iograph.hist_cap == (record ? hist_cap : 0) && !timing)
+        return;
+    drop_one(iograph);
+    build_graph(iograph, 0, record, 0, io_sys, io);
+}
+
+void msg_handle::build_graph(StepGraph &gr, int kind, bool record, uint64_t seed, int io_sys, double *const io[3])
+{
     CK(cudaStreamSynchronize(st));
     flush_timers();
     cudaGraph_t g;
@@ -1265,10 +1331,30 @@ void msg_handle::ensure_graph(int kind, bool record, uint64_t seed)
     CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     capturing = true;
     use_cond = 1;
+    if (io_sys >= 0) {
+        // io[] are the mapped device addresses of the caller's page-locked arrays:
+        // the conversion kernels read and write them directly, no staging copies
+        const int nb = (hs[io_sys].n + STATE_BLOCK - 1) / STATE_BLOCK;
+        k_state_in<<<nb, STATE_BLOCK, 0, st>>>(dsys, io_sys, io[0], io[1], io[2], pos[0], vel[0], acc[0], posfx, inv,
+                                               record ? stepctr : nullptr);
+        launches += 1;
+        io_ro = io[0];
+        io_ro_sys = io_sys;
+    }
     if (kind == 0)
         enqueue_md_step(record);
     else
         enqueue_bd_step(seed, nullptr, nullptr, record);
+    io_ro = nullptr;
+    io_ro_sys = -1;
+    if (io_sys >= 0) {
+        if (io[1] || io[2]) {
+            const int nb = (hs[io_sys].n + STATE_BLOCK - 1) / STATE_BLOCK;
+            k_state_out<<<nb, STATE_BLOCK, 0, st>>>(dsys, io_sys, pos[0], vel[0], acc[0], nullptr, io[1], io[2], inv);
+            launches += 1;
+        }
+        if (io[0] && kind == 0) CK(cudaStreamWaitEvent(st, ev_io1, 0));
+    }
     use_cond = 0;
     // the rebuild: an IF node after everything captured so far
     tbeg(TM_REBUILD);
@@ -1286,6 +1372,14 @@ void msg_handle::ensure_graph(int kind, bool record, uint64_t seed)
     CK(cudaGraphAddNode(&cn, g, deps, nd, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     CK(cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies));
+    if (io_sys >= 0) {
+        // read-backs after the rebuild, straight into the mapped pinned block: the
+        // longest rows (list growth), the energies, the error word
+        k_readback<<<1, 256, 0, st>>>(nmaxrow, nsys, record ? hist : nullptr, record ? nsys * ESZ : 0, errw,
+                                      map_host(pin_rows()), record ? map_host(pin_hist((size_t)nsys * ESZ)) : nullptr,
+                                      map_host(pin_err()));
+        launches += 1;
+    }
     cudaEvent_t rb_begin = timing ? open_ev[TM_REBUILD] : nullptr;
     if (timing) {
         cudaEvent_t b = get_event();
@@ -1304,39 +1398,43 @@ void msg_handle::ensure_graph(int kind, bool record, uint64_t seed)
     cudaGraph_t bdone;
     CK(cudaStreamEndCapture(st, &bdone));
     timing = tsave;
-    CK(cudaGraphInstantiate(&graph.exec, g, 0));
+    CK(cudaGraphInstantiate(&gr.exec, g, 0));
     CK(cudaGraphDestroy(g));
-    graph.kind = kind;
-    graph.record = record;
-    graph.timing = timing;
-    graph.seed = seed;
-    graph.hist = record ? hist : nullptr;
-    graph.hist_cap = record ? hist_cap : 0;
-    graph.launches = launches - l0;
+    gr.kind = kind;
+    gr.record = record;
+    gr.timing = timing;
+    gr.seed = seed;
+    gr.hist = record ? hist : nullptr;
+    gr.hist_cap = record ? hist_cap : 0;
+    gr.launches = launches - l0;
+    gr.io_sys = io_sys;
+    for (int k = 0; k < 3; ++k) gr.io[k] = io[k];
     launches = l0;
     // events captured as graph nodes stay with the graph and are read after each launch
     for (size_t q = p0; q < pend_k.size(); ++q) {
-        graph.tk.push_back(pend_k[q]);
-        graph.ta.push_back(pend_a[q]);
-        graph.tb.push_back(pend_b[q]);
+        gr.tk.push_back(pend_k[q]);
+        gr.ta.push_back(pend_a[q]);
+        gr.tb.push_back(pend_b[q]);
     }
     pend_k.resize(p0);
     pend_a.resize(p0);
     pend_b.resize(p0);
 }
 
-void msg_handle::launch_graph()
+void msg_handle::launch_graph() { launch_one(graph); }
+
+void msg_handle::launch_one(StepGraph &gr)
 {
-    CK(cudaGraphLaunch(graph.exec, st));
-    launches += graph.launches;
-    if (graph.timing) {
+    CK(cudaGraphLaunch(gr.exec, st));
+    launches += gr.launches;
+    if (gr.timing) {
         // the graph's event nodes are re-recorded by every launch: read them now
         CK(cudaStreamSynchronize(st));
-        for (size_t q = 0; q < graph.tk.size(); ++q) {
+        for (size_t q = 0; q < gr.tk.size(); ++q) {
             float ms = 0.0f;
-            CK(cudaEventElapsedTime(&ms, graph.ta[q], graph.tb[q]));
-            tm_ms[graph.tk[q]] += ms;
-            tm_n[graph.tk[q]] += 1;
+            CK(cudaEventElapsedTime(&ms, gr.ta[q], gr.tb[q]));
+            tm_ms[gr.tk[q]] += ms;
+            tm_n[gr.tk[q]] += 1;
         }
     }
 }
@@ -1355,6 +1453,13 @@ int msg_handle::check()
     }
     CK(cudaGetLastError());
     flush_timers();
+    return check_word(e);
+}
+
+// Turns a device error word into a status and message, and clears what an aborted
+// step may have left behind.
+int msg_handle::check_word(const ErrWord &e)
+{
     if (e.code) {
         static const char *names[] = {"ok", "r2 < r2umin (pair below the table minimum)", "table interval overrun",
                                       "neighbour-list capacity exceeded", "cuda", "device timeout", "argument",
@@ -1484,7 +1589,7 @@ static void upload_state(msg_handle *h, int32_t isys, const double *ro, const do
     const SysDev &S = h->hs[isys];
     // one staging region per array, so the copies and conversions do not wait on each other
     h->ensure_stage(9 * (size_t)S.n);
-    const int c = h->cur, nb = (S.n + 255) / 256;
+    const int c = h->cur, nb = (S.n + STATE_BLOCK - 1) / STATE_BLOCK;
     const double *src[3] = {ro, rod, rodd};
     const double *stg[3] = {nullptr, nullptr, nullptr};
     for (int k = 0; k < 3; ++k) {
@@ -1494,8 +1599,8 @@ static void upload_state(msg_handle *h, int32_t isys, const double *ro, const do
         stg[k] = p;
     }
     if (ro || rod || rodd) {
-        k_state_in<<<nb, 256, 0, h->st>>>(h->dsys, isys, stg[0], stg[1], stg[2], h->pos[c], h->vel[c], h->acc[c],
-                                          h->posfx, h->inv);
+        k_state_in<<<nb, STATE_BLOCK, 0, h->st>>>(h->dsys, isys, stg[0], stg[1], stg[2], h->pos[c], h->vel[c],
+                                                  h->acc[c], h->posfx, h->inv, nullptr);
         h->launches += 1;
     }
     if (ro) h->placed[isys] = 1;
@@ -1506,14 +1611,14 @@ static void download_state(msg_handle *h, int32_t isys, double *ro, double *rod,
 {
     const SysDev &S = h->hs[isys];
     h->ensure_stage(9 * (size_t)S.n);
-    const int c = h->cur, nb = (S.n + 255) / 256;
+    const int c = h->cur, nb = (S.n + STATE_BLOCK - 1) / STATE_BLOCK;
     double *dst[3] = {ro, rod, rodd};
     double *stg[3] = {nullptr, nullptr, nullptr};
     for (int k = 0; k < 3; ++k)
         if (dst[k]) stg[k] = h->stage + 3 * (size_t)S.n * k;
     if (ro || rod || rodd) {
-        k_state_out<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->pos[c], h->vel[c], h->acc[c], stg[0], stg[1], stg[2],
-                                           h->inv);
+        k_state_out<<<nb, STATE_BLOCK, 0, h->st>>>(h->dsys, isys, h->pos[c], h->vel[c], h->acc[c], stg[0], stg[1],
+                                                   stg[2], h->inv);
         h->launches += 1;
     }
     for (int k = 0; k < 3; ++k)
@@ -1763,14 +1868,71 @@ extern "C" int msg_velver(msg_handle *h, int32_t nsteps, int32_t isys, msg_energ
     API_END
 }
 
+// The device address of a caller's host array of `bytes` bytes when the GPU may
+// read and write it in place: page-locked, mapped at the same address, 8-byte
+// aligned, and wholly inside one page-locked allocation (the driver's address-range
+// attributes).  Null otherwise, and for a null array.
+static double *mapped_span(double *p, size_t bytes)
+{
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 7)) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || a.devicePointer != static_cast<void *>(p)) return nullptr;
+    using RangeFn = CUresult (*)(void *, CUpointer_attribute, CUdeviceptr);
+    static RangeFn get = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuPointerGetAttribute", &fn, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            fn = nullptr;
+        }
+        return reinterpret_cast<RangeFn>(fn);
+    }();
+    if (!get) return nullptr;
+    CUdeviceptr start = 0;
+    size_t size = 0;
+    const CUdeviceptr at = reinterpret_cast<CUdeviceptr>(p);
+    if (get(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, at) != CUDA_SUCCESS ||
+        get(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, at) != CUDA_SUCCESS)
+        return nullptr;
+    if (at < start || at - start + bytes > size) return nullptr;
+    return p;
+}
+
 extern "C" int msg_velver_host(msg_handle *h, int32_t isys, int32_t nsteps, double *ro, double *rod, double *rodd,
                                msg_energy *e)
 {
     if (!h || isys < 0 || isys >= h->nsys || nsteps < 0) return MSG_ERR_ARG;
     API_BEGIN
+    const bool rec = e != nullptr;
+    // one step on page-locked host arrays: the whole exchange is one graph launch and one wait
+    const size_t nbytes = 3 * sizeof(double) * (size_t)h->hs[isys].n;
+    double *io[3] = {mapped_span(ro, nbytes), mapped_span(rod, nbytes), mapped_span(rodd, nbytes)};
+    if (h->use_graphs && !h->timing && nsteps == 1 && h->dpin && h->pin_rows() &&
+        (!rec || h->pin_hist((size_t)h->nsys * ESZ)) && (ro || rod || rodd) && (!ro || io[0]) &&
+        (!rod || io[1]) && (!rodd || io[2])) {
+        if (rec && h->hist_cap < 1) prepare_hist(h, 1);
+        h->ensure_io_graph(rec, isys, io);
+        if (ro) h->placed[isys] = 1;
+        h->launch_one(h->iograph);
+        CK(cudaStreamSynchronize(h->st));
+        CK(cudaGetLastError());
+        const int rc = h->check_word(*h->pin_err());
+        if (rc) return rc;
+        if (rec) fill_energy(h->pin_hist((size_t)h->nsys * ESZ) + (size_t)isys * ESZ, h->hs[isys].natat, e);
+        if (h->grow_lists(h->pin_rows())) {
+            std::vector<int> all(h->placed.begin(), h->placed.end());
+            return h->rebuild_checked(all);
+        }
+        return MSG_OK;
+    }
     // the host arrays continue the device's trajectory: the list and drosum stay valid
     upload_state(h, isys, ro, rod, rodd);
-    const bool rec = e != nullptr;
     if (rec) prepare_hist(h, nsteps);
     if (h->use_graphs && nsteps > 0) {
         h->ensure_graph(0, rec, 0);

@@ -571,50 +571,96 @@ __global__ void k_to_molsim(const double4 *__restrict__ src, double *__restrict_
     dst[3 * o + 2] = v.z * scale;
 }
 
+// Particles one block of k_state_in / k_state_out converts.
+constexpr int STATE_BLOCK = 256;
+
 // Positions, velocities and accelerations of one system from MOLSIM layout
-// (three staged [n][3] arrays; a null one is skipped) into the internal
-// order, with the fixed-point mirror of the positions: one launch per state.
-__global__ void k_state_in(const SysDev *__restrict__ sysv, int sys, const double *__restrict__ sro,
-                           const double *__restrict__ srod, const double *__restrict__ srodd,
-                           double4 *__restrict__ pos, double4 *__restrict__ vel, double4 *__restrict__ acc,
-                           int4 *__restrict__ posfx, const int *__restrict__ inv)
+// ([n][3] arrays; a null one is skipped) into the internal order, with the
+// fixed-point mirror of the positions: one launch per state.  The arrays are read
+// through shared memory so that every warp load covers contiguous doubles: the
+// sources may be device staging buffers or the caller's mapped page-locked
+// arrays, read straight over the bus.  A non-null zero_ctr is cleared by the
+// first thread.
+__global__ void __launch_bounds__(STATE_BLOCK) k_state_in(
+    const SysDev *__restrict__ sysv, int sys, const double *__restrict__ sro, const double *__restrict__ srod,
+    const double *__restrict__ srodd, double4 *__restrict__ pos, double4 *__restrict__ vel,
+    double4 *__restrict__ acc, int4 *__restrict__ posfx, const int *__restrict__ inv,
+    unsigned long long *__restrict__ zero_ctr)
 {
+    __shared__ double sb[3][3 * STATE_BLOCK];
     const SysDev &S = sysv[sys];
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= S.n) return;
-    const int i = inv[S.off + o];
+    const int o0 = blockIdx.x * STATE_BLOCK, t = threadIdx.x;
+    if (zero_ctr && blockIdx.x == 0 && t == 0) *zero_ctr = 0ull;
+    const int cnt = min(STATE_BLOCK, S.n - o0);
+    if (cnt <= 0) return;
+    const double *src[3] = {sro, srod, srodd};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (!src[k]) continue;
+        const double *p = src[k] + 3 * (size_t)o0;
+        for (int e = t; e < 3 * cnt; e += STATE_BLOCK) sb[k][e] = p[e];
+    }
+    __syncthreads();
+    if (t >= cnt) return;
+    const int i = inv[S.off + o0 + t];
     if (sro) {
         double4 v = pos[i];                       // .w holds the charge
-        v.x = sro[3 * o];
-        v.y = sro[3 * o + 1];
-        v.z = sro[3 * o + 2];
+        v.x = sb[0][3 * t];
+        v.y = sb[0][3 * t + 1];
+        v.z = sb[0][3 * t + 2];
         pos[i] = v;
         posfx[i] = fx_pos(v, S);
     }
-    if (srod) vel[i] = make_double4(srod[3 * o], srod[3 * o + 1], srod[3 * o + 2], 0.0);
-    if (srodd) acc[i] = make_double4(srodd[3 * o], srodd[3 * o + 1], srodd[3 * o + 2], 0.0);
+    if (srod) vel[i] = make_double4(sb[1][3 * t], sb[1][3 * t + 1], sb[1][3 * t + 2], 0.0);
+    if (srodd) acc[i] = make_double4(sb[2][3 * t], sb[2][3 * t + 1], sb[2][3 * t + 2], 0.0);
 }
 
-// The reverse: internal order -> three MOLSIM-layout staging arrays.
-__global__ void k_state_out(const SysDev *__restrict__ sysv, int sys, const double4 *__restrict__ pos,
-                            const double4 *__restrict__ vel, const double4 *__restrict__ acc,
-                            double *__restrict__ dro, double *__restrict__ drod, double *__restrict__ drodd,
-                            const int *__restrict__ inv)
+// The reverse: internal order -> MOLSIM-layout arrays (device staging buffers or
+// mapped page-locked host arrays), written through shared memory in contiguous runs.
+__global__ void __launch_bounds__(STATE_BLOCK) k_state_out(
+    const SysDev *__restrict__ sysv, int sys, const double4 *__restrict__ pos, const double4 *__restrict__ vel,
+    const double4 *__restrict__ acc, double *__restrict__ dro, double *__restrict__ drod,
+    double *__restrict__ drodd, const int *__restrict__ inv)
 {
+    __shared__ double sb[3][3 * STATE_BLOCK];
     const SysDev &S = sysv[sys];
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= S.n) return;
-    const int i = inv[S.off + o];
+    const int o0 = blockIdx.x * STATE_BLOCK, t = threadIdx.x;
+    const int cnt = min(STATE_BLOCK, S.n - o0);
+    if (cnt <= 0) return;
     const double4 *src[3] = {pos, vel, acc};
     double *dst[3] = {dro, drod, drodd};
+    if (t < cnt) {
+        const int i = inv[S.off + o0 + t];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (!dst[k]) continue;
+            const double4 v = src[k][i];
+            sb[k][3 * t] = v.x;
+            sb[k][3 * t + 1] = v.y;
+            sb[k][3 * t + 2] = v.z;
+        }
+    }
+    __syncthreads();
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         if (!dst[k]) continue;
-        const double4 v = src[k][i];
-        dst[k][3 * o] = v.x;
-        dst[k][3 * o + 1] = v.y;
-        dst[k][3 * o + 2] = v.z;
+        double *p = dst[k] + 3 * (size_t)o0;
+        for (int e = t; e < 3 * cnt; e += STATE_BLOCK) p[e] = sb[k][e];
     }
+}
+
+// End-of-step read-back into the handle's mapped pinned block: the longest row of
+// every system, one step of energy history (nh doubles, hist may be null) and the
+// error word -- one small launch in place of three copies.
+__global__ void k_readback(const int *__restrict__ nmaxrow, int nsys, const double *__restrict__ hist, int nh,
+                           const ErrWord *__restrict__ errw, int *__restrict__ prow, double *__restrict__ phist,
+                           ErrWord *__restrict__ perr)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    for (int s = t; s < nsys; s += nt) prow[s] = nmaxrow[s];
+    if (hist)
+        for (int e = t; e < nh; e += nt) phist[e] = hist[e];
+    if (t == 0) *perr = *errw;
 }
 
 // rodd = massip * forceo (GetLinAcc, Src/md.F90:601-617)

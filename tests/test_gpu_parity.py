@@ -271,11 +271,17 @@ def test_config2_colloid_bd_full_size(precision):
     assert np.abs(d).max() < (1e-9 if precision == "fp64" else 1e-5)
 
 
+@pytest.mark.parametrize("host", ["pageable", "pinned", "registered"])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_velver_host_equals_put_step_get(precision):
+def test_velver_host_equals_put_step_get(precision, host):
     """msg_velver_host (state in, steps, state out in one call) gives what
     msg_put_state + msg_velver + msg_get_state give: bit for bit in the mixed path;
-    to FP64 rounding in the FP64 path (its charge grid is summed with FP64 atomics)."""
+    to FP64 rounding in the FP64 path (its charge grid is summed with FP64 atomics).
+    Page-locked host arrays (allocated pinned, or plain arrays registered with
+    cudaHostRegister) take the one-graph zero-copy path (one step per call),
+    pageable ones the call-by-call path."""
+    import torch
+
     s = dict(Hp.pe_small())
     t = Hp.oracle_table(s)
     a = Engine(s, t, precision=precision)
@@ -285,11 +291,35 @@ def test_velver_host_equals_put_step_get(precision):
         g.GetLinAcc()
     sa = a.get_state()
     sb = b.get_state()
-    for _ in range(3):
+    pinned = host != "pageable"
+    registered = []
+    if host == "pinned":
+        for k in ("ro", "rod", "rodd"):
+            buf = torch.empty(sb[k].shape, dtype=torch.float64, pin_memory=True).numpy()
+            buf[:] = sb[k]
+            sb[k] = buf
+    elif host == "registered":
+        rt = torch.cuda.cudart()
+        for k in ("ro", "rod", "rodd"):
+            sb[k] = np.ascontiguousarray(sb[k])
+            # cudaHostRegisterMapped = 2
+            assert int(rt.cudaHostRegister(sb[k].ctypes.data, sb[k].nbytes, 2)) == 0
+            registered.append(sb[k])
+    nstep = 1 if pinned else 2
+    for _ in range(4):
         a.put_state(0, sa["ro"], sa["rod"], sa["rodd"], keep_list=True)
-        ea = a.VelVer(2)
+        la = a.launch_count()
+        ea = a.VelVer(nstep)
+        la = a.launch_count() - la
         sa = a.get_state()
-        eb = b.VelVerHost(sb, nsteps=2)
+        lb = b.launch_count()
+        eb = b.VelVerHost(sb, nsteps=nstep)
+        lb = b.launch_count() - lb
+        # pageable: conversion in, the step graph, conversion out; page-locked: the same
+        # step graph carrying conversion in, positions out early, the rest out and the read-back
+        assert lb == la + (4 if pinned else 2), (la, lb)
+    for arr in registered:
+        assert int(torch.cuda.cudart().cudaHostUnregister(arr.ctypes.data)) == 0
     box = s["boxlen"][0]
     for k in ("ro", "rod", "rodd"):
         if precision == "mixed":
