@@ -151,6 +151,23 @@ double or_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
     return xnew;
 }
 
+/* AlphaToNcut, Src/energy.F90:7066-7081 (charged system, lq2sum == 0) */
+int32_t or_alpha_to_ncut(double uewaldtol, double q2sum, double epsi_four_pi, double boxlenshort,
+                         double ualpha, int32_t *status)
+{
+    double y = (uewaldtol / (q2sum * epsi_four_pi)) * (Pi * Pi / ((ualpha * ualpha) * boxlenshort));
+    double xold = 1.0, xnew = 0.0;
+    int i;
+    for (i = 1; i <= 40; ++i) {
+        xnew = (ualpha * boxlenshort / Pi) *
+               sqrt(-log(y * xold / (1.0 + 1.0 / (ualpha * boxlenshort * sqrt(xold)))));
+        if (fabs(xold - xnew) / xnew < 1.0e-6) break;
+        xold = xnew;
+    }
+    if (status) *status = (i > 40) ? 6 : 0;
+    return (int32_t)(xnew + 1.0);
+}
+
 /* EwaldErrorUReal, Src/potential.F90:2995-3018 (charges) */
 double or_ewald_error_ureal(double q2sum, double l, double alpha, double rcut, double unit)
 {
@@ -500,6 +517,11 @@ struct or_sys {
     int maxnneigh; int32_t *nneighpn, *jpnlist;
     int lewald, order, s, lsurf; double ualpha, epsfp;
     double *meshfac, *energyfac, *virfac, *qmesh, *fqmesh;
+    /* standard Ewald (lewald == 2): k-space cut, kfac in the sums' order, work arrays */
+    int ncut, ncut2, nkvec;
+    double *kfac;
+    double *eik[3];          /* [np][ncut+1] complex (re, im) */
+    double *eyz, *eikr;      /* [np] 2 complex; [np] 4 complex */
     int nbond; int32_t *bond_ij; double *bond_k, *bond_eq; int32_t *bond_p;
     double tstep;
     int lcellbuild;
@@ -511,6 +533,37 @@ static void *dup(const void *p, size_t n)
     if (p && n) memcpy(q, p, n);
     else memset(q, 0, n ? n : 1);
     return q;
+}
+
+/* EwaldSetup, txewaldrec = 'std': ncut2 from ncutregion and kfac over the
+ * k-vectors in the order the sums visit them, Src/energy.F90:6752-6782 */
+static void ewald_setup_std(or_sys *s, int ncut, int cube)
+{
+    int nx, ny, nz, n = 0, m;
+    double tpbi[3], fac0 = 2.0 * Pi / s->vol;
+    for (m = 0; m < 3; ++m) tpbi[m] = 2.0 * Pi * s->boxleni[m];
+    s->ncut = ncut;
+    s->ncut2 = cube ? 3 * ncut * ncut : ncut * ncut;
+    s->kfac = malloc(sizeof(double) * ((size_t)ncut + 1) * (ncut + 1) * (ncut + 1));
+    for (nz = 0; nz <= ncut; ++nz) {
+        double facz = (nz == 0) ? 1.0 : 2.0;
+        for (ny = 0; ny <= ncut; ++ny) {
+            double facy = (ny == 0) ? 0.5 : 1.0;
+            for (nx = 0; nx <= ncut; ++nx) {
+                double facx, k2;
+                if (nx * nx + ny * ny + nz * nz > s->ncut2) continue;
+                if (nx == 0 && ny == 0 && nz == 0) continue;
+                facx = (nx == 0) ? 0.5 : 1.0;
+                k2 = (nx * tpbi[0]) * (nx * tpbi[0]) + (ny * tpbi[1]) * (ny * tpbi[1]) +
+                     (nz * tpbi[2]) * (nz * tpbi[2]);
+                s->kfac[n++] = fac0 * facz * facy * facx * exp(-k2 / (4.0 * (s->ualpha * s->ualpha))) / k2;
+            }
+        }
+    }
+    s->nkvec = n;
+    for (m = 0; m < 3; ++m) s->eik[m] = malloc(sizeof(double) * 2 * (size_t)s->np * (ncut + 1));
+    s->eyz = malloc(sizeof(double) * 4 * (size_t)s->np);
+    s->eikr = malloc(sizeof(double) * 8 * (size_t)s->np);
 }
 
 or_sys *or_create(const or_params *p)
@@ -562,7 +615,9 @@ or_sys *or_create(const or_params *p)
     s->lsurf = p->lsurf;
     s->ualpha = p->ualpha;
     s->epsfp = p->epsi_four_pi;
-    if (s->lewald) {
+    if (s->lewald == 2) {
+        ewald_setup_std(s, p->ncut, p->ncutregion);
+    } else if (s->lewald) {
         size_t n = (size_t)s->s * s->s * s->s;
         h = s->s / 2 + 1;
         s->meshfac = malloc(sizeof(double) * h * h * h);
@@ -591,6 +646,7 @@ void or_destroy(or_sys *s)
     free(s->ubuf); free(s->iubuflow); free(s->r2umin); free(s->r2atat);
     free(s->nneighpn); free(s->jpnlist);
     free(s->meshfac); free(s->energyfac); free(s->virfac); free(s->qmesh); free(s->fqmesh);
+    free(s->kfac); free(s->eik[0]); free(s->eik[1]); free(s->eik[2]); free(s->eyz); free(s->eikr);
     free(s->bond_ij); free(s->bond_k); free(s->bond_eq); free(s->bond_p);
     free(s);
 }
@@ -890,12 +946,113 @@ static void uewald_rec_spm(or_sys *s, double *urec, double *virrec)
     *virrec = virloc;
 }
 
+/* Complex arithmetic on (re, im) pairs, as Fortran complex(8) evaluates it. */
+typedef struct { double r, i; } cx;
+static cx cmul(cx a, cx b)
+{
+    cx c;
+    c.r = a.r * b.r - a.i * b.i;
+    c.i = a.r * b.i + a.i * b.r;
+    return c;
+}
+
+/* UEwaldRecStd (serial branch) with EwaldSetArray, Src/energy.F90:1045-1100, 1401-1426.
+ * Returns the reciprocal energy and virial before the EpsiFourPi scale of UEwald and
+ * adds the reciprocal forces (already scaled by EpsiFourPi) into s->force. */
+static void uewald_rec_std(or_sys *s, double *urec, double *virrec)
+{
+    const int np = s->np, nc = s->ncut, ncut2 = s->ncut2;
+    const size_t w = (size_t)nc + 1;
+    cx *ex = (cx *)s->eik[0], *ey = (cx *)s->eik[1], *ez = (cx *)s->eik[2];
+    cx *eyz = (cx *)s->eyz, *eikr = (cx *)s->eikr;
+    double tpbi[3], uloc = 0.0, virloc = *virrec;
+    int ia, nx, ny, nz, m, kn = 0, icut;
+    cx *e[3];
+    e[0] = ex; e[1] = ey; e[2] = ez;
+    for (m = 0; m < 3; ++m) tpbi[m] = 2.0 * Pi * s->boxleni[m];
+    /* EwaldSetArray: e(0) = 1, e(1) = exp(i 2pi/L r), e(n) = e(n-1) e(1) */
+    for (ia = 0; ia < np; ++ia)
+        for (m = 0; m < 3; ++m) {
+            cx *t = e[m] + (size_t)ia * w;
+            t[0].r = 1.0; t[0].i = 0.0;
+            t[1].r = cos(tpbi[m] * s->ro[3 * ia + m]);
+            t[1].i = sin(tpbi[m] * s->ro[3 * ia + m]);
+        }
+    for (icut = 2; icut <= nc; ++icut)
+        for (ia = 0; ia < np; ++ia)
+            for (m = 0; m < 3; ++m) {
+                cx *t = e[m] + (size_t)ia * w;
+                t[icut] = cmul(t[icut - 1], t[1]);
+            }
+    for (nz = 0; nz <= nc; ++nz) {
+        for (ny = 0; ny <= nc; ++ny) {
+            if (ny * ny + nz * nz > ncut2) continue;
+            for (ia = 0; ia < np; ++ia) {
+                cx yc = ey[(size_t)ia * w + ny], zz = ez[(size_t)ia * w + nz];
+                cx yconj;
+                yconj.r = yc.r; yconj.i = -yc.i;
+                eyz[2 * ia] = cmul(yconj, zz);      /* eikyzm */
+                eyz[2 * ia + 1] = cmul(yc, zz);     /* eikyzp */
+            }
+            for (nx = 0; nx <= nc; ++nx) {
+                cx sum[4];
+                double term, kfac2, kx, ky, kz, k2;
+                int c;
+                if (nx * nx + ny * ny + nz * nz > ncut2) continue;
+                if (nx == 0 && ny == 0 && nz == 0) continue;
+                for (c = 0; c < 4; ++c) sum[c].r = sum[c].i = 0.0;
+                for (ia = 0; ia < np; ++ia) {
+                    cx x = ex[(size_t)ia * w + nx], qxc, qx;
+                    const double q = s->az[ia];
+                    qxc.r = q * x.r; qxc.i = q * (-x.i);    /* az * conjg(eikx) */
+                    qx.r = q * x.r; qx.i = q * x.i;         /* az * eikx */
+                    eikr[4 * ia] = cmul(qxc, eyz[2 * ia]);
+                    eikr[4 * ia + 1] = cmul(qxc, eyz[2 * ia + 1]);
+                    eikr[4 * ia + 2] = cmul(qx, eyz[2 * ia]);
+                    eikr[4 * ia + 3] = cmul(qx, eyz[2 * ia + 1]);
+                    for (c = 0; c < 4; ++c) {
+                        sum[c].r = sum[c].r + eikr[4 * ia + c].r;
+                        sum[c].i = sum[c].i + eikr[4 * ia + c].i;
+                    }
+                }
+                term = 0.0;
+                for (c = 0; c < 4; ++c) term = term + (sum[c].r * sum[c].r + sum[c].i * sum[c].i);
+                term = s->kfac[kn] * term;
+                uloc = uloc + term;
+                kfac2 = s->epsfp * 2.0 * s->kfac[kn];
+                kx = kfac2 * nx * tpbi[0];
+                ky = kfac2 * ny * tpbi[1];
+                kz = kfac2 * nz * tpbi[2];
+                for (ia = 0; ia < np; ++ia) {
+                    const cx *r = eikr + 4 * (size_t)ia;
+                    double fmm = -r[0].r * sum[0].i + r[0].i * sum[0].r;
+                    double fmp = -r[1].r * sum[1].i + r[1].i * sum[1].r;
+                    double fpm = -r[2].r * sum[2].i + r[2].i * sum[2].r;
+                    double fpp = -r[3].r * sum[3].i + r[3].i * sum[3].r;
+                    s->force[3 * ia] = s->force[3 * ia] + kx * (-fmm - fmp + fpm + fpp);
+                    s->force[3 * ia + 1] = s->force[3 * ia + 1] + ky * (-fmm + fmp - fpm + fpp);
+                    s->force[3 * ia + 2] = s->force[3 * ia + 2] + kz * (fmm + fmp + fpm + fpp);
+                }
+                k2 = (nx * tpbi[0]) * (nx * tpbi[0]) + (ny * tpbi[1]) * (ny * tpbi[1]) +
+                     (nz * tpbi[2]) * (nz * tpbi[2]);
+                virloc = virloc - (1.0 - k2 / (2.0 * (s->ualpha * s->ualpha))) * term;
+                ++kn;
+            }
+        }
+    }
+    *urec = uloc;
+    *virrec = virloc;
+}
+
 /* UEwald + UEwaldSelf + UEwaldSurf, Src/energy.F90:905-958, 1301-1371 (monoatomic) */
 static void uewald(or_sys *s, double *urec_out, double *utot, double *virial)
 {
     double urec = 0.0, virrec = 0.0, q2 = 0.0;
     int ia;
-    uewald_rec_spm(s, &urec, &virrec);
+    if (s->lewald == 2)
+        uewald_rec_std(s, &urec, &virrec);
+    else
+        uewald_rec_spm(s, &urec, &virrec);
     for (ia = 0; ia < s->np; ++ia) q2 += s->az[ia] * s->az[ia];
     urec = urec - s->ualpha / sqrt(Pi) * q2;
     if (s->lsurf) {

@@ -39,6 +39,8 @@ void   or_cardinal_bspline(int order, double pos, int32_t *kmax,
                            double *values, double *derivs);  /* Src/mollib.F90:1629-1683 */
 double or_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
                         double boxlenshort, double rcut, int32_t *status); /* Src/energy.F90:7090-7105 */
+int32_t or_alpha_to_ncut(double uewaldtol, double q2sum, double epsi_four_pi,
+                         double boxlenshort, double ualpha, int32_t *status); /* Src/energy.F90:7066-7081 */
 double or_ewald_error_ureal(double q2sum, double l, double alpha, double rcut,
                             double unit);                   /* Src/potential.F90:2995-3018 */
 
@@ -92,7 +94,8 @@ typedef struct or_params {
     const int32_t *iubuflow; /* [natat] 1-based */
     const double *r2umin;    /* [natat] */
     const double *r2atat;    /* [natat] */
-    int32_t lewald, order, nmesh, lsurf;
+    int32_t lewald;          /* 0 none; 1 SPME (txewaldrec 'spm'); 2 standard Ewald ('std') */
+    int32_t order, nmesh, lsurf;
     double ualpha, epsi_four_pi;
     int32_t nbond;
     const int32_t *bond_ij;  /* [nbond][2] 1-based, in chain order */
@@ -102,6 +105,8 @@ typedef struct or_params {
     double tstep;
     int32_t maxnneigh;       /* row capacity of jpnlist */
     int32_t lcellbuild;      /* 1: build the Verlet list through cells (same pair set) */
+    int32_t ncut;            /* standard Ewald: largest |n| component of k = 2 pi n / L */
+    int32_t ncutregion;      /* standard Ewald: 0 'sphere' (|n|^2 <= ncut^2), 1 'cube' */
 } or_params;
 
 typedef struct or_sys or_sys;

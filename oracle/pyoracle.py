@@ -32,7 +32,8 @@ class Params(C.Structure):
                 ("nmesh", C.c_int32), ("lsurf", C.c_int32), ("ualpha", C.c_double),
                 ("epsi_four_pi", C.c_double), ("nbond", C.c_int32), ("bond_ij", i32p),
                 ("bond_k", f64p), ("bond_eq", f64p), ("bond_p", i32p), ("tstep", C.c_double),
-                ("maxnneigh", C.c_int32), ("lcellbuild", C.c_int32)]
+                ("maxnneigh", C.c_int32), ("lcellbuild", C.c_int32), ("ncut", C.c_int32),
+                ("ncutregion", C.c_int32)]
 
 
 def lib():
@@ -51,6 +52,8 @@ def lib():
         L.or_cardinal_bspline.argtypes = [C.c_int, C.c_double, i32p, f64p, f64p]
         L.or_rcut_to_alpha.restype = C.c_double
         L.or_rcut_to_alpha.argtypes = [C.c_double] * 5 + [i32p]
+        L.or_alpha_to_ncut.restype = C.c_int32
+        L.or_alpha_to_ncut.argtypes = [C.c_double] * 5 + [i32p]
         L.or_ewald_error_ureal.restype = C.c_double
         L.or_ewald_error_ureal.argtypes = [C.c_double] * 5
         L.or_pot_1_6_12.argtypes = [C.POINTER(TabParams), C.c_int, C.c_int, C.c_double, f64p, f64p, f64p]
@@ -112,6 +115,21 @@ def rcut_to_alpha(uewaldtol, q2sum, epsfp, boxlenshort, rcut):
     if st.value:
         raise RuntimeError("RcutToAlpha did not converge")
     return a
+
+
+def alpha_to_ncut(uewaldtol, q2sum, epsfp, boxlenshort, ualpha):
+    st = C.c_int32()
+    n = lib().or_alpha_to_ncut(uewaldtol, q2sum, epsfp, boxlenshort, ualpha, C.byref(st))
+    if st.value:
+        raise RuntimeError("AlphaToNcut did not converge")
+    return int(n)
+
+
+def ewald_mode(sysd):
+    """lewald as the oracle takes it: 0 none, 1 SPME, 2 standard Ewald (txewaldrec 'std')."""
+    if not sysd["lewald"]:
+        return 0
+    return 2 if sysd.get("ewaldrec", "spm") == "std" else 1
 
 
 def tab_params(pot):
@@ -210,10 +228,11 @@ class System:
                    _p(k["iptpn"], C.c_int32), _p(k["az"], C.c_double), _p(k["masspt"], C.c_double),
                    _p(k["ubuf"], C.c_double), len(k["ubuf"]), _p(k["iubuflow"], C.c_int32),
                    _p(k["r2umin"], C.c_double), _p(k["r2atat"], C.c_double),
-                   int(sysd["lewald"]), int(sysd["order"]), int(sysd["nmesh"]), int(sysd["lsurf"]),
+                   ewald_mode(sysd), int(sysd["order"]), int(sysd["nmesh"]), int(sysd["lsurf"]),
                    sysd["ualpha"], sysd["epsi_four_pi"], nb, _p(k["bond_ij"], C.c_int32),
                    _p(k["bond_k"], C.c_double), _p(k["bond_eq"], C.c_double),
-                   _p(k["bond_p"], C.c_int32), sysd["tstep"], self.maxnneigh, int(lcellbuild))
+                   _p(k["bond_p"], C.c_int32), sysd["tstep"], self.maxnneigh, int(lcellbuild),
+                   int(sysd.get("ncut", 0)), 1 if sysd.get("ncutregion", "sphere") == "cube" else 0)
         self.h = L.or_create(C.byref(P))
 
     def __del__(self):

@@ -19,12 +19,28 @@ def oracle_table(s):
     t = O.pot_tab(pot)
     t["ualpha"] = alpha
     t["r2atat"] = np.zeros(len(t["r2umin"]))
+    if s["lewald"] and s.get("ewaldrec", "spm") == "std":
+        # EwaldSetup iewaldopt=3: ncut from alpha (AlphaToNcut) unless the system fixes it
+        t["ncut"] = int(s.get("ncut") or O.alpha_to_ncut(s["uewaldtol"], q2, s["epsi_four_pi"],
+                                                         min(s["boxlen"]), alpha))
     return t
+
+
+def std_ewald(s, ncut=None, region="sphere"):
+    """The same system with standard Ewald (txewaldrec 'std') in reciprocal space."""
+    d = dict(s)
+    d["ewaldrec"] = "std"
+    d["ncutregion"] = region
+    if ncut:
+        d["ncut"] = int(ncut)
+    return d
 
 
 def oracle_system(s, t, cell=False, maxnneigh=None):
     d = dict(s)
     d["ualpha"] = t["ualpha"]
+    if "ncut" in t:
+        d["ncut"] = t["ncut"]
     return O.System(d, t, maxnneigh=maxnneigh or s["np"], lcellbuild=cell)
 
 

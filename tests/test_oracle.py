@@ -221,7 +221,8 @@ def test_madelung_constant_rock_salt():
 
 
 def _direct_ewald(ro, q, L, alpha, kmax=14):
-    """Independent standard Ewald sum (reciprocal part) for the SPME check."""
+    """Independent standard Ewald sum (reciprocal part): energy and forces (minus the
+    energy gradient), both in units of e^2/A before the EpsiFourPi scale."""
     V = L ** 3
     e = 0.0
     f = np.zeros_like(ro)
@@ -233,7 +234,7 @@ def _direct_ewald(ro, q, L, alpha, kmax=14):
     Sk = (q[:, None] * np.exp(1j * phase)).sum(0)
     w = 4 * np.pi / V * np.exp(-k2 / (4 * alpha ** 2)) / k2
     e = 0.5 * np.sum(w * np.abs(Sk) ** 2)
-    f = (q[:, None] * ((np.imag(np.exp(-1j * phase) * Sk[None, :]) * w[None, :]) @ K))
+    f = -(q[:, None] * ((np.imag(np.exp(-1j * phase) * Sk[None, :]) * w[None, :]) @ K))
     return e, f
 
 
@@ -333,3 +334,72 @@ def test_velocity_verlet_conserves_energy():
         e0 = e if e0 is None else e0
         drift.append(e - e0)
     assert max(abs(x) for x in drift) < 2e-3 * abs(ek)
+
+
+# ---------------------------------------------------------------- standard Ewald
+
+def test_alpha_to_ncut_fixed_point():
+    """AlphaToNcut (Src/energy.F90:7066-7081): the 40-step fixed point, restated
+    here as a plain loop, and ncut grows as the tolerance tightens."""
+    q2, epsfp, L, alpha = 1.0, 17.72, 100.0, 0.0876
+    for tol in (1e-3, 1e-5, 1e-7):
+        y = (tol / (q2 * epsfp)) * (math.pi ** 2 / (alpha ** 2 * L))
+        xo = 1.0
+        for _ in range(40):
+            xn = (alpha * L / math.pi) * math.sqrt(-math.log(y * xo / (1 + 1 / (alpha * L * math.sqrt(xo)))))
+            if abs(xo - xn) / xn < 1e-6:
+                break
+            xo = xn
+        assert O.alpha_to_ncut(tol, q2, epsfp, L, alpha) == int(xn + 1)
+    assert O.alpha_to_ncut(1e-3, q2, epsfp, L, alpha) < O.alpha_to_ncut(1e-7, q2, epsfp, L, alpha)
+
+
+def _std_result(s, ncut, region):
+    d = Hp.std_ewald(s, ncut=ncut, region=region)
+    t = Hp.oracle_table(d)
+    o = Hp.oracle_system(d, t)
+    o.set_state(d["ro"], d["rod"])
+    o.set_vlist()
+    return o.utotal(), t
+
+
+def test_std_ewald_cube_equals_direct_sum():
+    """ncutregion 'cube' sums every k = 2 pi n / L with |n_i| <= ncut, as the direct
+    sum above does: the reciprocal energy agrees to rounding, and the difference of
+    two cut-offs (which cancels the pair forces) gives the direct sum's force
+    difference to rounding."""
+    s = dict(Hp.electrolyte_small())
+    q = np.asarray(s["az"], float)
+    ro = np.asarray(s["ro"], float)
+    L = s["boxlen"][0]
+    epsfp = s["epsi_four_pi"]
+    r6, t = _std_result(s, 6, "cube")
+    r3, _ = _std_result(s, 3, "cube")
+    alpha = t["ualpha"]
+    self_term = alpha / math.sqrt(math.pi) * np.sum(q * q)
+    e6, f6 = _direct_ewald(ro, q, L, alpha, kmax=6)
+    e3, f3 = _direct_ewald(ro, q, L, alpha, kmax=3)
+    assert abs(r6["urec"] / epsfp + self_term - e6) <= 1e-11 * abs(e6)
+    assert abs(r3["urec"] / epsfp + self_term - e3) <= 1e-11 * abs(e3)
+    df = r6["force"] - r3["force"]
+    want = epsfp * (f6 - f3)
+    assert Hp.rel_rms(df, want) <= 1e-9
+
+
+def test_std_ewald_sphere_agrees_with_converged_spme():
+    """With ncut from AlphaToNcut at uewaldtol (sphere), standard Ewald and an SPME
+    of order 6 on a fine grid compute the same Ewald sum: totals agree to the
+    tolerances both methods are set up for."""
+    s = dict(Hp.electrolyte_small())
+    s["nmesh"] = 48
+    s["order"] = 6
+    rs, t = _std_result(s, None, "sphere")
+    assert t["ncut"] >= 3
+    ts = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, ts)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    rp = o.utotal()
+    assert Hp.rel_rms(rs["force"], rp["force"]) <= 1e-4
+    assert Hp.rel(rs["urec"], rp["urec"]) <= 1e-5
+    assert Hp.rel(rs["virial"], rp["virial"]) <= 1e-5
