@@ -17,7 +17,7 @@
  *   msg_set_state / msg_get_state  -> the ro/rod/rodd globals (Src/mol.F90:1087-1098)
  *   msg_build_nlist                -> SetVList -> SetVListMD (Src/nlist.F90:686-759)
  *   msg_utotal                     -> UTotal (Src/energy.F90:280-434) with
- *                                     UTwoBodyA, UEwald(SPM), UBond
+ *                                     UTwoBodyA, UEwald (SPM or standard), UBond
  *   msg_get_linacc                 -> GetLinAcc (Src/md.F90:601-617)
  *   msg_velver                     -> MDDriver iSimulationStep: VelVer +
  *                                     GetKinEnergy (Src/md.F90:154-168, 252-410)
@@ -26,6 +26,7 @@
  *                                     (Src/bd.F90:53-59, 120-155) followed by NList
  * Set-up helpers that restate MOLSIM's own set-up for callers without it:
  *   msg_rcut_to_alpha              -> RcutToAlpha (Src/energy.F90:7090-7105)
+ *   msg_alpha_to_ncut              -> AlphaToNcut (Src/energy.F90:7066-7081)
  *   msg_pot_tab                    -> PotTwoBodyTab1/2/3 with Pot_1_6_12
  *                                     (Src/potential.F90:868-1258, 1349-1425)
  *
@@ -70,7 +71,8 @@ typedef struct msg_params {
     const int32_t *iubuflow; /* [natat] 1-based start of each type pair's table         */
     const double  *r2umin;   /* [natat] lower table limit, A^2                          */
     const double  *r2atat;   /* [natat] hard-core r^2 (0: none), A^2                    */
-    int32_t lewald;          /* 1: SPME reciprocal space                                */
+    int32_t lewald;          /* 0: none; 1: SPME (txewaldrec 'spm'); 2: standard Ewald
+                              * ('std', UEwaldRecStd, Src/energy.F90:964-1104)          */
     int32_t order;           /* B-spline order                                          */
     int32_t nmesh;           /* SPME grid edge (even)                                   */
     int32_t lsurf;           /* 1: add the surface (dipole) term                        */
@@ -85,6 +87,8 @@ typedef struct msg_params {
     const double  *bd_fac1;  /* [npt] BD drift factor (Src/bd.F90:138), may be NULL    */
     const double  *bd_fac2;  /* [npt] BD noise factor (Src/bd.F90:139), may be NULL    */
     int32_t maxnneigh;       /* row capacity hint for the neighbour list (0: automatic) */
+    int32_t ncut;            /* lewald 2: k = 2 pi n / L with 0 <= n_i <= ncut (1..100)  */
+    int32_t ncutregion;      /* lewald 2: 0 'sphere' (|n|^2 <= ncut^2), 1 'cube'         */
 } msg_params;
 
 typedef struct msg_handle msg_handle;
@@ -245,6 +249,9 @@ int  msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen[3], doubl
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,
                          double boxlenshort, double rcut, int32_t *status);
+/* ncut of the standard Ewald sum for alpha at uewaldtol (iewaldopt 3). */
+int32_t msg_alpha_to_ncut(double uewaldtol, double q2sum, double epsi_four_pi,
+                          double boxlenshort, double ualpha, int32_t *status);
 
 typedef struct msg_tab_params {
     int32_t npt;

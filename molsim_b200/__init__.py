@@ -5,4 +5,4 @@ C-ABI in include/molsim_gpu.h).  This package holds the Python mirror of the
 reference's entry points (engine.py), the seeded system generators
 (systems.py) and the build recipe (build.py).
 """
-from .engine import Engine, MolsimGpuError, pot_tab, prepare, rcut_to_alpha  # noqa: F401
+from .engine import Engine, MolsimGpuError, alpha_to_ncut, pot_tab, prepare, rcut_to_alpha  # noqa: F401

@@ -29,7 +29,8 @@ class MsgParams(C.Structure):
                 ("lewald", C.c_int32), ("order", C.c_int32), ("nmesh", C.c_int32), ("lsurf", C.c_int32),
                 ("ualpha", C.c_double), ("epsi_four_pi", C.c_double), ("nbond", C.c_int32),
                 ("bond_ij", i32p), ("bond_k", f64p), ("bond_eq", f64p), ("bond_p", i32p),
-                ("tstep", C.c_double), ("bd_fac1", f64p), ("bd_fac2", f64p), ("maxnneigh", C.c_int32)]
+                ("tstep", C.c_double), ("bd_fac1", f64p), ("bd_fac2", f64p), ("maxnneigh", C.c_int32),
+                ("ncut", C.c_int32), ("ncutregion", C.c_int32)]
 
 
 class MsgEnergy(C.Structure):
@@ -83,6 +84,7 @@ SIGNATURES = {
                                        C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, i32p, f64p,
                                        f64p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "msg_rcut_to_alpha": (C.c_double, [C.c_double] * 5 + [i32p]),
+    "msg_alpha_to_ncut": (C.c_int32, [C.c_double] * 5 + [i32p]),
     "msg_pot_tab": (C.c_int, [C.POINTER(MsgTabParams), f64p, C.c_int32, i32p, i32p, f64p, i32p]),
 }
 

@@ -63,6 +63,15 @@ struct SysDev {
     float pad3;
     uint64_t seed;              // Philox key of this system's Brownian noise
     unsigned long long pad2;
+    // standard Ewald (txewaldrec 'std'; lewald = 1 with recstd = 1)
+    int recstd;                 // 1: reciprocal space by the standard Ewald sum, not SPME
+    int ew_ncut;                // k = 2 pi n / L, 0 <= n_i <= ew_ncut
+    int ew_nkv, ew_kv_off;      // k-vectors (n, kfac) of this system and their first entry
+    long long ew_eik_off;       // first double2 of this system's exp(i k x) tables
+    long long ew_part_off;      // first 4-double2 record of the partial structure factors
+    int ew_nchunk, ew_clen;     // particle chunks of the structure-factor sum and their length
+    long long ew_fks_off;       // first double4 of the per-slice reciprocal forces
+    int ew_nks, ew_klen;        // k-vector slices of the force sum and their length
 };
 
 // One type pair's slice of the concatenated table.

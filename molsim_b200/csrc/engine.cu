@@ -23,6 +23,7 @@
 #include "common.cuh"
 #include "kernels_force.cuh"
 #include "kernels_md.cuh"
+#include "kernels_ewald.cuh"
 #include "radix_sort.cuh"
 #include "setup.h"
 
@@ -57,9 +58,9 @@ struct HostSys {
     msg_params p;
 };
 
-enum { TM_POS, TM_PAIR, TM_SPREAD, TM_FFT, TM_INFL, TM_FINAL, TM_REBUILD, TM_N };
+enum { TM_POS, TM_PAIR, TM_SPREAD, TM_FFT, TM_INFL, TM_FINAL, TM_REBUILD, TM_EWSTD, TM_N };
 const char *const kTimerNames[TM_N] = {"position_update_skin", "pair", "spread", "fft", "influence",
-                                        "gather_finalize", "rebuild"};
+                                        "gather_finalize", "rebuild", "ewald_std"};
 
 // cuFFT plans are cached process-wide by (edge, batch, type, direction) and
 // run on a work area that the owning handle allocates stream-ordered, so
@@ -202,8 +203,16 @@ struct msg_handle {
     // bonds
     int *bptr = nullptr, *bpart = nullptr, *bpw = nullptr;
     double *bk = nullptr, *beq = nullptr;
+    // Ewald sums: any_ewald = any system with one (SPME or standard), any_spme / any_std by method
+    int any_ewald = 0, any_spme = 0, any_std = 0;
+    // standard Ewald: k-vectors, tables, partial and full structure factors, force slices, work items
+    int4 *ew_kv = nullptr, *ew_kitems = nullptr, *ew_ritems = nullptr, *ew_fitems = nullptr;
+    double *ew_kfac = nullptr;
+    double2 *ew_eik = nullptr, *ew_part = nullptr, *ew_sk = nullptr;
+    double4 *ew_fks = nullptr;
+    int ew_nk = 0, ew_nr = 0, ew_nf = 0;
+    size_t ew_smem = 0;
     // SPME
-    int any_ewald = 0;
     double *rgrid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
     double2 *cgrid = nullptr;
     float *rgrid32 = nullptr;
@@ -387,7 +396,9 @@ static void free_all(msg_handle *h)
                     h->t128, h->ptask, h->psrange, h->psched, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
-                    h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys};
+                    h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
+                    h->ew_kv, h->ew_kitems, h->ew_ritems, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
+                    h->ew_sk, h->ew_fks};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -453,7 +464,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     hs.resize(n);
     hn.resize(n);
     placed.assign(n, 0);
-    order = P[0].order;
+    order = 4;
+    for (int s = n - 1; s >= 0; --s)
+        if (P[s].lewald == 1) order = P[s].order;   // the spline order of the first SPME system
     std::vector<HostSys> H(n);
     ntot = 0;
     int type_tot = 0, pt_tot = 0, ptmap_tot = 0, cell_tot = 0, t128 = 0, nch = 0;
@@ -462,9 +475,12 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     for (int s = 0; s < n; ++s) {
         const msg_params &p = P[s];
         if (p.np < 1 || p.npt < 1 || p.npt > MAXT) throw CudaError{MSG_ERR_ARG, "np >= 1 and 1 <= npt <= 4 required"};
-        if (p.lewald && (p.order < 4 || p.order > 6 || p.nmesh < 4 || (p.nmesh & 1)))
+        if (p.lewald < 0 || p.lewald > 2) throw CudaError{MSG_ERR_ARG, "lewald must be 0, 1 (SPME) or 2 (standard Ewald)"};
+        if (p.lewald == 1 && (p.order < 4 || p.order > 6 || p.nmesh < 4 || (p.nmesh & 1)))
             throw CudaError{MSG_ERR_ARG, "SPME needs 4 <= order <= 6 and an even nmesh"};
-        if (p.lewald && p.order != order) throw CudaError{MSG_ERR_ARG, "all systems of a handle share one spline order"};
+        if (p.lewald == 1 && p.order != order) throw CudaError{MSG_ERR_ARG, "all SPME systems of a handle share one spline order"};
+        if (p.lewald == 2 && (p.ncut < 1 || p.ncut > EW_MAXCUT || p.ncutregion < 0 || p.ncutregion > 1))
+            throw CudaError{MSG_ERR_ARG, "standard Ewald needs 1 <= ncut <= 100 and ncutregion 0 (sphere) or 1 (cube)"};
         if (!p.iptpn || !p.az || !p.masspt || !p.ubuf || !p.iubuflow || !p.r2umin)
             throw CudaError{MSG_ERR_ARG, "iptpn, az, masspt, ubuf, iubuflow and r2umin are required"};
         SysDev &S = hs[s];
@@ -475,6 +491,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         S.natat = p.npt * (p.npt + 1) / 2;
         S.pt_off = pt_tot;
         S.lewald = p.lewald ? 1 : 0;
+        S.recstd = p.lewald == 2 ? 1 : 0;
         S.lsurf = (p.lewald && p.lsurf) ? 1 : 0;
         for (int d = 0; d < 3; ++d) {
             S.box[d] = p.boxlen[d];
@@ -507,9 +524,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         S.cap = cap;
         S.nbl_off = nbl_acc;
         nbl_acc += (long long)cap * p.np;
-        S.s = p.lewald ? p.nmesh : 0;
+        S.s = p.lewald == 1 ? p.nmesh : 0;
         S.order = p.order;
-        for (int d = 0; d < 3; ++d) S.dkdr[d] = p.lewald ? (double)p.nmesh / p.boxlen[d] : 0.0;
+        for (int d = 0; d < 3; ++d) S.dkdr[d] = p.lewald == 1 ? (double)p.nmesh / p.boxlen[d] : 0.0;
         S.epsfp = p.epsi_four_pi;
         S.alpha = p.ualpha;
         double q2 = 0.0;
@@ -536,6 +553,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         H[s].p = p;
         if (p.bd_fac1 && p.bd_fac2) has_bd = 1;
         if (p.lewald) any_ewald = 1;
+        if (p.lewald == 1) any_spme = 1;
+        if (p.lewald == 2) any_std = 1;
     }
     ncell_tot = cell_tot;
     cell_bits = 1;
@@ -545,10 +564,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     nchunk = nch;
 
     // --- SPME grids grouped by edge, one batched cuFFT plan pair per edge ---
-    if (any_ewald) {
+    if (any_spme) {
         std::map<int, std::vector<int>> bys;
         for (int s = 0; s < n; ++s)
-            if (hs[s].lewald) bys[hs[s].s].push_back(s);
+            if (hs[s].lewald && !hs[s].recstd) bys[hs[s].s].push_back(s);
         long long go = 0, co = 0, fo_acc = 0;
         for (auto &kv : bys) {
             const int e = kv.first;
@@ -566,7 +585,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             fft.push_back(fc);
         }
         for (int s = 0; s < n; ++s)
-            if (hs[s].lewald) {
+            if (hs[s].lewald && !hs[s].recstd) {
                 const int h = hs[s].s / 2 + 1;
                 hs[s].fac_off = fo_acc;
                 fo_acc += (long long)h * h * h;
@@ -583,7 +602,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         }
         std::vector<double> hm(fo_acc), he(fo_acc), hv(fo_acc);
         for (int s = 0; s < n; ++s)
-            if (hs[s].lewald)
+            if (hs[s].lewald && !hs[s].recstd)
                 spme_factors(hs[s].s, hs[s].order, hs[s].alpha, hs[s].box, hm.data() + hs[s].fac_off,
                              he.data() + hs[s].fac_off, hv.data() + hs[s].fac_off);
         mfac = dalloc<double>(fo_acc);
@@ -596,7 +615,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         // influence work items
         std::vector<int4> it;
         for (int s = 0; s < n; ++s) {
-            if (!hs[s].lewald) continue;
+            if (!hs[s].lewald || hs[s].recstd) continue;
             const int e = hs[s].s;
             const int nc = e * e * (e / 2 + 1);
             hs[s].infl_off = (int)it.size();
@@ -606,6 +625,86 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         ninfl = (int)it.size();
         infl = dalloc<int4>(ninfl);
         up(infl, it.data(), it.size() * sizeof(int4));
+    }
+
+
+    // --- standard Ewald: k-vectors in the reference's order with kfac, work lists ---
+    if (any_std) {
+        std::vector<int4> kv, ki, ri, fi;
+        std::vector<double> kf;
+        long long eik_acc = 0, part_acc = 0, fks_acc = 0;
+        int maxw = 0;
+        for (int s = 0; s < n; ++s) {
+            SysDev &S = hs[s];
+            if (!S.recstd) continue;
+            const int nc = P[s].ncut;
+            const int ncut2 = P[s].ncutregion ? 3 * nc * nc : nc * nc;
+            const double tp = 2.0 * 3.1415926535897932, fac0 = tp / S.vol;
+            // kfac of EwaldSetup 'std' (Src/energy.F90:6762-6782), in the order the sums visit k
+            S.ew_kv_off = (int)kv.size();
+            for (int nz = 0; nz <= nc; ++nz) {
+                const double facz = nz == 0 ? 1.0 : 2.0;
+                for (int ny = 0; ny <= nc; ++ny) {
+                    const double facy = ny == 0 ? 0.5 : 1.0;
+                    for (int nx = 0; nx <= nc; ++nx) {
+                        if (nx * nx + ny * ny + nz * nz > ncut2) continue;
+                        if (nx == 0 && ny == 0 && nz == 0) continue;
+                        const double facx = nx == 0 ? 0.5 : 1.0;
+                        const double kx = nx * (tp * S.boxi[0]), ky = ny * (tp * S.boxi[1]), kz = nz * (tp * S.boxi[2]);
+                        const double k2 = kx * kx + ky * ky + kz * kz;
+                        kf.push_back(fac0 * facz * facy * facx * std::exp(-k2 / (4.0 * (S.alpha * S.alpha))) / k2);
+                        kv.push_back(make_int4(nx, ny, nz, 0));
+                    }
+                }
+            }
+            S.ew_nkv = (int)kv.size() - S.ew_kv_off;
+            S.ew_ncut = nc;
+            maxw = std::max(maxw, nc + 1);
+            S.ew_eik_off = eik_acc;
+            eik_acc += (long long)S.n * 3 * (nc + 1);
+            // chunks of the structure-factor sum (about four blocks per SM of a 148-SM B200) and
+            // slices of the force sum (about two): from the system's own sizes only, so a
+            // system's sums come out the same whatever else shares the handle
+            const int ktiles = (S.ew_nkv + EWK_THREADS - 1) / EWK_THREADS;
+            const int nch = std::max(1, std::min((4 * 148 + ktiles - 1) / ktiles, (S.n + 31) / 32));
+            S.ew_clen = (S.n + nch - 1) / nch;
+            S.ew_nchunk = (S.n + S.ew_clen - 1) / S.ew_clen;
+            S.ew_part_off = part_acc;
+            part_acc += (long long)S.ew_nchunk * S.ew_nkv;
+            for (int kt = 0; kt < ktiles; ++kt) {
+                for (int c = 0; c < S.ew_nchunk; ++c) ki.push_back(make_int4(s, kt * EWK_THREADS, c, 0));
+                ri.push_back(make_int4(s, kt * EWK_THREADS, 0, 0));
+            }
+            const int ptiles = (S.n + EWF_THREADS - 1) / EWF_THREADS;
+            const int nks = std::max(1, std::min((2 * 148 + ptiles - 1) / ptiles, std::max(1, S.ew_nkv / EWF_TILE)));
+            S.ew_klen = (S.ew_nkv + nks - 1) / nks;
+            S.ew_nks = (S.ew_nkv + S.ew_klen - 1) / S.ew_klen;
+            S.ew_fks_off = fks_acc;
+            fks_acc += (long long)S.ew_nks * S.n;
+            for (int pt = 0; pt < ptiles; ++pt)
+                for (int k = 0; k < S.ew_nks; ++k)
+                    fi.push_back(make_int4(s, S.off + pt * EWF_THREADS, S.off + std::min(S.n, (pt + 1) * EWF_THREADS), k));
+        }
+        ew_nk = (int)ki.size();
+        ew_nr = (int)ri.size();
+        ew_nf = (int)fi.size();
+        ew_kv = dalloc<int4>(kv.size());
+        ew_kfac = dalloc<double>(kf.size());
+        ew_kitems = dalloc<int4>(ki.size());
+        ew_ritems = dalloc<int4>(ri.size());
+        ew_fitems = dalloc<int4>(fi.size());
+        ew_eik = dalloc<double2>(eik_acc);
+        ew_part = dalloc<double2>(part_acc * 4);
+        ew_sk = dalloc<double2>(kv.size() * 4);
+        ew_fks = dalloc<double4>(fks_acc);
+        up(ew_kv, kv.data(), kv.size() * sizeof(int4));
+        up(ew_kfac, kf.data(), kf.size() * sizeof(double));
+        up(ew_kitems, ki.data(), ki.size() * sizeof(int4));
+        up(ew_ritems, ri.data(), ri.size() * sizeof(int4));
+        up(ew_fitems, fi.data(), fi.size() * sizeof(int4));
+        ew_smem = (size_t)EW_SUB * 3 * maxw * sizeof(double2);
+        if (!dry && ew_smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_ew_sk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ew_smem));
     }
 
     // --- pair tables: per type pair, intervals from MOLSIM's ubuf ---
@@ -1107,9 +1206,24 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
     h->tbeg(TM_FINAL);
     h->launches += 1;
     k_finalize<P, PR><<<h->nt128, FIN_THREADS, 0, h->st>>>(
-        h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->eacc, h->massip, h->massp,
+        h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->ew_fks, h->eacc, h->massip, h->massp,
         h->ftot, h->fo[0], h->vel[0], h->acc[0], mode, fo, h->errw);
     h->tend(TM_FINAL);
+}
+
+// Standard Ewald chain (tables, partial and reduced structure factors with the
+// energy and virial, force slices); the finalize kernel adds the slices.
+static void launch_ewald_std(msg_handle *h)
+{
+    h->tbeg(TM_EWSTD);
+    k_ew_eik<<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->ew_eik, h->eacc);
+    k_ew_sk<<<h->ew_nk, EWK_THREADS, h->ew_smem, h->st>>>(h->dsys, h->ew_kitems, h->ew_kv, h->ew_eik, h->ew_part);
+    k_ew_reduce<<<h->ew_nr, EWK_THREADS, 0, h->st>>>(h->dsys, h->ew_ritems, h->ew_kv, h->ew_kfac, h->ew_part, h->ew_sk,
+                                                     h->eacc);
+    k_ew_force<<<h->ew_nf, EWF_THREADS, 0, h->st>>>(h->dsys, h->ew_fitems, h->pos[0], h->ew_kv, h->ew_kfac, h->ew_sk,
+                                                    h->ew_fks);
+    h->launches += 4;
+    h->tend(TM_EWSTD);
 }
 
 template <class PR>
@@ -1169,7 +1283,8 @@ static void launch_forces(msg_handle *h, int mode, bool record, bool skin)
     }
     h->tend(TM_PAIR);
     h->launches += 1;
-    if (h->any_ewald) {
+    if (h->any_std) launch_ewald_std(h);
+    if (h->any_spme) {
         switch (h->order) {
         case 4: launch_spme<4, PR>(h); break;
         case 5: launch_spme<5, PR>(h); break;

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(const SysDev *__restr
     __shared__ R sq[SPREAD_PART];
     const Tile T = tiles[blockIdx.x / (128 / SPREAD_PART)];
     const SysDev &S = sysv[T.sys];
-    if (!S.lewald) return;
+    if (!S.lewald || S.recstd) return;
     const int p0 = T.i0 + (int)(blockIdx.x % (128 / SPREAD_PART)) * SPREAD_PART;
     const int np = max(0, min(SPREAD_PART, T.i1 - p0));
     const int s = S.s;
@@ -245,7 +245,7 @@ template <int P, class PR>
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
     const int *__restrict__ typ, const double *__restrict__ grid, const float *__restrict__ grid32,
-    const double4 *__restrict__ fsr, long long *__restrict__ eacc,
+    const double4 *__restrict__ fsr, const double4 *__restrict__ fks, long long *__restrict__ eacc,
     const double *__restrict__ massip, const double *__restrict__ massp, double4 *__restrict__ ftot,
     double4 *__restrict__ forceo, double4 *__restrict__ vel, double4 *__restrict__ acc, int mode, FinOut out,
     ErrWord *err)
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 aold = acc[i];
             }
         }
-        if (S.lewald) {
+        if (S.lewald && !S.recstd) {
             const int s = S.s;
             const double xc[3] = {x.x, x.y, x.z};
             R th[3][P], dth[3][P];
@@ -327,9 +327,19 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     if (i < T.i1 && g == 0) {
         double Fx = f0.x, Fy = f0.y, Fz = f0.z;
         if (S.lewald) {
-            Fx -= x.w * (double)e0 * S.dkdr[0] * S.epsfp;
-            Fy -= x.w * (double)e1 * S.dkdr[1] * S.epsfp;
-            Fz -= x.w * (double)e2 * S.dkdr[2] * S.epsfp;
+            if (S.recstd) {
+                // standard Ewald: the k-vector slices of k_ew_force, in slice order
+                for (int k = 0; k < S.ew_nks; ++k) {
+                    const double4 f = fks[S.ew_fks_off + (size_t)k * S.n + (i - S.off)];
+                    Fx += f.x;
+                    Fy += f.y;
+                    Fz += f.z;
+                }
+            } else {
+                Fx -= x.w * (double)e0 * S.dkdr[0] * S.epsfp;
+                Fy -= x.w * (double)e1 * S.dkdr[1] * S.epsfp;
+                Fz -= x.w * (double)e2 * S.dkdr[2] * S.epsfp;
+            }
             if (S.lsurf) {
                 const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
                 Fx -= S.epsfp * (2.0 * fac) * x.w * sq[0];

@@ -163,6 +163,24 @@ extern "C" double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_
     return xnew;
 }
 
+extern "C" int32_t msg_alpha_to_ncut(double uewaldtol, double q2sum, double epsi_four_pi, double boxlenshort,
+                                     double ualpha, int32_t *status)
+{
+    // AlphaToNcut (Src/energy.F90:7066-7081): the k-space cut of the standard Ewald
+    // sum from the Kolafa-Perram estimate of its error at uewaldtol.
+    const double y = (uewaldtol / (q2sum * epsi_four_pi)) * (msg::kPi * msg::kPi / ((ualpha * ualpha) * boxlenshort));
+    double xold = 1.0, xnew = 0.0;
+    int i;
+    for (i = 1; i <= 40; ++i) {
+        xnew = (ualpha * boxlenshort / msg::kPi) *
+               std::sqrt(-std::log(y * xold / (1.0 + 1.0 / (ualpha * boxlenshort * std::sqrt(xold)))));
+        if (std::fabs(xold - xnew) / xnew < 1.0e-6) break;
+        xold = xnew;
+    }
+    if (status) *status = (i > 40) ? MSG_ERR_ARG : MSG_OK;
+    return (int32_t)(xnew + 1.0);
+}
+
 extern "C" int msg_pot_tab(const msg_tab_params *p, double *ubuf, int32_t nbuf, int32_t *iubuflow,
                            int32_t *nugrid, double *r2umin, int32_t *nused)
 {

@@ -34,6 +34,26 @@ def rcut_to_alpha(uewaldtol, q2sum, epsi_four_pi, boxlenshort, rcut):
     return a
 
 
+def alpha_to_ncut(uewaldtol, q2sum, epsi_four_pi, boxlenshort, ualpha):
+    """AlphaToNcut (Src/energy.F90:7066-7081): the standard Ewald k-space cut."""
+    st = C.c_int32()
+    n = _lib.lib().msg_alpha_to_ncut(uewaldtol, q2sum, epsi_four_pi, boxlenshort, ualpha, C.byref(st))
+    if st.value:
+        raise MolsimGpuError(st.value, "AlphaToNcut did not converge")
+    return int(n)
+
+
+def ewald_mode(sysd):
+    """msg_params.lewald: 0 no Ewald sum, 1 SPME (txewaldrec 'spm', the default),
+    2 standard Ewald (txewaldrec 'std')."""
+    if not sysd["lewald"]:
+        return 0
+    rec = sysd.get("ewaldrec", "spm")
+    if rec not in ("spm", "std"):
+        raise ValueError("ewaldrec must be 'spm' or 'std'")
+    return 2 if rec == "std" else 1
+
+
 def pot_tab(sysd, ualpha, nbuf=100000):
     """MOLSIM's pair table (PotTwoBodyTab1/2/3, Src/potential.F90:868-1135) for the (1,6,12)
     potential of the system's types."""
@@ -65,6 +85,10 @@ def prepare(sysd):
     natat = sysd["npt"] * (sysd["npt"] + 1) // 2
     tab["r2atat"] = np.zeros(natat)
     tab["ualpha"] = alpha
+    if ewald_mode(sysd) == 2:
+        # EwaldSetup iewaldopt=3: ncut from alpha unless the system fixes it
+        tab["ncut"] = int(sysd.get("ncut") or alpha_to_ncut(sysd["uewaldtol"], q2sum, sysd["epsi_four_pi"],
+                                                            min(sysd["boxlen"]), alpha))
     return tab
 
 
@@ -146,12 +170,14 @@ class Engine:
         return MsgParams(int(s["np"]), int(s["npt"]), (C.c_double * 3)(*s["boxlen"]), s["rcut"], s["drnlist"],
                          _p(k["iptpn"], C.c_int32), _p(k["az"], C.c_double), _p(k["masspt"], C.c_double),
                          _p(k["ubuf"], C.c_double), len(k["ubuf"]), _p(k["iubuflow"], C.c_int32),
-                         _p(k["r2umin"], C.c_double), _p(k["r2atat"], C.c_double), int(s["lewald"]),
+                         _p(k["r2umin"], C.c_double), _p(k["r2atat"], C.c_double), ewald_mode(s),
                          int(s["order"]), int(s["nmesh"]), int(s["lsurf"]), t["ualpha"] if "ualpha" in t else s["ualpha"],
                          s["epsi_four_pi"], len(k["bond_p"]), _p(k["bond_ij"], C.c_int32),
                          _p(k["bond_k"], C.c_double), _p(k["bond_eq"], C.c_double), _p(k["bond_p"], C.c_int32),
                          s["tstep"], _p(k["fac1"], C.c_double) if "fac1" in k else null,
-                         _p(k["fac2"], C.c_double) if "fac2" in k else null, int(maxnneigh))
+                         _p(k["fac2"], C.c_double) if "fac2" in k else null, int(maxnneigh),
+                         int(t.get("ncut", s.get("ncut", 0)) or 0),
+                         1 if s.get("ncutregion", "sphere") == "cube" else 0)
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -36,6 +36,7 @@ module MolsimGpu
       real(c_double)     :: tstep
       type(c_ptr)        :: bd_fac1, bd_fac2
       integer(c_int32_t) :: maxnneigh
+      integer(c_int32_t) :: ncut, ncutregion
    end type msg_params
 
    ! struct msg_energy
@@ -141,6 +142,13 @@ module MolsimGpu
          real(c_double), value :: uewaldtol, q2sum, epsi_four_pi, boxlenshort, rcut
          integer(c_int32_t), intent(out) :: status
       end function msg_rcut_to_alpha
+
+      integer(c_int32_t) function msg_alpha_to_ncut(uewaldtol, q2sum, epsi_four_pi, boxlenshort, ualpha, status) &
+            bind(c, name='msg_alpha_to_ncut')
+         import :: c_double, c_int32_t
+         real(c_double), value :: uewaldtol, q2sum, epsi_four_pi, boxlenshort, ualpha
+         integer(c_int32_t), intent(out) :: status
+      end function msg_alpha_to_ncut
    end interface
 
 contains
