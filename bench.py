@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=512,
                     help="systems in the batched ensemble (0: skip)")
     ap.add_argument("--bd", type=int, default=1, help="time the 200,000-particle BD system (0: skip)")
+    ap.add_argument("--ewald-std", type=int, default=1,
+                    help="time the 1000-ion electrolyte with standard Ewald reciprocal space (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=200,
                     help="jobs in the serving stream (Poisson arrivals at 200/s; 0: skip)")
     ap.add_argument("--serve-budget-gib", type=float, default=4.0)
@@ -323,6 +325,96 @@ def run_bd(a, flush):
     return out
 
 
+def _std_nkv(ncut, cube=False):
+    """k-vectors of the standard Ewald sum (0 <= n_i <= ncut, |n|^2 within the region, n != 0)."""
+    c2 = 3 * ncut * ncut if cube else ncut * ncut
+    r = range(ncut + 1)
+    return sum(1 for x in r for y in r for z in r if 0 < x * x + y * y + z * z <= c2)
+
+
+# FP64 operations per (k-vector, particle) as k_ew_sk (44) and k_ew_force (67) issue them
+STD_FLOP_PER_KP = 111
+
+
+def run_ewald_std(a, flush):
+    """The 1000-ion electrolyte (500 + 500 ions, L = 100 A, rc = 30 A) with standard Ewald
+    reciprocal space (txewaldrec 'std', sphere, ncut from AlphaToNcut at uewaldtol = 1e-5):
+    device time per MD step with the L2 flushed before each, FP64 drop-in and mixed, beside
+    the same system on SPME (32^3 order 4) and the oracle on one host core."""
+    import torch
+
+    from molsim_b200 import Engine, prepare
+    from molsim_b200 import systems as S
+
+    s = S.electrolyte(0)
+    d = dict(s)
+    d["ewaldrec"] = "std"
+    d["ncutregion"] = "sphere"
+    t = prepare(d)
+    n, ncut = int(s["np"]), int(t["ncut"])
+    nkv = _std_nkv(ncut)
+    K = max(10, a.steps // 10)
+    out = {"workload": "electrolyte_1000 (L = 100 A, rc = 30 A)", "ncut": ncut, "k_vectors": nkv,
+           "unit": METRIC, "steps": K}
+    for prec in ("fp64", "mixed"):
+        e = Engine(d, t, precision=prec)
+        e.UTotal()
+        e.GetLinAcc()
+        ms = timed_md_steps(e, K, flush, a.warmup)
+        out["value" if prec == "fp64" else "mixed_value"] = n * K / (ms / 1000.0)
+        out["ms_per_step" if prec == "fp64" else "mixed_ms_per_step"] = ms / K
+        if prec == "fp64":
+            ext = torch.cuda.ExternalStream(e.stream())
+            e.set_timing(True)
+            for _ in range(K):
+                with torch.cuda.stream(ext):
+                    flush()
+                e.VelVer(1, energies=False)
+            kt = e.kernel_times()
+            e.set_timing(False)
+            tot, cnt = kt.get("ewald_std", (0.0, 0))
+            if cnt:
+                ms_ew = tot / cnt
+                out["ewald_std_ms_per_step"] = ms_ew
+                out["ewald_std_fp64_tflops"] = STD_FLOP_PER_KP * nkv * n / (ms_ew / 1000.0) / 1e12
+        del e
+    es = Engine(s, precision="fp64")
+    es.UTotal()
+    es.GetLinAcc()
+    out["spme_fp64_value"] = n * K / (timed_md_steps(es, K, flush, a.warmup) / 1000.0)
+    del es
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import numpy as np
+        import pyoracle as O
+        q2 = float(np.mean(s["az"] ** 2))
+        pot = dict(npt=s["npt"], zat=s["zat"], sigat=s["sigat"], epsat=s["epsat"], rcut=s["rcut"],
+                   ualpha=t["ualpha"], epsi_four_pi=s["epsi_four_pi"], lewald=1, lljcut=1,
+                   **{k: s[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab",
+                                        "fmaxtab", "rumaxfac")})
+        ot = O.pot_tab(pot)
+        ot["r2atat"] = np.zeros(3)
+        od = dict(d)
+        od["ualpha"] = t["ualpha"]
+        od["ncut"] = O.alpha_to_ncut(s["uewaldtol"], q2, s["epsi_four_pi"], min(s["boxlen"]), t["ualpha"])
+        o = O.System(od, ot, maxnneigh=n)
+        o.set_state(s["ro"], s["rod"])
+        o.set_vlist()
+        fo = o.utotal()["forceo"]
+        st = o.get_state()
+        o.set_state(st["ro"], st["rod"], fo / s["masspt"][s["iptpn"] - 1][:, None])
+        steps = 3
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            o.velver_step()
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n * steps / cpu_s, "unit": METRIC, "cores": 1, "kind": "port",
+                               "sample": "%d velocity-Verlet steps of the same system, oracle (FP64 C "
+                                         "restatement of UEwaldRecStd and the rest of the serial path), "
+                                         "1 thread" % steps}
+    return out
+
+
 def run_serving(a):
     """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
     half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
@@ -520,9 +612,11 @@ def run_gpu(a):
                "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
                          "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
 
-    ensemble = serving = bd = None
+    ensemble = serving = bd = ewstd = None
     if rank == 0 and world == 1 and a.bd:
         bd = run_bd(a, flush)
+    if rank == 0 and world == 1 and a.ewald_std:
+        ewstd = run_ewald_std(a, flush)
     if rank == 0 and world == 1 and a.ensemble > 0:
         ensemble = run_ensemble(a, flush)
     if rank == 0 and world == 1 and a.serve_jobs > 0:
@@ -542,7 +636,7 @@ def run_gpu(a):
                        "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
                        "rebuilds_in_timed_steps": int(rebuilds), "pair_kernel": tuned},
             "fp64_value": fp64_value, "batched": batched, "ensemble": ensemble, "serving": serving,
-            "bd_200k": bd,
+            "bd_200k": bd, "ewald_std_1000": ewstd,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -676,7 +676,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                 ri.push_back(make_int4(s, kt * EWK_THREADS, 0, 0));
             }
             const int ptiles = (S.n + EWF_THREADS - 1) / EWF_THREADS;
-            const int nks = std::max(1, std::min((2 * 148 + ptiles - 1) / ptiles, std::max(1, S.ew_nkv / EWF_TILE)));
+            // (a slice holds at least 32 k-vectors; one that starts inside a row of n_x first
+            // advances its exponentials, at most ncut products)
+            const int nks = std::max(1, std::min((2 * 148 + ptiles - 1) / ptiles, std::max(1, S.ew_nkv / 32)));
             S.ew_klen = (S.ew_nkv + nks - 1) / nks;
             S.ew_nks = (S.ew_nkv + S.ew_klen - 1) / S.ew_klen;
             S.ew_fks_off = fks_acc;
