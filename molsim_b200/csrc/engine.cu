@@ -206,11 +206,12 @@ struct msg_handle {
     // Ewald sums: any_ewald = any system with one (SPME or standard), any_spme / any_std by method
     int any_ewald = 0, any_spme = 0, any_std = 0;
     // standard Ewald: k-vectors, tables, partial and full structure factors, force slices, work items
-    int4 *ew_kv = nullptr, *ew_kitems = nullptr, *ew_ritems = nullptr, *ew_fitems = nullptr;
+    int4 *ew_kv = nullptr, *ew_kitems = nullptr, *ew_fitems = nullptr;
+    unsigned *ew_tiledone = nullptr;   // per k tile: chunks finished this step
     double *ew_kfac = nullptr;
     double2 *ew_eik = nullptr, *ew_part = nullptr, *ew_sk = nullptr;
     double4 *ew_fks = nullptr;
-    int ew_nk = 0, ew_nr = 0, ew_nf = 0;
+    int ew_nk = 0, ew_ntile = 0, ew_nf = 0;
     size_t ew_smem = 0;
     // SPME
     double *rgrid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
@@ -397,7 +398,7 @@ static void free_all(msg_handle *h)
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
-                    h->ew_kv, h->ew_kitems, h->ew_ritems, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
+                    h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
                     h->ew_sk, h->ew_fks};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
@@ -630,7 +631,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 
     // --- standard Ewald: k-vectors in the reference's order with kfac, work lists ---
     if (any_std) {
-        std::vector<int4> kv, ki, ri, fi;
+        std::vector<int4> kv, ki, fi;
+        int ntile = 0;
         std::vector<double> kf;
         long long eik_acc = 0, part_acc = 0, fks_acc = 0;
         int maxw = 0;
@@ -666,19 +668,17 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             // slices of the force sum (about two): from the system's own sizes only, so a
             // system's sums come out the same whatever else shares the handle
             const int ktiles = (S.ew_nkv + EWK_THREADS - 1) / EWK_THREADS;
-            const int nch = std::max(1, std::min((4 * 148 + ktiles - 1) / ktiles, (S.n + 31) / 32));
+            const int nch = std::max(1, std::min((4 * 148 + ktiles - 1) / ktiles, (S.n + 127) / 128));
             S.ew_clen = (S.n + nch - 1) / nch;
             S.ew_nchunk = (S.n + S.ew_clen - 1) / S.ew_clen;
             S.ew_part_off = part_acc;
             part_acc += (long long)S.ew_nchunk * S.ew_nkv;
-            for (int kt = 0; kt < ktiles; ++kt) {
-                for (int c = 0; c < S.ew_nchunk; ++c) ki.push_back(make_int4(s, kt * EWK_THREADS, c, 0));
-                ri.push_back(make_int4(s, kt * EWK_THREADS, 0, 0));
-            }
+            for (int kt = 0; kt < ktiles; ++kt, ++ntile)
+                for (int c = 0; c < S.ew_nchunk; ++c) ki.push_back(make_int4(s, kt * EWK_THREADS, c, ntile));
             const int ptiles = (S.n + EWF_THREADS - 1) / EWF_THREADS;
-            // (a slice holds at least 32 k-vectors; one that starts inside a row of n_x first
-            // advances its exponentials, at most ncut products)
-            const int nks = std::max(1, std::min((2 * 148 + ptiles - 1) / ptiles, std::max(1, S.ew_nkv / 32)));
+            // (a chunk holds at least 128 particles, a slice at least 16 k-vectors; a slice that
+            // starts inside a row of n_x first advances its exponentials, at most ncut products)
+            const int nks = std::max(1, std::min((2 * 148 + ptiles - 1) / ptiles, std::max(1, S.ew_nkv / 16)));
             S.ew_klen = (S.ew_nkv + nks - 1) / nks;
             S.ew_nks = (S.ew_nkv + S.ew_klen - 1) / S.ew_klen;
             S.ew_fks_off = fks_acc;
@@ -688,12 +688,13 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                     fi.push_back(make_int4(s, S.off + pt * EWF_THREADS, S.off + std::min(S.n, (pt + 1) * EWF_THREADS), k));
         }
         ew_nk = (int)ki.size();
-        ew_nr = (int)ri.size();
+        ew_ntile = ntile;
         ew_nf = (int)fi.size();
         ew_kv = dalloc<int4>(kv.size());
         ew_kfac = dalloc<double>(kf.size());
         ew_kitems = dalloc<int4>(ki.size());
-        ew_ritems = dalloc<int4>(ri.size());
+        ew_tiledone = dalloc<unsigned>(ntile);
+        if (!dry) CK(cudaMemsetAsync(ew_tiledone, 0, ntile * sizeof(unsigned), st));
         ew_fitems = dalloc<int4>(fi.size());
         ew_eik = dalloc<double2>(eik_acc);
         ew_part = dalloc<double2>(part_acc * 4);
@@ -702,7 +703,6 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         up(ew_kv, kv.data(), kv.size() * sizeof(int4));
         up(ew_kfac, kf.data(), kf.size() * sizeof(double));
         up(ew_kitems, ki.data(), ki.size() * sizeof(int4));
-        up(ew_ritems, ri.data(), ri.size() * sizeof(int4));
         up(ew_fitems, fi.data(), fi.size() * sizeof(int4));
         ew_smem = (size_t)EW_SUB * 3 * maxw * sizeof(double2);
         if (!dry && ew_smem > 48 * 1024)
@@ -1213,18 +1213,18 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
     h->tend(TM_FINAL);
 }
 
-// Standard Ewald chain (tables, partial and reduced structure factors with the
-// energy and virial, force slices); the finalize kernel adds the slices.
+// Standard Ewald chain (tables; partial structure factors reduced by each k tile's
+// last chunk, with the energy and virial; force slices); the finalize kernel adds
+// the slices.
 static void launch_ewald_std(msg_handle *h)
 {
     h->tbeg(TM_EWSTD);
     k_ew_eik<<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->ew_eik, h->eacc);
-    k_ew_sk<<<h->ew_nk, EWK_THREADS, h->ew_smem, h->st>>>(h->dsys, h->ew_kitems, h->ew_kv, h->ew_eik, h->ew_part);
-    k_ew_reduce<<<h->ew_nr, EWK_THREADS, 0, h->st>>>(h->dsys, h->ew_ritems, h->ew_kv, h->ew_kfac, h->ew_part, h->ew_sk,
-                                                     h->eacc);
+    k_ew_sk<<<h->ew_nk, EWK_THREADS, h->ew_smem, h->st>>>(h->dsys, h->ew_kitems, h->ew_kv, h->ew_kfac, h->ew_eik,
+                                                          h->ew_part, h->ew_sk, h->ew_tiledone, h->eacc);
     k_ew_force<<<h->ew_nf, EWF_THREADS, 0, h->st>>>(h->dsys, h->ew_fitems, h->pos[0], h->ew_kv, h->ew_kfac, h->ew_sk,
                                                     h->ew_fks);
-    h->launches += 4;
+    h->launches += 3;
     h->tend(TM_EWSTD);
 }
 

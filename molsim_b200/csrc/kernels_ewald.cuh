@@ -9,10 +9,10 @@
 //               recurrence e(n) = e(n-1) e(1), the x table scaled by the charge
 //               (az * eikx), and the block sums of q r for the surface term;
 //   k_ew_sk     k-vectors across threads, the particles of one chunk staged through
-//               shared memory: partial structure factors per (chunk, k);
-//   k_ew_reduce the chunks summed in a fixed order into S(k), the energy
-//               kfac |S|^2 and virial -(1 - k^2/2alpha^2) kfac |S|^2 added to the
-//               system's fixed-point accumulators;
+//               shared memory: partial structure factors per (chunk, k); the last
+//               chunk of each k tile sums the chunks in a fixed order into S(k) and
+//               adds the energy kfac |S|^2 and virial -(1 - k^2/2alpha^2) kfac |S|^2
+//               to the system's fixed-point accumulators;
 //   k_ew_force  particles across threads, k-vectors in the reference's order with
 //               the exponentials advanced by the same recurrence: each particle's
 //               reciprocal force over one slice of the k-vectors.  The slices are
@@ -83,13 +83,20 @@ __global__ void __launch_bounds__(128) k_ew_eik(const SysDev *__restrict__ sysv,
 }
 
 // Partial structure factors of one (k tile, particle chunk): item = {sys, first k,
-// chunk, -}.  Dynamic shared memory: EW_SUB particles' tables, EW_SUB*3*(ncut+1)
-// double2, for the largest ncut of the handle.
+// chunk, tile}.  Dynamic shared memory: EW_SUB particles' tables, EW_SUB*3*(ncut+1)
+// double2, for the largest ncut of the handle.  The last chunk of a tile to finish
+// sums the tile's partials in chunk order into S(k) and adds the energy
+// kfac |S|^2 and virial -(1 - k^2/2alpha^2) kfac |S|^2 to the system's fixed-point
+// accumulators; it then clears the tile's counter for the next step.
 __global__ void __launch_bounds__(EWK_THREADS) k_ew_sk(const SysDev *__restrict__ sysv, const int4 *__restrict__ items,
-                                                       const int4 *__restrict__ kv, const double2 *__restrict__ eik,
-                                                       double2 *__restrict__ part)
+                                                       const int4 *__restrict__ kv, const double *__restrict__ kfac,
+                                                       const double2 *__restrict__ eik, double2 *__restrict__ part,
+                                                       double2 *__restrict__ sk, unsigned *__restrict__ tiledone,
+                                                       long long *__restrict__ eacc)
 {
     extern __shared__ double2 stab[];
+    __shared__ double red[2][EWK_THREADS / 32];
+    __shared__ bool last;
     const int4 W = items[blockIdx.x];
     const SysDev &S = sysv[W.x];
     const int kn = W.y + threadIdx.x;
@@ -125,29 +132,25 @@ __global__ void __launch_bounds__(EWK_THREADS) k_ew_sk(const SysDev *__restrict_
 #pragma unroll
         for (int c = 0; c < 4; ++c) o[c] = a[c];
     }
-}
-
-// S(k) = sum over chunks (fixed order), energy and virial: item = {sys, first k, -, -}.
-__global__ void __launch_bounds__(EWK_THREADS) k_ew_reduce(const SysDev *__restrict__ sysv, const int4 *__restrict__ items,
-                                                           const int4 *__restrict__ kv, const double *__restrict__ kfac,
-                                                           const double2 *__restrict__ part, double2 *__restrict__ sk,
-                                                           long long *__restrict__ eacc)
-{
-    __shared__ double red[2][EWK_THREADS / 32];
-    const int4 W = items[blockIdx.x];
-    const SysDev &S = sysv[W.x];
-    const int kn = W.y + threadIdx.x;
+    // ---- the tile's last chunk: S(k), energy and virial ----
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&tiledone[W.w], 1u) == (unsigned)(S.ew_nchunk - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
     double e = 0.0, v = 0.0;
-    if (kn < S.ew_nkv) {
-        double2 a[4];
+    if (on) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) a[c] = make_double2(0.0, 0.0);
+#pragma unroll 4
         for (int ch = 0; ch < S.ew_nchunk; ++ch) {
             const double2 *p = part + (S.ew_part_off + (size_t)ch * S.ew_nkv + kn) * 4;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                a[c].x += p[c].x;
-                a[c].y += p[c].y;
+                const double2 q = __ldcg(p + c);
+                a[c].x += q.x;
+                a[c].y += q.y;
             }
         }
         double t = 0.0;
@@ -157,7 +160,6 @@ __global__ void __launch_bounds__(EWK_THREADS) k_ew_reduce(const SysDev *__restr
             t = t + (a[c].x * a[c].x + a[c].y * a[c].y);
         }
         t = kfac[S.ew_kv_off + kn] * t;
-        const int4 n = kv[S.ew_kv_off + kn];
         const double tp = 2.0 * 3.1415926535897932;
         const double kx = n.x * (tp * S.boxi[0]), ky = n.y * (tp * S.boxi[1]), kz = n.z * (tp * S.boxi[2]);
         const double k2 = kx * kx + ky * ky + kz * kz;
@@ -174,6 +176,7 @@ __global__ void __launch_bounds__(EWK_THREADS) k_ew_reduce(const SysDev *__restr
         for (int k = 0; k < EWK_THREADS / 32; ++k) s += red[threadIdx.x][k];
         acc_add(eacc + (size_t)W.x * EA_N + EA_UREC + threadIdx.x, s);
     }
+    if (threadIdx.x == 0) tiledone[W.w] = 0u;
 }
 
 // Reciprocal forces of up to EWF_THREADS particles over one slice of the
