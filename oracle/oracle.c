@@ -522,6 +522,9 @@ struct or_sys {
     double *kfac;
     double *eik[3];          /* [np][ncut+1] complex (re, im) */
     double *eyz, *eikr;      /* [np] 2 complex; [np] 4 complex */
+    double *sumeikr;         /* [nkvec][4] complex: structure factors of the last UTotal / MC update */
+    /* Random's SAVEd state (Src/mollib.F90:2683-2687) */
+    int32_t rix, riy;
     int nbond; int32_t *bond_ij; double *bond_k, *bond_eq; int32_t *bond_p;
     double tstep;
     int lcellbuild;
@@ -561,6 +564,7 @@ static void ewald_setup_std(or_sys *s, int ncut, int cube)
         }
     }
     s->nkvec = n;
+    s->sumeikr = calloc(8 * (size_t)(n > 0 ? n : 1), sizeof(double));
     for (m = 0; m < 3; ++m) s->eik[m] = malloc(sizeof(double) * 2 * (size_t)s->np * (ncut + 1));
     s->eyz = malloc(sizeof(double) * 4 * (size_t)s->np);
     s->eikr = malloc(sizeof(double) * 8 * (size_t)s->np);
@@ -647,6 +651,7 @@ void or_destroy(or_sys *s)
     free(s->nneighpn); free(s->jpnlist);
     free(s->meshfac); free(s->energyfac); free(s->virfac); free(s->qmesh); free(s->fqmesh);
     free(s->kfac); free(s->eik[0]); free(s->eik[1]); free(s->eik[2]); free(s->eyz); free(s->eikr);
+    free(s->sumeikr);
     free(s->bond_ij); free(s->bond_k); free(s->bond_eq); free(s->bond_p);
     free(s);
 }
@@ -1017,6 +1022,7 @@ static void uewald_rec_std(or_sys *s, double *urec, double *virrec)
                 }
                 term = 0.0;
                 for (c = 0; c < 4; ++c) term = term + (sum[c].r * sum[c].r + sum[c].i * sum[c].i);
+                for (c = 0; c < 4; ++c) ((cx *)s->sumeikr)[4 * (size_t)kn + c] = sum[c];
                 term = s->kfac[kn] * term;
                 uloc = uloc + term;
                 kfac2 = s->epsfp * 2.0 * s->kfac[kn];
@@ -1243,4 +1249,293 @@ double or_gau_random(int32_t *iseed, int32_t *flag, double *save)
     }
     *flag = 1;
     return *save;
+}
+
+/* ------------------------------------------------------------------ */
+/* Monte Carlo: single-particle translations                          */
+/* ------------------------------------------------------------------ */
+
+/* Random, Src/mollib.F90:2689-2708: Marsaglia xorshift (period 2^32-1) combined with
+ * Park-Miller by Schrage's method (period 2^31-2), masked to a nonzero 31-bit
+ * integer and scaled by am = nearest(1.0,-1.0)/im, a default-real (single
+ * precision) quotient: (1 - 2^-24) 2^-31 exactly. */
+static const double or_am = (1.0 - 5.9604644775390625e-08) * 4.656612873077392578125e-10;
+
+void or_random_init(int32_t iseed, int32_t state[2])
+{
+    int32_t a = iseed < 0 ? -iseed : iseed;
+    state[1] = (888889999 ^ a) | 1;          /* iy */
+    state[0] = 777755555 ^ a;                /* ix */
+}
+
+double or_random_next(int32_t state[2])
+{
+    uint32_t x = (uint32_t)state[0];
+    int32_t iy = state[1], k;
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    state[0] = (int32_t)x;
+    k = iy / 127773;
+    iy = 16807 * (iy - k * 127773) - 2836 * k;
+    if (iy < 0) iy += 2147483647;
+    state[1] = iy;
+    return or_am * (double)((2147483647 & (state[0] ^ state[1])) | 1);
+}
+
+void or_mc_seed(or_sys *s, int32_t iseed)
+{
+    int32_t st[2];
+    or_random_init(iseed, st);
+    s->rix = st[0];
+    s->riy = st[1];
+}
+
+static double mc_random(or_sys *s)
+{
+    int32_t st[2];
+    double r;
+    st[0] = s->rix;
+    st[1] = s->riy;
+    r = or_random_next(st);
+    s->rix = st[0];
+    s->riy = st[1];
+    return r;
+}
+
+/* u(r2) of one type pair by the table walk of UTwoBodyANewCellList,
+ * Src/energy.F90:779-785 pattern (0-based iptjpt). */
+static double tab_u(const or_sys *s, int iptjpt, double r2)
+{
+    int ibuf = s->iubuflow[iptjpt] - 1;
+    double d;
+    while (r2 < s->ubuf[ibuf]) ibuf += 12;
+    d = r2 - s->ubuf[ibuf];
+    return s->ubuf[ibuf + 1] + d * (s->ubuf[ibuf + 2] + d * (s->ubuf[ibuf + 3] + d * (s->ubuf[ibuf + 4] +
+           d * (s->ubuf[ibuf + 5] + d * s->ubuf[ibuf + 6]))));
+}
+
+/* npass MCPass sweeps of SPartMove (Src/mc.F90:1470-1583, 1583-1755) with one
+ * particle per trial: GetRandomTrialPos (:4527-4580), CheckPartBCTM with txbc 'xyz'
+ * (PBC, :4810-4858), DUTotal (Src/denergy.F90:110-230) = DUTwoBody with the cell-list
+ * routines' pair set (every partner inside rcut, :728-912: a hard-core or below-table
+ * partner rejects the move) + DUTwoBodyEwald (:1240-1335 'std' and :1504-1536 surface)
+ * + DUBond (:2893-2957), Metropolis (Src/mc.F90:5135-5175, weight 1) and MCUpdate
+ * (:5203-5236, EwaldUpdateArray Src/denergy.F90:1776-1792).  u = [tot, twob(0..natat),
+ * rec, bond] from the last UTotal, advanced by every accepted move.  Counts: accepted,
+ * hard-core rejects. */
+int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta, double *u,
+               int64_t *accepted, int64_t *hsreject)
+{
+    const int np = s->np, natat = s->natat;
+    int pass, ipass, k;
+    double *dtwob = malloc(sizeof(double) * (natat + 1)), *unew = malloc(sizeof(double) * (natat + 1));
+    double *uold = malloc(sizeof(double) * (natat + 1));
+    cx *tm[3] = {NULL, NULL, NULL}, *stm = NULL, *yzt = NULL;
+    const size_t w = (size_t)s->ncut + 1;
+    if (s->lewald && s->lewald != 2) { free(dtwob); free(unew); free(uold); return 6; }
+    if (s->lewald == 2) {
+        for (k = 0; k < 3; ++k) tm[k] = malloc(sizeof(cx) * w);
+        stm = malloc(sizeof(cx) * 4 * (size_t)(s->nkvec > 0 ? s->nkvec : 1));
+        yzt = malloc(sizeof(cx) * 2);
+    }
+    for (pass = 0; pass < npass; ++pass) {
+        for (ipass = 0; ipass < np; ++ipass) {
+            int ip, ipt, jp, m, overlap = 0;
+            double dtr, d[3], rtm[3], dutot = 0.0, durec = 0.0, dubond = 0.0, dured;
+            /* select a particle */
+            if (isamp == 0) {
+                ip = ipass + 1;
+            } else {
+                ip = 1 + (int)(np * mc_random(s));
+            }
+            ip = ip < 1 ? 1 : (ip > np ? np : ip);
+            ip -= 1;
+            ipt = s->iptpn[ip] - 1;
+            dtr = dtran[ipt];
+            /* GetRandomTrialPos */
+            if (dtr >= 0.0) {
+                d[0] = (mc_random(s) - 0.5) * dtr;
+                d[1] = (mc_random(s) - 0.5) * dtr;
+                d[2] = (mc_random(s) - 0.5) * dtr;
+            } else {
+                for (;;) {
+                    d[0] = mc_random(s) - 0.5;
+                    d[1] = mc_random(s) - 0.5;
+                    d[2] = mc_random(s) - 0.5;
+                    if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < 0.5 * 0.5) break;
+                }
+                for (m = 0; m < 3; ++m) d[m] = d[m] * fabs(dtr);
+            }
+            for (m = 0; m < 3; ++m) rtm[m] = s->ro[3 * ip + m] + d[m];
+            /* CheckPartBCTM, txbc 'xyz': PBC */
+            for (m = 0; m < 3; ++m) rtm[m] = pbc1(rtm[m], s->boxlen2[m], s->boxlen[m], s->boxleni[m]);
+            /* DUTwoBody: new configuration, with the overlap checks */
+            for (k = 0; k <= natat; ++k) unew[k] = uold[k] = 0.0;
+            for (jp = 0; jp < np && !overlap; ++jp) {
+                double dx, dy, dz, r2;
+                int ij;
+                if (jp == ip) continue;
+                dx = rtm[0] - s->ro[3 * jp];
+                dy = rtm[1] - s->ro[3 * jp + 1];
+                dz = rtm[2] - s->ro[3 * jp + 2];
+                r2 = pbcr2(s, &dx, &dy, &dz);
+                if (!(r2 < s->rcut2)) continue;
+                ij = pair_index(s->npt, ipt + 1, s->iptpn[jp]);        /* 1-based iptjpt */
+                if (r2 < s->r2atat[ij - 1] || r2 < s->r2umin[ij - 1]) { overlap = 1; break; }
+                unew[ij] += tab_u(s, ij - 1, r2);
+            }
+            if (overlap) {
+                if (hsreject) ++*hsreject;
+                continue;                            /* Metropolis: imchsreject, no random number */
+            }
+            for (jp = 0; jp < np; ++jp) {
+                double dx, dy, dz, r2;
+                int ij;
+                if (jp == ip) continue;
+                dx = s->ro[3 * ip] - s->ro[3 * jp];
+                dy = s->ro[3 * ip + 1] - s->ro[3 * jp + 1];
+                dz = s->ro[3 * ip + 2] - s->ro[3 * jp + 2];
+                r2 = pbcr2(s, &dx, &dy, &dz);
+                if (!(r2 < s->rcut2)) continue;
+                ij = pair_index(s->npt, ipt + 1, s->iptpn[jp]);
+                uold[ij] += tab_u(s, ij - 1, r2);
+            }
+            for (k = 1; k <= natat; ++k) { unew[0] += unew[k]; uold[0] += uold[k]; }
+            for (k = 0; k <= natat; ++k) dtwob[k] = unew[k] - uold[k];
+            dutot = dutot + dtwob[0];
+            /* DUTwoBodyEwald: 'std' reciprocal sum and the surface term */
+            if (s->lewald == 2) {
+                const int nc = s->ncut, ncut2 = s->ncut2;
+                const double q = s->az[ip];
+                const cx *ex = (const cx *)s->eik[0] + (size_t)ip * w;
+                const cx *ey = (const cx *)s->eik[1] + (size_t)ip * w;
+                const cx *ez = (const cx *)s->eik[2] + (size_t)ip * w;
+                const cx *S4 = (const cx *)s->sumeikr;
+                double tpbi[3];
+                int nx, ny, nz, kn = 0, icut;
+                for (m = 0; m < 3; ++m) tpbi[m] = 2.0 * Pi * s->boxleni[m];
+                /* EwaldSetArrayTM (Src/energy.F90:1440-1466 pattern): tables of the trial position */
+                for (m = 0; m < 3; ++m) {
+                    tm[m][0].r = 1.0; tm[m][0].i = 0.0;
+                    tm[m][1].r = cos(tpbi[m] * rtm[m]);
+                    tm[m][1].i = sin(tpbi[m] * rtm[m]);
+                    for (icut = 2; icut <= nc; ++icut) tm[m][icut] = cmul(tm[m][icut - 1], tm[m][1]);
+                }
+                for (nz = 0; nz <= nc; ++nz) {
+                    for (ny = 0; ny <= nc; ++ny) {
+                        cx yc, yct, yzm, yzp, yzmt, yzpt;
+                        if (ny * ny + nz * nz > ncut2) continue;
+                        yc.r = ey[ny].r; yc.i = -ey[ny].i;
+                        yzm = cmul(yc, ez[nz]);
+                        yzp = cmul(ey[ny], ez[nz]);
+                        yct.r = tm[1][ny].r; yct.i = -tm[1][ny].i;
+                        yzmt = cmul(yct, tm[2][nz]);
+                        yzpt = cmul(tm[1][ny], tm[2][nz]);
+                        for (nx = 0; nx <= nc; ++nx) {
+                            cx xo = ex[nx], xt = tm[0][nx], xoc, xtc, a, b, *st;
+                            double termnew, termold;
+                            if (nx * nx + ny * ny + nz * nz > ncut2) continue;
+                            if (nx == 0 && ny == 0 && nz == 0) continue;
+                            xoc.r = xo.r; xoc.i = -xo.i;
+                            xtc.r = xt.r; xtc.i = -xt.i;
+                            st = stm + 4 * (size_t)kn;
+                            for (k = 0; k < 4; ++k) st[k] = S4[4 * (size_t)kn + k];
+                            /* sumeikrtm = sumeikr + az*(new - old), per sign pattern */
+                            a = cmul(xtc, yzmt); b = cmul(xoc, yzm);
+                            st[0].r = st[0].r + q * (a.r - b.r); st[0].i = st[0].i + q * (a.i - b.i);
+                            a = cmul(xtc, yzpt); b = cmul(xoc, yzp);
+                            st[1].r = st[1].r + q * (a.r - b.r); st[1].i = st[1].i + q * (a.i - b.i);
+                            a = cmul(xt, yzmt); b = cmul(xo, yzm);
+                            st[2].r = st[2].r + q * (a.r - b.r); st[2].i = st[2].i + q * (a.i - b.i);
+                            a = cmul(xt, yzpt); b = cmul(xo, yzp);
+                            st[3].r = st[3].r + q * (a.r - b.r); st[3].i = st[3].i + q * (a.i - b.i);
+                            termnew = st[0].r * st[0].r + st[0].i * st[0].i + st[1].r * st[1].r + st[1].i * st[1].i +
+                                      st[2].r * st[2].r + st[2].i * st[2].i + st[3].r * st[3].r + st[3].i * st[3].i;
+                            {
+                                const cx *so = S4 + 4 * (size_t)kn;
+                                termold = so[0].r * so[0].r + so[0].i * so[0].i + so[1].r * so[1].r +
+                                          so[1].i * so[1].i + so[2].r * so[2].r + so[2].i * so[2].i +
+                                          so[3].r * so[3].r + so[3].i * so[3].i;
+                            }
+                            durec = durec + s->kfac[kn] * (termnew - termold);
+                            ++kn;
+                        }
+                    }
+                }
+                if (s->lsurf) {
+                    const double fac = 2.0 * Pi / (3.0 * s->vol);
+                    double sx = 0.0, sy = 0.0, sz = 0.0, tx, ty, tz;
+                    int ia;
+                    for (ia = 0; ia < np; ++ia) {
+                        sx += s->az[ia] * s->ro[3 * ia];
+                        sy += s->az[ia] * s->ro[3 * ia + 1];
+                        sz += s->az[ia] * s->ro[3 * ia + 2];
+                    }
+                    tx = sx + q * (rtm[0] - s->ro[3 * ip]);
+                    ty = sy + q * (rtm[1] - s->ro[3 * ip + 1]);
+                    tz = sz + q * (rtm[2] - s->ro[3 * ip + 2]);
+                    durec = durec + fac * ((tx * tx + ty * ty + tz * tz) - (sx * sx + sy * sy + sz * sz));
+                }
+                durec = s->epsfp * durec;
+                dutot = dutot + durec;
+            }
+            /* DUBond: every bond of the moved particle, lower neighbour first */
+            if (s->nbond > 0) {
+                int b;
+                for (b = 0; b < s->nbond; ++b) {
+                    int a1 = s->bond_ij[2 * b] - 1, a2 = s->bond_ij[2 * b + 1] - 1, other, pw, e;
+                    double dx, dy, dz, r2n, r2o, xn, xo, pn = 1.0, po = 1.0;
+                    if (a1 != ip && a2 != ip) continue;
+                    other = (a1 == ip) ? a2 : a1;
+                    dx = rtm[0] - s->ro[3 * other];
+                    dy = rtm[1] - s->ro[3 * other + 1];
+                    dz = rtm[2] - s->ro[3 * other + 2];
+                    r2n = pbcr2(s, &dx, &dy, &dz);
+                    dx = s->ro[3 * ip] - s->ro[3 * other];
+                    dy = s->ro[3 * ip + 1] - s->ro[3 * other + 1];
+                    dz = s->ro[3 * ip + 2] - s->ro[3 * other + 2];
+                    r2o = pbcr2(s, &dx, &dy, &dz);
+                    xn = sqrt(r2n) - s->bond_eq[b];
+                    xo = sqrt(r2o) - s->bond_eq[b];
+                    pw = s->bond_p[b];
+                    for (e = 0; e < pw; ++e) { pn *= xn; po *= xo; }
+                    dubond = dubond + s->bond_k[b] * (pn - po);
+                }
+                dutot = dutot + dubond;
+            }
+            /* Metropolis, weight 1, expmax = 87 (Src/mol.F90:62) */
+            dured = dutot * beta;
+            {
+                int accept;
+                if (dured > 87.0) {
+                    accept = 0;
+                } else if (dured < -87.0) {
+                    accept = 1;
+                } else {
+                    double fac = exp(-dured);
+                    accept = (fac > 1.0) ? 1 : (fac > mc_random(s));
+                }
+                if (!accept) continue;
+            }
+            /* MCUpdate */
+            if (accepted) ++*accepted;
+            u[0] = u[0] + dutot;
+            for (k = 0; k <= natat; ++k) u[1 + k] = u[1 + k] + dtwob[k];
+            if (s->lewald) u[2 + natat] = u[2 + natat] + durec;
+            if (s->nbond > 0) u[3 + natat] = u[3 + natat] + dubond;
+            if (s->lewald == 2) {
+                for (m = 0; m < 3; ++m) memcpy((cx *)s->eik[m] + (size_t)ip * w, tm[m], sizeof(cx) * w);
+                memcpy(s->sumeikr, stm, sizeof(cx) * 4 * (size_t)s->nkvec);
+            }
+            for (m = 0; m < 3; ++m) {
+                s->ro[3 * ip + m] = rtm[m];
+                s->drostep[3 * ip + m] += d[m];
+            }
+        }
+    }
+    free(dtwob); free(unew); free(uold);
+    for (k = 0; k < 3; ++k) free(tm[k]);
+    free(stm); free(yzt);
+    return 0;
 }

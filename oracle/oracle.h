@@ -141,6 +141,19 @@ double or_gau_random(int32_t *iseed, int32_t *flag, double *save);
  * drostep; updates drosum, returns 1 when a rebuild is due. */
 int  or_skin_test(or_sys *s, const double *drostep, double *max1, double *max2);
 
+/* ---- Monte Carlo: single-particle translations ---- */
+/* Random, Src/mollib.F90:2689-2708: state = {ix, iy}; or_random_init is its
+ * first-call initialisation from iseed. */
+void   or_random_init(int32_t iseed, int32_t state[2]);
+double or_random_next(int32_t state[2]);
+void   or_mc_seed(or_sys *s, int32_t iseed);
+/* npass MCPass sweeps of single-particle translations (SPartMove, DUTotal,
+ * Metropolis, MCUpdate).  dtran[npt] (>0 cube, <0 sphere), beta = 1/kT in the
+ * energy unit; u = [tot, twob(0..natat), rec, bond] from the last or_utotal, advanced
+ * by every accepted move.  Needs lewald 0 or 2 (standard Ewald); returns 6 otherwise. */
+int    or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta, double *u,
+                  int64_t *accepted, int64_t *hsreject);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,13 @@ def lib():
         L.or_cardinal_bspline.argtypes = [C.c_int, C.c_double, i32p, f64p, f64p]
         L.or_rcut_to_alpha.restype = C.c_double
         L.or_rcut_to_alpha.argtypes = [C.c_double] * 5 + [i32p]
+        L.or_random_next.restype = C.c_double
+        L.or_random_next.argtypes = [i32p]
+        L.or_random_init.argtypes = [C.c_int32, i32p]
+        L.or_mc_seed.argtypes = [C.c_void_p, C.c_int32]
+        L.or_mc_pass.restype = C.c_int
+        L.or_mc_pass.argtypes = [C.c_void_p, C.c_int, C.c_int, f64p, C.c_double, f64p,
+                                 C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.or_alpha_to_ncut.restype = C.c_int32
         L.or_alpha_to_ncut.argtypes = [C.c_double] * 5 + [i32p]
         L.or_ewald_error_ureal.restype = C.c_double
@@ -295,6 +302,26 @@ class System:
             raise RuntimeError("BDStep failed: %d" % rc)
         return bool(rb.value)
 
+    def mc_seed(self, iseed):
+        lib().or_mc_seed(self.h, int(iseed))
+
+    def mc_pass(self, npass, dtran, beta, u, isamp=0):
+        """npass MC sweeps; u (the utotal() energies) is advanced in place.
+        Returns (accepted, hard-core rejects)."""
+        d = np.ascontiguousarray(dtran, np.float64)
+        uu = np.concatenate([[u["utot"]], u["utwob"], [u["urec"], u["ubond"]]]).astype(np.float64)
+        acc = C.c_int64(0)
+        hs = C.c_int64(0)
+        rc = lib().or_mc_pass(self.h, int(npass), int(isamp), _p(d, C.c_double), float(beta),
+                              _p(uu, C.c_double), C.byref(acc), C.byref(hs))
+        if rc:
+            raise RuntimeError("MC pass failed: %d" % rc)
+        u["utot"] = uu[0]
+        u["utwob"] = uu[1:2 + self.natat].copy()
+        u["urec"] = uu[2 + self.natat]
+        u["ubond"] = uu[3 + self.natat]
+        return acc.value, hs.value
+
     def set_drosum(self, drosum):
         d = np.ascontiguousarray(drosum, np.float64)
         lib().or_set_drosum(self.h, _p(d, C.c_double))
@@ -305,6 +332,13 @@ class System:
         m2 = C.c_double()
         r = lib().or_skin_test(self.h, _p(d, C.c_double), C.byref(m1), C.byref(m2))
         return bool(r), m1.value, m2.value
+
+
+def random_stream(iseed, n):
+    """n successive Random(iseed) values from the first call (Src/mollib.F90:2689-2708)."""
+    st = (C.c_int32 * 2)()
+    lib().or_random_init(int(iseed), st)
+    return np.array([lib().or_random_next(st) for _ in range(n)])
 
 
 def gau_random_stream(iseed, n):

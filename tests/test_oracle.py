@@ -403,3 +403,81 @@ def test_std_ewald_sphere_agrees_with_converged_spme():
     assert Hp.rel_rms(rs["force"], rp["force"]) <= 1e-4
     assert Hp.rel(rs["urec"], rp["urec"]) <= 1e-5
     assert Hp.rel(rs["virial"], rp["virial"]) <= 1e-5
+
+
+# ---------------------------------------------------------------- Monte Carlo
+
+def _random_py(iseed, n):
+    """Random (Src/mollib.F90:2689-2708) restated with Python integers: 32-bit
+    xorshift and Park-Miller by Schrage's method; am is nearest(1.0,-1.0)/im in
+    single precision."""
+    am = float(np.float32(np.nextafter(np.float32(1.0), np.float32(0.0))) / np.float32(2147483647))
+    a = abs(iseed)
+    iy = (888889999 ^ a) | 1
+    ix = 777755555 ^ a
+    out = []
+    for _ in range(n):
+        ix &= 0xFFFFFFFF
+        ix ^= (ix << 13) & 0xFFFFFFFF
+        ix ^= ix >> 17
+        ix ^= (ix << 5) & 0xFFFFFFFF
+        k = iy // 127773
+        iy = 16807 * (iy - k * 127773) - 2836 * k
+        if iy < 0:
+            iy += 2147483647
+        six = ix - (1 << 32) if ix >= (1 << 31) else ix
+        out.append(am * ((2147483647 & (six ^ iy)) | 1))
+    return np.array(out)
+
+
+def test_random_stream_matches_restatement():
+    for seed in (1, 17, 123457, -5):
+        a = O.random_stream(seed, 2000)
+        b = _random_py(seed, 2000)
+        assert np.array_equal(a, b)
+        assert a.min() > 0.0 and a.max() < 1.0
+        assert abs(a.mean() - 0.5) < 0.03
+
+
+def _mc_system(s, seed=11):
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    u = o.utotal()
+    o.mc_seed(seed)
+    return o, u
+
+
+@pytest.mark.parametrize("which", ["std", "std_surf", "std_bonds", "noewald"])
+def test_mc_running_energy_equals_fresh_utotal(which):
+    """After MC sweeps the energies carried by the accepted moves' differences
+    (MCUpdate) equal a fresh UTotal of the final configuration: the restatement's
+    DUTotal is consistent with its UTotal (the check MOLSIM's TestSimulation makes)."""
+    if which == "std":
+        s = Hp.std_ewald(Hp.electrolyte_small())
+    elif which == "std_surf":
+        s = Hp.std_ewald(Hp.electrolyte_small(lsurf=True))
+    elif which == "std_bonds":
+        s = Hp.std_ewald(Hp.pe_small())
+    else:
+        s = dict(Hp.electrolyte_small())
+        s["lewald"] = False
+    o, u = _mc_system(s)
+    beta = 1.0 / S.kT(s["temp"])
+    acc, hs = o.mc_pass(3, [2.0] * s["npt"], beta, u, isamp=1)
+    n = 3 * s["np"]
+    assert 0.1 * n < acc < 0.95 * n
+    o.set_vlist()                       # the moves went past the list's skin
+    fresh = o.utotal()
+    scale = abs(fresh["utwob"][0]) + abs(fresh["urec"]) + abs(fresh["ubond"]) + 1.0
+    for k in ("utot", "urec", "ubond"):
+        assert abs(u[k] - fresh[k]) <= 1e-9 * scale, (k, u[k], fresh[k])
+    assert np.abs(np.asarray(u["utwob"]) - np.asarray(fresh["utwob"])).max() <= 1e-9 * scale
+
+
+def test_mc_rejects_spme():
+    s = dict(Hp.electrolyte_small())
+    o, u = _mc_system(s)
+    with pytest.raises(RuntimeError):
+        o.mc_pass(1, [1.0] * s["npt"], 1.0, u)
