@@ -22,6 +22,8 @@
  *   msg_velver                     -> MDDriver iSimulationStep: VelVer +
  *                                     GetKinEnergy (Src/md.F90:154-168, 252-410)
  *                                     followed by NList (Src/nlist.F90:597-621)
+ *   msg_mc_seed / msg_mc_pass      -> MCDriver iSimulationStep: MCPass with SPartMove
+ *                                     (Src/mc.F90:1470-1755), DUTotal, Metropolis, MCUpdate
  *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
  *                                     (Src/bd.F90:53-59, 120-155) followed by NList
  * Set-up helpers that restate MOLSIM's own set-up for callers without it:
@@ -155,6 +157,30 @@ int  msg_tune(msg_handle *h, int32_t key, int32_t value);
 
 /* rodd = massip * forceo (GetLinAcc) from the last msg_utotal. */
 int  msg_get_linacc(msg_handle *h);
+
+/* Monte Carlo with single-particle translations (MCPass with SPartMove,
+ * Src/mc.F90:1470-1755; DUTotal, Src/denergy.F90:110-230; Metropolis and MCUpdate,
+ * Src/mc.F90:5135-5236).  Parameters of one system's sweeps: */
+typedef struct msg_mc_params {
+    double beta;             /* 1/kT in mol/kJ (MOLSIM's beta)                          */
+    const double *dtran;     /* [npt] displacement per type: > 0 cube side, < 0 sphere   */
+    int32_t isamp;           /* 0: particles in order; 1: a random particle per trial    */
+    int32_t pad;
+} msg_mc_params;
+
+/* Random's state of system isys from iseed (its first call, Src/mollib.F90:2689-2708).
+ * A system never seeded starts from iseed = isys + 1. */
+int  msg_mc_seed(msg_handle *h, int32_t isys, int32_t iseed);
+
+/* npass sweeps of np trial moves for every system (p[nsys]), one Metropolis chain per
+ * system, each drawing the reference's random numbers in the reference's order.
+ * accepted / hsreject [nsys] (optional): moves accepted and moves rejected for a
+ * hard-core or below-table overlap in this call.  e (optional): energies of system
+ * isys after the sweeps, from a UTotal at the start plus the accepted moves'
+ * differences (MCUpdate).  The lists are rebuilt afterwards.  Systems must use the
+ * standard Ewald sum (lewald 2) or none: MSG_ERR_ARG for SPME. */
+int  msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p, int64_t *accepted,
+                 int64_t *hsreject, int32_t isys, msg_energy *e);
 
 /* nsteps velocity-Verlet steps of every system, entirely on the device.
  * e (optional): [nsteps] energies of system isys after each step. */

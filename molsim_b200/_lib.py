@@ -42,6 +42,10 @@ class MsgEnergy(C.Structure):
                     ubond=self.ubond, virial=self.virial, ekin=self.ekin)
 
 
+class MsgMcParams(C.Structure):
+    _fields_ = [("beta", C.c_double), ("dtran", f64p), ("isamp", C.c_int32), ("pad", C.c_int32)]
+
+
 class MsgTabParams(C.Structure):
     _fields_ = [("npt", C.c_int32), ("zat", f64p), ("sigat", f64p), ("epsat", f64p), ("rcut", C.c_double),
                 ("ualpha", C.c_double), ("epsi_four_pi", C.c_double), ("lewald", C.c_int32),
@@ -62,6 +66,9 @@ SIGNATURES = {
     "msg_build_nlist": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(C.c_int64)]),
     "msg_utotal": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),
     "msg_get_linacc": (C.c_int, [C.c_void_p]),
+    "msg_mc_seed": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "msg_mc_pass": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(MsgMcParams), C.POINTER(C.c_int64),
+                              C.POINTER(C.c_int64), C.c_int32, C.POINTER(MsgEnergy)]),
     "msg_get_forces": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p]),
     "msg_tune": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "msg_velver": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(MsgEnergy)]),

@@ -24,6 +24,7 @@
 #include "kernels_force.cuh"
 #include "kernels_md.cuh"
 #include "kernels_ewald.cuh"
+#include "kernels_mc.cuh"
 #include "radix_sort.cuh"
 #include "setup.h"
 
@@ -212,6 +213,15 @@ struct msg_handle {
     double2 *ew_eik = nullptr, *ew_part = nullptr, *ew_sk = nullptr;
     double4 *ew_fks = nullptr;
     int ew_nk = 0, ew_ntile = 0, ew_nf = 0;
+    // Monte Carlo: Random's state, running energies, counts (accepted, hard-core rejects),
+    // sweep parameters, displacement per type, trial structure factors
+    int2 *mc_rng = nullptr;
+    double *mc_u = nullptr, *mc_dtr = nullptr;
+    long long *mc_cnt = nullptr;
+    McPar *mc_par = nullptr;
+    double2 *ew_sktm = nullptr;
+    int type_tot = 0, ew_nkv_tot = 0, ew_maxw = 0;
+    void ensure_mc();
     size_t ew_smem = 0;
     // SPME
     double *rgrid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
@@ -399,7 +409,7 @@ static void free_all(msg_handle *h)
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
                     h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
-                    h->ew_sk, h->ew_fks};
+                    h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -558,6 +568,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         if (p.lewald == 2) any_std = 1;
     }
     ncell_tot = cell_tot;
+    this->type_tot = type_tot;
     cell_bits = 1;
     while ((1u << cell_bits) <= (unsigned)cell_tot) ++cell_bits;
     nbl_tot = nbl_acc;
@@ -705,6 +716,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         up(ew_kitems, ki.data(), ki.size() * sizeof(int4));
         up(ew_fitems, fi.data(), fi.size() * sizeof(int4));
         ew_smem = (size_t)EW_SUB * 3 * maxw * sizeof(double2);
+        ew_nkv_tot = (int)kv.size();
+        ew_maxw = maxw;
         if (!dry && ew_smem > 48 * 1024)
             CK(cudaFuncSetAttribute(k_ew_sk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ew_smem));
     }
@@ -1930,6 +1943,98 @@ extern "C" int msg_get_linacc(msg_handle *h)
     const int c = h->cur;
     k_linacc<<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->fo[c], h->typ[c], h->massip, h->acc[c]);
     return h->check();
+    API_END
+}
+
+// Random's first-call state from iseed (Src/mollib.F90:2696-2701).
+static int2 mc_seed_state(int32_t iseed)
+{
+    const int32_t a = iseed < 0 ? -iseed : iseed;
+    return make_int2(777755555 ^ a, (888889999 ^ a) | 1);
+}
+
+// Monte Carlo buffers, made on first use; an unseeded system starts from iseed = isys + 1.
+void msg_handle::ensure_mc()
+{
+    if (mc_rng) return;
+    mc_rng = dalloc<int2>(nsys);
+    mc_u = dalloc<double>((size_t)nsys * ESZ);
+    mc_cnt = dalloc<long long>(2 * (size_t)nsys);
+    mc_par = dalloc<McPar>(nsys);
+    mc_dtr = dalloc<double>(std::max(1, type_tot));
+    if (any_std) ew_sktm = dalloc<double2>(4 * (size_t)ew_nkv_tot);
+    std::vector<int2> st(nsys);
+    for (int s = 0; s < nsys; ++s) st[s] = mc_seed_state(s + 1);
+    up(mc_rng, st.data(), nsys * sizeof(int2));
+}
+
+extern "C" int msg_mc_seed(msg_handle *h, int32_t isys, int32_t iseed)
+{
+    if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
+    API_BEGIN
+    h->ensure_mc();
+    const int2 st = mc_seed_state(iseed);
+    CK(cudaMemcpyAsync(h->mc_rng + isys, &st, sizeof(int2), cudaMemcpyHostToDevice, h->st));
+    return h->check();
+    API_END
+}
+
+extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p, int64_t *accepted,
+                           int64_t *hsreject, int32_t isys, msg_energy *e)
+{
+    if (!h || !p || npass < 0 || (e && (isys < 0 || isys >= h->nsys))) return MSG_ERR_ARG;
+    API_BEGIN
+    std::vector<McPar> par(h->nsys);
+    std::vector<double> dtr(std::max(1, h->type_tot), 0.0);
+    for (int s = 0; s < h->nsys; ++s) {
+        const SysDev &S = h->hs[s];
+        if (S.lewald && !S.recstd) {
+            h->err = "Monte Carlo moves need the standard Ewald sum (lewald 2) or none: the SPME energy "
+                     "difference of a trial move transforms the whole mesh";
+            return MSG_ERR_ARG;
+        }
+        if (!p[s].dtran || (p[s].isamp != 0 && p[s].isamp != 1)) {
+            h->err = "msg_mc_params needs dtran[npt] and isamp 0 or 1";
+            return MSG_ERR_ARG;
+        }
+        par[s].beta = p[s].beta;
+        par[s].isamp = p[s].isamp;
+        par[s].pad = 0;
+        for (int t = 0; t < S.npt; ++t) dtr[S.type_off + t] = p[s].dtran[t];
+    }
+    h->ensure_mc();
+    h->up(h->mc_par, par.data(), h->nsys * sizeof(McPar));
+    h->up(h->mc_dtr, dtr.data(), dtr.size() * sizeof(double));
+    CK(cudaMemsetAsync(h->mc_cnt, 0, 2 * sizeof(long long) * h->nsys, h->st));
+    // energies and structure factors of the current configuration (UTotal), carried
+    // from here by the accepted moves' differences (MCUpdate)
+    h->enqueue_forces(0, false);
+    CK(cudaMemcpyAsync(h->mc_u, h->esys, sizeof(double) * ESZ * h->nsys, cudaMemcpyDeviceToDevice, h->st));
+    if (npass > 0) {
+        const size_t smem = h->any_std ? 6 * (size_t)h->ew_maxw * sizeof(double2) : 0;
+        k_mc_pass<<<h->nsys, MC_THREADS, smem, h->st>>>(
+            h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tz, h->tc, h->ew_kv, h->ew_kfac, h->ew_sk,
+            h->ew_sktm, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bk, h->beq, h->bpw, h->mc_par, h->mc_dtr,
+            h->mc_rng, h->mc_u, h->mc_cnt, npass);
+        h->launches += 1;
+    }
+    std::vector<long long> cnt(2 * (size_t)h->nsys);
+    CK(cudaMemcpyAsync(cnt.data(), h->mc_cnt, cnt.size() * sizeof(long long), cudaMemcpyDeviceToHost, h->st));
+    double he[ESZ];
+    if (e) CK(cudaMemcpyAsync(he, h->mc_u + (size_t)isys * ESZ, sizeof(he), cudaMemcpyDeviceToHost, h->st));
+    int rc = h->check();
+    if (rc) return rc;
+    for (int s = 0; s < h->nsys; ++s) {
+        if (accepted) accepted[s] = cnt[2 * (size_t)s];
+        if (hsreject) hsreject[s] = cnt[2 * (size_t)s + 1];
+    }
+    if (e) fill_energy(he, h->hs[isys].natat, e);
+    // the particles moved: every list is rebuilt (NList after the sweeps)
+    if (npass > 0) {
+        std::vector<int> all(h->placed.begin(), h->placed.end());
+        return h->rebuild_checked(all);
+    }
+    return MSG_OK;
     API_END
 }
 

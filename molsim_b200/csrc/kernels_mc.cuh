@@ -1,0 +1,314 @@
+// kernels_mc.cuh -- Monte Carlo single-particle translations (MCPass with
+// SPartMove, Src/mc.F90:1470-1755): trial position (GetRandomTrialPos, :4527-4580;
+// CheckPartBCTM with PBC, :4810-4858), energy difference (DUTotal,
+// Src/denergy.F90:110-230: DUTwoBody over every partner inside rcut as the
+// cell-list routines see them, :728-912; DUTwoBodyEwald 'std' and surface,
+// :1240-1335, 1504-1536; DUBond, :2893-2957), Metropolis (Src/mc.F90:5135-5175)
+// and MCUpdate (:5203-5236).
+//
+// A Metropolis chain is sequential, so one block runs one system's chain and
+// spreads each trial's work over its threads: the pair differences over the
+// system's particles, the structure-factor update over its k-vectors.  Thread 0
+// draws the reference's random numbers (Random, Src/mollib.F90:2689-2708) in the
+// reference's order and decides.  Every reduction has a fixed order: a system's
+// chain is the same alone or beside others.  FP64 throughout.
+#pragma once
+
+#include "common.cuh"
+#include "kernels_ewald.cuh"
+
+namespace msg {
+
+constexpr int MC_THREADS = 256;
+
+// Per-system parameters of a sweep.
+struct McPar {
+    double beta;        // 1/kT in mol/kJ
+    int isamp;          // 0: particles in order, 1: a random particle per trial
+    int pad;
+};
+
+// Random (Src/mollib.F90:2689-2708): xorshift (13, 17, 5) combined with Park-Miller
+// by Schrage's method, masked to a nonzero 31-bit integer, times
+// am = (1 - 2^-24) 2^-31 (nearest(1.0,-1.0)/im in single precision).
+__device__ __forceinline__ double mc_random(int2 &st)
+{
+    unsigned x = (unsigned)st.x;
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    st.x = (int)x;
+    int iy = st.y;
+    const int k = iy / 127773;
+    iy = 16807 * (iy - k * 127773) - 2836 * k;
+    if (iy < 0) iy += 2147483647;
+    st.y = iy;
+    const double am = (1.0 - 5.9604644775390625e-08) * 4.656612873077392578125e-10;
+    return __dmul_rn(am, (double)((2147483647 & (st.x ^ st.y)) | 1));
+}
+
+// u(r2) of one type pair: the reference's table walk from the pair's first
+// interval (the lookup of UTwoBodyANewCellList, Src/denergy.F90:779-785).
+__device__ __forceinline__ double mc_tab_u(const PairTab &T, const double *__restrict__ tz,
+                                           const double *__restrict__ tc, double r2)
+{
+    int k = T.k0;
+    while (r2 < tz[k]) ++k;
+    const double *c = tc + (size_t)12 * k;
+    const double d = r2 - c[0];
+    return c[1] + d * (c[2] + d * (c[3] + d * (c[4] + d * (c[5] + d * c[6]))));
+}
+
+// Block sum of v into slot `slot` of red (thread 0 reads the result after the
+// next barrier).
+__device__ __forceinline__ void mc_block_add(double v, double (*red)[MC_THREADS / 32], int slot)
+{
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[slot][threadIdx.x >> 5] = v;
+}
+
+// npass sweeps of one system per block.  Dynamic shared memory: six rows of
+// ncut+1 double2 (new and old exp(i k x) of the moved particle) for standard
+// Ewald systems.
+__global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
+    const SysDev *__restrict__ sysv, double4 *__restrict__ pos, const int *__restrict__ typ,
+    const int *__restrict__ inv, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
+    const double *__restrict__ tz, const double *__restrict__ tc, const int4 *__restrict__ kv,
+    const double *__restrict__ kfac, double2 *__restrict__ sk, double2 *__restrict__ sktm,
+    const int *__restrict__ bptr, const int *__restrict__ bpart, const double *__restrict__ bk,
+    const double *__restrict__ beq, const int *__restrict__ bpw, const McPar *__restrict__ par,
+    const double *__restrict__ dtr, int2 *__restrict__ rng, double *__restrict__ mcu,
+    long long *__restrict__ cnt, int npass)
+{
+    extern __shared__ double2 etab[];          // [6][ncut+1]: new x, y, z; old x, y, z
+    constexpr int NSLOT = 10 + 4;              // type pairs, reciprocal, dipole x, y, z
+    __shared__ double red[NSLOT][MC_THREADS / 32];
+    __shared__ double srt[3], sro[3], sq;
+    __shared__ int si, sip, sty, sover, sacc;
+    const int sys = blockIdx.x;
+    const SysDev &S = sysv[sys];
+    if (S.lewald && !S.recstd) return;         // SPME systems are refused on the host
+    const int t = threadIdx.x;
+    const int natat = S.natat, w = S.ew_ncut + 1;
+    const McPar P = par[sys];
+    int2 st = rng[sys];                        // used by thread 0 only
+    double *u = mcu + (size_t)sys * ESZ;
+    long long nacc = 0, nhs = 0;
+    const double tp = 2.0 * 3.1415926535897932;
+    for (int pass = 0; pass < npass; ++pass) {
+        for (int ipass = 0; ipass < S.n; ++ipass) {
+            // ---- trial move: particle, displacement, periodic wrap (thread 0) ----
+            if (t == 0) {
+                int ip = (P.isamp == 0) ? ipass + 1 : 1 + (int)(S.n * mc_random(st));
+                ip = max(1, min(ip, S.n)) - 1;
+                const int i = inv[S.off + ip];
+                const int ty = typ[i];
+                const double dt = dtr[S.type_off + ty];
+                double d[3];
+                if (dt >= 0.0) {
+                    for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(mc_random(st) - 0.5, dt);
+                } else {
+                    for (;;) {
+                        for (int m = 0; m < 3; ++m) d[m] = mc_random(st) - 0.5;
+                        if (__dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2])) <
+                            0.25)
+                            break;
+                    }
+                    for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(d[m], fabs(dt));
+                }
+                const double4 x = pos[i];
+                const double xo[3] = {x.x, x.y, x.z};
+                for (int m = 0; m < 3; ++m) {
+                    sro[m] = xo[m];
+                    srt[m] = pbc_wrap(__dadd_rn(xo[m], d[m]), S.half[m], S.box[m], S.boxi[m]);
+                }
+                sq = x.w;
+                si = i;
+                sip = ip;
+                sty = ty;
+                sover = 0;
+            }
+            __syncthreads();
+            const int i = si, ty = sty;
+            const double q = sq;
+            const double rt[3] = {srt[0], srt[1], srt[2]}, r0[3] = {sro[0], sro[1], sro[2]};
+            // ---- exp(i 2pi n x / L) of the trial and the current position (standard Ewald) ----
+            if (S.recstd && t < 6) {
+                const int m = t % 3;
+                const double xm = (t < 3) ? rt[m] : r0[m];
+                double sn, cs;
+                sincos(tp * S.boxi[m] * xm, &sn, &cs);
+                const double2 e1 = make_double2(cs, sn);
+                double2 *row = etab + t * w;
+                double2 e = make_double2(1.0, 0.0);
+                row[0] = e;
+                for (int n = 1; n < w; ++n) {
+                    e = (n == 1) ? e1 : cmul(e, e1);
+                    row[n] = e;
+                }
+            }
+            // ---- pair differences (and the dipole sum of the surface term) ----
+            double du[10];
+#pragma unroll
+            for (int p = 0; p < 10; ++p) du[p] = 0.0;
+            double dip0 = 0.0, dip1 = 0.0, dip2 = 0.0;
+            bool over = false;
+            for (int j = S.off + t; j < S.off + S.n; j += MC_THREADS) {
+                const double4 xj = pos[j];
+                if (S.lsurf) {
+                    dip0 += xj.w * xj.x;
+                    dip1 += xj.w * xj.y;
+                    dip2 += xj.w * xj.z;
+                }
+                if (j == i) continue;
+                const int pg = pair_of(ptmap, S, ty, typ[j]);
+                const PairTab &T = ptab[pg];
+                const int pl = pg - S.pt_off;
+                double dx = rt[0] - xj.x, dy = rt[1] - xj.y, dz = rt[2] - xj.z;
+                const double r2n = pbcr2_exact(dx, dy, dz, S);
+                double v = 0.0;
+                if (r2n < S.rcut2) {
+                    if (r2n < T.r2atat || r2n < T.r2umin)
+                        over = true;
+                    else
+                        v += mc_tab_u(T, tz, tc, r2n);
+                }
+                dx = r0[0] - xj.x;
+                dy = r0[1] - xj.y;
+                dz = r0[2] - xj.z;
+                const double r2o = pbcr2_exact(dx, dy, dz, S);
+                if (r2o < S.rcut2) v -= mc_tab_u(T, tz, tc, r2o);
+#pragma unroll
+                for (int p = 0; p < 10; ++p)
+                    if (p == pl) du[p] += v;
+            }
+            if (over) sover = 1;
+            __syncthreads();                   // tables ready
+            // ---- structure factors of the trial (standard Ewald) ----
+            double dr = 0.0;
+            if (S.recstd) {
+                const double2 *tx = etab, *ty_ = etab + w, *tzn = etab + 2 * w;
+                const double2 *ox = etab + 3 * w, *oy = etab + 4 * w, *oz = etab + 5 * w;
+                for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {
+                    const size_t g = (size_t)S.ew_kv_off + kn;
+                    const int4 n = kv[g];
+                    const double2 yzm = cmul(cconj(oy[n.y]), oz[n.z]), yzp = cmul(oy[n.y], oz[n.z]);
+                    const double2 yzmt = cmul(cconj(ty_[n.y]), tzn[n.z]), yzpt = cmul(ty_[n.y], tzn[n.z]);
+                    const double2 xo = ox[n.x], xt = tx[n.x];
+                    const double2 nw[4] = {cmul(cconj(xt), yzmt), cmul(cconj(xt), yzpt), cmul(xt, yzmt), cmul(xt, yzpt)};
+                    const double2 od[4] = {cmul(cconj(xo), yzm), cmul(cconj(xo), yzp), cmul(xo, yzm), cmul(xo, yzp)};
+                    double tnew = 0.0, told = 0.0;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const double2 s0 = sk[g * 4 + c];
+                        const double2 s1 = make_double2(s0.x + q * (nw[c].x - od[c].x), s0.y + q * (nw[c].y - od[c].y));
+                        sktm[g * 4 + c] = s1;
+                        tnew = tnew + (s1.x * s1.x + s1.y * s1.y);
+                        told = told + (s0.x * s0.x + s0.y * s0.y);
+                    }
+                    dr = dr + kfac[g] * (tnew - told);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < 10; ++p)
+                if (p < natat) mc_block_add(du[p], red, p);
+            mc_block_add(dr, red, 10);
+            if (S.lsurf) {
+                mc_block_add(dip0, red, 11);
+                mc_block_add(dip1, red, 12);
+                mc_block_add(dip2, red, 13);
+            }
+            __syncthreads();
+            // ---- DUTotal's sum, bonds, surface, Metropolis (thread 0) ----
+            if (t == 0) {
+                int acc = 0;
+                double dtw[10], dutot = 0.0, durec = 0.0, dubond = 0.0;
+                if (sover) {
+                    ++nhs;                     // Metropolis: hard-core reject, no random number
+                } else {
+                    double d0 = 0.0;
+                    for (int p = 0; p < natat; ++p) {
+                        double a = 0.0;
+                        for (int k = 0; k < MC_THREADS / 32; ++k) a += red[p][k];
+                        dtw[p] = a;
+                        d0 += a;
+                    }
+                    dutot = d0;
+                    if (S.lewald) {
+                        for (int k = 0; k < MC_THREADS / 32; ++k) durec += red[10][k];
+                        if (S.lsurf) {
+                            double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+                            for (int k = 0; k < MC_THREADS / 32; ++k) {
+                                m0 += red[11][k];
+                                m1 += red[12][k];
+                                m2 += red[13][k];
+                            }
+                            const double fac = tp / (3.0 * S.vol);
+                            const double a0 = m0 + q * (rt[0] - r0[0]), a1 = m1 + q * (rt[1] - r0[1]),
+                                         a2 = m2 + q * (rt[2] - r0[2]);
+                            durec += fac * ((a0 * a0 + a1 * a1 + a2 * a2) - (m0 * m0 + m1 * m1 + m2 * m2));
+                        }
+                        durec = S.epsfp * durec;
+                        dutot += durec;
+                    }
+                    const int ip = sip;
+                    for (int b = bptr ? bptr[S.off + ip] : 0; bptr && b < bptr[S.off + ip + 1]; ++b) {
+                        const double4 xb = pos[inv[S.off + bpart[b]]];
+                        double dx = rt[0] - xb.x, dy = rt[1] - xb.y, dz = rt[2] - xb.z;
+                        const double r2n = pbcr2_exact(dx, dy, dz, S);
+                        dx = r0[0] - xb.x;
+                        dy = r0[1] - xb.y;
+                        dz = r0[2] - xb.z;
+                        const double r2o = pbcr2_exact(dx, dy, dz, S);
+                        const double xn = sqrt(r2n) - beq[b], xo = sqrt(r2o) - beq[b];
+                        double pn = 1.0, po = 1.0;
+                        for (int e = 0; e < bpw[b]; ++e) {
+                            pn *= xn;
+                            po *= xo;
+                        }
+                        dubond += bk[b] * (pn - po);
+                    }
+                    dutot += dubond;
+                    const double dured = dutot * P.beta;
+                    if (dured > 87.0)
+                        acc = 0;
+                    else if (dured < -87.0)
+                        acc = 1;
+                    else {
+                        const double fac = exp(-dured);
+                        acc = (fac > 1.0) ? 1 : (fac > mc_random(st) ? 1 : 0);
+                    }
+                    if (acc) {
+                        ++nacc;
+                        u[0] += dutot;
+                        u[1] += d0;
+                        for (int p = 0; p < natat; ++p) u[2 + p] += dtw[p];
+                        if (S.lewald) u[12] += durec;
+                        u[13] += dubond;
+                        double4 x = pos[i];
+                        x.x = rt[0];
+                        x.y = rt[1];
+                        x.z = rt[2];
+                        pos[i] = x;
+                    }
+                }
+                sacc = acc;
+            }
+            __syncthreads();
+            if (sacc && S.recstd)
+                for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {
+                    const size_t g = (size_t)S.ew_kv_off + kn;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) sk[g * 4 + c] = sktm[g * 4 + c];
+                }
+            __syncthreads();
+        }
+    }
+    if (t == 0) {
+        rng[sys] = st;
+        cnt[2 * (size_t)sys] += nacc;
+        cnt[2 * (size_t)sys + 1] += nhs;
+    }
+}
+
+}  // namespace msg

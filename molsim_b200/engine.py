@@ -254,6 +254,34 @@ class Engine:
         self._check(_lib.lib().msg_velver(self.h, nsteps, isys, e))
         return [e[k].as_dict(self.natat[isys]) for k in range(nsteps)]
 
+    def mc_seed(self, iseed, isys=0):
+        """Random's state of system isys from iseed (MOLSIM's iseed)."""
+        self._check(_lib.lib().msg_mc_seed(self.h, isys, int(iseed)))
+
+    def MCPass(self, npass=1, dtran=None, beta=None, isamp=0, isys=0):
+        """npass MCPass sweeps of single-particle translations (Src/mc.F90:1470-1755) for every
+        system.  dtran: per-type displacements ([npt], or one list per system); beta: 1/kT in
+        mol/kJ (one value or one per system; default from each system's temperature).
+        Returns (accepted[nsys], hard-core rejects[nsys], energies of system isys)."""
+        from ._lib import MsgMcParams
+        from .systems import kT
+
+        par = (MsgMcParams * self.nsys)()
+        keep = []
+        for k, s in enumerate(self.systems):
+            d = dtran[k] if dtran is not None and np.ndim(dtran) == 2 else dtran
+            d = np.ascontiguousarray(d if d is not None else [1.0] * s["npt"], np.float64)
+            keep.append(d)
+            b = beta[k] if isinstance(beta, (list, tuple, np.ndarray)) else beta
+            b = float(b) if b is not None else 1.0 / kT(s["temp"])
+            par[k] = MsgMcParams(b, _p(d, C.c_double), int(isamp), 0)
+        acc = np.zeros(self.nsys, np.int64)
+        hs = np.zeros(self.nsys, np.int64)
+        e = MsgEnergy()
+        self._check(_lib.lib().msg_mc_pass(self.h, int(npass), par, _p(acc, C.c_int64), _p(hs, C.c_int64), isys,
+                                           C.byref(e)))
+        return acc, hs, e.as_dict(self.natat[isys])
+
     def BDStep(self, nsteps=1, seed=0, isys=0, xi=None, return_noise=False, energies=True):
         """nsteps of BDDriver(iSimulationStep) + NList.  xi: caller noise [nsteps][np][3]."""
         n = int(self.systems[isys]["np"])
