@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=512,
                     help="systems in the batched ensemble (0: skip)")
     ap.add_argument("--bd", type=int, default=1, help="time the 200,000-particle BD system (0: skip)")
+    ap.add_argument("--mc", type=int, default=1,
+                    help="time Monte Carlo sweeps of the 1000-ion electrolyte, one chain and an ensemble (0: skip)")
     ap.add_argument("--ewald-std", type=int, default=1,
                     help="time the 1000-ion electrolyte with standard Ewald reciprocal space (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=200,
@@ -415,6 +417,80 @@ def run_ewald_std(a, flush):
     return out
 
 
+def run_mc(a):
+    """Monte Carlo single-particle translations (MCPass/SPartMove/DUTotal/Metropolis) of the
+    1000-ion electrolyte with standard Ewald (ncut from AlphaToNcut at 1e-5, sphere), displacement
+    2 A, at 298 K: trial moves per second for one chain and for an ensemble of 592 chains (four per
+    SM, one seed each), device time around each call (a UTotal, the sweeps and the list rebuild),
+    beside the oracle's chain on one host core."""
+    import torch
+
+    from molsim_b200 import Engine, prepare
+    from molsim_b200 import systems as S
+
+    s = S.electrolyte(0)
+    d = dict(s)
+    d["ewaldrec"] = "std"
+    t = prepare(d)
+    n = int(s["np"])
+    beta = 1.0 / S.kT(s["temp"])
+    dtran = [2.0] * s["npt"]
+    out = {"workload": "electrolyte_1000, standard Ewald (ncut %d), dtran 2 A, 298 K" % t["ncut"],
+           "unit": "trial moves/s"}
+
+    def timed(e, npass):
+        ext = torch.cuda.ExternalStream(e.stream())
+        e.MCPass(1, dtran, beta)                       # warm-up
+        torch.cuda.synchronize()
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st.record(ext)
+        acc, _, _ = e.MCPass(npass, dtran, beta)
+        en.record(ext)
+        torch.cuda.synchronize()
+        return st.elapsed_time(en) / 1000.0, acc
+
+    e1 = Engine(d, t, precision="fp64")
+    e1.mc_seed(1)
+    sweeps = 5
+    sec, acc = timed(e1, sweeps)
+    out["single"] = {"value": n * sweeps / sec, "sweeps": sweeps, "acceptance": float(acc[0]) / (n * sweeps)}
+    del e1
+    nrep = 4 * 148
+    er = Engine([dict(d) for _ in range(nrep)], [t] * nrep, precision="fp64")
+    for k in range(nrep):
+        er.mc_seed(1 + k, isys=k)
+    sec, acc = timed(er, sweeps)
+    out["ensemble"] = {"value": nrep * n * sweeps / sec, "chains": nrep, "sweeps": sweeps,
+                       "acceptance": float(acc.sum()) / (nrep * n * sweeps)}
+    del er
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import numpy as np
+        import pyoracle as O
+        q2 = float(np.mean(s["az"] ** 2))
+        pot = dict(npt=s["npt"], zat=s["zat"], sigat=s["sigat"], epsat=s["epsat"], rcut=s["rcut"],
+                   ualpha=t["ualpha"], epsi_four_pi=s["epsi_four_pi"], lewald=1, lljcut=1,
+                   **{k: s[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab",
+                                        "fmaxtab", "rumaxfac")})
+        ot = O.pot_tab(pot)
+        ot["r2atat"] = np.zeros(3)
+        od = dict(d)
+        od["ualpha"] = t["ualpha"]
+        od["ncut"] = O.alpha_to_ncut(s["uewaldtol"], q2, s["epsi_four_pi"], min(s["boxlen"]), t["ualpha"])
+        o = O.System(od, ot, maxnneigh=n)
+        o.set_state(s["ro"], s["rod"])
+        o.set_vlist()
+        u = o.utotal()
+        o.mc_seed(1)
+        t0 = time.perf_counter()
+        o.mc_pass(1, dtran, beta, u)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / cpu_s, "unit": "trial moves/s", "cores": 1, "kind": "port",
+                               "sample": "one sweep (1000 trial moves) of the same chain, oracle (FP64 C "
+                                         "restatement of SPartMove/DUTotal/Metropolis/MCUpdate), 1 thread"}
+    return out
+
+
 def run_serving(a):
     """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
     half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
@@ -612,11 +688,13 @@ def run_gpu(a):
                "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
                          "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
 
-    ensemble = serving = bd = ewstd = None
+    ensemble = serving = bd = ewstd = mc = None
     if rank == 0 and world == 1 and a.bd:
         bd = run_bd(a, flush)
     if rank == 0 and world == 1 and a.ewald_std:
         ewstd = run_ewald_std(a, flush)
+    if rank == 0 and world == 1 and a.mc:
+        mc = run_mc(a)
     if rank == 0 and world == 1 and a.ensemble > 0:
         ensemble = run_ensemble(a, flush)
     if rank == 0 and world == 1 and a.serve_jobs > 0:
@@ -636,7 +714,7 @@ def run_gpu(a):
                        "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
                        "rebuilds_in_timed_steps": int(rebuilds), "pair_kernel": tuned},
             "fp64_value": fp64_value, "batched": batched, "ensemble": ensemble, "serving": serving,
-            "bd_200k": bd, "ewald_std_1000": ewstd,
+            "bd_200k": bd, "ewald_std_1000": ewstd, "mc_1000": mc,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

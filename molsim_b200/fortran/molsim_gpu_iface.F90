@@ -44,6 +44,13 @@ module MolsimGpu
       real(c_double) :: utot, utwob0, utwob(10), urec, ubond, virial, ekin
    end type msg_energy
 
+   ! struct msg_mc_params
+   type, bind(c) :: msg_mc_params
+      real(c_double)     :: beta                 ! MOLSIM's beta
+      type(c_ptr)        :: dtran                ! c_loc(dtran(1:npt))
+      integer(c_int32_t) :: isamp, pad
+   end type msg_mc_params
+
    interface
       integer(c_int) function msg_create(p, precision, h) bind(c, name='msg_create')
          import :: c_int, c_int32_t, c_ptr, msg_params
@@ -112,6 +119,21 @@ module MolsimGpu
          integer(c_int32_t), value :: isys, nsteps
          type(c_ptr), value        :: ro, rod, rodd, e   ! (3,np) real(8) each; e: msg_energy(nsteps) or c_null_ptr
       end function msg_velver_host
+
+      integer(c_int) function msg_mc_seed(h, isys, iseed) bind(c, name='msg_mc_seed')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys, iseed
+      end function msg_mc_seed
+
+      integer(c_int) function msg_mc_pass(h, npass, p, accepted, hsreject, isys, e) bind(c, name='msg_mc_pass')
+         import :: c_int, c_int32_t, c_ptr, msg_mc_params
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: npass
+         type(msg_mc_params), intent(in) :: p(*)
+         type(c_ptr), value        :: accepted, hsreject, e   ! int64(nsys), int64(nsys), msg_energy, or c_null_ptr
+         integer(c_int32_t), value :: isys
+      end function msg_mc_pass
 
       integer(c_int) function msg_bd_step(h, nsteps, seed, isys, xi, xi_out, e) bind(c, name='msg_bd_step')
          import :: c_int, c_int32_t, c_int64_t, c_ptr
