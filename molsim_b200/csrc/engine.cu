@@ -2013,7 +2013,7 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
     if (npass > 0) {
         const size_t smem = h->any_std ? 6 * (size_t)h->ew_maxw * sizeof(double2) : 0;
         k_mc_pass<<<h->nsys, MC_THREADS, smem, h->st>>>(
-            h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tz, h->tc, h->ew_kv, h->ew_kfac, h->ew_sk,
+            h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tz, h->tc, h->bst, h->ew_kv, h->ew_kfac, h->ew_sk,
             h->ew_sktm, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bk, h->beq, h->bpw, h->mc_par, h->mc_dtr,
             h->mc_rng, h->mc_u, h->mc_cnt, npass);
         h->launches += 1;

@@ -47,12 +47,21 @@ __device__ __forceinline__ double mc_random(int2 &st)
     return __dmul_rn(am, (double)((2147483647 & (st.x ^ st.y)) | 1));
 }
 
-// u(r2) of one type pair: the reference's table walk from the pair's first
-// interval (the lookup of UTwoBodyANewCellList, Src/denergy.F90:779-785).
+// u(r2) of one type pair: the reference's table walk (the lookup of
+// UTwoBodyANewCellList, Src/denergy.F90:779-785), entered at the bucket start, which
+// only skips intervals the walk from the pair's first interval would pass.
 __device__ __forceinline__ double mc_tab_u(const PairTab &T, const double *__restrict__ tz,
-                                           const double *__restrict__ tc, double r2)
+                                           const double *__restrict__ tc, const unsigned short *__restrict__ bst,
+                                           double r2)
 {
-    int k = T.k0;
+    int k = 0;
+    const float r2f = (float)r2;
+    if (r2f < T.fz_hi) {
+        int b = (int)((r2f - T.fz_lo) * T.finv_h);
+        b = b < 0 ? 0 : (b >= MSG_NBUCKET ? MSG_NBUCKET - 1 : b);
+        k = bst[T.b0 + b];
+    }
+    k += T.k0;
     while (r2 < tz[k]) ++k;
     const double *c = tc + (size_t)12 * k;
     const double d = r2 - c[0];
@@ -73,7 +82,8 @@ __device__ __forceinline__ void mc_block_add(double v, double (*red)[MC_THREADS 
 __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     const SysDev *__restrict__ sysv, double4 *__restrict__ pos, const int *__restrict__ typ,
     const int *__restrict__ inv, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
-    const double *__restrict__ tz, const double *__restrict__ tc, const int4 *__restrict__ kv,
+    const double *__restrict__ tz, const double *__restrict__ tc, const unsigned short *__restrict__ bst,
+    const int4 *__restrict__ kv,
     const double *__restrict__ kfac, double2 *__restrict__ sk, double2 *__restrict__ sktm,
     const int *__restrict__ bptr, const int *__restrict__ bpart, const double *__restrict__ bk,
     const double *__restrict__ beq, const int *__restrict__ bpw, const McPar *__restrict__ par,
@@ -171,13 +181,13 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                     if (r2n < T.r2atat || r2n < T.r2umin)
                         over = true;
                     else
-                        v += mc_tab_u(T, tz, tc, r2n);
+                        v += mc_tab_u(T, tz, tc, bst, r2n);
                 }
                 dx = r0[0] - xj.x;
                 dy = r0[1] - xj.y;
                 dz = r0[2] - xj.z;
                 const double r2o = pbcr2_exact(dx, dy, dz, S);
-                if (r2o < S.rcut2) v -= mc_tab_u(T, tz, tc, r2o);
+                if (r2o < S.rcut2) v -= mc_tab_u(T, tz, tc, bst, r2o);
 #pragma unroll
                 for (int p = 0; p < 10; ++p)
                     if (p == pl) du[p] += v;
