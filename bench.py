@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=512,
                     help="systems in the batched ensemble (0: skip)")
     ap.add_argument("--bd", type=int, default=1, help="time the 200,000-particle BD system (0: skip)")
+    ap.add_argument("--serve-wait", type=float, default=0.0,
+                    help="serving: batching window in seconds before a cohort forms")
+    ap.add_argument("--serve-ahead", type=int, default=2, help="serving: step chunks enqueued per cohort")
     ap.add_argument("--mc", type=int, default=1,
                     help="time Monte Carlo sweeps of the 1000-ion electrolyte, one chain and an ensemble (0: skip)")
     ap.add_argument("--ewald-std", type=int, default=1,
@@ -505,7 +508,8 @@ def run_serving(a):
     # load the library and fill the cuFFT plan cache outside the measured stream
     warm = poisson_stream(seed=12, rate=1e6, njobs=4, nmin=100, nmax=400, nsteps=20)
     Server(1 << 30, precision="mixed", chunk=10).run(warm, realtime=False)
-    srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50)
+    srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50,
+                 batch_wait_s=a.serve_wait, ahead=a.serve_ahead)
     torch.cuda.synchronize()
     m = srv.run(jobs)
     m.pop("latencies", None)

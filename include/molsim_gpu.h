@@ -117,6 +117,10 @@ int32_t msg_nsys(const msg_handle *h);
 /* Positions ro, velocities rod, accelerations rodd of system isys, [np][3]; NULL skips. */
 int  msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd);
 int  msg_get_state(msg_handle *h, int32_t isys, double *ro, double *rod, double *rodd);
+/* msg_set_state for every system at once: ro, rod, rodd hold the systems' [np][3]
+ * blocks one after another in handle order (rod, rodd may be NULL); every list is
+ * rebuilt; one wait for the device. */
+int  msg_set_state_all(msg_handle *h, const double *ro, const double *rod, const double *rodd);
 
 /* Rebuild the Verlet list now (SetVListMD semantics: r2 < (rcut+drnlist)^2 with
  * MOLSIM's PBCr2).  Optionally export it in MOLSIM's layout: nneighpn[np] and

@@ -62,6 +62,7 @@ SIGNATURES = {
     "msg_last_error": (C.c_char_p, [C.c_void_p]),
     "msg_nsys": (C.c_int32, [C.c_void_p]),
     "msg_set_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p]),
+    "msg_set_state_all": (C.c_int, [C.c_void_p, f64p, f64p, f64p]),
     "msg_get_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p]),
     "msg_build_nlist": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(C.c_int64)]),
     "msg_utotal": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, C.POINTER(MsgEnergy)]),

@@ -449,6 +449,20 @@ void msg_handle::ensure_stage(size_t n)
     stage_n = n;
 }
 
+// For the buckets b = 0..MSG_NBUCKET-1 at z(b) = z_lo + (b + frac) h: where the
+// reference's table walk stops, the first kk with kk == nk-1 or z(b) >= z[kk] (z falls
+// with kk).  z(b) grows with b, so the stop never moves up as b grows: one pointer
+// walked from the top bucket down gives every stop in O(buckets + intervals).
+static void bucket_stops(const double *z, int nk, double z_lo, double h, double frac, int *out)
+{
+    int kk = 0;
+    for (int b = MSG_NBUCKET - 1; b >= 0; --b) {
+        const double zq = z_lo + (b + frac) * h;
+        while (kk < nk - 1 && zq < z[kk]) ++kk;
+        out[b] = kk;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Set-up of all systems.
 // ---------------------------------------------------------------------------
@@ -613,7 +627,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             cgrid = dalloc<double2>(cgrid_tot);
         }
         std::vector<double> hm(fo_acc), he(fo_acc), hv(fo_acc);
-        for (int s = 0; s < n; ++s)
+        for (int s = 0; s < n && !dry; ++s)
             if (hs[s].lewald && !hs[s].recstd)
                 spme_factors(hs[s].s, hs[s].order, hs[s].alpha, hs[s].box, hm.data() + hs[s].fac_off,
                              he.data() + hs[s].fac_off, hv.data() + hs[s].fac_off);
@@ -762,12 +776,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                 T.fz_hi = (float)T.z_hi;
                 T.finv_h = (float)T.inv_h;
                 T.b0 = (int)vb.size();
-                for (int b = 0; b < MSG_NBUCKET; ++b) {
-                    const double zq = T.z_lo + (b + 2) * h;
-                    int kk = 0;
-                    while (kk < T.nk - 1 && zq < z[kk]) ++kk;
-                    vb.push_back((unsigned short)kk);
-                }
+                int stop[MSG_NBUCKET];
+                bucket_stops(z, T.nk, T.z_lo, h, 2.0, stop);
+                for (int b = 0; b < MSG_NBUCKET; ++b) vb.push_back((unsigned short)stop[b]);
             }
         S.tab_k0 = pt[S.pt_off].k0;
         if ((int)vz.size() - S.tab_k0 > 65535) throw CudaError{MSG_ERR_ARG, "more than 65535 table intervals in one system"};
@@ -812,10 +823,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
                 const PairTab &T = pt[hs[s].pt_off + q];
                 const double *z = vz.data() + T.k0;
                 const double h = (T.z_hi > T.z_lo) ? (T.z_hi - T.z_lo) / MSG_NBUCKET : 1.0;
+                int stop[MSG_NBUCKET];
+                bucket_stops(z, T.nk, T.z_lo, h, 1.01, stop);
                 for (int b = 0; b < MSG_NBUCKET; ++b) {
-                    const double zq = T.z_lo + (b + 1.01) * h;
-                    int kk = 0;
-                    while (kk < T.nk - 1 && zq < z[kk]) ++kk;
+                    const int kk = stop[b];
                     float zf = (float)z[kk];
                     int zi;
                     std::memcpy(&zi, &zf, sizeof(zi));
@@ -1095,12 +1106,22 @@ void msg_handle::plan_fft()
                 cufftHandle hp = 0;
                 size_t ws = 0;
                 if (dry) {
-                    int dims[3] = {fc.s, fc.s, fc.s};
-                    const cufftType t = dir ? (f32 ? CUFFT_R2C : CUFFT_D2Z) : (f32 ? CUFFT_C2R : CUFFT_Z2D);
-                    // without a device cuFFT cannot estimate: assume one complex grid per transform
-                    if (cufftEstimateMany(3, dims, nullptr, 1, dir ? (int)rs : (int)cs, nullptr, 1,
-                                          dir ? (int)cs : (int)rs, t, c, &ws) != CUFFT_SUCCESS)
-                        ws = (size_t)c * (size_t)cs * (f32 ? sizeof(float2) : sizeof(double2));
+                    // the estimate depends on the plan's shape only: asked once per shape
+                    static std::mutex est_mu;
+                    static std::map<PlanKey, size_t> est_cache;
+                    std::lock_guard<std::mutex> lk(est_mu);
+                    auto it = est_cache.find(key);
+                    if (it != est_cache.end()) {
+                        ws = it->second;
+                    } else {
+                        int dims[3] = {fc.s, fc.s, fc.s};
+                        const cufftType t = dir ? (f32 ? CUFFT_R2C : CUFFT_D2Z) : (f32 ? CUFFT_C2R : CUFFT_Z2D);
+                        // without a device cuFFT cannot estimate: assume one complex grid per transform
+                        if (cufftEstimateMany(3, dims, nullptr, 1, dir ? (int)rs : (int)cs, nullptr, 1,
+                                              dir ? (int)cs : (int)rs, t, c, &ws) != CUFFT_SUCCESS)
+                            ws = (size_t)c * (size_t)cs * (f32 ? sizeof(float2) : sizeof(double2));
+                        est_cache[key] = ws;
+                    }
                 } else {
                     {
                         std::lock_guard<std::mutex> lk(g_plan_mu);
@@ -1773,6 +1794,21 @@ extern "C" int msg_set_state(msg_handle *h, int32_t isys, const double *ro, cons
     if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
     API_BEGIN
     return put_state(h, isys, ro, rod, rodd, false);
+    API_END
+}
+
+extern "C" int msg_set_state_all(msg_handle *h, const double *ro, const double *rod, const double *rodd)
+{
+    if (!h || !ro) return MSG_ERR_ARG;
+    API_BEGIN
+    // every system's copies and conversion on the stream, then one rebuild of every list
+    size_t at = 0;
+    for (int s = 0; s < h->nsys; ++s) {
+        upload_state(h, s, ro + at, rod ? rod + at : nullptr, rodd ? rodd + at : nullptr);
+        at += 3 * (size_t)h->hs[s].n;
+    }
+    std::vector<int> all(h->nsys, 1);
+    return h->rebuild_checked(all);
     API_END
 }
 

@@ -64,11 +64,12 @@ class Job:
 class GpuCohort:
     """A cohort on the device: one batch handle, stepped asynchronously."""
 
-    def __init__(self, jobs, precision, chunk):
+    def __init__(self, jobs, precision, chunk, ahead=2):
         from .engine import Engine
 
         self.jobs = jobs
         self.chunk = chunk
+        self.ahead = ahead
         self.eng = Engine([j.system for j in jobs], [j.table for j in jobs], precision=precision)
         self.eng.UTotal(0)            # forces and energies of every system
         self.eng.GetLinAcc()
@@ -76,9 +77,9 @@ class GpuCohort:
         self.nbytes = self.eng.device_bytes()
 
     def pump(self):
-        """Keep up to two chunks in flight; True once every step has run."""
+        """Keep up to `ahead` chunks in flight; True once every step has run."""
         pend = self.eng.pending()
-        while self.left > 0 and pend < 2:
+        while self.left > 0 and pend < self.ahead:
             k = min(self.chunk, self.left)
             self.eng.velver_async(k)
             self.left -= k
@@ -103,6 +104,9 @@ class Server:
     max_cohorts:  cohorts resident at once (streams in use).
     max_jobs:     jobs per cohort.
     chunk:        steps per asynchronous enqueue.
+    batch_wait_s: batching window: a cohort is formed once the queue holds max_jobs
+                  jobs, its head job has waited this long, or no arrivals remain (0: at once).
+    ahead:        step chunks each cohort keeps enqueued.
     headroom:     factor on each job's set-up estimate reserved at admission; the
                   Verlet rows may grow past their initial capacity (x1.5 of the longest
                   row) when the first list is built.  Once a cohort exists its reservation
@@ -110,7 +114,7 @@ class Server:
     """
 
     def __init__(self, budget_bytes, precision="mixed", max_cohorts=8, max_jobs=64, chunk=50,
-                 backend=None, clock=None, estimate=None, headroom=1.5):
+                 backend=None, clock=None, estimate=None, headroom=1.5, batch_wait_s=0.0, ahead=2):
         self.budget = int(budget_bytes)
         self.precision = precision
         self.max_cohorts = max_cohorts
@@ -125,6 +129,8 @@ class Server:
                 return estimate_bytes(job.system, job.table, precision)
         self.estimate = estimate
         self.headroom = headroom
+        self.batch_wait_s = batch_wait_s
+        self.ahead = ahead
         self.used = 0
         self.device_now = 0
         self.peak_device = 0
@@ -173,6 +179,9 @@ class Server:
                 queue.append(j)
             # admission
             while queue and len(running) < self.max_cohorts:
+                if (self.batch_wait_s > 0 and ia < len(pending) and len(queue) < self.max_jobs
+                        and now - queue[0].arrival < self.batch_wait_s):
+                    break                           # batching window still open
                 take, tot = self._form(queue, self.budget - self.used)
                 if not take:
                     break
@@ -180,7 +189,8 @@ class Server:
                 queue = [j for j in queue if id(j) not in ids]
                 tadm = self.clock() - t0
                 try:
-                    c = self.backend(take, self.precision, self.chunk)
+                    c = self.backend(take, self.precision, self.chunk, self.ahead) \
+                        if self.backend is GpuCohort else self.backend(take, self.precision, self.chunk)
                 except Exception as exc:          # set-up failed: these jobs fail, the server goes on
                     self._fail(take, exc, self.clock() - t0, finished)
                     continue

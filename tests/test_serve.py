@@ -180,3 +180,19 @@ def test_device_error_fails_the_cohort_and_the_server_goes_on():
     assert m["failed"] == 1 and "r2umin" in jobs[1].error
     assert all(j.result for j in jobs if j.jid != 1)
     assert srv.used == 0
+
+
+def test_batching_window_gathers_early_arrivals():
+    """With a batching window, the first cohort waits for the jobs arriving inside it
+    instead of starting with the first job alone; without one it starts at once."""
+    def run(wait):
+        jobs = _jobs([(100, 20, 0.001 * k, 1) for k in range(30)])
+        srv = Server(1000, backend=FakeCohort, clock=TickClock(), estimate=lambda j: j.nbytes,
+                     max_cohorts=4, max_jobs=64, chunk=5, batch_wait_s=wait)
+        m = srv.run(jobs, poll_s=0)
+        assert m["jobs"] == 30 and m["failed"] == 0
+        return srv.cohort_sizes
+
+    at_once, windowed = run(0.0), run(0.01)
+    assert windowed[0] > at_once[0] + 2
+    assert len(windowed) < len(at_once)
