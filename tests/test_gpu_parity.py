@@ -332,3 +332,28 @@ def test_velver_host_equals_put_step_get(precision, host):
     for x, y in zip(ea, eb):
         for k in ("utot", "virial", "ekin"):
             assert x[k] == y[k] if precision == "mixed" else abs(x[k] - y[k]) <= 1e-9 * abs(x[k]), k
+
+
+def test_set_state_all_equals_set_state_per_system():
+    """msg_set_state_all (every system's state, one rebuild, one wait) leaves a batch
+    handle exactly as msg_set_state per system does: same lists, forces and energies."""
+    import ctypes as C
+
+    from molsim_b200 import _lib
+
+    sy = [dict(Hp.pe_small()), dict(Hp.electrolyte_small()), dict(Hp.electrolyte_small(seed=5))]
+    tb = [Hp.oracle_table(s) for s in sy]
+    a = Engine(sy, tb, precision="mixed")            # built through msg_set_state_all
+    b = Engine(sy, tb, precision="mixed")
+    for k, s in enumerate(sy):
+        b.set_state(k, s["ro"], s.get("rod"), s.get("rodd"))
+    for g in (a, b):
+        g.UTotal(0)
+    for k, s in enumerate(sy):
+        na, ja, pa = a.SetVList(k, export=True, maxnneigh=s["np"])
+        nb, jb, pb = b.SetVList(k, export=True, maxnneigh=s["np"])
+        assert pa == pb and np.array_equal(na, nb) and np.array_equal(ja, jb)
+        assert np.array_equal(a.forces(k)[0], b.forces(k)[0])
+        assert a.energy(k) == b.energy(k)
+    assert _lib.lib().msg_set_state_all(a.h, None, None, None) == 6
+    del C
