@@ -337,8 +337,6 @@ def test_velver_host_equals_put_step_get(precision, host):
 def test_set_state_all_equals_set_state_per_system():
     """msg_set_state_all (every system's state, one rebuild, one wait) leaves a batch
     handle exactly as msg_set_state per system does: same lists, forces and energies."""
-    import ctypes as C
-
     from molsim_b200 import _lib
 
     sy = [dict(Hp.pe_small()), dict(Hp.electrolyte_small()), dict(Hp.electrolyte_small(seed=5))]
@@ -356,4 +354,3 @@ def test_set_state_all_equals_set_state_per_system():
         assert np.array_equal(a.forces(k)[0], b.forces(k)[0])
         assert a.energy(k) == b.energy(k)
     assert _lib.lib().msg_set_state_all(a.h, None, None, None) == 6
-    del C
