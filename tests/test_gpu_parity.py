@@ -339,7 +339,8 @@ def test_set_state_all_equals_set_state_per_system():
     handle exactly as msg_set_state per system does: same lists, forces and energies."""
     from molsim_b200 import _lib
 
-    sy = [dict(Hp.pe_small()), dict(Hp.electrolyte_small()), dict(Hp.electrolyte_small(seed=5))]
+    sy = [dict(Hp.electrolyte_small()), dict(Hp.electrolyte_small(seed=5)),
+          dict(Hp.electrolyte_small(n_pairs=50, L=36.0, seed=4))]
     tb = [Hp.oracle_table(s) for s in sy]
     a = Engine(sy, tb, precision="mixed")            # built through msg_set_state_all
     b = Engine(sy, tb, precision="mixed")
