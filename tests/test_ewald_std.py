@@ -145,3 +145,26 @@ def test_repeat_is_bitwise_mixed():
     r2 = g.UTotal()
     assert np.array_equal(r1["force"], r2["force"])
     assert r1["urec"] == r2["urec"] and r1["virial"] == r2["virial"]
+
+
+@pytest.mark.gpu
+def test_bd_with_injected_noise_std():
+    """Brownian dynamics (BDStep, Src/bd.F90:120-155) with the caller's noise on the
+    standard Ewald sum: five steps against the oracle."""
+    s = Hp.std_ewald(Hp.colloid_small())
+    t, o, g = _pair(s, "fp64")
+    o.utotal()
+    g.UTotal()
+    rng = np.random.default_rng(9)
+    xi = rng.standard_normal((5, s["np"], 3))
+    fac1, fac2 = s["bd_fac"]
+    eg = g.BDStep(5, xi=xi)
+    for k in range(5):
+        o.bd_step(xi[k], fac1, fac2)
+    d = g.get_state()["ro"] - o.get_state()["ro"]
+    box = s["boxlen"][0]
+    d -= box * np.round(d / box)
+    assert np.abs(d).max() < 1e-9
+    rg, ro = g.UTotal(), o.utotal()
+    _check(ro, rg, 1e-10)
+    assert Hp.rel(eg[-1]["utot"], ro["utot"]) < ENERGY_TOL
