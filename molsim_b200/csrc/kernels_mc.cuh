@@ -105,215 +105,222 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     double *u = mcu + (size_t)sys * ESZ;
     long long nacc = 0, nhs = 0;
     const double tp = 2.0 * 3.1415926535897932;
-    for (int pass = 0; pass < npass; ++pass) {
-        for (int ipass = 0; ipass < S.n; ++ipass) {
-            // ---- trial move: particle, displacement, periodic wrap (thread 0) ----
-            if (t == 0) {
-                int ip = (P.isamp == 0) ? ipass + 1 : 1 + (int)(S.n * mc_random(st));
-                ip = max(1, min(ip, S.n)) - 1;
-                const int i = inv[S.off + ip];
-                const int ty = typ[i];
-                const double dt = dtr[S.type_off + ty];
-                double d[3];
-                if (dt >= 0.0) {
-                    for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(mc_random(st) - 0.5, dt);
-                } else {
-                    for (;;) {
-                        for (int m = 0; m < 3; ++m) d[m] = mc_random(st) - 0.5;
-                        if (__dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2])) <
-                            0.25)
-                            break;
-                    }
-                    for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(d[m], fabs(dt));
-                }
-                const double4 x = pos[i];
-                const double xo[3] = {x.x, x.y, x.z};
-                for (int m = 0; m < 3; ++m) {
-                    sro[m] = xo[m];
-                    srt[m] = pbc_wrap(__dadd_rn(xo[m], d[m]), S.half[m], S.box[m], S.boxi[m]);
-                }
-                sq = x.w;
-                si = i;
-                sip = ip;
-                sty = ty;
-                sover = 0;
+    const long long ntrial = (long long)npass * S.n;
+    // Thread 0 sets up a trial: particle, displacement, periodic wrap.
+    auto setup = [&](int ipass) {
+        int ip = (P.isamp == 0) ? ipass + 1 : 1 + (int)(S.n * mc_random(st));
+        ip = max(1, min(ip, S.n)) - 1;
+        const int i = inv[S.off + ip];
+        const int ty = typ[i];
+        const double dt = dtr[S.type_off + ty];
+        double d[3];
+        if (dt >= 0.0) {
+            for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(mc_random(st) - 0.5, dt);
+        } else {
+            for (;;) {
+                for (int m = 0; m < 3; ++m) d[m] = mc_random(st) - 0.5;
+                if (__dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2])) < 0.25)
+                    break;
             }
-            __syncthreads();
-            const int i = si, ty = sty;
-            const double q = sq;
-            const double rt[3] = {srt[0], srt[1], srt[2]}, r0[3] = {sro[0], sro[1], sro[2]};
-            // ---- exp(i 2pi n x / L) of the trial and the current position (standard Ewald) ----
-            if (S.recstd && t < 6) {
-                const int m = t % 3;
-                const double xm = (t < 3) ? rt[m] : r0[m];
-                double sn, cs;
-                sincos(tp * S.boxi[m] * xm, &sn, &cs);
-                const double2 e1 = make_double2(cs, sn);
-                double2 *row = etab + t * w;
-                double2 e = make_double2(1.0, 0.0);
-                row[0] = e;
-                for (int n = 1; n < w; ++n) {
-                    e = (n == 1) ? e1 : cmul(e, e1);
-                    row[n] = e;
-                }
+            for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(d[m], fabs(dt));
+        }
+        const double4 x = pos[i];
+        const double xo[3] = {x.x, x.y, x.z};
+        for (int m = 0; m < 3; ++m) {
+            sro[m] = xo[m];
+            srt[m] = pbc_wrap(__dadd_rn(xo[m], d[m]), S.half[m], S.box[m], S.boxi[m]);
+        }
+        sq = x.w;
+        si = i;
+        sip = ip;
+        sty = ty;
+        sover = 0;
+    };
+    // the structure factors in use and the trial's, swapped when a move is accepted
+    double2 *scur = sk, *stry = sktm;
+    if (t == 0 && ntrial > 0) setup(0);
+    __syncthreads();
+    for (long long m = 0; m < ntrial; ++m) {
+        const int i = si, ty = sty;
+        const double q = sq;
+        const double rt[3] = {srt[0], srt[1], srt[2]}, r0[3] = {sro[0], sro[1], sro[2]};
+        // ---- exp(i 2pi n x / L) of the trial and the current position (standard Ewald) ----
+        if (S.recstd && t < 6) {
+            const int c3 = t % 3;
+            const double xm = (t < 3) ? rt[c3] : r0[c3];
+            double sn, cs;
+            sincos(tp * S.boxi[c3] * xm, &sn, &cs);
+            const double2 e1 = make_double2(cs, sn);
+            double2 *row = etab + t * w;
+            double2 e = make_double2(1.0, 0.0);
+            row[0] = e;
+            for (int n = 1; n < w; ++n) {
+                e = (n == 1) ? e1 : cmul(e, e1);
+                row[n] = e;
             }
-            // ---- pair differences (and the dipole sum of the surface term) ----
-            double du[10];
+        }
+        // ---- pair differences (and the dipole sum of the surface term) ----
+        double du[10];
 #pragma unroll
-            for (int p = 0; p < 10; ++p) du[p] = 0.0;
-            double dip0 = 0.0, dip1 = 0.0, dip2 = 0.0;
-            bool over = false;
-            for (int j = S.off + t; j < S.off + S.n; j += MC_THREADS) {
-                const double4 xj = pos[j];
-                if (S.lsurf) {
-                    dip0 += xj.w * xj.x;
-                    dip1 += xj.w * xj.y;
-                    dip2 += xj.w * xj.z;
-                }
-                if (j == i) continue;
-                const int pg = pair_of(ptmap, S, ty, typ[j]);
-                const PairTab &T = ptab[pg];
-                const int pl = pg - S.pt_off;
-                double dx = rt[0] - xj.x, dy = rt[1] - xj.y, dz = rt[2] - xj.z;
-                const double r2n = pbcr2_exact(dx, dy, dz, S);
-                double v = 0.0;
-                if (r2n < S.rcut2) {
-                    if (r2n < T.r2atat || r2n < T.r2umin)
-                        over = true;
-                    else
-                        v += mc_tab_u(T, tz, tc, bst, r2n);
-                }
-                dx = r0[0] - xj.x;
-                dy = r0[1] - xj.y;
-                dz = r0[2] - xj.z;
-                const double r2o = pbcr2_exact(dx, dy, dz, S);
-                if (r2o < S.rcut2) v -= mc_tab_u(T, tz, tc, bst, r2o);
-#pragma unroll
-                for (int p = 0; p < 10; ++p)
-                    if (p == pl) du[p] += v;
+        for (int p = 0; p < 10; ++p) du[p] = 0.0;
+        double dip0 = 0.0, dip1 = 0.0, dip2 = 0.0;
+        bool over = false;
+        for (int j = S.off + t; j < S.off + S.n; j += MC_THREADS) {
+            const double4 xj = pos[j];
+            if (S.lsurf) {
+                dip0 += xj.w * xj.x;
+                dip1 += xj.w * xj.y;
+                dip2 += xj.w * xj.z;
             }
-            if (over) sover = 1;
-            __syncthreads();                   // tables ready
-            // ---- structure factors of the trial (standard Ewald) ----
-            double dr = 0.0;
-            if (S.recstd) {
-                const double2 *tx = etab, *ty_ = etab + w, *tzn = etab + 2 * w;
-                const double2 *ox = etab + 3 * w, *oy = etab + 4 * w, *oz = etab + 5 * w;
-                for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {
-                    const size_t g = (size_t)S.ew_kv_off + kn;
-                    const int4 n = kv[g];
-                    const double2 yzm = cmul(cconj(oy[n.y]), oz[n.z]), yzp = cmul(oy[n.y], oz[n.z]);
-                    const double2 yzmt = cmul(cconj(ty_[n.y]), tzn[n.z]), yzpt = cmul(ty_[n.y], tzn[n.z]);
-                    const double2 xo = ox[n.x], xt = tx[n.x];
-                    const double2 nw[4] = {cmul(cconj(xt), yzmt), cmul(cconj(xt), yzpt), cmul(xt, yzmt), cmul(xt, yzpt)};
-                    const double2 od[4] = {cmul(cconj(xo), yzm), cmul(cconj(xo), yzp), cmul(xo, yzm), cmul(xo, yzp)};
-                    double tnew = 0.0, told = 0.0;
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const double2 s0 = sk[g * 4 + c];
-                        const double2 s1 = make_double2(s0.x + q * (nw[c].x - od[c].x), s0.y + q * (nw[c].y - od[c].y));
-                        sktm[g * 4 + c] = s1;
-                        tnew = tnew + (s1.x * s1.x + s1.y * s1.y);
-                        told = told + (s0.x * s0.x + s0.y * s0.y);
-                    }
-                    dr = dr + kfac[g] * (tnew - told);
-                }
+            if (j == i) continue;
+            const int pg = pair_of(ptmap, S, ty, typ[j]);
+            const PairTab &T = ptab[pg];
+            const int pl = pg - S.pt_off;
+            double dx = rt[0] - xj.x, dy = rt[1] - xj.y, dz = rt[2] - xj.z;
+            const double r2n = pbcr2_exact(dx, dy, dz, S);
+            double v = 0.0;
+            if (r2n < S.rcut2) {
+                if (r2n < T.r2atat || r2n < T.r2umin)
+                    over = true;
+                else
+                    v += mc_tab_u(T, tz, tc, bst, r2n);
             }
+            dx = r0[0] - xj.x;
+            dy = r0[1] - xj.y;
+            dz = r0[2] - xj.z;
+            const double r2o = pbcr2_exact(dx, dy, dz, S);
+            if (r2o < S.rcut2) v -= mc_tab_u(T, tz, tc, bst, r2o);
 #pragma unroll
             for (int p = 0; p < 10; ++p)
-                if (p < natat) mc_block_add(du[p], red, p);
-            mc_block_add(dr, red, 10);
-            if (S.lsurf) {
-                mc_block_add(dip0, red, 11);
-                mc_block_add(dip1, red, 12);
-                mc_block_add(dip2, red, 13);
-            }
-            __syncthreads();
-            // ---- DUTotal's sum, bonds, surface, Metropolis (thread 0) ----
-            if (t == 0) {
-                int acc = 0;
-                double dtw[10], dutot = 0.0, durec = 0.0, dubond = 0.0;
-                if (sover) {
-                    ++nhs;                     // Metropolis: hard-core reject, no random number
-                } else {
-                    double d0 = 0.0;
-                    for (int p = 0; p < natat; ++p) {
-                        double a = 0.0;
-                        for (int k = 0; k < MC_THREADS / 32; ++k) a += red[p][k];
-                        dtw[p] = a;
-                        d0 += a;
-                    }
-                    dutot = d0;
-                    if (S.lewald) {
-                        for (int k = 0; k < MC_THREADS / 32; ++k) durec += red[10][k];
-                        if (S.lsurf) {
-                            double m0 = 0.0, m1 = 0.0, m2 = 0.0;
-                            for (int k = 0; k < MC_THREADS / 32; ++k) {
-                                m0 += red[11][k];
-                                m1 += red[12][k];
-                                m2 += red[13][k];
-                            }
-                            const double fac = tp / (3.0 * S.vol);
-                            const double a0 = m0 + q * (rt[0] - r0[0]), a1 = m1 + q * (rt[1] - r0[1]),
-                                         a2 = m2 + q * (rt[2] - r0[2]);
-                            durec += fac * ((a0 * a0 + a1 * a1 + a2 * a2) - (m0 * m0 + m1 * m1 + m2 * m2));
-                        }
-                        durec = S.epsfp * durec;
-                        dutot += durec;
-                    }
-                    const int ip = sip;
-                    for (int b = bptr ? bptr[S.off + ip] : 0; bptr && b < bptr[S.off + ip + 1]; ++b) {
-                        const double4 xb = pos[inv[S.off + bpart[b]]];
-                        double dx = rt[0] - xb.x, dy = rt[1] - xb.y, dz = rt[2] - xb.z;
-                        const double r2n = pbcr2_exact(dx, dy, dz, S);
-                        dx = r0[0] - xb.x;
-                        dy = r0[1] - xb.y;
-                        dz = r0[2] - xb.z;
-                        const double r2o = pbcr2_exact(dx, dy, dz, S);
-                        const double xn = sqrt(r2n) - beq[b], xo = sqrt(r2o) - beq[b];
-                        double pn = 1.0, po = 1.0;
-                        for (int e = 0; e < bpw[b]; ++e) {
-                            pn *= xn;
-                            po *= xo;
-                        }
-                        dubond += bk[b] * (pn - po);
-                    }
-                    dutot += dubond;
-                    const double dured = dutot * P.beta;
-                    if (dured > 87.0)
-                        acc = 0;
-                    else if (dured < -87.0)
-                        acc = 1;
-                    else {
-                        const double fac = exp(-dured);
-                        acc = (fac > 1.0) ? 1 : (fac > mc_random(st) ? 1 : 0);
-                    }
-                    if (acc) {
-                        ++nacc;
-                        u[0] += dutot;
-                        u[1] += d0;
-                        for (int p = 0; p < natat; ++p) u[2 + p] += dtw[p];
-                        if (S.lewald) u[12] += durec;
-                        u[13] += dubond;
-                        double4 x = pos[i];
-                        x.x = rt[0];
-                        x.y = rt[1];
-                        x.z = rt[2];
-                        pos[i] = x;
-                    }
-                }
-                sacc = acc;
-            }
-            __syncthreads();
-            if (sacc && S.recstd)
-                for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {
-                    const size_t g = (size_t)S.ew_kv_off + kn;
+                if (p == pl) du[p] += v;
+        }
+        if (over) sover = 1;
+        __syncthreads();                       // tables ready, overlap flag final
+        // ---- structure factors of the trial (standard Ewald) ----
+        double dr = 0.0;
+        if (S.recstd) {
+            const double2 *tx = etab, *ty_ = etab + w, *tzn = etab + 2 * w;
+            const double2 *ox = etab + 3 * w, *oy = etab + 4 * w, *oz = etab + 5 * w;
+            for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {
+                const size_t g = (size_t)S.ew_kv_off + kn;
+                const int4 n = kv[g];
+                const double2 yzm = cmul(cconj(oy[n.y]), oz[n.z]), yzp = cmul(oy[n.y], oz[n.z]);
+                const double2 yzmt = cmul(cconj(ty_[n.y]), tzn[n.z]), yzpt = cmul(ty_[n.y], tzn[n.z]);
+                const double2 xo = ox[n.x], xt = tx[n.x];
+                const double2 nw[4] = {cmul(cconj(xt), yzmt), cmul(cconj(xt), yzpt), cmul(xt, yzmt), cmul(xt, yzpt)};
+                const double2 od[4] = {cmul(cconj(xo), yzm), cmul(cconj(xo), yzp), cmul(xo, yzm), cmul(xo, yzp)};
+                double tnew = 0.0, told = 0.0;
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) sk[g * 4 + c] = sktm[g * 4 + c];
+                for (int c = 0; c < 4; ++c) {
+                    const double2 s0 = scur[g * 4 + c];
+                    const double2 s1 = make_double2(s0.x + q * (nw[c].x - od[c].x), s0.y + q * (nw[c].y - od[c].y));
+                    stry[g * 4 + c] = s1;
+                    tnew = tnew + (s1.x * s1.x + s1.y * s1.y);
+                    told = told + (s0.x * s0.x + s0.y * s0.y);
                 }
-            __syncthreads();
+                dr = dr + kfac[g] * (tnew - told);
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < 10; ++p)
+            if (p < natat) mc_block_add(du[p], red, p);
+        mc_block_add(dr, red, 10);
+        if (S.lsurf) {
+            mc_block_add(dip0, red, 11);
+            mc_block_add(dip1, red, 12);
+            mc_block_add(dip2, red, 13);
+        }
+        __syncthreads();
+        // ---- DUTotal's sum, bonds, surface, Metropolis; then the next trial (thread 0) ----
+        if (t == 0) {
+            int acc = 0;
+            double dtw[10], dutot = 0.0, durec = 0.0, dubond = 0.0;
+            if (sover) {
+                ++nhs;                         // Metropolis: hard-core reject, no random number
+            } else {
+                double d0 = 0.0;
+                for (int p = 0; p < natat; ++p) {
+                    double a = 0.0;
+                    for (int k = 0; k < MC_THREADS / 32; ++k) a += red[p][k];
+                    dtw[p] = a;
+                    d0 += a;
+                }
+                dutot = d0;
+                if (S.lewald) {
+                    for (int k = 0; k < MC_THREADS / 32; ++k) durec += red[10][k];
+                    if (S.lsurf) {
+                        double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+                        for (int k = 0; k < MC_THREADS / 32; ++k) {
+                            m0 += red[11][k];
+                            m1 += red[12][k];
+                            m2 += red[13][k];
+                        }
+                        const double fac = tp / (3.0 * S.vol);
+                        const double a0 = m0 + q * (rt[0] - r0[0]), a1 = m1 + q * (rt[1] - r0[1]),
+                                     a2 = m2 + q * (rt[2] - r0[2]);
+                        durec += fac * ((a0 * a0 + a1 * a1 + a2 * a2) - (m0 * m0 + m1 * m1 + m2 * m2));
+                    }
+                    durec = S.epsfp * durec;
+                    dutot += durec;
+                }
+                const int ip = sip;
+                for (int b = bptr ? bptr[S.off + ip] : 0; bptr && b < bptr[S.off + ip + 1]; ++b) {
+                    const double4 xb = pos[inv[S.off + bpart[b]]];
+                    double dx = rt[0] - xb.x, dy = rt[1] - xb.y, dz = rt[2] - xb.z;
+                    const double r2n = pbcr2_exact(dx, dy, dz, S);
+                    dx = r0[0] - xb.x;
+                    dy = r0[1] - xb.y;
+                    dz = r0[2] - xb.z;
+                    const double r2o = pbcr2_exact(dx, dy, dz, S);
+                    const double xn = sqrt(r2n) - beq[b], xo = sqrt(r2o) - beq[b];
+                    double pn = 1.0, po = 1.0;
+                    for (int e = 0; e < bpw[b]; ++e) {
+                        pn *= xn;
+                        po *= xo;
+                    }
+                    dubond += bk[b] * (pn - po);
+                }
+                dutot += dubond;
+                const double dured = dutot * P.beta;
+                if (dured > 87.0)
+                    acc = 0;
+                else if (dured < -87.0)
+                    acc = 1;
+                else {
+                    const double fac = exp(-dured);
+                    acc = (fac > 1.0) ? 1 : (fac > mc_random(st) ? 1 : 0);
+                }
+                if (acc) {
+                    ++nacc;
+                    u[0] += dutot;
+                    u[1] += d0;
+                    for (int p = 0; p < natat; ++p) u[2 + p] += dtw[p];
+                    if (S.lewald) u[12] += durec;
+                    u[13] += dubond;
+                    double4 x = pos[i];
+                    x.x = rt[0];
+                    x.y = rt[1];
+                    x.z = rt[2];
+                    pos[i] = x;
+                }
+            }
+            sacc = acc;
+            if (m + 1 < ntrial) setup((int)((m + 1) % S.n));
+        }
+        __syncthreads();                       // decision and the next trial's set-up
+        if (sacc) {
+            double2 *tmp = scur;
+            scur = stry;
+            stry = tmp;
         }
     }
+    // the structure factors end where the last accepted move left them: back into sk
+    if (S.recstd && scur != sk)
+        for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {
+            const size_t g = (size_t)S.ew_kv_off + kn;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) sk[g * 4 + c] = scur[g * 4 + c];
+        }
     if (t == 0) {
         rng[sys] = st;
         cnt[2 * (size_t)sys] += nacc;
