@@ -2047,11 +2047,21 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
     h->enqueue_forces(0, false);
     CK(cudaMemcpyAsync(h->mc_u, h->esys, sizeof(double) * ESZ * h->nsys, cudaMemcpyDeviceToDevice, h->st));
     if (npass > 0) {
-        const size_t smem = h->any_std ? 6 * (size_t)h->ew_maxw * sizeof(double2) : 0;
+        // a chain reads its system from shared memory when every system's share fits and
+        // there are no more chains than SMs (each such block holds an SM on its own)
+        const int wmax = h->any_std ? h->ew_maxw : 1;
+        const size_t etab = 6 * (size_t)wmax * sizeof(double2);
+        size_t need = 0;
+        for (int s = 0; s < h->nsys; ++s)
+            need = std::max(need, mc_cache_bytes(h->hs[s].n, h->hs[s].tab_nk, h->hs[s].natat));
+        const int cache = (h->nsys <= h->nsm && etab + need <= 200 * 1024) ? 1 : 0;
+        const size_t smem = etab + (cache ? need : 0);
+        if (smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(k_mc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_mc_pass<<<h->nsys, MC_THREADS, smem, h->st>>>(
-            h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tz, h->tc, h->bst, h->ew_kv, h->ew_kfac, h->ew_sk,
+            h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tc, h->bst, h->ew_kv, h->ew_kfac, h->ew_sk,
             h->ew_sktm, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bk, h->beq, h->bpw, h->mc_par, h->mc_dtr,
-            h->mc_rng, h->mc_u, h->mc_cnt, npass);
+            h->mc_rng, h->mc_u, h->mc_cnt, npass, cache, wmax);
         h->launches += 1;
     }
     std::vector<long long> cnt(2 * (size_t)h->nsys);

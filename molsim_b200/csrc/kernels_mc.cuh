@@ -50,19 +50,23 @@ __device__ __forceinline__ double mc_random(int2 &st)
 // u(r2) of one type pair: the reference's table walk (the lookup of
 // UTwoBodyANewCellList, Src/denergy.F90:779-785), entered at the bucket start, which
 // only skips intervals the walk from the pair's first interval would pass.
-__device__ __forceinline__ double mc_tab_u(const PairTab &T, const double *__restrict__ tz,
-                                           const double *__restrict__ tc, const unsigned short *__restrict__ bst,
-                                           double r2)
+// tc/bst are the handle's arrays (koff = boff = 0) or the system's slices staged in
+// shared memory (koff = its first interval, boff = its first bucket).
+__device__ __forceinline__ double mc_tab_u(const PairTab &T, const double *__restrict__ tc,
+                                           const unsigned short *__restrict__ bst, int koff, int boff, double r2)
 {
     int k = 0;
     const float r2f = (float)r2;
     if (r2f < T.fz_hi) {
         int b = (int)((r2f - T.fz_lo) * T.finv_h);
         b = b < 0 ? 0 : (b >= MSG_NBUCKET ? MSG_NBUCKET - 1 : b);
-        k = bst[T.b0 + b];
+        k = bst[T.b0 - boff + b];
     }
-    k += T.k0;
-    while (r2 < tz[k]) ++k;
+    k += T.k0 - koff;
+    // column 0 of a row is its z_low; the walk never leaves the pair's own rows (a pair
+    // below the table minimum would, and the old configuration is not checked for one)
+    const int kend = T.k0 - koff + T.nk - 1;
+    while (k < kend && r2 < tc[(size_t)12 * k]) ++k;
     const double *c = tc + (size_t)12 * k;
     const double d = r2 - c[0];
     return c[1] + d * (c[2] + d * (c[3] + d * (c[4] + d * (c[5] + d * c[6]))));
@@ -77,18 +81,23 @@ __device__ __forceinline__ void mc_block_add(double v, double (*red)[MC_THREADS 
 }
 
 // npass sweeps of one system per block.  Dynamic shared memory: six rows of
-// ncut+1 double2 (new and old exp(i k x) of the moved particle) for standard
-// Ewald systems.
+// wmax double2 (new and old exp(i k x) of the moved particle, standard Ewald), then,
+// when `cache` is set, the system's positions and types, its table rows and its
+// bucket starts, staged once so that the pair differences read shared memory.
+__host__ __device__ inline size_t mc_cache_bytes(int n, int nk, int natat)
+{
+    return ((36 * (size_t)n + 15) / 16) * 16 + 96 * (size_t)nk + 2 * (size_t)natat * MSG_NBUCKET;
+}
+
 __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     const SysDev *__restrict__ sysv, double4 *__restrict__ pos, const int *__restrict__ typ,
     const int *__restrict__ inv, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
-    const double *__restrict__ tz, const double *__restrict__ tc, const unsigned short *__restrict__ bst,
-    const int4 *__restrict__ kv,
+    const double *__restrict__ tc, const unsigned short *__restrict__ bst, const int4 *__restrict__ kv,
     const double *__restrict__ kfac, double2 *__restrict__ sk, double2 *__restrict__ sktm,
     const int *__restrict__ bptr, const int *__restrict__ bpart, const double *__restrict__ bk,
     const double *__restrict__ beq, const int *__restrict__ bpw, const McPar *__restrict__ par,
     const double *__restrict__ dtr, int2 *__restrict__ rng, double *__restrict__ mcu,
-    long long *__restrict__ cnt, int npass)
+    long long *__restrict__ cnt, int npass, int cache, int wmax)
 {
     extern __shared__ double2 etab[];          // [6][ncut+1]: new x, y, z; old x, y, z
     constexpr int NSLOT = 10 + 4;              // type pairs, reciprocal, dipole x, y, z
@@ -106,12 +115,40 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     long long nacc = 0, nhs = 0;
     const double tp = 2.0 * 3.1415926535897932;
     const long long ntrial = (long long)npass * S.n;
+    // where the system's particles and table rows are read from
+    const double4 *P4 = pos;
+    const int *PT = typ;
+    const double *TC = tc;
+    const unsigned short *BS = bst;
+    int poff = 0, koff = 0, boff = 0;
+    double4 *cpos = nullptr;
+    if (cache) {
+        unsigned char *base = reinterpret_cast<unsigned char *>(etab + 6 * wmax);
+        cpos = reinterpret_cast<double4 *>(base);
+        int *ctyp = reinterpret_cast<int *>(cpos + S.n);
+        double *ctc = reinterpret_cast<double *>(base + ((36 * (size_t)S.n + 15) / 16) * 16);
+        unsigned short *cbst = reinterpret_cast<unsigned short *>(ctc + (size_t)12 * S.tab_nk);
+        for (int e = t; e < S.n; e += MC_THREADS) {
+            cpos[e] = pos[S.off + e];
+            ctyp[e] = typ[S.off + e];
+        }
+        for (int e = t; e < 12 * S.tab_nk; e += MC_THREADS) ctc[e] = tc[(size_t)12 * S.tab_k0 + e];
+        for (int e = t; e < S.natat * MSG_NBUCKET; e += MC_THREADS) cbst[e] = bst[S.tab_b0 + e];
+        P4 = cpos;
+        PT = ctyp;
+        TC = ctc;
+        BS = cbst;
+        poff = S.off;
+        koff = S.tab_k0;
+        boff = S.tab_b0;
+        __syncthreads();
+    }
     // Thread 0 sets up a trial: particle, displacement, periodic wrap.
     auto setup = [&](int ipass) {
         int ip = (P.isamp == 0) ? ipass + 1 : 1 + (int)(S.n * mc_random(st));
         ip = max(1, min(ip, S.n)) - 1;
         const int i = inv[S.off + ip];
-        const int ty = typ[i];
+        const int ty = PT[i - poff];
         const double dt = dtr[S.type_off + ty];
         double d[3];
         if (dt >= 0.0) {
@@ -124,7 +161,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
             }
             for (int m = 0; m < 3; ++m) d[m] = __dmul_rn(d[m], fabs(dt));
         }
-        const double4 x = pos[i];
+        const double4 x = P4[i - poff];
         const double xo[3] = {x.x, x.y, x.z};
         for (int m = 0; m < 3; ++m) {
             sro[m] = xo[m];
@@ -166,14 +203,14 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
         double dip0 = 0.0, dip1 = 0.0, dip2 = 0.0;
         bool over = false;
         for (int j = S.off + t; j < S.off + S.n; j += MC_THREADS) {
-            const double4 xj = pos[j];
+            const double4 xj = P4[j - poff];
             if (S.lsurf) {
                 dip0 += xj.w * xj.x;
                 dip1 += xj.w * xj.y;
                 dip2 += xj.w * xj.z;
             }
             if (j == i) continue;
-            const int pg = pair_of(ptmap, S, ty, typ[j]);
+            const int pg = pair_of(ptmap, S, ty, PT[j - poff]);
             const PairTab &T = ptab[pg];
             const int pl = pg - S.pt_off;
             double dx = rt[0] - xj.x, dy = rt[1] - xj.y, dz = rt[2] - xj.z;
@@ -183,13 +220,13 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                 if (r2n < T.r2atat || r2n < T.r2umin)
                     over = true;
                 else
-                    v += mc_tab_u(T, tz, tc, bst, r2n);
+                    v += mc_tab_u(T, TC, BS, koff, boff, r2n);
             }
             dx = r0[0] - xj.x;
             dy = r0[1] - xj.y;
             dz = r0[2] - xj.z;
             const double r2o = pbcr2_exact(dx, dy, dz, S);
-            if (r2o < S.rcut2) v -= mc_tab_u(T, tz, tc, bst, r2o);
+            if (r2o < S.rcut2) v -= mc_tab_u(T, TC, BS, koff, boff, r2o);
 #pragma unroll
             for (int p = 0; p < 10; ++p)
                 if (p == pl) du[p] += v;
@@ -265,7 +302,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                 }
                 const int ip = sip;
                 for (int b = bptr ? bptr[S.off + ip] : 0; bptr && b < bptr[S.off + ip + 1]; ++b) {
-                    const double4 xb = pos[inv[S.off + bpart[b]]];
+                    const double4 xb = P4[inv[S.off + bpart[b]] - poff];
                     double dx = rt[0] - xb.x, dy = rt[1] - xb.y, dz = rt[2] - xb.z;
                     const double r2n = pbcr2_exact(dx, dy, dz, S);
                     dx = r0[0] - xb.x;
@@ -297,11 +334,12 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                     for (int p = 0; p < natat; ++p) u[2 + p] += dtw[p];
                     if (S.lewald) u[12] += durec;
                     u[13] += dubond;
-                    double4 x = pos[i];
+                    double4 x = P4[i - poff];
                     x.x = rt[0];
                     x.y = rt[1];
                     x.z = rt[2];
                     pos[i] = x;
+                    if (cpos) cpos[i - poff] = x;
                 }
             }
             sacc = acc;
