@@ -1985,7 +1985,8 @@ extern "C" int msg_get_linacc(msg_handle *h)
 // Random's first-call state from iseed (Src/mollib.F90:2696-2701).
 static int2 mc_seed_state(int32_t iseed)
 {
-    const int32_t a = iseed < 0 ? -iseed : iseed;
+    // abs(iseed) in two's complement (INT_MIN stays INT_MIN, as a 32-bit abs wraps)
+    const int32_t a = iseed < 0 ? (int32_t)(0u - (uint32_t)iseed) : iseed;
     return make_int2(777755555 ^ a, (888889999 ^ a) | 1);
 }
 

@@ -1263,7 +1263,7 @@ static const double or_am = (1.0 - 5.9604644775390625e-08) * 4.65661287307739257
 
 void or_random_init(int32_t iseed, int32_t state[2])
 {
-    int32_t a = iseed < 0 ? -iseed : iseed;
+    int32_t a = iseed < 0 ? (int32_t)(0u - (uint32_t)iseed) : iseed;   /* abs, wrapping at INT_MIN */
     state[1] = (888889999 ^ a) | 1;          /* iy */
     state[0] = 777755555 ^ a;                /* ix */
 }
