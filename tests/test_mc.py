@@ -131,3 +131,27 @@ def test_spme_is_refused():
     with pytest.raises(MolsimGpuError) as ei:
         g.MCPass(1, [1.0] * s["npt"], 1.0)
     assert ei.value.code == 6
+
+
+def test_zero_sweeps_and_bad_arguments():
+    """npass = 0 returns the current energies (a UTotal) and moves nothing; an isamp
+    other than 0 or 1 and a missing dtran are refused with MSG_ERR_ARG."""
+    import ctypes as C
+
+    from molsim_b200 import _lib
+
+    s = _systems()["std"]
+    t = Hp.oracle_table(s)
+    g = Engine(s, t, precision="fp64")
+    ro0 = g.get_state()["ro"]
+    acc, hs, e = g.MCPass(0, [2.0] * s["npt"], 1.0)
+    assert int(acc[0]) == 0 and int(hs[0]) == 0
+    assert np.array_equal(g.get_state()["ro"], ro0)
+    u = g.UTotal()
+    assert abs(e["utot"] - u["utot"]) <= 1e-12 * abs(u["utot"])
+    with pytest.raises(MolsimGpuError) as ei:
+        g.MCPass(1, [2.0] * s["npt"], 1.0, isamp=2)
+    assert ei.value.code == 6
+    par = (_lib.MsgMcParams * 1)()
+    par[0] = _lib.MsgMcParams(1.0, C.POINTER(C.c_double)(), 0, 0)
+    assert _lib.lib().msg_mc_pass(g.h, 1, par, None, None, 0, None) == 6
