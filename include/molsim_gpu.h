@@ -22,6 +22,7 @@
  *   msg_velver                     -> MDDriver iSimulationStep: VelVer +
  *                                     GetKinEnergy (Src/md.F90:154-168, 252-410)
  *                                     followed by NList (Src/nlist.F90:597-621)
+ *   msg_utwobody_p                 -> UTwoBodyP (Src/energy.F90:786-896), polyatomic particles
  *   msg_mc_seed / msg_mc_pass      -> MCDriver iSimulationStep: MCPass with SPartMove
  *                                     (Src/mc.F90:1470-1755), DUTotal, Metropolis, MCUpdate
  *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
@@ -275,6 +276,23 @@ int  msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen[3], doubl
                           int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
                           const double *r2umin, const double *r2atat, double *force, double *utwob,
                           double *virial, void *stream);
+
+/* UTwoBodyP (Src/energy.F90:786-896): site-site pair energy, forces and virial of
+ * polyatomic particles over MOLSIM's particle list, as UTotal calls it for molecules.
+ * Host arrays in MOLSIM's layout, 1-based indices: ro [np][3] particle positions,
+ * r [na][3] atom positions, iptpn [np] particle type, ianpn [np] first atom of each
+ * particle, napt [npt] atoms per particle type, iatan [na] atom type (nat types),
+ * nneighpn [np] and jpnlist [np][maxnneigh] the particle list; ubuf/iubuflow/r2umin
+ * the atom-type table (natat = nat(nat+1)/2 pairs).  A pair interacts when its centres
+ * are within rcut after PBC2's box shift (box cell).  Out: force [na][3] (kJ/(mol A),
+ * overwritten), utwob [npt(npt+1)/2 + 1] = u%twob(0:nptpt) by particle-type pair,
+ * virial [1]; kernel_ms (optional): device time of the computation.
+ * MSG_ERR_TABLE_MIN for an atom pair below r2umin (StopUTwoBodyP). */
+int  msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3], double rcut,
+                    const double *ro, const double *r, const int32_t *iptpn, const int32_t *ianpn,
+                    const int32_t *napt, const int32_t *iatan, const int32_t *nneighpn, const int32_t *jpnlist,
+                    int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
+                    const double *r2umin, double *force, double *utwob, double *virial, float *kernel_ms);
 
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 LIB = os.path.join(HERE, "libmolsim_gpu.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "noalloc.cu", "setup.cpp")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "noalloc.cu", "polyatomic.cu", "setup.cpp")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "molsim_gpu.h")]
 

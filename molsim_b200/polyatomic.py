@@ -1,0 +1,42 @@
+"""Polyatomic particles: UTwoBodyP (Src/energy.F90:786-896) on the GPU through the C-ABI
+(msg_utwobody_p).  The caller's arrays follow MOLSIM's layout (see
+systems.rigid_molecules); the atom-type table comes from engine.pot_tab."""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .engine import MolsimGpuError
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def utwobody_p(s, table):
+    """Site-site pair energy, forces and virial of polyatomic system s with its atom-type table.
+    Returns dict(force [na][3], utwob [nptpt+1] = u%twob(0:nptpt), virial, kernel_ms)."""
+    k = {}
+    for key, dt in (("ro", np.float64), ("r", np.float64), ("iptpn", np.int32), ("ianpn", np.int32),
+                    ("napt", np.int32), ("iatan", np.int32), ("nneighpn", np.int32), ("jpnlist", np.int32)):
+        k[key] = np.ascontiguousarray(s[key], dt)
+    k["ubuf"] = np.ascontiguousarray(table["ubuf"], np.float64)
+    k["iubuflow"] = np.ascontiguousarray(table["iubuflow"], np.int32)
+    k["r2umin"] = np.ascontiguousarray(table["r2umin"], np.float64)
+    na, npt = int(s["na"]), int(s["npt"])
+    force = np.zeros((na, 3))
+    utwob = np.zeros(npt * (npt + 1) // 2 + 1)
+    vir = C.c_double()
+    ms = C.c_float()
+    box = (C.c_double * 3)(*s["boxlen"])
+    i32 = C.c_int32
+    rc = _lib.lib().msg_utwobody_p(int(s["np"]), na, npt, int(s["nat"]), box, float(s["rcut"]),
+                                   _p(k["ro"], C.c_double), _p(k["r"], C.c_double), _p(k["iptpn"], i32),
+                                   _p(k["ianpn"], i32), _p(k["napt"], i32), _p(k["iatan"], i32),
+                                   _p(k["nneighpn"], i32), _p(k["jpnlist"], i32), int(k["jpnlist"].shape[1]),
+                                   _p(k["ubuf"], C.c_double), len(k["ubuf"]), _p(k["iubuflow"], i32),
+                                   _p(k["r2umin"], C.c_double), _p(force, C.c_double), _p(utwob, C.c_double),
+                                   C.byref(vir), C.byref(ms))
+    if rc:
+        raise MolsimGpuError(rc, "msg_utwobody_p")
+    return dict(force=force, utwob=utwob, virial=vir.value, kernel_ms=ms.value)

@@ -268,3 +268,76 @@ def _grid_for(L, spacing=3.9):
         if L / g <= spacing:
             return g
     return 128
+
+
+def _random_rotations(rng, n):
+    """n uniformly random rotation matrices (from normalised random quaternions)."""
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+        np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+        np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+def particle_list(ro, box, rlist):
+    """MOLSIM's particle list over positions ro (SetVListMD's rule, Src/nlist.F90:724-759):
+    every pair within rlist stored once, in row ip (1-based) when (ip < jp and ip + jp odd)
+    or (ip > jp and ip + jp even).  Returns nneighpn [np], jpnlist [np][maxnneigh] (1-based)."""
+    from scipy.spatial import cKDTree
+
+    L = float(box)
+    t = cKDTree(np.mod(np.asarray(ro) + L / 2, L), boxsize=L)
+    pairs = t.query_pairs(rlist, output_type="ndarray")
+    n = len(ro)
+    rows = [[] for _ in range(n)]
+    for a, b in pairs:
+        ip, jp = int(a) + 1, int(b) + 1
+        lo, hi = min(ip, jp), max(ip, jp)
+        own = lo if (lo + hi) % 2 == 1 else hi
+        rows[own - 1].append(hi if own == lo else lo)
+    maxn = max(1, max(len(r) for r in rows))
+    nn = np.array([len(r) for r in rows], np.int32)
+    jp = np.zeros((n, maxn), np.int32)
+    for i, r in enumerate(rows):
+        jp[i, :len(r)] = sorted(r)
+    return nn, jp
+
+
+def rigid_molecules(seed=0, nmol=400, nsolute=200, L=50.0, rcut=12.0, drnlist=1.0, temp=298.0, relp=78.4):
+    """Polyatomic test system for UTwoBodyP: rigid three-site molecules (particle type 1:
+    an A site at the centre and two B sites 1 A away, 109.47 degrees apart; charges -0.8,
+    +0.4, +0.4) and one-site solutes (particle type 2: a neutral C site), random
+    orientations, centres uniform without overlap.  Atom types A, B, C carry the (1,6,12)
+    parameters of the site-site table.  Returns the particle and atom arrays in MOLSIM's
+    layout (1-based) with the particle list."""
+    rng = np.random.default_rng(seed)
+    npart = nmol + nsolute
+    ro = place_uniform(rng, npart, L, 4.0)
+    ang = np.deg2rad(109.47)
+    frame = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [np.cos(ang), np.sin(ang), 0.0]])
+    rot = _random_rotations(rng, nmol)
+    r_mol = ro[:nmol, None, :] + np.einsum("nij,kj->nki", rot, frame)
+    r = np.concatenate([r_mol.reshape(-1, 3), ro[nmol:]])
+    iptpn = np.array([1] * nmol + [2] * nsolute, np.int32)
+    napt = np.array([3, 1], np.int32)
+    ianpn = np.concatenate([1 + 3 * np.arange(nmol), 1 + 3 * nmol + np.arange(nsolute)]).astype(np.int32)
+    iatan = np.array([1, 2, 2] * nmol + [3] * nsolute, np.int32)
+    s = dict(np=npart, na=len(r), npt=2, nat=3, boxlen=[float(L)] * 3, rcut=float(rcut), drnlist=float(drnlist),
+             temp=float(temp), relpermitt=float(relp), epsi_four_pi=EPSI0_FOUR_PI / relp, ro=ro, r=r, iptpn=iptpn,
+             napt=napt, ianpn=ianpn, iatan=iatan, zat=np.array([-0.8, 0.4, 0.0]), sigat=np.array([3.0, 1.0, 4.0]),
+             epsat=np.array([0.6, 0.05, 0.5]) * kT(temp), lewald=False, lljcut=False, **POT_DEFAULTS)
+    s["nneighpn"], s["jpnlist"] = particle_list(ro, L, rcut + drnlist)
+    s["name"] = "rigid_molecules_%d" % npart
+    return s
+
+
+def site_table_params(s):
+    """Parameters of the site-site (atom-type) table of a rigid_molecules system: the table
+    reaches past rcut by the largest site distance from a centre (twice), as MOLSIM's
+    rumax = 1.1 (rcut + racom) does."""
+    d = dict(s)
+    d["npt"] = s["nat"]
+    d["rcut"] = s["rcut"] + 2.0
+    return d

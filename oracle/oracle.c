@@ -1539,3 +1539,79 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
     free(stm); free(yzt);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Polyatomic particles: UTwoBodyP                                     */
+/* ------------------------------------------------------------------ */
+
+/* UTwoBodyP, Src/energy.F90:786-896 (box cell), with PBC2 (Src/molaux.F90:193-210):
+ * the particle list decides the pairs (particle centres within rcut), every site
+ * pair of the two particles interacts through the atom-type table with the centres'
+ * periodic shift.  1-based MOLSIM arrays; force [na][3] is overwritten (kJ/(mol A)),
+ * utwob [nptpt+1] = u%twob(0:nptpt) by particle-type pair, *virial the pair virial.
+ * Returns 1 when an atom pair lies below r2umin (StopUTwoBodyP), 2 on a table overrun. */
+int or_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3], double rcut,
+                  const double *ro, const double *r, const int32_t *iptpn, const int32_t *ianpn,
+                  const int32_t *napt, const int32_t *iatan, const int32_t *nneighpn, const int32_t *jpnlist,
+                  int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
+                  const double *r2umin, double *force, double *utwob, double *virial)
+{
+    const double rcut2 = rcut * rcut;
+    const int nptpt = npt * (npt + 1) / 2;
+    double half[3], vir = 0.0;
+    int ip, m, k;
+    for (m = 0; m < 3; ++m) half[m] = boxlen[m] / 2.0;
+    for (k = 0; k < 3 * na; ++k) force[k] = 0.0;
+    for (k = 0; k <= nptpt; ++k) utwob[k] = 0.0;
+    for (ip = 0; ip < np; ++ip) {
+        const int ipt = iptpn[ip], ialow = ianpn[ip] - 1, iaupp = ialow + napt[ipt - 1] - 1;
+        int jploc;
+        for (jploc = 0; jploc < nneighpn[ip]; ++jploc) {
+            const int jp = jpnlist[(size_t)ip * maxnneigh + jploc] - 1;
+            const int jpt = iptpn[jp], iptjpt = pair_index(npt, ipt, jpt);
+            const int jalow = ianpn[jp] - 1, jaupp = jalow + napt[jpt - 1] - 1;
+            double d[3], sh[3], r2, usum = 0.0;
+            int ia, ja;
+            for (m = 0; m < 3; ++m) {
+                d[m] = ro[3 * ip + m] - ro[3 * jp + m];
+                sh[m] = fabs(d[m]) > half[m] ? copysign(boxlen[m], d[m]) : 0.0;   /* PBC2 */
+                d[m] = d[m] - sh[m];
+            }
+            r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            if (r2 > rcut2) continue;
+            for (ia = ialow; ia <= iaupp; ++ia) {
+                const int iat = iatan[ia];
+                for (ja = jalow; ja <= jaupp; ++ja) {
+                    const int jat = iatan[ja], iatjat = pair_index(nat, iat, jat);
+                    double dx = r[3 * ia] - r[3 * ja] - sh[0];
+                    double dy = r[3 * ia + 1] - r[3 * ja + 1] - sh[1];
+                    double dz = r[3 * ia + 2] - r[3 * ja + 2] - sh[2];
+                    double a2 = dx * dx + dy * dy + dz * dz, dd, fsum;
+                    int ibuf;
+                    if (a2 < r2umin[iatjat - 1]) return 1;
+                    ibuf = iubuflow[iatjat - 1] - 1;
+                    while (a2 < ubuf[ibuf]) {
+                        ibuf += 12;
+                        if (ibuf + 12 > nbuf) return 2;
+                    }
+                    dd = a2 - ubuf[ibuf];
+                    usum = usum + ubuf[ibuf + 1] + dd * (ubuf[ibuf + 2] + dd * (ubuf[ibuf + 3] +
+                           dd * (ubuf[ibuf + 4] + dd * (ubuf[ibuf + 5] + dd * ubuf[ibuf + 6]))));
+                    fsum = ubuf[ibuf + 7] + dd * (ubuf[ibuf + 8] + dd * (ubuf[ibuf + 9] +
+                           dd * (ubuf[ibuf + 10] + dd * ubuf[ibuf + 11])));
+                    force[3 * ia] += fsum * dx;
+                    force[3 * ia + 1] += fsum * dy;
+                    force[3 * ia + 2] += fsum * dz;
+                    force[3 * ja] -= fsum * dx;
+                    force[3 * ja + 1] -= fsum * dy;
+                    force[3 * ja + 2] -= fsum * dz;
+                    vir = vir - fsum * a2;
+                }
+            }
+            utwob[iptjpt] = utwob[iptjpt] + usum;
+        }
+    }
+    for (k = 1; k <= nptpt; ++k) utwob[0] += utwob[k];
+    *virial = vir;
+    return 0;
+}

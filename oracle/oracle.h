@@ -154,6 +154,17 @@ void   or_mc_seed(or_sys *s, int32_t iseed);
 int    or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta, double *u,
                   int64_t *accepted, int64_t *hsreject);
 
+/* ---- polyatomic particles ---- */
+/* UTwoBodyP (Src/energy.F90:786-896): site-site pair energy, forces and virial over the
+ * particle list; 1-based MOLSIM arrays; force [na][3] overwritten, utwob [nptpt+1],
+ * virial [1].  Returns 1 for an atom pair below r2umin, 2 for a table overrun. */
+int    or_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3], double rcut,
+                     const double *ro, const double *r, const int32_t *iptpn, const int32_t *ianpn,
+                     const int32_t *napt, const int32_t *iatan, const int32_t *nneighpn,
+                     const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                     const int32_t *iubuflow, const double *r2umin, double *force, double *utwob,
+                     double *virial);
+
 #ifdef __cplusplus
 }
 #endif

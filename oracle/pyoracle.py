@@ -59,6 +59,9 @@ def lib():
         L.or_mc_pass.restype = C.c_int
         L.or_mc_pass.argtypes = [C.c_void_p, C.c_int, C.c_int, f64p, C.c_double, f64p,
                                  C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.or_utwobody_p.restype = C.c_int
+        L.or_utwobody_p.argtypes = [C.c_int32] * 4 + [f64p, C.c_double, f64p, f64p] + [i32p] * 6 + \
+            [C.c_int32, f64p, C.c_int32, i32p, f64p, f64p, f64p, f64p]
         L.or_alpha_to_ncut.restype = C.c_int32
         L.or_alpha_to_ncut.argtypes = [C.c_double] * 5 + [i32p]
         L.or_ewald_error_ureal.restype = C.c_double
@@ -332,6 +335,32 @@ class System:
         m2 = C.c_double()
         r = lib().or_skin_test(self.h, _p(d, C.c_double), C.byref(m1), C.byref(m2))
         return bool(r), m1.value, m2.value
+
+
+def utwobody_p(s, table):
+    """UTwoBodyP (oracle) for a polyatomic system dict (molsim_b200.systems.rigid_molecules
+    layout) and its atom-type table.  Returns dict(force, utwob, virial)."""
+    k = {}
+    for key, dt in (("ro", np.float64), ("r", np.float64), ("iptpn", np.int32), ("ianpn", np.int32),
+                    ("napt", np.int32), ("iatan", np.int32), ("nneighpn", np.int32), ("jpnlist", np.int32)):
+        k[key] = np.ascontiguousarray(s[key], dt)
+    ub = np.ascontiguousarray(table["ubuf"], np.float64)
+    iub = np.ascontiguousarray(table["iubuflow"], np.int32)
+    r2 = np.ascontiguousarray(table["r2umin"], np.float64)
+    na, npt = int(s["na"]), int(s["npt"])
+    force = np.zeros((na, 3))
+    utwob = np.zeros(npt * (npt + 1) // 2 + 1)
+    vir = C.c_double()
+    box = (C.c_double * 3)(*s["boxlen"])
+    rc = lib().or_utwobody_p(int(s["np"]), na, npt, int(s["nat"]), box, float(s["rcut"]),
+                             _p(k["ro"], C.c_double), _p(k["r"], C.c_double), _p(k["iptpn"], C.c_int32),
+                             _p(k["ianpn"], C.c_int32), _p(k["napt"], C.c_int32), _p(k["iatan"], C.c_int32),
+                             _p(k["nneighpn"], C.c_int32), _p(k["jpnlist"], C.c_int32), int(k["jpnlist"].shape[1]),
+                             _p(ub, C.c_double), len(ub), _p(iub, C.c_int32), _p(r2, C.c_double),
+                             _p(force, C.c_double), _p(utwob, C.c_double), C.byref(vir))
+    if rc:
+        raise RuntimeError("UTwoBodyP failed: %d" % rc)
+    return dict(force=force, utwob=utwob, virial=vir.value)
 
 
 def random_stream(iseed, n):

@@ -90,3 +90,18 @@ def config2():
     s = S.colloid_bd(seed=0)
     s["bd_fac"] = S.bd_factors(s)
     return s
+
+
+def site_table(s):
+    """The atom-type (site-site) table of a polyatomic system from the oracle."""
+    d = S.site_table_params(s)
+    pot = dict(npt=d["npt"], zat=d["zat"], sigat=d["sigat"], epsat=d["epsat"], rcut=d["rcut"], ualpha=0.0,
+               epsi_four_pi=d["epsi_four_pi"], lewald=0, lljcut=int(d["lljcut"]),
+               **{k: d[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab",
+                                    "fmaxtab", "rumaxfac")})
+    return O.pot_tab(pot)
+
+
+@functools.lru_cache(maxsize=None)
+def rigid_small():
+    return S.rigid_molecules(seed=2, nmol=150, nsolute=60, L=30.0, rcut=10.0)
