@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--serve-wait", type=float, default=0.0,
                     help="serving: batching window in seconds before a cohort forms")
     ap.add_argument("--serve-ahead", type=int, default=2, help="serving: step chunks enqueued per cohort")
+    ap.add_argument("--poly", type=int, default=1,
+                    help="time UTwoBodyP on 50000 rigid molecules and solutes (0: skip)")
     ap.add_argument("--mc", type=int, default=1,
                     help="time Monte Carlo sweeps of the 1000-ion electrolyte, one chain and an ensemble (0: skip)")
     ap.add_argument("--ewald-std", type=int, default=1,
@@ -494,6 +496,51 @@ def run_mc(a):
     return out
 
 
+def run_poly(a):
+    """UTwoBodyP (polyatomic particles) on 40000 rigid three-site molecules and 10000 one-site
+    solutes (L = 185 A, rc = 10 A): the device time of the site-site pair computation, the whole
+    call (host arrays in and out), and the oracle on one host core."""
+    import numpy as np
+
+    from molsim_b200 import systems as S
+    from molsim_b200.engine import pot_tab
+    from molsim_b200.polyatomic import utwobody_p
+
+    s = S.rigid_molecules(seed=0, nmol=40000, nsolute=10000, L=185.0, rcut=10.0)
+    d = S.site_table_params(s)
+    t = pot_tab(d, 0.0)
+    # site pairs of the particle pairs within rcut
+    ro = np.asarray(s["ro"])
+    npairs = 0
+    napt = np.asarray(s["napt"])
+    ipt = np.asarray(s["iptpn"]) - 1
+    L = s["boxlen"][0]
+    for i in range(s["np"]):
+        js = s["jpnlist"][i, :s["nneighpn"][i]] - 1
+        dd = ro[i] - ro[js]
+        dd -= L * np.round(dd / L)
+        ok = (dd * dd).sum(1) <= s["rcut"] ** 2
+        npairs += int((napt[ipt[i]] * napt[ipt[js[ok]]]).sum())
+    utwobody_p(s, t)                                  # warm-up
+    reps = 5
+    kms, t0 = [], time.perf_counter()
+    for _ in range(reps):
+        kms.append(utwobody_p(s, t)["kernel_ms"])
+    call_ms = (time.perf_counter() - t0) / reps * 1000.0
+    out = {"workload": "40000 rigid 3-site molecules + 10000 solutes, L = 185 A, rc = 10 A",
+           "site_pairs": npairs, "kernel_ms": float(np.median(kms)), "call_ms": call_ms,
+           "site_pairs_per_s": npairs / (float(np.median(kms)) / 1000.0), "unit": "site pairs/s"}
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        t0 = time.perf_counter()
+        O.utwobody_p(s, t)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": npairs / cpu_s, "unit": "site pairs/s", "cores": 1, "kind": "port",
+                               "sample": "one UTwoBodyP evaluation of the same system, oracle, 1 thread"}
+    return out
+
+
 def run_serving(a):
     """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
     half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
@@ -692,13 +739,15 @@ def run_gpu(a):
                "sample": "%d velocity-Verlet steps of the same 16000-particle polyelectrolyte, "
                          "oracle (FP64 C restatement of MOLSIM's serial path, -O2), 1 thread" % cpu_steps}
 
-    ensemble = serving = bd = ewstd = mc = None
+    ensemble = serving = bd = ewstd = mc = poly = None
     if rank == 0 and world == 1 and a.bd:
         bd = run_bd(a, flush)
     if rank == 0 and world == 1 and a.ewald_std:
         ewstd = run_ewald_std(a, flush)
     if rank == 0 and world == 1 and a.mc:
         mc = run_mc(a)
+    if rank == 0 and world == 1 and a.poly:
+        poly = run_poly(a)
     if rank == 0 and world == 1 and a.ensemble > 0:
         ensemble = run_ensemble(a, flush)
     if rank == 0 and world == 1 and a.serve_jobs > 0:
@@ -718,7 +767,7 @@ def run_gpu(a):
                        "l2": "flushed before every timed step (256 MB write, then 256 MB read)",
                        "rebuilds_in_timed_steps": int(rebuilds), "pair_kernel": tuned},
             "fp64_value": fp64_value, "batched": batched, "ensemble": ensemble, "serving": serving,
-            "bd_200k": bd, "ewald_std_1000": ewstd, "mc_1000": mc,
+            "bd_200k": bd, "ewald_std_1000": ewstd, "mc_1000": mc, "utwobody_p_50000": poly,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 3 * 24 * n,
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
