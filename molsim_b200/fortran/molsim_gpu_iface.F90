@@ -120,6 +120,20 @@ module MolsimGpu
          type(c_ptr), value        :: ro, rod, rodd, e   ! (3,np) real(8) each; e: msg_energy(nsteps) or c_null_ptr
       end function msg_velver_host
 
+      integer(c_int) function msg_utwobody_p(np, na, npt, nat, boxlen, rcut, ro, r, iptpn, ianpn, napt, iatan, &
+            nneighpn, jpnlist, maxnneigh, ubuf, nbuf, iubuflow, r2umin, force, utwob, virial, kernel_ms) &
+            bind(c, name='msg_utwobody_p')
+         import :: c_int, c_int32_t, c_double, c_ptr
+         integer(c_int32_t), value :: np, na, npt, nat
+         real(c_double), intent(in) :: boxlen(3)
+         real(c_double), value     :: rcut
+         type(c_ptr), value        :: ro, r, iptpn, ianpn, napt, iatan, nneighpn, jpnlist
+         integer(c_int32_t), value :: maxnneigh
+         type(c_ptr), value        :: ubuf
+         integer(c_int32_t), value :: nbuf
+         type(c_ptr), value        :: iubuflow, r2umin, force, utwob, virial, kernel_ms
+      end function msg_utwobody_p
+
       integer(c_int) function msg_mc_seed(h, isys, iseed) bind(c, name='msg_mc_seed')
          import :: c_int, c_int32_t, c_ptr
          type(c_ptr), value        :: h
