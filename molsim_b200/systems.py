@@ -341,3 +341,57 @@ def site_table_params(s):
     d["npt"] = s["nat"]
     d["rcut"] = s["rcut"] + 2.0
     return d
+
+
+def qua_to_ori(q):
+    """QuaToOri (Src/mollib.F90:2221-2255) for quaternions q [n][4]: ori [n][3][3], which takes
+    a particle's principal-frame vectors to the lab frame."""
+    q = np.asarray(q, np.float64)
+    q0, q1, q2, q3 = q.T
+    o = np.empty((len(q), 3, 3))
+    o[:, 0, 0] = -q2 * q2 + q1 * q1 - q3 * q3 + q0 * q0
+    o[:, 1, 0] = 2 * (q0 * q3 - q1 * q2)
+    o[:, 2, 0] = 2 * (q1 * q3 + q0 * q2)
+    o[:, 0, 1] = -2 * (q1 * q2 + q0 * q3)
+    o[:, 1, 1] = q2 * q2 - q1 * q1 - q3 * q3 + q0 * q0
+    o[:, 2, 1] = 2 * (q0 * q1 - q2 * q3)
+    o[:, 0, 2] = 2 * (q1 * q3 - q0 * q2)
+    o[:, 1, 2] = -2 * (q2 * q3 + q0 * q1)
+    o[:, 2, 2] = -q2 * q2 - q1 * q1 + q3 * q3 + q0 * q0
+    return o
+
+
+def rigid_bodies(seed=0, nmol=300, nsolute=100, L=40.0, rcut=10.0, drnlist=1.5, temp=298.0, relp=78.4,
+                 tstep=0.001):
+    """Rigid-body MD test system: three-site molecules (an O-like site of mass 16 and two H-like
+    sites of mass 1, 1 A bonds at 109.47 degrees; charges -0.8, +0.4, +0.4) and one-site solutes
+    (mass 23, neutral), with centres of mass, principal frames (sites `ra` in them, masses and
+    principal moments `momp` per particle type), random orientations (quaternions `qua`) and
+    Maxwell-Boltzmann centre velocities; quaternion velocities and accelerations start at zero.
+    The site positions r = ro + ori(qua) ra and the particle list are included."""
+    rng = np.random.default_rng(seed)
+    s = rigid_molecules(seed=seed, nmol=nmol, nsolute=nsolute, L=L, rcut=rcut, drnlist=drnlist, temp=temp,
+                        relp=relp)
+    ang = np.deg2rad(109.47)
+    sites = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [np.cos(ang), np.sin(ang), 0.0]])
+    m = np.array([16.0, 1.0, 1.0])
+    com = (m[:, None] * sites).sum(0) / m.sum()
+    x = sites - com
+    inertia = (m[:, None, None] * ((x * x).sum(1)[:, None, None] * np.eye(3) - x[:, :, None] * x[:, None, :])).sum(0)
+    mom, axes = np.linalg.eigh(inertia)
+    ra = np.zeros((2, 3, 3))
+    ra[0] = x @ axes                                   # principal-frame sites
+    momp = np.array([mom, [1.0, 1.0, 1.0]])            # a one-site solute: no torque, any moment
+    masspt = np.array([m.sum(), 23.0])
+    q = rng.standard_normal((s["np"], 4))
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    ori = qua_to_ori(q)
+    ro = np.asarray(s["ro"])
+    ipt = np.asarray(s["iptpn"]) - 1
+    r = np.concatenate([(ro[:nmol, None, :] + np.einsum("nij,kj->nki", ori[:nmol], ra[0])).reshape(-1, 3),
+                        ro[nmol:]])
+    s.update(ra=ra, maxsite=3, masspt=masspt, momp=momp, qua=q, quad=np.zeros_like(q), quadd=np.zeros_like(q),
+             r=r, rod=maxwell_velocities(rng, masspt[ipt], temp), rodd=np.zeros((s["np"], 3)), tstep=float(tstep),
+             nvvite=2, tvvite=0.0)
+    s["name"] = "rigid_bodies_%d" % s["np"]
+    return s

@@ -1615,3 +1615,169 @@ int or_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, const double
     *virial = vir;
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Rigid polyatomic particles: VelVer with lpolyatom                   */
+/* ------------------------------------------------------------------ */
+
+/* QuaToOri, Src/mollib.F90:2221-2255: ori[3][3] (row i, column j) of one quaternion */
+static void qua_to_ori(const double *q, double *o)
+{
+    const double q00 = q[0] * q[0], q11 = q[1] * q[1], q22 = q[2] * q[2], q33 = q[3] * q[3];
+    const double q01 = q[0] * q[1], q02 = q[0] * q[2], q03 = q[0] * q[3];
+    const double q12 = q[1] * q[2], q13 = q[1] * q[3], q23 = q[2] * q[3];
+    o[0] = -q22 + q11 - q33 + q00;          /* ori(1,1) */
+    o[3] = 2.0 * (q03 - q12);               /* ori(2,1) */
+    o[6] = 2.0 * (q13 + q02);               /* ori(3,1) */
+    o[1] = -2.0 * (q12 + q03);              /* ori(1,2) */
+    o[4] = q22 - q11 - q33 + q00;           /* ori(2,2) */
+    o[7] = 2.0 * (q01 - q23);               /* ori(3,2) */
+    o[2] = 2.0 * (q13 - q02);               /* ori(1,3) */
+    o[5] = -2.0 * (q23 + q01);              /* ori(2,3) */
+    o[8] = -q22 - q11 + q33 + q00;          /* ori(3,3) */
+}
+
+/* QuaNorm, Src/mollib.F90:2594-2612 */
+static void qua_norm(double *q)
+{
+    const double norm = 1.0 / sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    int k;
+    for (k = 0; k < 4; ++k) q[k] = q[k] * norm;
+}
+
+/* QuaVelToAngVel, Src/mollib.F90:2651-2669 */
+static void qua_vel_to_ang_vel(const double *q, const double *qd, double *w)
+{
+    w[0] = 2.0 * (-q[3] * qd[2] + q[0] * qd[1] + q[2] * qd[3] - q[1] * qd[0]);
+    w[1] = 2.0 * (-q[0] * qd[2] - q[3] * qd[1] + q[1] * qd[3] + q[2] * qd[0]);
+    w[2] = 2.0 * (+q[1] * qd[2] - q[2] * qd[1] + q[0] * qd[3] - q[3] * qd[0]);
+}
+
+/* GetAngAcc, Src/md.F90:628-663: quaternion acceleration from the lab-frame torque */
+static void get_ang_acc(const double *tor, const double *o, const double *w, const double *momp,
+                        const double *q, const double *qd, double *qdd)
+{
+    const double t1 = tor[0] * o[0] + tor[1] * o[3] + tor[2] * o[6];
+    const double t2 = tor[0] * o[1] + tor[1] * o[4] + tor[2] * o[7];
+    const double t3 = tor[0] * o[2] + tor[1] * o[5] + tor[2] * o[8];
+    const double a1 = (t1 + w[1] * w[2] * (momp[1] - momp[2])) * (1.0 / momp[0]);
+    const double a2 = (t2 + w[2] * w[0] * (momp[2] - momp[0])) * (1.0 / momp[1]);
+    const double a3 = (t3 + w[0] * w[1] * (momp[0] - momp[1])) * (1.0 / momp[2]);
+    const double fac = -2.0 * (qd[2] * qd[2] + qd[1] * qd[1] + qd[3] * qd[3] + qd[0] * qd[0]);
+    qdd[0] = 0.5 * (-q[1] * a1 + q[2] * a2 - q[3] * a3 + q[0] * fac);
+    qdd[1] = 0.5 * (+q[0] * a1 - q[3] * a2 - q[2] * a3 + q[1] * fac);
+    qdd[2] = 0.5 * (-q[3] * a1 - q[0] * a2 + q[1] * a3 + q[2] * fac);
+    qdd[3] = 0.5 * (+q[2] * a1 + q[1] * a2 + q[0] * a3 + q[3] * fac);
+}
+
+/* SetAtomPos (ra), Src/molaux.F90:526-545: r = ro + ori ra for the sites of every particle */
+static void set_atom_pos(int32_t np, const double *ro, const double *ori, const int32_t *iptpn,
+                         const int32_t *ianpn, const int32_t *napt, const double *ra, int32_t maxsite, double *r)
+{
+    int ip, a, m;
+    for (ip = 0; ip < np; ++ip) {
+        const int ipt = iptpn[ip] - 1, ia0 = ianpn[ip] - 1;
+        const double *o = ori + 9 * (size_t)ip;
+        for (a = 0; a < napt[ipt]; ++a) {
+            const double *x = ra + 3 * ((size_t)ipt * maxsite + a);
+            for (m = 0; m < 3; ++m)
+                r[3 * (size_t)(ia0 + a) + m] = ro[3 * ip + m] + o[3 * m] * x[0] + o[3 * m + 1] * x[1] + o[3 * m + 2] * x[2];
+        }
+    }
+}
+
+/* Forces, torques and the molecular virial of UTotal, Src/energy.F90:403-426 (no site
+ * torques): force (kJ/(mol A)) is converted in place; forceo/torqueo per particle. */
+static double rigid_forces(int32_t np, const double *ro, const double *r, const int32_t *iptpn, const int32_t *ianpn,
+                           const int32_t *napt, double *force, double *forceo, double *torqueo)
+{
+    const double fac = (sclene / scllen) / sclfor();
+    double virmol = 0.0;
+    int ip, a;
+    for (ip = 0; ip < np; ++ip) {
+        const int ia0 = ianpn[ip] - 1, nat_ = napt[iptpn[ip] - 1];
+        double *fo = forceo + 3 * (size_t)ip, *to = torqueo + 3 * (size_t)ip;
+        fo[0] = fo[1] = fo[2] = to[0] = to[1] = to[2] = 0.0;
+        for (a = 0; a < nat_; ++a) {
+            double *f = force + 3 * (size_t)(ia0 + a);
+            const double dx = r[3 * (size_t)(ia0 + a)] - ro[3 * ip];
+            const double dy = r[3 * (size_t)(ia0 + a) + 1] - ro[3 * ip + 1];
+            const double dz = r[3 * (size_t)(ia0 + a) + 2] - ro[3 * ip + 2];
+            virmol = virmol + dx * f[0] + dy * f[1] + dz * f[2];
+            f[0] = f[0] * fac;
+            f[1] = f[1] * fac;
+            f[2] = f[2] * fac;
+            fo[0] = fo[0] + f[0];
+            fo[1] = fo[1] + f[1];
+            fo[2] = fo[2] + f[2];
+            to[0] = to[0] + dy * f[2] - dz * f[1];
+            to[1] = to[1] + dz * f[0] - dx * f[2];
+            to[2] = to[2] + dx * f[1] - dy * f[0];
+        }
+    }
+    return virmol;
+}
+
+/* nsteps of VelVer for rigid polyatomic particles, Src/md.F90:252-410 (lpolyatom, the
+ * particle list held fixed): linear and quaternion position update, QuaNorm, QuaToOri,
+ * PBC of the centres, SetAtomPos, UTotal's pair part (UTwoBodyP) with forces, torques
+ * and the molecular virial, GetLinAcc and the linear half-kick, then the quaternion
+ * velocities by nvvite iterations of QuaVelToAngVel + GetAngAcc (tvvite's trial step).
+ * State arrays (MOLSIM layout) are advanced in place; ra [npt][maxsite][3] are the
+ * sites in the principal frame, masspt [npt] and momp [npt][3] the particle masses and
+ * principal moments.  Energies and virial of the last step.  Returns UTwoBodyP's status. */
+int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod, double *rodd,
+                double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn, const int32_t *ianpn,
+                const int32_t *napt, const int32_t *iatan, const double *ra, int32_t maxsite, const double *masspt,
+                const double *momp, const int32_t *nneighpn, const int32_t *jpnlist, int32_t maxnneigh,
+                const double *ubuf, int32_t nbuf, const int32_t *iubuflow, const double *r2umin, double *utwob,
+                double *virial)
+{
+    const double fac = 0.5 * tstep * tstep;
+    double *ori = malloc(sizeof(double) * 9 * (size_t)np), *force = malloc(sizeof(double) * 3 * (size_t)na);
+    double *forceo = malloc(sizeof(double) * 3 * (size_t)np), *torqueo = malloc(sizeof(double) * 3 * (size_t)np);
+    double half[3];
+    int step, ip, m, k, it, rc = 0;
+    for (m = 0; m < 3; ++m) half[m] = boxlen[m] / 2.0;
+    for (step = 0; step < nsteps && !rc; ++step) {
+        double vpair = 0.0;
+        for (ip = 0; ip < np; ++ip) {
+            for (m = 0; m < 3; ++m) {
+                const double d = tstep * rod[3 * ip + m] + fac * rodd[3 * ip + m];
+                ro[3 * ip + m] = pbc1(ro[3 * ip + m] + d, half[m], boxlen[m], 1.0 / boxlen[m]);
+            }
+            for (k = 0; k < 4; ++k) qua[4 * ip + k] = qua[4 * ip + k] + tstep * quad[4 * ip + k] + fac * quadd[4 * ip + k];
+            qua_norm(qua + 4 * ip);
+            qua_to_ori(qua + 4 * ip, ori + 9 * (size_t)ip);
+        }
+        set_atom_pos(np, ro, ori, iptpn, ianpn, napt, ra, maxsite, r);
+        rc = or_utwobody_p(np, na, npt, nat, boxlen, rcut, ro, r, iptpn, ianpn, napt, iatan, nneighpn, jpnlist,
+                           maxnneigh, ubuf, nbuf, iubuflow, r2umin, force, utwob, &vpair);
+        if (rc) break;
+        *virial = vpair + rigid_forces(np, ro, r, iptpn, ianpn, napt, force, forceo, torqueo);
+        for (ip = 0; ip < np; ++ip) {
+            const int ipt = iptpn[ip] - 1;
+            const double mi = 1.0 / masspt[ipt];
+            double qdo[4], qddo[4], w[3];
+            for (m = 0; m < 3; ++m) {                         /* GetLinAcc and the half-kick */
+                const double ao = rodd[3 * ip + m];
+                rodd[3 * ip + m] = forceo[3 * ip + m] * mi;
+                rod[3 * ip + m] = rod[3 * ip + m] + 0.5 * tstep * (rodd[3 * ip + m] + ao);
+            }
+            for (k = 0; k < 4; ++k) {
+                qddo[k] = quadd[4 * ip + k];
+                qdo[k] = quad[4 * ip + k];
+                quad[4 * ip + k] = qdo[k] + (tvvite * tstep) * qddo[k];
+            }
+            for (it = 0; it < nvvite; ++it) {
+                qua_vel_to_ang_vel(qua + 4 * ip, quad + 4 * ip, w);
+                get_ang_acc(torqueo + 3 * ip, ori + 9 * (size_t)ip, w, momp + 3 * ipt, qua + 4 * ip, quad + 4 * ip,
+                            quadd + 4 * ip);
+                for (k = 0; k < 4; ++k) quad[4 * ip + k] = qdo[k] + (0.5 * tstep) * (quadd[4 * ip + k] + qddo[k]);
+            }
+        }
+    }
+    free(ori); free(force); free(forceo); free(torqueo);
+    return rc;
+}

@@ -165,6 +165,17 @@ int    or_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, const dou
                      const int32_t *iubuflow, const double *r2umin, double *force, double *utwob,
                      double *virial);
 
+/* nsteps of VelVer for rigid polyatomic particles (Src/md.F90:252-410, lpolyatom), the
+ * particle list held fixed; state arrays advanced in place (qua/quad/quadd [np][4]);
+ * ra [npt][maxsite][3] sites in the principal frame, masspt [npt], momp [npt][3]. */
+int    or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                   double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
+                   double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
+                   const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
+                   int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
+                   const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                   const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial);
+
 #ifdef __cplusplus
 }
 #endif

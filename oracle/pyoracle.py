@@ -363,6 +363,43 @@ def utwobody_p(s, table):
     return dict(force=force, utwob=utwob, virial=vir.value)
 
 
+def velver_p(s, table, nsteps):
+    """nsteps of rigid-body VelVer (oracle) on a systems.rigid_bodies dict, advanced in place
+    (ro, rod, rodd, qua, quad, quadd, r).  Returns dict(utwob, virial) of the last step."""
+    L = lib()
+    if not getattr(L, "_velver_p_typed", False):
+        L.or_velver_p.restype = C.c_int
+        L.or_velver_p.argtypes = [C.c_int32] * 5 + [f64p, C.c_double, C.c_double, C.c_int32, C.c_double] + \
+            [f64p] * 7 + [i32p] * 4 + [f64p, C.c_int32, f64p, f64p, i32p, i32p, C.c_int32, f64p, C.c_int32,
+                                         i32p, f64p, f64p, f64p]
+        L._velver_p_typed = True
+    k = {}
+    for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r", "ra", "masspt", "momp"):
+        k[key] = np.ascontiguousarray(s[key], np.float64)
+    for key in ("iptpn", "ianpn", "napt", "iatan", "nneighpn", "jpnlist"):
+        k[key] = np.ascontiguousarray(s[key], np.int32)
+    ub = np.ascontiguousarray(table["ubuf"], np.float64)
+    iub = np.ascontiguousarray(table["iubuflow"], np.int32)
+    r2 = np.ascontiguousarray(table["r2umin"], np.float64)
+    npt = int(s["npt"])
+    utwob = np.zeros(npt * (npt + 1) // 2 + 1)
+    vir = C.c_double()
+    box = (C.c_double * 3)(*s["boxlen"])
+    rc = L.or_velver_p(int(nsteps), int(s["np"]), int(s["na"]), npt, int(s["nat"]), box, float(s["rcut"]),
+                       float(s["tstep"]), int(s["nvvite"]), float(s["tvvite"]),
+                       *[_p(k[x], C.c_double) for x in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r")],
+                       *[_p(k[x], C.c_int32) for x in ("iptpn", "ianpn", "napt", "iatan")],
+                       _p(k["ra"], C.c_double), int(s["maxsite"]), _p(k["masspt"], C.c_double),
+                       _p(k["momp"], C.c_double), _p(k["nneighpn"], C.c_int32), _p(k["jpnlist"], C.c_int32),
+                       int(k["jpnlist"].shape[1]), _p(ub, C.c_double), len(ub), _p(iub, C.c_int32),
+                       _p(r2, C.c_double), _p(utwob, C.c_double), C.byref(vir))
+    if rc:
+        raise RuntimeError("VelVer (polyatomic) failed: %d" % rc)
+    for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
+        s[key] = k[key]
+    return dict(utwob=utwob, virial=vir.value)
+
+
 def random_stream(iseed, n):
     """n successive Random(iseed) values from the first call (Src/mollib.F90:2689-2708)."""
     st = (C.c_int32 * 2)()
