@@ -23,6 +23,8 @@
  *                                     GetKinEnergy (Src/md.F90:154-168, 252-410)
  *                                     followed by NList (Src/nlist.F90:597-621)
  *   msg_utwobody_p                 -> UTwoBodyP (Src/energy.F90:786-896), polyatomic particles
+ *   msg_velver_p                   -> MDDriver with VelVer for rigid polyatomic particles
+ *                                     (Src/md.F90:252-410, 628-663)
  *   msg_mc_seed / msg_mc_pass      -> MCDriver iSimulationStep: MCPass with SPartMove
  *                                     (Src/mc.F90:1470-1755), DUTotal, Metropolis, MCUpdate
  *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
@@ -293,6 +295,23 @@ int  msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, const doub
                     const int32_t *napt, const int32_t *iatan, const int32_t *nneighpn, const int32_t *jpnlist,
                     int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
                     const double *r2umin, double *force, double *utwob, double *virial, float *kernel_ms);
+
+/* nsteps of MDDriver for rigid polyatomic particles (VelVer with lpolyatom,
+ * Src/md.F90:252-410), the particle list held fixed: centre and quaternion update,
+ * QuaNorm, QuaToOri, PBC of the centres, SetAtomPos, UTwoBodyP, forces, torques and
+ * the molecular virial (UTotal, Src/energy.F90:403-426), GetLinAcc, and nvvite rounds of
+ * QuaVelToAngVel + GetAngAcc for the quaternion velocities (tvvite: their trial step).
+ * State (host arrays, MOLSIM layout) advanced in place: ro, rod, rodd [np][3], qua, quad,
+ * quadd [np][4] (qua(0:3)), r [na][3]; ra [npt][maxsite][3] the sites in the principal
+ * frame, masspt [npt], momp [npt][3] the principal moments; the rest as msg_utwobody_p.
+ * utwob and virial of the last step; kernel_ms (optional): device time of the steps. */
+int  msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                  double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod, double *rodd,
+                  double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn, const int32_t *ianpn,
+                  const int32_t *napt, const int32_t *iatan, const double *ra, int32_t maxsite,
+                  const double *masspt, const double *momp, const int32_t *nneighpn, const int32_t *jpnlist,
+                  int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
+                  const double *r2umin, double *utwob, double *virial, float *kernel_ms);
 
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,

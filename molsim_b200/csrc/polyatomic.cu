@@ -130,6 +130,157 @@ __global__ void k_utwobody_p_out(int na, int nptpt, const unsigned long long *__
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rigid-body velocity Verlet (VelVer with lpolyatom, Src/md.F90:252-410).
+// ---------------------------------------------------------------------------
+struct RigidArgs {
+    int np, nvvite;
+    double tstep, tvvite, fac;          // fac = dt^2 / 2
+    double box[3], half[3], boxi[3];
+    int maxsite;
+    double ffac;                        // (sclene / scllen) / sclfor: kJ/(mol A) -> internal force units
+};
+
+// Position and quaternion update, QuaNorm, QuaToOri, PBC of the centre, SetAtomPos
+// (Src/md.F90:290-318, Src/mollib.F90:2221-2255, 2594-2612, Src/molaux.F90:526-545),
+// in the reference's operation order.
+__global__ void k_rigid_move(RigidArgs A, double *__restrict__ ro, const double *__restrict__ rod,
+                             const double *__restrict__ rodd, double *__restrict__ qua,
+                             const double *__restrict__ quad, const double *__restrict__ quadd,
+                             double *__restrict__ ori, double *__restrict__ r, const int *__restrict__ iptpn,
+                             const int *__restrict__ ianpn, const int *__restrict__ napt, const double *__restrict__ ra)
+{
+    const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ip >= A.np) return;
+    double x[3];
+    for (int m = 0; m < 3; ++m) {
+        const double d = __dadd_rn(__dmul_rn(A.tstep, rod[3 * ip + m]), __dmul_rn(A.fac, rodd[3 * ip + m]));
+        double v = __dadd_rn(ro[3 * ip + m], d);
+        if (fabs(v) > A.half[m]) v = __dsub_rn(v, __dmul_rn(A.box[m], round(__dmul_rn(v, A.boxi[m]))));
+        ro[3 * ip + m] = v;
+        x[m] = v;
+    }
+    double q[4];
+    for (int k = 0; k < 4; ++k)
+        q[k] = __dadd_rn(__dadd_rn(qua[4 * ip + k], __dmul_rn(A.tstep, quad[4 * ip + k])),
+                         __dmul_rn(A.fac, quadd[4 * ip + k]));
+    const double nn = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(q[0], q[0]), __dmul_rn(q[1], q[1])), __dmul_rn(q[2], q[2])),
+                                __dmul_rn(q[3], q[3]));
+    const double norm = 1.0 / sqrt(nn);
+    for (int k = 0; k < 4; ++k) {
+        q[k] = __dmul_rn(q[k], norm);
+        qua[4 * ip + k] = q[k];
+    }
+    const double q00 = __dmul_rn(q[0], q[0]), q11 = __dmul_rn(q[1], q[1]), q22 = __dmul_rn(q[2], q[2]),
+                 q33 = __dmul_rn(q[3], q[3]), q01 = __dmul_rn(q[0], q[1]), q02 = __dmul_rn(q[0], q[2]),
+                 q03 = __dmul_rn(q[0], q[3]), q12 = __dmul_rn(q[1], q[2]), q13 = __dmul_rn(q[1], q[3]),
+                 q23 = __dmul_rn(q[2], q[3]);
+    double o[9];
+    o[0] = __dadd_rn(__dsub_rn(__dadd_rn(-q22, q11), q33), q00);
+    o[3] = __dmul_rn(2.0, __dsub_rn(q03, q12));
+    o[6] = __dmul_rn(2.0, __dadd_rn(q13, q02));
+    o[1] = -__dmul_rn(2.0, __dadd_rn(q12, q03));
+    o[4] = __dadd_rn(__dsub_rn(__dsub_rn(q22, q11), q33), q00);
+    o[7] = __dmul_rn(2.0, __dsub_rn(q01, q23));
+    o[2] = __dmul_rn(2.0, __dsub_rn(q13, q02));
+    o[5] = -__dmul_rn(2.0, __dadd_rn(q23, q01));
+    o[8] = __dadd_rn(__dadd_rn(__dsub_rn(-q22, q11), q33), q00);
+    for (int k = 0; k < 9; ++k) ori[9 * (size_t)ip + k] = o[k];
+    const int ipt = iptpn[ip] - 1, ia0 = ianpn[ip] - 1;
+    for (int a = 0; a < napt[ipt]; ++a) {
+        const double *s = ra + 3 * ((size_t)ipt * A.maxsite + a);
+        for (int m = 0; m < 3; ++m)
+            r[3 * (size_t)(ia0 + a) + m] =
+                __dadd_rn(__dadd_rn(__dadd_rn(x[m], __dmul_rn(o[3 * m], s[0])), __dmul_rn(o[3 * m + 1], s[1])),
+                          __dmul_rn(o[3 * m + 2], s[2]));
+    }
+}
+
+// UTotal's forces, torques and molecular virial (Src/energy.F90:403-426), GetLinAcc and the
+// half-kick, then the quaternion velocities: nvvite rounds of QuaVelToAngVel and GetAngAcc
+// (Src/md.F90:360-402, 628-663; Src/mollib.F90:2651-2669).  One thread per particle; the
+// sites' forces come from k_utwobody_p_out in kJ/(mol A).
+__global__ void k_rigid_kick(RigidArgs A, const double *__restrict__ ro, double *__restrict__ rod,
+                             double *__restrict__ rodd, const double *__restrict__ qua, double *__restrict__ quad,
+                             double *__restrict__ quadd, const double *__restrict__ ori, const double *__restrict__ r,
+                             const double *__restrict__ force, const int *__restrict__ iptpn,
+                             const int *__restrict__ ianpn, const int *__restrict__ napt,
+                             const double *__restrict__ masspt, const double *__restrict__ momp,
+                             unsigned long long *__restrict__ vmfix)
+{
+    const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ip >= A.np) return;
+    const int ipt = iptpn[ip] - 1, ia0 = ianpn[ip] - 1;
+    double fo[3] = {0.0, 0.0, 0.0}, to[3] = {0.0, 0.0, 0.0}, vm = 0.0;
+    for (int a = 0; a < napt[ipt]; ++a) {
+        const size_t ia = (size_t)(ia0 + a);
+        const double dx = __dsub_rn(r[3 * ia], ro[3 * ip]), dy = __dsub_rn(r[3 * ia + 1], ro[3 * ip + 1]),
+                     dz = __dsub_rn(r[3 * ia + 2], ro[3 * ip + 2]);
+        double f0 = force[3 * ia], f1 = force[3 * ia + 1], f2 = force[3 * ia + 2];
+        vm = __dadd_rn(__dadd_rn(__dadd_rn(vm, __dmul_rn(dx, f0)), __dmul_rn(dy, f1)), __dmul_rn(dz, f2));
+        f0 = __dmul_rn(f0, A.ffac);
+        f1 = __dmul_rn(f1, A.ffac);
+        f2 = __dmul_rn(f2, A.ffac);
+        fo[0] = __dadd_rn(fo[0], f0);
+        fo[1] = __dadd_rn(fo[1], f1);
+        fo[2] = __dadd_rn(fo[2], f2);
+        // torqueo + dy f3 - dz f2, left to right as the reference writes it
+        to[0] = __dsub_rn(__dadd_rn(to[0], __dmul_rn(dy, f2)), __dmul_rn(dz, f1));
+        to[1] = __dsub_rn(__dadd_rn(to[1], __dmul_rn(dz, f0)), __dmul_rn(dx, f2));
+        to[2] = __dsub_rn(__dadd_rn(to[2], __dmul_rn(dx, f1)), __dmul_rn(dy, f0));
+    }
+    atomicAdd(vmfix, (unsigned long long)__double2ll_rn(vm * kPFix));
+    const double mi = 1.0 / masspt[ipt];
+    for (int m = 0; m < 3; ++m) {
+        const double ao = rodd[3 * ip + m];
+        const double an = __dmul_rn(fo[m], mi);
+        rodd[3 * ip + m] = an;
+        rod[3 * ip + m] = __dadd_rn(rod[3 * ip + m], __dmul_rn(__dmul_rn(0.5, A.tstep), __dadd_rn(an, ao)));
+    }
+    const double *o = ori + 9 * (size_t)ip, *mp = momp + 3 * ipt;
+    double q[4], qd[4], qdo[4], qddo[4], qdd[4];
+    for (int k = 0; k < 4; ++k) {
+        q[k] = qua[4 * ip + k];
+        qddo[k] = quadd[4 * ip + k];
+        qdo[k] = quad[4 * ip + k];
+        qd[k] = __dadd_rn(qdo[k], __dmul_rn(__dmul_rn(A.tvvite, A.tstep), qddo[k]));
+        qdd[k] = qddo[k];
+    }
+    const double t1 = __dadd_rn(__dadd_rn(__dmul_rn(to[0], o[0]), __dmul_rn(to[1], o[3])), __dmul_rn(to[2], o[6]));
+    const double t2 = __dadd_rn(__dadd_rn(__dmul_rn(to[0], o[1]), __dmul_rn(to[1], o[4])), __dmul_rn(to[2], o[7]));
+    const double t3 = __dadd_rn(__dadd_rn(__dmul_rn(to[0], o[2]), __dmul_rn(to[1], o[5])), __dmul_rn(to[2], o[8]));
+    const double mi1 = 1.0 / mp[0], mi2 = 1.0 / mp[1], mi3 = 1.0 / mp[2];
+    for (int it = 0; it < A.nvvite; ++it) {
+        // QuaVelToAngVel
+        const double w1 = __dmul_rn(2.0, __dsub_rn(__dadd_rn(__dadd_rn(-__dmul_rn(q[3], qd[2]), __dmul_rn(q[0], qd[1])),
+                                                             __dmul_rn(q[2], qd[3])), __dmul_rn(q[1], qd[0])));
+        const double w2 = __dmul_rn(2.0, __dadd_rn(__dadd_rn(__dsub_rn(-__dmul_rn(q[0], qd[2]), __dmul_rn(q[3], qd[1])),
+                                                             __dmul_rn(q[1], qd[3])), __dmul_rn(q[2], qd[0])));
+        const double w3 = __dmul_rn(2.0, __dsub_rn(__dadd_rn(__dsub_rn(__dmul_rn(q[1], qd[2]), __dmul_rn(q[2], qd[1])),
+                                                             __dmul_rn(q[0], qd[3])), __dmul_rn(q[3], qd[0])));
+        // GetAngAcc
+        const double a1 = __dmul_rn(__dadd_rn(t1, __dmul_rn(__dmul_rn(w2, w3), __dsub_rn(mp[1], mp[2]))), mi1);
+        const double a2 = __dmul_rn(__dadd_rn(t2, __dmul_rn(__dmul_rn(w3, w1), __dsub_rn(mp[2], mp[0]))), mi2);
+        const double a3 = __dmul_rn(__dadd_rn(t3, __dmul_rn(__dmul_rn(w1, w2), __dsub_rn(mp[0], mp[1]))), mi3);
+        const double fq = __dmul_rn(-2.0, __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(qd[2], qd[2]), __dmul_rn(qd[1], qd[1])),
+                                                              __dmul_rn(qd[3], qd[3])), __dmul_rn(qd[0], qd[0])));
+        qdd[0] = __dmul_rn(0.5, __dadd_rn(__dsub_rn(__dadd_rn(-__dmul_rn(q[1], a1), __dmul_rn(q[2], a2)),
+                                                    __dmul_rn(q[3], a3)), __dmul_rn(q[0], fq)));
+        qdd[1] = __dmul_rn(0.5, __dadd_rn(__dsub_rn(__dsub_rn(__dmul_rn(q[0], a1), __dmul_rn(q[3], a2)),
+                                                    __dmul_rn(q[2], a3)), __dmul_rn(q[1], fq)));
+        qdd[2] = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dsub_rn(-__dmul_rn(q[3], a1), __dmul_rn(q[0], a2)),
+                                                    __dmul_rn(q[1], a3)), __dmul_rn(q[2], fq)));
+        qdd[3] = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(q[2], a1), __dmul_rn(q[1], a2)),
+                                                    __dmul_rn(q[0], a3)), __dmul_rn(q[3], fq)));
+        for (int k = 0; k < 4; ++k)
+            qd[k] = __dadd_rn(qdo[k], __dmul_rn(__dmul_rn(0.5, A.tstep), __dadd_rn(qdd[k], qddo[k])));
+    }
+    for (int k = 0; k < 4; ++k) {
+        quad[4 * ip + k] = qd[k];
+        quadd[4 * ip + k] = qdd[k];
+    }
+}
+
 template <class T>
 T *dev_copy(const T *h, size_t n, cudaError_t &e)
 {
@@ -220,6 +371,139 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
     for (void *p : {(void *)dro, (void *)dr, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat, (void *)dnn,
                     (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)ffix, (void *)dforce, (void *)duv,
                     (void *)derr})
+        if (p) cudaFree(p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return MSG_ERR_CUDA;
+    }
+    if (herr == 1) return MSG_ERR_TABLE_MIN;
+    if (herr == 2) return MSG_ERR_TABLE_RANGE;
+    return MSG_OK;
+}
+
+extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                            double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
+                            double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
+                            const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
+                            int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
+                            const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                            const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial,
+                            float *kernel_ms)
+{
+    if (nsteps < 0 || np < 1 || na < 1 || npt < 1 || nat < 1 || maxsite < 1 || maxnneigh < 1 || nbuf < 12 ||
+        nvvite < 0 || !boxlen || !ro || !rod || !rodd || !qua || !quad || !quadd || !r || !iptpn || !ianpn ||
+        !napt || !iatan || !ra || !masspt || !momp || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin ||
+        !utwob || !virial)
+        return MSG_ERR_ARG;
+    for (int t = 0; t < npt; ++t)
+        if (napt[t] < 1 || napt[t] > maxsite || !(masspt[t] > 0.0) || !(momp[3 * t] > 0.0) || !(momp[3 * t + 1] > 0.0) ||
+            !(momp[3 * t + 2] > 0.0))
+            return MSG_ERR_ARG;
+    for (int i = 0; i < np; ++i) {
+        if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na)
+            return MSG_ERR_ARG;
+        if (nneighpn[i] < 0 || nneighpn[i] > maxnneigh) return MSG_ERR_ARG;
+        for (int k = 0; k < nneighpn[i]; ++k) {
+            const int j = jpnlist[(size_t)i * maxnneigh + k];
+            if (j < 1 || j > np) return MSG_ERR_ARG;
+        }
+    }
+    const int natat = nat * (nat + 1) / 2, nptpt = npt * (npt + 1) / 2;
+    for (int a = 0; a < na; ++a)
+        if (iatan[a] < 1 || iatan[a] > nat) return MSG_ERR_ARG;
+    for (int q = 0; q < natat; ++q)
+        if (iubuflow[q] < 1 || iubuflow[q] + 11 > nbuf) return MSG_ERR_ARG;
+    RigidArgs A;
+    A.np = np;
+    A.nvvite = nvvite;
+    A.tstep = tstep;
+    A.tvvite = tvvite;
+    A.fac = 0.5 * tstep * tstep;
+    for (int m = 0; m < 3; ++m) {
+        A.box[m] = boxlen[m];
+        A.half[m] = boxlen[m] / 2.0;
+        A.boxi[m] = 1.0 / boxlen[m];
+    }
+    A.maxsite = maxsite;
+    {
+        // (sclene / scllen) / sclfor with MOLSIM's scales (Src/molsim.F90:786-805)
+        const double scllen = 1.0e-10, sclmas = 1.0e-03, scltim = 1.0e-12, sclene = 1.0e+03;
+        const double sclvel = scllen / scltim, sclacc = sclvel / scltim;
+        A.ffac = (sclene / scllen) / (sclacc * sclmas);
+    }
+    cudaError_t e = cudaSuccess;
+    double *dro = dev_copy(ro, 3 * (size_t)np, e), *drod = dev_copy(rod, 3 * (size_t)np, e),
+           *drodd = dev_copy(rodd, 3 * (size_t)np, e), *dqua = dev_copy(qua, 4 * (size_t)np, e),
+           *dquad = dev_copy(quad, 4 * (size_t)np, e), *dquadd = dev_copy(quadd, 4 * (size_t)np, e),
+           *dr = dev_copy(r, 3 * (size_t)na, e), *dra = dev_copy(ra, 3 * (size_t)npt * maxsite, e),
+           *dmass = dev_copy(masspt, (size_t)npt, e), *dmom = dev_copy(momp, 3 * (size_t)npt, e);
+    int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e);
+    int *dnapt = dev_copy(napt, (size_t)npt, e), *diat = dev_copy(iatan, (size_t)na, e);
+    int *dnn = dev_copy(nneighpn, (size_t)np, e), *djp = dev_copy(jpnlist, (size_t)np * maxnneigh, e);
+    double *dub = dev_copy(ubuf, (size_t)nbuf, e), *dr2 = dev_copy(r2umin, (size_t)natat, e);
+    int *diub = dev_copy(iubuflow, (size_t)natat, e);
+    unsigned long long *ffix = nullptr;
+    double *dforce = nullptr, *duv = nullptr, *dori = nullptr;
+    int *derr = nullptr;
+    const size_t nfix = 3 * (size_t)na + nptpt + 2;           // site forces, energies, pair and molecular virial
+    if (e == cudaSuccess) e = cudaMalloc(&ffix, nfix * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&duv, (nptpt + 2) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dori, 9 * (size_t)np * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
+    int herr = 0;
+    double vmol = 0.0;
+    if (e == cudaSuccess && nsteps > 0) {
+        unsigned long long *ufix = ffix + 3 * (size_t)na, *vfix = ufix + nptpt, *vmfix = vfix + 1;
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (kernel_ms) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, 0);
+        }
+        const int pb = (np + 127) / 128;
+        for (int step = 0; step < nsteps; ++step) {
+            cudaMemsetAsync(ffix, 0, nfix * sizeof(unsigned long long), 0);
+            k_rigid_move<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dipt, dian, dnapt, dra);
+            k_utwobody_p<<<np, kPThreads>>>(np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut,
+                                            dro, dr, dipt, dian, dnapt, diat, dnn, djp, maxnneigh, dub, nbuf, diub,
+                                            dr2, ffix, ufix, vfix, derr);
+            k_utwobody_p_out<<<(int)((3 * (size_t)na + 255) / 256), 256>>>(na, nptpt, ffix, ufix, vfix, dforce, duv);
+            k_rigid_kick<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dforce, dipt, dian, dnapt,
+                                      dmass, dmom, vmfix);
+        }
+        if (kernel_ms) {
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(kernel_ms, a, b);
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+        unsigned long long vm = 0;
+        if (e == cudaSuccess) e = cudaMemcpy(&vm, vmfix, sizeof(vm), cudaMemcpyDeviceToHost);
+        vmol = (double)(long long)vm * kPFixInv;
+    }
+    if (e == cudaSuccess && !herr) {
+        std::vector<double> uv(nptpt + 2, 0.0);
+        if (nsteps > 0) e = cudaMemcpy(uv.data(), duv, uv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        struct Back { double *h, *d; size_t n; } back[] = {
+            {ro, dro, 3 * (size_t)np}, {rod, drod, 3 * (size_t)np}, {rodd, drodd, 3 * (size_t)np},
+            {qua, dqua, 4 * (size_t)np}, {quad, dquad, 4 * (size_t)np}, {quadd, dquadd, 4 * (size_t)np},
+            {r, dr, 3 * (size_t)na}};
+        for (const Back &x : back)
+            if (e == cudaSuccess) e = cudaMemcpy(x.h, x.d, x.n * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && nsteps > 0) {
+            for (int q = 0; q <= nptpt; ++q) utwob[q] = uv[q];
+            *virial = uv[nptpt + 1] + vmol;
+        }
+    }
+    for (void *p : {(void *)dro, (void *)drod, (void *)drodd, (void *)dqua, (void *)dquad, (void *)dquadd, (void *)dr,
+                    (void *)dra, (void *)dmass, (void *)dmom, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat,
+                    (void *)dnn, (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)ffix, (void *)dforce,
+                    (void *)duv, (void *)dori, (void *)derr})
         if (p) cudaFree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();

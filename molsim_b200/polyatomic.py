@@ -1,5 +1,6 @@
-"""Polyatomic particles: UTwoBodyP (Src/energy.F90:786-896) on the GPU through the C-ABI
-(msg_utwobody_p).  The caller's arrays follow MOLSIM's layout (see
+"""Polyatomic particles: UTwoBodyP (Src/energy.F90:786-896) and the rigid-body MD step
+(VelVer with lpolyatom, Src/md.F90:252-410) on the GPU through the C-ABI (msg_utwobody_p,
+msg_velver_p).  The caller's arrays follow MOLSIM's layout (see
 systems.rigid_molecules); the atom-type table comes from engine.pot_tab."""
 import ctypes as C
 
@@ -40,3 +41,36 @@ def utwobody_p(s, table):
     if rc:
         raise MolsimGpuError(rc, "msg_utwobody_p")
     return dict(force=force, utwob=utwob, virial=vir.value, kernel_ms=ms.value)
+
+
+def velver_p(s, table, nsteps=1):
+    """nsteps of the rigid-body MD step for a systems.rigid_bodies dict, its state (ro, rod,
+    rodd, qua, quad, quadd, r) advanced in place.  Returns dict(utwob, virial, kernel_ms) of
+    the last step."""
+    k = {}
+    for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r", "ra", "masspt", "momp"):
+        k[key] = np.ascontiguousarray(s[key], np.float64)
+    for key in ("iptpn", "ianpn", "napt", "iatan", "nneighpn", "jpnlist"):
+        k[key] = np.ascontiguousarray(s[key], np.int32)
+    ub = np.ascontiguousarray(table["ubuf"], np.float64)
+    iub = np.ascontiguousarray(table["iubuflow"], np.int32)
+    r2 = np.ascontiguousarray(table["r2umin"], np.float64)
+    npt = int(s["npt"])
+    utwob = np.zeros(npt * (npt + 1) // 2 + 1)
+    vir = C.c_double()
+    ms = C.c_float()
+    box = (C.c_double * 3)(*s["boxlen"])
+    i32 = C.c_int32
+    rc = _lib.lib().msg_velver_p(int(nsteps), int(s["np"]), int(s["na"]), npt, int(s["nat"]), box, float(s["rcut"]),
+                                 float(s["tstep"]), int(s["nvvite"]), float(s["tvvite"]),
+                                 *[_p(k[x], C.c_double) for x in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r")],
+                                 *[_p(k[x], i32) for x in ("iptpn", "ianpn", "napt", "iatan")],
+                                 _p(k["ra"], C.c_double), int(s["maxsite"]), _p(k["masspt"], C.c_double),
+                                 _p(k["momp"], C.c_double), _p(k["nneighpn"], i32), _p(k["jpnlist"], i32),
+                                 int(k["jpnlist"].shape[1]), _p(ub, C.c_double), len(ub), _p(iub, i32),
+                                 _p(r2, C.c_double), _p(utwob, C.c_double), C.byref(vir), C.byref(ms))
+    if rc:
+        raise MolsimGpuError(rc, "msg_velver_p")
+    for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
+        s[key] = k[key]
+    return dict(utwob=utwob, virial=vir.value, kernel_ms=ms.value)
