@@ -134,6 +134,24 @@ module MolsimGpu
          type(c_ptr), value        :: iubuflow, r2umin, force, utwob, virial, kernel_ms
       end function msg_utwobody_p
 
+      integer(c_int) function msg_velver_p(nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, &
+            rodd, qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist, &
+            maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial, kernel_ms) bind(c, name='msg_velver_p')
+         import :: c_int, c_int32_t, c_double, c_ptr
+         integer(c_int32_t), value :: nsteps, np, na, npt, nat
+         real(c_double), intent(in) :: boxlen(3)
+         real(c_double), value     :: rcut, tstep
+         integer(c_int32_t), value :: nvvite
+         real(c_double), value     :: tvvite
+         type(c_ptr), value        :: ro, rod, rodd, qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra
+         integer(c_int32_t), value :: maxsite
+         type(c_ptr), value        :: masspt, momp, nneighpn, jpnlist
+         integer(c_int32_t), value :: maxnneigh
+         type(c_ptr), value        :: ubuf
+         integer(c_int32_t), value :: nbuf
+         type(c_ptr), value        :: iubuflow, r2umin, utwob, virial, kernel_ms
+      end function msg_velver_p
+
       integer(c_int) function msg_mc_seed(h, isys, iseed) bind(c, name='msg_mc_seed')
          import :: c_int, c_int32_t, c_ptr
          type(c_ptr), value        :: h
