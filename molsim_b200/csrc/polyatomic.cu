@@ -6,7 +6,7 @@
 // PBC2 (Src/molaux.F90:193-210); then every site of one particle meets every site
 // of the other through the atom-type table, shifted by the centres' box shift.
 //
-// One block per particle, one thread per list entry.  A thread walks the two
+// One warp per particle (four per block), one lane per list entry.  A lane walks the two
 // particles' sites; the forces on both sites, the energy of the particle-type pair
 // and the virial are added as 64-bit fixed point (2^-40 of the unit), so the sums do
 // not depend on the order the threads land in.  FP64 throughout.
@@ -23,7 +23,11 @@
 
 namespace {
 
-constexpr int kPThreads = 128;
+constexpr int kPThreads = 128;             // four warps: one particle's list row per warp
+constexpr int kPWarps = kPThreads / 32;
+constexpr int kPBuckets = 1024;            // bucket starts per atom-type pair of the site table
+constexpr int kPMaxType = 4;               // particle types (their energies ride in registers)
+constexpr int kPMaxPair = kPMaxType * (kPMaxType + 1) / 2;
 // 64-bit fixed point at 2^-40 of the unit: |force|, |energy| and |virial| sums up to
 // 8e6 (kJ/(mol A), kJ/mol) fit, far above what a tabulated pair potential produces.
 constexpr double kPFix = 1099511627776.0;       // 2^40
@@ -37,19 +41,36 @@ __host__ __device__ inline int type_pair(int n, int a, int b)
     return (lo - 1) * n - (lo - 1) * (lo - 2) / 2 + (hi - lo);
 }
 
+// Bucket grid of one atom-type pair's table: z_lo = r2umin, z_hi = the top interval's z_low.
+struct SiteBuckets {
+    double z_lo, z_hi, inv_h, pad;
+};
+
 __global__ void __launch_bounds__(kPThreads) k_utwobody_p(
     int np, int npt, int nat, double3 box, double rcut2, const double *__restrict__ ro,
     const double *__restrict__ r, const int *__restrict__ iptpn, const int *__restrict__ ianpn,
     const int *__restrict__ napt, const int *__restrict__ iatan, const int *__restrict__ nneighpn,
     const int *__restrict__ jpnlist, int maxnneigh, const double *__restrict__ ubuf, int nbuf,
-    const int *__restrict__ iubuflow, const double *__restrict__ r2umin, unsigned long long *__restrict__ ffix,
+    const int *__restrict__ iubuflow, const double *__restrict__ r2umin, const SiteBuckets *__restrict__ sb,
+    const int *__restrict__ bstart, int maxsite, unsigned long long *__restrict__ ffix,
     unsigned long long *__restrict__ ufix, unsigned long long *__restrict__ vfix, int *__restrict__ err)
 {
-    const int ip = blockIdx.x;
+    // per warp: the row particle's site forces, summed in shared memory before one
+    // global add per component (every lane of the warp adds to the same sites)
+    extern __shared__ unsigned long long sfi[];
+    const int warp = (int)(threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int ip = blockIdx.x * kPWarps + warp;
+    if (ip >= np) return;                      // a whole warp: only warp-level syncs below
+    unsigned long long *fi_w = sfi + (size_t)warp * 3 * maxsite;
     const double half[3] = {0.5 * box.x, 0.5 * box.y, 0.5 * box.z}, len[3] = {box.x, box.y, box.z};
-    const int ipt = iptpn[ip], ialow = ianpn[ip] - 1, iaupp = ialow + napt[ipt - 1] - 1;
+    const int ipt = iptpn[ip], ialow = ianpn[ip] - 1, nsi = napt[ipt - 1];
+    for (int k = lane; k < 3 * nsi; k += 32) fi_w[k] = 0ull;
+    __syncwarp();
     long long vir = 0;
-    for (int jploc = threadIdx.x; jploc < nneighpn[ip]; jploc += kPThreads) {
+    long long ue[kPMaxPair];                   // energy by particle-type pair, this lane's entries
+#pragma unroll
+    for (int q = 0; q < kPMaxPair; ++q) ue[q] = 0;
+    for (int jploc = lane; jploc < nneighpn[ip]; jploc += 32) {
         const int jp = jpnlist[(size_t)ip * maxnneigh + jploc] - 1;
         const int jpt = iptpn[jp];
         const int jalow = ianpn[jp] - 1, jaupp = jalow + napt[jpt - 1] - 1;
@@ -62,7 +83,8 @@ __global__ void __launch_bounds__(kPThreads) k_utwobody_p(
         const double rr = __dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2]));
         if (rr > rcut2) continue;
         double usum = 0.0;
-        for (int ia = ialow; ia <= iaupp; ++ia) {
+        for (int il = 0; il < nsi; ++il) {
+            const int ia = ialow + il;
             const int iat = iatan[ia];
             double fi[3] = {0.0, 0.0, 0.0};
             for (int ja = jalow; ja <= jaupp; ++ja) {
@@ -75,7 +97,14 @@ __global__ void __launch_bounds__(kPThreads) k_utwobody_p(
                     atomicCAS(err, 0, 1);      // StopUTwoBodyP: below the table
                     continue;
                 }
+                // the walk starts at the bucket's start, which never passes the interval sought
+                const SiteBuckets B = sb[q];
                 int ib = iubuflow[q] - 1;
+                if (a2 < B.z_hi) {
+                    int bk = (int)((a2 - B.z_lo) * B.inv_h);
+                    bk = bk < 0 ? 0 : (bk >= kPBuckets ? kPBuckets - 1 : bk);
+                    ib += 12 * bstart[q * kPBuckets + bk];
+                }
                 bool bad = false;
                 while (a2 < ubuf[ib]) {
                     ib += 12;
@@ -101,14 +130,32 @@ __global__ void __launch_bounds__(kPThreads) k_utwobody_p(
                 atomicAdd(fj + 2, (unsigned long long)__double2ll_rn(-(fs * dz) * kPFix));
                 vir += __double2ll_rn(-(fs * a2) * kPFix);
             }
-            unsigned long long *fa = ffix + 3 * (size_t)ia;
-            atomicAdd(fa, (unsigned long long)__double2ll_rn(fi[0] * kPFix));
-            atomicAdd(fa + 1, (unsigned long long)__double2ll_rn(fi[1] * kPFix));
-            atomicAdd(fa + 2, (unsigned long long)__double2ll_rn(fi[2] * kPFix));
+            atomicAdd(fi_w + 3 * il, (unsigned long long)__double2ll_rn(fi[0] * kPFix));
+            atomicAdd(fi_w + 3 * il + 1, (unsigned long long)__double2ll_rn(fi[1] * kPFix));
+            atomicAdd(fi_w + 3 * il + 2, (unsigned long long)__double2ll_rn(fi[2] * kPFix));
         }
-        atomicAdd(ufix + type_pair(npt, ipt, jpt), (unsigned long long)__double2ll_rn(usum * kPFix));
+        const long long uq = __double2ll_rn(usum * kPFix);
+        const int pq = type_pair(npt, ipt, jpt);
+#pragma unroll
+        for (int q = 0; q < kPMaxPair; ++q) ue[q] += (q == pq) ? uq : 0;
     }
-    if (vir) atomicAdd(vfix, (unsigned long long)vir);
+    // warp sums (integers: exact, order-free), then one global add each
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vir += __shfl_xor_sync(0xffffffffu, vir, o);
+#pragma unroll
+    for (int q = 0; q < kPMaxPair; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ue[q] += __shfl_xor_sync(0xffffffffu, ue[q], o);
+    __syncwarp();
+    for (int k = lane; k < 3 * nsi; k += 32)
+        if (fi_w[k]) atomicAdd(ffix + 3 * (size_t)ialow + k, fi_w[k]);
+    if (lane == 0) {
+        if (vir) atomicAdd(vfix, (unsigned long long)vir);
+        const int nptpt = npt * (npt + 1) / 2;
+#pragma unroll
+        for (int q = 0; q < kPMaxPair; ++q)
+            if (q < nptpt && ue[q]) atomicAdd(ufix + q, (unsigned long long)ue[q]);
+    }
 }
 
 __global__ void k_utwobody_p_out(int na, int nptpt, const unsigned long long *__restrict__ ffix,
@@ -281,6 +328,47 @@ __global__ void k_rigid_kick(RigidArgs A, const double *__restrict__ ro, double 
     }
 }
 
+// The site table's bucket grid and starts, per atom-type pair q: buckets over
+// [r2umin, top interval's z_low); a bucket's start is the interval where the reference's
+// walk from the top stops for z = z_lo + (b + 2) h, one bucket above b's top, so it never
+// passes the interval of any r2 in the bucket (the stop only moves down as z grows).
+void site_buckets(int natat, const double *ubuf, int nbuf, const int32_t *iubuflow, const double *r2umin,
+                  std::vector<SiteBuckets> &sb, std::vector<int> &bs)
+{
+    sb.assign(natat, SiteBuckets{0.0, 0.0, 1.0, 0.0});
+    bs.assign((size_t)natat * kPBuckets, 0);
+    for (int q = 0; q < natat; ++q) {
+        const int first = iubuflow[q] - 1;
+        const double z_lo = r2umin[q], z_top = ubuf[first];
+        int nk = 0;
+        while (first + 12 * (nk + 1) <= nbuf) {
+            ++nk;
+            if (ubuf[first + 12 * (nk - 1)] <= z_lo) break;
+        }
+        const double h = (z_top > z_lo) ? (z_top - z_lo) / kPBuckets : 1.0;
+        sb[q] = SiteBuckets{z_lo, z_top, 1.0 / h, 0.0};
+        int kk = 0;
+        for (int b = kPBuckets - 1; b >= 0; --b) {
+            const double zq = z_lo + (b + 2.0) * h;
+            while (kk < nk - 1 && zq < ubuf[first + 12 * kk]) ++kk;
+            bs[(size_t)q * kPBuckets + b] = kk;
+        }
+    }
+}
+
+int max_sites(int npt, const int32_t *napt)
+{
+    int m = 1;
+    for (int t = 0; t < npt; ++t) m = std::max(m, (int)napt[t]);
+    return m;
+}
+
+// shared memory of k_utwobody_p: each warp's row-particle site forces
+size_t site_smem(int npt, const int32_t *napt)
+{
+    return (size_t)kPWarps * 3 * max_sites(npt, napt) * sizeof(unsigned long long);
+}
+
 template <class T>
 T *dev_copy(const T *h, size_t n, cudaError_t &e)
 {
@@ -299,13 +387,14 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
                               const int32_t *iubuflow, const double *r2umin, double *force, double *utwob,
                               double *virial, float *kernel_ms)
 {
-    if (np < 1 || na < 1 || npt < 1 || nat < 1 || maxnneigh < 1 || nbuf < 12 || !boxlen || !ro || !r || !iptpn ||
+    if (np < 1 || na < 1 || npt < 1 || npt > kPMaxType || nat < 1 || maxnneigh < 1 || nbuf < 12 || !boxlen || !ro ||
+        !r || !iptpn ||
         !ianpn || !napt || !iatan || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin || !force || !utwob ||
         !virial)
         return MSG_ERR_ARG;
     // host-side checks of the indices the kernel follows
     for (int t = 0; t < npt; ++t)
-        if (napt[t] < 1) return MSG_ERR_ARG;
+        if (napt[t] < 1 || napt[t] > 256) return MSG_ERR_ARG;
     for (int i = 0; i < np; ++i) {
         if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na)
             return MSG_ERR_ARG;
@@ -327,6 +416,11 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
     int *dnn = dev_copy(nneighpn, (size_t)np, e), *djp = dev_copy(jpnlist, (size_t)np * maxnneigh, e);
     double *dub = dev_copy(ubuf, (size_t)nbuf, e), *dr2 = dev_copy(r2umin, (size_t)natat, e);
     int *diub = dev_copy(iubuflow, (size_t)natat, e);
+    std::vector<SiteBuckets> hsb;
+    std::vector<int> hbs;
+    site_buckets(natat, ubuf, nbuf, iubuflow, r2umin, hsb, hbs);
+    SiteBuckets *dsb = dev_copy(hsb.data(), hsb.size(), e);
+    int *dbs = dev_copy(hbs.data(), hbs.size(), e);
     unsigned long long *ffix = nullptr, *ufix = nullptr;
     double *dforce = nullptr, *duv = nullptr;
     int *derr = nullptr;
@@ -346,9 +440,9 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
             cudaEventCreate(&b);
             cudaEventRecord(a, 0);
         }
-        k_utwobody_p<<<np, kPThreads>>>(np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut, dro,
-                                        dr, dipt, dian, dnapt, diat, dnn, djp, maxnneigh, dub, nbuf, diub, dr2, ffix,
-                                        ufix, ufix + nptpt, derr);
+        k_utwobody_p<<<(np + kPWarps - 1) / kPWarps, kPThreads, site_smem(npt, napt)>>>(
+            np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut, dro, dr, dipt, dian, dnapt, diat,
+            dnn, djp, maxnneigh, dub, nbuf, diub, dr2, dsb, dbs, max_sites(npt, napt), ffix, ufix, ufix + nptpt, derr);
         k_utwobody_p_out<<<(int)((3 * (size_t)na + 255) / 256), 256>>>(na, nptpt, ffix, ufix, ufix + nptpt, dforce,
                                                                         duv);
         if (kernel_ms) {
@@ -369,8 +463,8 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
         }
     }
     for (void *p : {(void *)dro, (void *)dr, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat, (void *)dnn,
-                    (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)ffix, (void *)dforce, (void *)duv,
-                    (void *)derr})
+                    (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)dsb, (void *)dbs, (void *)ffix,
+                    (void *)dforce, (void *)duv, (void *)derr})
         if (p) cudaFree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -390,7 +484,8 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
                             const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial,
                             float *kernel_ms)
 {
-    if (nsteps < 0 || np < 1 || na < 1 || npt < 1 || nat < 1 || maxsite < 1 || maxnneigh < 1 || nbuf < 12 ||
+    if (nsteps < 0 || np < 1 || na < 1 || npt < 1 || npt > kPMaxType || nat < 1 || maxsite < 1 || maxsite > 256 ||
+        maxnneigh < 1 || nbuf < 12 ||
         nvvite < 0 || !boxlen || !ro || !rod || !rodd || !qua || !quad || !quadd || !r || !iptpn || !ianpn ||
         !napt || !iatan || !ra || !masspt || !momp || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin ||
         !utwob || !virial)
@@ -442,6 +537,11 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
     int *dnn = dev_copy(nneighpn, (size_t)np, e), *djp = dev_copy(jpnlist, (size_t)np * maxnneigh, e);
     double *dub = dev_copy(ubuf, (size_t)nbuf, e), *dr2 = dev_copy(r2umin, (size_t)natat, e);
     int *diub = dev_copy(iubuflow, (size_t)natat, e);
+    std::vector<SiteBuckets> hsb;
+    std::vector<int> hbs;
+    site_buckets(natat, ubuf, nbuf, iubuflow, r2umin, hsb, hbs);
+    SiteBuckets *dsb = dev_copy(hsb.data(), hsb.size(), e);
+    int *dbs = dev_copy(hbs.data(), hbs.size(), e);
     unsigned long long *ffix = nullptr;
     double *dforce = nullptr, *duv = nullptr, *dori = nullptr;
     int *derr = nullptr;
@@ -466,9 +566,9 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
         for (int step = 0; step < nsteps; ++step) {
             cudaMemsetAsync(ffix, 0, nfix * sizeof(unsigned long long), 0);
             k_rigid_move<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dipt, dian, dnapt, dra);
-            k_utwobody_p<<<np, kPThreads>>>(np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut,
-                                            dro, dr, dipt, dian, dnapt, diat, dnn, djp, maxnneigh, dub, nbuf, diub,
-                                            dr2, ffix, ufix, vfix, derr);
+            k_utwobody_p<<<(np + kPWarps - 1) / kPWarps, kPThreads, site_smem(npt, napt)>>>(
+                np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut, dro, dr, dipt, dian, dnapt,
+                diat, dnn, djp, maxnneigh, dub, nbuf, diub, dr2, dsb, dbs, max_sites(npt, napt), ffix, ufix, vfix, derr);
             k_utwobody_p_out<<<(int)((3 * (size_t)na + 255) / 256), 256>>>(na, nptpt, ffix, ufix, vfix, dforce, duv);
             k_rigid_kick<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dforce, dipt, dian, dnapt,
                                       dmass, dmom, vmfix);
@@ -502,8 +602,8 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
     }
     for (void *p : {(void *)dro, (void *)drod, (void *)drodd, (void *)dqua, (void *)dquad, (void *)dquadd, (void *)dr,
                     (void *)dra, (void *)dmass, (void *)dmom, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat,
-                    (void *)dnn, (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)ffix, (void *)dforce,
-                    (void *)duv, (void *)dori, (void *)derr})
+                    (void *)dnn, (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)dsb, (void *)dbs,
+                    (void *)ffix, (void *)dforce, (void *)duv, (void *)dori, (void *)derr})
         if (p) cudaFree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
