@@ -25,6 +25,9 @@
  *   msg_utwobody_p                 -> UTwoBodyP (Src/energy.F90:786-896), polyatomic particles
  *   msg_velver_p                   -> MDDriver with VelVer for rigid polyatomic particles
  *                                     (Src/md.F90:252-410, 628-663)
+ *   msg_uewald_sites               -> UEwald over the sites of polyatomic particles: UEwaldRecStd,
+ *                                     UEwaldSelf with its molecular term, UEwaldSurf
+ *                                     (Src/energy.F90:905-1104, 1301-1371)
  *   msg_mc_seed / msg_mc_pass      -> MCDriver iSimulationStep: MCPass with SPartMove
  *                                     (Src/mc.F90:1470-1755), DUTotal, Metropolis, MCUpdate
  *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
@@ -312,6 +315,20 @@ int  msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t n
                   const double *masspt, const double *momp, const int32_t *nneighpn, const int32_t *jpnlist,
                   int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
                   const double *r2umin, double *utwob, double *virial, float *kernel_ms);
+
+/* UEwald over the sites of polyatomic particles (Src/energy.F90:905-958) with the
+ * standard reciprocal sum (UEwaldRecStd, :964-1104; k-vectors of EwaldSetup 'std' from
+ * ncut and ncutregion 0 sphere / 1 cube), UEwaldSelf's atomic term and its molecular term
+ * (the erf(alpha r)/r of every site pair inside a particle, :1301-1345) and, when lsurf,
+ * UEwaldSurf (:1349-1371).  Sites r [na][3] with charges az [na]; the particles' sites
+ * from iptpn, ianpn (1-based) and napt [npt].  force [na][3] is overwritten with the
+ * Ewald forces; urec = u%rec and virrec its virial, both scaled by epsfp (EpsiFourPi)
+ * as UEwald does.  The sums are deterministic (fixed point, fixed order).
+ * MSG_ERR_ARG for ncut outside 1..100 or a particle whose sites leave 1..na. */
+int  msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
+                      int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                      const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
+                      double *force, double *urec, double *virrec, float *kernel_ms);
 
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,

@@ -73,6 +73,9 @@ SIGNATURES = {
                                    f64p, f64p, C.POINTER(C.c_float)]),
     "msg_utwobody_p": (C.c_int, [C.c_int32] * 4 + [f64p, C.c_double, f64p, f64p] + [i32p] * 6 +
                        [C.c_int32, f64p, C.c_int32, i32p, f64p, f64p, f64p, f64p, C.POINTER(C.c_float)]),
+    "msg_uewald_sites": (C.c_int, [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double, f64p,
+                                   f64p, C.c_int32, i32p, i32p, i32p, C.c_int32, f64p, f64p, f64p,
+                                   C.POINTER(C.c_float)]),
     "msg_mc_pass": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(MsgMcParams), C.POINTER(C.c_int64),
                               C.POINTER(C.c_int64), C.c_int32, C.POINTER(MsgEnergy)]),
     "msg_get_forces": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p]),

@@ -613,3 +613,274 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
     if (herr == 2) return MSG_ERR_TABLE_RANGE;
     return MSG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// UEwald over the sites of polyatomic particles (Src/energy.F90:905-958 with the
+// standard reciprocal sum, UEwaldRecStd :964-1104, and UEwaldSelf's atomic and
+// molecular terms, :1301-1345).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kSK = 128;                  // k-vectors per structure-factor block
+constexpr int kSChunk = 512;              // sites per partial sum
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// exp(i 2pi n x / L), n = 0..ncut, by EwaldSetArray's recurrence (Src/energy.F90:1401-1426);
+// the x row is scaled by the site's charge (az * eikx).
+__global__ void k_site_eik(int na, int w, double3 tpbi, const double *__restrict__ r, const double *__restrict__ az,
+                           double2 *__restrict__ eik)
+{
+    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ia >= na) return;
+    const double t[3] = {tpbi.x, tpbi.y, tpbi.z};
+    for (int m = 0; m < 3; ++m) {
+        double sn, cs;
+        sincos(t[m] * r[3 * (size_t)ia + m], &sn, &cs);
+        const double2 e1 = make_double2(cs, sn);
+        const double sc = (m == 0) ? az[ia] : 1.0;
+        double2 *row = eik + ((size_t)ia * 3 + m) * w;
+        double2 e = make_double2(1.0, 0.0);
+        row[0] = make_double2(sc, 0.0);
+        for (int n = 1; n < w; ++n) {
+            e = (n == 1) ? e1 : zmul(e, e1);
+            row[n] = make_double2(sc * e.x, sc * e.y);
+        }
+    }
+}
+
+// Partial structure factors of (k tile blockIdx.x, site chunk blockIdx.y): part[chunk][k][4].
+__global__ void __launch_bounds__(kSK) k_site_sk(int na, int nkv, int w, const int4 *__restrict__ kv,
+                                                 const double2 *__restrict__ eik, double2 *__restrict__ part)
+{
+    const int kn = blockIdx.x * kSK + threadIdx.x;
+    if (kn >= nkv) return;
+    const int4 n = kv[kn];
+    const int a0 = blockIdx.y * kSChunk, a1 = min(na, a0 + kSChunk);
+    double2 s[4];
+    for (int c = 0; c < 4; ++c) s[c] = make_double2(0.0, 0.0);
+    for (int ia = a0; ia < a1; ++ia) {
+        const double2 *t = eik + (size_t)ia * 3 * w;
+        const double2 qx = t[n.x], ey = t[w + n.y], ez = t[2 * w + n.z];
+        const double2 yzm = zmul(zconj(ey), ez), yzp = zmul(ey, ez), qxc = zconj(qx);
+        const double2 v[4] = {zmul(qxc, yzm), zmul(qxc, yzp), zmul(qx, yzm), zmul(qx, yzp)};
+        for (int c = 0; c < 4; ++c) {
+            s[c].x += v[c].x;
+            s[c].y += v[c].y;
+        }
+    }
+    double2 *o = part + ((size_t)blockIdx.y * nkv + kn) * 4;
+    for (int c = 0; c < 4; ++c) o[c] = s[c];
+}
+
+// S(k) = the chunks in order; energy kfac |S|^2 and virial -(1 - k^2/2alpha^2) kfac |S|^2
+// in 64-bit fixed point (2^-40).
+__global__ void __launch_bounds__(kSK) k_site_reduce(int nkv, int nchunk, double alpha2, double3 tpbi,
+                                                     const int4 *__restrict__ kv, const double *__restrict__ kfac,
+                                                     const double2 *__restrict__ part, double2 *__restrict__ sk,
+                                                     unsigned long long *__restrict__ efix)
+{
+    const int kn = blockIdx.x * kSK + threadIdx.x;
+    long long e = 0, v = 0;
+    if (kn < nkv) {
+        double2 s[4];
+        for (int c = 0; c < 4; ++c) s[c] = make_double2(0.0, 0.0);
+        for (int ch = 0; ch < nchunk; ++ch)
+            for (int c = 0; c < 4; ++c) {
+                const double2 p = part[((size_t)ch * nkv + kn) * 4 + c];
+                s[c].x += p.x;
+                s[c].y += p.y;
+            }
+        double t = 0.0;
+        for (int c = 0; c < 4; ++c) {
+            sk[(size_t)kn * 4 + c] = s[c];
+            t = t + (s[c].x * s[c].x + s[c].y * s[c].y);
+        }
+        t = kfac[kn] * t;
+        const int4 n = kv[kn];
+        const double kx = n.x * tpbi.x, ky = n.y * tpbi.y, kz = n.z * tpbi.z;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        e = __double2ll_rn(t * kPFix);
+        v = __double2ll_rn(-((1.0 - k2 / (2.0 * alpha2)) * t) * kPFix);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (e) atomicAdd(efix, (unsigned long long)e);
+        if (v) atomicAdd(efix + 1, (unsigned long long)v);
+    }
+}
+
+// Reciprocal force of each site over every k-vector, in the reference's order
+// (Src/energy.F90:1078-1092): F += kfac2 k (combinations of Im(eikr conj S)).
+__global__ void k_site_force(int na, int nkv, int w, double epsfp, double3 tpbi, const int4 *__restrict__ kv,
+                             const double *__restrict__ kfac, const double2 *__restrict__ sk,
+                             const double2 *__restrict__ eik, double *__restrict__ force)
+{
+    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ia >= na) return;
+    const double2 *t = eik + (size_t)ia * 3 * w;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int kn = 0; kn < nkv; ++kn) {
+        const int4 n = kv[kn];
+        const double2 qx = t[n.x], ey = t[w + n.y], ez = t[2 * w + n.z];
+        const double2 yzm = zmul(zconj(ey), ez), yzp = zmul(ey, ez), qxc = zconj(qx);
+        const double2 r0 = zmul(qxc, yzm), r1 = zmul(qxc, yzp), r2 = zmul(qx, yzm), r3 = zmul(qx, yzp);
+        const double2 *S = sk + (size_t)kn * 4;
+        const double fmm = -r0.x * S[0].y + r0.y * S[0].x, fmp = -r1.x * S[1].y + r1.y * S[1].x;
+        const double fpm = -r2.x * S[2].y + r2.y * S[2].x, fpp = -r3.x * S[3].y + r3.y * S[3].x;
+        const double kf2 = epsfp * 2.0 * kfac[kn];
+        fx += (kf2 * n.x * tpbi.x) * (-fmm - fmp + fpm + fpp);
+        fy += (kf2 * n.y * tpbi.y) * (-fmm + fmp - fpm + fpp);
+        fz += (kf2 * n.z * tpbi.z) * (fmm + fmp + fpm + fpp);
+    }
+    force[3 * (size_t)ia] = fx;
+    force[3 * (size_t)ia + 1] = fy;
+    force[3 * (size_t)ia + 2] = fz;
+}
+
+// UEwaldSelf's molecular term (Src/energy.F90:1315-1343): every site pair inside a
+// particle subtracts q q erf(alpha r)/r; its forces are added into `force`.
+__global__ void k_site_self(int np, double alpha, double ewaldfac1, double epsfp, const double *__restrict__ r,
+                            const double *__restrict__ az, const int *__restrict__ iptpn,
+                            const int *__restrict__ ianpn, const int *__restrict__ napt, double *__restrict__ force,
+                            unsigned long long *__restrict__ efix)
+{
+    const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+    long long eu = 0;
+    if (ip < np) {
+        const int ialow = ianpn[ip] - 1, iaupp = ialow + napt[iptpn[ip] - 1] - 1;
+        for (int i = ialow; i <= iaupp; ++i)
+            for (int j = i + 1; j <= iaupp; ++j) {
+                const double dx = r[3 * (size_t)i] - r[3 * (size_t)j], dy = r[3 * (size_t)i + 1] - r[3 * (size_t)j + 1],
+                             dz = r[3 * (size_t)i + 2] - r[3 * (size_t)j + 2];
+                const double r2 = dx * dx + dy * dy + dz * dz, r1 = sqrt(r2);
+                double r1i = 1.0 / r1;
+                const double r2i = r1i * r1i, ex = exp(-(alpha * alpha) * r2);
+                r1i = r1i * erf(alpha * r1);
+                const double r3i = r2i * (r1i - ewaldfac1 * ex);
+                eu += __double2ll_rn(-(az[i] * az[j] * r1i) * kPFix);
+                const double fac = epsfp * az[i] * az[j] * r3i;
+                // the particle's own sites: this thread is the only writer
+                force[3 * (size_t)i] -= fac * dx;
+                force[3 * (size_t)i + 1] -= fac * dy;
+                force[3 * (size_t)i + 2] -= fac * dz;
+                force[3 * (size_t)j] += fac * dx;
+                force[3 * (size_t)j + 1] += fac * dy;
+                force[3 * (size_t)j + 2] += fac * dz;
+            }
+    }
+    for (int o = 16; o > 0; o >>= 1) eu += __shfl_xor_sync(0xffffffffu, eu, o);
+    if ((threadIdx.x & 31) == 0 && eu) atomicAdd(efix + 2, (unsigned long long)eu);
+}
+
+}  // namespace
+
+extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
+                                int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                                const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
+                                double *force, double *urec, double *virrec, float *kernel_ms)
+{
+    if (na < 1 || np < 1 || npt < 1 || ncut < 1 || ncut > 100 || ncutregion < 0 || ncutregion > 1 ||
+        !(ualpha > 0.0) || !boxlen || !r || !az || !iptpn || !ianpn || !napt || !force || !urec || !virrec)
+        return MSG_ERR_ARG;
+    for (int t = 0; t < npt; ++t)
+        if (napt[t] < 1) return MSG_ERR_ARG;
+    for (int i = 0; i < np; ++i)
+        if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na)
+            return MSG_ERR_ARG;
+    const double pi = 3.1415926535897932;
+    const double vol = boxlen[0] * boxlen[1] * boxlen[2];
+    const double3 tpbi = make_double3(2.0 * pi * (1.0 / boxlen[0]), 2.0 * pi * (1.0 / boxlen[1]),
+                                      2.0 * pi * (1.0 / boxlen[2]));
+    // k-vectors and kfac in the order of EwaldSetup 'std' (Src/energy.F90:6762-6782)
+    std::vector<int4> kv;
+    std::vector<double> kf;
+    const int ncut2 = ncutregion ? 3 * ncut * ncut : ncut * ncut;
+    for (int nz = 0; nz <= ncut; ++nz)
+        for (int ny = 0; ny <= ncut; ++ny)
+            for (int nx = 0; nx <= ncut; ++nx) {
+                if (nx * nx + ny * ny + nz * nz > ncut2 || (nx == 0 && ny == 0 && nz == 0)) continue;
+                const double facz = nz == 0 ? 1.0 : 2.0, facy = ny == 0 ? 0.5 : 1.0, facx = nx == 0 ? 0.5 : 1.0;
+                const double kx = nx * tpbi.x, ky = ny * tpbi.y, kz = nz * tpbi.z, k2 = kx * kx + ky * ky + kz * kz;
+                kf.push_back(2.0 * pi / vol * facz * facy * facx * std::exp(-k2 / (4.0 * (ualpha * ualpha))) / k2);
+                kv.push_back(make_int4(nx, ny, nz, 0));
+            }
+    const int nkv = (int)kv.size(), w = ncut + 1, nchunk = (na + kSChunk - 1) / kSChunk;
+    // the surface term on the host (UEwaldSurf, Src/energy.F90:1349-1371)
+    double mx = 0.0, my = 0.0, mz = 0.0, q2 = 0.0;
+    for (int a = 0; a < na; ++a) {
+        mx += az[a] * r[3 * (size_t)a];
+        my += az[a] * r[3 * (size_t)a + 1];
+        mz += az[a] * r[3 * (size_t)a + 2];
+        q2 += az[a] * az[a];
+    }
+    cudaError_t e = cudaSuccess;
+    double *dr = dev_copy(r, 3 * (size_t)na, e), *daz = dev_copy(az, (size_t)na, e), *dkf = dev_copy(kf.data(), kf.size(), e);
+    int4 *dkv = dev_copy(kv.data(), kv.size(), e);
+    int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e), *dnapt = dev_copy(napt, (size_t)npt, e);
+    double2 *eik = nullptr, *part = nullptr, *sk = nullptr;
+    double *dforce = nullptr;
+    unsigned long long *efix = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&efix, 3 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(efix, 0, 3 * sizeof(unsigned long long));
+    unsigned long long hfix[3] = {0, 0, 0};
+    if (e == cudaSuccess) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (kernel_ms) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, 0);
+        }
+        k_site_eik<<<(na + 127) / 128, 128>>>(na, w, tpbi, dr, daz, eik);
+        k_site_sk<<<dim3((nkv + kSK - 1) / kSK, nchunk), kSK>>>(na, nkv, w, dkv, eik, part);
+        k_site_reduce<<<(nkv + kSK - 1) / kSK, kSK>>>(nkv, nchunk, ualpha * ualpha, tpbi, dkv, dkf, part, sk, efix);
+        k_site_force<<<(na + 127) / 128, 128>>>(na, nkv, w, epsfp, tpbi, dkv, dkf, sk, eik, dforce);
+        const double ewaldfac1 = (1.0 / (std::sqrt(pi) * ualpha)) * 2.0 * (ualpha * ualpha);
+        k_site_self<<<(np + 127) / 128, 128>>>(np, ualpha, ewaldfac1, epsfp, dr, daz, dipt, dian, dnapt, dforce, efix);
+        if (kernel_ms) {
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(kernel_ms, a, b);
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(force, dforce, 3 * (size_t)na * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(hfix, efix, sizeof(hfix), cudaMemcpyDeviceToHost);
+    }
+    for (void *p : {(void *)dr, (void *)daz, (void *)dkf, (void *)dkv, (void *)dipt, (void *)dian, (void *)dnapt,
+                    (void *)eik, (void *)part, (void *)sk, (void *)dforce, (void *)efix})
+        if (p) cudaFree(p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return MSG_ERR_CUDA;
+    }
+    // UEwald's sum: reciprocal, atomic and molecular self terms, surface; scaled by EpsiFourPi
+    double u = (double)(long long)hfix[0] * kPFixInv - ualpha / std::sqrt(pi) * q2 + (double)(long long)hfix[2] * kPFixInv;
+    double vr = (double)(long long)hfix[1] * kPFixInv;
+    if (lsurf) {
+        const double fac = 2.0 * pi / (3.0 * vol);
+        const double term = fac * (mx * mx + my * my + mz * mz);
+        u += term;
+        vr -= term;
+        for (int a = 0; a < na; ++a) {
+            force[3 * (size_t)a] -= epsfp * (2.0 * fac) * az[a] * mx;
+            force[3 * (size_t)a + 1] -= epsfp * (2.0 * fac) * az[a] * my;
+            force[3 * (size_t)a + 2] -= epsfp * (2.0 * fac) * az[a] * mz;
+        }
+    }
+    *urec = epsfp * u;
+    *virrec = epsfp * vr;
+    return MSG_OK;
+}

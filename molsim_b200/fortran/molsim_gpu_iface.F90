@@ -152,6 +152,23 @@ module MolsimGpu
          type(c_ptr), value        :: iubuflow, r2umin, utwob, virial, kernel_ms
       end function msg_velver_p
 
+      integer(c_int) function msg_uewald_sites(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, r, az, np, &
+            iptpn, ianpn, napt, npt, force, urec, virrec, kernel_ms) bind(c, name='msg_uewald_sites')
+         import :: c_int, c_int32_t, c_double, c_ptr
+         integer(c_int32_t), value :: na
+         real(c_double), intent(in) :: boxlen(3)
+         real(c_double), value     :: ualpha
+         integer(c_int32_t), value :: ncut, ncutregion, lsurf
+         real(c_double), value     :: epsfp
+         type(c_ptr), value        :: r, az
+         integer(c_int32_t), value :: np
+         type(c_ptr), value        :: iptpn, ianpn, napt
+         integer(c_int32_t), value :: npt
+         type(c_ptr), value        :: force
+         real(c_double), intent(out) :: urec, virrec
+         type(c_ptr), value        :: kernel_ms
+      end function msg_uewald_sites
+
       integer(c_int) function msg_mc_seed(h, isys, iseed) bind(c, name='msg_mc_seed')
          import :: c_int, c_int32_t, c_ptr
          type(c_ptr), value        :: h

@@ -1,5 +1,6 @@
-"""Polyatomic particles: UTwoBodyP (Src/energy.F90:786-896) and the rigid-body MD step
-(VelVer with lpolyatom, Src/md.F90:252-410) on the GPU through the C-ABI (msg_utwobody_p,
+"""Polyatomic particles: UTwoBodyP (Src/energy.F90:786-896), UEwald over the sites
+(Src/energy.F90:905-1104, 1301-1371) and the rigid-body MD step (VelVer with lpolyatom,
+Src/md.F90:252-410) on the GPU through the C-ABI (msg_utwobody_p, msg_uewald_sites,
 msg_velver_p).  The caller's arrays follow MOLSIM's layout (see
 systems.rigid_molecules); the atom-type table comes from engine.pot_tab."""
 import ctypes as C
@@ -74,3 +75,31 @@ def velver_p(s, table, nsteps=1):
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
         s[key] = k[key]
     return dict(utwob=utwob, virial=vir.value, kernel_ms=ms.value)
+
+
+def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
+    """UEwald over the sites of polyatomic system s with site charges az [na]: the standard
+    reciprocal sum with ncut (region 'sphere' or 'cube'), the atomic and molecular self
+    terms and, when lsurf, the surface term.  Returns dict(force [na][3], urec, virrec,
+    kernel_ms), urec and virrec scaled by EpsiFourPi as UEwald does."""
+    r = np.ascontiguousarray(s["r"], np.float64)
+    q = np.ascontiguousarray(az, np.float64)
+    ipt = np.ascontiguousarray(s["iptpn"], np.int32)
+    ian = np.ascontiguousarray(s["ianpn"], np.int32)
+    napt = np.ascontiguousarray(s["napt"], np.int32)
+    na = int(s["na"])
+    if q.shape != (na,):
+        raise ValueError("az must hold one charge per site")
+    force = np.zeros((na, 3))
+    urec = C.c_double()
+    vir = C.c_double()
+    ms = C.c_float()
+    box = (C.c_double * 3)(*s["boxlen"])
+    i32 = C.c_int32
+    rc = _lib.lib().msg_uewald_sites(na, box, float(ualpha), int(ncut), 1 if region == "cube" else 0, int(bool(lsurf)),
+                                     float(s["epsi_four_pi"]), _p(r, C.c_double), _p(q, C.c_double), int(s["np"]),
+                                     _p(ipt, i32), _p(ian, i32), _p(napt, i32), len(napt), _p(force, C.c_double),
+                                     C.byref(urec), C.byref(vir), C.byref(ms))
+    if rc:
+        raise MolsimGpuError(rc, "msg_uewald_sites")
+    return dict(force=force, urec=urec.value, virrec=vir.value, kernel_ms=ms.value)

@@ -1781,3 +1781,82 @@ int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat
     free(ori); free(force); free(forceo); free(torqueo);
     return rc;
 }
+
+/* UEwald over the sites of polyatomic particles (Src/energy.F90:905-958): the standard
+ * reciprocal sum over sites (UEwaldRecStd), UEwaldSelf's atomic and molecular parts
+ * (Src/energy.F90:1301-1345: the intramolecular site pairs' erf(alpha r)/r, with
+ * ErfLocal = Erf2) and the surface term when lsurf.  Sites r [na][3], charges az [na];
+ * particles give the molecules (iptpn, ianpn, napt, 1-based).  force [na][3] is
+ * overwritten with the Ewald forces (kJ/(mol A)); *urec = u%rec, *virrec its virial
+ * (both scaled by EpsiFourPi as UEwald does). */
+int or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
+                    int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                    const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force, double *urec,
+                    double *virrec)
+{
+    static const int32_t one = 1;
+    static const double dummy_buf[12] = {0.0};
+    or_params p;
+    or_sys *s;
+    int32_t *types = malloc(sizeof(int32_t) * (size_t)na);
+    double mass = 1.0, r2u = 0.0, ua = 0.0, utot = 0.0, vir = 0.0;
+    int ia, ip;
+    for (ia = 0; ia < na; ++ia) types[ia] = 1;
+    memset(&p, 0, sizeof(p));
+    p.np = na;
+    p.npt = 1;
+    memcpy(p.boxlen, boxlen, sizeof(double) * 3);
+    p.rcut = 1.0;
+    p.iptpn = types;
+    p.az = az;
+    p.masspt = &mass;
+    p.ubuf = dummy_buf;
+    p.nbuf = 12;
+    p.iubuflow = &one;
+    p.r2umin = &r2u;
+    p.r2atat = &r2u;
+    p.lewald = 2;
+    p.lsurf = lsurf;
+    p.ualpha = ualpha;
+    p.epsi_four_pi = epsfp;
+    p.maxnneigh = 1;
+    p.ncut = ncut;
+    p.ncutregion = ncutregion;
+    s = or_create(&p);
+    or_set_state(s, r, NULL, NULL);
+    for (ia = 0; ia < 3 * na; ++ia) s->force[ia] = 0.0;
+    uewald(s, &ua, &utot, &vir);          /* reciprocal sum, atomic self term, surface */
+    /* UEwaldSelf, molecular contribution: every site pair inside a particle */
+    {
+        const double ewaldfac1 = (1.0 / (sqrt(Pi) * ualpha)) * 2.0 * (ualpha * ualpha);
+        double umol = 0.0;
+        for (ip = 0; ip < np; ++ip) {
+            const int ialow = ianpn[ip] - 1, iaupp = ialow + napt[iptpn[ip] - 1] - 1;
+            int i, j;
+            for (i = ialow; i <= iaupp; ++i)
+                for (j = i + 1; j <= iaupp; ++j) {
+                    const double dx = r[3 * i] - r[3 * j], dy = r[3 * i + 1] - r[3 * j + 1],
+                                 dz = r[3 * i + 2] - r[3 * j + 2];
+                    const double r2 = dx * dx + dy * dy + dz * dz, r1 = sqrt(r2);
+                    double r1i = 1.0 / r1, r2i = r1i * r1i, ex = exp(-(ualpha * ualpha) * r2), r3i, fac;
+                    r1i = r1i * or_erf2(ualpha * r1);
+                    r3i = r2i * (r1i - ewaldfac1 * ex);
+                    umol = umol - (az[i] * az[j] * r1i);
+                    fac = epsfp * az[i] * az[j] * r3i;
+                    s->force[3 * i] -= fac * dx;
+                    s->force[3 * i + 1] -= fac * dy;
+                    s->force[3 * i + 2] -= fac * dz;
+                    s->force[3 * j] += fac * dx;
+                    s->force[3 * j + 1] += fac * dy;
+                    s->force[3 * j + 2] += fac * dz;
+                }
+        }
+        ua = ua + epsfp * umol;
+    }
+    memcpy(force, s->force, sizeof(double) * 3 * (size_t)na);
+    *urec = ua;
+    *virrec = vir;
+    or_destroy(s);
+    free(types);
+    return 0;
+}

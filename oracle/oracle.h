@@ -176,6 +176,13 @@ int    or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t 
                    const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
                    const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial);
 
+/* UEwald over the sites of polyatomic particles: standard reciprocal sum, UEwaldSelf's
+ * atomic and molecular (intramolecular erf) terms, surface term; force [na][3] overwritten. */
+int    or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
+                       int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                       const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force,
+                       double *urec, double *virrec);
+
 #ifdef __cplusplus
 }
 #endif

@@ -400,6 +400,32 @@ def velver_p(s, table, nsteps):
     return dict(utwob=utwob, virial=vir.value)
 
 
+def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
+    """UEwald over the sites of a polyatomic system dict (oracle): dict(force, urec, virrec)."""
+    L = lib()
+    if not getattr(L, "_uewald_sites_typed", False):
+        L.or_uewald_sites.restype = C.c_int
+        L.or_uewald_sites.argtypes = [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                      f64p, f64p, C.c_int32, i32p, i32p, i32p, f64p, f64p, f64p]
+        L._uewald_sites_typed = True
+    r = np.ascontiguousarray(s["r"], np.float64)
+    q = np.ascontiguousarray(az, np.float64)
+    ipt = np.ascontiguousarray(s["iptpn"], np.int32)
+    ian = np.ascontiguousarray(s["ianpn"], np.int32)
+    napt = np.ascontiguousarray(s["napt"], np.int32)
+    force = np.zeros((int(s["na"]), 3))
+    urec = C.c_double()
+    vir = C.c_double()
+    box = (C.c_double * 3)(*s["boxlen"])
+    rc = L.or_uewald_sites(int(s["na"]), box, float(ualpha), int(ncut), 1 if region == "cube" else 0, int(lsurf),
+                           float(s["epsi_four_pi"]), _p(r, C.c_double), _p(q, C.c_double), int(s["np"]),
+                           _p(ipt, C.c_int32), _p(ian, C.c_int32), _p(napt, C.c_int32), _p(force, C.c_double),
+                           C.byref(urec), C.byref(vir))
+    if rc:
+        raise RuntimeError("UEwald over sites failed: %d" % rc)
+    return dict(force=force, urec=urec.value, virrec=vir.value)
+
+
 def random_stream(iseed, n):
     """n successive Random(iseed) values from the first call (Src/mollib.F90:2689-2708)."""
     st = (C.c_int32 * 2)()

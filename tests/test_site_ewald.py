@@ -1,0 +1,160 @@
+"""UEwald over the sites of polyatomic particles (Src/energy.F90:905-958): the standard
+reciprocal sum over sites (UEwaldRecStd, :964-1104), UEwaldSelf's atomic and molecular
+terms (:1301-1345) and UEwaldSurf (:1349-1371), on the GPU (msg_uewald_sites) against
+the oracle.
+
+The oracle's restatement is pinned two ways: in the monoatomic limit (one site per
+particle, no intramolecular pairs) its u%rec and forces are those of the monoatomic
+UTotal with standard Ewald; on rigid three-site molecules the Ewald total (the
+erfc-screened site pairs of UTwoBodyP plus the site sum) does not depend on alpha.
+GPU bars: u%rec within 1e-10 of the self-energy scale EpsiFourPi alpha/sqrt(pi) sum q^2
+(u%rec is a small difference of terms that size), its virial within 1e-10 relative,
+forces within 1e-10 relative RMS (64-bit fixed-point energy sums, structure factors
+summed in a fixed order)."""
+import numpy as np
+import pytest
+
+import helpers as Hp
+import pyoracle as O
+from molsim_b200 import systems as S
+
+
+def _monoatomic_as_polyatomic(s, o):
+    nn, jp = o.get_vlist()
+    n = s["np"]
+    return dict(np=n, na=n, npt=s["npt"], nat=s["npt"], boxlen=s["boxlen"], rcut=s["rcut"], ro=s["ro"], r=s["ro"],
+                iptpn=s["iptpn"], ianpn=np.arange(1, n + 1, dtype=np.int32), napt=np.ones(s["npt"], np.int32),
+                iatan=s["iptpn"], nneighpn=nn, jpnlist=jp, epsi_four_pi=s["epsi_four_pi"])
+
+
+def _site_charges(s):
+    return np.asarray(s["zat"], np.float64)[np.asarray(s["iatan"]) - 1]
+
+
+def _screened_site_table(s, alpha, tol):
+    """The atom-type table of a rigid_molecules system with erfc(alpha r)/r screening."""
+    d = S.site_table_params(s)
+    pot = dict(npt=d["npt"], zat=d["zat"], sigat=d["sigat"], epsat=d["epsat"], rcut=d["rcut"], ualpha=alpha,
+               epsi_four_pi=d["epsi_four_pi"], lewald=1, lljcut=int(d["lljcut"]), utoltab=tol, ftoltab=tol,
+               **{k: d[k] for k in ("ljrcut", "ljushift", "r2uminin", "umaxtab", "fmaxtab", "rumaxfac")})
+    return O.pot_tab(pot)
+
+
+def _self_scale(s, az, alpha):
+    return s["epsi_four_pi"] * alpha / np.sqrt(np.pi) * float(np.sum(np.asarray(az) ** 2))
+
+
+def _molecules():
+    return S.rigid_molecules(seed=3, nmol=120, nsolute=0, L=24.0, rcut=11.0)
+
+
+@pytest.mark.parametrize("lsurf", [False, True])
+def test_monoatomic_limit_equals_utotal_std(lsurf):
+    s = Hp.std_ewald(Hp.electrolyte_small(lsurf=lsurf), ncut=8)
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    ref = o.utotal()
+    p = _monoatomic_as_polyatomic(s, o)
+    pair = O.utwobody_p(p, t)
+    e = O.uewald_sites(p, s["az"], t["ualpha"], t["ncut"], lsurf=lsurf)
+    assert e["urec"] == pytest.approx(ref["urec"], rel=1e-14, abs=1e-12)
+    assert Hp.rel_rms(pair["force"] + e["force"], ref["force"]) < 1e-13
+
+
+def test_ewald_total_is_independent_of_alpha():
+    """Site pairs screened with erfc(alpha r)/r (table tolerance 1e-7) plus the site Ewald sum:
+    the total energy of 120 rigid three-site molecules agrees across alpha within 1e-3 kJ/mol
+    (about 5e-6 relative; without the molecular self term it would move by hundreds of kJ/mol),
+    the forces within 1e-3 of their largest, and the net force vanishes."""
+    s = _molecules()
+    az = _site_charges(s)
+    assert abs(az.sum()) < 1e-12
+    tot, forces = [], []
+    for alpha, ncut in ((0.35, 16), (0.45, 20)):
+        pair = O.utwobody_p(s, _screened_site_table(s, alpha, 1e-7))
+        e = O.uewald_sites(s, az, alpha, ncut)
+        f = pair["force"] + e["force"]
+        assert np.abs(f.sum(0)).max() <= 1e-10 * np.abs(f).max()
+        tot.append(pair["utwob"][0] + e["urec"])
+        forces.append(f)
+    assert abs(tot[0] - tot[1]) < 1e-3, tot
+    assert np.abs(forces[0] - forces[1]).max() < 1e-3 * np.abs(forces[0]).max()
+
+
+def test_bad_arguments_are_refused_on_the_host():
+    from molsim_b200.engine import MolsimGpuError
+    from molsim_b200.polyatomic import uewald_sites
+
+    s = dict(_molecules())
+    az = _site_charges(s)
+    with pytest.raises(MolsimGpuError) as ei:
+        uewald_sites(s, az, 0.35, 0)
+    assert ei.value.code == 6
+    with pytest.raises(MolsimGpuError) as ei:
+        uewald_sites(s, az, 0.35, 101)
+    assert ei.value.code == 6
+    ian = np.array(s["ianpn"], np.int32)
+    ian[-1] = s["na"]                        # the last particle's sites run past na
+    bad = dict(s)
+    bad["ianpn"] = ian
+    with pytest.raises(MolsimGpuError) as ei:
+        uewald_sites(bad, az, 0.35, 8)
+    assert ei.value.code == 6
+    with pytest.raises(ValueError):
+        uewald_sites(s, az[:-1], 0.35, 8)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("region,lsurf", [("sphere", False), ("cube", True)])
+def test_gpu_matches_oracle(region, lsurf):
+    from molsim_b200.polyatomic import uewald_sites
+
+    s = _molecules()
+    az = _site_charges(s)
+    ref = O.uewald_sites(s, az, 0.35, 12, region=region, lsurf=lsurf)
+    got = uewald_sites(s, az, 0.35, 12, region=region, lsurf=lsurf)
+    assert abs(got["urec"] - ref["urec"]) <= 1e-10 * _self_scale(s, az, 0.35)
+    assert got["virrec"] == pytest.approx(ref["virrec"], rel=1e-10)
+    assert Hp.rel_rms(got["force"], ref["force"]) < 1e-10
+    again = uewald_sites(s, az, 0.35, 12, region=region, lsurf=lsurf)
+    assert again["urec"] == got["urec"] and np.array_equal(again["force"], got["force"])
+
+
+@pytest.mark.gpu
+def test_gpu_monoatomic_limit_matches_the_handle():
+    """One site per particle: the GPU site sum plus the GPU site pairs give the FP64
+    handle's UTotal with standard Ewald."""
+    from molsim_b200 import Engine
+    from molsim_b200.polyatomic import uewald_sites, utwobody_p
+
+    s = Hp.std_ewald(Hp.electrolyte_small(lsurf=True), ncut=8)
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    p = _monoatomic_as_polyatomic(s, o)
+    pair = utwobody_p(p, t)
+    e = uewald_sites(p, s["az"], t["ualpha"], t["ncut"], lsurf=True)
+    g = Engine(s, t, precision="fp64").UTotal()
+    assert abs(e["urec"] - g["urec"]) <= 1e-10 * _self_scale(s, s["az"], t["ualpha"])
+    assert Hp.rel_rms(pair["force"] + e["force"], g["force"]) < 1e-10
+
+
+@pytest.mark.gpu
+def test_gpu_large_system_net_force_and_alpha():
+    """4000 molecules (12000 sites, several site chunks of the structure-factor sum): the
+    net force is zero and the GPU's Ewald total agrees across alpha as the oracle's does."""
+    from molsim_b200.polyatomic import uewald_sites, utwobody_p
+
+    s = S.rigid_molecules(seed=5, nmol=4000, nsolute=0, L=75.0, rcut=11.0)
+    az = _site_charges(s)
+    tot = []
+    for alpha, ncut in ((0.35, 40), (0.45, 52)):
+        pair = utwobody_p(s, _screened_site_table(s, alpha, 1e-7))
+        e = uewald_sites(s, az, alpha, ncut)
+        f = pair["force"] + e["force"]
+        assert np.abs(f.sum(0)).max() <= 1e-9 * np.abs(f).max()
+        tot.append(pair["utwob"][0] + e["urec"])
+    assert abs(tot[0] - tot[1]) <= 5e-6 * abs(tot[0]), tot
