@@ -622,7 +622,10 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
 namespace {
 
 constexpr int kSK = 128;                  // k-vectors per structure-factor block
-constexpr int kSChunk = 512;              // sites per partial sum
+constexpr int kSF = 128;                  // sites per force block
+constexpr int kSFTile = 256;              // k-vectors staged per shared-memory round of k_site_force
+constexpr int kSMaxCut = 100;             // largest ncut accepted
+constexpr int kSSmem = 48 * 1024;         // k_site_sk's staged tables stay within the default limit
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b)
 {
@@ -654,27 +657,40 @@ __global__ void k_site_eik(int na, int w, double3 tpbi, const double *__restrict
 }
 
 // Partial structure factors of (k tile blockIdx.x, site chunk blockIdx.y): part[chunk][k][4].
-__global__ void __launch_bounds__(kSK) k_site_sk(int na, int nkv, int w, const int4 *__restrict__ kv,
-                                                 const double2 *__restrict__ eik, double2 *__restrict__ part)
+// The chunk's sites pass through shared memory `sub` at a time (their tables, sub*3*w double2).
+__global__ void __launch_bounds__(kSK) k_site_sk(int na, int nkv, int w, int clen, int sub,
+                                                 const int4 *__restrict__ kv, const double2 *__restrict__ eik,
+                                                 double2 *__restrict__ part)
 {
+    extern __shared__ double2 stab[];
     const int kn = blockIdx.x * kSK + threadIdx.x;
-    if (kn >= nkv) return;
-    const int4 n = kv[kn];
-    const int a0 = blockIdx.y * kSChunk, a1 = min(na, a0 + kSChunk);
+    const bool on = kn < nkv;
+    const int4 n = on ? kv[kn] : make_int4(0, 0, 0, 0);
+    const int a0 = blockIdx.y * clen, a1 = min(na, a0 + clen);
     double2 s[4];
     for (int c = 0; c < 4; ++c) s[c] = make_double2(0.0, 0.0);
-    for (int ia = a0; ia < a1; ++ia) {
-        const double2 *t = eik + (size_t)ia * 3 * w;
-        const double2 qx = t[n.x], ey = t[w + n.y], ez = t[2 * w + n.z];
-        const double2 yzm = zmul(zconj(ey), ez), yzp = zmul(ey, ez), qxc = zconj(qx);
-        const double2 v[4] = {zmul(qxc, yzm), zmul(qxc, yzp), zmul(qx, yzm), zmul(qx, yzp)};
-        for (int c = 0; c < 4; ++c) {
-            s[c].x += v[c].x;
-            s[c].y += v[c].y;
-        }
+    for (int q0 = a0; q0 < a1; q0 += sub) {
+        const int nq = min(sub, a1 - q0);
+        const double2 *src = eik + (size_t)q0 * 3 * w;
+        __syncthreads();
+        for (int e = threadIdx.x; e < nq * 3 * w; e += kSK) stab[e] = src[e];
+        __syncthreads();
+        if (on)
+            for (int p = 0; p < nq; ++p) {
+                const double2 *t = stab + (size_t)p * 3 * w;
+                const double2 qx = t[n.x], ey = t[w + n.y], ez = t[2 * w + n.z];
+                const double2 yzm = zmul(zconj(ey), ez), yzp = zmul(ey, ez), qxc = zconj(qx);
+                const double2 v0 = zmul(qxc, yzm), v1 = zmul(qxc, yzp), v2 = zmul(qx, yzm), v3 = zmul(qx, yzp);
+                s[0].x += v0.x; s[0].y += v0.y;
+                s[1].x += v1.x; s[1].y += v1.y;
+                s[2].x += v2.x; s[2].y += v2.y;
+                s[3].x += v3.x; s[3].y += v3.y;
+            }
     }
-    double2 *o = part + ((size_t)blockIdx.y * nkv + kn) * 4;
-    for (int c = 0; c < 4; ++c) o[c] = s[c];
+    if (on) {
+        double2 *o = part + ((size_t)blockIdx.y * nkv + kn) * 4;
+        for (int c = 0; c < 4; ++c) o[c] = s[c];
+    }
 }
 
 // S(k) = the chunks in order; energy kfac |S|^2 and virial -(1 - k^2/2alpha^2) kfac |S|^2
@@ -717,32 +733,94 @@ __global__ void __launch_bounds__(kSK) k_site_reduce(int nkv, int nchunk, double
     }
 }
 
-// Reciprocal force of each site over every k-vector, in the reference's order
-// (Src/energy.F90:1078-1092): F += kfac2 k (combinations of Im(eikr conj S)).
-__global__ void k_site_force(int na, int nkv, int w, double epsfp, double3 tpbi, const int4 *__restrict__ kv,
-                             const double *__restrict__ kfac, const double2 *__restrict__ sk,
-                             const double2 *__restrict__ eik, double *__restrict__ force)
+// Reciprocal force of the sites of block blockIdx.x over the k-vector slice blockIdx.y
+// (klen k-vectors), in the reference's order (Src/energy.F90:1078-1092):
+// F += kfac2 k (combinations of Im(eikr conj S)).  The k-vectors, kfac and S(k) pass
+// through shared memory a tile at a time; each site advances its exponentials by
+// EwaldSetArray's recurrence e(n) = e(n-1) e(1), so they equal the tables' entries.
+// Output fks[slice][site][3]; k_site_fsum adds the slices in order.
+__global__ void __launch_bounds__(kSF) k_site_force(int na, int nkv, int klen, double epsfp, double3 tpbi,
+                                                    const double *__restrict__ r, const double *__restrict__ az,
+                                                    const int4 *__restrict__ kv, const double *__restrict__ kfac,
+                                                    const double2 *__restrict__ sk, double *__restrict__ fks)
 {
-    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ia >= na) return;
-    const double2 *t = eik + (size_t)ia * 3 * w;
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int kn = 0; kn < nkv; ++kn) {
-        const int4 n = kv[kn];
-        const double2 qx = t[n.x], ey = t[w + n.y], ez = t[2 * w + n.z];
-        const double2 yzm = zmul(zconj(ey), ez), yzp = zmul(ey, ez), qxc = zconj(qx);
-        const double2 r0 = zmul(qxc, yzm), r1 = zmul(qxc, yzp), r2 = zmul(qx, yzm), r3 = zmul(qx, yzp);
-        const double2 *S = sk + (size_t)kn * 4;
-        const double fmm = -r0.x * S[0].y + r0.y * S[0].x, fmp = -r1.x * S[1].y + r1.y * S[1].x;
-        const double fpm = -r2.x * S[2].y + r2.y * S[2].x, fpp = -r3.x * S[3].y + r3.y * S[3].x;
-        const double kf2 = epsfp * 2.0 * kfac[kn];
-        fx += (kf2 * n.x * tpbi.x) * (-fmm - fmp + fpm + fpp);
-        fy += (kf2 * n.y * tpbi.y) * (-fmm + fmp - fpm + fpp);
-        fz += (kf2 * n.z * tpbi.z) * (fmm + fmp + fpm + fpp);
+    __shared__ int4 skv[kSFTile];
+    __shared__ double2 ssk[kSFTile][4];
+    __shared__ double3 skk[kSFTile];        // kfac2 n 2pi/L per component, as the reference forms it
+    const int ia = blockIdx.x * kSF + threadIdx.x;
+    const bool on = ia < na;
+    const int k0 = blockIdx.y * klen, k1 = min(nkv, k0 + klen);
+    double x[3] = {0.0, 0.0, 0.0}, q = 0.0;
+    if (on) {
+        for (int m = 0; m < 3; ++m) x[m] = r[3 * (size_t)ia + m];
+        q = az[ia];
     }
-    force[3 * (size_t)ia] = fx;
-    force[3 * (size_t)ia + 1] = fy;
-    force[3 * (size_t)ia + 2] = fz;
+    const double tp[3] = {tpbi.x, tpbi.y, tpbi.z};
+    double2 e1[3];
+    for (int m = 0; m < 3; ++m) {
+        double sn, cs;
+        sincos(tp[m] * x[m], &sn, &cs);
+        e1[m] = make_double2(cs, sn);
+    }
+    double2 ex = make_double2(1.0, 0.0), ey = ex, ez = ex, yzm = ex, yzp = ex;
+    int cx = 0, cy = 0, cz = 0, row = -1;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int t0 = k0; t0 < k1; t0 += kSFTile) {
+        const int nt = min(kSFTile, k1 - t0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nt; e += kSF) {
+            const size_t g = (size_t)t0 + e;
+            const int4 n = kv[g];
+            const double kf2 = epsfp * 2.0 * kfac[g];
+            skv[e] = n;
+            skk[e] = make_double3(kf2 * n.x * tp[0], kf2 * n.y * tp[1], kf2 * n.z * tp[2]);
+            for (int c = 0; c < 4; ++c) ssk[e][c] = sk[g * 4 + c];
+        }
+        __syncthreads();
+        for (int e = 0; e < nt; ++e) {
+            const int4 n = skv[e];
+            const int key = n.z * (kSMaxCut + 1) + n.y;
+            if (key != row) {
+                if (n.z != cz) {
+                    while (cz < n.z) { ez = (cz == 0) ? e1[2] : zmul(ez, e1[2]); ++cz; }
+                    ey = make_double2(1.0, 0.0);
+                    cy = 0;
+                }
+                while (cy < n.y) { ey = (cy == 0) ? e1[1] : zmul(ey, e1[1]); ++cy; }
+                yzm = zmul(zconj(ey), ez);
+                yzp = zmul(ey, ez);
+                ex = make_double2(1.0, 0.0);
+                cx = 0;
+                row = key;
+            }
+            while (cx < n.x) { ex = (cx == 0) ? e1[0] : zmul(ex, e1[0]); ++cx; }
+            const double2 qx = make_double2(q * ex.x, q * ex.y), qxc = zconj(qx);
+            const double2 r0 = zmul(qxc, yzm), r1 = zmul(qxc, yzp), r2 = zmul(qx, yzm), r3 = zmul(qx, yzp);
+            const double2 s0 = ssk[e][0], s1 = ssk[e][1], s2 = ssk[e][2], s3 = ssk[e][3];
+            const double fmm = -r0.x * s0.y + r0.y * s0.x, fmp = -r1.x * s1.y + r1.y * s1.x;
+            const double fpm = -r2.x * s2.y + r2.y * s2.x, fpp = -r3.x * s3.y + r3.y * s3.x;
+            const double3 K = skk[e];
+            fx += K.x * (-fmm - fmp + fpm + fpp);
+            fy += K.y * (-fmm + fmp - fpm + fpp);
+            fz += K.z * (fmm + fmp + fpm + fpp);
+        }
+    }
+    if (on) {
+        double *o = fks + ((size_t)blockIdx.y * na + ia) * 3;
+        o[0] = fx;
+        o[1] = fy;
+        o[2] = fz;
+    }
+}
+
+// force[site] = the k slices' forces added in slice order.
+__global__ void k_site_fsum(int na, int nks, const double *__restrict__ fks, double *__restrict__ force)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * na) return;
+    double f = 0.0;
+    for (int k = 0; k < nks; ++k) f += fks[(size_t)k * 3 * na + i];
+    force[i] = f;
 }
 
 // UEwaldSelf's molecular term (Src/energy.F90:1315-1343): every site pair inside a
@@ -787,7 +865,7 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
                                 const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
                                 double *force, double *urec, double *virrec, float *kernel_ms)
 {
-    if (na < 1 || np < 1 || npt < 1 || ncut < 1 || ncut > 100 || ncutregion < 0 || ncutregion > 1 ||
+    if (na < 1 || np < 1 || npt < 1 || ncut < 1 || ncut > kSMaxCut || ncutregion < 0 || ncutregion > 1 ||
         !(ualpha > 0.0) || !boxlen || !r || !az || !iptpn || !ianpn || !napt || !force || !urec || !virrec)
         return MSG_ERR_ARG;
     for (int t = 0; t < npt; ++t)
@@ -812,7 +890,16 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
                 kf.push_back(2.0 * pi / vol * facz * facy * facx * std::exp(-k2 / (4.0 * (ualpha * ualpha))) / k2);
                 kv.push_back(make_int4(nx, ny, nz, 0));
             }
-    const int nkv = (int)kv.size(), w = ncut + 1, nchunk = (na + kSChunk - 1) / kSChunk;
+    const int nkv = (int)kv.size(), w = ncut + 1;
+    // site chunks of the structure-factor sum (about eight blocks per SM of a 148-SM B200, a
+    // chunk at least 128 sites) and k slices of the force sum (about four blocks per SM, a slice
+    // at least 16 k-vectors): from the system's sizes only, so the sums repeat bit for bit
+    const int ktiles = (nkv + kSK - 1) / kSK, ptiles = (na + kSF - 1) / kSF;
+    const int nch = std::max(1, std::min((8 * 148 + ktiles - 1) / ktiles, (na + 127) / 128));
+    const int clen = (na + nch - 1) / nch, nchunk = (na + clen - 1) / clen;
+    const int nks0 = std::max(1, std::min((4 * 148 + ptiles - 1) / ptiles, std::max(1, nkv / 16)));
+    const int klen = (nkv + nks0 - 1) / nks0, nks = (nkv + klen - 1) / klen;
+    const int sub = std::max(1, std::min(16, kSSmem / (3 * w * (int)sizeof(double2))));
     // the surface term on the host (UEwaldSurf, Src/energy.F90:1349-1371)
     double mx = 0.0, my = 0.0, mz = 0.0, q2 = 0.0;
     for (int a = 0; a < na; ++a) {
@@ -826,12 +913,13 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
     int4 *dkv = dev_copy(kv.data(), kv.size(), e);
     int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e), *dnapt = dev_copy(napt, (size_t)npt, e);
     double2 *eik = nullptr, *part = nullptr, *sk = nullptr;
-    double *dforce = nullptr;
+    double *dforce = nullptr, *fks = nullptr;
     unsigned long long *efix = nullptr;
     if (e == cudaSuccess) e = cudaMalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&fks, (size_t)nks * 3 * na * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&efix, 3 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(efix, 0, 3 * sizeof(unsigned long long));
     unsigned long long hfix[3] = {0, 0, 0};
@@ -843,9 +931,11 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
             cudaEventRecord(a, 0);
         }
         k_site_eik<<<(na + 127) / 128, 128>>>(na, w, tpbi, dr, daz, eik);
-        k_site_sk<<<dim3((nkv + kSK - 1) / kSK, nchunk), kSK>>>(na, nkv, w, dkv, eik, part);
-        k_site_reduce<<<(nkv + kSK - 1) / kSK, kSK>>>(nkv, nchunk, ualpha * ualpha, tpbi, dkv, dkf, part, sk, efix);
-        k_site_force<<<(na + 127) / 128, 128>>>(na, nkv, w, epsfp, tpbi, dkv, dkf, sk, eik, dforce);
+        k_site_sk<<<dim3(ktiles, nchunk), kSK, (size_t)sub * 3 * w * sizeof(double2)>>>(na, nkv, w, clen, sub, dkv,
+                                                                                    eik, part);
+        k_site_reduce<<<ktiles, kSK>>>(nkv, nchunk, ualpha * ualpha, tpbi, dkv, dkf, part, sk, efix);
+        k_site_force<<<dim3(ptiles, nks), kSF>>>(na, nkv, klen, epsfp, tpbi, dr, daz, dkv, dkf, sk, fks);
+        k_site_fsum<<<(3 * na + 255) / 256, 256>>>(na, nks, fks, dforce);
         const double ewaldfac1 = (1.0 / (std::sqrt(pi) * ualpha)) * 2.0 * (ualpha * ualpha);
         k_site_self<<<(np + 127) / 128, 128>>>(np, ualpha, ewaldfac1, epsfp, dr, daz, dipt, dian, dnapt, dforce, efix);
         if (kernel_ms) {
@@ -860,7 +950,7 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
         if (e == cudaSuccess) e = cudaMemcpy(hfix, efix, sizeof(hfix), cudaMemcpyDeviceToHost);
     }
     for (void *p : {(void *)dr, (void *)daz, (void *)dkf, (void *)dkv, (void *)dipt, (void *)dian, (void *)dnapt,
-                    (void *)eik, (void *)part, (void *)sk, (void *)dforce, (void *)efix})
+                    (void *)eik, (void *)part, (void *)sk, (void *)dforce, (void *)fks, (void *)efix})
         if (p) cudaFree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
