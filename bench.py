@@ -587,6 +587,31 @@ def run_poly(a):
                               "unit": "site k-vector terms/s", "cores": 1, "kind": "port",
                               "sample": "one site Ewald sum of 1000 molecules (3000 sites, L = 47 A, ncut = 25), "
                                         "oracle, 1 thread"}
+    # the rigid-body MD step with the site Ewald sum: 4000 molecules + 1000 solutes (13000 sites)
+    re_ = S.rigid_bodies(seed=0, nmol=4000, nsolute=1000, L=85.0, rcut=10.0, drnlist=2.0, tstep=0.001)
+    dre = S.site_table_params(re_)
+    dre["lewald"] = 1
+    tre = pot_tab(dre, 0.35)
+    ewp = dict(az=np.asarray(re_["zat"], np.float64)[np.asarray(re_["iatan"]) - 1], ualpha=0.35, ncut=45)
+    velver_p(copy.deepcopy(re_), tre, 2, ewald=ewp)     # warm-up
+    k = 10
+    ms = velver_p(copy.deepcopy(re_), tre, k, ewald=ewp)["kernel_ms"]
+    mde = {"workload": "4000 rigid 3-site molecules + 1000 solutes (13000 sites), L = 85 A, rc = 10 A, "
+                       "site Ewald alpha = 0.35, ncut = 45, dt = 1 fs",
+           "steps": k, "ms_per_step": ms / k, "value": re_["np"] * k / (ms / 1000.0), "unit": METRIC}
+    if not a.no_cpu_baseline:
+        rs = S.rigid_bodies(seed=0, nmol=1000, nsolute=250, L=52.0, rcut=10.0, drnlist=2.0, tstep=0.001)
+        drs = S.site_table_params(rs)
+        drs["lewald"] = 1
+        trs = pot_tab(drs, 0.35)
+        ews = dict(az=np.asarray(rs["zat"], np.float64)[np.asarray(rs["iatan"]) - 1], ualpha=0.35, ncut=28)
+        t0 = time.perf_counter()
+        O.velver_p(rs, trs, 2, ewald=ews)
+        mde["cpu_baseline"] = {"value": rs["np"] * 2 / (time.perf_counter() - t0), "unit": METRIC, "cores": 1,
+                               "kind": "port",
+                               "sample": "two rigid-body steps with site Ewald of 1000 molecules + 250 solutes "
+                                         "(L = 52 A, ncut = 28), oracle, 1 thread"}
+    ew["rigid_md_ewald_5000"] = mde
     out["uewald_sites_12000"] = ew
     return out
 

@@ -25,6 +25,8 @@
  *   msg_utwobody_p                 -> UTwoBodyP (Src/energy.F90:786-896), polyatomic particles
  *   msg_velver_p                   -> MDDriver with VelVer for rigid polyatomic particles
  *                                     (Src/md.F90:252-410, 628-663)
+ *   msg_velver_p_ewald             -> the same steps with lewald: UTotal's UEwald over the sites
+ *                                     (Src/energy.F90:335-352) in every step's forces and virial
  *   msg_uewald_sites               -> UEwald over the sites of polyatomic particles: UEwaldRecStd,
  *                                     UEwaldSelf with its molecular term, UEwaldSurf
  *                                     (Src/energy.F90:905-1104, 1301-1371)
@@ -329,6 +331,21 @@ int  msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t
                       int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
                       const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
                       double *force, double *urec, double *virrec, float *kernel_ms);
+
+/* msg_velver_p with lewald: every step adds the site Ewald sum of msg_uewald_sites (site
+ * charges az [na], ualpha, ncut, ncutregion, lsurf, epsfp) to the site forces before the
+ * forces, torques and molecular virial (UTotal, Src/energy.F90:335-352, 403-426), and its
+ * reciprocal virial to virial; urec = u%rec of the last step.  The table ubuf carries the
+ * erfc-screened site pairs (lewald in PotTwoBodyTab).  MSG_ERR_ARG as msg_uewald_sites. */
+int  msg_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                        double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
+                        double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
+                        const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
+                        int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
+                        const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                        const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha,
+                        int32_t ncut, int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob, double *urec,
+                        double *virial, float *kernel_ms);
 
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,

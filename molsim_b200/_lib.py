@@ -71,6 +71,11 @@ SIGNATURES = {
     "msg_velver_p": (C.c_int, [C.c_int32] * 5 + [f64p, C.c_double, C.c_double, C.c_int32, C.c_double] + [f64p] * 7 +
                      [i32p] * 4 + [f64p, C.c_int32, f64p, f64p, i32p, i32p, C.c_int32, f64p, C.c_int32, i32p, f64p,
                                    f64p, f64p, C.POINTER(C.c_float)]),
+    "msg_velver_p_ewald": (C.c_int, [C.c_int32] * 5 + [f64p, C.c_double, C.c_double, C.c_int32, C.c_double] +
+                           [f64p] * 7 + [i32p] * 4 + [f64p, C.c_int32, f64p, f64p, i32p, i32p, C.c_int32, f64p,
+                                                      C.c_int32, i32p, f64p, f64p, C.c_double, C.c_int32,
+                                                      C.c_int32, C.c_int32, C.c_double, f64p, f64p, f64p,
+                                                      C.POINTER(C.c_float)]),
     "msg_utwobody_p": (C.c_int, [C.c_int32] * 4 + [f64p, C.c_double, f64p, f64p] + [i32p] * 6 +
                        [C.c_int32, f64p, C.c_int32, i32p, f64p, f64p, f64p, f64p, C.POINTER(C.c_float)]),
     "msg_uewald_sites": (C.c_int, [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double, f64p,

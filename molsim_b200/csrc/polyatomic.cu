@@ -475,145 +475,6 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
     return MSG_OK;
 }
 
-extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
-                            double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
-                            double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
-                            const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
-                            int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
-                            const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
-                            const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial,
-                            float *kernel_ms)
-{
-    if (nsteps < 0 || np < 1 || na < 1 || npt < 1 || npt > kPMaxType || nat < 1 || maxsite < 1 || maxsite > 256 ||
-        maxnneigh < 1 || nbuf < 12 ||
-        nvvite < 0 || !boxlen || !ro || !rod || !rodd || !qua || !quad || !quadd || !r || !iptpn || !ianpn ||
-        !napt || !iatan || !ra || !masspt || !momp || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin ||
-        !utwob || !virial)
-        return MSG_ERR_ARG;
-    for (int t = 0; t < npt; ++t)
-        if (napt[t] < 1 || napt[t] > maxsite || !(masspt[t] > 0.0) || !(momp[3 * t] > 0.0) || !(momp[3 * t + 1] > 0.0) ||
-            !(momp[3 * t + 2] > 0.0))
-            return MSG_ERR_ARG;
-    for (int i = 0; i < np; ++i) {
-        if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na)
-            return MSG_ERR_ARG;
-        if (nneighpn[i] < 0 || nneighpn[i] > maxnneigh) return MSG_ERR_ARG;
-        for (int k = 0; k < nneighpn[i]; ++k) {
-            const int j = jpnlist[(size_t)i * maxnneigh + k];
-            if (j < 1 || j > np) return MSG_ERR_ARG;
-        }
-    }
-    const int natat = nat * (nat + 1) / 2, nptpt = npt * (npt + 1) / 2;
-    for (int a = 0; a < na; ++a)
-        if (iatan[a] < 1 || iatan[a] > nat) return MSG_ERR_ARG;
-    for (int q = 0; q < natat; ++q)
-        if (iubuflow[q] < 1 || iubuflow[q] + 11 > nbuf) return MSG_ERR_ARG;
-    RigidArgs A;
-    A.np = np;
-    A.nvvite = nvvite;
-    A.tstep = tstep;
-    A.tvvite = tvvite;
-    A.fac = 0.5 * tstep * tstep;
-    for (int m = 0; m < 3; ++m) {
-        A.box[m] = boxlen[m];
-        A.half[m] = boxlen[m] / 2.0;
-        A.boxi[m] = 1.0 / boxlen[m];
-    }
-    A.maxsite = maxsite;
-    {
-        // (sclene / scllen) / sclfor with MOLSIM's scales (Src/molsim.F90:786-805)
-        const double scllen = 1.0e-10, sclmas = 1.0e-03, scltim = 1.0e-12, sclene = 1.0e+03;
-        const double sclvel = scllen / scltim, sclacc = sclvel / scltim;
-        A.ffac = (sclene / scllen) / (sclacc * sclmas);
-    }
-    cudaError_t e = cudaSuccess;
-    double *dro = dev_copy(ro, 3 * (size_t)np, e), *drod = dev_copy(rod, 3 * (size_t)np, e),
-           *drodd = dev_copy(rodd, 3 * (size_t)np, e), *dqua = dev_copy(qua, 4 * (size_t)np, e),
-           *dquad = dev_copy(quad, 4 * (size_t)np, e), *dquadd = dev_copy(quadd, 4 * (size_t)np, e),
-           *dr = dev_copy(r, 3 * (size_t)na, e), *dra = dev_copy(ra, 3 * (size_t)npt * maxsite, e),
-           *dmass = dev_copy(masspt, (size_t)npt, e), *dmom = dev_copy(momp, 3 * (size_t)npt, e);
-    int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e);
-    int *dnapt = dev_copy(napt, (size_t)npt, e), *diat = dev_copy(iatan, (size_t)na, e);
-    int *dnn = dev_copy(nneighpn, (size_t)np, e), *djp = dev_copy(jpnlist, (size_t)np * maxnneigh, e);
-    double *dub = dev_copy(ubuf, (size_t)nbuf, e), *dr2 = dev_copy(r2umin, (size_t)natat, e);
-    int *diub = dev_copy(iubuflow, (size_t)natat, e);
-    std::vector<SiteBuckets> hsb;
-    std::vector<int> hbs;
-    site_buckets(natat, ubuf, nbuf, iubuflow, r2umin, hsb, hbs);
-    SiteBuckets *dsb = dev_copy(hsb.data(), hsb.size(), e);
-    int *dbs = dev_copy(hbs.data(), hbs.size(), e);
-    unsigned long long *ffix = nullptr;
-    double *dforce = nullptr, *duv = nullptr, *dori = nullptr;
-    int *derr = nullptr;
-    const size_t nfix = 3 * (size_t)na + nptpt + 2;           // site forces, energies, pair and molecular virial
-    if (e == cudaSuccess) e = cudaMalloc(&ffix, nfix * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&duv, (nptpt + 2) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&dori, 9 * (size_t)np * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
-    int herr = 0;
-    double vmol = 0.0;
-    if (e == cudaSuccess && nsteps > 0) {
-        unsigned long long *ufix = ffix + 3 * (size_t)na, *vfix = ufix + nptpt, *vmfix = vfix + 1;
-        cudaEvent_t a = nullptr, b = nullptr;
-        if (kernel_ms) {
-            cudaEventCreate(&a);
-            cudaEventCreate(&b);
-            cudaEventRecord(a, 0);
-        }
-        const int pb = (np + 127) / 128;
-        for (int step = 0; step < nsteps; ++step) {
-            cudaMemsetAsync(ffix, 0, nfix * sizeof(unsigned long long), 0);
-            k_rigid_move<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dipt, dian, dnapt, dra);
-            k_utwobody_p<<<(np + kPWarps - 1) / kPWarps, kPThreads, site_smem(npt, napt)>>>(
-                np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut, dro, dr, dipt, dian, dnapt,
-                diat, dnn, djp, maxnneigh, dub, nbuf, diub, dr2, dsb, dbs, max_sites(npt, napt), ffix, ufix, vfix, derr);
-            k_utwobody_p_out<<<(int)((3 * (size_t)na + 255) / 256), 256>>>(na, nptpt, ffix, ufix, vfix, dforce, duv);
-            k_rigid_kick<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dforce, dipt, dian, dnapt,
-                                      dmass, dmom, vmfix);
-        }
-        if (kernel_ms) {
-            cudaEventRecord(b, 0);
-            cudaEventSynchronize(b);
-            cudaEventElapsedTime(kernel_ms, a, b);
-            cudaEventDestroy(a);
-            cudaEventDestroy(b);
-        }
-        e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
-        unsigned long long vm = 0;
-        if (e == cudaSuccess) e = cudaMemcpy(&vm, vmfix, sizeof(vm), cudaMemcpyDeviceToHost);
-        vmol = (double)(long long)vm * kPFixInv;
-    }
-    if (e == cudaSuccess && !herr) {
-        std::vector<double> uv(nptpt + 2, 0.0);
-        if (nsteps > 0) e = cudaMemcpy(uv.data(), duv, uv.size() * sizeof(double), cudaMemcpyDeviceToHost);
-        struct Back { double *h, *d; size_t n; } back[] = {
-            {ro, dro, 3 * (size_t)np}, {rod, drod, 3 * (size_t)np}, {rodd, drodd, 3 * (size_t)np},
-            {qua, dqua, 4 * (size_t)np}, {quad, dquad, 4 * (size_t)np}, {quadd, dquadd, 4 * (size_t)np},
-            {r, dr, 3 * (size_t)na}};
-        for (const Back &x : back)
-            if (e == cudaSuccess) e = cudaMemcpy(x.h, x.d, x.n * sizeof(double), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess && nsteps > 0) {
-            for (int q = 0; q <= nptpt; ++q) utwob[q] = uv[q];
-            *virial = uv[nptpt + 1] + vmol;
-        }
-    }
-    for (void *p : {(void *)dro, (void *)drod, (void *)drodd, (void *)dqua, (void *)dquad, (void *)dquadd, (void *)dr,
-                    (void *)dra, (void *)dmass, (void *)dmom, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat,
-                    (void *)dnn, (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)dsb, (void *)dbs,
-                    (void *)ffix, (void *)dforce, (void *)duv, (void *)dori, (void *)derr})
-        if (p) cudaFree(p);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return MSG_ERR_CUDA;
-    }
-    if (herr == 1) return MSG_ERR_TABLE_MIN;
-    if (herr == 2) return MSG_ERR_TABLE_RANGE;
-    return MSG_OK;
-}
-
 // ---------------------------------------------------------------------------
 // UEwald over the sites of polyatomic particles (Src/energy.F90:905-958 with the
 // standard reciprocal sum, UEwaldRecStd :964-1104, and UEwaldSelf's atomic and
@@ -626,6 +487,9 @@ constexpr int kSF = 128;                  // sites per force block
 constexpr int kSFTile = 256;              // k-vectors staged per shared-memory round of k_site_force
 constexpr int kSMaxCut = 100;             // largest ncut accepted
 constexpr int kSSmem = 48 * 1024;         // k_site_sk's staged tables stay within the default limit
+// the dipole sum of the surface term in 64-bit fixed point at 2^-32: |sum q r| up to 2e9
+constexpr double kDipFix = 4294967296.0;
+constexpr double kDipFixInv = 1.0 / 4294967296.0;
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b)
 {
@@ -813,14 +677,37 @@ __global__ void __launch_bounds__(kSF) k_site_force(int na, int nkv, int klen, d
     }
 }
 
-// force[site] = the k slices' forces added in slice order.
-__global__ void k_site_fsum(int na, int nks, const double *__restrict__ fks, double *__restrict__ force)
+// The sites' dipole sum q r of the surface term, in 64-bit fixed point (2^-32) at efix[3..5].
+__global__ void k_site_dipole(int na, const double *__restrict__ r, const double *__restrict__ az,
+                              unsigned long long *__restrict__ efix)
+{
+    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
+    long long m[3] = {0, 0, 0};
+    if (ia < na)
+        for (int c = 0; c < 3; ++c) m[c] = __double2ll_rn(az[ia] * r[3 * (size_t)ia + c] * kDipFix);
+    for (int o = 16; o > 0; o >>= 1)
+        for (int c = 0; c < 3; ++c) m[c] += __shfl_xor_sync(0xffffffffu, m[c], o);
+    if ((threadIdx.x & 31) == 0)
+        for (int c = 0; c < 3; ++c)
+            if (m[c]) atomicAdd(efix + 3 + c, (unsigned long long)m[c]);
+}
+
+// The sites' reciprocal force: the k slices added in slice order, less the surface term's
+// force epsfp 2 fac q M (UEwaldSurf, Src/energy.F90:1349-1371) when sfac = 2 fac is not 0;
+// stored, or added to the force already there when add is set.
+__global__ void k_site_fsum(int na, int nks, int add, double epsfp, double sfac, const double *__restrict__ az,
+                            const unsigned long long *__restrict__ efix, const double *__restrict__ fks,
+                            double *__restrict__ force)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 3 * na) return;
     double f = 0.0;
     for (int k = 0; k < nks; ++k) f += fks[(size_t)k * 3 * na + i];
-    force[i] = f;
+    if (sfac != 0.0) {
+        const double M = (double)(long long)efix[3 + i % 3] * kDipFixInv;
+        f = f - epsfp * sfac * az[i / 3] * M;
+    }
+    force[i] = add ? force[i] + f : f;
 }
 
 // UEwaldSelf's molecular term (Src/energy.F90:1315-1343): every site pair inside a
@@ -858,6 +745,134 @@ __global__ void k_site_self(int np, double alpha, double ewaldfac1, double epsfp
     if ((threadIdx.x & 31) == 0 && eu) atomicAdd(efix + 2, (unsigned long long)eu);
 }
 
+// The site Ewald sum of one system: set-up on the host (k-vectors, kfac, launch shapes,
+// device buffers) and a launch sequence on the caller's device arrays, so one set-up
+// serves every step of a run.  Device accumulators efix: reciprocal energy, its virial,
+// the molecular self energy (2^-40) and the dipole sum (2^-32).
+struct SiteEwald {
+    int na = 0, np = 0, nkv = 0, w = 0, lsurf = 0;
+    int ktiles = 0, ptiles = 0, clen = 0, nchunk = 0, klen = 0, nks = 0, sub = 0;
+    double alpha = 0.0, epsfp = 0.0, vol = 0.0, q2 = 0.0, ewaldfac1 = 0.0;
+    double3 tpbi = make_double3(0.0, 0.0, 0.0);
+    double *daz = nullptr, *dkf = nullptr, *fks = nullptr;
+    int4 *dkv = nullptr;
+    double2 *eik = nullptr, *part = nullptr, *sk = nullptr;
+    unsigned long long *efix = nullptr;
+
+    static constexpr double kPi = 3.1415926535897932;
+
+    // MSG_ERR_ARG for arguments outside what the reference accepts, else the CUDA status.
+    int setup(int32_t na_, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion, int32_t lsurf_,
+              double epsfp_, const double *az, int32_t np_, const int32_t *iptpn, const int32_t *ianpn,
+              const int32_t *napt, int32_t npt)
+    {
+        if (na_ < 1 || np_ < 1 || npt < 1 || ncut < 1 || ncut > kSMaxCut || ncutregion < 0 || ncutregion > 1 ||
+            !(ualpha > 0.0) || !boxlen || !az || !iptpn || !ianpn || !napt)
+            return MSG_ERR_ARG;
+        for (int t = 0; t < npt; ++t)
+            if (napt[t] < 1) return MSG_ERR_ARG;
+        for (int i = 0; i < np_; ++i)
+            if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na_)
+                return MSG_ERR_ARG;
+        na = na_;
+        np = np_;
+        lsurf = lsurf_ ? 1 : 0;
+        alpha = ualpha;
+        epsfp = epsfp_;
+        vol = boxlen[0] * boxlen[1] * boxlen[2];
+        tpbi = make_double3(2.0 * kPi * (1.0 / boxlen[0]), 2.0 * kPi * (1.0 / boxlen[1]), 2.0 * kPi * (1.0 / boxlen[2]));
+        ewaldfac1 = (1.0 / (std::sqrt(kPi) * ualpha)) * 2.0 * (ualpha * ualpha);
+        q2 = 0.0;
+        for (int a = 0; a < na; ++a) q2 += az[a] * az[a];
+        // k-vectors and kfac in the order of EwaldSetup 'std' (Src/energy.F90:6762-6782)
+        std::vector<int4> kv;
+        std::vector<double> kf;
+        const int ncut2 = ncutregion ? 3 * ncut * ncut : ncut * ncut;
+        for (int nz = 0; nz <= ncut; ++nz)
+            for (int ny = 0; ny <= ncut; ++ny)
+                for (int nx = 0; nx <= ncut; ++nx) {
+                    if (nx * nx + ny * ny + nz * nz > ncut2 || (nx == 0 && ny == 0 && nz == 0)) continue;
+                    const double facz = nz == 0 ? 1.0 : 2.0, facy = ny == 0 ? 0.5 : 1.0, facx = nx == 0 ? 0.5 : 1.0;
+                    const double kx = nx * tpbi.x, ky = ny * tpbi.y, kz = nz * tpbi.z, k2 = kx * kx + ky * ky + kz * kz;
+                    kf.push_back(2.0 * kPi / vol * facz * facy * facx * std::exp(-k2 / (4.0 * (ualpha * ualpha))) / k2);
+                    kv.push_back(make_int4(nx, ny, nz, 0));
+                }
+        nkv = (int)kv.size();
+        w = ncut + 1;
+        // site chunks of the structure-factor sum (about eight blocks per SM of a 148-SM B200, a
+        // chunk at least 128 sites) and k slices of the force sum (about four blocks per SM, a
+        // slice at least 16 k-vectors): from the system's sizes only, so the sums repeat bit for bit
+        ktiles = (nkv + kSK - 1) / kSK;
+        ptiles = (na + kSF - 1) / kSF;
+        const int nch = std::max(1, std::min((8 * 148 + ktiles - 1) / ktiles, (na + 127) / 128));
+        clen = (na + nch - 1) / nch;
+        nchunk = (na + clen - 1) / clen;
+        const int nks0 = std::max(1, std::min((4 * 148 + ptiles - 1) / ptiles, std::max(1, nkv / 16)));
+        klen = (nkv + nks0 - 1) / nks0;
+        nks = (nkv + klen - 1) / klen;
+        sub = std::max(1, std::min(16, kSSmem / (3 * w * (int)sizeof(double2))));
+        cudaError_t e = cudaSuccess;
+        daz = dev_copy(az, (size_t)na, e);
+        dkf = dev_copy(kf.data(), kf.size(), e);
+        dkv = dev_copy(kv.data(), kv.size(), e);
+        if (e == cudaSuccess) e = cudaMalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
+        if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
+        if (e == cudaSuccess) e = cudaMalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
+        if (e == cudaSuccess) e = cudaMalloc(&fks, (size_t)nks * 3 * na * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&efix, 6 * sizeof(unsigned long long));
+        return e == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
+    }
+
+    // One evaluation at the sites dr: the Ewald forces stored into dforce (add = 0) or added
+    // to it (add = 1); the accumulators restart.
+    void launch(const double *dr, const int *dipt, const int *dian, const int *dnapt, double *dforce, int add,
+                cudaStream_t st) const
+    {
+        cudaMemsetAsync(efix, 0, 6 * sizeof(unsigned long long), st);
+        k_site_eik<<<(na + 127) / 128, 128, 0, st>>>(na, w, tpbi, dr, daz, eik);
+        k_site_sk<<<dim3(ktiles, nchunk), kSK, (size_t)sub * 3 * w * sizeof(double2), st>>>(na, nkv, w, clen, sub,
+                                                                                          dkv, eik, part);
+        k_site_reduce<<<ktiles, kSK, 0, st>>>(nkv, nchunk, alpha * alpha, tpbi, dkv, dkf, part, sk, efix);
+        k_site_force<<<dim3(ptiles, nks), kSF, 0, st>>>(na, nkv, klen, epsfp, tpbi, dr, daz, dkv, dkf, sk, fks);
+        double sfac = 0.0;
+        if (lsurf) {
+            k_site_dipole<<<(na + 127) / 128, 128, 0, st>>>(na, dr, daz, efix);
+            sfac = 2.0 * (2.0 * kPi / (3.0 * vol));
+        }
+        k_site_fsum<<<(3 * na + 255) / 256, 256, 0, st>>>(na, nks, add, epsfp, sfac, daz, efix, fks, dforce);
+        k_site_self<<<(np + 127) / 128, 128, 0, st>>>(np, alpha, ewaldfac1, epsfp, dr, daz, dipt, dian, dnapt, dforce,
+                                                      efix);
+    }
+
+    // u%rec and its virial (scaled by EpsiFourPi as UEwald does) of the last launch.
+    cudaError_t energies(double &urec, double &virrec) const
+    {
+        unsigned long long h[6];
+        const cudaError_t e = cudaMemcpy(h, efix, sizeof(h), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return e;
+        double u = (double)(long long)h[0] * kPFixInv - alpha / std::sqrt(kPi) * q2 + (double)(long long)h[2] * kPFixInv;
+        double vr = (double)(long long)h[1] * kPFixInv;
+        if (lsurf) {
+            const double fac = 2.0 * kPi / (3.0 * vol);
+            double M[3];
+            for (int c = 0; c < 3; ++c) M[c] = (double)(long long)h[3 + c] * kDipFixInv;
+            const double term = fac * (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]);
+            u += term;
+            vr -= term;
+        }
+        urec = epsfp * u;
+        virrec = epsfp * vr;
+        return cudaSuccess;
+    }
+
+    ~SiteEwald()
+    {
+        for (void *p : {(void *)daz, (void *)dkf, (void *)dkv, (void *)eik, (void *)part, (void *)sk, (void *)fks,
+                        (void *)efix})
+            if (p) cudaFree(p);
+    }
+};
+
 }  // namespace
 
 extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
@@ -865,64 +880,14 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
                                 const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
                                 double *force, double *urec, double *virrec, float *kernel_ms)
 {
-    if (na < 1 || np < 1 || npt < 1 || ncut < 1 || ncut > kSMaxCut || ncutregion < 0 || ncutregion > 1 ||
-        !(ualpha > 0.0) || !boxlen || !r || !az || !iptpn || !ianpn || !napt || !force || !urec || !virrec)
-        return MSG_ERR_ARG;
-    for (int t = 0; t < npt; ++t)
-        if (napt[t] < 1) return MSG_ERR_ARG;
-    for (int i = 0; i < np; ++i)
-        if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na)
-            return MSG_ERR_ARG;
-    const double pi = 3.1415926535897932;
-    const double vol = boxlen[0] * boxlen[1] * boxlen[2];
-    const double3 tpbi = make_double3(2.0 * pi * (1.0 / boxlen[0]), 2.0 * pi * (1.0 / boxlen[1]),
-                                      2.0 * pi * (1.0 / boxlen[2]));
-    // k-vectors and kfac in the order of EwaldSetup 'std' (Src/energy.F90:6762-6782)
-    std::vector<int4> kv;
-    std::vector<double> kf;
-    const int ncut2 = ncutregion ? 3 * ncut * ncut : ncut * ncut;
-    for (int nz = 0; nz <= ncut; ++nz)
-        for (int ny = 0; ny <= ncut; ++ny)
-            for (int nx = 0; nx <= ncut; ++nx) {
-                if (nx * nx + ny * ny + nz * nz > ncut2 || (nx == 0 && ny == 0 && nz == 0)) continue;
-                const double facz = nz == 0 ? 1.0 : 2.0, facy = ny == 0 ? 0.5 : 1.0, facx = nx == 0 ? 0.5 : 1.0;
-                const double kx = nx * tpbi.x, ky = ny * tpbi.y, kz = nz * tpbi.z, k2 = kx * kx + ky * ky + kz * kz;
-                kf.push_back(2.0 * pi / vol * facz * facy * facx * std::exp(-k2 / (4.0 * (ualpha * ualpha))) / k2);
-                kv.push_back(make_int4(nx, ny, nz, 0));
-            }
-    const int nkv = (int)kv.size(), w = ncut + 1;
-    // site chunks of the structure-factor sum (about eight blocks per SM of a 148-SM B200, a
-    // chunk at least 128 sites) and k slices of the force sum (about four blocks per SM, a slice
-    // at least 16 k-vectors): from the system's sizes only, so the sums repeat bit for bit
-    const int ktiles = (nkv + kSK - 1) / kSK, ptiles = (na + kSF - 1) / kSF;
-    const int nch = std::max(1, std::min((8 * 148 + ktiles - 1) / ktiles, (na + 127) / 128));
-    const int clen = (na + nch - 1) / nch, nchunk = (na + clen - 1) / clen;
-    const int nks0 = std::max(1, std::min((4 * 148 + ptiles - 1) / ptiles, std::max(1, nkv / 16)));
-    const int klen = (nkv + nks0 - 1) / nks0, nks = (nkv + klen - 1) / klen;
-    const int sub = std::max(1, std::min(16, kSSmem / (3 * w * (int)sizeof(double2))));
-    // the surface term on the host (UEwaldSurf, Src/energy.F90:1349-1371)
-    double mx = 0.0, my = 0.0, mz = 0.0, q2 = 0.0;
-    for (int a = 0; a < na; ++a) {
-        mx += az[a] * r[3 * (size_t)a];
-        my += az[a] * r[3 * (size_t)a + 1];
-        mz += az[a] * r[3 * (size_t)a + 2];
-        q2 += az[a] * az[a];
-    }
-    cudaError_t e = cudaSuccess;
-    double *dr = dev_copy(r, 3 * (size_t)na, e), *daz = dev_copy(az, (size_t)na, e), *dkf = dev_copy(kf.data(), kf.size(), e);
-    int4 *dkv = dev_copy(kv.data(), kv.size(), e);
+    if (!r || !force || !urec || !virrec) return MSG_ERR_ARG;
+    SiteEwald E;
+    const int rc = E.setup(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
+    if (rc == MSG_ERR_ARG) return rc;
+    cudaError_t e = rc == MSG_OK ? cudaSuccess : cudaErrorMemoryAllocation;
+    double *dr = dev_copy(r, 3 * (size_t)na, e), *dforce = nullptr;
     int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e), *dnapt = dev_copy(napt, (size_t)npt, e);
-    double2 *eik = nullptr, *part = nullptr, *sk = nullptr;
-    double *dforce = nullptr, *fks = nullptr;
-    unsigned long long *efix = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&fks, (size_t)nks * 3 * na * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&efix, 3 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(efix, 0, 3 * sizeof(unsigned long long));
-    unsigned long long hfix[3] = {0, 0, 0};
     if (e == cudaSuccess) {
         cudaEvent_t a = nullptr, b = nullptr;
         if (kernel_ms) {
@@ -930,14 +895,7 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
             cudaEventCreate(&b);
             cudaEventRecord(a, 0);
         }
-        k_site_eik<<<(na + 127) / 128, 128>>>(na, w, tpbi, dr, daz, eik);
-        k_site_sk<<<dim3(ktiles, nchunk), kSK, (size_t)sub * 3 * w * sizeof(double2)>>>(na, nkv, w, clen, sub, dkv,
-                                                                                    eik, part);
-        k_site_reduce<<<ktiles, kSK>>>(nkv, nchunk, ualpha * ualpha, tpbi, dkv, dkf, part, sk, efix);
-        k_site_force<<<dim3(ptiles, nks), kSF>>>(na, nkv, klen, epsfp, tpbi, dr, daz, dkv, dkf, sk, fks);
-        k_site_fsum<<<(3 * na + 255) / 256, 256>>>(na, nks, fks, dforce);
-        const double ewaldfac1 = (1.0 / (std::sqrt(pi) * ualpha)) * 2.0 * (ualpha * ualpha);
-        k_site_self<<<(np + 127) / 128, 128>>>(np, ualpha, ewaldfac1, epsfp, dr, daz, dipt, dian, dnapt, dforce, efix);
+        E.launch(dr, dipt, dian, dnapt, dforce, 0, 0);
         if (kernel_ms) {
             cudaEventRecord(b, 0);
             cudaEventSynchronize(b);
@@ -947,30 +905,196 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
         }
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(force, dforce, 3 * (size_t)na * sizeof(double), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(hfix, efix, sizeof(hfix), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = E.energies(*urec, *virrec);
     }
-    for (void *p : {(void *)dr, (void *)daz, (void *)dkf, (void *)dkv, (void *)dipt, (void *)dian, (void *)dnapt,
-                    (void *)eik, (void *)part, (void *)sk, (void *)dforce, (void *)fks, (void *)efix})
+    for (void *p : {(void *)dr, (void *)dipt, (void *)dian, (void *)dnapt, (void *)dforce})
         if (p) cudaFree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return MSG_ERR_CUDA;
     }
-    // UEwald's sum: reciprocal, atomic and molecular self terms, surface; scaled by EpsiFourPi
-    double u = (double)(long long)hfix[0] * kPFixInv - ualpha / std::sqrt(pi) * q2 + (double)(long long)hfix[2] * kPFixInv;
-    double vr = (double)(long long)hfix[1] * kPFixInv;
-    if (lsurf) {
-        const double fac = 2.0 * pi / (3.0 * vol);
-        const double term = fac * (mx * mx + my * my + mz * mz);
-        u += term;
-        vr -= term;
-        for (int a = 0; a < na; ++a) {
-            force[3 * (size_t)a] -= epsfp * (2.0 * fac) * az[a] * mx;
-            force[3 * (size_t)a + 1] -= epsfp * (2.0 * fac) * az[a] * my;
-            force[3 * (size_t)a + 2] -= epsfp * (2.0 * fac) * az[a] * mz;
+    return MSG_OK;
+}
+
+// The rigid-body MD steps of msg_velver_p and msg_velver_p_ewald: ew (optional) adds the
+// site Ewald sum to the site forces of every step before the kick, and its reciprocal
+// virial to the returned virial; urec receives u%rec of the last step.
+static int velver_p_run(const SiteEwald *ew, double *urec, int32_t nsteps, int32_t np, int32_t na, int32_t npt,
+                        int32_t nat, const double boxlen[3], double rcut, double tstep, int32_t nvvite, double tvvite,
+                        double *ro, double *rod, double *rodd, double *qua, double *quad, double *quadd, double *r,
+                        const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, const int32_t *iatan,
+                        const double *ra, int32_t maxsite, const double *masspt, const double *momp,
+                        const int32_t *nneighpn, const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf,
+                        int32_t nbuf, const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial,
+                        float *kernel_ms)
+{
+    if (nsteps < 0 || np < 1 || na < 1 || npt < 1 || npt > kPMaxType || nat < 1 || maxsite < 1 || maxsite > 256 ||
+        maxnneigh < 1 || nbuf < 12 ||
+        nvvite < 0 || !boxlen || !ro || !rod || !rodd || !qua || !quad || !quadd || !r || !iptpn || !ianpn ||
+        !napt || !iatan || !ra || !masspt || !momp || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin ||
+        !utwob || !virial)
+        return MSG_ERR_ARG;
+    for (int t = 0; t < npt; ++t)
+        if (napt[t] < 1 || napt[t] > maxsite || !(masspt[t] > 0.0) || !(momp[3 * t] > 0.0) || !(momp[3 * t + 1] > 0.0) ||
+            !(momp[3 * t + 2] > 0.0))
+            return MSG_ERR_ARG;
+    for (int i = 0; i < np; ++i) {
+        if (iptpn[i] < 1 || iptpn[i] > npt || ianpn[i] < 1 || ianpn[i] - 1 + napt[iptpn[i] - 1] > na)
+            return MSG_ERR_ARG;
+        if (nneighpn[i] < 0 || nneighpn[i] > maxnneigh) return MSG_ERR_ARG;
+        for (int k = 0; k < nneighpn[i]; ++k) {
+            const int j = jpnlist[(size_t)i * maxnneigh + k];
+            if (j < 1 || j > np) return MSG_ERR_ARG;
         }
     }
-    *urec = epsfp * u;
-    *virrec = epsfp * vr;
+    const int natat = nat * (nat + 1) / 2, nptpt = npt * (npt + 1) / 2;
+    for (int a = 0; a < na; ++a)
+        if (iatan[a] < 1 || iatan[a] > nat) return MSG_ERR_ARG;
+    for (int q = 0; q < natat; ++q)
+        if (iubuflow[q] < 1 || iubuflow[q] + 11 > nbuf) return MSG_ERR_ARG;
+    RigidArgs A;
+    A.np = np;
+    A.nvvite = nvvite;
+    A.tstep = tstep;
+    A.tvvite = tvvite;
+    A.fac = 0.5 * tstep * tstep;
+    for (int m = 0; m < 3; ++m) {
+        A.box[m] = boxlen[m];
+        A.half[m] = boxlen[m] / 2.0;
+        A.boxi[m] = 1.0 / boxlen[m];
+    }
+    A.maxsite = maxsite;
+    {
+        // (sclene / scllen) / sclfor with MOLSIM's scales (Src/molsim.F90:786-805)
+        const double scllen = 1.0e-10, sclmas = 1.0e-03, scltim = 1.0e-12, sclene = 1.0e+03;
+        const double sclvel = scllen / scltim, sclacc = sclvel / scltim;
+        A.ffac = (sclene / scllen) / (sclacc * sclmas);
+    }
+    cudaError_t e = cudaSuccess;
+    double *dro = dev_copy(ro, 3 * (size_t)np, e), *drod = dev_copy(rod, 3 * (size_t)np, e),
+           *drodd = dev_copy(rodd, 3 * (size_t)np, e), *dqua = dev_copy(qua, 4 * (size_t)np, e),
+           *dquad = dev_copy(quad, 4 * (size_t)np, e), *dquadd = dev_copy(quadd, 4 * (size_t)np, e),
+           *dr = dev_copy(r, 3 * (size_t)na, e), *dra = dev_copy(ra, 3 * (size_t)npt * maxsite, e),
+           *dmass = dev_copy(masspt, (size_t)npt, e), *dmom = dev_copy(momp, 3 * (size_t)npt, e);
+    int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e);
+    int *dnapt = dev_copy(napt, (size_t)npt, e), *diat = dev_copy(iatan, (size_t)na, e);
+    int *dnn = dev_copy(nneighpn, (size_t)np, e), *djp = dev_copy(jpnlist, (size_t)np * maxnneigh, e);
+    double *dub = dev_copy(ubuf, (size_t)nbuf, e), *dr2 = dev_copy(r2umin, (size_t)natat, e);
+    int *diub = dev_copy(iubuflow, (size_t)natat, e);
+    std::vector<SiteBuckets> hsb;
+    std::vector<int> hbs;
+    site_buckets(natat, ubuf, nbuf, iubuflow, r2umin, hsb, hbs);
+    SiteBuckets *dsb = dev_copy(hsb.data(), hsb.size(), e);
+    int *dbs = dev_copy(hbs.data(), hbs.size(), e);
+    unsigned long long *ffix = nullptr;
+    double *dforce = nullptr, *duv = nullptr, *dori = nullptr;
+    int *derr = nullptr;
+    const size_t nfix = 3 * (size_t)na + nptpt + 2;           // site forces, energies, pair and molecular virial
+    if (e == cudaSuccess) e = cudaMalloc(&ffix, nfix * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&duv, (nptpt + 2) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dori, 9 * (size_t)np * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
+    int herr = 0;
+    double vmol = 0.0;
+    if (e == cudaSuccess && nsteps > 0) {
+        unsigned long long *ufix = ffix + 3 * (size_t)na, *vfix = ufix + nptpt, *vmfix = vfix + 1;
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (kernel_ms) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, 0);
+        }
+        const int pb = (np + 127) / 128;
+        for (int step = 0; step < nsteps; ++step) {
+            cudaMemsetAsync(ffix, 0, nfix * sizeof(unsigned long long), 0);
+            k_rigid_move<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dipt, dian, dnapt, dra);
+            k_utwobody_p<<<(np + kPWarps - 1) / kPWarps, kPThreads, site_smem(npt, napt)>>>(
+                np, npt, nat, make_double3(boxlen[0], boxlen[1], boxlen[2]), rcut * rcut, dro, dr, dipt, dian, dnapt,
+                diat, dnn, djp, maxnneigh, dub, nbuf, diub, dr2, dsb, dbs, max_sites(npt, napt), ffix, ufix, vfix, derr);
+            k_utwobody_p_out<<<(int)((3 * (size_t)na + 255) / 256), 256>>>(na, nptpt, ffix, ufix, vfix, dforce, duv);
+            if (ew) ew->launch(dr, dipt, dian, dnapt, dforce, 1, 0);
+            k_rigid_kick<<<pb, 128>>>(A, dro, drod, drodd, dqua, dquad, dquadd, dori, dr, dforce, dipt, dian, dnapt,
+                                      dmass, dmom, vmfix);
+        }
+        if (kernel_ms) {
+            cudaEventRecord(b, 0);
+            cudaEventSynchronize(b);
+            cudaEventElapsedTime(kernel_ms, a, b);
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+        unsigned long long vm = 0;
+        if (e == cudaSuccess) e = cudaMemcpy(&vm, vmfix, sizeof(vm), cudaMemcpyDeviceToHost);
+        vmol = (double)(long long)vm * kPFixInv;
+    }
+    if (e == cudaSuccess && !herr) {
+        std::vector<double> uv(nptpt + 2, 0.0);
+        if (nsteps > 0) e = cudaMemcpy(uv.data(), duv, uv.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        struct Back { double *h, *d; size_t n; } back[] = {
+            {ro, dro, 3 * (size_t)np}, {rod, drod, 3 * (size_t)np}, {rodd, drodd, 3 * (size_t)np},
+            {qua, dqua, 4 * (size_t)np}, {quad, dquad, 4 * (size_t)np}, {quadd, dquadd, 4 * (size_t)np},
+            {r, dr, 3 * (size_t)na}};
+        for (const Back &x : back)
+            if (e == cudaSuccess) e = cudaMemcpy(x.h, x.d, x.n * sizeof(double), cudaMemcpyDeviceToHost);
+        double ur = 0.0, vr = 0.0;
+        if (e == cudaSuccess && nsteps > 0 && ew) e = ew->energies(ur, vr);
+        if (e == cudaSuccess && nsteps > 0) {
+            for (int q = 0; q <= nptpt; ++q) utwob[q] = uv[q];
+            *virial = uv[nptpt + 1] + vr + vmol;
+            if (urec) *urec = ur;
+        }
+    }
+    for (void *p : {(void *)dro, (void *)drod, (void *)drodd, (void *)dqua, (void *)dquad, (void *)dquadd, (void *)dr,
+                    (void *)dra, (void *)dmass, (void *)dmom, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat,
+                    (void *)dnn, (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)dsb, (void *)dbs,
+                    (void *)ffix, (void *)dforce, (void *)duv, (void *)dori, (void *)derr})
+        if (p) cudaFree(p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return MSG_ERR_CUDA;
+    }
+    if (herr == 1) return MSG_ERR_TABLE_MIN;
+    if (herr == 2) return MSG_ERR_TABLE_RANGE;
     return MSG_OK;
+}
+
+extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                            double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
+                            double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
+                            const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
+                            int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
+                            const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                            const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial,
+                            float *kernel_ms)
+{
+    return velver_p_run(nullptr, nullptr, nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, rodd,
+                        qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist,
+                        maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial, kernel_ms);
+}
+
+extern "C" int msg_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat,
+                                  const double boxlen[3], double rcut, double tstep, int32_t nvvite, double tvvite,
+                                  double *ro, double *rod, double *rodd, double *qua, double *quad, double *quadd,
+                                  double *r, const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt,
+                                  const int32_t *iatan, const double *ra, int32_t maxsite, const double *masspt,
+                                  const double *momp, const int32_t *nneighpn, const int32_t *jpnlist,
+                                  int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
+                                  const double *r2umin, const double *az, double ualpha, int32_t ncut,
+                                  int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob, double *urec,
+                                  double *virial, float *kernel_ms)
+{
+    if (!urec) return MSG_ERR_ARG;
+    SiteEwald E;
+    const int rc = E.setup(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
+    if (rc != MSG_OK) {
+        cudaGetLastError();
+        return rc;
+    }
+    return velver_p_run(&E, urec, nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, rodd, qua,
+                        quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist,
+                        maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial, kernel_ms);
 }

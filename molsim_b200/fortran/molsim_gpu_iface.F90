@@ -152,6 +152,31 @@ module MolsimGpu
          type(c_ptr), value        :: iubuflow, r2umin, utwob, virial, kernel_ms
       end function msg_velver_p
 
+      integer(c_int) function msg_velver_p_ewald(nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, &
+            ro, rod, rodd, qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, &
+            jpnlist, maxnneigh, ubuf, nbuf, iubuflow, r2umin, az, ualpha, ncut, ncutregion, lsurf, epsfp, utwob, &
+            urec, virial, kernel_ms) bind(c, name='msg_velver_p_ewald')
+         import :: c_int, c_int32_t, c_double, c_ptr
+         integer(c_int32_t), value :: nsteps, np, na, npt, nat
+         real(c_double), intent(in) :: boxlen(3)
+         real(c_double), value     :: rcut, tstep
+         integer(c_int32_t), value :: nvvite
+         real(c_double), value     :: tvvite
+         type(c_ptr), value        :: ro, rod, rodd, qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra
+         integer(c_int32_t), value :: maxsite
+         type(c_ptr), value        :: masspt, momp, nneighpn, jpnlist
+         integer(c_int32_t), value :: maxnneigh
+         type(c_ptr), value        :: ubuf
+         integer(c_int32_t), value :: nbuf
+         type(c_ptr), value        :: iubuflow, r2umin, az
+         real(c_double), value     :: ualpha
+         integer(c_int32_t), value :: ncut, ncutregion, lsurf
+         real(c_double), value     :: epsfp
+         type(c_ptr), value        :: utwob
+         real(c_double), intent(out) :: urec, virial
+         type(c_ptr), value        :: kernel_ms
+      end function msg_velver_p_ewald
+
       integer(c_int) function msg_uewald_sites(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, r, az, np, &
             iptpn, ianpn, napt, npt, force, urec, virrec, kernel_ms) bind(c, name='msg_uewald_sites')
          import :: c_int, c_int32_t, c_double, c_ptr

@@ -44,10 +44,11 @@ def utwobody_p(s, table):
     return dict(force=force, utwob=utwob, virial=vir.value, kernel_ms=ms.value)
 
 
-def velver_p(s, table, nsteps=1):
+def velver_p(s, table, nsteps=1, ewald=None):
     """nsteps of the rigid-body MD step for a systems.rigid_bodies dict, its state (ro, rod,
-    rodd, qua, quad, quadd, r) advanced in place.  Returns dict(utwob, virial, kernel_ms) of
-    the last step."""
+    rodd, qua, quad, quadd, r) advanced in place.  ewald (optional): dict(az, ualpha, ncut,
+    region, lsurf) adds the site Ewald sum (msg_velver_p_ewald) to every step.  Returns
+    dict(utwob, virial, kernel_ms[, urec]) of the last step."""
     k = {}
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r", "ra", "masspt", "momp"):
         k[key] = np.ascontiguousarray(s[key], np.float64)
@@ -62,19 +63,34 @@ def velver_p(s, table, nsteps=1):
     ms = C.c_float()
     box = (C.c_double * 3)(*s["boxlen"])
     i32 = C.c_int32
-    rc = _lib.lib().msg_velver_p(int(nsteps), int(s["np"]), int(s["na"]), npt, int(s["nat"]), box, float(s["rcut"]),
-                                 float(s["tstep"]), int(s["nvvite"]), float(s["tvvite"]),
-                                 *[_p(k[x], C.c_double) for x in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r")],
-                                 *[_p(k[x], i32) for x in ("iptpn", "ianpn", "napt", "iatan")],
-                                 _p(k["ra"], C.c_double), int(s["maxsite"]), _p(k["masspt"], C.c_double),
-                                 _p(k["momp"], C.c_double), _p(k["nneighpn"], i32), _p(k["jpnlist"], i32),
-                                 int(k["jpnlist"].shape[1]), _p(ub, C.c_double), len(ub), _p(iub, i32),
-                                 _p(r2, C.c_double), _p(utwob, C.c_double), C.byref(vir), C.byref(ms))
+    args = [int(nsteps), int(s["np"]), int(s["na"]), npt, int(s["nat"]), box, float(s["rcut"]),
+            float(s["tstep"]), int(s["nvvite"]), float(s["tvvite"]),
+            *[_p(k[x], C.c_double) for x in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r")],
+            *[_p(k[x], i32) for x in ("iptpn", "ianpn", "napt", "iatan")],
+            _p(k["ra"], C.c_double), int(s["maxsite"]), _p(k["masspt"], C.c_double),
+            _p(k["momp"], C.c_double), _p(k["nneighpn"], i32), _p(k["jpnlist"], i32),
+            int(k["jpnlist"].shape[1]), _p(ub, C.c_double), len(ub), _p(iub, i32), _p(r2, C.c_double)]
+    urec = C.c_double()
+    if ewald is None:
+        name = "msg_velver_p"
+        rc = _lib.lib().msg_velver_p(*args, _p(utwob, C.c_double), C.byref(vir), C.byref(ms))
+    else:
+        name = "msg_velver_p_ewald"
+        az = np.ascontiguousarray(ewald["az"], np.float64)
+        if az.shape != (int(s["na"]),):
+            raise ValueError("ewald['az'] must hold one charge per site")
+        rc = _lib.lib().msg_velver_p_ewald(*args, _p(az, C.c_double), float(ewald["ualpha"]), int(ewald["ncut"]),
+                                           1 if ewald.get("region", "sphere") == "cube" else 0,
+                                           int(bool(ewald.get("lsurf"))), float(s["epsi_four_pi"]),
+                                           _p(utwob, C.c_double), C.byref(urec), C.byref(vir), C.byref(ms))
     if rc:
-        raise MolsimGpuError(rc, "msg_velver_p")
+        raise MolsimGpuError(rc, name)
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
         s[key] = k[key]
-    return dict(utwob=utwob, virial=vir.value, kernel_ms=ms.value)
+    out = dict(utwob=utwob, virial=vir.value, kernel_ms=ms.value)
+    if ewald is not None:
+        out["urec"] = urec.value
+    return out
 
 
 def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):

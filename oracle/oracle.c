@@ -1726,13 +1726,20 @@ static double rigid_forces(int32_t np, const double *ro, const double *r, const 
  * State arrays (MOLSIM layout) are advanced in place; ra [npt][maxsite][3] are the
  * sites in the principal frame, masspt [npt] and momp [npt][3] the particle masses and
  * principal moments.  Energies and virial of the last step.  Returns UTwoBodyP's status. */
-int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
-                double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod, double *rodd,
-                double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn, const int32_t *ianpn,
-                const int32_t *napt, const int32_t *iatan, const double *ra, int32_t maxsite, const double *masspt,
-                const double *momp, const int32_t *nneighpn, const int32_t *jpnlist, int32_t maxnneigh,
-                const double *ubuf, int32_t nbuf, const int32_t *iubuflow, const double *r2umin, double *utwob,
-                double *virial)
+/* Site Ewald parameters of the rigid-body step (or_velver_p_ewald). */
+typedef struct {
+    const double *az;
+    double ualpha, epsfp;
+    int32_t ncut, ncutregion, lsurf;
+} site_ew;
+
+static int velver_p_impl(const site_ew *ew, double *urec, int32_t nsteps, int32_t np, int32_t na, int32_t npt,
+                         int32_t nat, const double boxlen[3], double rcut, double tstep, int32_t nvvite, double tvvite,
+                         double *ro, double *rod, double *rodd, double *qua, double *quad, double *quadd, double *r,
+                         const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, const int32_t *iatan,
+                         const double *ra, int32_t maxsite, const double *masspt, const double *momp,
+                         const int32_t *nneighpn, const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf,
+                         int32_t nbuf, const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial)
 {
     const double fac = 0.5 * tstep * tstep;
     double *ori = malloc(sizeof(double) * 9 * (size_t)np), *force = malloc(sizeof(double) * 3 * (size_t)na);
@@ -1755,6 +1762,14 @@ int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat
         rc = or_utwobody_p(np, na, npt, nat, boxlen, rcut, ro, r, iptpn, ianpn, napt, iatan, nneighpn, jpnlist,
                            maxnneigh, ubuf, nbuf, iubuflow, r2umin, force, utwob, &vpair);
         if (rc) break;
+        if (ew) {                                  /* UTotal's UEwald over the sites (Src/energy.F90:335-352) */
+            double *fe = malloc(sizeof(double) * 3 * (size_t)na), vr = 0.0;
+            or_uewald_sites(na, boxlen, ew->ualpha, ew->ncut, ew->ncutregion, ew->lsurf, ew->epsfp, r, ew->az, np,
+                            iptpn, ianpn, napt, fe, urec, &vr);
+            for (m = 0; m < 3 * na; ++m) force[m] = force[m] + fe[m];
+            vpair = vpair + vr;
+            free(fe);
+        }
         *virial = vpair + rigid_forces(np, ro, r, iptpn, ianpn, napt, force, forceo, torqueo);
         for (ip = 0; ip < np; ++ip) {
             const int ipt = iptpn[ip] - 1;
@@ -1780,6 +1795,43 @@ int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat
     }
     free(ori); free(force); free(forceo); free(torqueo);
     return rc;
+}
+
+int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod, double *rodd,
+                double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn, const int32_t *ianpn,
+                const int32_t *napt, const int32_t *iatan, const double *ra, int32_t maxsite, const double *masspt,
+                const double *momp, const int32_t *nneighpn, const int32_t *jpnlist, int32_t maxnneigh,
+                const double *ubuf, int32_t nbuf, const int32_t *iubuflow, const double *r2umin, double *utwob,
+                double *virial)
+{
+    return velver_p_impl(NULL, NULL, nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, rodd, qua,
+                         quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist,
+                         maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial);
+}
+
+/* The rigid-body step with the site Ewald sum in UTotal (lewald with polyatomic particles):
+ * the Ewald site forces join the pair forces before the forces, torques and molecular virial;
+ * the reciprocal virial joins the virial; *urec = u%rec of the last step. */
+int or_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                      double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod, double *rodd,
+                      double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
+                      const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
+                      int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
+                      const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                      const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha, int32_t ncut,
+                      int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob, double *urec, double *virial)
+{
+    site_ew ew;
+    ew.az = az;
+    ew.ualpha = ualpha;
+    ew.epsfp = epsfp;
+    ew.ncut = ncut;
+    ew.ncutregion = ncutregion;
+    ew.lsurf = lsurf;
+    return velver_p_impl(&ew, urec, nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, rodd, qua,
+                         quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist,
+                         maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial);
 }
 
 /* UEwald over the sites of polyatomic particles (Src/energy.F90:905-958): the standard

@@ -176,6 +176,18 @@ int    or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t 
                    const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
                    const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial);
 
+/* or_velver_p with the site Ewald sum (or_uewald_sites) in every step's forces and virial;
+ * *urec = u%rec of the last step. */
+int    or_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
+                         double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
+                         double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
+                         const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
+                         int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
+                         const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
+                         const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha,
+                         int32_t ncut, int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob,
+                         double *urec, double *virial);
+
 /* UEwald over the sites of polyatomic particles: standard reciprocal sum, UEwaldSelf's
  * atomic and molecular (intramolecular erf) terms, surface term; force [na][3] overwritten. */
 int    or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,

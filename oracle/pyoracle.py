@@ -363,15 +363,21 @@ def utwobody_p(s, table):
     return dict(force=force, utwob=utwob, virial=vir.value)
 
 
-def velver_p(s, table, nsteps):
+def velver_p(s, table, nsteps, ewald=None):
     """nsteps of rigid-body VelVer (oracle) on a systems.rigid_bodies dict, advanced in place
-    (ro, rod, rodd, qua, quad, quadd, r).  Returns dict(utwob, virial) of the last step."""
+    (ro, rod, rodd, qua, quad, quadd, r).  ewald (optional): dict(az, ualpha, ncut, region,
+    lsurf) adds the site Ewald sum to every step.  Returns dict(utwob, virial[, urec]) of the
+    last step."""
     L = lib()
     if not getattr(L, "_velver_p_typed", False):
-        L.or_velver_p.restype = C.c_int
-        L.or_velver_p.argtypes = [C.c_int32] * 5 + [f64p, C.c_double, C.c_double, C.c_int32, C.c_double] + \
+        common = [C.c_int32] * 5 + [f64p, C.c_double, C.c_double, C.c_int32, C.c_double] + \
             [f64p] * 7 + [i32p] * 4 + [f64p, C.c_int32, f64p, f64p, i32p, i32p, C.c_int32, f64p, C.c_int32,
-                                         i32p, f64p, f64p, f64p]
+                                         i32p, f64p]
+        L.or_velver_p.restype = C.c_int
+        L.or_velver_p.argtypes = common + [f64p, f64p]
+        L.or_velver_p_ewald.restype = C.c_int
+        L.or_velver_p_ewald.argtypes = common + [f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                                 f64p, f64p, f64p]
         L._velver_p_typed = True
     k = {}
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r", "ra", "masspt", "momp"):
@@ -385,19 +391,29 @@ def velver_p(s, table, nsteps):
     utwob = np.zeros(npt * (npt + 1) // 2 + 1)
     vir = C.c_double()
     box = (C.c_double * 3)(*s["boxlen"])
-    rc = L.or_velver_p(int(nsteps), int(s["np"]), int(s["na"]), npt, int(s["nat"]), box, float(s["rcut"]),
-                       float(s["tstep"]), int(s["nvvite"]), float(s["tvvite"]),
-                       *[_p(k[x], C.c_double) for x in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r")],
-                       *[_p(k[x], C.c_int32) for x in ("iptpn", "ianpn", "napt", "iatan")],
-                       _p(k["ra"], C.c_double), int(s["maxsite"]), _p(k["masspt"], C.c_double),
-                       _p(k["momp"], C.c_double), _p(k["nneighpn"], C.c_int32), _p(k["jpnlist"], C.c_int32),
-                       int(k["jpnlist"].shape[1]), _p(ub, C.c_double), len(ub), _p(iub, C.c_int32),
-                       _p(r2, C.c_double), _p(utwob, C.c_double), C.byref(vir))
+    args = [int(nsteps), int(s["np"]), int(s["na"]), npt, int(s["nat"]), box, float(s["rcut"]),
+            float(s["tstep"]), int(s["nvvite"]), float(s["tvvite"]),
+            *[_p(k[x], C.c_double) for x in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r")],
+            *[_p(k[x], C.c_int32) for x in ("iptpn", "ianpn", "napt", "iatan")],
+            _p(k["ra"], C.c_double), int(s["maxsite"]), _p(k["masspt"], C.c_double),
+            _p(k["momp"], C.c_double), _p(k["nneighpn"], C.c_int32), _p(k["jpnlist"], C.c_int32),
+            int(k["jpnlist"].shape[1]), _p(ub, C.c_double), len(ub), _p(iub, C.c_int32), _p(r2, C.c_double)]
+    urec = C.c_double()
+    if ewald is None:
+        rc = L.or_velver_p(*args, _p(utwob, C.c_double), C.byref(vir))
+    else:
+        az = np.ascontiguousarray(ewald["az"], np.float64)
+        rc = L.or_velver_p_ewald(*args, _p(az, C.c_double), float(ewald["ualpha"]), int(ewald["ncut"]),
+                                 1 if ewald.get("region", "sphere") == "cube" else 0, int(bool(ewald.get("lsurf"))),
+                                 float(s["epsi_four_pi"]), _p(utwob, C.c_double), C.byref(urec), C.byref(vir))
     if rc:
         raise RuntimeError("VelVer (polyatomic) failed: %d" % rc)
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
         s[key] = k[key]
-    return dict(utwob=utwob, virial=vir.value)
+    out = dict(utwob=utwob, virial=vir.value)
+    if ewald is not None:
+        out["urec"] = urec.value
+    return out
 
 
 def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
