@@ -558,7 +558,44 @@ def run_poly(a):
         O.velver_p(ro, tb, 2)
         md["cpu_baseline"] = {"value": rb["np"] * 2 / (time.perf_counter() - t0), "unit": METRIC, "cores": 1,
                               "kind": "port", "sample": "two rigid-body steps of the same system, oracle, 1 thread"}
+    # the same rigid bodies with SPME over the sites (order 5, 96^3 mesh)
+    db = S.site_table_params(rb)
+    db["lewald"] = 1
+    tbs = pot_tab(db, 0.35)
+    ewb = dict(az=np.asarray(rb["zat"], np.float64)[np.asarray(rb["iatan"]) - 1], ualpha=0.35, order=5, nmesh=96)
+    velver_p(copy.deepcopy(rb), tbs, 2, ewald=ewb)    # warm-up
+    ms = velver_p(copy.deepcopy(rb), tbs, k, ewald=ewb)["kernel_ms"]
+    mds = {"workload": "16000 rigid 3-site molecules + 4000 solutes (52000 sites), L = 136 A, rc = 10 A, "
+                       "SPME over sites alpha = 0.35, order 5, 96^3, dt = 1 fs",
+           "steps": k, "ms_per_step": ms / k, "value": rb["np"] * k / (ms / 1000.0), "unit": METRIC}
+    if not a.no_cpu_baseline:
+        ro = copy.deepcopy(rb)
+        t0 = time.perf_counter()
+        O.velver_p(ro, tbs, 1, ewald=ewb)
+        mds["cpu_baseline"] = {"value": rb["np"] / (time.perf_counter() - t0), "unit": METRIC, "cores": 1,
+                               "kind": "port", "sample": "one rigid-body step with SPME over sites of the same "
+                                                         "system, oracle, 1 thread"}
+    md["rigid_md_spm_20000"] = mds
     out["rigid_md_20000"] = md
+    # SPME over the 130000 sites of the UTwoBodyP system (order 5, 128^3 mesh, alpha 0.35)
+    from molsim_b200.polyatomic import uewald_sites as _uew
+
+    azs = np.asarray(s["zat"], np.float64)[np.asarray(s["iatan"]) - 1]
+    _uew(s, azs, 0.35, order=5, nmesh=128)             # warm-up
+    kms, calls = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        kms.append(_uew(s, azs, 0.35, order=5, nmesh=128)["kernel_ms"])
+        calls.append((time.perf_counter() - t0) * 1000.0)
+    km = float(np.median(kms))
+    sp = {"workload": "SPME over the 130000 sites of the system above, alpha = 0.35, order 5, 128^3",
+          "kernel_ms": km, "call_ms": float(np.median(calls)), "value": s["na"] / (km / 1000.0), "unit": "sites/s"}
+    if not a.no_cpu_baseline:
+        t0 = time.perf_counter()
+        O.uewald_sites(s, azs, 0.35, order=5, nmesh=128)
+        sp["cpu_baseline"] = {"value": s["na"] / (time.perf_counter() - t0), "unit": "sites/s", "cores": 1,
+                              "kind": "port", "sample": "one SPME site sum of the same system, oracle, 1 thread"}
+    out["uewald_sites_spm_130000"] = sp
     # UEwald over sites: 4000 rigid 3-site molecules (12000 sites), standard Ewald, alpha 0.35
     from molsim_b200.polyatomic import uewald_sites
 

@@ -30,6 +30,7 @@
  *   msg_uewald_sites               -> UEwald over the sites of polyatomic particles: UEwaldRecStd,
  *                                     UEwaldSelf with its molecular term, UEwaldSurf
  *                                     (Src/energy.F90:905-1104, 1301-1371)
+ *   msg_uewald_sites_spm           -> the same with UEwaldRecSPM (Src/energy.F90:1207-1297)
  *   msg_mc_seed / msg_mc_pass      -> MCDriver iSimulationStep: MCPass with SPartMove
  *                                     (Src/mc.F90:1470-1755), DUTotal, Metropolis, MCUpdate
  *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
@@ -332,20 +333,38 @@ int  msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t
                       const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
                       double *force, double *urec, double *virrec, float *kernel_ms);
 
-/* msg_velver_p with lewald: every step adds the site Ewald sum of msg_uewald_sites (site
- * charges az [na], ualpha, ncut, ncutregion, lsurf, epsfp) to the site forces before the
- * forces, torques and molecular virial (UTotal, Src/energy.F90:335-352, 403-426), and its
- * reciprocal virial to virial; urec = u%rec of the last step.  The table ubuf carries the
- * erfc-screened site pairs (lewald in PotTwoBodyTab).  MSG_ERR_ARG as msg_uewald_sites. */
+/* The site Ewald sum of msg_velver_p_ewald: MOLSIM's txewaldrec over the sites. */
+typedef struct msg_site_ewald {
+    int32_t lewald;                 /* 1: SPME ('spm'), 2: standard Ewald ('std') */
+    int32_t order, nmesh;           /* SPME: spline order 4..8, mesh edge (even) */
+    int32_t ncut, ncutregion;       /* standard Ewald: 1..100; 0 sphere, 1 cube */
+    int32_t lsurf;                  /* UEwaldSurf */
+    double ualpha, epsi_four_pi;
+    const double *az;               /* [na] site charges, zat(iatan(ia)) */
+} msg_site_ewald;
+
+/* msg_uewald_sites with SPME over the sites (UEwaldRecSPM, Src/energy.F90:1207-1297, with
+ * SPMFFTRec :6525-6587 and EwaldSetup's mesh factors :6980-7018): spline order 4..8, nmesh
+ * even, 8..1024.  The charge mesh is spread in 64-bit fixed point, so the result repeats
+ * bit for bit. */
+int  msg_uewald_sites_spm(int32_t na, const double boxlen[3], double ualpha, int32_t order, int32_t nmesh,
+                          int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                          const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
+                          double *force, double *urec, double *virrec, float *kernel_ms);
+
+/* msg_velver_p with lewald: every step adds the site Ewald sum (as msg_uewald_sites or
+ * msg_uewald_sites_spm computes it) to the site forces before the forces, torques and
+ * molecular virial (UTotal, Src/energy.F90:335-352, 403-426), and its reciprocal virial to
+ * virial; urec = u%rec of the last step.  The table ubuf carries the erfc-screened site
+ * pairs (lewald in PotTwoBodyTab).  MSG_ERR_ARG as the site Ewald calls. */
 int  msg_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
                         double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod,
                         double *rodd, double *qua, double *quad, double *quadd, double *r, const int32_t *iptpn,
                         const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
                         int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
                         const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
-                        const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha,
-                        int32_t ncut, int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob, double *urec,
-                        double *virial, float *kernel_ms);
+                        const int32_t *iubuflow, const double *r2umin, const msg_site_ewald *ew, double *utwob,
+                        double *urec, double *virial, float *kernel_ms);
 
 /* Set-up helpers (host only). */
 double msg_rcut_to_alpha(double uewaldtol, double q2sum, double epsi_four_pi,

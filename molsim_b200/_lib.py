@@ -46,6 +46,12 @@ class MsgMcParams(C.Structure):
     _fields_ = [("beta", C.c_double), ("dtran", f64p), ("isamp", C.c_int32), ("pad", C.c_int32)]
 
 
+class MsgSiteEwald(C.Structure):
+    _fields_ = [("lewald", C.c_int32), ("order", C.c_int32), ("nmesh", C.c_int32), ("ncut", C.c_int32),
+                ("ncutregion", C.c_int32), ("lsurf", C.c_int32), ("ualpha", C.c_double),
+                ("epsi_four_pi", C.c_double), ("az", f64p)]
+
+
 class MsgTabParams(C.Structure):
     _fields_ = [("npt", C.c_int32), ("zat", f64p), ("sigat", f64p), ("epsat", f64p), ("rcut", C.c_double),
                 ("ualpha", C.c_double), ("epsi_four_pi", C.c_double), ("lewald", C.c_int32),
@@ -73,14 +79,16 @@ SIGNATURES = {
                                    f64p, f64p, C.POINTER(C.c_float)]),
     "msg_velver_p_ewald": (C.c_int, [C.c_int32] * 5 + [f64p, C.c_double, C.c_double, C.c_int32, C.c_double] +
                            [f64p] * 7 + [i32p] * 4 + [f64p, C.c_int32, f64p, f64p, i32p, i32p, C.c_int32, f64p,
-                                                      C.c_int32, i32p, f64p, f64p, C.c_double, C.c_int32,
-                                                      C.c_int32, C.c_int32, C.c_double, f64p, f64p, f64p,
-                                                      C.POINTER(C.c_float)]),
+                                                      C.c_int32, i32p, f64p, C.POINTER(MsgSiteEwald), f64p, f64p,
+                                                      f64p, C.POINTER(C.c_float)]),
     "msg_utwobody_p": (C.c_int, [C.c_int32] * 4 + [f64p, C.c_double, f64p, f64p] + [i32p] * 6 +
                        [C.c_int32, f64p, C.c_int32, i32p, f64p, f64p, f64p, f64p, C.POINTER(C.c_float)]),
     "msg_uewald_sites": (C.c_int, [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double, f64p,
                                    f64p, C.c_int32, i32p, i32p, i32p, C.c_int32, f64p, f64p, f64p,
                                    C.POINTER(C.c_float)]),
+    "msg_uewald_sites_spm": (C.c_int, [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                       f64p, f64p, C.c_int32, i32p, i32p, i32p, C.c_int32, f64p, f64p, f64p,
+                                       C.POINTER(C.c_float)]),
     "msg_mc_pass": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(MsgMcParams), C.POINTER(C.c_int64),
                               C.POINTER(C.c_int64), C.c_int32, C.POINTER(MsgEnergy)]),
     "msg_get_forces": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p]),

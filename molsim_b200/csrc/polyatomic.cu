@@ -19,7 +19,11 @@
 #include <cmath>
 #include <vector>
 
+#include <cufft.h>
+
 #include "../../include/molsim_gpu.h"
+#include "common.cuh"
+#include "setup.h"
 
 namespace {
 
@@ -745,29 +749,158 @@ __global__ void k_site_self(int np, double alpha, double ewaldfac1, double epsfp
     if ((threadIdx.x & 31) == 0 && eu) atomicAdd(efix + 2, (unsigned long long)eu);
 }
 
+// ---- SPME over the sites (UEwaldRecSPM + SPMFFTRec, Src/energy.F90:1207-1297, 6525-6587) ----
+// the charge mesh in 64-bit fixed point at 2^-40 while it is spread, so it repeats bit for bit
+constexpr double kGFix = 1099511627776.0;
+constexpr double kGFixInv = 1.0 / 1099511627776.0;
+
+// Q(k - i) += q Mx My Mz over the site's order^3 mesh points (Src/energy.F90:1226-1245).
+template <int P>
+__global__ void k_sspm_spread(int na, int s, double3 dkdr, const double *__restrict__ r,
+                              const double *__restrict__ az, unsigned long long *__restrict__ igrid)
+{
+    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ia >= na) return;
+    const double dk[3] = {dkdr.x, dkdr.y, dkdr.z};
+    double th[3][P], dth[3][P];
+    int km[3];
+    for (int m = 0; m < 3; ++m) km[m] = msg::bspline_at<P, double>(dk[m] * r[3 * (size_t)ia + m], s, th[m], dth[m]);
+    const double q = az[ia];
+    for (int iz = 0; iz < P; ++iz) {
+        int nz = km[2] - iz;
+        nz += (nz < 0) ? s : 0;
+        const double qz = q * th[2][iz];
+        for (int iy = 0; iy < P; ++iy) {
+            int ny = km[1] - iy;
+            ny += (ny < 0) ? s : 0;
+            const double qyz = qz * th[1][iy];
+            for (int ix = 0; ix < P; ++ix) {
+                int nx = km[0] - ix;
+                nx += (nx < 0) ? s : 0;
+                const double v = qyz * th[0][ix];
+                atomicAdd(igrid + ((size_t)nz * s + ny) * s + nx, (unsigned long long)__double2ll_rn(v * kGFix));
+            }
+        }
+    }
+}
+
+// The fixed-point mesh to FP64 for the transform, cleared for the next spread.
+__global__ void k_sspm_to_f64(size_t n, unsigned long long *__restrict__ igrid, double *__restrict__ grid)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        grid[k] = (double)(long long)igrid[k] * kGFixInv;
+        igrid[k] = 0ull;
+    }
+}
+
+// F *= meshfac; energy |F|^2 emf and virial -|F|^2 vmf over the r2c half spectrum (the
+// reference's mirror loop resolved into per-entry weights; Src/energy.F90:6550-6578), summed
+// in 64-bit fixed point (2^-40).
+__global__ void __launch_bounds__(256) k_sspm_influence(int s, double2 *__restrict__ cg, const double *__restrict__ mfac,
+                                                        const double *__restrict__ emf, const double *__restrict__ vmf,
+                                                        unsigned long long *__restrict__ efix)
+{
+    const int h = s / 2 + 1;
+    const size_t n = (size_t)s * s * h;
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    long long e = 0, v = 0;
+    if (c < n) {
+        const int kx = (int)(c % h), rr = (int)(c / h), ky = rr % s, kz = rr / s;
+        const int fy = ky <= s / 2 ? ky : s - ky, fz = kz <= s / 2 ? kz : s - kz;
+        const size_t f = kx + (size_t)h * (fy + (size_t)h * fz);
+        double2 q = cg[c];
+        const double q2 = q.x * q.x + q.y * q.y, m = mfac[f];
+        q.x *= m;
+        q.y *= m;
+        cg[c] = q;
+        e = __double2ll_rn(q2 * emf[f] * kPFix);
+        v = __double2ll_rn(-(q2 * vmf[f]) * kPFix);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (e) atomicAdd(efix, (unsigned long long)e);
+        if (v) atomicAdd(efix + 1, (unsigned long long)v);
+    }
+}
+
+// The sites' reciprocal forces from the convolved mesh (Src/energy.F90:1258-1285), less the
+// surface term's force when sfac = 2 fac is not 0; stored, or added when add is set.
+template <int P>
+__global__ void k_sspm_gather(int na, int s, double3 dkdr, int add, double epsfp, double sfac,
+                              const double *__restrict__ r, const double *__restrict__ az,
+                              const double *__restrict__ grid, const unsigned long long *__restrict__ efix,
+                              double *__restrict__ force)
+{
+    const int ia = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ia >= na) return;
+    const double dk[3] = {dkdr.x, dkdr.y, dkdr.z};
+    double th[3][P], dth[3][P];
+    int km[3];
+    for (int m = 0; m < 3; ++m) km[m] = msg::bspline_at<P, double>(dk[m] * r[3 * (size_t)ia + m], s, th[m], dth[m]);
+    double es[3] = {0.0, 0.0, 0.0};
+    for (int iz = 0; iz < P; ++iz) {
+        int nz = km[2] - iz;
+        nz += (nz < 0) ? s : 0;
+        for (int iy = 0; iy < P; ++iy) {
+            int ny = km[1] - iy;
+            ny += (ny < 0) ? s : 0;
+            const double *row = grid + ((size_t)nz * s + ny) * s;
+            for (int ix = 0; ix < P; ++ix) {
+                int nx = km[0] - ix;
+                nx += (nx < 0) ? s : 0;
+                const double Q = row[nx];
+                es[0] = es[0] + dth[0][ix] * th[1][iy] * th[2][iz] * Q;
+                es[1] = es[1] + th[0][ix] * dth[1][iy] * th[2][iz] * Q;
+                es[2] = es[2] + th[0][ix] * th[1][iy] * dth[2][iz] * Q;
+            }
+        }
+    }
+    const double q = az[ia];
+    for (int m = 0; m < 3; ++m) {
+        double f = -(q * es[m] * dk[m] * epsfp);
+        if (sfac != 0.0) f = f - epsfp * sfac * q * ((double)(long long)efix[3 + m] * kDipFixInv);
+        double *o = force + 3 * (size_t)ia + m;
+        *o = add ? *o + f : f;
+    }
+}
+
 // The site Ewald sum of one system: set-up on the host (k-vectors, kfac, launch shapes,
 // device buffers) and a launch sequence on the caller's device arrays, so one set-up
 // serves every step of a run.  Device accumulators efix: reciprocal energy, its virial,
 // the molecular self energy (2^-40) and the dipole sum (2^-32).
 struct SiteEwald {
-    int na = 0, np = 0, nkv = 0, w = 0, lsurf = 0;
-    int ktiles = 0, ptiles = 0, clen = 0, nchunk = 0, klen = 0, nks = 0, sub = 0;
+    int lewald = 0;                 // 1: SPME over the sites, 2: standard Ewald
+    int na = 0, np = 0, lsurf = 0;
     double alpha = 0.0, epsfp = 0.0, vol = 0.0, q2 = 0.0, ewaldfac1 = 0.0;
+    double *daz = nullptr;
+    unsigned long long *efix = nullptr;
+    // standard Ewald
+    int nkv = 0, w = 0, ktiles = 0, ptiles = 0, clen = 0, nchunk = 0, klen = 0, nks = 0, sub = 0;
     double3 tpbi = make_double3(0.0, 0.0, 0.0);
-    double *daz = nullptr, *dkf = nullptr, *fks = nullptr;
+    double *dkf = nullptr, *fks = nullptr;
     int4 *dkv = nullptr;
     double2 *eik = nullptr, *part = nullptr, *sk = nullptr;
-    unsigned long long *efix = nullptr;
+    // SPME
+    int smesh = 0, order = 0;
+    double3 dkdr = make_double3(0.0, 0.0, 0.0);
+    unsigned long long *igrid = nullptr;
+    double *grid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
+    double2 *cgrid = nullptr;
+    cufftHandle pf = 0, pb = 0;
+    bool plans = false;
 
     static constexpr double kPi = 3.1415926535897932;
 
-    // MSG_ERR_ARG for arguments outside what the reference accepts, else the CUDA status.
-    int setup(int32_t na_, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion, int32_t lsurf_,
-              double epsfp_, const double *az, int32_t np_, const int32_t *iptpn, const int32_t *ianpn,
-              const int32_t *napt, int32_t npt)
+    // Checks and the parts both methods share.  MSG_ERR_ARG for arguments outside what the
+    // reference accepts, else the CUDA status.
+    int common(int32_t na_, const double boxlen[3], double ualpha, int32_t lsurf_, double epsfp_, const double *az,
+               int32_t np_, const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt)
     {
-        if (na_ < 1 || np_ < 1 || npt < 1 || ncut < 1 || ncut > kSMaxCut || ncutregion < 0 || ncutregion > 1 ||
-            !(ualpha > 0.0) || !boxlen || !az || !iptpn || !ianpn || !napt)
+        if (na_ < 1 || np_ < 1 || npt < 1 || !(ualpha > 0.0) || !boxlen || !az || !iptpn || !ianpn || !napt)
             return MSG_ERR_ARG;
         for (int t = 0; t < npt; ++t)
             if (napt[t] < 1) return MSG_ERR_ARG;
@@ -780,10 +913,25 @@ struct SiteEwald {
         alpha = ualpha;
         epsfp = epsfp_;
         vol = boxlen[0] * boxlen[1] * boxlen[2];
-        tpbi = make_double3(2.0 * kPi * (1.0 / boxlen[0]), 2.0 * kPi * (1.0 / boxlen[1]), 2.0 * kPi * (1.0 / boxlen[2]));
         ewaldfac1 = (1.0 / (std::sqrt(kPi) * ualpha)) * 2.0 * (ualpha * ualpha);
         q2 = 0.0;
         for (int a = 0; a < na; ++a) q2 += az[a] * az[a];
+        cudaError_t e = cudaSuccess;
+        daz = dev_copy(az, (size_t)na, e);
+        if (e == cudaSuccess) e = cudaMalloc(&efix, 6 * sizeof(unsigned long long));
+        return e == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
+    }
+
+    // Standard Ewald (txewaldrec 'std'): ncut 1..100, ncutregion 0 sphere / 1 cube.
+    int setup(int32_t na_, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion, int32_t lsurf_,
+              double epsfp_, const double *az, int32_t np_, const int32_t *iptpn, const int32_t *ianpn,
+              const int32_t *napt, int32_t npt)
+    {
+        if (ncut < 1 || ncut > kSMaxCut || ncutregion < 0 || ncutregion > 1) return MSG_ERR_ARG;
+        const int rc = common(na_, boxlen, ualpha, lsurf_, epsfp_, az, np_, iptpn, ianpn, napt, npt);
+        if (rc != MSG_OK) return rc;
+        lewald = 2;
+        tpbi = make_double3(2.0 * kPi * (1.0 / boxlen[0]), 2.0 * kPi * (1.0 / boxlen[1]), 2.0 * kPi * (1.0 / boxlen[2]));
         // k-vectors and kfac in the order of EwaldSetup 'std' (Src/energy.F90:6762-6782)
         std::vector<int4> kv;
         std::vector<double> kf;
@@ -812,15 +960,63 @@ struct SiteEwald {
         nks = (nkv + klen - 1) / klen;
         sub = std::max(1, std::min(16, kSSmem / (3 * w * (int)sizeof(double2))));
         cudaError_t e = cudaSuccess;
-        daz = dev_copy(az, (size_t)na, e);
         dkf = dev_copy(kf.data(), kf.size(), e);
         dkv = dev_copy(kv.data(), kv.size(), e);
         if (e == cudaSuccess) e = cudaMalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
         if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
         if (e == cudaSuccess) e = cudaMalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
         if (e == cudaSuccess) e = cudaMalloc(&fks, (size_t)nks * 3 * na * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&efix, 6 * sizeof(unsigned long long));
         return e == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
+    }
+
+    // SPME (txewaldrec 'spm'): order 4..8, nmesh even, 8..1024 (EwaldSetup SPM branch,
+    // Src/energy.F90:6980-7018, for the mesh factors).
+    int setup_spm(int32_t na_, const double boxlen[3], double ualpha, int32_t order_, int32_t nmesh, int32_t lsurf_,
+                  double epsfp_, const double *az, int32_t np_, const int32_t *iptpn, const int32_t *ianpn,
+                  const int32_t *napt, int32_t npt)
+    {
+        if (order_ < 4 || order_ > 8 || nmesh < 8 || nmesh > 1024 || (nmesh & 1)) return MSG_ERR_ARG;
+        const int rc = common(na_, boxlen, ualpha, lsurf_, epsfp_, az, np_, iptpn, ianpn, napt, npt);
+        if (rc != MSG_OK) return rc;
+        lewald = 1;
+        smesh = nmesh;
+        order = order_;
+        dkdr = make_double3(nmesh / boxlen[0], nmesh / boxlen[1], nmesh / boxlen[2]);
+        const int h = nmesh / 2 + 1;
+        const size_t nf = (size_t)h * h * h, ng = (size_t)nmesh * nmesh * nmesh, nc = (size_t)nmesh * nmesh * h;
+        std::vector<double> hm(nf), he(nf), hv(nf);
+        msg::spme_factors(nmesh, order, ualpha, boxlen, hm.data(), he.data(), hv.data());
+        cudaError_t e = cudaSuccess;
+        mfac = dev_copy(hm.data(), nf, e);
+        emf = dev_copy(he.data(), nf, e);
+        vmf = dev_copy(hv.data(), nf, e);
+        if (e == cudaSuccess) e = cudaMalloc(&igrid, ng * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemset(igrid, 0, ng * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMalloc(&grid, ng * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&cgrid, nc * sizeof(double2));
+        if (e != cudaSuccess) return MSG_ERR_CUDA;
+        if (cufftPlan3d(&pf, nmesh, nmesh, nmesh, CUFFT_D2Z) != CUFFT_SUCCESS) return MSG_ERR_CUDA;
+        if (cufftPlan3d(&pb, nmesh, nmesh, nmesh, CUFFT_Z2D) != CUFFT_SUCCESS) {
+            cufftDestroy(pf);
+            return MSG_ERR_CUDA;
+        }
+        plans = true;
+        return MSG_OK;
+    }
+
+    template <int P>
+    void launch_spm(const double *dr, double *dforce, int add, double sfac, cudaStream_t st) const
+    {
+        const size_t ng = (size_t)smesh * smesh * smesh, nc = (size_t)smesh * smesh * (smesh / 2 + 1);
+        k_sspm_spread<P><<<(na + 127) / 128, 128, 0, st>>>(na, smesh, dkdr, dr, daz, igrid);
+        k_sspm_to_f64<<<(unsigned)((ng + 255) / 256), 256, 0, st>>>(ng, igrid, grid);
+        cufftSetStream(pf, st);
+        cufftExecD2Z(pf, grid, reinterpret_cast<cufftDoubleComplex *>(cgrid));
+        k_sspm_influence<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(smesh, cgrid, mfac, emf, vmf, efix);
+        cufftSetStream(pb, st);
+        cufftExecZ2D(pb, reinterpret_cast<cufftDoubleComplex *>(cgrid), grid);
+        k_sspm_gather<P><<<(na + 127) / 128, 128, 0, st>>>(na, smesh, dkdr, add, epsfp, sfac, dr, daz, grid, efix,
+                                                           dforce);
     }
 
     // One evaluation at the sites dr: the Ewald forces stored into dforce (add = 0) or added
@@ -829,17 +1025,27 @@ struct SiteEwald {
                 cudaStream_t st) const
     {
         cudaMemsetAsync(efix, 0, 6 * sizeof(unsigned long long), st);
-        k_site_eik<<<(na + 127) / 128, 128, 0, st>>>(na, w, tpbi, dr, daz, eik);
-        k_site_sk<<<dim3(ktiles, nchunk), kSK, (size_t)sub * 3 * w * sizeof(double2), st>>>(na, nkv, w, clen, sub,
-                                                                                          dkv, eik, part);
-        k_site_reduce<<<ktiles, kSK, 0, st>>>(nkv, nchunk, alpha * alpha, tpbi, dkv, dkf, part, sk, efix);
-        k_site_force<<<dim3(ptiles, nks), kSF, 0, st>>>(na, nkv, klen, epsfp, tpbi, dr, daz, dkv, dkf, sk, fks);
         double sfac = 0.0;
         if (lsurf) {
             k_site_dipole<<<(na + 127) / 128, 128, 0, st>>>(na, dr, daz, efix);
             sfac = 2.0 * (2.0 * kPi / (3.0 * vol));
         }
-        k_site_fsum<<<(3 * na + 255) / 256, 256, 0, st>>>(na, nks, add, epsfp, sfac, daz, efix, fks, dforce);
+        if (lewald == 2) {
+            k_site_eik<<<(na + 127) / 128, 128, 0, st>>>(na, w, tpbi, dr, daz, eik);
+            k_site_sk<<<dim3(ktiles, nchunk), kSK, (size_t)sub * 3 * w * sizeof(double2), st>>>(na, nkv, w, clen, sub,
+                                                                                              dkv, eik, part);
+            k_site_reduce<<<ktiles, kSK, 0, st>>>(nkv, nchunk, alpha * alpha, tpbi, dkv, dkf, part, sk, efix);
+            k_site_force<<<dim3(ptiles, nks), kSF, 0, st>>>(na, nkv, klen, epsfp, tpbi, dr, daz, dkv, dkf, sk, fks);
+            k_site_fsum<<<(3 * na + 255) / 256, 256, 0, st>>>(na, nks, add, epsfp, sfac, daz, efix, fks, dforce);
+        } else {
+            switch (order) {
+            case 4: launch_spm<4>(dr, dforce, add, sfac, st); break;
+            case 5: launch_spm<5>(dr, dforce, add, sfac, st); break;
+            case 6: launch_spm<6>(dr, dforce, add, sfac, st); break;
+            case 7: launch_spm<7>(dr, dforce, add, sfac, st); break;
+            default: launch_spm<8>(dr, dforce, add, sfac, st); break;
+            }
+        }
         k_site_self<<<(np + 127) / 128, 128, 0, st>>>(np, alpha, ewaldfac1, epsfp, dr, daz, dipt, dian, dnapt, dforce,
                                                       efix);
     }
@@ -867,24 +1073,25 @@ struct SiteEwald {
 
     ~SiteEwald()
     {
-        for (void *p : {(void *)daz, (void *)dkf, (void *)dkv, (void *)eik, (void *)part, (void *)sk, (void *)fks,
-                        (void *)efix})
+        if (plans) {
+            cufftDestroy(pf);
+            cufftDestroy(pb);
+        }
+        for (void *p : {(void *)daz, (void *)efix, (void *)dkf, (void *)dkv, (void *)eik, (void *)part, (void *)sk,
+                        (void *)fks, (void *)igrid, (void *)grid, (void *)cgrid, (void *)mfac, (void *)emf,
+                        (void *)vmf})
             if (p) cudaFree(p);
     }
 };
 
 }  // namespace
 
-extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
-                                int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
-                                const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
-                                double *force, double *urec, double *virrec, float *kernel_ms)
+// One site Ewald evaluation of host arrays through a set-up SiteEwald.
+static int uewald_sites_call(const SiteEwald &E, int32_t na, const double *r, int32_t np, const int32_t *iptpn,
+                             const int32_t *ianpn, const int32_t *napt, int32_t npt, double *force, double *urec,
+                             double *virrec, float *kernel_ms)
 {
-    if (!r || !force || !urec || !virrec) return MSG_ERR_ARG;
-    SiteEwald E;
-    const int rc = E.setup(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
-    if (rc == MSG_ERR_ARG) return rc;
-    cudaError_t e = rc == MSG_OK ? cudaSuccess : cudaErrorMemoryAllocation;
+    cudaError_t e = cudaSuccess;
     double *dr = dev_copy(r, 3 * (size_t)na, e), *dforce = nullptr;
     int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e), *dnapt = dev_copy(napt, (size_t)npt, e);
     if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
@@ -914,6 +1121,36 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
         return MSG_ERR_CUDA;
     }
     return MSG_OK;
+}
+
+extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
+                                int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                                const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
+                                double *force, double *urec, double *virrec, float *kernel_ms)
+{
+    if (!r || !force || !urec || !virrec) return MSG_ERR_ARG;
+    SiteEwald E;
+    const int rc = E.setup(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
+    if (rc != MSG_OK) {
+        cudaGetLastError();
+        return rc;
+    }
+    return uewald_sites_call(E, na, r, np, iptpn, ianpn, napt, npt, force, urec, virrec, kernel_ms);
+}
+
+extern "C" int msg_uewald_sites_spm(int32_t na, const double boxlen[3], double ualpha, int32_t order, int32_t nmesh,
+                                    int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                                    const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
+                                    double *force, double *urec, double *virrec, float *kernel_ms)
+{
+    if (!r || !force || !urec || !virrec) return MSG_ERR_ARG;
+    SiteEwald E;
+    const int rc = E.setup_spm(na, boxlen, ualpha, order, nmesh, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
+    if (rc != MSG_OK) {
+        cudaGetLastError();
+        return rc;
+    }
+    return uewald_sites_call(E, na, r, np, iptpn, ianpn, napt, npt, force, urec, virrec, kernel_ms);
 }
 
 // The rigid-body MD steps of msg_velver_p and msg_velver_p_ewald: ew (optional) adds the
@@ -1083,13 +1320,16 @@ extern "C" int msg_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_
                                   const int32_t *iatan, const double *ra, int32_t maxsite, const double *masspt,
                                   const double *momp, const int32_t *nneighpn, const int32_t *jpnlist,
                                   int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
-                                  const double *r2umin, const double *az, double ualpha, int32_t ncut,
-                                  int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob, double *urec,
+                                  const double *r2umin, const msg_site_ewald *ew, double *utwob, double *urec,
                                   double *virial, float *kernel_ms)
 {
-    if (!urec) return MSG_ERR_ARG;
+    if (!urec || !ew || (ew->lewald != 1 && ew->lewald != 2)) return MSG_ERR_ARG;
     SiteEwald E;
-    const int rc = E.setup(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
+    const int rc = ew->lewald == 2
+                       ? E.setup(na, boxlen, ew->ualpha, ew->ncut, ew->ncutregion, ew->lsurf, ew->epsi_four_pi, ew->az,
+                                 np, iptpn, ianpn, napt, npt)
+                       : E.setup_spm(na, boxlen, ew->ualpha, ew->order, ew->nmesh, ew->lsurf, ew->epsi_four_pi,
+                                     ew->az, np, iptpn, ianpn, napt, npt);
     if (rc != MSG_OK) {
         cudaGetLastError();
         return rc;

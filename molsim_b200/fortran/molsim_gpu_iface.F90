@@ -51,6 +51,16 @@ module MolsimGpu
       integer(c_int32_t) :: isamp, pad
    end type msg_mc_params
 
+   ! struct msg_site_ewald
+   type, bind(c) :: msg_site_ewald
+      integer(c_int32_t) :: lewald               ! 1: 'spm', 2: 'std'
+      integer(c_int32_t) :: order, nmesh         ! SPME
+      integer(c_int32_t) :: ncut, ncutregion     ! standard Ewald (0 sphere, 1 cube)
+      integer(c_int32_t) :: lsurf
+      real(c_double)     :: ualpha, epsi_four_pi
+      type(c_ptr)        :: az                   ! c_loc(az(1:na))
+   end type msg_site_ewald
+
    interface
       integer(c_int) function msg_create(p, precision, h) bind(c, name='msg_create')
          import :: c_int, c_int32_t, c_ptr, msg_params
@@ -154,9 +164,9 @@ module MolsimGpu
 
       integer(c_int) function msg_velver_p_ewald(nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, &
             ro, rod, rodd, qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, &
-            jpnlist, maxnneigh, ubuf, nbuf, iubuflow, r2umin, az, ualpha, ncut, ncutregion, lsurf, epsfp, utwob, &
-            urec, virial, kernel_ms) bind(c, name='msg_velver_p_ewald')
-         import :: c_int, c_int32_t, c_double, c_ptr
+            jpnlist, maxnneigh, ubuf, nbuf, iubuflow, r2umin, ew, utwob, urec, virial, kernel_ms) &
+            bind(c, name='msg_velver_p_ewald')
+         import :: c_int, c_int32_t, c_double, c_ptr, msg_site_ewald
          integer(c_int32_t), value :: nsteps, np, na, npt, nat
          real(c_double), intent(in) :: boxlen(3)
          real(c_double), value     :: rcut, tstep
@@ -168,10 +178,8 @@ module MolsimGpu
          integer(c_int32_t), value :: maxnneigh
          type(c_ptr), value        :: ubuf
          integer(c_int32_t), value :: nbuf
-         type(c_ptr), value        :: iubuflow, r2umin, az
-         real(c_double), value     :: ualpha
-         integer(c_int32_t), value :: ncut, ncutregion, lsurf
-         real(c_double), value     :: epsfp
+         type(c_ptr), value        :: iubuflow, r2umin
+         type(msg_site_ewald), intent(in) :: ew
          type(c_ptr), value        :: utwob
          real(c_double), intent(out) :: urec, virial
          type(c_ptr), value        :: kernel_ms
@@ -193,6 +201,23 @@ module MolsimGpu
          real(c_double), intent(out) :: urec, virrec
          type(c_ptr), value        :: kernel_ms
       end function msg_uewald_sites
+
+      integer(c_int) function msg_uewald_sites_spm(na, boxlen, ualpha, order, nmesh, lsurf, epsfp, r, az, np, &
+            iptpn, ianpn, napt, npt, force, urec, virrec, kernel_ms) bind(c, name='msg_uewald_sites_spm')
+         import :: c_int, c_int32_t, c_double, c_ptr
+         integer(c_int32_t), value :: na
+         real(c_double), intent(in) :: boxlen(3)
+         real(c_double), value     :: ualpha
+         integer(c_int32_t), value :: order, nmesh, lsurf
+         real(c_double), value     :: epsfp
+         type(c_ptr), value        :: r, az
+         integer(c_int32_t), value :: np
+         type(c_ptr), value        :: iptpn, ianpn, napt
+         integer(c_int32_t), value :: npt
+         type(c_ptr), value        :: force
+         real(c_double), intent(out) :: urec, virrec
+         type(c_ptr), value        :: kernel_ms
+      end function msg_uewald_sites_spm
 
       integer(c_int) function msg_mc_seed(h, isys, iseed) bind(c, name='msg_mc_seed')
          import :: c_int, c_int32_t, c_ptr

@@ -44,11 +44,22 @@ def utwobody_p(s, table):
     return dict(force=force, utwob=utwob, virial=vir.value, kernel_ms=ms.value)
 
 
+def site_ewald_params(ewald, epsi_four_pi, az):
+    """msg_site_ewald from dict(ualpha, lsurf and either ncut, region (standard Ewald) or
+    order, nmesh (SPME)); az must stay alive while the struct is used."""
+    spm = "nmesh" in ewald
+    return _lib.MsgSiteEwald(1 if spm else 2, int(ewald.get("order", 0)), int(ewald.get("nmesh", 0)),
+                             int(ewald.get("ncut", 0)), 1 if ewald.get("region", "sphere") == "cube" else 0,
+                             int(bool(ewald.get("lsurf"))), float(ewald["ualpha"]), float(epsi_four_pi),
+                             _p(az, C.c_double))
+
+
 def velver_p(s, table, nsteps=1, ewald=None):
     """nsteps of the rigid-body MD step for a systems.rigid_bodies dict, its state (ro, rod,
-    rodd, qua, quad, quadd, r) advanced in place.  ewald (optional): dict(az, ualpha, ncut,
-    region, lsurf) adds the site Ewald sum (msg_velver_p_ewald) to every step.  Returns
-    dict(utwob, virial, kernel_ms[, urec]) of the last step."""
+    rodd, qua, quad, quadd, r) advanced in place.  ewald (optional): dict(az, ualpha, lsurf and
+    either ncut, region (standard Ewald) or order, nmesh (SPME)) adds the site Ewald sum
+    (msg_velver_p_ewald) to every step.  Returns dict(utwob, virial, kernel_ms[, urec]) of
+    the last step."""
     k = {}
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r", "ra", "masspt", "momp"):
         k[key] = np.ascontiguousarray(s[key], np.float64)
@@ -79,10 +90,9 @@ def velver_p(s, table, nsteps=1, ewald=None):
         az = np.ascontiguousarray(ewald["az"], np.float64)
         if az.shape != (int(s["na"]),):
             raise ValueError("ewald['az'] must hold one charge per site")
-        rc = _lib.lib().msg_velver_p_ewald(*args, _p(az, C.c_double), float(ewald["ualpha"]), int(ewald["ncut"]),
-                                           1 if ewald.get("region", "sphere") == "cube" else 0,
-                                           int(bool(ewald.get("lsurf"))), float(s["epsi_four_pi"]),
-                                           _p(utwob, C.c_double), C.byref(urec), C.byref(vir), C.byref(ms))
+        ep = site_ewald_params(ewald, s["epsi_four_pi"], az)
+        rc = _lib.lib().msg_velver_p_ewald(*args, C.byref(ep), _p(utwob, C.c_double), C.byref(urec), C.byref(vir),
+                                           C.byref(ms))
     if rc:
         raise MolsimGpuError(rc, name)
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
@@ -93,11 +103,12 @@ def velver_p(s, table, nsteps=1, ewald=None):
     return out
 
 
-def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
+def uewald_sites(s, az, ualpha, ncut=None, region="sphere", lsurf=False, order=None, nmesh=None):
     """UEwald over the sites of polyatomic system s with site charges az [na]: the standard
-    reciprocal sum with ncut (region 'sphere' or 'cube'), the atomic and molecular self
-    terms and, when lsurf, the surface term.  Returns dict(force [na][3], urec, virrec,
-    kernel_ms), urec and virrec scaled by EpsiFourPi as UEwald does."""
+    reciprocal sum with ncut (region 'sphere' or 'cube'; msg_uewald_sites) or SPME with order
+    and nmesh (msg_uewald_sites_spm), the atomic and molecular self terms and, when lsurf,
+    the surface term.  Returns dict(force [na][3], urec, virrec, kernel_ms), urec and virrec
+    scaled by EpsiFourPi as UEwald does."""
     r = np.ascontiguousarray(s["r"], np.float64)
     q = np.ascontiguousarray(az, np.float64)
     ipt = np.ascontiguousarray(s["iptpn"], np.int32)
@@ -112,10 +123,13 @@ def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
     ms = C.c_float()
     box = (C.c_double * 3)(*s["boxlen"])
     i32 = C.c_int32
-    rc = _lib.lib().msg_uewald_sites(na, box, float(ualpha), int(ncut), 1 if region == "cube" else 0, int(bool(lsurf)),
-                                     float(s["epsi_four_pi"]), _p(r, C.c_double), _p(q, C.c_double), int(s["np"]),
-                                     _p(ipt, i32), _p(ian, i32), _p(napt, i32), len(napt), _p(force, C.c_double),
-                                     C.byref(urec), C.byref(vir), C.byref(ms))
+    if nmesh:
+        name, fn, a1, a2 = "msg_uewald_sites_spm", _lib.lib().msg_uewald_sites_spm, int(order), int(nmesh)
+    else:
+        name, fn, a1, a2 = "msg_uewald_sites", _lib.lib().msg_uewald_sites, int(ncut), 1 if region == "cube" else 0
+    rc = fn(na, box, float(ualpha), a1, a2, int(bool(lsurf)), float(s["epsi_four_pi"]), _p(r, C.c_double),
+            _p(q, C.c_double), int(s["np"]), _p(ipt, i32), _p(ian, i32), _p(napt, i32), len(napt),
+            _p(force, C.c_double), C.byref(urec), C.byref(vir), C.byref(ms))
     if rc:
-        raise MolsimGpuError(rc, "msg_uewald_sites")
+        raise MolsimGpuError(rc, name)
     return dict(force=force, urec=urec.value, virrec=vir.value, kernel_ms=ms.value)

@@ -1730,8 +1730,13 @@ static double rigid_forces(int32_t np, const double *ro, const double *r, const 
 typedef struct {
     const double *az;
     double ualpha, epsfp;
-    int32_t ncut, ncutregion, lsurf;
+    int32_t lewald, ncut, ncutregion, order, nmesh, lsurf;
 } site_ew;
+
+static int uewald_sites_impl(int32_t lewald, int32_t na, const double boxlen[3], double ualpha, int32_t ncut,
+                             int32_t ncutregion, int32_t order, int32_t nmesh, int32_t lsurf, double epsfp,
+                             const double *r, const double *az, int32_t np, const int32_t *iptpn,
+                             const int32_t *ianpn, const int32_t *napt, double *force, double *urec, double *virrec);
 
 static int velver_p_impl(const site_ew *ew, double *urec, int32_t nsteps, int32_t np, int32_t na, int32_t npt,
                          int32_t nat, const double boxlen[3], double rcut, double tstep, int32_t nvvite, double tvvite,
@@ -1764,8 +1769,8 @@ static int velver_p_impl(const site_ew *ew, double *urec, int32_t nsteps, int32_
         if (rc) break;
         if (ew) {                                  /* UTotal's UEwald over the sites (Src/energy.F90:335-352) */
             double *fe = malloc(sizeof(double) * 3 * (size_t)na), vr = 0.0;
-            or_uewald_sites(na, boxlen, ew->ualpha, ew->ncut, ew->ncutregion, ew->lsurf, ew->epsfp, r, ew->az, np,
-                            iptpn, ianpn, napt, fe, urec, &vr);
+            uewald_sites_impl(ew->lewald, na, boxlen, ew->ualpha, ew->ncut, ew->ncutregion, ew->order, ew->nmesh,
+                              ew->lsurf, ew->epsfp, r, ew->az, np, iptpn, ianpn, napt, fe, urec, &vr);
             for (m = 0; m < 3 * na; ++m) force[m] = force[m] + fe[m];
             vpair = vpair + vr;
             free(fe);
@@ -1810,8 +1815,8 @@ int or_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat
                          maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial);
 }
 
-/* The rigid-body step with the site Ewald sum in UTotal (lewald with polyatomic particles):
- * the Ewald site forces join the pair forces before the forces, torques and molecular virial;
+/* The rigid-body step with the site Ewald sum in UTotal (lewald with polyatomic particles;
+ * lewald 1: SPME with order, nmesh; 2: standard Ewald with ncut, ncutregion): the Ewald site forces join the pair forces before the forces, torques and molecular virial;
  * the reciprocal virial joins the virial; *urec = u%rec of the last step. */
 int or_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32_t nat, const double boxlen[3],
                       double rcut, double tstep, int32_t nvvite, double tvvite, double *ro, double *rod, double *rodd,
@@ -1819,15 +1824,19 @@ int or_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32
                       const int32_t *ianpn, const int32_t *napt, const int32_t *iatan, const double *ra,
                       int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
                       const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
-                      const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha, int32_t ncut,
-                      int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob, double *urec, double *virial)
+                      const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha,
+                      int32_t lewald, int32_t ncut, int32_t ncutregion, int32_t order, int32_t nmesh, int32_t lsurf,
+                      double epsfp, double *utwob, double *urec, double *virial)
 {
     site_ew ew;
     ew.az = az;
     ew.ualpha = ualpha;
     ew.epsfp = epsfp;
+    ew.lewald = lewald;
     ew.ncut = ncut;
     ew.ncutregion = ncutregion;
+    ew.order = order;
+    ew.nmesh = nmesh;
     ew.lsurf = lsurf;
     return velver_p_impl(&ew, urec, nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, rodd, qua,
                          quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist,
@@ -1841,10 +1850,10 @@ int or_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, int32
  * particles give the molecules (iptpn, ianpn, napt, 1-based).  force [na][3] is
  * overwritten with the Ewald forces (kJ/(mol A)); *urec = u%rec, *virrec its virial
  * (both scaled by EpsiFourPi as UEwald does). */
-int or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
-                    int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
-                    const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force, double *urec,
-                    double *virrec)
+static int uewald_sites_impl(int32_t lewald, int32_t na, const double boxlen[3], double ualpha, int32_t ncut,
+                             int32_t ncutregion, int32_t order, int32_t nmesh, int32_t lsurf, double epsfp,
+                             const double *r, const double *az, int32_t np, const int32_t *iptpn,
+                             const int32_t *ianpn, const int32_t *napt, double *force, double *urec, double *virrec)
 {
     static const int32_t one = 1;
     static const double dummy_buf[12] = {0.0};
@@ -1867,13 +1876,15 @@ int or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t n
     p.iubuflow = &one;
     p.r2umin = &r2u;
     p.r2atat = &r2u;
-    p.lewald = 2;
+    p.lewald = lewald;
     p.lsurf = lsurf;
     p.ualpha = ualpha;
     p.epsi_four_pi = epsfp;
     p.maxnneigh = 1;
     p.ncut = ncut;
     p.ncutregion = ncutregion;
+    p.order = order;
+    p.nmesh = nmesh;
     s = or_create(&p);
     or_set_state(s, r, NULL, NULL);
     for (ia = 0; ia < 3 * na; ++ia) s->force[ia] = 0.0;
@@ -1911,4 +1922,23 @@ int or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t n
     or_destroy(s);
     free(types);
     return 0;
+}
+
+int or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_t ncut, int32_t ncutregion,
+                    int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                    const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force, double *urec,
+                    double *virrec)
+{
+    return uewald_sites_impl(2, na, boxlen, ualpha, ncut, ncutregion, 0, 0, lsurf, epsfp, r, az, np, iptpn, ianpn,
+                             napt, force, urec, virrec);
+}
+
+/* The same with SPME over the sites (UEwaldRecSPM, Src/energy.F90:1207-1297: order, nmesh). */
+int or_uewald_sites_spm(int32_t na, const double boxlen[3], double ualpha, int32_t order, int32_t nmesh,
+                        int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                        const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force,
+                        double *urec, double *virrec)
+{
+    return uewald_sites_impl(1, na, boxlen, ualpha, 0, 0, order, nmesh, lsurf, epsfp, r, az, np, iptpn, ianpn, napt,
+                             force, urec, virrec);
 }

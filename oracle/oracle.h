@@ -185,8 +185,8 @@ int    or_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_t npt, in
                          int32_t maxsite, const double *masspt, const double *momp, const int32_t *nneighpn,
                          const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
                          const int32_t *iubuflow, const double *r2umin, const double *az, double ualpha,
-                         int32_t ncut, int32_t ncutregion, int32_t lsurf, double epsfp, double *utwob,
-                         double *urec, double *virial);
+                         int32_t lewald, int32_t ncut, int32_t ncutregion, int32_t order, int32_t nmesh,
+                         int32_t lsurf, double epsfp, double *utwob, double *urec, double *virial);
 
 /* UEwald over the sites of polyatomic particles: standard reciprocal sum, UEwaldSelf's
  * atomic and molecular (intramolecular erf) terms, surface term; force [na][3] overwritten. */
@@ -194,6 +194,11 @@ int    or_uewald_sites(int32_t na, const double boxlen[3], double ualpha, int32_
                        int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
                        const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force,
                        double *urec, double *virrec);
+/* The same with SPME over the sites (order, nmesh). */
+int    or_uewald_sites_spm(int32_t na, const double boxlen[3], double ualpha, int32_t order, int32_t nmesh,
+                           int32_t lsurf, double epsfp, const double *r, const double *az, int32_t np,
+                           const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, double *force,
+                           double *urec, double *virrec);
 
 #ifdef __cplusplus
 }

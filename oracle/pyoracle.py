@@ -365,8 +365,8 @@ def utwobody_p(s, table):
 
 def velver_p(s, table, nsteps, ewald=None):
     """nsteps of rigid-body VelVer (oracle) on a systems.rigid_bodies dict, advanced in place
-    (ro, rod, rodd, qua, quad, quadd, r).  ewald (optional): dict(az, ualpha, ncut, region,
-    lsurf) adds the site Ewald sum to every step.  Returns dict(utwob, virial[, urec]) of the
+    (ro, rod, rodd, qua, quad, quadd, r).  ewald (optional): dict(az, ualpha, lsurf and either
+    ncut, region (standard Ewald) or order, nmesh (SPME)) adds the site Ewald sum to every step.  Returns dict(utwob, virial[, urec]) of the
     last step."""
     L = lib()
     if not getattr(L, "_velver_p_typed", False):
@@ -376,8 +376,8 @@ def velver_p(s, table, nsteps, ewald=None):
         L.or_velver_p.restype = C.c_int
         L.or_velver_p.argtypes = common + [f64p, f64p]
         L.or_velver_p_ewald.restype = C.c_int
-        L.or_velver_p_ewald.argtypes = common + [f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
-                                                 f64p, f64p, f64p]
+        L.or_velver_p_ewald.argtypes = common + [f64p, C.c_double] + [C.c_int32] * 6 + [C.c_double, f64p, f64p,
+                                                                                         f64p]
         L._velver_p_typed = True
     k = {}
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r", "ra", "masspt", "momp"):
@@ -403,9 +403,12 @@ def velver_p(s, table, nsteps, ewald=None):
         rc = L.or_velver_p(*args, _p(utwob, C.c_double), C.byref(vir))
     else:
         az = np.ascontiguousarray(ewald["az"], np.float64)
-        rc = L.or_velver_p_ewald(*args, _p(az, C.c_double), float(ewald["ualpha"]), int(ewald["ncut"]),
-                                 1 if ewald.get("region", "sphere") == "cube" else 0, int(bool(ewald.get("lsurf"))),
-                                 float(s["epsi_four_pi"]), _p(utwob, C.c_double), C.byref(urec), C.byref(vir))
+        spm = "nmesh" in ewald
+        rc = L.or_velver_p_ewald(*args, _p(az, C.c_double), float(ewald["ualpha"]), 1 if spm else 2,
+                                 int(ewald.get("ncut", 0)), 1 if ewald.get("region", "sphere") == "cube" else 0,
+                                 int(ewald.get("order", 0)), int(ewald.get("nmesh", 0)),
+                                 int(bool(ewald.get("lsurf"))), float(s["epsi_four_pi"]), _p(utwob, C.c_double),
+                                 C.byref(urec), C.byref(vir))
     if rc:
         raise RuntimeError("VelVer (polyatomic) failed: %d" % rc)
     for key in ("ro", "rod", "rodd", "qua", "quad", "quadd", "r"):
@@ -416,13 +419,15 @@ def velver_p(s, table, nsteps, ewald=None):
     return out
 
 
-def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
-    """UEwald over the sites of a polyatomic system dict (oracle): dict(force, urec, virrec)."""
+def uewald_sites(s, az, ualpha, ncut=None, region="sphere", lsurf=False, order=None, nmesh=None):
+    """UEwald over the sites of a polyatomic system dict (oracle): dict(force, urec, virrec).
+    Standard Ewald with ncut (region 'sphere' or 'cube'), or SPME with order and nmesh."""
     L = lib()
     if not getattr(L, "_uewald_sites_typed", False):
-        L.or_uewald_sites.restype = C.c_int
-        L.or_uewald_sites.argtypes = [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
-                                      f64p, f64p, C.c_int32, i32p, i32p, i32p, f64p, f64p, f64p]
+        for fn in (L.or_uewald_sites, L.or_uewald_sites_spm):
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                           f64p, f64p, C.c_int32, i32p, i32p, i32p, f64p, f64p, f64p]
         L._uewald_sites_typed = True
     r = np.ascontiguousarray(s["r"], np.float64)
     q = np.ascontiguousarray(az, np.float64)
@@ -433,10 +438,11 @@ def uewald_sites(s, az, ualpha, ncut, region="sphere", lsurf=False):
     urec = C.c_double()
     vir = C.c_double()
     box = (C.c_double * 3)(*s["boxlen"])
-    rc = L.or_uewald_sites(int(s["na"]), box, float(ualpha), int(ncut), 1 if region == "cube" else 0, int(lsurf),
-                           float(s["epsi_four_pi"]), _p(r, C.c_double), _p(q, C.c_double), int(s["np"]),
-                           _p(ipt, C.c_int32), _p(ian, C.c_int32), _p(napt, C.c_int32), _p(force, C.c_double),
-                           C.byref(urec), C.byref(vir))
+    fn, a1, a2 = (L.or_uewald_sites_spm, int(order), int(nmesh)) if nmesh else \
+        (L.or_uewald_sites, int(ncut), 1 if region == "cube" else 0)
+    rc = fn(int(s["na"]), box, float(ualpha), a1, a2, int(lsurf), float(s["epsi_four_pi"]), _p(r, C.c_double),
+            _p(q, C.c_double), int(s["np"]), _p(ipt, C.c_int32), _p(ian, C.c_int32), _p(napt, C.c_int32),
+            _p(force, C.c_double), C.byref(urec), C.byref(vir))
     if rc:
         raise RuntimeError("UEwald over sites failed: %d" % rc)
     return dict(force=force, urec=urec.value, virrec=vir.value)

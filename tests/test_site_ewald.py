@@ -256,3 +256,86 @@ def test_gpu_rigid_body_ewald_steps_match_oracle(lsurf):
     assert abs(ug["urec"] - uo["urec"]) <= 1e-10 * _self_scale(s, ew["az"], 0.35)
     assert np.abs(ug["utwob"] - uo["utwob"]).max() <= 1e-8 * np.abs(uo["utwob"]).max()
     assert abs(ug["virial"] - uo["virial"]) <= 1e-8 * abs(uo["virial"])
+
+
+# ------------------------------------------------------------------ SPME over the sites
+
+@pytest.mark.parametrize("lsurf", [False, True])
+def test_spm_monoatomic_limit_equals_utotal_spme(lsurf):
+    """SPME over sites, one site per particle: u%rec and forces of the monoatomic UTotal with SPME."""
+    s = Hp.electrolyte_small(lsurf=lsurf)
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    ref = o.utotal()
+    p = _monoatomic_as_polyatomic(s, o)
+    pair = O.utwobody_p(p, t)
+    e = O.uewald_sites(p, s["az"], t["ualpha"], order=s["order"], nmesh=s["nmesh"], lsurf=lsurf)
+    assert e["urec"] == pytest.approx(ref["urec"], rel=1e-14, abs=1e-12)
+    assert Hp.rel_rms(pair["force"] + e["force"], ref["force"]) < 1e-13
+
+
+def test_spm_converges_to_the_standard_sum():
+    """On rigid molecules, SPME over the sites approaches the standard Ewald sum as the mesh
+    refines: order 8 on a 64^3 mesh agrees within 1e-6 of the self-energy scale in u%rec and
+    1e-6 of the largest force."""
+    s = _molecules()
+    az = _site_charges(s)
+    std = O.uewald_sites(s, az, 0.35, 16)
+    spm = O.uewald_sites(s, az, 0.35, order=8, nmesh=64)
+    assert abs(spm["urec"] - std["urec"]) < 1e-6 * _self_scale(s, az, 0.35)
+    assert np.abs(spm["force"] - std["force"]).max() < 1e-6 * np.abs(std["force"]).max()
+
+
+def test_spm_bad_arguments_are_refused_on_the_host():
+    from molsim_b200.engine import MolsimGpuError
+    from molsim_b200.polyatomic import uewald_sites
+
+    s = _molecules()
+    az = _site_charges(s)
+    for order, nmesh in ((3, 32), (9, 32), (5, 33), (5, 6)):
+        with pytest.raises(MolsimGpuError) as ei:
+            uewald_sites(s, az, 0.35, order=order, nmesh=nmesh)
+        assert ei.value.code == 6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order,nmesh,lsurf", [(5, 32, False), (6, 40, True), (8, 64, False)])
+def test_gpu_spm_matches_oracle(order, nmesh, lsurf):
+    from molsim_b200.polyatomic import uewald_sites
+
+    s = _molecules()
+    az = _site_charges(s)
+    ref = O.uewald_sites(s, az, 0.35, order=order, nmesh=nmesh, lsurf=lsurf)
+    got = uewald_sites(s, az, 0.35, order=order, nmesh=nmesh, lsurf=lsurf)
+    # the mesh sums of u%rec and its virial (weights of both signs over the spectrum, a cuFFT
+    # transform against the oracle's) are held to the self-energy scale
+    assert abs(got["urec"] - ref["urec"]) <= 1e-10 * _self_scale(s, az, 0.35)
+    assert abs(got["virrec"] - ref["virrec"]) <= 1e-10 * _self_scale(s, az, 0.35)
+    assert Hp.rel_rms(got["force"], ref["force"]) < 1e-10
+    again = uewald_sites(s, az, 0.35, order=order, nmesh=nmesh, lsurf=lsurf)
+    assert again["urec"] == got["urec"] and np.array_equal(again["force"], got["force"])
+
+
+@pytest.mark.gpu
+def test_gpu_rigid_body_spm_steps_match_oracle():
+    """Ten rigid-body steps with SPME over the sites (order 5, 32^3) on the GPU against the oracle."""
+    import copy
+
+    from molsim_b200.polyatomic import velver_p
+
+    s = _rigid_charged()
+    t = _screened_site_table(s, 0.35, 1e-7)
+    ew = dict(az=_site_charges(s), ualpha=0.35, order=5, nmesh=32, lsurf=True)
+    so, sg = copy.deepcopy(s), copy.deepcopy(s)
+    uo = O.velver_p(so, t, 10, ewald=ew)
+    ug = velver_p(sg, t, 10, ewald=ew)
+    box = s["boxlen"][0]
+    d = np.asarray(sg["ro"]) - np.asarray(so["ro"])
+    d -= box * np.round(d / box)
+    assert np.abs(d).max() < 1e-8
+    for key in ("rod", "qua", "quad"):
+        assert np.abs(np.asarray(sg[key]) - np.asarray(so[key])).max() <= 1e-8 * max(1.0, np.abs(so[key]).max()), key
+    assert abs(ug["urec"] - uo["urec"]) <= 1e-10 * _self_scale(s, ew["az"], 0.35)
+    assert abs(ug["virial"] - uo["virial"]) <= 1e-8 * abs(uo["virial"])
