@@ -100,6 +100,9 @@ typedef struct msg_params {
     int32_t maxnneigh;       /* row capacity hint for the neighbour list (0: automatic) */
     int32_t ncut;            /* lewald 2: k = 2 pi n / L with 0 <= n_i <= ncut (1..100)  */
     int32_t ncutregion;      /* lewald 2: 0 'sphere' (|n|^2 <= ncut^2), 1 'cube'         */
+    int32_t lewald2dlc;      /* 1: 2D layer correction (UEwaldRecStd2dlc, lewald 2) and    */
+                             /*    UEwaldSurf's 2d-periodic form (Src/energy.F90:1106-1203, */
+                             /*    1362-1369); Monte Carlo refuses it                       */
 } msg_params;
 
 typedef struct msg_handle msg_handle;

@@ -30,7 +30,7 @@ class MsgParams(C.Structure):
                 ("ualpha", C.c_double), ("epsi_four_pi", C.c_double), ("nbond", C.c_int32),
                 ("bond_ij", i32p), ("bond_k", f64p), ("bond_eq", f64p), ("bond_p", i32p),
                 ("tstep", C.c_double), ("bd_fac1", f64p), ("bd_fac2", f64p), ("maxnneigh", C.c_int32),
-                ("ncut", C.c_int32), ("ncutregion", C.c_int32)]
+                ("ncut", C.c_int32), ("ncutregion", C.c_int32), ("lewald2dlc", C.c_int32)]
 
 
 class MsgEnergy(C.Structure):

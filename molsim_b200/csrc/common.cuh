@@ -72,6 +72,10 @@ struct SysDev {
     int ew_nchunk, ew_clen;     // particle chunks of the structure-factor sum and their length
     long long ew_fks_off;       // first double4 of the per-slice reciprocal forces
     int ew_nks, ew_klen;        // k-vector slices of the force sum and their length
+    // 2D layer correction (lewald2dlc): its forces are one more slice after the ew_nks
+    int elc;                    // 1: layer correction (with recstd) and the 2D surface term
+    int elc_nkv, elc_kv_off;    // 2D k-vectors (nx, ny) of this system and their first entry
+    int elc_pad;
 };
 
 // One type pair's slice of the concatenated table.

@@ -213,6 +213,10 @@ struct msg_handle {
     double2 *ew_eik = nullptr, *ew_part = nullptr, *ew_sk = nullptr;
     double4 *ew_fks = nullptr;
     int ew_nk = 0, ew_ntile = 0, ew_nf = 0;
+    // 2D layer correction: 2D k-vectors {nx, ny, system}, kfac2d, the eight sums per k-vector
+    int4 *elc_kv = nullptr;
+    double *elc_kfac = nullptr, *elc_st = nullptr;
+    int elc_nk = 0;
     // Monte Carlo: Random's state, running energies, counts (accepted, hard-core rejects),
     // sweep parameters, displacement per type, trial structure factors
     int2 *mc_rng = nullptr;
@@ -409,7 +413,8 @@ static void free_all(msg_handle *h)
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
                     h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
-                    h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm};
+                    h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
+                    h->elc_kv, h->elc_kfac, h->elc_st};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -518,6 +523,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         S.lewald = p.lewald ? 1 : 0;
         S.recstd = p.lewald == 2 ? 1 : 0;
         S.lsurf = (p.lewald && p.lsurf) ? 1 : 0;
+        S.elc = (p.lewald && p.lewald2dlc) ? 1 : 0;
         for (int d = 0; d < 3; ++d) {
             S.box[d] = p.boxlen[d];
             S.half[d] = p.boxlen[d] / 2.0;
@@ -656,7 +662,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 
     // --- standard Ewald: k-vectors in the reference's order with kfac, work lists ---
     if (any_std) {
-        std::vector<int4> kv, ki, fi;
+        std::vector<int4> kv, ki, fi, ekv;
+        std::vector<double> ekf;
         int ntile = 0;
         std::vector<double> kf;
         long long eik_acc = 0, part_acc = 0, fks_acc = 0;
@@ -707,7 +714,25 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             S.ew_klen = (S.ew_nkv + nks - 1) / nks;
             S.ew_nks = (S.ew_nkv + S.ew_klen - 1) / S.ew_klen;
             S.ew_fks_off = fks_acc;
-            fks_acc += (long long)S.ew_nks * S.n;
+            fks_acc += (long long)(S.ew_nks + S.elc) * S.n;     // the layer correction's slice last
+            if (S.elc) {
+                // EwaldSetup lewald2dlc (Src/energy.F90:6785-6851): ncut2d = ncut, ncut2d2 = ncut2d^2
+                // ('sphere') or 2 ncut2d^2 ('cube'); ny outer; kfac2d = -2pi/(Lx Ly) fac /
+                // (kp (exp(kp Lz) - 1)) with fac = 4 when nx and ny are both nonzero
+                const int c2 = P[s].ncutregion ? 2 * nc * nc : nc * nc;
+                const double f0 = tp / (S.box[0] * S.box[1]);
+                S.elc_kv_off = (int)ekv.size();
+                for (int ny = 0; ny <= nc; ++ny)
+                    for (int nx = 0; nx <= nc; ++nx) {
+                        if (nx * nx + ny * ny > c2 || (nx == 0 && ny == 0)) continue;
+                        const double fac = (nx != 0 && ny != 0) ? 4.0 : 1.0;
+                        const double kp = std::sqrt((nx * (tp * S.boxi[0])) * (nx * (tp * S.boxi[0])) +
+                                                    (ny * (tp * S.boxi[1])) * (ny * (tp * S.boxi[1])));
+                        ekf.push_back(-f0 * fac / (kp * (std::exp(kp * S.box[2]) - 1.0)));
+                        ekv.push_back(make_int4(nx, ny, s, 0));
+                    }
+                S.elc_nkv = (int)ekv.size() - S.elc_kv_off;
+            }
             for (int pt = 0; pt < ptiles; ++pt)
                 for (int k = 0; k < S.ew_nks; ++k)
                     fi.push_back(make_int4(s, S.off + pt * EWF_THREADS, S.off + std::min(S.n, (pt + 1) * EWF_THREADS), k));
@@ -725,6 +750,14 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         ew_part = dalloc<double2>(part_acc * 4);
         ew_sk = dalloc<double2>(kv.size() * 4);
         ew_fks = dalloc<double4>(fks_acc);
+        elc_nk = (int)ekv.size();
+        if (elc_nk) {
+            elc_kv = dalloc<int4>(ekv.size());
+            elc_kfac = dalloc<double>(ekf.size());
+            elc_st = dalloc<double>(8 * ekv.size());
+            up(elc_kv, ekv.data(), ekv.size() * sizeof(int4));
+            up(elc_kfac, ekf.data(), ekf.size() * sizeof(double));
+        }
         up(ew_kv, kv.data(), kv.size() * sizeof(int4));
         up(ew_kfac, kf.data(), kf.size() * sizeof(double));
         up(ew_kitems, ki.data(), ki.size() * sizeof(int4));
@@ -1259,6 +1292,12 @@ static void launch_ewald_std(msg_handle *h)
     k_ew_force<<<h->ew_nf, EWF_THREADS, 0, h->st>>>(h->dsys, h->ew_fitems, h->pos[0], h->ew_kv, h->ew_kfac, h->ew_sk,
                                                     h->ew_fks);
     h->launches += 3;
+    if (h->elc_nk) {
+        k_elc_sum<<<h->elc_nk, ELC_THREADS, 0, h->st>>>(h->dsys, h->elc_kv, h->elc_kfac, h->pos[0], h->elc_st, h->eacc);
+        k_elc_force<<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->elc_kv, h->elc_kfac, h->elc_st,
+                                                 h->ew_fks);
+        h->launches += 2;
+    }
     h->tend(TM_EWSTD);
 }
 
@@ -2028,6 +2067,10 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
         if (S.lewald && !S.recstd) {
             h->err = "Monte Carlo moves need the standard Ewald sum (lewald 2) or none: the SPME energy "
                      "difference of a trial move transforms the whole mesh";
+            return MSG_ERR_ARG;
+        }
+        if (S.elc) {
+            h->err = "Monte Carlo moves do not take the 2D layer correction (lewald2dlc)";
             return MSG_ERR_ARG;
         }
         if (!p[s].dtran || (p[s].isamp != 0 && p[s].isamp != 1)) {

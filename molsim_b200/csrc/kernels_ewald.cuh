@@ -250,4 +250,141 @@ __global__ void __launch_bounds__(EWF_THREADS) k_ew_force(const SysDev *__restri
     if (on) fks[S.ew_fks_off + (size_t)W.w * S.n + (i - S.off)] = make_double4(fx, fy, fz, 0.0);
 }
 
+// ---------------------------------------------------------------------------
+// 2D layer correction (UEwaldRecStd2dlc with EwaldSetArray2d, Src/energy.F90:1106-1203,
+// 1435-1463).  2D k-vectors kv2 = {nx, ny, system, 0} in the reference's order (ny outer)
+// with kfac2d.  The trigonometric tables follow the reference: sin and cos of n = 1 from
+// the coordinate, higher n by the angle-sum recurrence, and sin(0) = cos(0) = 1.
+// ---------------------------------------------------------------------------
+constexpr int ELC_THREADS = 128;
+
+// sin, cos of n 2pi x / L by the recurrence from e1 = (cos, sin) of n = 1; n = 0 gives (1, 1).
+__device__ __forceinline__ void elc_trig(int n, double2 e1, double &sn, double &cs)
+{
+    if (n == 0) {
+        sn = 1.0;
+        cs = 1.0;
+        return;
+    }
+    double2 e = e1;
+    for (int k = 2; k <= n; ++k) e = cmul(e, e1);
+    sn = e.y;
+    cs = e.x;
+}
+
+// One 2D k-vector per block: the eight sums over the system's particles (fixed partition
+// over the threads, then a fixed-order reduction), stored in st2[k][8]; the energy term
+// kfac2d (-S1^2 - S2^2 - S3^2 - S4^2 + S5^2 + S6^2 + S7^2 + S8^2) is added to u%rec.
+__global__ void __launch_bounds__(ELC_THREADS) k_elc_sum(const SysDev *__restrict__ sysv, const int4 *__restrict__ kv2,
+                                                         const double *__restrict__ kfac2,
+                                                         const double4 *__restrict__ pos, double *__restrict__ st2,
+                                                         long long *__restrict__ eacc)
+{
+    __shared__ double red[8][ELC_THREADS / 32];
+    const int4 K = kv2[blockIdx.x];
+    const SysDev &S = sysv[K.z];
+    const double tp = 2.0 * 3.1415926535897932;
+    const double tpx = tp * S.boxi[0], tpy = tp * S.boxi[1];
+    const double kx = K.x * tpx, ky = K.y * tpy, kp = sqrt(kx * kx + ky * ky);
+    double a[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = 0.0;
+    for (int i = S.off + threadIdx.x; i < S.off + S.n; i += ELC_THREADS) {
+        const double4 x = pos[i];
+        double s1, c1, sx, cx, sy, cy;
+        sincos(tpx * x.x, &s1, &c1);
+        elc_trig(K.x, make_double2(c1, s1), sx, cx);
+        sincos(tpy * x.y, &s1, &c1);
+        elc_trig(K.y, make_double2(c1, s1), sy, cy);
+        const double e = exp(kp * x.z), ei = 1.0 / e;
+        const double sh = 0.5 * (e - ei), ch = 0.5 * (e + ei), q = x.w;
+        a[0] = a[0] + q * sx * sy * sh;
+        a[1] = a[1] + q * cx * sy * sh;
+        a[2] = a[2] + q * sx * cy * sh;
+        a[3] = a[3] + q * cx * cy * sh;
+        a[4] = a[4] + q * sx * sy * ch;
+        a[5] = a[5] + q * cx * sy * ch;
+        a[6] = a[6] + q * sx * cy * ch;
+        a[7] = a[7] + q * cx * cy * ch;
+    }
+    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const double v = warp_sum(a[c]);
+        if (lane == 0) red[c][wi] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double t = 0.0;
+        for (int k = 0; k < ELC_THREADS / 32; ++k) t += red[threadIdx.x][k];
+        st2[(size_t)blockIdx.x * 8 + threadIdx.x] = t;
+        red[threadIdx.x][0] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double *q = &red[0][0];
+        const int ld = ELC_THREADS / 32;
+        const double term = kfac2[blockIdx.x] * (-q[0] * q[0] - q[ld] * q[ld] - q[2 * ld] * q[2 * ld] -
+                                                 q[3 * ld] * q[3 * ld] + q[4 * ld] * q[4 * ld] +
+                                                 q[5 * ld] * q[5 * ld] + q[6 * ld] * q[6 * ld] +
+                                                 q[7 * ld] * q[7 * ld]);
+        acc_add(eacc + (size_t)K.z * EA_N + EA_UREC, term);
+    }
+}
+
+// The layer correction's force on every particle of a system with elc, over the system's 2D
+// k-vectors in order, as the reference forms it per k (Src/energy.F90:1170-1197); written
+// as the force slice after the standard sum's slices.
+__global__ void __launch_bounds__(128) k_elc_force(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                   const double4 *__restrict__ pos, const int4 *__restrict__ kv2,
+                                                   const double *__restrict__ kfac2, const double *__restrict__ st2,
+                                                   double4 *__restrict__ fks)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    if (!S.elc || !S.recstd) return;
+    const int i = T.i0 + threadIdx.x;
+    if (i >= T.i1) return;
+    const double4 x = pos[i];
+    const double tp = 2.0 * 3.1415926535897932;
+    const double tpx = tp * S.boxi[0], tpy = tp * S.boxi[1];
+    double s1, c1;
+    sincos(tpx * x.x, &s1, &c1);
+    const double2 e1x = make_double2(c1, s1);
+    sincos(tpy * x.y, &s1, &c1);
+    const double2 e1y = make_double2(c1, s1);
+    const double q = x.w;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    // running exponentials along the reference's (ny outer, nx inner) order
+    double2 ex = make_double2(1.0, 0.0), ey = ex;
+    int cxn = 0, cyn = 0;
+    for (int k = S.elc_kv_off; k < S.elc_kv_off + S.elc_nkv; ++k) {
+        const int4 K = kv2[k];
+        if (K.y != cyn) {
+            while (cyn < K.y) { ey = (cyn == 0) ? e1y : cmul(ey, e1y); ++cyn; }
+            ex = make_double2(1.0, 0.0);
+            cxn = 0;
+        }
+        while (cxn < K.x) { ex = (cxn == 0) ? e1x : cmul(ex, e1x); ++cxn; }
+        const double sx = K.x ? ex.y : 1.0, cx = K.x ? ex.x : 1.0;
+        const double sy = K.y ? ey.y : 1.0, cy = K.y ? ey.x : 1.0;
+        const double kx = K.x * tpx, ky = K.y * tpy, kp = sqrt(kx * kx + ky * ky);
+        const double e = exp(kp * x.z), ei = 1.0 / e;
+        const double sh = 0.5 * (e - ei), ch = 0.5 * (e + ei);
+        const double *t = st2 + (size_t)k * 8;
+        const double kf2 = S.epsfp * 2.0 * kfac2[k];
+        const double kxx = kf2 * kx, kyy = kf2 * ky, kpp = kf2 * kp;
+        fx = fx - kxx * q * (-(cx) * (sy) * sh * t[0] - (-sx) * (sy) * sh * t[1] - (cx) * (cy) * sh * t[2] -
+                             (-sx) * (cy) * sh * t[3] + (cx) * (sy) * ch * t[4] + (-sx) * (sy) * ch * t[5] +
+                             (cx) * (cy) * ch * t[6] + (-sx) * (cy) * ch * t[7]);
+        fy = fy - kyy * q * (-(sx) * (cy) * sh * t[0] - (cx) * (cy) * sh * t[1] - (sx) * (-sy) * sh * t[2] -
+                             (cx) * (-sy) * sh * t[3] + (sx) * (cy) * ch * t[4] + (cx) * (cy) * ch * t[5] +
+                             (sx) * (-sy) * ch * t[6] + (cx) * (-sy) * ch * t[7]);
+        fz = fz - kpp * q * (-(sx) * (sy) * ch * t[0] - (cx) * (sy) * ch * t[1] - (sx) * (cy) * ch * t[2] -
+                             (cx) * (cy) * ch * t[3] + (sx) * (sy) * sh * t[4] + (cx) * (sy) * sh * t[5] +
+                             (sx) * (cy) * sh * t[6] + (cx) * (cy) * sh * t[7]);
+    }
+    fks[S.ew_fks_off + (size_t)S.ew_nks * S.n + (i - S.off)] = make_double4(fx, fy, fz, 0.0);
+}
+
 }  // namespace msg

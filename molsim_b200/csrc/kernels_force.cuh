@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
         if (S.lewald) {
             if (S.recstd) {
                 // standard Ewald: the k-vector slices of k_ew_force, in slice order
-                for (int k = 0; k < S.ew_nks; ++k) {
+                for (int k = 0; k < S.ew_nks + S.elc; ++k) {
                     const double4 f = fks[S.ew_fks_off + (size_t)k * S.n + (i - S.off)];
                     Fx += f.x;
                     Fy += f.y;
@@ -340,7 +340,11 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 Fy -= x.w * (double)e1 * S.dkdr[1] * S.epsfp;
                 Fz -= x.w * (double)e2 * S.dkdr[2] * S.epsfp;
             }
-            if (S.lsurf) {
+            if (S.lsurf && S.elc) {
+                // 2d-periodic form (Src/energy.F90:1362-1369): the z dipole only
+                const double fac = 2.0 * 3.1415926535897932 / S.vol;
+                Fz -= S.epsfp * (2.0 * fac) * x.w * sq[2];
+            } else if (S.lsurf) {
                 const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
                 Fx -= S.epsfp * (2.0 * fac) * x.w * sq[0];
                 Fy -= S.epsfp * (2.0 * fac) * x.w * sq[1];
@@ -401,9 +405,10 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
             urec = a[EA_UREC] + S.uself;
             virrec = a[EA_VIRREC];
             if (S.lsurf) {
-                const double fac = 2.0 * 3.1415926535897932 / (3.0 * S.vol);
-                const double term =
-                    fac * (a[EA_DIP] * a[EA_DIP] + a[EA_DIP + 1] * a[EA_DIP + 1] + a[EA_DIP + 2] * a[EA_DIP + 2]);
+                const double fac = S.elc ? 2.0 * 3.1415926535897932 / S.vol : 2.0 * 3.1415926535897932 / (3.0 * S.vol);
+                const double term = S.elc ? fac * (a[EA_DIP + 2] * a[EA_DIP + 2])
+                                          : fac * (a[EA_DIP] * a[EA_DIP] + a[EA_DIP + 1] * a[EA_DIP + 1] +
+                                                   a[EA_DIP + 2] * a[EA_DIP + 2]);
                 urec += term;
                 virrec -= term;
             }

@@ -187,7 +187,8 @@ class Engine:
                          s["tstep"], _p(k["fac1"], C.c_double) if "fac1" in k else null,
                          _p(k["fac2"], C.c_double) if "fac2" in k else null, int(maxnneigh),
                          int(t.get("ncut", s.get("ncut", 0)) or 0),
-                         1 if s.get("ncutregion", "sphere") == "cube" else 0)
+                         1 if s.get("ncutregion", "sphere") == "cube" else 0,
+                         int(bool(s.get("lewald2dlc", False))))
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -37,6 +37,7 @@ module MolsimGpu
       type(c_ptr)        :: bd_fac1, bd_fac2
       integer(c_int32_t) :: maxnneigh
       integer(c_int32_t) :: ncut, ncutregion
+      integer(c_int32_t) :: lewald2dlc
    end type msg_params
 
    ! struct msg_energy

@@ -523,6 +523,10 @@ struct or_sys {
     double *eik[3];          /* [np][ncut+1] complex (re, im) */
     double *eyz, *eikr;      /* [np] 2 complex; [np] 4 complex */
     double *sumeikr;         /* [nkvec][4] complex: structure factors of the last UTotal / MC update */
+    /* 2D layer correction (lewald2dlc): 2D k-vectors (nx, ny) with kfac2d, sin/cos tables */
+    int elc, ncut2d2, nkvec2d;
+    double *kfac2d;
+    double *trig2d;          /* [np][4][ncut+1]: sin kx, cos kx, sin ky, cos ky */
     /* Random's SAVEd state (Src/mollib.F90:2683-2687) */
     int32_t rix, riy;
     int nbond; int32_t *bond_ij; double *bond_k, *bond_eq; int32_t *bond_p;
@@ -568,6 +572,30 @@ static void ewald_setup_std(or_sys *s, int ncut, int cube)
     for (m = 0; m < 3; ++m) s->eik[m] = malloc(sizeof(double) * 2 * (size_t)s->np * (ncut + 1));
     s->eyz = malloc(sizeof(double) * 4 * (size_t)s->np);
     s->eikr = malloc(sizeof(double) * 8 * (size_t)s->np);
+}
+
+/* EwaldSetup, lewald2dlc (Src/energy.F90:6785-6851): ncut2d = ncut; ncut2d2 = ncut2d^2
+ * ('sphere') or 2 ncut2d^2 ('cube'); for each (nx, ny) != 0 with nx^2 + ny^2 <= ncut2d2, ny
+ * outer, kfac2d = -2pi/(Lx Ly) fac / (kp (exp(kp Lz) - 1)), fac = 4 when both are nonzero. */
+static void ewald_setup_2dlc(or_sys *s, int cube)
+{
+    const int nc = s->ncut;
+    const double fac0 = 2.0 * Pi / (s->boxlen[0] * s->boxlen[1]);
+    int nx, ny, n = 0;
+    s->ncut2d2 = cube ? 2 * nc * nc : nc * nc;
+    s->kfac2d = malloc(sizeof(double) * ((size_t)nc + 1) * (nc + 1));
+    for (ny = 0; ny <= nc; ++ny)
+        for (nx = 0; nx <= nc; ++nx) {
+            double fac = 1.0, kp;
+            if (nx * nx + ny * ny > s->ncut2d2) continue;
+            if (nx == 0 && ny == 0) continue;
+            if (nx != 0 && ny != 0) fac = 4.0 * fac;
+            kp = sqrt((nx * (2.0 * Pi * s->boxleni[0])) * (nx * (2.0 * Pi * s->boxleni[0])) +
+                      (ny * (2.0 * Pi * s->boxleni[1])) * (ny * (2.0 * Pi * s->boxleni[1])));
+            s->kfac2d[n++] = -fac0 * fac / (kp * (exp(kp * s->boxlen[2]) - 1.0));
+        }
+    s->nkvec2d = n;
+    s->trig2d = malloc(sizeof(double) * 4 * (size_t)s->np * ((size_t)nc + 1));
 }
 
 or_sys *or_create(const or_params *p)
@@ -619,8 +647,10 @@ or_sys *or_create(const or_params *p)
     s->lsurf = p->lsurf;
     s->ualpha = p->ualpha;
     s->epsfp = p->epsi_four_pi;
+    s->elc = p->lewald2dlc ? 1 : 0;
     if (s->lewald == 2) {
         ewald_setup_std(s, p->ncut, p->ncutregion);
+        if (s->elc) ewald_setup_2dlc(s, p->ncutregion);
     } else if (s->lewald) {
         size_t n = (size_t)s->s * s->s * s->s;
         h = s->s / 2 + 1;
@@ -650,6 +680,7 @@ void or_destroy(or_sys *s)
     free(s->ubuf); free(s->iubuflow); free(s->r2umin); free(s->r2atat);
     free(s->nneighpn); free(s->jpnlist);
     free(s->meshfac); free(s->energyfac); free(s->virfac); free(s->qmesh); free(s->fqmesh);
+    free(s->kfac2d); free(s->trig2d);
     free(s->kfac); free(s->eik[0]); free(s->eik[1]); free(s->eik[2]); free(s->eyz); free(s->eikr);
     free(s->sumeikr);
     free(s->bond_ij); free(s->bond_k); free(s->bond_eq); free(s->bond_p);
@@ -1050,18 +1081,110 @@ static void uewald_rec_std(or_sys *s, double *urec, double *virrec)
     *virrec = virloc;
 }
 
+/* UEwaldRecStd2dlc with EwaldSetArray2d, Src/energy.F90:1106-1203, 1435-1463: the layer
+ * correction of Arnold et al. over the 2D k-vectors.  The tables keep the reference's
+ * sin(0) = cos(0) = 1 at n = 0.  Adds to *urec (before the EpsiFourPi scale) and the
+ * forces (scaled); the virial is untouched, as in the reference. */
+static void uewald_rec_std2dlc(or_sys *s, double *urec)
+{
+    const int np = s->np, nc = s->ncut;
+    const size_t w = (size_t)nc + 1;
+    double tpbi[2], uloc = *urec;
+    int ia, nx, ny, icut, kn = 0, c;
+    tpbi[0] = 2.0 * Pi * s->boxleni[0];
+    tpbi[1] = 2.0 * Pi * s->boxleni[1];
+    for (ia = 0; ia < np; ++ia) {
+        double *t = s->trig2d + (size_t)ia * 4 * w;       /* sx, cx, sy, cy rows */
+        t[0] = 1.0; t[w] = 1.0; t[2 * w] = 1.0; t[3 * w] = 1.0;
+        if (nc >= 1) {
+            t[1] = sin(tpbi[0] * s->ro[3 * ia]);
+            t[w + 1] = cos(tpbi[0] * s->ro[3 * ia]);
+            t[2 * w + 1] = sin(tpbi[1] * s->ro[3 * ia + 1]);
+            t[3 * w + 1] = cos(tpbi[1] * s->ro[3 * ia + 1]);
+        }
+        for (icut = 2; icut <= nc; ++icut) {
+            t[icut] = t[icut - 1] * t[w + 1] + t[w + icut - 1] * t[1];
+            t[w + icut] = t[w + icut - 1] * t[w + 1] - t[icut - 1] * t[1];
+            t[2 * w + icut] = t[2 * w + icut - 1] * t[3 * w + 1] + t[3 * w + icut - 1] * t[2 * w + 1];
+            t[3 * w + icut] = t[3 * w + icut - 1] * t[3 * w + 1] - t[2 * w + icut - 1] * t[2 * w + 1];
+        }
+    }
+    for (ny = 0; ny <= nc; ++ny) {
+        const double ky = ny * tpbi[1];
+        for (nx = 0; nx <= nc; ++nx) {
+            const double kx = nx * tpbi[0];
+            double kp, st[8], term, kfac2, kxx, kyy, kpp;
+            if (nx * nx + ny * ny > s->ncut2d2) continue;
+            if (nx == 0 && ny == 0) continue;
+            kp = sqrt(kx * kx + ky * ky);
+            for (c = 0; c < 8; ++c) st[c] = 0.0;
+            for (ia = 0; ia < np; ++ia) {
+                const double *t = s->trig2d + (size_t)ia * 4 * w;
+                const double sx = t[nx], cx = t[w + nx], sy = t[2 * w + ny], cy = t[3 * w + ny];
+                const double e = exp(kp * s->ro[3 * ia + 2]), ei = 1.0 / e;
+                const double sh = 0.5 * (e - ei), ch = 0.5 * (e + ei), q = s->az[ia];
+                st[0] = st[0] + q * sx * sy * sh;
+                st[1] = st[1] + q * cx * sy * sh;
+                st[2] = st[2] + q * sx * cy * sh;
+                st[3] = st[3] + q * cx * cy * sh;
+                st[4] = st[4] + q * sx * sy * ch;
+                st[5] = st[5] + q * cx * sy * ch;
+                st[6] = st[6] + q * sx * cy * ch;
+                st[7] = st[7] + q * cx * cy * ch;
+            }
+            term = s->kfac2d[kn] * (-st[0] * st[0] - st[1] * st[1] - st[2] * st[2] - st[3] * st[3] +
+                                    st[4] * st[4] + st[5] * st[5] + st[6] * st[6] + st[7] * st[7]);
+            uloc = uloc + term;
+            kfac2 = s->epsfp * 2.0 * s->kfac2d[kn];
+            kxx = kfac2 * kx;
+            kyy = kfac2 * ky;
+            kpp = kfac2 * kp;
+            for (ia = 0; ia < np; ++ia) {
+                const double *t = s->trig2d + (size_t)ia * 4 * w;
+                const double sx = t[nx], cx = t[w + nx], sy = t[2 * w + ny], cy = t[3 * w + ny];
+                const double e = exp(kp * s->ro[3 * ia + 2]), ei = 1.0 / e;
+                const double sh = 0.5 * (e - ei), ch = 0.5 * (e + ei), q = s->az[ia];
+                s->force[3 * ia] = s->force[3 * ia] -
+                    kxx * q * (-(cx) * (sy) * sh * st[0] - (-sx) * (sy) * sh * st[1] - (cx) * (cy) * sh * st[2] -
+                               (-sx) * (cy) * sh * st[3] + (cx) * (sy) * ch * st[4] + (-sx) * (sy) * ch * st[5] +
+                               (cx) * (cy) * ch * st[6] + (-sx) * (cy) * ch * st[7]);
+                s->force[3 * ia + 1] = s->force[3 * ia + 1] -
+                    kyy * q * (-(sx) * (cy) * sh * st[0] - (cx) * (cy) * sh * st[1] - (sx) * (-sy) * sh * st[2] -
+                               (cx) * (-sy) * sh * st[3] + (sx) * (cy) * ch * st[4] + (cx) * (cy) * ch * st[5] +
+                               (sx) * (-sy) * ch * st[6] + (cx) * (-sy) * ch * st[7]);
+                s->force[3 * ia + 2] = s->force[3 * ia + 2] -
+                    kpp * q * (-(sx) * (sy) * ch * st[0] - (cx) * (sy) * ch * st[1] - (sx) * (cy) * ch * st[2] -
+                               (cx) * (cy) * ch * st[3] + (sx) * (sy) * sh * st[4] + (cx) * (sy) * sh * st[5] +
+                               (sx) * (cy) * sh * st[6] + (cx) * (cy) * sh * st[7]);
+            }
+            ++kn;
+        }
+    }
+    *urec = uloc;
+}
+
 /* UEwald + UEwaldSelf + UEwaldSurf, Src/energy.F90:905-958, 1301-1371 (monoatomic) */
 static void uewald(or_sys *s, double *urec_out, double *utot, double *virial)
 {
     double urec = 0.0, virrec = 0.0, q2 = 0.0;
     int ia;
-    if (s->lewald == 2)
+    if (s->lewald == 2) {
         uewald_rec_std(s, &urec, &virrec);
-    else
+        if (s->elc) uewald_rec_std2dlc(s, &urec);
+    } else {
         uewald_rec_spm(s, &urec, &virrec);
+    }
     for (ia = 0; ia < s->np; ++ia) q2 += s->az[ia] * s->az[ia];
     urec = urec - s->ualpha / sqrt(Pi) * q2;
-    if (s->lsurf) {
+    if (s->lsurf && s->elc) {                  /* 2d-periodic system (Src/energy.F90:1362-1369) */
+        double fac = 2.0 * Pi / s->vol, sz = 0.0, term;
+        for (ia = 0; ia < s->np; ++ia) sz += s->az[ia] * s->ro[3 * ia + 2];
+        term = fac * (sz * sz);
+        urec = urec + term;
+        for (ia = 0; ia < s->np; ++ia)
+            s->force[3 * ia + 2] = s->force[3 * ia + 2] - s->epsfp * (2.0 * fac) * s->az[ia] * sz;
+        virrec = virrec - term;
+    } else if (s->lsurf) {
         double fac = 2.0 * Pi / (3.0 * s->vol), sx = 0.0, sy = 0.0, sz = 0.0, term;
         for (ia = 0; ia < s->np; ++ia) {
             sx += s->az[ia] * s->ro[3 * ia];
@@ -1333,7 +1456,8 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
     double *uold = malloc(sizeof(double) * (natat + 1));
     cx *tm[3] = {NULL, NULL, NULL}, *stm = NULL, *yzt = NULL;
     const size_t w = (size_t)s->ncut + 1;
-    if (s->lewald && s->lewald != 2) { free(dtwob); free(unew); free(uold); return 6; }
+    /* SPME and the 2D layer correction have no trial-move difference here */
+    if ((s->lewald && s->lewald != 2) || s->elc) { free(dtwob); free(unew); free(uold); return 6; }
     if (s->lewald == 2) {
         for (k = 0; k < 3; ++k) tm[k] = malloc(sizeof(cx) * w);
         stm = malloc(sizeof(cx) * 4 * (size_t)(s->nkvec > 0 ? s->nkvec : 1));

@@ -107,6 +107,7 @@ typedef struct or_params {
     int32_t lcellbuild;      /* 1: build the Verlet list through cells (same pair set) */
     int32_t ncut;            /* standard Ewald: largest |n| component of k = 2 pi n / L */
     int32_t ncutregion;      /* standard Ewald: 0 'sphere' (|n|^2 <= ncut^2), 1 'cube' */
+    int32_t lewald2dlc;      /* 1: the 2D layer correction (UEwaldRecStd2dlc) and UEwaldSurf's 2D form */
 } or_params;
 
 typedef struct or_sys or_sys;

@@ -33,7 +33,7 @@ class Params(C.Structure):
                 ("epsi_four_pi", C.c_double), ("nbond", C.c_int32), ("bond_ij", i32p),
                 ("bond_k", f64p), ("bond_eq", f64p), ("bond_p", i32p), ("tstep", C.c_double),
                 ("maxnneigh", C.c_int32), ("lcellbuild", C.c_int32), ("ncut", C.c_int32),
-                ("ncutregion", C.c_int32)]
+                ("ncutregion", C.c_int32), ("lewald2dlc", C.c_int32)]
 
 
 def lib():
@@ -242,7 +242,8 @@ class System:
                    sysd["ualpha"], sysd["epsi_four_pi"], nb, _p(k["bond_ij"], C.c_int32),
                    _p(k["bond_k"], C.c_double), _p(k["bond_eq"], C.c_double),
                    _p(k["bond_p"], C.c_int32), sysd["tstep"], self.maxnneigh, int(lcellbuild),
-                   int(sysd.get("ncut", 0)), 1 if sysd.get("ncutregion", "sphere") == "cube" else 0)
+                   int(sysd.get("ncut", 0)), 1 if sysd.get("ncutregion", "sphere") == "cube" else 0,
+                   int(bool(sysd.get("lewald2dlc", False))))
         self.h = L.or_create(C.byref(P))
 
     def __del__(self):

@@ -105,3 +105,22 @@ def site_table(s):
 @functools.lru_cache(maxsize=None)
 def rigid_small():
     return S.rigid_molecules(seed=2, nmol=150, nsolute=60, L=30.0, rcut=10.0)
+
+
+def slab_small(Lz=120.0, seed=3, lsurf=True, ncut=12, region="sphere", elc=True):
+    """The small electrolyte as a slab: its ions placed in |z| < 10 A (at least 4 A apart) of
+    a 40 x 40 x Lz box, standard Ewald with ncut, the 2D layer correction (lewald2dlc) on."""
+    rng = np.random.default_rng(seed)
+    s = dict(electrolyte_small(lsurf=lsurf))
+    n = s["np"]
+    pts = []
+    while len(pts) < n:
+        x = np.array([rng.uniform(-20, 20), rng.uniform(-20, 20), rng.uniform(-10, 10)])
+        if all(np.sum(((x - p + 20) % 40 - 20)[:2] ** 2) + (x - p)[2] ** 2 > 16.0 for p in pts):
+            pts.append(x)
+    s["boxlen"] = np.array([40.0, 40.0, float(Lz)])
+    s["ro"] = np.array(pts)
+    s["rod"] = np.zeros((n, 3))
+    d = std_ewald(s, ncut=ncut, region=region)
+    d["lewald2dlc"] = bool(elc)
+    return d
