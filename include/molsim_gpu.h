@@ -102,7 +102,7 @@ typedef struct msg_params {
     int32_t ncutregion;      /* lewald 2: 0 'sphere' (|n|^2 <= ncut^2), 1 'cube'         */
     int32_t lewald2dlc;      /* 1: 2D layer correction (UEwaldRecStd2dlc, lewald 2) and    */
                              /*    UEwaldSurf's 2d-periodic form (Src/energy.F90:1106-1203, */
-                             /*    1362-1369); Monte Carlo refuses it                       */
+                             /*    1362-1369), in UTotal and in the Monte Carlo difference */
 } msg_params;
 
 typedef struct msg_handle msg_handle;

@@ -215,7 +215,7 @@ struct msg_handle {
     int ew_nk = 0, ew_ntile = 0, ew_nf = 0;
     // 2D layer correction: 2D k-vectors {nx, ny, system}, kfac2d, the eight sums per k-vector
     int4 *elc_kv = nullptr;
-    double *elc_kfac = nullptr, *elc_st = nullptr;
+    double *elc_kfac = nullptr, *elc_st = nullptr, *elc_sttm = nullptr;   // elc_sttm: a Monte Carlo trial's sums
     int elc_nk = 0;
     // Monte Carlo: Random's state, running energies, counts (accepted, hard-core rejects),
     // sweep parameters, displacement per type, trial structure factors
@@ -414,7 +414,7 @@ static void free_all(msg_handle *h)
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
                     h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
                     h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
-                    h->elc_kv, h->elc_kfac, h->elc_st};
+                    h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -2039,6 +2039,7 @@ void msg_handle::ensure_mc()
     mc_par = dalloc<McPar>(nsys);
     mc_dtr = dalloc<double>(std::max(1, type_tot));
     if (any_std) ew_sktm = dalloc<double2>(4 * (size_t)ew_nkv_tot);
+    if (elc_nk) elc_sttm = dalloc<double>(8 * (size_t)elc_nk);
     std::vector<int2> st(nsys);
     for (int s = 0; s < nsys; ++s) st[s] = mc_seed_state(s + 1);
     up(mc_rng, st.data(), nsys * sizeof(int2));
@@ -2069,10 +2070,7 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
                      "difference of a trial move transforms the whole mesh";
             return MSG_ERR_ARG;
         }
-        if (S.elc) {
-            h->err = "Monte Carlo moves do not take the 2D layer correction (lewald2dlc)";
-            return MSG_ERR_ARG;
-        }
+
         if (!p[s].dtran || (p[s].isamp != 0 && p[s].isamp != 1)) {
             h->err = "msg_mc_params needs dtran[npt] and isamp 0 or 1";
             return MSG_ERR_ARG;
@@ -2105,7 +2103,7 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
         k_mc_pass<<<h->nsys, MC_THREADS, smem, h->st>>>(
             h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tc, h->bst, h->ew_kv, h->ew_kfac, h->ew_sk,
             h->ew_sktm, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bk, h->beq, h->bpw, h->mc_par, h->mc_dtr,
-            h->mc_rng, h->mc_u, h->mc_cnt, npass, cache, wmax);
+            h->mc_rng, h->mc_u, h->mc_cnt, npass, cache, wmax, h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm);
         h->launches += 1;
     }
     std::vector<long long> cnt(2 * (size_t)h->nsys);

@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     const int *__restrict__ bptr, const int *__restrict__ bpart, const double *__restrict__ bk,
     const double *__restrict__ beq, const int *__restrict__ bpw, const McPar *__restrict__ par,
     const double *__restrict__ dtr, int2 *__restrict__ rng, double *__restrict__ mcu,
-    long long *__restrict__ cnt, int npass, int cache, int wmax)
+    long long *__restrict__ cnt, int npass, int cache, int wmax, const int4 *__restrict__ kv2,
+    const double *__restrict__ kfac2, double *__restrict__ st2, double *__restrict__ st2tm)
 {
     extern __shared__ double2 etab[];          // [6][ncut+1]: new x, y, z; old x, y, z
     constexpr int NSLOT = 10 + 4;              // type pairs, reciprocal, dipole x, y, z
@@ -173,8 +174,10 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
         sty = ty;
         sover = 0;
     };
-    // the structure factors in use and the trial's, swapped when a move is accepted
+    // the structure factors in use and the trial's, swapped when a move is accepted (and the
+    // layer correction's eight sums per 2D k-vector, the same way)
     double2 *scur = sk, *stry = sktm;
+    double *ecur = st2, *etry = st2tm;
     if (t == 0 && ntrial > 0) setup(0);
     __syncthreads();
     for (long long m = 0; m < ntrial; ++m) {
@@ -258,6 +261,51 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                 dr = dr + kfac[g] * (tnew - told);
             }
         }
+        // ---- the layer correction's sums of the trial (DUTwoBodyEwaldRec2dlc,
+        //      Src/denergy.F90:1339-1409; the old values by the same recurrence as the
+        //      tables the reference keeps) ----
+        if (S.elc && S.recstd) {
+            const double tpx = tp * S.boxi[0], tpy = tp * S.boxi[1];
+            double s1, c1;
+            sincos(tpx * rt[0], &s1, &c1);
+            const double2 etx = make_double2(c1, s1);
+            sincos(tpy * rt[1], &s1, &c1);
+            const double2 ety = make_double2(c1, s1);
+            sincos(tpx * r0[0], &s1, &c1);
+            const double2 eox = make_double2(c1, s1);
+            sincos(tpy * r0[1], &s1, &c1);
+            const double2 eoy = make_double2(c1, s1);
+            for (int kn = t; kn < S.elc_nkv; kn += MC_THREADS) {
+                const size_t g = (size_t)S.elc_kv_off + kn;
+                const int4 K = kv2[g];
+                double sxt, cxt, syt, cyt, sxo, cxo, syo, cyo;
+                elc_trig(K.x, etx, sxt, cxt);
+                elc_trig(K.y, ety, syt, cyt);
+                elc_trig(K.x, eox, sxo, cxo);
+                elc_trig(K.y, eoy, syo, cyo);
+                const double kx = K.x * tpx, ky = K.y * tpy, kp = sqrt(kx * kx + ky * ky);
+                double e = exp(kp * rt[2]), ei = 1.0 / e;
+                const double sht = 0.5 * (e - ei), cht = 0.5 * (e + ei);
+                e = exp(kp * r0[2]);
+                ei = 1.0 / e;
+                const double sho = 0.5 * (e - ei), cho = 0.5 * (e + ei);
+                const double *so = ecur + g * 8;
+                double *sn = etry + g * 8;
+                sn[0] = so[0] + q * (sxt * syt * sht - sxo * syo * sho);
+                sn[1] = so[1] + q * (cxt * syt * sht - cxo * syo * sho);
+                sn[2] = so[2] + q * (sxt * cyt * sht - sxo * cyo * sho);
+                sn[3] = so[3] + q * (cxt * cyt * sht - cxo * cyo * sho);
+                sn[4] = so[4] + q * (sxt * syt * cht - sxo * syo * cho);
+                sn[5] = so[5] + q * (cxt * syt * cht - cxo * syo * cho);
+                sn[6] = so[6] + q * (sxt * cyt * cht - sxo * cyo * cho);
+                sn[7] = so[7] + q * (cxt * cyt * cht - cxo * cyo * cho);
+                const double tn = -sn[0] * sn[0] - sn[1] * sn[1] - sn[2] * sn[2] - sn[3] * sn[3] + sn[4] * sn[4] +
+                                  sn[5] * sn[5] + sn[6] * sn[6] + sn[7] * sn[7];
+                const double to = -so[0] * so[0] - so[1] * so[1] - so[2] * so[2] - so[3] * so[3] + so[4] * so[4] +
+                                  so[5] * so[5] + so[6] * so[6] + so[7] * so[7];
+                dr = dr + kfac2[g] * (tn - to);
+            }
+        }
 #pragma unroll
         for (int p = 0; p < 10; ++p)
             if (p < natat) mc_block_add(du[p], red, p);
@@ -292,10 +340,17 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                             m1 += red[12][k];
                             m2 += red[13][k];
                         }
-                        const double fac = tp / (3.0 * S.vol);
-                        const double a0 = m0 + q * (rt[0] - r0[0]), a1 = m1 + q * (rt[1] - r0[1]),
-                                     a2 = m2 + q * (rt[2] - r0[2]);
-                        durec += fac * ((a0 * a0 + a1 * a1 + a2 * a2) - (m0 * m0 + m1 * m1 + m2 * m2));
+                        if (S.elc) {
+                            // DUTwoBodyEwaldSurf, 2d-periodic form (Src/denergy.F90:1527-1536)
+                            const double fac = tp / S.vol;
+                            const double a2 = m2 + q * (rt[2] - r0[2]);
+                            durec += fac * (a2 * a2 - m2 * m2);
+                        } else {
+                            const double fac = tp / (3.0 * S.vol);
+                            const double a0 = m0 + q * (rt[0] - r0[0]), a1 = m1 + q * (rt[1] - r0[1]),
+                                         a2 = m2 + q * (rt[2] - r0[2]);
+                            durec += fac * ((a0 * a0 + a1 * a1 + a2 * a2) - (m0 * m0 + m1 * m1 + m2 * m2));
+                        }
                     }
                     durec = S.epsfp * durec;
                     dutot += durec;
@@ -350,8 +405,13 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
             double2 *tmp = scur;
             scur = stry;
             stry = tmp;
+            double *etmp = ecur;
+            ecur = etry;
+            etry = etmp;
         }
     }
+    if (S.elc && S.recstd && ecur != st2)
+        for (int e = t; e < 8 * S.elc_nkv; e += MC_THREADS) st2[(size_t)8 * S.elc_kv_off + e] = ecur[(size_t)8 * S.elc_kv_off + e];
     // the structure factors end where the last accepted move left them: back into sk
     if (S.recstd && scur != sk)
         for (int kn = t; kn < S.ew_nkv; kn += MC_THREADS) {

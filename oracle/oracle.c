@@ -527,6 +527,7 @@ struct or_sys {
     int elc, ncut2d2, nkvec2d;
     double *kfac2d;
     double *trig2d;          /* [np][4][ncut+1]: sin kx, cos kx, sin ky, cos ky */
+    double *sumtrig;         /* [nkvec2d][8]: the sums of the last UTotal / MC update */
     /* Random's SAVEd state (Src/mollib.F90:2683-2687) */
     int32_t rix, riy;
     int nbond; int32_t *bond_ij; double *bond_k, *bond_eq; int32_t *bond_p;
@@ -596,6 +597,7 @@ static void ewald_setup_2dlc(or_sys *s, int cube)
         }
     s->nkvec2d = n;
     s->trig2d = malloc(sizeof(double) * 4 * (size_t)s->np * ((size_t)nc + 1));
+    s->sumtrig = calloc(8 * (size_t)(n > 0 ? n : 1), sizeof(double));
 }
 
 or_sys *or_create(const or_params *p)
@@ -680,7 +682,7 @@ void or_destroy(or_sys *s)
     free(s->ubuf); free(s->iubuflow); free(s->r2umin); free(s->r2atat);
     free(s->nneighpn); free(s->jpnlist);
     free(s->meshfac); free(s->energyfac); free(s->virfac); free(s->qmesh); free(s->fqmesh);
-    free(s->kfac2d); free(s->trig2d);
+    free(s->kfac2d); free(s->trig2d); free(s->sumtrig);
     free(s->kfac); free(s->eik[0]); free(s->eik[1]); free(s->eik[2]); free(s->eyz); free(s->eikr);
     free(s->sumeikr);
     free(s->bond_ij); free(s->bond_k); free(s->bond_eq); free(s->bond_p);
@@ -1135,6 +1137,7 @@ static void uewald_rec_std2dlc(or_sys *s, double *urec)
             term = s->kfac2d[kn] * (-st[0] * st[0] - st[1] * st[1] - st[2] * st[2] - st[3] * st[3] +
                                     st[4] * st[4] + st[5] * st[5] + st[6] * st[6] + st[7] * st[7]);
             uloc = uloc + term;
+            for (c = 0; c < 8; ++c) s->sumtrig[8 * (size_t)kn + c] = st[c];
             kfac2 = s->epsfp * 2.0 * s->kfac2d[kn];
             kxx = kfac2 * kx;
             kyy = kfac2 * ky;
@@ -1455,13 +1458,18 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
     double *dtwob = malloc(sizeof(double) * (natat + 1)), *unew = malloc(sizeof(double) * (natat + 1));
     double *uold = malloc(sizeof(double) * (natat + 1));
     cx *tm[3] = {NULL, NULL, NULL}, *stm = NULL, *yzt = NULL;
+    double *trigtm = NULL, *sttm = NULL;     /* layer correction: trial tables and sums */
     const size_t w = (size_t)s->ncut + 1;
-    /* SPME and the 2D layer correction have no trial-move difference here */
-    if ((s->lewald && s->lewald != 2) || s->elc) { free(dtwob); free(unew); free(uold); return 6; }
+    /* SPME has no trial-move difference here */
+    if (s->lewald && s->lewald != 2) { free(dtwob); free(unew); free(uold); return 6; }
     if (s->lewald == 2) {
         for (k = 0; k < 3; ++k) tm[k] = malloc(sizeof(cx) * w);
         stm = malloc(sizeof(cx) * 4 * (size_t)(s->nkvec > 0 ? s->nkvec : 1));
         yzt = malloc(sizeof(cx) * 2);
+    }
+    if (s->elc) {
+        trigtm = malloc(sizeof(double) * 4 * w);
+        sttm = malloc(sizeof(double) * 8 * (size_t)(s->nkvec2d > 0 ? s->nkvec2d : 1));
     }
     for (pass = 0; pass < npass; ++pass) {
         for (ipass = 0; ipass < np; ++ipass) {
@@ -1587,7 +1595,67 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
                         }
                     }
                 }
-                if (s->lsurf) {
+                if (s->elc) {
+                    /* DUTwoBodyEwaldRec2dlc (Src/denergy.F90:1339-1409) with EwaldSetArray2dTM */
+                    const double *to = s->trig2d + (size_t)ip * 4 * w;
+                    for (m = 0; m < 4; ++m) trigtm[m * w] = 1.0;
+                    if (nc >= 1) {
+                        trigtm[1] = sin(tpbi[0] * rtm[0]);
+                        trigtm[w + 1] = cos(tpbi[0] * rtm[0]);
+                        trigtm[2 * w + 1] = sin(tpbi[1] * rtm[1]);
+                        trigtm[3 * w + 1] = cos(tpbi[1] * rtm[1]);
+                    }
+                    for (icut = 2; icut <= nc; ++icut) {
+                        trigtm[icut] = trigtm[icut - 1] * trigtm[w + 1] + trigtm[w + icut - 1] * trigtm[1];
+                        trigtm[w + icut] = trigtm[w + icut - 1] * trigtm[w + 1] - trigtm[icut - 1] * trigtm[1];
+                        trigtm[2 * w + icut] = trigtm[2 * w + icut - 1] * trigtm[3 * w + 1] +
+                                               trigtm[3 * w + icut - 1] * trigtm[2 * w + 1];
+                        trigtm[3 * w + icut] = trigtm[3 * w + icut - 1] * trigtm[3 * w + 1] -
+                                               trigtm[2 * w + icut - 1] * trigtm[2 * w + 1];
+                    }
+                    kn = 0;
+                    for (ny = 0; ny <= nc; ++ny) {
+                        const double ky = ny * tpbi[1];
+                        for (nx = 0; nx <= nc; ++nx) {
+                            const double kx = nx * tpbi[0];
+                            double kp, e, ei, sht, cht, sho, cho, tn, to_, *st = sttm + 8 * (size_t)kn;
+                            const double *so = s->sumtrig + 8 * (size_t)kn;
+                            const double sxt = trigtm[nx], cxt = trigtm[w + nx], syt = trigtm[2 * w + ny],
+                                         cyt = trigtm[3 * w + ny];
+                            const double sxo = to[nx], cxo = to[w + nx], syo = to[2 * w + ny], cyo = to[3 * w + ny];
+                            if (nx * nx + ny * ny > s->ncut2d2) continue;
+                            if (nx == 0 && ny == 0) continue;
+                            kp = sqrt(kx * kx + ky * ky);
+                            e = exp(kp * rtm[2]); ei = 1.0 / e;
+                            sht = 0.5 * (e - ei); cht = 0.5 * (e + ei);
+                            e = exp(kp * s->ro[3 * ip + 2]); ei = 1.0 / e;
+                            sho = 0.5 * (e - ei); cho = 0.5 * (e + ei);
+                            st[0] = so[0] + q * (sxt * syt * sht - sxo * syo * sho);
+                            st[1] = so[1] + q * (cxt * syt * sht - cxo * syo * sho);
+                            st[2] = so[2] + q * (sxt * cyt * sht - sxo * cyo * sho);
+                            st[3] = so[3] + q * (cxt * cyt * sht - cxo * cyo * sho);
+                            st[4] = so[4] + q * (sxt * syt * cht - sxo * syo * cho);
+                            st[5] = so[5] + q * (cxt * syt * cht - cxo * syo * cho);
+                            st[6] = so[6] + q * (sxt * cyt * cht - sxo * cyo * cho);
+                            st[7] = so[7] + q * (cxt * cyt * cht - cxo * cyo * cho);
+                            tn = -st[0] * st[0] - st[1] * st[1] - st[2] * st[2] - st[3] * st[3] +
+                                 st[4] * st[4] + st[5] * st[5] + st[6] * st[6] + st[7] * st[7];
+                            to_ = -so[0] * so[0] - so[1] * so[1] - so[2] * so[2] - so[3] * so[3] +
+                                  so[4] * so[4] + so[5] * so[5] + so[6] * so[6] + so[7] * so[7];
+                            durec = durec + s->kfac2d[kn] * (tn - to_);
+                            ++kn;
+                        }
+                    }
+                }
+                if (s->lsurf && s->elc) {
+                    /* DUTwoBodyEwaldSurf, 2d-periodic form: the z dipole */
+                    const double fac = 2.0 * Pi / s->vol;
+                    double sz = 0.0, tz;
+                    int ia;
+                    for (ia = 0; ia < np; ++ia) sz += s->az[ia] * s->ro[3 * ia + 2];
+                    tz = sz + q * (rtm[2] - s->ro[3 * ip + 2]);
+                    durec = durec + fac * (tz * tz - sz * sz);
+                } else if (s->lsurf) {
                     const double fac = 2.0 * Pi / (3.0 * s->vol);
                     double sx = 0.0, sy = 0.0, sz = 0.0, tx, ty, tz;
                     int ia;
@@ -1652,6 +1720,10 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
                 for (m = 0; m < 3; ++m) memcpy((cx *)s->eik[m] + (size_t)ip * w, tm[m], sizeof(cx) * w);
                 memcpy(s->sumeikr, stm, sizeof(cx) * 4 * (size_t)s->nkvec);
             }
+            if (s->elc) {
+                memcpy(s->trig2d + (size_t)ip * 4 * w, trigtm, sizeof(double) * 4 * w);
+                memcpy(s->sumtrig, sttm, sizeof(double) * 8 * (size_t)s->nkvec2d);
+            }
             for (m = 0; m < 3; ++m) {
                 s->ro[3 * ip + m] = rtm[m];
                 s->drostep[3 * ip + m] += d[m];
@@ -1660,7 +1732,7 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
     }
     free(dtwob); free(unew); free(uold);
     for (k = 0; k < 3; ++k) free(tm[k]);
-    free(stm); free(yzt);
+    free(stm); free(yzt); free(trigtm); free(sttm);
     return 0;
 }
 

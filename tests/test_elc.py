@@ -100,10 +100,44 @@ def test_gpu_velver_short_trajectory():
     assert Hp.rel(eg[-1]["urec"], o.utotal()["urec"]) < 1e-9
 
 
-@pytest.mark.gpu
-def test_gpu_mc_refuses_the_correction():
+def test_oracle_mc_running_energy_equals_fresh_utotal():
+    """Monte Carlo with the correction (DUTwoBodyEwaldRec2dlc and the 2d-periodic surface
+    difference): the energies carried by the accepted moves equal a fresh UTotal of the
+    final configuration."""
+    from molsim_b200 import systems as S
+
     s = Hp.slab_small()
-    g = Engine(s, Hp.oracle_table(s), precision="fp64")
-    with pytest.raises(MolsimGpuError) as ei:
-        g.MCPass(1, [1.0] * s["npt"], 1.0)
-    assert ei.value.code == 6
+    t, o = _oracle(s)
+    u = o.utotal()
+    o.mc_seed(11)
+    acc, _ = o.mc_pass(2, [2.0] * s["npt"], 1.0 / S.kT(s["temp"]), u)
+    assert acc > 0
+    o.set_vlist()
+    fresh = o.utotal()
+    sc = abs(fresh["utwob"][0]) + abs(fresh["urec"]) + 1.0
+    for k in ("utot", "urec"):
+        assert abs(u[k] - fresh[k]) <= 1e-9 * sc, (k, u[k], fresh[k])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("isamp", [0, 1])
+def test_gpu_mc_chain_matches_oracle(isamp):
+    """The GPU chain with the correction makes the oracle's moves: the same acceptances,
+    bit-identical positions, energies within 1e-9 of the energy scale."""
+    from molsim_b200 import systems as S
+
+    s = Hp.slab_small()
+    t, o = _oracle(s)
+    beta = 1.0 / S.kT(s["temp"])
+    dtran = [2.0] * s["npt"] if isamp == 0 else [-3.0] * s["npt"]
+    u = o.utotal()
+    o.mc_seed(7)
+    acc, hs = o.mc_pass(2, dtran, beta, u, isamp=isamp)
+    g = Engine(s, t, precision="fp64")
+    g.mc_seed(7)
+    ag, hg, eg = g.MCPass(2, dtran, beta, isamp)
+    assert (int(ag[0]), int(hg[0])) == (acc, hs)
+    assert np.array_equal(g.get_state()["ro"], o.get_state()["ro"])
+    sc = abs(u["utwob"][0]) + abs(u["urec"]) + 1.0
+    for k in ("utot", "urec"):
+        assert abs(eg[k] - u[k]) <= 1e-9 * sc, (k, eg[k], u[k])
