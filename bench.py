@@ -493,6 +493,32 @@ def run_mc(a):
         out["cpu_baseline"] = {"value": n / cpu_s, "unit": "trial moves/s", "cores": 1, "kind": "port",
                                "sample": "one sweep (1000 trial moves) of the same chain, oracle (FP64 C "
                                          "restatement of SPartMove/DUTotal/Metropolis/MCUpdate), 1 thread"}
+    # the same chain with SPME reciprocal space (32^3, order 4): the trial's energy difference from
+    # the spectrum and the two stencils' transforms
+    ds = dict(s)
+    tsp = prepare(ds)
+    e2 = Engine(ds, tsp, precision="fp64")
+    e2.mc_seed(1)
+    sec, acc = timed(e2, sweeps)
+    sp = {"workload": "electrolyte_1000, SPME %d^3 order %d, dtran 2 A, 298 K" % (s["nmesh"], s["order"]),
+          "value": n * sweeps / sec, "unit": "trial moves/s", "sweeps": sweeps,
+          "acceptance": float(acc[0]) / (n * sweeps)}
+    del e2
+    if not a.no_cpu_baseline:
+        ods = dict(ds)
+        ods["ualpha"] = tsp["ualpha"]
+        o2 = O.System(ods, ot, maxnneigh=n)
+        o2.set_state(s["ro"], s["rod"])
+        o2.set_vlist()
+        u2 = o2.utotal()
+        o2.mc_seed(1)
+        t0 = time.perf_counter()
+        o2.mc_pass(1, dtran, beta, u2)
+        sp["cpu_baseline"] = {"value": n / (time.perf_counter() - t0), "unit": "trial moves/s", "cores": 1,
+                              "kind": "port", "sample": "one sweep of the same SPME chain, oracle (the "
+                                                        "reference's way: the mesh re-transformed per trial), "
+                                                        "1 thread"}
+    out["spme"] = sp
     return out
 
 

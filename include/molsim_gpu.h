@@ -193,8 +193,10 @@ int  msg_mc_seed(msg_handle *h, int32_t isys, int32_t iseed);
  * accepted / hsreject [nsys] (optional): moves accepted and moves rejected for a
  * hard-core or below-table overlap in this call.  e (optional): energies of system
  * isys after the sweeps, from a UTotal at the start plus the accepted moves'
- * differences (MCUpdate).  The lists are rebuilt afterwards.  Systems must use the
- * standard Ewald sum (lewald 2) or none: MSG_ERR_ARG for SPME. */
+ * differences (MCUpdate).  The lists are rebuilt afterwards.  Any reciprocal method:
+ * standard Ewald (DUTwoBodyEwaldRecStd, with lewald2dlc its layer correction) or SPME
+ * (DUTwoBodyEwaldRecSPM, Src/denergy.F90:1413-1495, from the spectrum of the mesh at the
+ * call and the moved stencils' transforms). */
 int  msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p, int64_t *accepted,
                  int64_t *hsreject, int32_t isys, msg_energy *e);
 

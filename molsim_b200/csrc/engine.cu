@@ -216,6 +216,12 @@ struct msg_handle {
     // 2D layer correction: 2D k-vectors {nx, ny, system}, kfac2d, the eight sums per k-vector
     int4 *elc_kv = nullptr;
     double *elc_kfac = nullptr, *elc_st = nullptr, *elc_sttm = nullptr;   // elc_sttm: a Monte Carlo trial's sums
+    // Monte Carlo with SPME: the FP64 spectrum of each system's charge mesh (engine's grid
+    // offsets), its fixed-point and FP64 meshes, D2Z plans per mesh class
+    double2 *mc_F = nullptr;
+    double *mc_rg = nullptr;
+    unsigned long long *mc_ig = nullptr;
+    std::vector<cufftHandle> mc_plans;
     int elc_nk = 0;
     // Monte Carlo: Random's state, running energies, counts (accepted, hard-core rejects),
     // sweep parameters, displacement per type, trial structure factors
@@ -414,7 +420,7 @@ static void free_all(msg_handle *h)
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
                     h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
                     h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
-                    h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm};
+                    h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -442,6 +448,7 @@ static void free_all(msg_handle *h)
 
 msg_handle::~msg_handle()
 {
+    for (cufftHandle p : mc_plans) cufftDestroy(p);
     drop_graph();
     free_all(this);
 }
@@ -2040,6 +2047,19 @@ void msg_handle::ensure_mc()
     mc_dtr = dalloc<double>(std::max(1, type_tot));
     if (any_std) ew_sktm = dalloc<double2>(4 * (size_t)ew_nkv_tot);
     if (elc_nk) elc_sttm = dalloc<double>(8 * (size_t)elc_nk);
+    if (any_spme) {
+        mc_ig = dalloc<unsigned long long>(grid_tot);
+        CK(cudaMemsetAsync(mc_ig, 0, grid_tot * sizeof(unsigned long long), st));
+        mc_rg = dalloc<double>(grid_tot);
+        mc_F = dalloc<double2>(cgrid_tot);
+        for (const FftClass &fc : fft) {
+            cufftHandle p = 0;
+            int dims[3] = {fc.s, fc.s, fc.s};
+            const int rd = fc.s * fc.s * fc.s, cd = fc.s * fc.s * (fc.s / 2 + 1);
+            CKF(cufftPlanMany(&p, 3, dims, nullptr, 1, rd, nullptr, 1, cd, CUFFT_D2Z, fc.count));
+            mc_plans.push_back(p);
+        }
+    }
     std::vector<int2> st(nsys);
     for (int s = 0; s < nsys; ++s) st[s] = mc_seed_state(s + 1);
     up(mc_rng, st.data(), nsys * sizeof(int2));
@@ -2065,11 +2085,7 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
     std::vector<double> dtr(std::max(1, h->type_tot), 0.0);
     for (int s = 0; s < h->nsys; ++s) {
         const SysDev &S = h->hs[s];
-        if (S.lewald && !S.recstd) {
-            h->err = "Monte Carlo moves need the standard Ewald sum (lewald 2) or none: the SPME energy "
-                     "difference of a trial move transforms the whole mesh";
-            return MSG_ERR_ARG;
-        }
+
 
         if (!p[s].dtran || (p[s].isamp != 0 && p[s].isamp != 1)) {
             h->err = "msg_mc_params needs dtran[npt] and isamp 0 or 1";
@@ -2088,11 +2104,26 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
     // from here by the accepted moves' differences (MCUpdate)
     h->enqueue_forces(0, false);
     CK(cudaMemcpyAsync(h->mc_u, h->esys, sizeof(double) * ESZ * h->nsys, cudaMemcpyDeviceToDevice, h->st));
+    if (npass > 0 && h->any_spme) {
+        // the FP64 spectrum of every SPME system's charge mesh at the start of the pass
+        k_mc_spread<<<h->nt128, 128, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->mc_ig);
+        k_mc_mesh_f64<<<(unsigned)((h->grid_tot + 255) / 256), 256, 0, h->st>>>(h->grid_tot, h->mc_ig, h->mc_rg);
+        for (size_t c = 0; c < h->fft.size(); ++c) {
+            CKF(cufftSetStream(h->mc_plans[c], h->st));
+            CKF(cufftExecD2Z(h->mc_plans[c], h->mc_rg + h->fft[c].grid_off,
+                             reinterpret_cast<cufftDoubleComplex *>(h->mc_F + h->fft[c].cgrid_off)));
+        }
+        h->launches += 2;
+    }
     if (npass > 0) {
         // a chain reads its system from shared memory when every system's share fits and
         // there are no more chains than SMs (each such block holds an SM on its own)
         const int wmax = h->any_std ? h->ew_maxw : 1;
-        const size_t etab = 6 * (size_t)wmax * sizeof(double2);
+        int smax = 0;
+        for (int s = 0; s < h->nsys; ++s)
+            if (h->hs[s].lewald && !h->hs[s].recstd) smax = std::max(smax, h->hs[s].s);
+        const int etabn = std::max(6 * wmax, 7 * smax);
+        const size_t etab = (size_t)etabn * sizeof(double2);
         size_t need = 0;
         for (int s = 0; s < h->nsys; ++s)
             need = std::max(need, mc_cache_bytes(h->hs[s].n, h->hs[s].tab_nk, h->hs[s].natat));
@@ -2103,7 +2134,8 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
         k_mc_pass<<<h->nsys, MC_THREADS, smem, h->st>>>(
             h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tc, h->bst, h->ew_kv, h->ew_kfac, h->ew_sk,
             h->ew_sktm, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bk, h->beq, h->bpw, h->mc_par, h->mc_dtr,
-            h->mc_rng, h->mc_u, h->mc_cnt, npass, cache, wmax, h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm);
+            h->mc_rng, h->mc_u, h->mc_cnt, npass, cache, wmax, h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm,
+            h->mc_F, h->emf, etabn);
         h->launches += 1;
     }
     std::vector<long long> cnt(2 * (size_t)h->nsys);

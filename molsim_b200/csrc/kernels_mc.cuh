@@ -80,6 +80,89 @@ __device__ __forceinline__ void mc_block_add(double v, double (*red)[MC_THREADS 
     if ((threadIdx.x & 31) == 0) red[slot][threadIdx.x >> 5] = v;
 }
 
+// Cardinal B-spline values M_P(x + i), i = 0..order-1, of the mesh coordinate u
+// (CardinalBSpline, Src/mollib.F90:1629-1683) for a run-time order <= MSG_MAX_ORDER;
+// returns floor(u) wrapped into [0, s).
+__device__ __forceinline__ int mc_bspline(int order, double u, int s, double *v)
+{
+    const double fl = floor(u), x = u - fl;
+    double last[MSG_MAX_ORDER];
+    v[0] = x;
+    v[1] = 1.0 - x;
+    for (int n = 3; n <= order; ++n) {
+        for (int i = 0; i < n - 1; ++i) last[i] = v[i];
+        const double nm1 = (double)(n - 1);
+        v[0] = x * last[0] / nm1;
+        for (int i = 1; i <= n - 2; ++i) {
+            const double a = (double)i + x;
+            v[i] = (a * last[i] + ((double)n - a) * last[i - 1]) / nm1;
+        }
+        v[n - 1] = (1.0 - x) * last[n - 2] / nm1;
+    }
+    int k = (int)fl % s;
+    return k < 0 ? k + s : k;
+}
+
+// The charge mesh of an SPME system for a Monte Carlo pass: q Mx My Mz spread as 64-bit
+// fixed point (2^-40), one thread per particle, at the system's grid offset.
+__global__ void k_mc_spread(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                            const double4 *__restrict__ pos, unsigned long long *__restrict__ ig)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    if (!S.lewald || S.recstd) return;
+    const int i = T.i0 + threadIdx.x;
+    if (i >= T.i1) return;
+    const double4 x = pos[i];
+    const int s = S.s, P = S.order;
+    const double xc[3] = {x.x, x.y, x.z};
+    double th[3][MSG_MAX_ORDER];
+    int km[3];
+    for (int m = 0; m < 3; ++m) km[m] = mc_bspline(P, S.dkdr[m] * xc[m], s, th[m]);
+    for (int iz = 0; iz < P; ++iz) {
+        int nz = km[2] - iz;
+        nz += (nz < 0) ? s : 0;
+        const double qz = x.w * th[2][iz];
+        for (int iy = 0; iy < P; ++iy) {
+            int ny = km[1] - iy;
+            ny += (ny < 0) ? s : 0;
+            const double qyz = qz * th[1][iy];
+            for (int ix = 0; ix < P; ++ix) {
+                int nx = km[0] - ix;
+                nx += (nx < 0) ? s : 0;
+                atomicAdd(ig + S.grid_off + ((size_t)nz * s + ny) * s + nx,
+                          (unsigned long long)__double2ll_rn(qyz * th[0][ix] * kGridFix));
+            }
+        }
+    }
+}
+
+__global__ void k_mc_mesh_f64(long long n, unsigned long long *__restrict__ ig, double *__restrict__ g)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        g[k] = (double)(long long)ig[k] * kGridFixInv;
+        ig[k] = 0ull;
+    }
+}
+
+// The transform of one particle's stencil along one dimension,
+// B(k) = sum_i M(i) exp(-2 pi i k (km - i) / s), from the twiddles tw[m] = exp(-2 pi i m / s).
+__device__ __forceinline__ double2 mc_stencil_ft(int order, double u, int s, int k, const double2 *tw)
+{
+    double v[MSG_MAX_ORDER];
+    const int km = mc_bspline(order, u, s, v);
+    double2 b = make_double2(0.0, 0.0);
+    for (int i = 0; i < order; ++i) {
+        int n = km - i;
+        n += (n < 0) ? s : 0;
+        const double2 e = tw[(int)(((long long)k * n) % s)];
+        b.x += v[i] * e.x;
+        b.y += v[i] * e.y;
+    }
+    return b;
+}
+
 // npass sweeps of one system per block.  Dynamic shared memory: six rows of
 // wmax double2 (new and old exp(i k x) of the moved particle, standard Ewald), then,
 // when `cache` is set, the system's positions and types, its table rows and its
@@ -98,17 +181,20 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     const double *__restrict__ beq, const int *__restrict__ bpw, const McPar *__restrict__ par,
     const double *__restrict__ dtr, int2 *__restrict__ rng, double *__restrict__ mcu,
     long long *__restrict__ cnt, int npass, int cache, int wmax, const int4 *__restrict__ kv2,
-    const double *__restrict__ kfac2, double *__restrict__ st2, double *__restrict__ st2tm)
+    const double *__restrict__ kfac2, double *__restrict__ st2, double *__restrict__ st2tm,
+    double2 *__restrict__ mcF, const double *__restrict__ emf, int etabn)
 {
-    extern __shared__ double2 etab[];          // [6][ncut+1]: new x, y, z; old x, y, z
+    // etabn double2: standard Ewald [6][ncut+1] (new x, y, z; old x, y, z); SPME the twiddles
+    // [s] and the stencil transforms [2][3][s] (trial, current)
+    extern __shared__ double2 etab[];
     constexpr int NSLOT = 10 + 4;              // type pairs, reciprocal, dipole x, y, z
     __shared__ double red[NSLOT][MC_THREADS / 32];
     __shared__ double srt[3], sro[3], sq;
     __shared__ int si, sip, sty, sover, sacc;
     const int sys = blockIdx.x;
     const SysDev &S = sysv[sys];
-    if (S.lewald && !S.recstd) return;         // SPME systems are refused on the host
     const int t = threadIdx.x;
+    const bool spm = S.lewald && !S.recstd;
     const int natat = S.natat, w = S.ew_ncut + 1;
     const McPar P = par[sys];
     int2 st = rng[sys];                        // used by thread 0 only
@@ -124,7 +210,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     int poff = 0, koff = 0, boff = 0;
     double4 *cpos = nullptr;
     if (cache) {
-        unsigned char *base = reinterpret_cast<unsigned char *>(etab + 6 * wmax);
+        unsigned char *base = reinterpret_cast<unsigned char *>(etab + etabn);
         cpos = reinterpret_cast<double4 *>(base);
         int *ctyp = reinterpret_cast<int *>(cpos + S.n);
         double *ctc = reinterpret_cast<double *>(base + ((36 * (size_t)S.n + 15) / 16) * 16);
@@ -142,6 +228,14 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
         poff = S.off;
         koff = S.tab_k0;
         boff = S.tab_b0;
+        __syncthreads();
+    }
+    if (spm) {
+        for (int m = t; m < S.s; m += MC_THREADS) {
+            double sn, cs;
+            sincospi(2.0 * (double)m / (double)S.s, &sn, &cs);
+            etab[m] = make_double2(cs, -sn);
+        }
         __syncthreads();
     }
     // Thread 0 sets up a trial: particle, displacement, periodic wrap.
@@ -197,6 +291,15 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
             for (int n = 1; n < w; ++n) {
                 e = (n == 1) ? e1 : cmul(e, e1);
                 row[n] = e;
+            }
+        }
+        // ---- SPME: transforms of the trial's and the current stencil along each dimension ----
+        if (spm) {
+            const int sm = S.s;
+            for (int e = t; e < 6 * sm; e += MC_THREADS) {
+                const int set = e / (3 * sm), d = (e / sm) % 3, k = e % sm;
+                const double xm = set == 0 ? rt[d] : r0[d];
+                etab[sm + e] = mc_stencil_ft(S.order, S.dkdr[d] * xm, sm, k, etab);
             }
         }
         // ---- pair differences (and the dipole sum of the surface term) ----
@@ -259,6 +362,26 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
                     told = told + (s0.x * s0.x + s0.y * s0.y);
                 }
                 dr = dr + kfac[g] * (tnew - told);
+            }
+        }
+        // ---- SPME: u%rec(trial mesh) - u%rec(mesh) (DUTwoBodyEwaldRecSPM, Src/denergy.F90:1413-1495)
+        //      from the spectrum F and the stencils' transform dF = q (Bx By Bz - Bx' By' Bz'):
+        //      sum emf (2 Re(conj F dF) + |dF|^2) over the r2c half spectrum ----
+        if (spm) {
+            const int sm = S.s, h = sm / 2 + 1;
+            const double2 *Bn = etab + sm, *Bo = etab + 4 * sm;
+            const int nc = sm * sm * h;
+            // unrolled so that a warp keeps several of its spectrum loads in flight
+#pragma unroll 4
+            for (int c = t; c < nc; c += MC_THREADS) {
+                const int kx = c % h, rr = c / h, ky = rr % sm, kz = rr / sm;
+                const double2 pn = cmul(cmul(Bn[kx], Bn[sm + ky]), Bn[2 * sm + kz]);
+                const double2 po = cmul(cmul(Bo[kx], Bo[sm + ky]), Bo[2 * sm + kz]);
+                const double2 dF = make_double2(q * (pn.x - po.x), q * (pn.y - po.y));
+                const double2 F = mcF[S.cgrid_off + c];
+                const int fy = ky <= sm / 2 ? ky : sm - ky, fz = kz <= sm / 2 ? kz : sm - kz;
+                const double wgt = emf[S.fac_off + kx + (size_t)h * (fy + (size_t)h * fz)];
+                dr = dr + wgt * (2.0 * (F.x * dF.x + F.y * dF.y) + (dF.x * dF.x + dF.y * dF.y));
             }
         }
         // ---- the layer correction's sums of the trial (DUTwoBodyEwaldRec2dlc,
@@ -408,6 +531,26 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
             double *etmp = ecur;
             ecur = etry;
             etry = etmp;
+        }
+        if (spm) {
+            // MCUpdate: the spectrum follows the accepted move; the stencil transforms are
+            // read before the next trial overwrites them
+            if (sacc) {
+                const int sm = S.s, h = sm / 2 + 1;
+                const double2 *Bn = etab + sm, *Bo = etab + 4 * sm;
+                const int nc = sm * sm * h;
+#pragma unroll 4
+                for (int c = t; c < nc; c += MC_THREADS) {
+                    const int kx = c % h, rr = c / h, ky = rr % sm, kz = rr / sm;
+                    const double2 pn = cmul(cmul(Bn[kx], Bn[sm + ky]), Bn[2 * sm + kz]);
+                    const double2 po = cmul(cmul(Bo[kx], Bo[sm + ky]), Bo[2 * sm + kz]);
+                    double2 F = mcF[S.cgrid_off + c];
+                    F.x += q * (pn.x - po.x);
+                    F.y += q * (pn.y - po.y);
+                    mcF[S.cgrid_off + c] = F;
+                }
+            }
+            __syncthreads();
         }
     }
     if (S.elc && S.recstd && ecur != st2)

@@ -1450,6 +1450,61 @@ static double tab_u(const or_sys *s, int iptjpt, double r2)
  * (:5203-5236, EwaldUpdateArray Src/denergy.F90:1776-1792).  u = [tot, twob(0..natat),
  * rec, bond] from the last UTotal, advanced by every accepted move.  Counts: accepted,
  * hard-core rejects. */
+/* The SPME reciprocal energy of a charge mesh (before the EpsiFourPi scale): r2c transform
+ * and the energyfac sum of UEwaldRecSPM / DUTwoBodyEwaldRecSPM (Src/denergy.F90:1480-1495). */
+static double spm_mesh_energy(const or_sys *s, const double *Q, double *F)
+{
+    const int S = s->s, h = S / 2, hp = S / 2 + 1;
+    double u = 0.0;
+    int nx, ny, nz;
+    or_fft3_r2c(S, Q, F);
+    for (nz = 0; nz <= h; ++nz) {
+        const int nza = (S - nz) % S;
+        for (ny = 0; ny <= h; ++ny) {
+            const int nya = (S - ny) % S;
+            for (nx = 0; nx <= h; ++nx) {
+                const size_t f = (size_t)nx + (size_t)hp * ((size_t)ny + (size_t)hp * nz);
+                const size_t i1 = (size_t)nx + (size_t)hp * ((size_t)ny + (size_t)S * nz);
+                const size_t i2 = (size_t)nx + (size_t)hp * ((size_t)ny + (size_t)S * nza);
+                const size_t i3 = (size_t)nx + (size_t)hp * ((size_t)nya + (size_t)S * nz);
+                const size_t i4 = (size_t)nx + (size_t)hp * ((size_t)nya + (size_t)S * nza);
+                const double Qsum = F[2 * i1] * F[2 * i1] + F[2 * i1 + 1] * F[2 * i1 + 1] +
+                                    F[2 * i2] * F[2 * i2] + F[2 * i2 + 1] * F[2 * i2 + 1] +
+                                    F[2 * i3] * F[2 * i3] + F[2 * i3 + 1] * F[2 * i3 + 1] +
+                                    F[2 * i4] * F[2 * i4] + F[2 * i4 + 1] * F[2 * i4 + 1];
+                u = u + Qsum * s->energyfac[f];
+            }
+        }
+    }
+    return u;
+}
+
+/* q M M M of one particle at r added (sign +1) or removed (-1) on the charge mesh Q
+ * (Src/denergy.F90:1441-1470). */
+static void spm_stencil(const or_sys *s, double *Q, const double r[3], double q, double sign)
+{
+    const int S = s->s, order = s->order;
+    double spline[3][32], deriv[3][32];
+    int32_t km[3];
+    int m, ix, iy, iz;
+    for (m = 0; m < 3; ++m) {
+        or_cardinal_bspline(order, (S / s->boxlen[m]) * r[m], &km[m], spline[m], deriv[m]);
+        km[m] = (km[m] + S) % S;
+    }
+    for (iz = 0; iz < order; ++iz) {
+        const int nz = (S + km[2] - iz) % S;
+        const double qz = q * spline[2][iz];
+        for (iy = 0; iy < order; ++iy) {
+            const int ny = (S + km[1] - iy) % S;
+            const double qyz = qz * spline[1][iy];
+            for (ix = 0; ix < order; ++ix) {
+                const int nx = (S + km[0] - ix) % S;
+                Q[(size_t)nx + S * ((size_t)ny + (size_t)S * nz)] += sign * (qyz * spline[0][ix]);
+            }
+        }
+    }
+}
+
 int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta, double *u,
                int64_t *accepted, int64_t *hsreject)
 {
@@ -1459,15 +1514,24 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
     double *uold = malloc(sizeof(double) * (natat + 1));
     cx *tm[3] = {NULL, NULL, NULL}, *stm = NULL, *yzt = NULL;
     double *trigtm = NULL, *sttm = NULL;     /* layer correction: trial tables and sums */
+    double *qm = NULL, *qmtm = NULL, *fq = NULL, urecold = 0.0, urecnew = 0.0;   /* SPME */
     const size_t w = (size_t)s->ncut + 1;
-    /* SPME has no trial-move difference here */
-    if (s->lewald && s->lewald != 2) { free(dtwob); free(unew); free(uold); return 6; }
+    if (s->lewald == 1) {
+        /* DUTwoBodyEwaldRecSPM: the charge mesh of the configuration and its energy */
+        const size_t n = (size_t)s->s * s->s * s->s;
+        int ia;
+        qm = calloc(n, sizeof(double));
+        qmtm = malloc(sizeof(double) * n);
+        fq = malloc(sizeof(double) * 2 * (size_t)(s->s / 2 + 1) * s->s * s->s);
+        for (ia = 0; ia < np; ++ia) spm_stencil(s, qm, s->ro + 3 * ia, s->az[ia], 1.0);
+        urecold = spm_mesh_energy(s, qm, fq);
+    }
     if (s->lewald == 2) {
         for (k = 0; k < 3; ++k) tm[k] = malloc(sizeof(cx) * w);
         stm = malloc(sizeof(cx) * 4 * (size_t)(s->nkvec > 0 ? s->nkvec : 1));
         yzt = malloc(sizeof(cx) * 2);
     }
-    if (s->elc) {
+    if (s->elc && s->lewald == 2) {
         trigtm = malloc(sizeof(double) * 4 * w);
         sttm = malloc(sizeof(double) * 8 * (size_t)(s->nkvec2d > 0 ? s->nkvec2d : 1));
     }
@@ -1536,6 +1600,36 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
             for (k = 1; k <= natat; ++k) { unew[0] += unew[k]; uold[0] += uold[k]; }
             for (k = 0; k <= natat; ++k) dtwob[k] = unew[k] - uold[k];
             dutot = dutot + dtwob[0];
+            /* DUTwoBodyEwald: SPME reciprocal difference (the whole mesh re-transformed) */
+            if (s->lewald == 1) {
+                const double q = s->az[ip];
+                memcpy(qmtm, qm, sizeof(double) * (size_t)s->s * s->s * s->s);
+                spm_stencil(s, qmtm, s->ro + 3 * ip, q, -1.0);
+                spm_stencil(s, qmtm, rtm, q, 1.0);
+                urecnew = spm_mesh_energy(s, qmtm, fq);
+                durec = urecnew - urecold;
+                if (s->lsurf) {
+                    const double fac = 2.0 * Pi / (3.0 * s->vol);
+                    double sx = 0.0, sy = 0.0, sz = 0.0, tx, ty, tz;
+                    int ia;
+                    for (ia = 0; ia < np; ++ia) {
+                        sx += s->az[ia] * s->ro[3 * ia];
+                        sy += s->az[ia] * s->ro[3 * ia + 1];
+                        sz += s->az[ia] * s->ro[3 * ia + 2];
+                    }
+                    if (s->elc) {
+                        tz = sz + q * (rtm[2] - s->ro[3 * ip + 2]);
+                        durec = durec + (2.0 * Pi / s->vol) * (tz * tz - sz * sz);
+                    } else {
+                        tx = sx + q * (rtm[0] - s->ro[3 * ip]);
+                        ty = sy + q * (rtm[1] - s->ro[3 * ip + 1]);
+                        tz = sz + q * (rtm[2] - s->ro[3 * ip + 2]);
+                        durec = durec + fac * ((tx * tx + ty * ty + tz * tz) - (sx * sx + sy * sy + sz * sz));
+                    }
+                }
+                durec = s->epsfp * durec;
+                dutot = dutot + durec;
+            }
             /* DUTwoBodyEwald: 'std' reciprocal sum and the surface term */
             if (s->lewald == 2) {
                 const int nc = s->ncut, ncut2 = s->ncut2;
@@ -1720,9 +1814,15 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
                 for (m = 0; m < 3; ++m) memcpy((cx *)s->eik[m] + (size_t)ip * w, tm[m], sizeof(cx) * w);
                 memcpy(s->sumeikr, stm, sizeof(cx) * 4 * (size_t)s->nkvec);
             }
-            if (s->elc) {
+            if (s->elc && s->lewald == 2) {
                 memcpy(s->trig2d + (size_t)ip * 4 * w, trigtm, sizeof(double) * 4 * w);
                 memcpy(s->sumtrig, sttm, sizeof(double) * 8 * (size_t)s->nkvec2d);
+            }
+            if (s->lewald == 1) {
+                double *t_ = qm;
+                qm = qmtm;
+                qmtm = t_;
+                urecold = urecnew;
             }
             for (m = 0; m < 3; ++m) {
                 s->ro[3 * ip + m] = rtm[m];
@@ -1732,7 +1832,7 @@ int or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta
     }
     free(dtwob); free(unew); free(uold);
     for (k = 0; k < 3; ++k) free(tm[k]);
-    free(stm); free(yzt); free(trigtm); free(sttm);
+    free(stm); free(yzt); free(trigtm); free(sttm); free(qm); free(qmtm); free(fq);
     return 0;
 }
 

@@ -125,14 +125,6 @@ def test_mixed_handle_runs_the_same_chain():
     assert abs(ed["utot"] - em["utot"]) <= 1e-6 * _scale(ed)
 
 
-def test_spme_is_refused():
-    s = dict(Hp.electrolyte_small())
-    g = Engine(s, Hp.oracle_table(s), precision="fp64")
-    with pytest.raises(MolsimGpuError) as ei:
-        g.MCPass(1, [1.0] * s["npt"], 1.0)
-    assert ei.value.code == 6
-
-
 def test_zero_sweeps_and_bad_arguments():
     """npass = 0 returns the current energies (a UTotal) and moves nothing; an isamp
     other than 0 or 1 and a missing dtran are refused with MSG_ERR_ARG."""
