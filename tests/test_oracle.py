@@ -476,8 +476,12 @@ def test_mc_running_energy_equals_fresh_utotal(which):
     assert np.abs(np.asarray(u["utwob"]) - np.asarray(fresh["utwob"])).max() <= 1e-9 * scale
 
 
-def test_mc_rejects_spme():
+def test_mc_spme_sweep_moves_and_keeps_the_mesh_energy():
+    """The oracle's SPME chain (the mesh re-transformed per trial) accepts moves and its
+    carried u%rec equals a fresh UTotal's."""
     s = dict(Hp.electrolyte_small())
     o, u = _mc_system(s)
-    with pytest.raises(RuntimeError):
-        o.mc_pass(1, [1.0] * s["npt"], 1.0, u)
+    acc, _ = o.mc_pass(1, [1.0] * s["npt"], 1.0, u)
+    assert acc > 0
+    o.set_vlist()
+    assert abs(u["urec"] - o.utotal()["urec"]) <= 1e-9 * (abs(u["urec"]) + 1.0)
