@@ -519,6 +519,49 @@ def run_mc(a):
                                                         "reference's way: the mesh re-transformed per trial), "
                                                         "1 thread"}
     out["spme"] = sp
+    # MCAllPass on the 16000-particle polyelectrolyte: all particles displaced at once per trial
+    # (draws jumped ahead on the device), list rebuild, UTotal, Metropolis
+    pe = S.polyelectrolyte(seed=0)
+    tpe = prepare(pe)
+    ea = Engine(pe, tpe, precision="fp64")
+    ea.mc_seed(1)
+    dta = [0.05] * pe["npt"]
+    ext = torch.cuda.ExternalStream(ea.stream())
+    ea.MCAllPass(2, dta)                               # warm-up
+    torch.cuda.synchronize()
+    ntr = 20
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record(ext)
+    acc, _ = ea.MCAllPass(ntr, dta)
+    en.record(ext)
+    torch.cuda.synchronize()
+    sec = st.elapsed_time(en) / 1000.0
+    ma = {"workload": "polyelectrolyte_16000 (SPME 64^3), MCAll dtranall 0.05 A", "trials": ntr,
+          "value": pe["np"] * ntr / sec, "unit": "particle moves/s", "ms_per_trial": 1000.0 * sec / ntr,
+          "acceptance": float(acc[0]) / ntr}
+    del ea
+    if not a.no_cpu_baseline:
+        qpe = float(np.mean(pe["az"] ** 2))
+        ape = O.rcut_to_alpha(pe["uewaldtol"], qpe, pe["epsi_four_pi"], min(pe["boxlen"]), pe["rcut"])
+        ppe = dict(npt=pe["npt"], zat=pe["zat"], sigat=pe["sigat"], epsat=pe["epsat"], rcut=pe["rcut"],
+                   ualpha=ape, epsi_four_pi=pe["epsi_four_pi"], lewald=1, lljcut=1,
+                   **{k: pe[k] for k in ("ljrcut", "ljushift", "r2uminin", "utoltab", "ftoltab", "umaxtab",
+                                         "fmaxtab", "rumaxfac")})
+        otp = O.pot_tab(ppe)
+        otp["r2atat"] = np.zeros(len(otp["r2umin"]))
+        dpe = dict(pe)
+        dpe["ualpha"] = ape
+        op = O.System(dpe, otp, maxnneigh=512, lcellbuild=True)
+        op.set_state(pe["ro"], pe["rod"])
+        op.set_vlist()
+        upe = op.utotal()
+        op.mc_seed(1)
+        t0 = time.perf_counter()
+        op.mcall_pass(2, dta, 1.0 / S.kT(pe["temp"]), upe)
+        ma["cpu_baseline"] = {"value": pe["np"] * 2 / (time.perf_counter() - t0), "unit": "particle moves/s",
+                              "cores": 1, "kind": "port", "sample": "two MCAll trials of the same system, oracle, "
+                                                                    "1 thread"}
+    out["mcall_16000"] = ma
     return out
 
 

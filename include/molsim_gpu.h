@@ -33,6 +33,7 @@
  *   msg_uewald_sites_spm           -> the same with UEwaldRecSPM (Src/energy.F90:1207-1297)
  *   msg_mc_seed / msg_mc_pass      -> MCDriver iSimulationStep: MCPass with SPartMove
  *                                     (Src/mc.F90:1470-1755), DUTotal, Metropolis, MCUpdate
+ *   msg_mcall_pass                 -> MCAllDriver iSimulationStep: MCAllPass (Src/mc.F90:4024-4178)
  *   msg_bd_step                    -> BDDriver iSimulationStep: BDStep + UTotal
  *                                     (Src/bd.F90:53-59, 120-155) followed by NList
  * Set-up helpers that restate MOLSIM's own set-up for callers without it:
@@ -183,6 +184,27 @@ typedef struct msg_mc_params {
     int32_t isamp;           /* 0: particles in order; 1: a random particle per trial    */
     int32_t pad;
 } msg_mc_params;
+
+/* MCAll parameters of one system (MCAllPass, Src/mc.F90:4024-4178). */
+typedef struct msg_mcall_params {
+    double beta;                    /* MOLSIM's beta */
+    const double *dtranall;         /* [npt] */
+} msg_mcall_params;
+
+/* npass MCAll trials for every system (p[nsys]): all particles displaced at once by
+ * (Random - 1/2) dtranall(ipt) per coordinate, five draws per particle in MOLSIM order
+ * (three displacements and GetRandomTrialOri's two), PBC, the lists rebuilt, one UTotal
+ * of the trial and Metropolis on du%tot; a rejected trial restores the configuration and
+ * its energies.  The chains use the msg_mc_seed streams; the draws are made in parallel
+ * from each particle's place in the stream (the generator jumped ahead), equal to the
+ * sequential ones.  accepted [nsys] (optional); e (optional): energies of system isys. */
+int  msg_mcall_pass(msg_handle *h, int32_t npass, const msg_mcall_params *p, int64_t *accepted, int32_t isys,
+                    msg_energy *e);
+
+/* Random's SAVEd state (ix, iy) after k further draws (Src/mollib.F90:2689-2708), host
+ * only: the xorshift part by powers of its GF(2) matrix, the Park-Miller part by powers of
+ * 16807 mod 2^31 - 1.  MSG_ERR_ARG for iy <= 0. */
+int  msg_random_jump(int32_t ix, int32_t iy, uint32_t k, int32_t out[2]);
 
 /* Random's state of system isys from iseed (its first call, Src/mollib.F90:2689-2708).
  * A system never seeded starts from iseed = isys + 1. */

@@ -46,6 +46,10 @@ class MsgMcParams(C.Structure):
     _fields_ = [("beta", C.c_double), ("dtran", f64p), ("isamp", C.c_int32), ("pad", C.c_int32)]
 
 
+class MsgMcAllParams(C.Structure):
+    _fields_ = [("beta", C.c_double), ("dtranall", f64p)]
+
+
 class MsgSiteEwald(C.Structure):
     _fields_ = [("lewald", C.c_int32), ("order", C.c_int32), ("nmesh", C.c_int32), ("ncut", C.c_int32),
                 ("ncutregion", C.c_int32), ("lsurf", C.c_int32), ("ualpha", C.c_double),
@@ -89,6 +93,9 @@ SIGNATURES = {
     "msg_uewald_sites_spm": (C.c_int, [C.c_int32, f64p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                        f64p, f64p, C.c_int32, i32p, i32p, i32p, C.c_int32, f64p, f64p, f64p,
                                        C.POINTER(C.c_float)]),
+    "msg_mcall_pass": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(MsgMcAllParams), C.POINTER(C.c_int64), C.c_int32,
+                                 C.POINTER(MsgEnergy)]),
+    "msg_random_jump": (C.c_int, [C.c_int32, C.c_int32, C.c_uint32, C.POINTER(C.c_int32)]),
     "msg_mc_pass": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(MsgMcParams), C.POINTER(C.c_int64),
                               C.POINTER(C.c_int64), C.c_int32, C.POINTER(MsgEnergy)]),
     "msg_get_forces": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p]),

@@ -222,6 +222,11 @@ struct msg_handle {
     double *mc_rg = nullptr;
     unsigned long long *mc_ig = nullptr;
     std::vector<cufftHandle> mc_plans;
+    // MCAllPass: jump table of Random, saved positions (MOLSIM order) and energies, decisions
+    McJump *mc_jumpt = nullptr;
+    double4 *mca_psave = nullptr;
+    double *mca_esave = nullptr, *mca_beta = nullptr;
+    int *mca_acc = nullptr;
     int elc_nk = 0;
     // Monte Carlo: Random's state, running energies, counts (accepted, hard-core rejects),
     // sweep parameters, displacement per type, trial structure factors
@@ -420,7 +425,8 @@ static void free_all(msg_handle *h)
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
                     h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
                     h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
-                    h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig};
+                    h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig,
+                    h->mc_jumpt, h->mca_psave, h->mca_esave, h->mca_beta, h->mca_acc};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -2036,6 +2042,40 @@ static int2 mc_seed_state(int32_t iseed)
     return make_int2(777755555 ^ a, (888889999 ^ a) | 1);
 }
 
+// Random's jump table: the xorshift (13, 17, 5) step as a 32x32 bit matrix and its
+// squarings, and 16807^(2^b) mod (2^31 - 1).
+static McJump make_jump_table()
+{
+    McJump J;
+    for (int j = 0; j < 32; ++j) {
+        unsigned v = 1u << j;
+        v ^= v << 13;
+        v ^= v >> 17;
+        v ^= v << 5;
+        J.xs[0][j] = v;
+    }
+    for (int b = 1; b < 32; ++b)
+        for (int j = 0; j < 32; ++j) J.xs[b][j] = mc_xs_apply(J.xs[b - 1], J.xs[b - 1][j]);
+    J.pm[0] = 16807ull;
+    for (int b = 1; b < 32; ++b) J.pm[b] = (J.pm[b - 1] * J.pm[b - 1]) % 2147483647ull;
+    return J;
+}
+
+static const McJump &jump_table()
+{
+    static const McJump J = make_jump_table();
+    return J;
+}
+
+extern "C" int msg_random_jump(int32_t ix, int32_t iy, uint32_t k, int32_t out[2])
+{
+    if (!out || iy <= 0) return MSG_ERR_ARG;
+    const int2 r = mc_jump(jump_table(), make_int2(ix, iy), k);
+    out[0] = r.x;
+    out[1] = r.y;
+    return MSG_OK;
+}
+
 // Monte Carlo buffers, made on first use; an unseeded system starts from iseed = isys + 1.
 void msg_handle::ensure_mc()
 {
@@ -2060,6 +2100,12 @@ void msg_handle::ensure_mc()
             mc_plans.push_back(p);
         }
     }
+    mc_jumpt = dalloc<McJump>(1);
+    up(mc_jumpt, &jump_table(), sizeof(McJump));
+    mca_psave = dalloc<double4>(ntot);
+    mca_esave = dalloc<double>((size_t)nsys * ESZ);
+    mca_beta = dalloc<double>(nsys);
+    mca_acc = dalloc<int>(nsys);
     std::vector<int2> st(nsys);
     for (int s = 0; s < nsys; ++s) st[s] = mc_seed_state(s + 1);
     up(mc_rng, st.data(), nsys * sizeof(int2));
@@ -2437,4 +2483,70 @@ extern "C" int msg_kernel_time(const msg_handle *h, int32_t k, const char **name
     if (total_ms) *total_ms = h->tm_ms[k];
     if (launches) *launches = h->tm_n[k];
     return MSG_OK;
+}
+
+// MCAllPass (Src/mc.F90:4024-4178) for every system of the handle: npass trials, each
+// displacing all particles at once (Random drawn on the device from each chain's place in
+// the stream), rebuilding the lists, one UTotal of the trial, Metropolis on du%tot, and the
+// saved configuration and energies back on rejection.
+extern "C" int msg_mcall_pass(msg_handle *h, int32_t npass, const msg_mcall_params *p, int64_t *accepted,
+                              int32_t isys, msg_energy *e)
+{
+    if (!h || !p || npass < 0 || (e && (isys < 0 || isys >= h->nsys))) return MSG_ERR_ARG;
+    API_BEGIN
+    std::vector<double> dtr(std::max(1, h->type_tot), 0.0), beta(h->nsys);
+    for (int s = 0; s < h->nsys; ++s) {
+        const SysDev &S = h->hs[s];
+        if (!p[s].dtranall) {
+            h->err = "msg_mcall_params needs dtranall[npt]";
+            return MSG_ERR_ARG;
+        }
+        for (int t = 0; t < S.npt; ++t) dtr[S.type_off + t] = p[s].dtranall[t];
+        beta[s] = p[s].beta;
+    }
+    h->ensure_mc();
+    h->up(h->mc_dtr, dtr.data(), dtr.size() * sizeof(double));
+    h->up(h->mca_beta, beta.data(), beta.size() * sizeof(double));
+    CK(cudaMemsetAsync(h->mc_cnt, 0, 2 * sizeof(long long) * h->nsys, h->st));
+    h->enqueue_forces(0, false);                       // the energies of the configuration
+    int rc = h->check();
+    if (rc) return rc;
+    const long long n = h->ntot, nb = std::max<long long>(n, (long long)h->nsys * ESZ);
+    std::vector<int> all(h->placed.begin(), h->placed.end()), accf(h->nsys);
+    for (int pass = 0; pass < npass; ++pass) {
+        k_mcall_save<<<(unsigned)((nb + 255) / 256), 256, 0, h->st>>>(n, h->pos[0], h->inv, h->mca_psave, h->nsys,
+                                                                       h->esys, h->mca_esave);
+        k_mcall_trial<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(h->dsys, n, h->sysid, h->inv, h->typ[0],
+                                                                       h->pos[0], h->mc_rng, h->mc_jumpt, h->mc_dtr);
+        h->launches += 2;
+        rc = h->rebuild_checked(all);
+        if (rc) return rc;
+        h->enqueue_forces(0, false);
+        rc = h->check();
+        if (rc) return rc;
+        k_mcall_decide<<<(h->nsys + 127) / 128, 128, 0, h->st>>>(h->dsys, h->nsys, h->mc_rng, h->mc_jumpt,
+                                                                   h->mca_beta, h->esys, h->mca_esave, h->mca_acc,
+                                                                   h->mc_cnt);
+        k_mcall_restore<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(n, h->sysid, h->inv, h->mca_acc,
+                                                                         h->mca_psave, h->pos[0]);
+        h->launches += 2;
+        CK(cudaMemcpyAsync(accf.data(), h->mca_acc, h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        bool rej = false;
+        for (int s = 0; s < h->nsys; ++s) rej = rej || !accf[s];
+        if (rej) {
+            rc = h->rebuild_checked(all);              // the lists of the restored positions
+            if (rc) return rc;
+        }
+    }
+    std::vector<long long> cnt(2 * (size_t)h->nsys);
+    CK(cudaMemcpyAsync(cnt.data(), h->mc_cnt, cnt.size() * sizeof(long long), cudaMemcpyDeviceToHost, h->st));
+    double he[ESZ];
+    if (e) CK(cudaMemcpyAsync(he, h->esys + (size_t)isys * ESZ, sizeof(he), cudaMemcpyDeviceToHost, h->st));
+    rc = h->check();
+    if (rc) return rc;
+    for (int s = 0; s < h->nsys && accepted; ++s) accepted[s] = cnt[2 * (size_t)s];
+    if (e) fill_energy(he, h->hs[isys].natat, e);
+    return MSG_OK;
+    API_END
 }

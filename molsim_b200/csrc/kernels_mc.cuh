@@ -569,4 +569,113 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     }
 }
 
+// ---------------------------------------------------------------------------
+// MCAllPass (Src/mc.F90:4024-4178): every particle displaced at once, one UTotal of
+// the trial configuration, Metropolis on du%tot.  The reference draws, per particle
+// in order, three displacements and the two numbers of GetRandomTrialOri
+// (Src/mc.F90:4583-4622); here each particle's thread draws its own five from the
+// right place in the stream by jumping the generator ahead: the xorshift part is linear
+// over GF(2) (a 32x32 bit matrix, squared once per bit of the jump), the Park-Miller
+// part multiplicative mod 2^31 - 1 (a power of 16807), so the draws are the sequential
+// ones exactly.
+// ---------------------------------------------------------------------------
+struct McJump {
+    unsigned xs[32][32];            // [b][j]: column j of the xorshift map raised to 2^b
+    unsigned long long pm[32];      // 16807^(2^b) mod (2^31 - 1)
+};
+
+__host__ __device__ inline unsigned mc_xs_apply(const unsigned *col, unsigned v)
+{
+    unsigned r = 0u;
+    for (int j = 0; j < 32; ++j)
+        if ((v >> j) & 1u) r ^= col[j];
+    return r;
+}
+
+// The generator state after k further draws.
+__host__ __device__ inline int2 mc_jump(const McJump &J, int2 st, unsigned k)
+{
+    unsigned x = (unsigned)st.x;
+    unsigned long long y = (unsigned long long)(unsigned)st.y;
+    for (int b = 0; b < 32; ++b)
+        if ((k >> b) & 1u) {
+            x = mc_xs_apply(J.xs[b], x);
+            y = (y * J.pm[b]) % 2147483647ull;
+        }
+    return make_int2((int)x, (int)y);
+}
+
+// Positions of every particle in MOLSIM order into psave, and the energies into esave.
+__global__ void k_mcall_save(long long ntot, const double4 *__restrict__ pos, const int *__restrict__ inv,
+                             double4 *__restrict__ psave, int nsys, const double *__restrict__ esys,
+                             double *__restrict__ esave)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ntot) psave[g] = pos[inv[g]];
+    if (g < (long long)nsys * ESZ) esave[g] = esys[g];
+}
+
+// The trial configuration: particle ip of system s draws Random numbers 5 ip + 1 .. 5 ip + 5
+// of its chain; the first three displace it by (r - 1/2) dtranall(ipt), then PBC
+// (CheckPartBCTM, txbc 'xyz').
+__global__ void k_mcall_trial(const SysDev *__restrict__ sysv, long long ntot, const int *__restrict__ sysid,
+                              const int *__restrict__ inv, const int *__restrict__ typ, double4 *__restrict__ pos,
+                              const int2 *__restrict__ rng, const McJump *__restrict__ J,
+                              const double *__restrict__ dtr)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ntot) return;
+    const int s = sysid[g];
+    const SysDev &S = sysv[s];
+    const int ip = (int)(g - S.off);
+    int2 st = mc_jump(*J, rng[s], 5u * (unsigned)ip);
+    double d[3];
+    for (int m = 0; m < 3; ++m) d[m] = mc_random(st) - 0.5;
+    mc_random(st);                    // GetRandomTrialOri: the axis
+    mc_random(st);                    // and the angle
+    const int i = inv[g];
+    const double dt = dtr[S.type_off + typ[i]];
+    double4 x = pos[i];
+    x.x = pbc_wrap(__dadd_rn(x.x, __dmul_rn(d[0], dt)), S.half[0], S.box[0], S.boxi[0]);
+    x.y = pbc_wrap(__dadd_rn(x.y, __dmul_rn(d[1], dt)), S.half[1], S.box[1], S.boxi[1]);
+    x.z = pbc_wrap(__dadd_rn(x.z, __dmul_rn(d[2], dt)), S.half[2], S.box[2], S.boxi[2]);
+    pos[i] = x;
+}
+
+// Metropolis on du%tot = u%tot(trial) - u%tot(saved) per system, after the chain's 5 np
+// draws (Src/mc.F90:5135-5175); a rejected system gets its saved energies back.
+__global__ void k_mcall_decide(const SysDev *__restrict__ sysv, int nsys, int2 *__restrict__ rng,
+                               const McJump *__restrict__ J, const double *__restrict__ beta,
+                               double *__restrict__ esys, const double *__restrict__ esave,
+                               int *__restrict__ accf, long long *__restrict__ cnt)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    int2 st = mc_jump(*J, rng[s], 5u * (unsigned)sysv[s].n);
+    const double dured = (esys[(size_t)s * ESZ] - esave[(size_t)s * ESZ]) * beta[s];
+    int acc;
+    if (dured > 87.0)
+        acc = 0;
+    else if (dured < -87.0)
+        acc = 1;
+    else {
+        const double fac = exp(-dured);
+        acc = (fac > 1.0) ? 1 : (fac > mc_random(st) ? 1 : 0);
+    }
+    rng[s] = st;
+    accf[s] = acc;
+    cnt[2 * (size_t)s] += acc;
+    if (!acc)
+        for (int k = 0; k < ESZ; ++k) esys[(size_t)s * ESZ + k] = esave[(size_t)s * ESZ + k];
+}
+
+// A rejected system's particles back to their saved positions (MOLSIM order to internal).
+__global__ void k_mcall_restore(long long ntot, const int *__restrict__ sysid, const int *__restrict__ inv,
+                                const int *__restrict__ accf, const double4 *__restrict__ psave,
+                                double4 *__restrict__ pos)
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ntot && !accf[sysid[g]]) pos[inv[g]] = psave[g];
+}
+
 }  // namespace msg

@@ -293,6 +293,27 @@ class Engine:
                                            C.byref(e)))
         return acc, hs, e.as_dict(self.natat[isys])
 
+    def MCAllPass(self, npass=1, dtranall=None, beta=None, isys=0):
+        """npass MCAllPass trials (Src/mc.F90:4024-4178) for every system: all particles displaced
+        at once, UTotal, Metropolis.  dtranall: per-type displacements ([npt], or one list per
+        system); beta as in MCPass.  Returns (accepted[nsys], energies of system isys)."""
+        from ._lib import MsgMcAllParams
+        from .systems import kT
+
+        par = (MsgMcAllParams * self.nsys)()
+        keep = []
+        for k, s in enumerate(self.systems):
+            d = dtranall[k] if dtranall is not None and np.ndim(dtranall) == 2 else dtranall
+            d = np.ascontiguousarray(d if d is not None else [0.1] * s["npt"], np.float64)
+            keep.append(d)
+            b = beta[k] if isinstance(beta, (list, tuple, np.ndarray)) else beta
+            b = float(b) if b is not None else 1.0 / kT(s["temp"])
+            par[k] = MsgMcAllParams(b, _p(d, C.c_double))
+        acc = np.zeros(self.nsys, np.int64)
+        e = MsgEnergy()
+        self._check(_lib.lib().msg_mcall_pass(self.h, int(npass), par, _p(acc, C.c_int64), isys, C.byref(e)))
+        return acc, e.as_dict(self.natat[isys])
+
     def BDStep(self, nsteps=1, seed=0, isys=0, xi=None, return_noise=False, energies=True):
         """nsteps of BDDriver(iSimulationStep) + NList.  xi: caller noise [nsteps][np][3]."""
         n = int(self.systems[isys]["np"])

@@ -52,6 +52,12 @@ module MolsimGpu
       integer(c_int32_t) :: isamp, pad
    end type msg_mc_params
 
+   ! struct msg_mcall_params
+   type, bind(c) :: msg_mcall_params
+      real(c_double)     :: beta
+      type(c_ptr)        :: dtranall              ! c_loc(dtranall(1:npt))
+   end type msg_mcall_params
+
    ! struct msg_site_ewald
    type, bind(c) :: msg_site_ewald
       integer(c_int32_t) :: lewald               ! 1: 'spm', 2: 'std'
@@ -219,6 +225,21 @@ module MolsimGpu
          real(c_double), intent(out) :: urec, virrec
          type(c_ptr), value        :: kernel_ms
       end function msg_uewald_sites_spm
+
+      integer(c_int) function msg_mcall_pass(h, npass, p, accepted, isys, e) bind(c, name='msg_mcall_pass')
+         import :: c_int, c_int32_t, c_ptr, msg_mcall_params
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: npass
+         type(msg_mcall_params), intent(in) :: p(*)
+         type(c_ptr), value        :: accepted, e
+         integer(c_int32_t), value :: isys
+      end function msg_mcall_pass
+
+      integer(c_int) function msg_random_jump(ix, iy, k, out) bind(c, name='msg_random_jump')
+         import :: c_int, c_int32_t
+         integer(c_int32_t), value :: ix, iy, k
+         integer(c_int32_t), intent(out) :: out(2)
+      end function msg_random_jump
 
       integer(c_int) function msg_mc_seed(h, isys, iseed) bind(c, name='msg_mc_seed')
          import :: c_int, c_int32_t, c_ptr

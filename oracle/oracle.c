@@ -2238,3 +2238,51 @@ int or_uewald_sites_spm(int32_t na, const double boxlen[3], double ualpha, int32
     return uewald_sites_impl(1, na, boxlen, ualpha, 0, 0, order, nmesh, lsurf, epsfp, r, az, np, iptpn, ianpn, napt,
                              force, urec, virrec);
 }
+
+/* MCAllPass (Src/mc.F90:4024-4178), monoatomic, txbc 'xyz': per trial every particle in order
+ * draws (Random - 1/2) dtranall(ipt) for x, y, z and the two numbers of GetRandomTrialOri
+ * (Src/mc.F90:4583-4622, the orientation itself unused for points), is wrapped by PBC; the
+ * list is rebuilt and UTotal evaluated; Metropolis on du%tot; rejection restores the
+ * configuration.  u = [tot, twob(0..natat), rec, bond] of the current configuration. */
+int or_mcall_pass(or_sys *s, int npass, const double *dtranall, double beta, double *u, int64_t *accepted)
+{
+    const int np = s->np, nu = s->natat + 4;
+    double *save = malloc(sizeof(double) * 3 * (size_t)np), *unew = malloc(sizeof(double) * (size_t)nu);
+    double *f = malloc(sizeof(double) * 3 * (size_t)np), *fo = malloc(sizeof(double) * 3 * (size_t)np), vir;
+    int pass, ip, m, k, rc = 0;
+    for (pass = 0; pass < npass && !rc; ++pass) {
+        double dured;
+        int accept;
+        memcpy(save, s->ro, sizeof(double) * 3 * (size_t)np);
+        for (ip = 0; ip < np; ++ip) {
+            const double dt = dtranall[s->iptpn[ip] - 1];
+            double d[3];
+            for (m = 0; m < 3; ++m) d[m] = (mc_random(s) - 0.5) * dt;
+            (void)mc_random(s);                  /* GetRandomTrialOri: iaxis */
+            (void)mc_random(s);                  /* and drottemp */
+            for (m = 0; m < 3; ++m)
+                s->ro[3 * ip + m] = pbc1(s->ro[3 * ip + m] + d[m], s->boxlen2[m], s->boxlen[m], s->boxleni[m]);
+        }
+        rc = or_set_vlist(s);
+        if (!rc) rc = or_utotal(s, f, fo, unew, &vir);
+        if (rc) break;
+        dured = (unew[0] - u[0]) * beta;
+        if (dured > 87.0) {
+            accept = 0;
+        } else if (dured < -87.0) {
+            accept = 1;
+        } else {
+            const double fac = exp(-dured);
+            accept = (fac > 1.0) ? 1 : (fac > mc_random(s));
+        }
+        if (accept) {
+            if (accepted) ++*accepted;
+            for (k = 0; k < nu; ++k) u[k] = unew[k];
+        } else {
+            memcpy(s->ro, save, sizeof(double) * 3 * (size_t)np);
+            rc = or_set_vlist(s);
+        }
+    }
+    free(save); free(unew); free(f); free(fo);
+    return rc;
+}

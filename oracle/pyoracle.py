@@ -326,6 +326,23 @@ class System:
         u["ubond"] = uu[3 + self.natat]
         return acc.value, hs.value
 
+    def mcall_pass(self, npass, dtranall, beta, u):
+        """npass MCAll trials (all particles at once); u advanced in place.  Returns accepted."""
+        L = lib()
+        L.or_mcall_pass.restype = C.c_int
+        L.or_mcall_pass.argtypes = [C.c_void_p, C.c_int, f64p, C.c_double, f64p, C.POINTER(C.c_int64)]
+        d = np.ascontiguousarray(dtranall, np.float64)
+        uu = np.concatenate([[u["utot"]], u["utwob"], [u["urec"], u["ubond"]]]).astype(np.float64)
+        acc = C.c_int64(0)
+        rc = L.or_mcall_pass(self.h, int(npass), _p(d, C.c_double), float(beta), _p(uu, C.c_double), C.byref(acc))
+        if rc:
+            raise RuntimeError("MCAll pass failed: %d" % rc)
+        u["utot"] = uu[0]
+        u["utwob"] = uu[1:2 + self.natat].copy()
+        u["urec"] = uu[2 + self.natat]
+        u["ubond"] = uu[3 + self.natat]
+        return acc.value
+
     def set_drosum(self, drosum):
         d = np.ascontiguousarray(drosum, np.float64)
         lib().or_set_drosum(self.h, _p(d, C.c_double))
