@@ -224,7 +224,8 @@ struct msg_handle {
     std::vector<cufftHandle> mc_plans;
     // MCAllPass: jump table of Random, saved positions (MOLSIM order) and energies, decisions
     McJump *mc_jumpt = nullptr;
-    double4 *mca_psave = nullptr;
+    double4 *mca_psave = nullptr, *mca_step = nullptr;
+    int *mca_flag = nullptr;
     double *mca_esave = nullptr, *mca_beta = nullptr;
     int *mca_acc = nullptr;
     int elc_nk = 0;
@@ -426,7 +427,8 @@ static void free_all(msg_handle *h)
                     h->ew_kv, h->ew_kitems, h->ew_tiledone, h->ew_fitems, h->ew_kfac, h->ew_eik, h->ew_part,
                     h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
                     h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig,
-                    h->mc_jumpt, h->mca_psave, h->mca_esave, h->mca_beta, h->mca_acc};
+                    h->mc_jumpt, h->mca_psave, h->mca_esave, h->mca_beta, h->mca_acc, h->mca_step,
+                    h->mca_flag};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -2103,6 +2105,8 @@ void msg_handle::ensure_mc()
     mc_jumpt = dalloc<McJump>(1);
     up(mc_jumpt, &jump_table(), sizeof(McJump));
     mca_psave = dalloc<double4>(ntot);
+    mca_step = dalloc<double4>(ntot);
+    mca_flag = dalloc<int>(nsys);
     mca_esave = dalloc<double>((size_t)nsys * ESZ);
     mca_beta = dalloc<double>(nsys);
     mca_acc = dalloc<int>(nsys);
@@ -2512,32 +2516,37 @@ extern "C" int msg_mcall_pass(msg_handle *h, int32_t npass, const msg_mcall_para
     int rc = h->check();
     if (rc) return rc;
     const long long n = h->ntot, nb = std::max<long long>(n, (long long)h->nsys * ESZ);
-    std::vector<int> all(h->placed.begin(), h->placed.end()), accf(h->nsys);
+    int4 *fx = h->prec == MSG_PREC_MIXED ? h->posfx : nullptr;
+    std::vector<int> flags(h->nsys);
     for (int pass = 0; pass < npass; ++pass) {
         k_mcall_save<<<(unsigned)((nb + 255) / 256), 256, 0, h->st>>>(n, h->pos[0], h->inv, h->mca_psave, h->nsys,
                                                                        h->esys, h->mca_esave);
         k_mcall_trial<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(h->dsys, n, h->sysid, h->inv, h->typ[0],
-                                                                       h->pos[0], h->mc_rng, h->mc_jumpt, h->mc_dtr);
-        h->launches += 2;
-        rc = h->rebuild_checked(all);
-        if (rc) return rc;
+                                                                       h->pos[0], h->mc_rng, h->mc_jumpt, h->mc_dtr,
+                                                                       h->dsum[0], h->mca_step, fx);
+        // NList: a system's lists are rebuilt only when its displacements since the last build
+        // could have brought a pair from beyond rcut + drnlist inside rcut
+        k_mcall_skin<<<h->nsys, 256, 0, h->st>>>(h->dsys, h->dsum[0], h->mca_flag);
+        h->launches += 3;
+        CK(cudaMemcpyAsync(flags.data(), h->mca_flag, h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        bool any = false;
+        for (int s = 0; s < h->nsys; ++s) {
+            flags[s] = flags[s] && h->placed[s];
+            any = any || flags[s];
+        }
+        if (any) {
+            rc = h->rebuild_checked(flags);
+            if (rc) return rc;
+        }
         h->enqueue_forces(0, false);
-        rc = h->check();
-        if (rc) return rc;
         k_mcall_decide<<<(h->nsys + 127) / 128, 128, 0, h->st>>>(h->dsys, h->nsys, h->mc_rng, h->mc_jumpt,
                                                                    h->mca_beta, h->esys, h->mca_esave, h->mca_acc,
                                                                    h->mc_cnt);
-        k_mcall_restore<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(n, h->sysid, h->inv, h->mca_acc,
-                                                                         h->mca_psave, h->pos[0]);
+        k_mcall_restore<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(h->dsys, n, h->sysid, h->inv, h->mca_acc,
+                                                                         h->mca_psave, h->pos[0], h->dsum[0],
+                                                                         h->mca_step, fx);
         h->launches += 2;
-        CK(cudaMemcpyAsync(accf.data(), h->mca_acc, h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-        bool rej = false;
-        for (int s = 0; s < h->nsys; ++s) rej = rej || !accf[s];
-        if (rej) {
-            rc = h->rebuild_checked(all);              // the lists of the restored positions
-            if (rc) return rc;
-        }
     }
     std::vector<long long> cnt(2 * (size_t)h->nsys);
     CK(cudaMemcpyAsync(cnt.data(), h->mc_cnt, cnt.size() * sizeof(long long), cudaMemcpyDeviceToHost, h->st));

@@ -618,10 +618,13 @@ __global__ void k_mcall_save(long long ntot, const double4 *__restrict__ pos, co
 // The trial configuration: particle ip of system s draws Random numbers 5 ip + 1 .. 5 ip + 5
 // of its chain; the first three displace it by (r - 1/2) dtranall(ipt), then PBC
 // (CheckPartBCTM, txbc 'xyz').
+// The step is added to the particle's displacement since the last list build (dsum) and
+// kept in step[g] (MOLSIM order) for a rejection; the fixed-point mirror follows (mixed path).
 __global__ void k_mcall_trial(const SysDev *__restrict__ sysv, long long ntot, const int *__restrict__ sysid,
                               const int *__restrict__ inv, const int *__restrict__ typ, double4 *__restrict__ pos,
                               const int2 *__restrict__ rng, const McJump *__restrict__ J,
-                              const double *__restrict__ dtr)
+                              const double *__restrict__ dtr, double4 *__restrict__ dsum,
+                              double4 *__restrict__ step, int4 *__restrict__ posfx)
 {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ntot) return;
@@ -635,11 +638,60 @@ __global__ void k_mcall_trial(const SysDev *__restrict__ sysv, long long ntot, c
     mc_random(st);                    // and the angle
     const int i = inv[g];
     const double dt = dtr[S.type_off + typ[i]];
+    const double4 dd = make_double4(__dmul_rn(d[0], dt), __dmul_rn(d[1], dt), __dmul_rn(d[2], dt), 0.0);
     double4 x = pos[i];
-    x.x = pbc_wrap(__dadd_rn(x.x, __dmul_rn(d[0], dt)), S.half[0], S.box[0], S.boxi[0]);
-    x.y = pbc_wrap(__dadd_rn(x.y, __dmul_rn(d[1], dt)), S.half[1], S.box[1], S.boxi[1]);
-    x.z = pbc_wrap(__dadd_rn(x.z, __dmul_rn(d[2], dt)), S.half[2], S.box[2], S.boxi[2]);
+    x.x = pbc_wrap(__dadd_rn(x.x, dd.x), S.half[0], S.box[0], S.boxi[0]);
+    x.y = pbc_wrap(__dadd_rn(x.y, dd.y), S.half[1], S.box[1], S.boxi[1]);
+    x.z = pbc_wrap(__dadd_rn(x.z, dd.z), S.half[2], S.box[2], S.boxi[2]);
     pos[i] = x;
+    if (posfx) posfx[i] = fx_pos(x, S);
+    double4 ds = dsum[i];
+    ds.x += dd.x;
+    ds.y += dd.y;
+    ds.z += dd.z;
+    dsum[i] = ds;
+    step[g] = dd;
+}
+
+// NList's decision per system (Src/nlist.F90:600-615) on the displacements since the last
+// build, with the true two largest (never less conservative than the reference's scan):
+// flag[s] = 1 when they sum to more than drnlist.
+__global__ void __launch_bounds__(256) k_mcall_skin(const SysDev *__restrict__ sysv, const double4 *__restrict__ dsum,
+                                                    int *__restrict__ flag)
+{
+    __shared__ double r1[8], r2[8];
+    const SysDev &S = sysv[blockIdx.x];
+    double a1 = 0.0, a2 = 0.0;
+    for (int i = S.off + threadIdx.x; i < S.off + S.n; i += 256) {
+        const double4 d = dsum[i];
+        const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+        if (r > a1) {
+            a2 = a1;
+            a1 = r;
+        } else if (r > a2) {
+            a2 = r;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b1 = __shfl_xor_sync(0xffffffffu, a1, o), b2 = __shfl_xor_sync(0xffffffffu, a2, o);
+        const double m1 = fmax(a1, b1), m2 = fmax(fmin(a1, b1), fmax(a2, b2));
+        a1 = m1;
+        a2 = m2;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        r1[threadIdx.x >> 5] = a1;
+        r2[threadIdx.x >> 5] = a2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m1 = 0.0, m2 = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            const double n1 = fmax(m1, r1[w]), n2 = fmax(fmin(m1, r1[w]), fmax(m2, r2[w]));
+            m1 = n1;
+            m2 = n2;
+        }
+        flag[blockIdx.x] = (m1 + m2 > S.drnlist) ? 1 : 0;
+    }
 }
 
 // Metropolis on du%tot = u%tot(trial) - u%tot(saved) per system, after the chain's 5 np
@@ -669,13 +721,28 @@ __global__ void k_mcall_decide(const SysDev *__restrict__ sysv, int nsys, int2 *
         for (int k = 0; k < ESZ; ++k) esys[(size_t)s * ESZ + k] = esave[(size_t)s * ESZ + k];
 }
 
-// A rejected system's particles back to their saved positions (MOLSIM order to internal).
-__global__ void k_mcall_restore(long long ntot, const int *__restrict__ sysid, const int *__restrict__ inv,
-                                const int *__restrict__ accf, const double4 *__restrict__ psave,
-                                double4 *__restrict__ pos)
+// A rejected system's particles back to their saved positions (MOLSIM order to internal),
+// their steps taken back out of the displacements since the build, the mirror restored.
+__global__ void k_mcall_restore(const SysDev *__restrict__ sysv, long long ntot, const int *__restrict__ sysid,
+                                const int *__restrict__ inv, const int *__restrict__ accf,
+                                const double4 *__restrict__ psave, double4 *__restrict__ pos,
+                                double4 *__restrict__ dsum, const double4 *__restrict__ step,
+                                int4 *__restrict__ posfx)
 {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < ntot && !accf[sysid[g]]) pos[inv[g]] = psave[g];
+    if (g >= ntot) return;
+    const int s = sysid[g];
+    if (accf[s]) return;
+    const int i = inv[g];
+    const double4 x = psave[g];
+    pos[i] = x;
+    if (posfx) posfx[i] = fx_pos(x, sysv[s]);
+    const double4 dd = step[g];
+    double4 ds = dsum[i];
+    ds.x -= dd.x;
+    ds.y -= dd.y;
+    ds.z -= dd.z;
+    dsum[i] = ds;
 }
 
 }  // namespace msg

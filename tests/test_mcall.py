@@ -95,3 +95,23 @@ def test_gpu_systems_in_one_handle_run_their_own_chains():
         a1, _ = one.MCAllPass(5, [0.3] * s["npt"])
         assert int(a1[0]) == int(acc[k])
         assert np.array_equal(one.get_state()["ro"], both.get_state(k)["ro"])
+
+
+@pytest.mark.gpu
+def test_gpu_mixed_handle_makes_the_same_decisions():
+    """The mixed-precision handle (FP32 pair terms over the fixed-point position mirror, which
+    the trial and the restore keep current) accepts the trials the FP64 handle accepts and
+    ends at the same positions; with the list kept across trials by the skin test."""
+    s = dict(Hp.electrolyte_small(lsurf=True))
+    t = Hp.oracle_table(s)
+    out = []
+    for prec in ("fp64", "mixed"):
+        g = Engine(s, t, precision=prec)
+        g.mc_seed(21)
+        acc, e = g.MCAllPass(10, [0.3] * s["npt"])
+        out.append((int(acc[0]), g.get_state()["ro"], e["utot"], g.UTotal()["utot"]))
+    assert out[0][0] == out[1][0] and 0 < out[0][0] < 10
+    assert np.array_equal(out[0][1], out[1][1])
+    for a in out:
+        assert abs(a[2] - a[3]) <= 1e-9 * abs(a[3])      # carried = fresh UTotal
+    assert abs(out[0][2] - out[1][2]) <= 1e-6 * abs(out[0][2])
