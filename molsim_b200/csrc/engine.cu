@@ -2081,8 +2081,20 @@ extern "C" int msg_random_jump(int32_t ix, int32_t iy, uint32_t k, int32_t out[2
 // Monte Carlo buffers, made on first use; an unseeded system starts from iseed = isys + 1.
 void msg_handle::ensure_mc()
 {
-    if (mc_rng) return;
-    mc_rng = dalloc<int2>(nsys);
+    if (mc_rng) return;                // mc_rng is made last: a set-up that failed part-way starts over
+    {
+        void **parts[] = {(void **)&mc_u, (void **)&mc_cnt, (void **)&mc_par, (void **)&mc_dtr, (void **)&ew_sktm,
+                          (void **)&elc_sttm, (void **)&mc_ig, (void **)&mc_rg, (void **)&mc_F, (void **)&mc_jumpt,
+                          (void **)&mca_psave, (void **)&mca_step, (void **)&mca_flag, (void **)&mca_esave,
+                          (void **)&mca_beta, (void **)&mca_acc};
+        for (void **pp : parts)
+            if (*pp) {
+                dfree(*pp);
+                *pp = nullptr;
+            }
+        for (cufftHandle p : mc_plans) cufftDestroy(p);
+        mc_plans.clear();
+    }
     mc_u = dalloc<double>((size_t)nsys * ESZ);
     mc_cnt = dalloc<long long>(2 * (size_t)nsys);
     mc_par = dalloc<McPar>(nsys);
@@ -2112,7 +2124,9 @@ void msg_handle::ensure_mc()
     mca_acc = dalloc<int>(nsys);
     std::vector<int2> st(nsys);
     for (int s = 0; s < nsys; ++s) st[s] = mc_seed_state(s + 1);
-    up(mc_rng, st.data(), nsys * sizeof(int2));
+    int2 *rng = dalloc<int2>(nsys);
+    up(rng, st.data(), nsys * sizeof(int2));
+    mc_rng = rng;
 }
 
 extern "C" int msg_mc_seed(msg_handle *h, int32_t isys, int32_t iseed)
