@@ -2193,9 +2193,11 @@ extern "C" int msg_mc_pass(msg_handle *h, int32_t npass, const msg_mc_params *p,
             need = std::max(need, mc_cache_bytes(h->hs[s].n, h->hs[s].tab_nk, h->hs[s].natat));
         const int cache = (h->nsys <= h->nsm && etab + need <= 200 * 1024) ? 1 : 0;
         const size_t smem = etab + (cache ? need : 0);
+        const int feat = (h->any_spme ? 1 : 0) | (h->elc_nk ? 2 : 0);
+        auto kern = feat == 3 ? k_mc_pass<3> : feat == 2 ? k_mc_pass<2> : feat == 1 ? k_mc_pass<1> : k_mc_pass<0>;
         if (smem > 48 * 1024)
-            CK(cudaFuncSetAttribute(k_mc_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_mc_pass<<<h->nsys, MC_THREADS, smem, h->st>>>(
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<h->nsys, MC_THREADS, smem, h->st>>>(
             h->dsys, h->pos[0], h->typ[0], h->inv, h->ptmap, h->ptab, h->tc, h->bst, h->ew_kv, h->ew_kfac, h->ew_sk,
             h->ew_sktm, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bk, h->beq, h->bpw, h->mc_par, h->mc_dtr,
             h->mc_rng, h->mc_u, h->mc_cnt, npass, cache, wmax, h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm,

@@ -172,6 +172,9 @@ __host__ __device__ inline size_t mc_cache_bytes(int n, int nk, int natat)
     return ((36 * (size_t)n + 15) / 16) * 16 + 96 * (size_t)nk + 2 * (size_t)natat * MSG_NBUCKET;
 }
 
+// FEAT: the features compiled in (1: SPME systems, 2: the 2D layer correction), so that a
+// handle without them runs a kernel without their registers.
+template <int FEAT>
 __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     const SysDev *__restrict__ sysv, double4 *__restrict__ pos, const int *__restrict__ typ,
     const int *__restrict__ inv, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
@@ -194,7 +197,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
     const int sys = blockIdx.x;
     const SysDev &S = sysv[sys];
     const int t = threadIdx.x;
-    const bool spm = S.lewald && !S.recstd;
+    const bool spm = (FEAT & 1) && S.lewald && !S.recstd;
     const int natat = S.natat, w = S.ew_ncut + 1;
     const McPar P = par[sys];
     int2 st = rng[sys];                        // used by thread 0 only
@@ -387,7 +390,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
         // ---- the layer correction's sums of the trial (DUTwoBodyEwaldRec2dlc,
         //      Src/denergy.F90:1339-1409; the old values by the same recurrence as the
         //      tables the reference keeps) ----
-        if (S.elc && S.recstd) {
+        if ((FEAT & 2) && S.elc && S.recstd) {
             const double tpx = tp * S.boxi[0], tpy = tp * S.boxi[1];
             double s1, c1;
             sincos(tpx * rt[0], &s1, &c1);
@@ -553,7 +556,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc_pass(
             __syncthreads();
         }
     }
-    if (S.elc && S.recstd && ecur != st2)
+    if ((FEAT & 2) && S.elc && S.recstd && ecur != st2)
         for (int e = t; e < 8 * S.elc_nkv; e += MC_THREADS) st2[(size_t)8 * S.elc_kv_off + e] = ecur[(size_t)8 * S.elc_kv_off + e];
     // the structure factors end where the last accepted move left them: back into sk
     if (S.recstd && scur != sk)
