@@ -12,7 +12,7 @@
  *
  * Parity status: PARITY UNPINNED against the reference itself.  The
  * reference is Fortran, ships no golden vectors for this path, and no Fortran
- * compiler exists in this build environment, so no output of the compiled
+ * compiler is installed alongside this code, so no output of the compiled
  * reference is available.  These routines are checked instead against the
  * reference's own in-code self checks (CheckUBuffer tolerances, TestCellList
  * completeness, TestEwaldSPM-style SPME-vs-converged checks, standard Ewald)
