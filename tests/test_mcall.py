@@ -115,3 +115,11 @@ def test_gpu_mixed_handle_makes_the_same_decisions():
     for a in out:
         assert abs(a[2] - a[3]) <= 1e-9 * abs(a[3])      # carried = fresh UTotal
     assert abs(out[0][2] - out[1][2]) <= 1e-6 * abs(out[0][2])
+
+
+def test_entry_point_refuses_bad_arguments_on_the_host():
+    """No handle, or no per-system parameters: MSG_ERR_ARG before any device work."""
+    lib = _lib.lib()
+    par = (_lib.MsgMcAllParams * 1)()
+    assert lib.msg_mcall_pass(None, 1, par, None, 0, None) == 6
+    assert lib.msg_mcall_pass(None, 1, None, None, 0, None) == 6

@@ -339,3 +339,22 @@ def test_gpu_rigid_body_spm_steps_match_oracle():
         assert np.abs(np.asarray(sg[key]) - np.asarray(so[key])).max() <= 1e-8 * max(1.0, np.abs(so[key]).max()), key
     assert abs(ug["urec"] - uo["urec"]) <= 1e-10 * _self_scale(s, ew["az"], 0.35)
     assert abs(ug["virial"] - uo["virial"]) <= 1e-8 * abs(uo["virial"])
+
+
+def test_rigid_body_ewald_arguments_are_refused_on_the_host():
+    """msg_velver_p_ewald checks its site Ewald parameters before touching the device: an
+    unknown method, ncut outside 1..100, an SPME order outside 4..8 or an odd mesh."""
+    from molsim_b200.engine import MolsimGpuError
+    from molsim_b200.polyatomic import velver_p
+
+    s = _rigid_charged()
+    t = Hp.site_table(s)
+    az = _site_charges(s)
+    for ew in (dict(az=az, ualpha=0.35, ncut=0), dict(az=az, ualpha=0.35, ncut=101),
+               dict(az=az, ualpha=0.35, order=3, nmesh=32), dict(az=az, ualpha=0.35, order=5, nmesh=33),
+               dict(az=az, ualpha=-1.0, ncut=8)):
+        with pytest.raises(MolsimGpuError) as ei:
+            velver_p(dict(s), t, 1, ewald=ew)
+        assert ei.value.code == 6, ew
+    with pytest.raises(ValueError):
+        velver_p(dict(s), t, 1, ewald=dict(az=az[:-1], ualpha=0.35, ncut=8))
