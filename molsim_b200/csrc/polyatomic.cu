@@ -17,6 +17,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include <cufft.h>
@@ -373,11 +375,89 @@ size_t site_smem(int npt, const int32_t *napt)
     return (size_t)kPWarps * 3 * max_sites(npt, napt) * sizeof(unsigned long long);
 }
 
+// Device memory of the stateless entry points: a per-thread, per-device arena of blocks kept
+// across calls (cudaMalloc and cudaFree per call would dominate a call: cudaFree waits for
+// the whole device).  An entry point's ArenaScope hands everything back when it returns;
+// every entry point ends with a synchronous copy, so nothing in flight still uses it.
+struct Arena {
+    std::vector<std::pair<char *, size_t>> blocks;
+    size_t bi = 0, off = 0;
+    int depth = 0;
+};
+
+Arena &arena()
+{
+    static thread_local std::map<int, Arena> per_device;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return per_device[dev];
+}
+
+template <class T>
+cudaError_t pmalloc(T **p, size_t bytes)
+{
+    Arena &A = arena();
+    bytes = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+    while (A.bi < A.blocks.size()) {
+        if (A.off + bytes <= A.blocks[A.bi].second) {
+            *p = reinterpret_cast<T *>(A.blocks[A.bi].first + A.off);
+            A.off += bytes;
+            return cudaSuccess;
+        }
+        ++A.bi;
+        A.off = 0;
+    }
+    const size_t cap = std::max(bytes, (size_t)64 << 20);
+    char *q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, cap);
+    if (e != cudaSuccess) return e;
+    A.blocks.push_back({q, cap});
+    A.bi = A.blocks.size() - 1;
+    A.off = bytes;
+    *p = reinterpret_cast<T *>(q);
+    return cudaSuccess;
+}
+
+inline void pfree(void *) {}          // arena memory returns with its entry point's scope
+
+struct ArenaScope {
+    ArenaScope() { ++arena().depth; }
+    ~ArenaScope()
+    {
+        Arena &A = arena();
+        if (--A.depth == 0) {
+            A.bi = 0;
+            A.off = 0;
+        }
+    }
+};
+
+// cuFFT plans of the SPME site sum, per thread, device and mesh edge (D2Z, Z2D).
+bool spm_plans(int nmesh, cufftHandle &pf, cufftHandle &pb)
+{
+    static thread_local std::map<std::pair<int, int>, std::pair<cufftHandle, cufftHandle>> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto it = cache.find({dev, nmesh});
+    if (it == cache.end()) {
+        cufftHandle f = 0, b = 0;
+        if (cufftPlan3d(&f, nmesh, nmesh, nmesh, CUFFT_D2Z) != CUFFT_SUCCESS) return false;
+        if (cufftPlan3d(&b, nmesh, nmesh, nmesh, CUFFT_Z2D) != CUFFT_SUCCESS) {
+            cufftDestroy(f);
+            return false;
+        }
+        it = cache.emplace(std::make_pair(dev, nmesh), std::make_pair(f, b)).first;
+    }
+    pf = it->second.first;
+    pb = it->second.second;
+    return true;
+}
+
 template <class T>
 T *dev_copy(const T *h, size_t n, cudaError_t &e)
 {
     T *d = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&d, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaSuccess) e = pmalloc(&d, std::max<size_t>(n, 1) * sizeof(T));
     if (e == cudaSuccess && n) e = cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice);
     return d;
 }
@@ -391,6 +471,7 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
                               const int32_t *iubuflow, const double *r2umin, double *force, double *utwob,
                               double *virial, float *kernel_ms)
 {
+    ArenaScope scope;
     if (np < 1 || na < 1 || npt < 1 || npt > kPMaxType || nat < 1 || maxnneigh < 1 || nbuf < 12 || !boxlen || !ro ||
         !r || !iptpn ||
         !ianpn || !napt || !iatan || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin || !force || !utwob ||
@@ -429,12 +510,12 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
     double *dforce = nullptr, *duv = nullptr;
     int *derr = nullptr;
     const size_t nfix = 3 * (size_t)na + nptpt + 1;
-    if (e == cudaSuccess) e = cudaMalloc(&ffix, nfix * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = pmalloc(&ffix, nfix * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(ffix, 0, nfix * sizeof(unsigned long long));
     ufix = ffix ? ffix + 3 * (size_t)na : nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&duv, (nptpt + 2) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
+    if (e == cudaSuccess) e = pmalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = pmalloc(&duv, (nptpt + 2) * sizeof(double));
+    if (e == cudaSuccess) e = pmalloc(&derr, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
     int herr = 0;
     if (e == cudaSuccess) {
@@ -469,7 +550,7 @@ extern "C" int msg_utwobody_p(int32_t np, int32_t na, int32_t npt, int32_t nat, 
     for (void *p : {(void *)dro, (void *)dr, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat, (void *)dnn,
                     (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)dsb, (void *)dbs, (void *)ffix,
                     (void *)dforce, (void *)duv, (void *)derr})
-        if (p) cudaFree(p);
+        if (p) pfree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return MSG_ERR_CUDA;
@@ -890,8 +971,7 @@ struct SiteEwald {
     unsigned long long *igrid = nullptr;
     double *grid = nullptr, *mfac = nullptr, *emf = nullptr, *vmf = nullptr;
     double2 *cgrid = nullptr;
-    cufftHandle pf = 0, pb = 0;
-    bool plans = false;
+    cufftHandle pf = 0, pb = 0;       // from the per-thread plan cache
 
     static constexpr double kPi = 3.1415926535897932;
 
@@ -918,7 +998,7 @@ struct SiteEwald {
         for (int a = 0; a < na; ++a) q2 += az[a] * az[a];
         cudaError_t e = cudaSuccess;
         daz = dev_copy(az, (size_t)na, e);
-        if (e == cudaSuccess) e = cudaMalloc(&efix, 6 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = pmalloc(&efix, 6 * sizeof(unsigned long long));
         return e == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
     }
 
@@ -962,10 +1042,10 @@ struct SiteEwald {
         cudaError_t e = cudaSuccess;
         dkf = dev_copy(kf.data(), kf.size(), e);
         dkv = dev_copy(kv.data(), kv.size(), e);
-        if (e == cudaSuccess) e = cudaMalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
-        if (e == cudaSuccess) e = cudaMalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
-        if (e == cudaSuccess) e = cudaMalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
-        if (e == cudaSuccess) e = cudaMalloc(&fks, (size_t)nks * 3 * na * sizeof(double));
+        if (e == cudaSuccess) e = pmalloc(&eik, (size_t)na * 3 * w * sizeof(double2));
+        if (e == cudaSuccess) e = pmalloc(&part, (size_t)nchunk * nkv * 4 * sizeof(double2));
+        if (e == cudaSuccess) e = pmalloc(&sk, (size_t)nkv * 4 * sizeof(double2));
+        if (e == cudaSuccess) e = pmalloc(&fks, (size_t)nks * 3 * na * sizeof(double));
         return e == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
     }
 
@@ -990,17 +1070,12 @@ struct SiteEwald {
         mfac = dev_copy(hm.data(), nf, e);
         emf = dev_copy(he.data(), nf, e);
         vmf = dev_copy(hv.data(), nf, e);
-        if (e == cudaSuccess) e = cudaMalloc(&igrid, ng * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = pmalloc(&igrid, ng * sizeof(unsigned long long));
         if (e == cudaSuccess) e = cudaMemset(igrid, 0, ng * sizeof(unsigned long long));
-        if (e == cudaSuccess) e = cudaMalloc(&grid, ng * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&cgrid, nc * sizeof(double2));
+        if (e == cudaSuccess) e = pmalloc(&grid, ng * sizeof(double));
+        if (e == cudaSuccess) e = pmalloc(&cgrid, nc * sizeof(double2));
         if (e != cudaSuccess) return MSG_ERR_CUDA;
-        if (cufftPlan3d(&pf, nmesh, nmesh, nmesh, CUFFT_D2Z) != CUFFT_SUCCESS) return MSG_ERR_CUDA;
-        if (cufftPlan3d(&pb, nmesh, nmesh, nmesh, CUFFT_Z2D) != CUFFT_SUCCESS) {
-            cufftDestroy(pf);
-            return MSG_ERR_CUDA;
-        }
-        plans = true;
+        if (!spm_plans(nmesh, pf, pb)) return MSG_ERR_CUDA;
         return MSG_OK;
     }
 
@@ -1073,14 +1148,10 @@ struct SiteEwald {
 
     ~SiteEwald()
     {
-        if (plans) {
-            cufftDestroy(pf);
-            cufftDestroy(pb);
-        }
         for (void *p : {(void *)daz, (void *)efix, (void *)dkf, (void *)dkv, (void *)eik, (void *)part, (void *)sk,
                         (void *)fks, (void *)igrid, (void *)grid, (void *)cgrid, (void *)mfac, (void *)emf,
                         (void *)vmf})
-            if (p) cudaFree(p);
+            if (p) pfree(p);
     }
 };
 
@@ -1094,7 +1165,7 @@ static int uewald_sites_call(const SiteEwald &E, int32_t na, const double *r, in
     cudaError_t e = cudaSuccess;
     double *dr = dev_copy(r, 3 * (size_t)na, e), *dforce = nullptr;
     int *dipt = dev_copy(iptpn, (size_t)np, e), *dian = dev_copy(ianpn, (size_t)np, e), *dnapt = dev_copy(napt, (size_t)npt, e);
-    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = pmalloc(&dforce, 3 * (size_t)na * sizeof(double));
     if (e == cudaSuccess) {
         cudaEvent_t a = nullptr, b = nullptr;
         if (kernel_ms) {
@@ -1115,7 +1186,7 @@ static int uewald_sites_call(const SiteEwald &E, int32_t na, const double *r, in
         if (e == cudaSuccess) e = E.energies(*urec, *virrec);
     }
     for (void *p : {(void *)dr, (void *)dipt, (void *)dian, (void *)dnapt, (void *)dforce})
-        if (p) cudaFree(p);
+        if (p) pfree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return MSG_ERR_CUDA;
@@ -1128,6 +1199,7 @@ extern "C" int msg_uewald_sites(int32_t na, const double boxlen[3], double ualph
                                 const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
                                 double *force, double *urec, double *virrec, float *kernel_ms)
 {
+    ArenaScope scope;
     if (!r || !force || !urec || !virrec) return MSG_ERR_ARG;
     SiteEwald E;
     const int rc = E.setup(na, boxlen, ualpha, ncut, ncutregion, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
@@ -1143,6 +1215,7 @@ extern "C" int msg_uewald_sites_spm(int32_t na, const double boxlen[3], double u
                                     const int32_t *iptpn, const int32_t *ianpn, const int32_t *napt, int32_t npt,
                                     double *force, double *urec, double *virrec, float *kernel_ms)
 {
+    ArenaScope scope;
     if (!r || !force || !urec || !virrec) return MSG_ERR_ARG;
     SiteEwald E;
     const int rc = E.setup_spm(na, boxlen, ualpha, order, nmesh, lsurf, epsfp, az, np, iptpn, ianpn, napt, npt);
@@ -1227,11 +1300,11 @@ static int velver_p_run(const SiteEwald *ew, double *urec, int32_t nsteps, int32
     double *dforce = nullptr, *duv = nullptr, *dori = nullptr;
     int *derr = nullptr;
     const size_t nfix = 3 * (size_t)na + nptpt + 2;           // site forces, energies, pair and molecular virial
-    if (e == cudaSuccess) e = cudaMalloc(&ffix, nfix * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&dforce, 3 * (size_t)na * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&duv, (nptpt + 2) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&dori, 9 * (size_t)np * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
+    if (e == cudaSuccess) e = pmalloc(&ffix, nfix * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = pmalloc(&dforce, 3 * (size_t)na * sizeof(double));
+    if (e == cudaSuccess) e = pmalloc(&duv, (nptpt + 2) * sizeof(double));
+    if (e == cudaSuccess) e = pmalloc(&dori, 9 * (size_t)np * sizeof(double));
+    if (e == cudaSuccess) e = pmalloc(&derr, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
     int herr = 0;
     double vmol = 0.0;
@@ -1289,7 +1362,7 @@ static int velver_p_run(const SiteEwald *ew, double *urec, int32_t nsteps, int32
                     (void *)dra, (void *)dmass, (void *)dmom, (void *)dipt, (void *)dian, (void *)dnapt, (void *)diat,
                     (void *)dnn, (void *)djp, (void *)dub, (void *)dr2, (void *)diub, (void *)dsb, (void *)dbs,
                     (void *)ffix, (void *)dforce, (void *)duv, (void *)dori, (void *)derr})
-        if (p) cudaFree(p);
+        if (p) pfree(p);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return MSG_ERR_CUDA;
@@ -1308,6 +1381,7 @@ extern "C" int msg_velver_p(int32_t nsteps, int32_t np, int32_t na, int32_t npt,
                             const int32_t *iubuflow, const double *r2umin, double *utwob, double *virial,
                             float *kernel_ms)
 {
+    ArenaScope scope;
     return velver_p_run(nullptr, nullptr, nsteps, np, na, npt, nat, boxlen, rcut, tstep, nvvite, tvvite, ro, rod, rodd,
                         qua, quad, quadd, r, iptpn, ianpn, napt, iatan, ra, maxsite, masspt, momp, nneighpn, jpnlist,
                         maxnneigh, ubuf, nbuf, iubuflow, r2umin, utwob, virial, kernel_ms);
@@ -1323,6 +1397,7 @@ extern "C" int msg_velver_p_ewald(int32_t nsteps, int32_t np, int32_t na, int32_
                                   const double *r2umin, const msg_site_ewald *ew, double *utwob, double *urec,
                                   double *virial, float *kernel_ms)
 {
+    ArenaScope scope;
     if (!urec || !ew || (ew->lewald != 1 && ew->lewald != 2)) return MSG_ERR_ARG;
     SiteEwald E;
     const int rc = ew->lewald == 2
