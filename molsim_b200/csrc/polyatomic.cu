@@ -726,7 +726,19 @@ __global__ void __launch_bounds__(kSF) k_site_force(int na, int nkv, int klen, d
             for (int c = 0; c < 4; ++c) ssk[e][c] = sk[g * 4 + c];
         }
         __syncthreads();
-        for (int e = 0; e < nt; ++e) {
+        // one k-vector's terms, added to the site's force in k order
+        auto term = [&](int e, double2 exv, double &gx, double &gy, double &gz) {
+            const double2 qx = make_double2(q * exv.x, q * exv.y), qxc = zconj(qx);
+            const double2 r0 = zmul(qxc, yzm), r1 = zmul(qxc, yzp), r2 = zmul(qx, yzm), r3 = zmul(qx, yzp);
+            const double2 s0 = ssk[e][0], s1 = ssk[e][1], s2 = ssk[e][2], s3 = ssk[e][3];
+            const double fmm = -r0.x * s0.y + r0.y * s0.x, fmp = -r1.x * s1.y + r1.y * s1.x;
+            const double fpm = -r2.x * s2.y + r2.y * s2.x, fpp = -r3.x * s3.y + r3.y * s3.x;
+            const double3 K = skk[e];
+            gx = K.x * (-fmm - fmp + fpm + fpp);
+            gy = K.y * (-fmm + fmp - fpm + fpp);
+            gz = K.z * (fmm + fmp + fpm + fpp);
+        };
+        for (int e = 0; e < nt;) {
             const int4 n = skv[e];
             const int key = n.z * (kSMaxCut + 1) + n.y;
             if (key != row) {
@@ -743,15 +755,30 @@ __global__ void __launch_bounds__(kSF) k_site_force(int na, int nkv, int klen, d
                 row = key;
             }
             while (cx < n.x) { ex = (cx == 0) ? e1[0] : zmul(ex, e1[0]); ++cx; }
-            const double2 qx = make_double2(q * ex.x, q * ex.y), qxc = zconj(qx);
-            const double2 r0 = zmul(qxc, yzm), r1 = zmul(qxc, yzp), r2 = zmul(qx, yzm), r3 = zmul(qx, yzp);
-            const double2 s0 = ssk[e][0], s1 = ssk[e][1], s2 = ssk[e][2], s3 = ssk[e][3];
-            const double fmm = -r0.x * s0.y + r0.y * s0.x, fmp = -r1.x * s1.y + r1.y * s1.x;
-            const double fpm = -r2.x * s2.y + r2.y * s2.x, fpp = -r3.x * s3.y + r3.y * s3.x;
-            const double3 K = skk[e];
-            fx += K.x * (-fmm - fmp + fpm + fpp);
-            fy += K.y * (-fmm + fmp - fpm + fpp);
-            fz += K.z * (fmm + fmp + fpm + fpp);
+            // two k-vectors at a time when the next one is the same row's next nx (the common
+            // case): their terms are independent work for the scheduler; the sums keep k order
+            if (e + 1 < nt && skv[e + 1].x == n.x + 1 && skv[e + 1].y == n.y && skv[e + 1].z == n.z) {
+                const double2 ex2 = (cx == 0) ? e1[0] : zmul(ex, e1[0]);
+                double ax, ay, az_, bx, by, bz;
+                term(e, ex, ax, ay, az_);
+                term(e + 1, ex2, bx, by, bz);
+                fx += ax;
+                fy += ay;
+                fz += az_;
+                fx += bx;
+                fy += by;
+                fz += bz;
+                ex = ex2;
+                ++cx;
+                e += 2;
+            } else {
+                double ax, ay, az_;
+                term(e, ex, ax, ay, az_);
+                fx += ax;
+                fy += ay;
+                fz += az_;
+                ++e;
+            }
         }
     }
     if (on) {
