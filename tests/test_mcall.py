@@ -123,3 +123,20 @@ def test_entry_point_refuses_bad_arguments_on_the_host():
     par = (_lib.MsgMcAllParams * 1)()
     assert lib.msg_mcall_pass(None, 1, par, None, 0, None) == 6
     assert lib.msg_mcall_pass(None, 1, None, None, 0, None) == 6
+
+
+def test_random_jump_composes():
+    """Jumping k1 then k2 draws equals jumping k1 + k2, jumping 0 changes nothing, and a jump
+    across 2^31 draws stays consistent (the Park-Miller part has period 2^31 - 2)."""
+    rng = np.random.default_rng(5)
+    st = (C.c_int32 * 2)()
+    O.lib().or_random_init(-77, st)
+    s0 = (int(st[0]), int(st[1]))
+    assert _jump(s0, 0) == s0
+    for _ in range(50):
+        k1, k2 = (int(x) for x in rng.integers(0, 2 ** 31, 2))
+        assert _jump(_jump(s0, k1), k2) == _jump(_jump(s0, k2), k1)
+        if k1 + k2 < 2 ** 32:
+            assert _jump(_jump(s0, k1), k2) == _jump(s0, k1 + k2)
+    # the Park-Miller part returns after its period 2^31 - 2
+    assert _jump(s0, 2 ** 31 - 2)[1] == s0[1]
