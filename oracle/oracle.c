@@ -2286,3 +2286,341 @@ int or_mcall_pass(or_sys *s, int npass, const double *dtranall, double beta, dou
     free(save); free(unew); free(f); free(fo);
     return rc;
 }
+
+/* MCPass with single-particle and chain moves: CallMove's selection (Src/mc.F90:669-708;
+ * MCPass :1470-1582), SPartMove and ChainMove (:2541-2636), GetRandomTrialPos (:4527-4580):
+ * a type with pspart >= 1 - 1e-15 makes single-particle moves only; otherwise Random picks
+ * a single-particle move below pspart and a chain move below pchain (MOLSIM's cumulative
+ * probabilities, [npt]).  A chain move translates the whole chain of the chosen particle by
+ * one displacement of dtranchain(ipt).  Chains: nchain contiguous ranges (chain_first
+ * 0-based, chain_len).  DUTotal over the moved set: pair differences between moved and fixed
+ * particles (pairs inside the set are unchanged, Src/denergy.F90:728-800), the reciprocal
+ * difference (standard Ewald with the layer correction, or SPME re-transformed), the surface
+ * term, and every bond with a moved end.  u as in or_mc_pass.  Returns 6 for a move type
+ * outside these two or a chain move of a particle in no chain. */
+int or_mc_pass_moves(or_sys *s, int npass, int isamp, const double *dtran, const double *pspart,
+                     const double *pchain, const double *dtranchain, int nchain, const int32_t *chain_first,
+                     const int32_t *chain_len, double beta, double *u, int64_t *accepted, int64_t *hsreject)
+{
+    const int np = s->np, natat = s->natat, nc = s->ncut;
+    const size_t w = (size_t)nc + 1;
+    int *moved = calloc((size_t)np, sizeof(int)), *mv = malloc(sizeof(int) * (size_t)np);
+    double *rtm = malloc(sizeof(double) * 3 * (size_t)np);
+    double *dtwob = malloc(sizeof(double) * (natat + 1)), *unew = malloc(sizeof(double) * (natat + 1));
+    double *uold = malloc(sizeof(double) * (natat + 1));
+    cx *tm = NULL, *stm = NULL;                      /* standard Ewald: [nmv][3][w], trial sums */
+    double *trigtm = NULL, *sttm = NULL;             /* layer correction */
+    double *qm = NULL, *qmtm = NULL, *fq = NULL, urecold = 0.0, urecnew = 0.0;   /* SPME */
+    int pass, ipass, k, m, rc = 0;
+    if (s->lewald == 2) {
+        tm = malloc(sizeof(cx) * 3 * w * (size_t)np);
+        stm = malloc(sizeof(cx) * 4 * (size_t)(s->nkvec > 0 ? s->nkvec : 1));
+        if (s->elc) {
+            trigtm = malloc(sizeof(double) * 4 * w * (size_t)np);
+            sttm = malloc(sizeof(double) * 8 * (size_t)(s->nkvec2d > 0 ? s->nkvec2d : 1));
+        }
+    } else if (s->lewald == 1) {
+        const size_t n = (size_t)s->s * s->s * s->s;
+        int ia;
+        qm = calloc(n, sizeof(double));
+        qmtm = malloc(sizeof(double) * n);
+        fq = malloc(sizeof(double) * 2 * (size_t)(s->s / 2 + 1) * s->s * s->s);
+        for (ia = 0; ia < np; ++ia) spm_stencil(s, qm, s->ro + 3 * ia, s->az[ia], 1.0);
+        urecold = spm_mesh_energy(s, qm, fq);
+    }
+    for (pass = 0; pass < npass && !rc; ++pass) {
+        for (ipass = 0; ipass < np && !rc; ++ipass) {
+            int ip, ipt, nmv = 0, chain = 0, overlap = 0, a;
+            double dtr, d[3], dutot = 0.0, durec = 0.0, dubond = 0.0, dured;
+            ip = (isamp == 0) ? ipass + 1 : 1 + (int)(np * mc_random(s));
+            ip = (ip < 1 ? 1 : (ip > np ? np : ip)) - 1;
+            ipt = s->iptpn[ip] - 1;
+            if (!(pspart[ipt] > 1.0 - 1e-15)) {
+                const double pr = mc_random(s);
+                if (pr < pspart[ipt]) chain = 0;
+                else if (pr < pchain[ipt]) chain = 1;
+                else { rc = 6; break; }
+            }
+            if (chain) {
+                int c, found = -1;
+                for (c = 0; c < nchain; ++c)
+                    if (ip >= chain_first[c] && ip < chain_first[c] + chain_len[c]) found = c;
+                if (found < 0) { rc = 6; break; }
+                for (a = 0; a < chain_len[found]; ++a) mv[nmv++] = chain_first[found] + a;
+                dtr = dtranchain[ipt];
+            } else {
+                mv[nmv++] = ip;
+                dtr = dtran[ipt];
+            }
+            /* GetRandomTrialPos: one displacement for the moved set */
+            if (dtr >= 0.0) {
+                for (m = 0; m < 3; ++m) d[m] = (mc_random(s) - 0.5) * dtr;
+            } else {
+                for (;;) {
+                    for (m = 0; m < 3; ++m) d[m] = mc_random(s) - 0.5;
+                    if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < 0.25) break;
+                }
+                for (m = 0; m < 3; ++m) d[m] = d[m] * fabs(dtr);
+            }
+            for (a = 0; a < nmv; ++a) {
+                const int i = mv[a];
+                moved[i] = 1;
+                for (m = 0; m < 3; ++m)
+                    rtm[3 * a + m] = pbc1(s->ro[3 * i + m] + d[m], s->boxlen2[m], s->boxlen[m], s->boxleni[m]);
+            }
+            /* DUTwoBody: moved against fixed particles; the new configuration first, with its checks */
+            for (k = 0; k <= natat; ++k) unew[k] = uold[k] = 0.0;
+            for (a = 0; a < nmv && !overlap; ++a) {
+                const int i = mv[a], it = s->iptpn[i];
+                int jp;
+                for (jp = 0; jp < np; ++jp) {
+                    double dx, dy, dz, r2;
+                    int ij;
+                    if (moved[jp]) continue;
+                    dx = rtm[3 * a] - s->ro[3 * jp];
+                    dy = rtm[3 * a + 1] - s->ro[3 * jp + 1];
+                    dz = rtm[3 * a + 2] - s->ro[3 * jp + 2];
+                    r2 = pbcr2(s, &dx, &dy, &dz);
+                    if (!(r2 < s->rcut2)) continue;
+                    ij = pair_index(s->npt, it, s->iptpn[jp]);
+                    if (r2 < s->r2atat[ij - 1] || r2 < s->r2umin[ij - 1]) { overlap = 1; break; }
+                    unew[ij] += tab_u(s, ij - 1, r2);
+                }
+            }
+            if (overlap) {
+                if (hsreject) ++*hsreject;
+                for (a = 0; a < nmv; ++a) moved[mv[a]] = 0;
+                continue;                            /* Metropolis: imchsreject, no random number */
+            }
+            for (a = 0; a < nmv; ++a) {
+                const int i = mv[a], it = s->iptpn[i];
+                int jp;
+                for (jp = 0; jp < np; ++jp) {
+                    double dx, dy, dz, r2;
+                    int ij;
+                    if (moved[jp]) continue;
+                    dx = s->ro[3 * i] - s->ro[3 * jp];
+                    dy = s->ro[3 * i + 1] - s->ro[3 * jp + 1];
+                    dz = s->ro[3 * i + 2] - s->ro[3 * jp + 2];
+                    r2 = pbcr2(s, &dx, &dy, &dz);
+                    if (!(r2 < s->rcut2)) continue;
+                    ij = pair_index(s->npt, it, s->iptpn[jp]);
+                    uold[ij] += tab_u(s, ij - 1, r2);
+                }
+            }
+            for (k = 1; k <= natat; ++k) { unew[0] += unew[k]; uold[0] += uold[k]; }
+            for (k = 0; k <= natat; ++k) dtwob[k] = unew[k] - uold[k];
+            dutot = dtwob[0];
+            /* DUTwoBodyEwald */
+            if (s->lewald == 2) {
+                const int ncut2 = s->ncut2;
+                const cx *S4 = (const cx *)s->sumeikr;
+                double tpbi[3];
+                int nx, ny, nz, kn = 0, icut;
+                for (m = 0; m < 3; ++m) tpbi[m] = 2.0 * Pi * s->boxleni[m];
+                for (a = 0; a < nmv; ++a)                /* EwaldSetArrayTM per moved particle */
+                    for (m = 0; m < 3; ++m) {
+                        cx *t = tm + ((size_t)a * 3 + m) * w;
+                        t[0].r = 1.0; t[0].i = 0.0;
+                        if (nc >= 1) {
+                            t[1].r = cos(tpbi[m] * rtm[3 * a + m]);
+                            t[1].i = sin(tpbi[m] * rtm[3 * a + m]);
+                        }
+                        for (icut = 2; icut <= nc; ++icut) t[icut] = cmul(t[icut - 1], t[1]);
+                    }
+                for (nz = 0; nz <= nc; ++nz)
+                    for (ny = 0; ny <= nc; ++ny) {
+                        if (ny * ny + nz * nz > ncut2) continue;
+                        for (nx = 0; nx <= nc; ++nx) {
+                            cx *st = stm + 4 * (size_t)kn;
+                            const cx *so = S4 + 4 * (size_t)kn;
+                            double termnew, termold;
+                            if (nx * nx + ny * ny + nz * nz > ncut2) continue;
+                            if (nx == 0 && ny == 0 && nz == 0) continue;
+                            for (k = 0; k < 4; ++k) st[k] = so[k];
+                            for (a = 0; a < nmv; ++a) {
+                                const int i = mv[a];
+                                const double q = s->az[i];
+                                const cx *ex = (const cx *)s->eik[0] + (size_t)i * w;
+                                const cx *ey = (const cx *)s->eik[1] + (size_t)i * w;
+                                const cx *ez = (const cx *)s->eik[2] + (size_t)i * w;
+                                const cx *tx = tm + ((size_t)a * 3) * w, *ty = tx + w, *tz = tx + 2 * w;
+                                cx yc, yct, yzm, yzp, yzmt, yzpt, xo = ex[nx], xt = tx[nx], xoc, xtc, p, o;
+                                yc.r = ey[ny].r; yc.i = -ey[ny].i;
+                                yzm = cmul(yc, ez[nz]);
+                                yzp = cmul(ey[ny], ez[nz]);
+                                yct.r = ty[ny].r; yct.i = -ty[ny].i;
+                                yzmt = cmul(yct, tz[nz]);
+                                yzpt = cmul(ty[ny], tz[nz]);
+                                xoc.r = xo.r; xoc.i = -xo.i;
+                                xtc.r = xt.r; xtc.i = -xt.i;
+                                p = cmul(xtc, yzmt); o = cmul(xoc, yzm);
+                                st[0].r += q * (p.r - o.r); st[0].i += q * (p.i - o.i);
+                                p = cmul(xtc, yzpt); o = cmul(xoc, yzp);
+                                st[1].r += q * (p.r - o.r); st[1].i += q * (p.i - o.i);
+                                p = cmul(xt, yzmt); o = cmul(xo, yzm);
+                                st[2].r += q * (p.r - o.r); st[2].i += q * (p.i - o.i);
+                                p = cmul(xt, yzpt); o = cmul(xo, yzp);
+                                st[3].r += q * (p.r - o.r); st[3].i += q * (p.i - o.i);
+                            }
+                            termnew = termold = 0.0;
+                            for (k = 0; k < 4; ++k) {
+                                termnew += st[k].r * st[k].r + st[k].i * st[k].i;
+                                termold += so[k].r * so[k].r + so[k].i * so[k].i;
+                            }
+                            durec += s->kfac[kn] * (termnew - termold);
+                            ++kn;
+                        }
+                    }
+                if (s->elc) {                            /* DUTwoBodyEwaldRec2dlc over the moved set */
+                    for (a = 0; a < nmv; ++a) {
+                        double *t = trigtm + (size_t)a * 4 * w;
+                        for (m = 0; m < 4; ++m) t[m * w] = 1.0;
+                        if (nc >= 1) {
+                            t[1] = sin(tpbi[0] * rtm[3 * a]);
+                            t[w + 1] = cos(tpbi[0] * rtm[3 * a]);
+                            t[2 * w + 1] = sin(tpbi[1] * rtm[3 * a + 1]);
+                            t[3 * w + 1] = cos(tpbi[1] * rtm[3 * a + 1]);
+                        }
+                        for (icut = 2; icut <= nc; ++icut) {
+                            t[icut] = t[icut - 1] * t[w + 1] + t[w + icut - 1] * t[1];
+                            t[w + icut] = t[w + icut - 1] * t[w + 1] - t[icut - 1] * t[1];
+                            t[2 * w + icut] = t[2 * w + icut - 1] * t[3 * w + 1] + t[3 * w + icut - 1] * t[2 * w + 1];
+                            t[3 * w + icut] = t[3 * w + icut - 1] * t[3 * w + 1] - t[2 * w + icut - 1] * t[2 * w + 1];
+                        }
+                    }
+                    kn = 0;
+                    for (ny = 0; ny <= nc; ++ny)
+                        for (nx = 0; nx <= nc; ++nx) {
+                            const double kx = nx * tpbi[0], ky = ny * tpbi[1];
+                            double kp, tn, to_, *st = sttm + 8 * (size_t)kn;
+                            const double *so = s->sumtrig + 8 * (size_t)kn;
+                            if (nx * nx + ny * ny > s->ncut2d2) continue;
+                            if (nx == 0 && ny == 0) continue;
+                            kp = sqrt(kx * kx + ky * ky);
+                            for (k = 0; k < 8; ++k) st[k] = so[k];
+                            for (a = 0; a < nmv; ++a) {
+                                const int i = mv[a];
+                                const double q = s->az[i], *tt = trigtm + (size_t)a * 4 * w;
+                                const double *to = s->trig2d + (size_t)i * 4 * w;
+                                double e = exp(kp * rtm[3 * a + 2]), ei = 1.0 / e;
+                                const double sht = 0.5 * (e - ei), cht = 0.5 * (e + ei);
+                                double sho, cho;
+                                e = exp(kp * s->ro[3 * i + 2]); ei = 1.0 / e;
+                                sho = 0.5 * (e - ei); cho = 0.5 * (e + ei);
+                                st[0] += q * (tt[nx] * tt[2 * w + ny] * sht - to[nx] * to[2 * w + ny] * sho);
+                                st[1] += q * (tt[w + nx] * tt[2 * w + ny] * sht - to[w + nx] * to[2 * w + ny] * sho);
+                                st[2] += q * (tt[nx] * tt[3 * w + ny] * sht - to[nx] * to[3 * w + ny] * sho);
+                                st[3] += q * (tt[w + nx] * tt[3 * w + ny] * sht - to[w + nx] * to[3 * w + ny] * sho);
+                                st[4] += q * (tt[nx] * tt[2 * w + ny] * cht - to[nx] * to[2 * w + ny] * cho);
+                                st[5] += q * (tt[w + nx] * tt[2 * w + ny] * cht - to[w + nx] * to[2 * w + ny] * cho);
+                                st[6] += q * (tt[nx] * tt[3 * w + ny] * cht - to[nx] * to[3 * w + ny] * cho);
+                                st[7] += q * (tt[w + nx] * tt[3 * w + ny] * cht - to[w + nx] * to[3 * w + ny] * cho);
+                            }
+                            tn = -st[0] * st[0] - st[1] * st[1] - st[2] * st[2] - st[3] * st[3] +
+                                 st[4] * st[4] + st[5] * st[5] + st[6] * st[6] + st[7] * st[7];
+                            to_ = -so[0] * so[0] - so[1] * so[1] - so[2] * so[2] - so[3] * so[3] +
+                                  so[4] * so[4] + so[5] * so[5] + so[6] * so[6] + so[7] * so[7];
+                            durec += s->kfac2d[kn] * (tn - to_);
+                            ++kn;
+                        }
+                }
+            } else if (s->lewald == 1) {
+                memcpy(qmtm, qm, sizeof(double) * (size_t)s->s * s->s * s->s);
+                for (a = 0; a < nmv; ++a) {
+                    spm_stencil(s, qmtm, s->ro + 3 * mv[a], s->az[mv[a]], -1.0);
+                    spm_stencil(s, qmtm, rtm + 3 * a, s->az[mv[a]], 1.0);
+                }
+                urecnew = spm_mesh_energy(s, qmtm, fq);
+                durec = urecnew - urecold;
+            }
+            if (s->lewald) {
+                if (s->lsurf) {                          /* DUTwoBodyEwaldSurf */
+                    double M[3] = {0.0, 0.0, 0.0}, T[3];
+                    int ia;
+                    for (ia = 0; ia < np; ++ia)
+                        for (m = 0; m < 3; ++m) M[m] += s->az[ia] * s->ro[3 * ia + m];
+                    for (m = 0; m < 3; ++m) {
+                        T[m] = M[m];
+                        for (a = 0; a < nmv; ++a) T[m] += s->az[mv[a]] * (rtm[3 * a + m] - s->ro[3 * mv[a] + m]);
+                    }
+                    if (s->elc)
+                        durec += (2.0 * Pi / s->vol) * (T[2] * T[2] - M[2] * M[2]);
+                    else
+                        durec += 2.0 * Pi / (3.0 * s->vol) *
+                                 ((T[0] * T[0] + T[1] * T[1] + T[2] * T[2]) - (M[0] * M[0] + M[1] * M[1] + M[2] * M[2]));
+                }
+                durec = s->epsfp * durec;
+                dutot += durec;
+            }
+            /* DUBond: every bond with a moved end, once */
+            if (s->nbond > 0) {
+                int b;
+                for (b = 0; b < s->nbond; ++b) {
+                    const int a1 = s->bond_ij[2 * b] - 1, a2 = s->bond_ij[2 * b + 1] - 1;
+                    double r1[3], r2v[3], dx, dy, dz, r2n, r2o, xn, xo, pn = 1.0, po = 1.0;
+                    int e, la;
+                    if (!moved[a1] && !moved[a2]) continue;
+                    for (m = 0; m < 3; ++m) { r1[m] = s->ro[3 * a1 + m]; r2v[m] = s->ro[3 * a2 + m]; }
+                    for (la = 0; la < nmv; ++la) {
+                        if (mv[la] == a1) for (m = 0; m < 3; ++m) r1[m] = rtm[3 * la + m];
+                        if (mv[la] == a2) for (m = 0; m < 3; ++m) r2v[m] = rtm[3 * la + m];
+                    }
+                    dx = r1[0] - r2v[0]; dy = r1[1] - r2v[1]; dz = r1[2] - r2v[2];
+                    r2n = pbcr2(s, &dx, &dy, &dz);
+                    dx = s->ro[3 * a1] - s->ro[3 * a2]; dy = s->ro[3 * a1 + 1] - s->ro[3 * a2 + 1];
+                    dz = s->ro[3 * a1 + 2] - s->ro[3 * a2 + 2];
+                    r2o = pbcr2(s, &dx, &dy, &dz);
+                    xn = sqrt(r2n) - s->bond_eq[b];
+                    xo = sqrt(r2o) - s->bond_eq[b];
+                    for (e = 0; e < s->bond_p[b]; ++e) { pn *= xn; po *= xo; }
+                    dubond += s->bond_k[b] * (pn - po);
+                }
+                dutot += dubond;
+            }
+            /* Metropolis, then MCUpdate */
+            dured = dutot * beta;
+            {
+                int accept;
+                if (dured > 87.0) accept = 0;
+                else if (dured < -87.0) accept = 1;
+                else {
+                    const double fac = exp(-dured);
+                    accept = (fac > 1.0) ? 1 : (fac > mc_random(s));
+                }
+                if (accept) {
+                    if (accepted) ++*accepted;
+                    u[0] += dutot;
+                    for (k = 0; k <= natat; ++k) u[1 + k] += dtwob[k];
+                    if (s->lewald) u[2 + natat] += durec;
+                    if (s->nbond > 0) u[3 + natat] += dubond;
+                    for (a = 0; a < nmv; ++a) {
+                        const int i = mv[a];
+                        if (s->lewald == 2) {
+                            for (m = 0; m < 3; ++m)
+                                memcpy((cx *)s->eik[m] + (size_t)i * w, tm + ((size_t)a * 3 + m) * w, sizeof(cx) * w);
+                            if (s->elc) memcpy(s->trig2d + (size_t)i * 4 * w, trigtm + (size_t)a * 4 * w, sizeof(double) * 4 * w);
+                        }
+                        for (m = 0; m < 3; ++m) {
+                            s->drostep[3 * i + m] += d[m];
+                            s->ro[3 * i + m] = rtm[3 * a + m];
+                        }
+                    }
+                    if (s->lewald == 2) {
+                        memcpy(s->sumeikr, stm, sizeof(cx) * 4 * (size_t)s->nkvec);
+                        if (s->elc) memcpy(s->sumtrig, sttm, sizeof(double) * 8 * (size_t)s->nkvec2d);
+                    } else if (s->lewald == 1) {
+                        double *t_ = qm;
+                        qm = qmtm;
+                        qmtm = t_;
+                        urecold = urecnew;
+                    }
+                }
+            }
+            for (a = 0; a < nmv; ++a) moved[mv[a]] = 0;
+        }
+    }
+    free(moved); free(mv); free(rtm); free(dtwob); free(unew); free(uold);
+    free(tm); free(stm); free(trigtm); free(sttm); free(qm); free(qmtm); free(fq);
+    return rc;
+}

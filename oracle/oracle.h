@@ -152,6 +152,12 @@ void   or_mc_seed(or_sys *s, int32_t iseed);
  * Metropolis, MCUpdate).  dtran[npt] (>0 cube, <0 sphere), beta = 1/kT in the
  * energy unit; u = [tot, twob(0..natat), rec, bond] from the last or_utotal, advanced
  * by every accepted move.  Needs lewald 0 or 2 (standard Ewald); returns 6 otherwise. */
+/* MCPass with single-particle and chain moves (CallMove's selection by the cumulative pspart,
+ * pchain [npt]; ChainMove translates a whole chain by one displacement of dtranchain).
+ * Chains are contiguous ranges chain_first (0-based) / chain_len. */
+int    or_mc_pass_moves(or_sys *s, int npass, int isamp, const double *dtran, const double *pspart,
+                        const double *pchain, const double *dtranchain, int nchain, const int32_t *chain_first,
+                        const int32_t *chain_len, double beta, double *u, int64_t *accepted, int64_t *hsreject);
 /* MCAllPass: all particles displaced at once (five draws each), UTotal, Metropolis. */
 int    or_mcall_pass(or_sys *s, int npass, const double *dtranall, double beta, double *u, int64_t *accepted);
 int    or_mc_pass(or_sys *s, int npass, int isamp, const double *dtran, double beta, double *u,

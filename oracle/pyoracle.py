@@ -326,6 +326,31 @@ class System:
         u["ubond"] = uu[3 + self.natat]
         return acc.value, hs.value
 
+    def mc_pass_moves(self, npass, dtran, beta, u, pspart, pchain, dtranchain, chains, isamp=0):
+        """npass MCPass sweeps with single-particle and chain moves (cumulative pspart, pchain
+        [npt]; dtranchain [npt]; chains: (first 0-based, length) pairs); u advanced in place.
+        Returns (accepted, hard-core rejects)."""
+        L = lib()
+        L.or_mc_pass_moves.restype = C.c_int
+        L.or_mc_pass_moves.argtypes = [C.c_void_p, C.c_int, C.c_int, f64p, f64p, f64p, f64p, C.c_int, i32p, i32p,
+                                       C.c_double, f64p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        arr = [np.ascontiguousarray(x, np.float64) for x in (dtran, pspart, pchain, dtranchain)]
+        cf = np.ascontiguousarray([c[0] for c in chains], np.int32)
+        cl = np.ascontiguousarray([c[1] for c in chains], np.int32)
+        uu = np.concatenate([[u["utot"]], u["utwob"], [u["urec"], u["ubond"]]]).astype(np.float64)
+        acc = C.c_int64(0)
+        hs = C.c_int64(0)
+        rc = L.or_mc_pass_moves(self.h, int(npass), int(isamp), *[_p(x, C.c_double) for x in arr], len(chains),
+                                _p(cf, C.c_int32), _p(cl, C.c_int32), float(beta), _p(uu, C.c_double),
+                                C.byref(acc), C.byref(hs))
+        if rc:
+            raise RuntimeError("MC pass with moves failed: %d" % rc)
+        u["utot"] = uu[0]
+        u["utwob"] = uu[1:2 + self.natat].copy()
+        u["urec"] = uu[2 + self.natat]
+        u["ubond"] = uu[3 + self.natat]
+        return acc.value, hs.value
+
     def mcall_pass(self, npass, dtranall, beta, u):
         """npass MCAll trials (all particles at once); u advanced in place.  Returns accepted."""
         L = lib()

@@ -485,3 +485,65 @@ def test_mc_spme_sweep_moves_and_keeps_the_mesh_energy():
     assert acc > 0
     o.set_vlist()
     assert abs(u["urec"] - o.utotal()["urec"]) <= 1e-9 * (abs(u["urec"]) + 1.0)
+
+
+# ---------------------------------------------------------------- chain moves (oracle)
+
+def _pe_oracle(ewald):
+    s = dict(Hp.pe_small())
+    if ewald == "std":
+        s = Hp.std_ewald(s)
+    t = Hp.oracle_table(s)
+    o = Hp.oracle_system(s, t)
+    o.set_state(s["ro"], s["rod"])
+    o.set_vlist()
+    return s, o, o.utotal()
+
+
+_CHAINS = [(0, 50), (50, 50), (100, 50), (150, 50)]
+
+
+def test_mc_moves_with_single_particle_moves_only_is_mcpass():
+    """With pspart = 1 for every type the move-selecting pass is MCPass: the same chain."""
+    s, o1, u1 = _pe_oracle("std")
+    _, o2, u2 = _pe_oracle("std")
+    beta = 1.0 / S.kT(s["temp"])
+    o1.mc_seed(3)
+    o2.mc_seed(3)
+    a1 = o1.mc_pass(2, [2.0, 2.0], beta, u1)
+    a2 = o2.mc_pass_moves(2, [2.0, 2.0], beta, u2, [1.0, 1.0], [1.0, 1.0], [5.0, 5.0], _CHAINS)
+    assert a1 == a2
+    assert np.array_equal(o1.get_state()["ro"], o2.get_state()["ro"])
+    assert abs(u1["utot"] - u2["utot"]) <= 1e-12 * abs(u1["utot"])
+
+
+@pytest.mark.parametrize("ewald", ["std", "spme"])
+def test_mc_chain_moves_keep_chains_rigid_and_energies_carried(ewald):
+    """Beads make only chain moves (pspart 0, pchain 1), counterions only single-particle moves:
+    the bonds keep their lengths (whole chains translate) and the carried energies equal a fresh
+    UTotal."""
+    s, o, u = _pe_oracle(ewald)
+    beta = 1.0 / S.kT(s["temp"])
+    bij = np.asarray(s["bond_ij"]) - 1
+
+    def lengths(ro):
+        d = ro[bij[:, 0]] - ro[bij[:, 1]]
+        d -= s["boxlen"][0] * np.round(d / s["boxlen"][0])
+        return np.sqrt((d * d).sum(1))
+
+    l0 = lengths(o.get_state()["ro"])
+    o.mc_seed(5)
+    acc, _ = o.mc_pass_moves(2, [2.0, 2.0], beta, u, [0.0, 1.0], [1.0, 1.0], [3.0, 3.0], _CHAINS)
+    assert acc > 0
+    assert np.abs(lengths(o.get_state()["ro"]) - l0).max() < 1e-11
+    o.set_vlist()
+    fresh = o.utotal()
+    sc = abs(fresh["utwob"][0]) + abs(fresh["urec"]) + abs(fresh["ubond"]) + 1.0
+    for k in ("utot", "urec", "ubond"):
+        assert abs(u[k] - fresh[k]) <= 1e-9 * sc, (k, u[k], fresh[k])
+
+
+def test_mc_chain_move_of_a_particle_in_no_chain_is_refused():
+    s, o, u = _pe_oracle("std")
+    with pytest.raises(RuntimeError):
+        o.mc_pass_moves(1, [2.0, 2.0], 1.0, u, [0.0, 0.0], [1.0, 1.0], [3.0, 3.0], _CHAINS)
