@@ -53,6 +53,16 @@ module MolsimGpu
    end type msg_mc_params
 
    ! struct msg_mcall_params
+   ! struct msg_tab_params (msg_pot_tab)
+   type, bind(c) :: msg_tab_params
+      integer(c_int32_t) :: npt
+      type(c_ptr)        :: zat, sigat, epsat   ! [npt]
+      real(c_double)     :: rcut, ualpha, epsi_four_pi
+      integer(c_int32_t) :: lewald, lljcut
+      real(c_double)     :: ljrcut, ljushift
+      real(c_double)     :: r2uminin, utoltab, ftoltab, umaxtab, fmaxtab, rumaxfac
+   end type msg_tab_params
+
    type, bind(c) :: msg_mcall_params
       real(c_double)     :: beta
       type(c_ptr)        :: dtranall              ! c_loc(dtranall(1:npt))
@@ -292,6 +302,122 @@ module MolsimGpu
          real(c_double), value :: uewaldtol, q2sum, epsi_four_pi, boxlenshort, ualpha
          integer(c_int32_t), intent(out) :: status
       end function msg_alpha_to_ncut
+      ! batches, serving, tuning, timing and set-up helpers
+
+      integer(c_int) function msg_create_batch(p, nsys, precision, h) bind(c, name='msg_create_batch')
+         import :: c_int, c_int32_t, c_ptr, msg_params
+         type(msg_params), intent(in)         :: p(*)
+         integer(c_int32_t), value            :: nsys, precision
+         type(c_ptr), intent(out)             :: h
+      end function msg_create_batch
+
+      integer(c_int32_t) function msg_nsys(h) bind(c, name='msg_nsys')
+         import :: c_int32_t, c_ptr
+         type(c_ptr), value :: h
+      end function msg_nsys
+
+      integer(c_int) function msg_set_state_all(h, ro, rod, rodd) bind(c, name='msg_set_state_all')
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h, ro, rod, rodd
+      end function msg_set_state_all
+
+      integer(c_int) function msg_get_forces(h, isys, force, forceo) bind(c, name='msg_get_forces')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(c_ptr), value        :: force, forceo
+      end function msg_get_forces
+
+      integer(c_int) function msg_get_energy(h, isys, e) bind(c, name='msg_get_energy')
+         import :: c_int, c_int32_t, c_ptr, msg_energy
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: isys
+         type(msg_energy), intent(out) :: e
+      end function msg_get_energy
+
+      integer(c_int) function msg_velver_async(h, nsteps) bind(c, name='msg_velver_async')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: nsteps
+      end function msg_velver_async
+
+      integer(c_int) function msg_pending(h) bind(c, name='msg_pending')
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function msg_pending
+
+      integer(c_int) function msg_estimate_bytes(p, nsys, precision, bytes) bind(c, name='msg_estimate_bytes')
+         import :: c_int, c_int32_t, c_int64_t, msg_params
+         type(msg_params), intent(in)    :: p(*)
+         integer(c_int32_t), value       :: nsys, precision
+         integer(c_int64_t), intent(out) :: bytes
+      end function msg_estimate_bytes
+
+      integer(c_int64_t) function msg_device_bytes(h) bind(c, name='msg_device_bytes')
+         import :: c_int64_t, c_ptr
+         type(c_ptr), value :: h
+      end function msg_device_bytes
+
+      integer(c_int) function msg_trim_caches() bind(c, name='msg_trim_caches')
+         import :: c_int
+      end function msg_trim_caches
+
+      type(c_ptr) function msg_stream(h) bind(c, name='msg_stream')
+         import :: c_ptr
+         type(c_ptr), value :: h
+      end function msg_stream
+
+      integer(c_int) function msg_tune(h, key, val) bind(c, name='msg_tune')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: key, val
+      end function msg_tune
+
+      integer(c_int64_t) function msg_launch_count(h) bind(c, name='msg_launch_count')
+         import :: c_int64_t, c_ptr
+         type(c_ptr), value :: h
+      end function msg_launch_count
+
+      integer(c_int) function msg_set_timing(h, on) bind(c, name='msg_set_timing')
+         import :: c_int, c_int32_t, c_ptr
+         type(c_ptr), value        :: h
+         integer(c_int32_t), value :: on
+      end function msg_set_timing
+
+      integer(c_int32_t) function msg_ntimers() bind(c, name='msg_ntimers')
+         import :: c_int32_t
+      end function msg_ntimers
+
+      integer(c_int) function msg_kernel_time(h, k, kname, total_ms, launches) bind(c, name='msg_kernel_time')
+         import :: c_int, c_int32_t, c_int64_t, c_double, c_ptr
+         type(c_ptr), value              :: h
+         integer(c_int32_t), value       :: k
+         type(c_ptr), intent(out)        :: kname       ! const char *
+         real(c_double), intent(out)     :: total_ms
+         integer(c_int64_t), intent(out) :: launches
+      end function msg_kernel_time
+
+      integer(c_int) function msg_pot_tab(p, ubuf, nbuf, iubuflow, nugrid, r2umin, nused) bind(c, name='msg_pot_tab')
+         import :: c_int, c_int32_t, c_ptr, msg_tab_params
+         type(msg_tab_params), intent(in) :: p
+         type(c_ptr), value               :: ubuf
+         integer(c_int32_t), value        :: nbuf
+         type(c_ptr), value               :: iubuflow, nugrid, r2umin
+         integer(c_int32_t), intent(out)  :: nused
+      end function msg_pot_tab
+
+      integer(c_int) function msg_utwobody_noalloc(np, npt, boxlen, rcut, ro, iptpn, nneighpn, jpnlist, maxnneigh, &
+            ubuf, nbuf, iubuflow, r2umin, r2atat, force, utwob, virial, stream) bind(c, name='msg_utwobody_noalloc')
+         import :: c_int, c_int32_t, c_double, c_ptr
+         integer(c_int32_t), value  :: np, npt
+         real(c_double), intent(in) :: boxlen(3)
+         real(c_double), value      :: rcut
+         type(c_ptr), value         :: ro, iptpn, nneighpn, jpnlist   ! device pointers
+         integer(c_int32_t), value  :: maxnneigh
+         type(c_ptr), value         :: ubuf
+         integer(c_int32_t), value  :: nbuf
+         type(c_ptr), value         :: iubuflow, r2umin, r2atat, force, utwob, virial, stream
+      end function msg_utwobody_noalloc
    end interface
 
 contains

@@ -65,3 +65,11 @@ def test_engine_fails_loudly_without_library(monkeypatch, tmp_path):
         assert "not built" in str(e)
     else:
         raise AssertionError("loading a missing library must fail")
+
+
+def test_fortran_module_binds_every_entry_point():
+    """The ISO_C_BINDING module declares every entry point of include/*.h under its C name."""
+    f = open(os.path.join(ROOT, "molsim_b200", "fortran", "molsim_gpu_iface.F90")).read()
+    bound = set(re.findall(r"name='(msg_[a-z0-9_]+)'", f))
+    missing = declared_symbols() - bound
+    assert not missing, sorted(missing)
