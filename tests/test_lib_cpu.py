@@ -73,3 +73,59 @@ def test_fortran_module_binds_every_entry_point():
     bound = set(re.findall(r"name='(msg_[a-z0-9_]+)'", f))
     missing = declared_symbols() - bound
     assert not missing, sorted(missing)
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """Every struct of include/molsim_gpu.h has the same size and field offsets in the ctypes
+    mirror as gcc gives it (a small C program compiled against the header prints them)."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    if not shutil.which("gcc"):
+        pytest.skip("gcc is not installed")
+    structs = {"msg_params": _lib.MsgParams, "msg_energy": _lib.MsgEnergy, "msg_mc_params": _lib.MsgMcParams,
+               "msg_mcall_params": _lib.MsgMcAllParams, "msg_site_ewald": _lib.MsgSiteEwald,
+               "msg_tab_params": _lib.MsgTabParams}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "molsim_gpu.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in cls._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
+    lines += ["return 0; }"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, cls in structs.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_oracle_params_match_the_c_layout(tmp_path):
+    """The oracle's or_params and its ctypes mirror (pyoracle.Params) agree field by field."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    if not shutil.which("gcc"):
+        pytest.skip("gcc is not installed")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "oracle.h"', "int main(void) {",
+             'printf("size %zu\\n", sizeof(or_params));']
+    for fname, _ in O.Params._fields_:
+        lines.append('printf("%s %%zu\\n", offsetof(or_params, %s));' % (fname, fname))
+    lines += ["return 0; }"]
+    src = tmp_path / "olayout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "olayout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "oracle"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {l.split()[0]: int(l.split()[1]) for l in out if l.strip()}
+    assert got["size"] == C.sizeof(O.Params)
+    for fname, _ in O.Params._fields_:
+        assert got[fname] == getattr(O.Params, fname).offset, fname
