@@ -129,3 +129,31 @@ def test_oracle_params_match_the_c_layout(tmp_path):
     assert got["size"] == C.sizeof(O.Params)
     for fname, _ in O.Params._fields_:
         assert got[fname] == getattr(O.Params, fname).offset, fname
+
+
+def test_fortran_types_follow_the_c_structs():
+    """Each bind(c) type of the Fortran module lists the fields of its C struct in the same order
+    (no Fortran compiler here: the declarations are compared as text)."""
+    f = open(os.path.join(ROOT, "molsim_b200", "fortran", "molsim_gpu_iface.F90")).read()
+    h = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "molsim_gpu.h")).read(), flags=re.S)
+    ftypes = re.findall(r"type, bind\(c\) :: (\w+)\n(.*?)end type \1", f, flags=re.S)
+    assert len(ftypes) >= 5
+    for name, body in ftypes:
+        fnames = []
+        for line in body.split("\n"):
+            line = line.split("!")[0]
+            if "::" not in line:
+                continue
+            decl = re.sub(r"\([^)]*\)", "", line.split("::", 1)[1])
+            fnames += [x.strip() for x in decl.split(",") if x.strip()]
+        m = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), h, flags=re.S)
+        assert m, name
+        cnames = []
+        for stmt in m.group(1).split(";"):
+            stmt = re.sub(r"\[[^\]]*\]", "", stmt).strip()
+            if not stmt:
+                continue
+            parts = [p.strip() for p in stmt.split(",")]
+            first = parts[0].replace("*", " ").split()[-1]
+            cnames += [first] + [p.replace("*", "").strip() for p in parts[1:]]
+        assert fnames == cnames, (name, fnames, cnames)
