@@ -55,6 +55,25 @@ def gather_metrics(local, group=None):
     return out
 
 
+def ensemble_share(n_particles, nbytes, rank, world, budget_bytes=None):
+    """Indices of the ensemble systems rank `rank` advances: every system takes the same
+    number of steps, so its work is its particle count.  Every rank computes the same
+    partition from the same (seeded) ensemble, without communicating."""
+    idx = list(range(len(n_particles)))
+    return my_share(idx, [float(n) for n in n_particles], nbytes, rank, world, budget_bytes)
+
+
+def combine_ensemble(per_rank):
+    """Whole-job ensemble throughput from per-rank results {particles, steps, device_ms}:
+    all ranks' particle-steps over the slowest rank's device time (ranks start together
+    after a barrier and run no collective until they finish)."""
+    work = float(sum(m["particles"] * m["steps"] for m in per_rank))
+    tmax = max(m["device_ms"] for m in per_rank)
+    return dict(systems=int(sum(m["systems"] for m in per_rank)), particles=int(sum(m["particles"] for m in per_rank)),
+                particle_steps=work, device_ms_max=tmax, value=work / (tmax / 1000.0) if tmax > 0 else 0.0,
+                ranks=len(per_rank))
+
+
 def combine_serving(per_rank):
     """Whole-job serving metrics from per-rank ones: particle-steps over the longest
     rank's span; latency percentiles over all jobs."""

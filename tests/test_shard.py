@@ -96,3 +96,52 @@ def test_two_rank_gloo_serving_partition():
     assert ids == list(range(24))
     assert njobs == 24
     assert work == want
+
+
+def _ensemble_rank_main(rank, world, port, out):
+    """One rank of the bench's ensemble partition: its share of a seeded ensemble, a
+    simulated device time proportional to its particles, metrics gathered and combined."""
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    from molsim_b200.shard import combine_ensemble, ensemble_share, gather_metrics
+
+    rng = np.random.default_rng(3)
+    npart = [int(x) for x in rng.integers(100, 2000, size=40) * 2]
+    nbytes = [n * 1000 for n in npart]
+    mine = ensemble_share(npart, nbytes, rank, world)
+    steps = 10
+    local = {"systems": len(mine), "particles": sum(npart[k] for k in mine), "steps": steps,
+             "device_ms": 1e-3 * sum(npart[k] for k in mine), "ids": mine}
+    per = gather_metrics(local)
+    if rank == 0:
+        out.put((sorted(i for m in per for i in m["ids"]), combine_ensemble(per), npart,
+                 [m["device_ms"] for m in per]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_gloo_ensemble_partition():
+    """The ensemble leg of bench.py under torchrun: the ranks' shares cover every system
+    once, the loads balance, and the whole-job value is all particle-steps over the
+    slowest rank's time."""
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ensemble_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    ids, comb, npart, times = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert ids == list(range(40))
+    assert comb["systems"] == 40 and comb["particles"] == sum(npart) and comb["ranks"] == 2
+    assert max(times) <= 1.05 * min(times)
+    assert abs(comb["value"] - sum(npart) * 10 / (max(times) / 1000.0)) <= 1e-6 * comb["value"]
