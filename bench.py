@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=200,
                     help="jobs in the serving stream (Poisson arrivals at 200/s; 0: skip)")
     ap.add_argument("--serve-budget-gib", type=float, default=4.0)
+    ap.add_argument("--serve-low-rate", type=float, default=50.0,
+                    help="serving: the same stream again at this arrival rate (jobs/s; 0: skip)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -189,9 +191,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_profile_traffic():
-    """Per-launch DRAM bytes of the pair kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "pair_kernel_polyelectrolyte_16000.md")
+def read_profile_traffic(name="pair_kernel_polyelectrolyte_16000.md"):
+    """Per-launch DRAM bytes of the pair kernel from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -244,20 +246,77 @@ def timed_md_steps(e, K, flush, warmup):
     return sum(x.elapsed_time(y) for x, y in zip(st, en))
 
 
-def run_ensemble(a, flush):
+def hbm_peak():
+    """(peak GB/s, source) for the roofline denominators."""
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+        if "hbm_gbs" in peaks:
+            return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6650 GB/s"
+
+
+def pair_bytes(e, s_pos, s_f=24):
+    """Algorithmic bytes of one pair-kernel launch over every system of engine e:
+    sum of N (s_pos + s_f) + 4 P_half, with P_half each system's half-list pair count
+    (the reference's SetVListMD rule, from a fresh list build)."""
+    tot = pairs = 0
+    for k, sd in enumerate(e.systems):
+        _, _, npair = e.SetVList(k, export=False)
+        tot += int(sd["np"]) * (s_pos + s_f) + 4 * int(npair)
+        pairs += int(npair)
+    return tot, pairs
+
+
+def pair_roofline(e, step, K, flush, b_pair, traffic=None):
+    """Roofline object of the pair kernel of engine e: its mean CUDA-event duration over K
+    steps (the library's per-kernel timers, which serialise the step's two branches), with
+    the L2 flushed before each step; `step` advances e by one step."""
+    import torch
+
+    ext = torch.cuda.ExternalStream(e.stream())
+    e.set_timing(True)
+    for _ in range(K):
+        with torch.cuda.stream(ext):
+            flush()
+        step()
+    kt = e.kernel_times()
+    e.set_timing(False)
+    tot, cnt = kt.get("pair", (0.0, 0))
+    t_pair = tot / cnt / 1000.0 if cnt else 0.0
+    peak, src = hbm_peak()
+    achieved = b_pair / t_pair / 1e9 if t_pair > 0 else 0.0
+    return {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if peak else None, "traffic": traffic, "algorithmic_bytes_per_launch": b_pair,
+            "pair_ms_per_launch": 1000.0 * t_pair, "peak_source": src}
+
+
+def run_ensemble(a, flush, rank=0, world=1):
     """The batched ensemble: electrolytes with N ~ U{200..4000}, rho*sigma^3 ~ U[0.01, 0.3],
     T ~ U[250, 400] K, SPME order 4 with the grid edge of each system chosen by the
     autotuner from {16, 24, 32, 48}; all systems in one handle, one CUDA-graph replay
-    per step.  Mixed precision, beside the same ensemble on the FP64 path."""
+    per step.  Mixed precision, beside the same ensemble on the FP64 path.  Under torchrun
+    the systems are partitioned across the ranks (longest-work-first, no exchange on the
+    data path): each rank advances its share in its own handle, and the whole-job figure
+    is all particle-steps over the slowest rank's device time."""
     import torch
 
     from molsim_b200 import Engine, prepare
     from molsim_b200.autotune import apply_grids, tune_grids, tune_pair_kernel
+    from molsim_b200.shard import combine_ensemble, ensemble_share, gather_metrics
     from molsim_b200.systems import batched_ensemble
 
     t0 = time.perf_counter()
-    systems = batched_ensemble(seed=0, nsys=a.ensemble)
-    tables = [prepare(s) for s in systems]
+    systems_all = batched_ensemble(seed=0, nsys=a.ensemble)
+    tables_all = [prepare(s) for s in systems_all]
+    if world > 1:
+        from molsim_b200.engine import estimate_bytes
+        nb = [estimate_bytes(s_, t_) for s_, t_ in zip(systems_all, tables_all)]
+        mine = ensemble_share([int(s_["np"]) for s_ in systems_all], nb, rank, world)
+    else:
+        mine = list(range(len(systems_all)))
+    systems = [systems_all[k] for k in mine]
+    tables = [tables_all[k] for k in mine]
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
     edges, rep = tune_grids(systems, tables)
@@ -269,20 +328,29 @@ def run_ensemble(a, flush):
     eng.GetLinAcc()
     best, lane_ms = tune_pair_kernel(eng)
     K = max(10, a.steps // 4)
+    if world > 1:
+        torch.distributed.barrier()
     ms = timed_md_steps(eng, K, flush, a.warmup)
-    value = ntot * K / (ms / 1000.0)
     del eng
     e64 = Engine(sy, tables, precision="fp64")
     e64.UTotal(0)
     e64.GetLinAcc()
+    if world > 1:
+        torch.distributed.barrier()
     ms64 = timed_md_steps(e64, K, flush, a.warmup)
     del e64
     torch.cuda.synchronize()
-    hist = {g: edges.count(g) for g in sorted(set(edges))}
-    return {"systems": len(sy), "particles": ntot, "value": value, "unit": METRIC, "steps": K,
-            "ms_per_step": ms / K, "precision": "mixed", "fp64_batched_value": ntot * K / (ms64 / 1000.0),
-            "vs_fp64_batched": ms64 / ms,
-            "autotune": {"grid_edges": hist, "target_met": int(sum(r["met"] for r in rep)),
+    per = gather_metrics({"systems": len(sy), "particles": ntot, "steps": K, "device_ms": ms,
+                          "device_ms_fp64": ms64, "edges": list(edges), "met": int(sum(r["met"] for r in rep))})
+    comb = combine_ensemble(per)
+    comb64 = combine_ensemble([dict(m, device_ms=m["device_ms_fp64"]) for m in per])
+    all_edges = [e_ for m in per for e_ in m["edges"]]
+    hist = {g: all_edges.count(g) for g in sorted(set(all_edges))}
+    return {"systems": comb["systems"], "particles": comb["particles"], "value": comb["value"], "unit": METRIC,
+            "steps": K, "ms_per_step": comb["device_ms_max"] / K, "precision": "mixed",
+            "fp64_batched_value": comb64["value"], "vs_fp64_batched": comb["value"] / comb64["value"],
+            "ranks": world, "partition": "longest-work-first over ranks, no collective on the data path",
+            "autotune": {"grid_edges": hist, "target_met": int(sum(m["met"] for m in per)),
                          "rule": "cheapest edge with measured reciprocal RMS force error <= Kolafa-Perram "
                                  "real-space estimate (reference 96^3 order 6)",
                          "pair_kernel": best, "pair_kernel_ms_per_step": lane_ms, "tune_s": t_tune},
@@ -327,6 +395,16 @@ def run_bd(a, flush):
         out["value" if prec == "mixed" else "fp64_value"] = n * K / (ms / 1000.0)
         out["ms_per_step" if prec == "mixed" else "fp64_ms_per_step"] = ms / K
         out["steps"] = K
+        if prec == "mixed":
+            b_pair, pairs = pair_bytes(e, 16)
+            e.BDStep(1, seed=7, energies=False)
+
+            def bd_step():
+                if L.msg_bd_step(e.h, 1, 7, 0, None, None, None):
+                    raise RuntimeError(L.msg_last_error(e.h).decode())
+            out["roofline"] = pair_roofline(e, bd_step, K, flush, b_pair,
+                                            traffic=read_profile_traffic("pair_kernel_bd_200000.md"))
+            out["half_list_pairs"] = pairs
         del e
     out["vs_fp64"] = out["value"] / out["fp64_value"]
     return out
@@ -722,25 +800,48 @@ def run_poly(a):
     return out
 
 
-def run_serving(a):
+def run_serving(a, rank=0, world=1):
     """The serving stream: Poisson arrivals at 200 jobs/s, N log-uniform over 100-20000,
     half electrolytes and half polyelectrolytes, 1000 MD steps each, mixed precision,
-    admitted by device-memory budget into concurrent cohorts.  Beside it: a sample of
-    the same jobs run alone, one after another, on the plain FP64 path."""
+    admitted by device-memory budget into concurrent cohorts; the same jobs again at a
+    rate the GPU keeps up with (a.serve_low_rate jobs/s), so that latency shows service
+    time rather than queueing.  Beside them: a sample of the same jobs run alone, one after
+    another, on the plain FP64 path.  Under torchrun each rank serves its share of the
+    stream (jobs partitioned by work, longest first; no exchange on the data path), and
+    the metrics of all ranks are combined: particle-steps over the longest rank's span,
+    latency percentiles over all jobs."""
     import torch
 
     from molsim_b200 import Engine
     from molsim_b200.serve import Server, poisson_stream
+    from molsim_b200.shard import combine_serving, gather_metrics, my_share
 
-    jobs = poisson_stream(seed=11, rate=200.0, njobs=a.serve_jobs, nmin=100, nmax=20000, nsteps=1000)
     # load the library and fill the cuFFT plan cache outside the measured stream
     warm = poisson_stream(seed=12, rate=1e6, njobs=4, nmin=100, nmax=400, nsteps=20)
     Server(1 << 30, precision="mixed", chunk=10).run(warm, realtime=False)
-    srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50,
-                 batch_wait_s=a.serve_wait, ahead=a.serve_ahead)
-    torch.cuda.synchronize()
-    m = srv.run(jobs)
-    m.pop("latencies", None)
+    out = None
+    for rate in (200.0, a.serve_low_rate):
+        if rate <= 0:
+            continue
+        jobs = poisson_stream(seed=11, rate=rate, njobs=a.serve_jobs, nmin=100, nmax=20000, nsteps=1000)
+        if world > 1:
+            jobs = my_share(jobs, [j.n * j.nsteps for j in jobs], [1] * len(jobs), rank, world)
+        srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50,
+                     batch_wait_s=a.serve_wait, ahead=a.serve_ahead, refill=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        m = srv.run(jobs)
+        per = gather_metrics(m)
+        comb = combine_serving(per) if world > 1 else dict(m)
+        comb.pop("latencies", None)
+        comb["jobs_per_s_offered"] = rate
+        if out is None:
+            out = comb
+            out["jobs_all"] = jobs
+        else:
+            out["low_rate"] = comb
+    jobs = out.pop("jobs_all")
     # the plain FP64 path, each job alone: a sample across sizes, 200 steps each
     smp = sorted(jobs, key=lambda j: j.n)[:: max(1, len(jobs) // 12)][:12]
     work = tsum = 0.0
@@ -757,11 +858,11 @@ def run_serving(a):
         work += j.n * j.nsteps
         del e
     alone = work / tsum if tsum else None
-    m.update({"unit": METRIC, "jobs_per_s_offered": 200.0, "nsteps_per_job": 1000,
-              "precision": "mixed", "fp64_alone_value": alone,
-              "fp64_alone_sample": "%d jobs across the size range, %d steps each, scaled to 1000" % (len(smp), ks),
-              "vs_fp64_alone": (m["value"] / alone) if alone else None})
-    return m
+    out.update({"unit": METRIC, "nsteps_per_job": 1000, "ranks": world,
+                "precision": "mixed", "fp64_alone_value": alone,
+                "fp64_alone_sample": "%d jobs across the size range, %d steps each, scaled to 1000" % (len(smp), ks),
+                "vs_fp64_alone": (out["value"] / alone) if alone else None})
+    return out
 
 
 def run_gpu(a):
@@ -840,11 +941,21 @@ def run_gpu(a):
 
     # ---- the plain FP64 path on the same system (the drop-in and the comparison base) ----
     fp64_value = None
+    errs = None
     if a.precision != "fp64":
         e64 = Engine(s, precision="fp64")
         e64.UTotal()
         e64.GetLinAcc()
         fp64_value = n * a.steps / (timed_steps(e64, a.steps) / 1000.0)
+        # the metric's accuracy condition: mixed forces against the plain FP64 GPU path, same state
+        st_m = eng.get_state(0)
+        e64.put_state(0, st_m["ro"], st_m["rod"], st_m["rodd"], keep_list=False)
+        r64, rmx = e64.UTotal(), eng.UTotal()
+        f64v, fmx = np.asarray(r64["force"]), np.asarray(rmx["force"])
+        errs = {"force_rms_rel": float(np.sqrt(((fmx - f64v) ** 2).sum() / (f64v ** 2).sum()))}
+        for k in ("utot", "urec", "virial", "ubond"):
+            errs[k + "_rel"] = abs(rmx[k] - r64[k]) / max(abs(r64[k]), 1e-300)
+        errs["utwob_rel"] = [abs(x - y) / max(abs(y), 1e-300) for x, y in zip(rmx["utwob"], r64["utwob"])]
         del e64
     # ---- batched: replicas of the workload advanced together in one handle ----
     batched = None
@@ -861,7 +972,20 @@ def run_gpu(a):
         batched = {"replicas": a.replicas, "pair_kernel": tuned_b, "value": n * a.replicas * kb / (tb / 1000.0), "unit": METRIC,
                    "steps": kb, "ms_per_step": tb / kb,
                    "vs_fp64_single": (n * a.replicas * kb / (tb / 1000.0)) / fp64_value if fp64_value else None}
+        b_pair_b, _ = pair_bytes(eb, 32 if a.precision == "fp64" else 16)
+        eb.VelVer(1, energies=False)
+        batched["roofline"] = pair_roofline(eb, lambda: eb.VelVer(1, energies=False), kb, flush, b_pair_b,
+                                            traffic=read_profile_traffic("pair_kernel_batched_32x16000.md"))
         del eb
+        if a.precision != "fp64":
+            # the same replicas on the FP64 path: the like-for-like comparison of the batched figure
+            e64b = Engine([dict(s) for _ in range(a.replicas)], precision="fp64")
+            e64b.UTotal(0)
+            e64b.GetLinAcc()
+            tb64 = timed_steps(e64b, kb)
+            del e64b
+            batched["fp64_value"] = n * a.replicas * kb / (tb64 / 1000.0)
+            batched["vs_fp64_batched"] = tb64 / tb
 
     # ---- per-kernel device times: the same K steps with the library's CUDA-event timers ----
     eng.set_timing(True)
@@ -904,11 +1028,7 @@ def run_gpu(a):
     s_f = 24
     b_pair = n * (s_pos + s_f) + 4 * npair
     t_pair = breakdown.get("pair", {}).get("ms_per_launch", 0.0) / 1000.0
-    peaks = {}
-    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(pk):
-        peaks = json.load(open(pk))
-    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak, peak_src = hbm_peak()
     achieved = b_pair / t_pair / 1e9 if t_pair > 0 else 0.0
     traffic = read_profile_traffic()
 
@@ -929,10 +1049,11 @@ def run_gpu(a):
         mc = run_mc(a)
     if rank == 0 and world == 1 and a.poly:
         poly = run_poly(a)
-    if rank == 0 and world == 1 and a.ensemble > 0:
-        ensemble = run_ensemble(a, flush)
-    if rank == 0 and world == 1 and a.serve_jobs > 0:
-        serving = run_serving(a)
+    # independent systems shard across ranks: every rank runs these legs on its share
+    if a.ensemble > 0:
+        ensemble = run_ensemble(a, flush, rank, world)
+    if a.serve_jobs > 0:
+        serving = run_serving(a, rank, world)
 
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -953,11 +1074,31 @@ def run_gpu(a):
                     "d2h_bytes_per_step": 3 * 24 * n + C.sizeof(_lib.MsgEnergy)},
             "roofline": {"kernel": "pair", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": b_pair,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
-                         else "fallback 6650 GB/s"},
+                         "algorithmic_bytes_per_launch": b_pair, "pair_ms_per_launch": 1000.0 * t_pair,
+                         "peak_source": peak_src},
             "kernels": breakdown, "gpu_launches": int(launches), "clocks": clk,
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "errors_vs_fp64_gpu": errs}
+    # like-for-like mixed/FP64 ratios and the other legs' headline figures as top-level scalars
+    def g(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict):
+                return None
+            d = d.get(k)
+        return d
+    line.update({
+        "vs_fp64_single": value / fp64_value if fp64_value else None,
+        "batched_value": g(batched, "value"), "batched_fp64_value": g(batched, "fp64_value"),
+        "vs_fp64_batched": g(batched, "vs_fp64_batched"),
+        "batched_roofline_frac": g(batched, "roofline", "frac"),
+        "ensemble_value": g(ensemble, "value"), "ensemble_fp64_value": g(ensemble, "fp64_batched_value"),
+        "vs_fp64_ensemble": g(ensemble, "vs_fp64_batched"),
+        "bd_200k_value": g(bd, "value"), "bd_200k_fp64_value": g(bd, "fp64_value"),
+        "vs_fp64_bd_200k": g(bd, "vs_fp64"), "bd_200k_roofline_frac": g(bd, "roofline", "frac"),
+        "serving_value": g(serving, "value"), "serving_p50_s": g(serving, "p50_s"),
+        "serving_p99_s": g(serving, "p99_s"), "serving_low_rate_p50_s": g(serving, "low_rate", "p50_s"),
+        "serving_low_rate_p99_s": g(serving, "low_rate", "p99_s"),
+        "force_rms_err_vs_fp64_gpu": g(errs, "force_rms_rel"),
+    })
     print(json.dumps(line), flush=True)
 
 

@@ -104,6 +104,12 @@ typedef struct msg_params {
     int32_t lewald2dlc;      /* 1: 2D layer correction (UEwaldRecStd2dlc, lewald 2) and    */
                              /*    UEwaldSurf's 2d-periodic form (Src/energy.F90:1106-1203, */
                              /*    1362-1369), in UTotal and in the Monte Carlo difference */
+    int32_t inlist;          /* NList update interval (Src/nlist.F90:600-620): 0 the skin  */
+                             /*    test; n > 0 a rebuild whenever mod(istep2, n) == 0,      */
+                             /*    istep2 counting steps since msg_nlist_before_macrostep   */
+    int32_t lvlistllist;     /* 1: the Verlet list is SetLList(rcut+drnlist) +             */
+                             /*    SetVListMDLList's (Src/nlist.F90:698-702, 769-811,      */
+                             /*    1168-1260): pair set and row order; at most 1000 cells  */
 } msg_params;
 
 typedef struct msg_handle msg_handle;
@@ -126,6 +132,10 @@ int  msg_create_batch(const msg_params *p, int32_t nsys, int32_t precision, msg_
 void msg_destroy(msg_handle *h);
 const char *msg_last_error(const msg_handle *h);
 int32_t msg_nsys(const msg_handle *h);
+
+/* NList(iBeforeMacrostep) (Src/nlist.F90:594-596) for every system of the handle:
+ * drosum = 0, and the step count istep2 of the inlist > 0 rule restarts. */
+int  msg_nlist_before_macrostep(msg_handle *h);
 
 /* Positions ro, velocities rod, accelerations rodd of system isys, [np][3]; NULL skips. */
 int  msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd);
@@ -156,9 +166,12 @@ int  msg_get_forces(msg_handle *h, int32_t isys, double *force, double *forceo);
  * mixed results by FP32 rounding (a lane's partial sum is regrouped), and stay
  * deterministic for each setting. */
 #define MSG_TUNE_PAIR_LANES 1
-/* MSG_TUNE_PAIR_KERNEL (mixed path): 1 (default) the lean FP32 pair kernel that
- * splits each pair's energy between its two ends, 0 the kernel shared with the
- * FP64 path; both within the mixed-precision tolerance of the FP64 result. */
+/* MSG_TUNE_PAIR_KERNEL (mixed path): 2 (default) the FP32 pair kernel with FP64
+ * energy and virial sums over a half list (each pair once, partner forces as
+ * 64-bit fixed-point atomics), 3 the same kernel over a full list (each pair from
+ * both ends, no atomics), 1 the lean FP32 kernel with FP32 energy terms, 0 the
+ * kernel shared with the FP64 path.  Switching between half and full lists
+ * rebuilds the lists.  Forces agree within the mixed-precision tolerance. */
 #define MSG_TUNE_PAIR_KERNEL 2
 /* MSG_TUNE_PAIR_UNROLL (lean kernel): row entries each lane keeps in flight,
  * 1, 2 (default) or 4.  Results do not depend on it. */
@@ -296,21 +309,28 @@ int     msg_kernel_time(const msg_handle *h, int32_t k, const char **name, doubl
  * cannot call cudaMalloc (a host whose device memory all comes from its own
  * pool or a framework allocator, or a memory budget that forbids a library to
  * grow).  All arrays are device-accessible memory the caller owns: ro [np][3],
- * iptpn [np] (1-based), nneighpn [np] and jpnlist [np][maxnneigh] (MOLSIM's
- * half list, 1-based partners), ubuf [nbuf]; force [np][3] is overwritten in
- * kJ/(mol A) (MOLSIM `force` before UTotal's unit scaling), utwob
- * [natat+1] receives u%twob(0..natat), virial [1] the pair virial.  boxlen,
- * iubuflow, r2umin and r2atat (may be NULL) are host arrays.  The only scratch
- * is a fixed static device array (about 88 KiB per GPU, held until exit), so
- * np <= 262144; larger np returns MSG_ERR_ARG.  The first call on a device
- * looks up that array's address: make it before any stream capture.  Calls
- * share the array; calls that overlap on the GPU race.  The call waits for
- * its work on `stream` (a cudaStream_t, NULL for the default stream). */
+ * iptpn [np] (1-based), nneighpn [np] and jpnlist [np][maxnneigh] (1-based
+ * partners), ubuf [nbuf]; force [np][3] is overwritten in kJ/(mol A) (MOLSIM
+ * `force` before UTotal's unit scaling), utwob [natat+1] receives
+ * u%twob(0..natat), virial [1] the pair virial.  lmc = 0: the list is MOLSIM's
+ * MD half list (SetVList, every pair in one row); lmc = 1: a full list (every
+ * pair in both rows, as Monte Carlo builds it), and pairs with jp < ip are
+ * skipped as UTwoBodyA does under lmc (Src/energy.F90:466-468).  A row longer
+ * than maxnneigh, or an index out of range, returns MSG_ERR_ARG.  boxlen,
+ * iubuflow, r2umin and r2atat (may be NULL) are host arrays; stop_ipjp (may be
+ * NULL) receives the 1-based ip and jp of the pair that raised a nonzero
+ * status (StopUTwoBodyA's report), zeros otherwise.  Rectangular periodic box
+ * only (PBCr2's lbcbox branch).  The only scratch is a fixed static device
+ * array (about 88 KiB per GPU, held until exit), so np <= 262144; larger np
+ * returns MSG_ERR_ARG.  The first call on a device looks up that array's
+ * address: make it before any stream capture.  Calls share the array; calls
+ * that overlap on the GPU race.  Every call waits for its work on `stream` (a
+ * cudaStream_t, NULL for the default stream) before it returns. */
 int  msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen[3], double rcut, const double *ro,
                           const int32_t *iptpn, const int32_t *nneighpn, const int32_t *jpnlist,
-                          int32_t maxnneigh, const double *ubuf, int32_t nbuf, const int32_t *iubuflow,
-                          const double *r2umin, const double *r2atat, double *force, double *utwob,
-                          double *virial, void *stream);
+                          int32_t maxnneigh, int32_t lmc, const double *ubuf, int32_t nbuf,
+                          const int32_t *iubuflow, const double *r2umin, const double *r2atat, double *force,
+                          double *utwob, double *virial, int32_t *stop_ipjp, void *stream);
 
 /* UTwoBodyP (Src/energy.F90:786-896): site-site pair energy, forces and virial of
  * polyatomic particles over MOLSIM's particle list, as UTotal calls it for molecules.

@@ -30,7 +30,8 @@ class MsgParams(C.Structure):
                 ("ualpha", C.c_double), ("epsi_four_pi", C.c_double), ("nbond", C.c_int32),
                 ("bond_ij", i32p), ("bond_k", f64p), ("bond_eq", f64p), ("bond_p", i32p),
                 ("tstep", C.c_double), ("bd_fac1", f64p), ("bd_fac2", f64p), ("maxnneigh", C.c_int32),
-                ("ncut", C.c_int32), ("ncutregion", C.c_int32), ("lewald2dlc", C.c_int32)]
+                ("ncut", C.c_int32), ("ncutregion", C.c_int32), ("lewald2dlc", C.c_int32),
+                ("inlist", C.c_int32), ("lvlistllist", C.c_int32)]
 
 
 class MsgEnergy(C.Structure):
@@ -72,6 +73,7 @@ SIGNATURES = {
     "msg_last_error": (C.c_char_p, [C.c_void_p]),
     "msg_nsys": (C.c_int32, [C.c_void_p]),
     "msg_set_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p]),
+    "msg_nlist_before_macrostep": (C.c_int, [C.c_void_p]),
     "msg_set_state_all": (C.c_int, [C.c_void_p, f64p, f64p, f64p]),
     "msg_get_state": (C.c_int, [C.c_void_p, C.c_int32, f64p, f64p, f64p]),
     "msg_build_nlist": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, C.c_int32, C.POINTER(C.c_int64)]),
@@ -117,8 +119,9 @@ SIGNATURES = {
     "msg_ntimers": (C.c_int32, []),
     "msg_kernel_time": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_char_p), f64p, C.POINTER(C.c_int64)]),
     "msg_utwobody_noalloc": (C.c_int, [C.c_int32, C.c_int32, f64p, C.c_double, C.c_void_p, C.c_void_p,
-                                       C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, i32p, f64p,
-                                       f64p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+                                       C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
+                                       i32p, f64p, f64p, C.c_void_p, C.c_void_p, C.c_void_p, i32p,
+                                       C.c_void_p]),
     "msg_rcut_to_alpha": (C.c_double, [C.c_double] * 5 + [i32p]),
     "msg_alpha_to_ncut": (C.c_int32, [C.c_double] * 5 + [i32p]),
     "msg_pot_tab": (C.c_int, [C.POINTER(MsgTabParams), f64p, C.c_int32, i32p, i32p, f64p, i32p]),

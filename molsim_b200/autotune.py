@@ -118,12 +118,14 @@ def tune_pair_lanes(engine, shifts=(-1, 0, 1), steps=10):
     return best, times
 
 
-def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2)):
-    """Shape of the pair kernel for this handle, by timing MD steps: lanes per particle
+def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2), kinds=(2, 3)):
+    """Shape of the pair kernel for this handle, by timing MD steps: the list layout
+    (kind 2: half list with partner atomics, 3: full list), lanes per particle
     (2^shift times the default), row entries in flight per lane (unroll), and pair blocks
     per SM (0: as many as fit; 2: room for the SPME chain beside it), one knob at a time
     from the defaults.  Leaves the engine on the best; returns ({knob: value}, {setting:
-    ms per step}).  Mixed precision only (the knobs belong to its pair kernel)."""
+    ms per step}).  Mixed precision only (the knobs belong to its pair kernel).  Every
+    setting gives the same results to FP32 rounding of the forces."""
     from . import _lib
 
     L = _lib.lib()
@@ -132,9 +134,10 @@ def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blo
         if L.msg_tune(engine.h, key, int(val)):
             raise RuntimeError("msg_tune(%d, %d) failed" % (key, val))
 
-    best = {"shift": 0, "unroll": 2, "blocks": 0}
+    best = {"kind": 2, "shift": 0, "unroll": 2, "blocks": 0}
     log = {}
-    for name, vals, key in (("shift", shifts, None), ("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
+    for name, vals, key in (("kind", kinds, _lib.MSG_TUNE_PAIR_KERNEL), ("shift", shifts, None),
+                            ("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
                             ("blocks", blocks, _lib.MSG_TUNE_PAIR_BLOCKS)):
         res = {}
         for v in vals:

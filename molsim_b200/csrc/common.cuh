@@ -75,7 +75,16 @@ struct SysDev {
     // 2D layer correction (lewald2dlc): its forces are one more slice after the ew_nks
     int elc;                    // 1: layer correction (with recstd) and the 2D surface term
     int elc_nkv, elc_kv_off;    // 2D k-vectors (nx, ny) of this system and their first entry
-    int elc_pad;
+    int inlist;                 // NList: 0 skin test; n > 0 rebuild whenever istep2 % n == 0
+    // lvlistllist: SetLList(rcut+drnlist) grid (lnd cells per dimension, lcelli = real(lnd)/boxlen)
+    // and SetNCell's probe distance lrcut = rcut
+    int llist, lnd[3];
+    double lcelli[3], lrcut;
+    // precise FP32 pair kernel: r2 from fixed-point differences (fxd = box/2^32 per
+    // dimension; cubic boxes use the integer sum of squares times fx2f = fxd^2 in FP32)
+    int fx_cubic, tab_smem_h;
+    float fx2f, pad4;
+    double fxd[3];
 };
 
 // One type pair's slice of the concatenated table.

@@ -160,6 +160,10 @@ struct msg_handle {
     int *typ[2] = {}, *orig[2] = {};
     int *cellid = nullptr, *inv = nullptr, *sysid = nullptr;
     double4 *fsr = nullptr, *ftot = nullptr;
+    // half list (each pair once): the pair kernel adds partner forces here as 2^-32 fixed point,
+    // x, y and z blocks of ntot entries; k_finalize adds them to fsr and clears them
+    int list_half = 0;
+    unsigned long long *fpart = nullptr;
     int4 *posfx = nullptr;
     // rebuild
     uint32_t *k0 = nullptr, *v0 = nullptr, *k1 = nullptr, *v1 = nullptr, *rhist = nullptr;
@@ -195,8 +199,10 @@ struct msg_handle {
     float *tz32 = nullptr, *tc32 = nullptr;
     unsigned short *bst = nullptr;                    // bucket starts per type pair
     int2 *bkz = nullptr;                              // lean kernel buckets: (absolute row, its z_low)
-    size_t pair_smem_m = 0;
-    int pair_lean = 1;                                // mixed path: k_pair_m (1) or k_pair (0)
+    size_t pair_smem_m = 0, pair_smem_h = 0;
+    float *tch = nullptr;                             // k_pair_h rows (ROW16 floats: hi/lo z_low, c1, c7)
+    // mixed path: k_pair_h over a half list (2) or a full list (3), k_pair_m (1) or k_pair (0)
+    int pair_lean = 1;
     int pair_unroll = 2;                              // k_pair_m: row entries in flight per lane
     int nsm = 148;
     double *massip = nullptr, *massp = nullptr, *fac1 = nullptr, *fac2 = nullptr;
@@ -206,6 +212,10 @@ struct msg_handle {
     double *bk = nullptr, *beq = nullptr;
     // Ewald sums: any_ewald = any system with one (SPME or standard), any_spme / any_std by method
     int any_ewald = 0, any_spme = 0, any_std = 0;
+    // lvlistllist: per-particle linked-list cell and SetNCell probe sets (k_llist_info)
+    int any_llist = 0;
+    int4 *llinfo = nullptr;
+    unsigned *istep2 = nullptr;       // per system: steps since NList(iBeforeMacrostep)
     // standard Ewald: k-vectors, tables, partial and full structure factors, force slices, work items
     int4 *ew_kv = nullptr, *ew_kitems = nullptr, *ew_fitems = nullptr;
     unsigned *ew_tiledone = nullptr;   // per k tile: chunks finished this step
@@ -327,7 +337,7 @@ struct msg_handle {
     int pair_blocks_max = 1, pair_blocks_lean = 1, pair_shift = 0;
     std::vector<PairTask> make_pair_tasks(int shift) const;
     void set_pair_chunks(const std::vector<PairTask> &pt, bool replace);
-    void set_pair_lanes(int shift);
+    void set_pair_lanes(int shift, bool force = false);
     void set_lean_grid(int nsm);
 
     ~msg_handle();
@@ -418,7 +428,7 @@ static void free_all(msg_handle *h)
 {
     void *ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->acc[0], h->acc[1], h->dsum[0], h->dsum[1],
                     h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
-                    h->sysid, h->fsr, h->ftot, h->posfx, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
+                    h->sysid, h->fsr, h->fpart, h->ftot, h->posfx, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
                     h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->flag, h->nrebuild,
                     h->t128, h->ptask, h->psrange, h->psched, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
@@ -428,7 +438,7 @@ static void free_all(msg_handle *h)
                     h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
                     h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig,
                     h->mc_jumpt, h->mca_psave, h->mca_esave, h->mca_beta, h->mca_acc, h->mca_step,
-                    h->mca_flag};
+                    h->mca_flag, h->llinfo, h->istep2, h->tch};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -490,6 +500,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
 {
     nsys = n;
     prec = precision;
+    // the mixed path streams a half list by default (k_pair_h); the FP64 path a full list
+    pair_lean = prec == MSG_PREC_MIXED ? 2 : 1;
+    list_half = pair_lean == 2 ? 1 : 0;
     if (!dry) {
         CK(cudaGetDevice(&dev));
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -528,8 +541,26 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             throw CudaError{MSG_ERR_ARG, "standard Ewald needs 1 <= ncut <= 100 and ncutregion 0 (sphere) or 1 (cube)"};
         if (!p.iptpn || !p.az || !p.masspt || !p.ubuf || !p.iubuflow || !p.r2umin)
             throw CudaError{MSG_ERR_ARG, "iptpn, az, masspt, ubuf, iubuflow and r2umin are required"};
+        if (p.inlist < 0) throw CudaError{MSG_ERR_ARG, "inlist negative"};   // NList's Stop, Src/nlist.F90:619
+        if (p.lvlistllist != 0 && p.lvlistllist != 1) throw CudaError{MSG_ERR_ARG, "lvlistllist must be 0 or 1"};
         SysDev &S = hs[s];
         std::memset(&S, 0, sizeof(S));
+        S.inlist = p.inlist;
+        if (p.lvlistllist) {
+            // SetLList(rcut+drnlist): ndivllist = int(boxlen/distance), celli = real(ndivllist)*boxleni
+            const double dist = p.rcut + p.drnlist;
+            long long nc = 1;
+            for (int d = 0; d < 3; ++d) {
+                S.lnd[d] = (int)(p.boxlen[d] / dist);
+                S.lcelli[d] = (double)(float)S.lnd[d] * (1.0 / p.boxlen[d]);
+                nc *= S.lnd[d];
+            }
+            if (nc < 1 || nc > 1000)
+                throw CudaError{MSG_ERR_ARG, "lvlistllist needs 1 to 1000 linked-list cells (Src/nlist.F90:1195)"};
+            S.llist = 1;
+            S.lrcut = p.rcut;
+            any_llist = 1;
+        }
         S.n = p.np;
         S.off = ntot;
         S.npt = p.npt;
@@ -548,7 +579,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         for (int d = 0; d < 3; ++d) {
             S.fxs[d] = 4294967296.0 / p.boxlen[d];
             S.fxi[d] = (float)(p.boxlen[d] / 4294967296.0);
+            S.fxd[d] = p.boxlen[d] / 4294967296.0;
         }
+        S.fx_cubic = (p.boxlen[0] == p.boxlen[1] && p.boxlen[0] == p.boxlen[2]) ? 1 : 0;
+        S.fx2f = (float)(S.fxd[0] * S.fxd[0]);
         S.rcut2 = p.rcut * p.rcut;
         const double rl = p.rcut + p.drnlist;
         S.rs2cut = rl * rl;
@@ -561,7 +595,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         cell_tot += S.ncell[0] * S.ncell[1] * S.ncell[2];
         const double dens = p.np / S.vol;
         const double vshell = 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl;
-        int cap = (int)std::ceil(2.0 * dens * vshell) + 64;
+        int cap = (int)std::ceil((list_half ? 1.0 : 2.0) * dens * vshell) + 64;
         if (p.maxnneigh > 0) cap = std::max(cap, (int)p.maxnneigh);
         cap = std::min(cap, ((p.np + 7) / 8) * 8);
         cap = std::max(cap, 8);
@@ -639,13 +673,14 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             }
         grid_tot = go;
         cgrid_tot = co;
+        // the forward transform is FP64 in both precisions (reciprocal energy and virial);
+        // the mixed path transforms back in FP32
+        igrid = dalloc<unsigned long long>(grid_tot);
+        rgrid = dalloc<double>(grid_tot);
+        cgrid = dalloc<double2>(cgrid_tot);
         if (prec == MSG_PREC_MIXED) {
-            igrid = dalloc<unsigned long long>(grid_tot);
             rgrid32 = dalloc<float>(grid_tot);
             cgrid32 = dalloc<float2>(cgrid_tot);
-        } else {
-            rgrid = dalloc<double>(grid_tot);
-            cgrid = dalloc<double2>(cgrid_tot);
         }
         std::vector<double> hm(fo_acc), he(fo_acc), hv(fo_acc);
         for (int s = 0; s < n && !dry; ++s)
@@ -840,6 +875,9 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             const size_t bm = lean_smem_bytes(S.tab_nk, S.natat * MSG_NBUCKET);
             S.tab_smem_m = bm <= 96 * 1024 ? 1 : 0;
             if (S.tab_smem_m) pair_smem_m = std::max(pair_smem_m, bm);
+            const size_t bh = lean_smem_bytes(S.tab_nk, S.natat * MSG_NBUCKET, ROW16);
+            S.tab_smem_h = bh <= 96 * 1024 ? 1 : 0;
+            if (S.tab_smem_h) pair_smem_h = std::max(pair_smem_h, bh);
         }
         S.r2umin_max = 0.0;
         S.r2atat_max = 0.0;
@@ -898,6 +936,26 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         tc32 = dalloc<float>(fc.size());
         up(tz32, fz.data(), fz.size() * sizeof(float));
         up(tc32, fc.data(), fc.size() * sizeof(float));
+        if (prec == MSG_PREC_MIXED) {
+            // rows of k_pair_h: z_low, c1 and c7 as FP32 (hi, lo) pairs
+            const size_t nk = vc.size() / 12;
+            std::vector<float> fh(nk * ROW16, 0.0f);
+            for (size_t k = 0; k < nk; ++k) {
+                const double *c = vc.data() + 12 * k;
+                float *o = fh.data() + ROW16 * k;
+                auto split = [](double v, float *hl) {
+                    hl[0] = (float)v;
+                    hl[1] = (float)(v - (double)hl[0]);
+                };
+                split(c[0], o);
+                split(c[1], o + 2);
+                for (int q = 2; q <= 6; ++q) o[2 + q] = (float)c[q];
+                split(c[7], o + 9);
+                for (int q = 8; q <= 11; ++q) o[3 + q] = (float)c[q];
+            }
+            tch = dalloc<float>(fh.size());
+            up(tch, fh.data(), fh.size() * sizeof(float));
+        }
     }
     up(massip, vmassip.data(), type_tot * sizeof(double));
     up(massp, vmassp.data(), type_tot * sizeof(double));
@@ -983,6 +1041,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     inv = dalloc<int>(ntot);
     sysid = dalloc<int>(ntot);
     fsr = dalloc<double4>(ntot);
+    if (prec == MSG_PREC_MIXED) fpart = dalloc<unsigned long long>(3 * (size_t)ntot);
     ftot = dalloc<double4>(ntot);
     posfx = dalloc<int4>(ntot);
     {
@@ -1026,6 +1085,8 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     sc = dalloc<SkinChunk>(nchunk);
     flag = dalloc<int>(n);
     nrebuild = dalloc<long long>(n);
+    istep2 = dalloc<unsigned>(n);
+    if (any_llist) llinfo = dalloc<int4>(ntot);
     eacc = dalloc<long long>((size_t)n * EA_N);
     esys = dalloc<double>((size_t)n * ESZ);
     stepctr = dalloc<unsigned long long>(1);
@@ -1065,8 +1126,15 @@ void msg_handle::set_lean_grid(int nsm)
     int perm = 0;
 #define MSG_LEAN_OCC(NTV, UV)                                                                                \
     do {                                                                                                     \
+        int ph = 0;                                                                                          \
         CK(cudaFuncSetAttribute(k_pair_m<NTV, UV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024)); \
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perm, k_pair_m<NTV, UV>, PAIR_BLOCK, pair_smem_m)); \
+        CK(cudaFuncSetAttribute(k_pair_h<NTV, UV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024)); \
+        CK(cudaFuncSetAttribute(k_pair_h<NTV, UV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024)); \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ph, k_pair_h<NTV, UV, true>, PAIR_BLOCK, pair_smem_h)); \
+        perm = std::min(perm, ph);                                                                           \
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ph, k_pair_h<NTV, UV, false>, PAIR_BLOCK, pair_smem_h)); \
+        perm = std::min(perm, ph);                                                                           \
     } while (0)
     if (max_npt <= 2) {
         if (pair_unroll == 1) MSG_LEAN_OCC(2, 1); else if (pair_unroll == 2) MSG_LEAN_OCC(2, 2); else MSG_LEAN_OCC(2, 4);
@@ -1086,7 +1154,7 @@ std::vector<PairTask> msg_handle::make_pair_tasks(int shift) const
     for (int s = 0; s < nsys; ++s) {
         const SysDev &S = hs[s];
         const double rl = std::sqrt(S.rs2cut);
-        const double nrow = S.n / S.vol * 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl;
+        const double nrow = S.n / S.vol * 4.0 / 3.0 * 3.1415926535897932 * rl * rl * rl * (list_half ? 0.5 : 1.0);
         int G = 4;
         while (G < 32 && 2 * G <= nrow / 4.0) G *= 2;
         for (int k = 0; k < shift && G < 32; ++k) G *= 2;
@@ -1114,9 +1182,9 @@ void msg_handle::set_pair_chunks(const std::vector<PairTask> &pt, bool replace)
     up(psrange, r.data(), r.size() * sizeof(int2));
 }
 
-void msg_handle::set_pair_lanes(int shift)
+void msg_handle::set_pair_lanes(int shift, bool force)
 {
-    if (shift == pair_shift) return;
+    if (shift == pair_shift && !force) return;
     drop_graph();
     CK(cudaStreamSynchronize(st));
     std::vector<PairTask> pt = make_pair_tasks(shift);
@@ -1150,7 +1218,8 @@ void msg_handle::plan_fft()
             go += rs * c;
             co += cs * c;
             for (int dir = 1; dir >= 0; --dir) {
-                const PlanKey key{fc.s, c, f32, dir};
+                // forward D2Z in both precisions; backward C2R (mixed) or Z2D (FP64)
+                const PlanKey key{fc.s, c, dir ? 0 : f32, dir};
                 cufftHandle hp = 0;
                 size_t ws = 0;
                 if (dry) {
@@ -1163,11 +1232,11 @@ void msg_handle::plan_fft()
                         ws = it->second;
                     } else {
                         int dims[3] = {fc.s, fc.s, fc.s};
-                        const cufftType t = dir ? (f32 ? CUFFT_R2C : CUFFT_D2Z) : (f32 ? CUFFT_C2R : CUFFT_Z2D);
+                        const cufftType t = dir ? CUFFT_D2Z : (f32 ? CUFFT_C2R : CUFFT_Z2D);
                         // without a device cuFFT cannot estimate: assume one complex grid per transform
                         if (cufftEstimateMany(3, dims, nullptr, 1, dir ? (int)rs : (int)cs, nullptr, 1,
                                               dir ? (int)cs : (int)rs, t, c, &ws) != CUFFT_SUCCESS)
-                            ws = (size_t)c * (size_t)cs * (f32 ? sizeof(float2) : sizeof(double2));
+                            ws = (size_t)c * (size_t)cs * (key.f32 ? sizeof(float2) : sizeof(double2));
                         est_cache[key] = ws;
                     }
                 } else {
@@ -1205,7 +1274,7 @@ void msg_handle::release_fft()
     std::lock_guard<std::mutex> lk(g_plan_mu);
     for (auto &fc : fft)
         for (auto &pt : fc.parts) {
-            if (pt.fwd) g_plan_idle[PlanKey{fc.s, pt.count, f32, 1}].push_back({pt.fwd, pt.ws_fwd});
+            if (pt.fwd) g_plan_idle[PlanKey{fc.s, pt.count, 0, 1}].push_back({pt.fwd, pt.ws_fwd});
             if (pt.bwd) g_plan_idle[PlanKey{fc.s, pt.count, f32, 0}].push_back({pt.bwd, pt.ws_bwd});
         }
     fft.clear();
@@ -1227,8 +1296,12 @@ void msg_handle::enqueue_rebuild()
                                       ntot);
     k_copyback<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1], fo[0],
                                        fo[1], typ[0], typ[1], orig[0], orig[1], dsum[0], posfx);
+    if (any_llist) {
+        k_llist_info<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], llinfo);
+        launches += 1;
+    }
     k_nlist<<<(ntot * 32 + 255) / 256, 256, 0, st>>>(dsys, sysid, flag, pos[0], typ[0], cellid, cstart, cend, nbl,
-                                                     nnb, ntot, nmaxrow, errw);
+                                                     nnb, ntot, nmaxrow, errw, list_half, orig[0], llinfo);
     tend(TM_REBUILD);
     launches += 4 + nsort;
 }
@@ -1237,25 +1310,16 @@ template <int P, class PR>
 static void launch_spme(msg_handle *h)
 {
     h->tbeg(TM_SPREAD);
-    if (!PR::mixed) CK(cudaMemsetAsync(h->rgrid, 0, sizeof(double) * h->grid_tot, h->st));
     k_spread<P, PR><<<h->nt128 * (128 / SPREAD_PART), SPREAD_THREADS, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->rgrid, h->igrid,
                                                   h->eacc);
     h->launches += 1;
-    if (PR::mixed) {
-        k_grid_to_f32<<<(unsigned)((h->grid_tot + 255) / 256), 256, 0, h->st>>>(h->igrid, h->rgrid32, h->grid_tot);
-        h->launches += 1;
-    }
+    k_grid_to_f64<<<(unsigned)((h->grid_tot + 255) / 256), 256, 0, h->st>>>(h->igrid, h->rgrid, h->grid_tot);
+    h->launches += 1;
     h->tend(TM_SPREAD);
     h->tbeg(TM_FFT);
     for (auto &fc : h->fft)
-        for (auto &f : fc.parts) {
-            if (PR::mixed)
-                CKF(cufftExecR2C(f.fwd, h->rgrid32 + f.grid_off,
-                                 reinterpret_cast<cufftComplex *>(h->cgrid32 + f.cgrid_off)));
-            else
-                CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off,
-                                 reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
-        }
+        for (auto &f : fc.parts)
+            CKF(cufftExecD2Z(f.fwd, h->rgrid + f.grid_off, reinterpret_cast<cufftDoubleComplex *>(h->cgrid + f.cgrid_off)));
     h->tend(TM_FFT);
     h->tbeg(TM_INFL);
     k_influence<PR><<<h->ninfl, INFL_THREADS, 0, h->st>>>(h->dsys, h->infl, h->cgrid, h->cgrid32, h->mfac, h->emf,
@@ -1290,7 +1354,8 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
     h->tbeg(TM_FINAL);
     h->launches += 1;
     k_finalize<P, PR><<<h->nt128, FIN_THREADS, 0, h->st>>>(
-        h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->ew_fks, h->eacc, h->massip, h->massp,
+        h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->list_half ? h->fpart : nullptr,
+        h->ntot, h->ew_fks, h->eacc, h->massip, h->massp,
         h->ftot, h->fo[0], h->vel[0], h->acc[0], mode, fo, h->errw);
     h->tend(TM_FINAL);
 }
@@ -1333,7 +1398,7 @@ static void launch_forces(msg_handle *h, int mode, bool record, bool skin)
     if (skin) {
         // the skin test's combine: needed only by the rebuild at the end of the step
         k_skin_combine<<<h->nsys, SK_THREADS, 0, ps>>>(h->dsys, h->r2o, h->sc, h->flag, h->nrebuild, h->skinout,
-                                                       h->cond, h->use_cond);
+                                                       h->cond, h->use_cond, h->istep2);
         h->launches += 1;
     }
     h->tbeg(TM_PAIR);
@@ -1341,7 +1406,29 @@ static void launch_forces(msg_handle *h, int mode, bool record, bool skin)
         reinterpret_cast<const typename PR::V4 *>(PR::mixed ? (const void *)h->posfx : (const void *)h->pos[0]);
     const typename PR::R *tzp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tz32 : (const void *)h->tz);
     const typename PR::R *tcp = reinterpret_cast<const typename PR::R *>(PR::mixed ? (const void *)h->tc32 : (const void *)h->tc);
-    if (PR::mixed && h->pair_lean) {
+    if (PR::mixed && h->pair_lean >= 2) {
+        const int per_sm = h->pair_per_sm > 0 ? h->pair_per_sm : (par ? 2 : 0);
+        const int cap = per_sm > 0 ? std::min(h->pair_blocks_lean, h->nsm * per_sm) : h->pair_blocks_lean;
+        const int grid = std::max(1, std::min(h->nptask, cap));
+#define MSG_HALF1(NTV, UV, HV)                                                                              \
+    k_pair_h<NTV, UV, HV><<<grid, PAIR_BLOCK, h->pair_smem_h, ps>>>(h->dsys, h->ptask, h->psrange, h->nsys,    \
+                                                                    h->nptask, h->psched, h->posfx, h->typ[0], \
+                                                                    h->nbl, h->nnb, h->ptmap, h->ptab, h->tch, \
+                                                                    h->bkz, h->fsr, h->fpart, h->ntot, h->eacc, \
+                                                                    h->errw)
+#define MSG_HALF(NTV, UV)                          \
+    do {                                           \
+        if (h->list_half) MSG_HALF1(NTV, UV, true); \
+        else MSG_HALF1(NTV, UV, false);            \
+    } while (0)
+        if (h->max_npt <= 2) {
+            if (h->pair_unroll == 1) MSG_HALF(2, 1); else if (h->pair_unroll == 2) MSG_HALF(2, 2); else MSG_HALF(2, 4);
+        } else {
+            if (h->pair_unroll == 1) MSG_HALF(4, 1); else if (h->pair_unroll == 2) MSG_HALF(4, 2); else MSG_HALF(4, 4);
+        }
+#undef MSG_HALF
+#undef MSG_HALF1
+    } else if (PR::mixed && h->pair_lean) {
         // beside the SPME chain the pair kernel leaves room on each SM for the chain's blocks
         const int per_sm = h->pair_per_sm > 0 ? h->pair_per_sm : (par ? 2 : 0);
         const int cap = per_sm > 0 ? std::min(h->pair_blocks_lean, h->nsm * per_sm) : h->pair_blocks_lean;
@@ -1843,6 +1930,16 @@ static int put_state(msg_handle *h, int32_t isys, const double *ro, const double
     return h->check();
 }
 
+extern "C" int msg_nlist_before_macrostep(msg_handle *h)
+{
+    if (!h) return MSG_ERR_ARG;
+    API_BEGIN
+    CK(cudaMemsetAsync(h->dsum[0], 0, sizeof(double4) * h->ntot, h->st));
+    CK(cudaMemsetAsync(h->istep2, 0, sizeof(unsigned) * h->nsys, h->st));
+    return h->check();
+    API_END
+}
+
 extern "C" int msg_set_state(msg_handle *h, int32_t isys, const double *ro, const double *rod, const double *rodd)
 {
     if (!h || isys < 0 || isys >= h->nsys) return MSG_ERR_ARG;
@@ -1899,22 +1996,25 @@ extern "C" int msg_build_nlist(msg_handle *h, int32_t isys, int32_t *nneighpn, i
         h->down(nn.data(), h->nnb + S.off, S.n * sizeof(int));
         long long tot = 0;
         for (int v : nn) tot += v;
-        *npair = tot / 2;
+        *npair = h->list_half ? tot : tot / 2;
     }
     if (nneighpn && jpnlist) {
         if (maxnneigh < 1) return MSG_ERR_ARG;
         int *dn = h->dalloc<int>(S.n);
-        int *dj = h->dalloc<int>((size_t)S.n * maxnneigh);
-        const int warps = 4;
-        k_export_nlist<<<(S.n + warps - 1) / warps, 32 * warps, warps * S.cap * sizeof(int), h->st>>>(
-            h->dsys, isys, h->nbl, h->nnb, h->orig[h->cur], dn, dj, maxnneigh, h->errw);
+        long long *dj = h->dalloc<long long>((size_t)S.n * maxnneigh);
+        int *ds = h->dalloc<int>((size_t)S.n * maxnneigh);
+        const unsigned nb = (unsigned)(((long long)S.n * 32 + 255) / 256);
+        k_export_scatter<<<nb, 256, 0, h->st>>>(h->dsys, isys, h->nbl, h->nnb, h->orig[h->cur], h->list_half,
+                                                h->llinfo, dn, dj, maxnneigh, h->errw);
+        k_export_sort<<<nb, 256, 0, h->st>>>(S.n, dn, dj, ds, maxnneigh);
         rc = h->check();
         if (!rc) {
             h->down(nneighpn, dn, S.n * sizeof(int));
-            h->down(jpnlist, dj, (size_t)S.n * maxnneigh * sizeof(int));
+            h->down(jpnlist, ds, (size_t)S.n * maxnneigh * sizeof(int));
         }
         h->dfree(dn);
         h->dfree(dj);
+        h->dfree(ds);
         return rc;
     }
     return MSG_OK;
@@ -2015,10 +2115,19 @@ extern "C" int msg_tune(msg_handle *h, int32_t key, int32_t value)
         return MSG_OK;
     }
     if (key == MSG_TUNE_PAIR_KERNEL) {
-        if (value != 0 && value != 1) return MSG_ERR_ARG;
+        if (value < 0 || value > 3 || (value >= 2 && h->prec != MSG_PREC_MIXED)) return MSG_ERR_ARG;
         if (h->pair_lean != value) {
             h->drop_graph();
+            const int half = value == 2 ? 1 : 0;
             h->pair_lean = value;
+            if (half != h->list_half) {
+                // the other list layout: new task sizes and every placed system's list rebuilt
+                h->list_half = half;
+                h->set_pair_lanes(h->pair_shift, true);
+                std::vector<int> all(h->placed.begin(), h->placed.end());
+                const int rc = h->rebuild_checked(all);
+                if (rc) return rc;
+            }
         }
         return MSG_OK;
     }

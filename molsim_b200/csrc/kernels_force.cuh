@@ -30,9 +30,12 @@ __device__ __forceinline__ void block_dipole(double qx, double qy, double qz, lo
 
 // ---------------------------------------------------------------------------
 // SPME charge spreading (Src/energy.F90:1226-1245): Q(k - i) += q*Mx*My*Mz.
-// PrecD: FP64 atomics into the FP64 grid.  PrecM: FP32 splines, each
-// contribution rounded to 2^-40 and added as a 64-bit integer, so the grid is
-// the same whatever order the atomics land in.
+// Each contribution is rounded to 2^-40 e and added as a 64-bit integer, so the
+// grid is the same whatever order the atomics land in (results repeat bit for
+// bit, alone or batched).  The splines are FP64 in both precisions: the charge
+// grid feeds the reciprocal energy and virial, which stay FP64.  A conversion
+// kernel then turns the integer grid into the FP64 input of the forward FFT and
+// clears it.
 // A block takes SPREAD_PART particles: one thread per particle forms the
 // splines into shared memory, then the block walks the particles' P^3
 // contributions x-fastest, so the lanes of a warp add into runs of P
@@ -47,7 +50,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(const SysDev *__restr
                                                            const double4 *__restrict__ pos, double *__restrict__ grid,
                                                            unsigned long long *__restrict__ igrid, long long *__restrict__ eacc)
 {
-    using R = typename PR::R;
+    using R = double;
     __shared__ R sth[SPREAD_PART][3][P];
     __shared__ int skm[SPREAD_PART][3];
     __shared__ R sq[SPREAD_PART];
@@ -80,21 +83,19 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(const SysDev *__restr
         nz += (nz < 0) ? s : 0;
         const R v = sq[pp] * sth[pp][2][iz] * sth[pp][1][iy] * sth[pp][0][ix];
         const size_t at = S.grid_off + ((size_t)nz * s + ny) * s + nx;
-        if (PR::mixed)
-            atomicAdd(igrid + at, (unsigned long long)__double2ll_rn((double)v * kGridFix));
-        else
-            atomicAdd(grid + at, (double)v);
+        atomicAdd(igrid + at, (unsigned long long)__double2ll_rn((double)v * kGridFix));
     }
+    (void)grid;
     if (S.lsurf) block_dipole(x.w * x.x, x.w * x.y, x.w * x.z, eacc + (size_t)T.sys * EA_N);
 }
 
-// Mixed path: fixed-point grid -> FP32 grid for the FP32 FFT, clearing the
-// fixed-point grid for the next step.
-__global__ void k_grid_to_f32(unsigned long long *__restrict__ igrid, float *__restrict__ g, long long n)
+// Fixed-point grid -> FP64 grid for the forward FFT, clearing the fixed-point
+// grid for the next step.
+__global__ void k_grid_to_f64(unsigned long long *__restrict__ igrid, double *__restrict__ g, long long n)
 {
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) {
-        g[k] = (float)((double)(long long)igrid[k] * kGridFixInv);
+        g[k] = (double)(long long)igrid[k] * kGridFixInv;
         igrid[k] = 0ull;
     }
 }
@@ -103,7 +104,10 @@ __global__ void k_grid_to_f32(unsigned long long *__restrict__ igrid, float *__r
 // Reciprocal-space multiply of SPMFFTRec (Src/energy.F90:6550-6578) over every
 // entry of the r2c half spectrum: F *= meshfac, E += |F|^2 * emf,
 // W -= |F|^2 * vmf, where emf/vmf carry the reference's halving at kx=0, s/2
-// and the mirror double counts in y and z are already resolved.
+// and the mirror double counts in y and z are already resolved.  The forward
+// transform is FP64 in both precisions, so E and W are FP64 sums of FP64
+// terms; the mixed path writes F * meshfac in FP32 for its FP32 backward
+// transform (the grid forces), the FP64 path in place.
 // ---------------------------------------------------------------------------
 constexpr int INFL_THREADS = 256;
 constexpr int INFL_TILE = 512;
@@ -124,20 +128,14 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence(const SysDev *__rest
         const int fy = ky <= s / 2 ? ky : s - ky, fz = kz <= s / 2 ? kz : s - kz;
         const size_t f = S.fac_off + kx + (size_t)h * (fy + (size_t)h * fz);
         const double m = mfac[f];
-        double q2;
-        if (PR::mixed) {
-            float2 q = cg32[S.cgrid_off + c];
-            q2 = (double)(q.x * q.x + q.y * q.y);
-            q.x *= (float)m;
-            q.y *= (float)m;
-            cg32[S.cgrid_off + c] = q;
-        } else {
-            double2 q = cg[S.cgrid_off + c];
-            q2 = q.x * q.x + q.y * q.y;
-            q.x *= m;
-            q.y *= m;
+        double2 q = cg[S.cgrid_off + c];
+        const double q2 = q.x * q.x + q.y * q.y;
+        q.x *= m;
+        q.y *= m;
+        if (PR::mixed)
+            cg32[S.cgrid_off + c] = make_float2((float)q.x, (float)q.y);
+        else
             cg[S.cgrid_off + c] = q;
-        }
         e += q2 * emf[f];
         v -= q2 * vmf[f];
     }
@@ -245,7 +243,8 @@ template <int P, class PR>
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
     const int *__restrict__ typ, const double *__restrict__ grid, const float *__restrict__ grid32,
-    const double4 *__restrict__ fsr, const double4 *__restrict__ fks, long long *__restrict__ eacc,
+    const double4 *__restrict__ fsr, unsigned long long *__restrict__ fpart, int fstride,
+    const double4 *__restrict__ fks, long long *__restrict__ eacc,
     const double *__restrict__ massip, const double *__restrict__ massp, double4 *__restrict__ ftot,
     double4 *__restrict__ forceo, double4 *__restrict__ vel, double4 *__restrict__ acc, int mode, FinOut out,
     ErrWord *err)
@@ -274,6 +273,16 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
         x = pos[i];
         if (g == 0) {
             f0 = fsr[i];
+            if (fpart) {
+                // partner shares of the half-list pair kernel (2^-32 fixed point), cleared for the next step
+                unsigned long long *px = fpart + i, *py = px + fstride, *pz = py + fstride;
+                f0.x += (double)(long long)*px * 2.3283064365386962890625e-10;
+                f0.y += (double)(long long)*py * 2.3283064365386962890625e-10;
+                f0.z += (double)(long long)*pz * 2.3283064365386962890625e-10;
+                *px = 0ull;
+                *py = 0ull;
+                *pz = 0ull;
+            }
             if (mode == 1) {
                 tyi = typ[i];
                 vold = vel[i];

@@ -174,11 +174,26 @@ __device__ void skin_chunk(int chunk, const double v[SK_PER], int o0, int o1, Sk
 __global__ void __launch_bounds__(SK_THREADS) k_skin_combine(
     const SysDev *__restrict__ sysv, const double *__restrict__ r2o, const SkinChunk *__restrict__ sc,
     int *__restrict__ flag, long long *__restrict__ nrebuild, double *__restrict__ skinout,
-    cudaGraphConditionalHandle cond, int use_cond)
+    cudaGraphConditionalHandle cond, int use_cond, unsigned *__restrict__ istep2)
 {
     __shared__ double smd[SK_THREADS / 32];
     const int s = blockIdx.x, t = threadIdx.x;
     const SysDev &S = sysv[s];
+    if (S.inlist > 0) {
+        // regular update interval: rebuild when mod(istep2, inlist) == 0 (Src/nlist.F90:616-617)
+        if (t == 0) {
+            const unsigned c = istep2[s] + 1u;
+            istep2[s] = c;
+            const int rebuild = (c % (unsigned)S.inlist) == 0u ? 1 : 0;
+            flag[s] = rebuild;
+            if (rebuild) {
+                nrebuild[s] += 1;
+                if (use_cond) cudaGraphSetConditional(cond, 1u);
+            }
+            if (skinout) { skinout[2 * s] = 0.0; skinout[2 * s + 1] = 0.0; }
+        }
+        return;
+    }
     // Combine the system's chunks in MOLSIM order, SK_THREADS chunks per pass.
     const int c0 = S.chunk_off;
     double carry = 0.0, m2 = 0.0;
@@ -224,6 +239,7 @@ __global__ void __launch_bounds__(SK_THREADS) k_skin_combine(
         carry = fmax(carry, block_max(bmx, smd));
     }
     if (t == 0) {
+        istep2[s] += 1u;
         const int rebuild = (sqrt(carry) + sqrt(m2) > S.drnlist) ? 1 : 0;
         flag[s] = rebuild;
         if (rebuild) {
@@ -270,10 +286,13 @@ __global__ void __launch_bounds__(SK_THREADS) k_vv_skin(
             x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
             pos[i] = x;
             if (posfx) posfx[i] = fx_pos(x, S);
-            d.x = __dadd_rn(d.x, sx);
-            d.y = __dadd_rn(d.y, sy);
-            d.z = __dadd_rn(d.z, sz);
-            dsum[i] = d;
+            if (S.inlist <= 0) {
+                // drosum += drostep only under the skin test (Src/nlist.F90:603-604)
+                d.x = __dadd_rn(d.x, sx);
+                d.y = __dadd_rn(d.y, sy);
+                d.z = __dadd_rn(d.z, sz);
+                dsum[i] = d;
+            }
             v[k] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
             r2o[o] = v[k];
         }
@@ -329,10 +348,13 @@ __global__ void __launch_bounds__(SK_THREADS) k_bd_skin(
             x.z = pbc_wrap(__dadd_rn(x.z, sz), S.half[2], S.box[2], S.boxi[2]);
             pos[i] = x;
             if (posfx) posfx[i] = fx_pos(x, S);
-            d.x = __dadd_rn(d.x, sx);
-            d.y = __dadd_rn(d.y, sy);
-            d.z = __dadd_rn(d.z, sz);
-            dsum[i] = d;
+            if (S.inlist <= 0) {
+                // drosum += drostep only under the skin test (Src/nlist.F90:603-604)
+                d.x = __dadd_rn(d.x, sx);
+                d.y = __dadd_rn(d.y, sy);
+                d.z = __dadd_rn(d.z, sz);
+                dsum[i] = d;
+            }
             v[k] = __dadd_rn(__dadd_rn(__dmul_rn(d.x, d.x), __dmul_rn(d.y, d.y)), __dmul_rn(d.z, d.z));
             r2o[o] = v[k];
         }
@@ -457,16 +479,87 @@ __device__ __forceinline__ int stencil1(int c, int nc, int *out)
     return nc;
 }
 
-// Full Verlet list, one warp per particle: every j != i in the stencil with
+// Pair (i, j) of internal indices belongs to row i of a half list: SetVListMD's
+// parity rule (Src/nlist.F90:741-744) applied to the internal order, so each
+// unordered pair is stored once and rows are balanced.
+__device__ __forceinline__ bool half_owner(int i, int j) { return (i < j) == (((i + j) & 1) != 0); }
+
+// ---------------------------------------------------------------------------
+// SetLList / SetNCell (Src/nlist.F90:1168-1260) for systems with lvlistllist.
+// Per particle: its linked-list cell (ix, iy, iz) = aint((ro + boxlen2) celli)
+// and, per dimension, the cells of SetNCell's probe points ro - rcut, ro,
+// ro + rcut after PBC.  The probes' 27 cells are the product of the three
+// per-dimension sets, so a particle j lies in a cell SetNCell marks for i iff
+// each of j's cell indices is in i's set of that dimension.  Packed 10 bits per
+// index (a grid has at most 1000 cells): x = cell, y/z/w = the x/y/z sets.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int llist_index(double r, double half, double celli, int nd)
+{
+    int c = (int)__dmul_rn(__dadd_rn(r, half), celli);
+    return min(max(c, 0), nd - 1);     // r = +boxlen2 exactly lies outside the reference's grid
+}
+
+__global__ void __launch_bounds__(128) k_llist_info(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                   const int *__restrict__ flag, const double4 *__restrict__ pos,
+                                                   int4 *__restrict__ info)
+{
+    const Tile T = tiles[blockIdx.x];
+    const SysDev &S = sysv[T.sys];
+    if (!flag[T.sys] || !S.llist) return;
+    const int j = T.i0 + threadIdx.x;
+    if (j >= T.i1) return;
+    const double4 x = pos[j];
+    const double xc[3] = {x.x, x.y, x.z};
+    int own = 0, set[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        own |= llist_index(xc[d], S.half[d], S.lcelli[d], S.lnd[d]) << (10 * d);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            // rr + idx*distance, idx = -1, 0, 1; then PBC (Src/nlist.F90:1248-1252)
+            const double q = pbc_wrap(__dadd_rn(xc[d], (double)(a - 1) * S.lrcut), S.half[d], S.box[d], S.boxi[d]);
+            set[d] |= llist_index(q, S.half[d], S.lcelli[d], S.lnd[d]) << (10 * a);
+        }
+    }
+    info[j] = make_int4(own, set[0], set[1], set[2]);
+}
+
+// Is cell `c` (packed as info.x) among the cells SetNCell marks for the particle with info A?
+__device__ __forceinline__ bool llist_marked(const int4 &A, int c)
+{
+    const int cs[3] = {A.y, A.z, A.w};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int v = (c >> (10 * d)) & 1023;
+        const int q = cs[d];
+        if (v != (q & 1023) && v != ((q >> 10) & 1023) && v != ((q >> 20) & 1023)) return false;
+    }
+    return true;
+}
+
+// SetVListMDLList's row rule (Src/nlist.F90:790-792) on 1-based MOLSIM indices: the
+// opposite rows from SetVListMD's.
+__device__ __forceinline__ bool llist_owner(int ip, int jp)
+{
+    const bool odd = ((ip + jp) & 1) != 0;
+    return ip != jp && (ip > jp ? odd : !odd);
+}
+
+// Verlet list, one warp per particle: every j != i in the stencil with
 // r2 < (rcut+drnlist)^2 (SetVListMD's test, Src/nlist.F90:746-751), compacted
 // with a warp ballot.  Rows are ordered by stencil cell, then by MOLSIM index.
+// half = 0: full list (each pair in both rows); half = 1: each pair once, in the
+// row half_owner names.  With lvlistllist a pair also needs its MOLSIM row owner
+// (SetVListMDLList's rule) to reach the partner's cell with SetNCell's probes, so
+// the list holds SetVListMDLList's pair set (which can leave out skin pairs).
 __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, const int *__restrict__ sys,
                                               const int *__restrict__ flag, const double4 *__restrict__ pos,
                                               const int *__restrict__ typ,
                                               const int *__restrict__ cellid, const int *__restrict__ cstart,
                                               const int *__restrict__ cend, int *__restrict__ nbl,
                                               int *__restrict__ nnb, int ntot, int *__restrict__ nmaxrow,
-                                              ErrWord *err)
+                                              ErrWord *err, int half, const int *__restrict__ orig,
+                                              const int4 *__restrict__ llinfo)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -482,6 +575,13 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
     int *row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
     int count = 0;
     const unsigned lt = (1u << lane) - 1u;
+    const bool ll = S.llist != 0;
+    int4 li = make_int4(0, 0, 0, 0);
+    int ip = 0;
+    if (ll) {
+        li = llinfo[i];
+        ip = orig[i] + 1;
+    }
     for (int a = 0; a < nz; ++a)
         for (int b = 0; b < ny; ++b)
             for (int e = 0; e < nx; ++e) {
@@ -490,10 +590,14 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
                 for (int jb = j0; jb < j1; jb += 32) {
                     const int j = jb + lane;
                     bool ok = false;
-                    if (j < j1 && j != i) {
+                    if (j < j1 && j != i && (!half || half_owner(i, j))) {
                         const double4 xj = pos[j];
                         double dx = __dsub_rn(xi.x, xj.x), dy = __dsub_rn(xi.y, xj.y), dz = __dsub_rn(xi.z, xj.z);
                         ok = pbcr2_exact(dx, dy, dz, S) < S.rs2cut;
+                        if (ok && ll) {
+                            const int4 lj = llinfo[j];
+                            ok = llist_owner(ip, orig[j] + 1) ? llist_marked(li, lj.x) : llist_marked(lj, li.x);
+                        }
                     }
                     const unsigned bal = __ballot_sync(0xffffffffu, ok);
                     if (ok) {
@@ -511,50 +615,72 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
     }
 }
 
-// MOLSIM-layout export of one system's list: partners owned by the parity
-// rule of SetVListMD (Src/nlist.F90:741-744), 1-based, ascending per row.
-__global__ void k_export_nlist(const SysDev *__restrict__ sysv, int s, const int *__restrict__ nbl,
-                               const int *__restrict__ nnb, const int *__restrict__ orig,
-                               int *__restrict__ nneigh_out, int *__restrict__ jp_out, int maxn,
-                               ErrWord *err)
+// MOLSIM-layout export of one system's list, pass 1: every unordered pair once
+// (every entry of a half list; the i < j entries of a full list) goes to the row
+// that MOLSIM's rule gives it -- SetVListMD's parity rule (Src/nlist.F90:741-744),
+// or SetVListMDLList's (:790-792) with lvlistllist -- at a slot taken from that
+// row's counter (nneigh_out, zeroed by the caller).  The slot holds a sort key:
+// the partner's 1-based index, preceded (high word) by its linked-list cell
+// number with lvlistllist, whose rows run cell by cell.  One warp per row.
+__device__ __forceinline__ long long export_key(const SysDev &S, int jp, const int4 *llinfo, int j)
 {
-    extern __shared__ int buf[];
+    if (!S.llist) return (long long)jp;
+    const int c = llinfo[j].x;
+    const long long cell = (c & 1023) + (long long)S.lnd[0] * (((c >> 10) & 1023) + (long long)S.lnd[1] * ((c >> 20) & 1023));
+    return (cell << 32) | (long long)jp;
+}
+
+__global__ void k_export_scatter(const SysDev *__restrict__ sysv, int s, const int *__restrict__ nbl,
+                                 const int *__restrict__ nnb, const int *__restrict__ orig, int half,
+                                 const int4 *__restrict__ llinfo, int *__restrict__ nneigh_out,
+                                 long long *__restrict__ key_out, int maxn, ErrWord *err)
+{
     const SysDev &S = sysv[s];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int li = blockIdx.x * (blockDim.x >> 5) + w;
+    const int li = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
     if (li >= S.n) return;
-    int *mine = buf + w * S.cap;
     const int i = S.off + li;
     const int ip = orig[i] + 1;
     const int *row = nbl + S.nbl_off + (long long)li * S.cap;
     const int n = nnb[i];
-    const unsigned lt = (1u << lane) - 1u;
-    int cnt = 0;
-    for (int kb = 0; kb < n; kb += 32) {
-        const int k = kb + lane;
-        int jp = 0;
-        bool ok = false;
-        if (k < n) {
-            jp = orig[row[k] & ((1 << 28) - 1)] + 1;
+    for (int k = lane; k < n; k += 32) {
+        const int j = row[k] & ((1 << 28) - 1);
+        if (!half && !(i < j)) continue;
+        const int jp = orig[j] + 1;
+        bool mine;
+        if (S.llist) {
+            mine = llist_owner(ip, jp);
+        } else {
             const int itemp = (ip + jp) % 2;
-            ok = !((ip < jp && itemp == 0) || (ip > jp && itemp != 0));
+            mine = (ip < jp && itemp != 0) || (ip > jp && itemp == 0);
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, ok);
-        if (ok) mine[cnt + __popc(bal & lt)] = jp;
-        cnt += __popc(bal);
+        const int own = mine ? ip : jp, other = mine ? jp : ip;
+        const int slot = atomicAdd(nneigh_out + own - 1, 1);
+        if (slot < maxn)
+            key_out[(long long)(own - 1) * maxn + slot] = export_key(S, other, llinfo, mine ? j : i);
+        else
+            raise_error(err, 3, s, own, slot + 1);
     }
-    __syncwarp();
-    if (cnt > maxn) {
-        if (lane == 0) raise_error(err, 3, s, ip, cnt);
-        return;
-    }
+}
+
+// Pass 2: each MOLSIM row in ascending key order (rank sort, one warp per row):
+// ascending jp for SetVListMD's rows, cell by cell then ascending jp for
+// SetVListMDLList's.
+__global__ void k_export_sort(int n, const int *__restrict__ nneigh, const long long *__restrict__ key_in,
+                              int *__restrict__ jp_out, int maxn)
+{
+    const int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    const int cnt = min(nneigh[r], maxn);
+    const long long *in = key_in + (long long)r * maxn;
+    int *out = jp_out + (long long)r * maxn;
     for (int k = lane; k < cnt; k += 32) {
-        const int v = mine[k];
-        int r = 0;
-        for (int m = 0; m < cnt; ++m) r += (mine[m] < v);
-        jp_out[(long long)(ip - 1) * maxn + r] = v;
+        const long long v = in[k];
+        int q = 0;
+        for (int m = 0; m < cnt; ++m) q += (in[m] < v);
+        out[q] = (int)(v & 0xffffffffLL);
     }
-    if (lane == 0) nneigh_out[ip - 1] = cnt;
 }
 
 // ---------------------------------------------------------------------------

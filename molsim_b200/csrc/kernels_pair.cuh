@@ -96,6 +96,44 @@ template <> struct Row12<float> {
     }
 };
 
+// Row of the half-list kernel's table: 16 floats, [z_hi, z_lo, c1_hi, c1_lo, c2..c6,
+// c7_hi, c7_lo, c8..c11, 0], the interval's z_low, u(z_low) and f(z_low) each as an
+// FP32 pair whose sum is the FP64 value to 2^-48 (Src/potential.F90:1192-1207 layout
+// otherwise).  With them d = r2 - z_low and the two polynomials' leading terms carry
+// no FP32 rounding of the table itself.
+struct Row16 {
+    float c[16];
+    __device__ __forceinline__ void load(const float *p)
+    {
+        const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float4 v = q[k];
+            c[4 * k] = v.x;
+            c[4 * k + 1] = v.y;
+            c[4 * k + 2] = v.z;
+            c[4 * k + 3] = v.w;
+        }
+    }
+};
+constexpr int ROW16 = 16;
+
+// r2 of a pair from its exact fixed-point coordinate differences: in a cubic box
+// the exact 64-bit integer sum of squares (each square < 2^62) rounded to FP32 and
+// scaled by (box/2^32)^2 in FP32 (two roundings); otherwise in FP64, rounded once.
+// Unlike dx^2 + dy^2 + dz^2 from FP32 differences it carries no error of the
+// coordinate conversions, whose bias would reach the energy sums.
+__device__ __forceinline__ float r2_from_fix(int ax, int ay, int az, const SysDev &S)
+{
+    if (S.fx_cubic) {
+        const unsigned long long q = (unsigned long long)((long long)ax * ax) + (unsigned long long)((long long)ay * ay) +
+                                     (unsigned long long)((long long)az * az);
+        return __ull2float_rn(q) * S.fx2f;
+    }
+    const double x = (double)ax * S.fxd[0], y = (double)ay * S.fxd[1], z = (double)az * S.fxd[2];
+    return __double2float_rn(fma(x, x, fma(y, y, z * z)));
+}
+
 // Shared-memory image of a system's table: coefficient rows, then bucket
 // starts.  Sized on the host (pair_smem_bytes); systems whose table does not
 // fit read it from global memory through the same generic pointers.
@@ -105,11 +143,11 @@ __host__ __device__ inline size_t pair_smem_bytes(int nk, int nbucket)
     return (size_t)nk * 12 * sizeof(R) + (size_t)nbucket * sizeof(unsigned short);
 }
 
-// Shared-memory image of a system's table for k_pair_m: FP32 coefficient rows,
-// then (row, z_low) buckets.
-__host__ __device__ inline size_t lean_smem_bytes(int nk, int nbucket)
+// Shared-memory image of a system's table for k_pair_m (12 floats a row) and
+// k_pair_h (16): FP32 coefficient rows, then (row, z_low) buckets.
+__host__ __device__ inline size_t lean_smem_bytes(int nk, int nbucket, int rowf = 12)
 {
-    return (size_t)nk * 12 * sizeof(float) + (size_t)nbucket * sizeof(int2);
+    return (size_t)nk * rowf * sizeof(float) + (size_t)nbucket * sizeof(int2);
 }
 
 // Lanes per batch: B row segments per lane are in flight together.
@@ -613,6 +651,271 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U == 1 ? 4 : (U == 2 ? 
     }
     if (held >= 0) flush(held);
     // the last block to finish resets the task counters for the next launch
+    __shared__ bool lastb;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        lastb = atomicAdd(&sched[nsys], 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (lastb) {
+        for (int k = threadIdx.x; k <= nsys; k += blockDim.x) sched[k] = 0;
+        __threadfence();
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// FP32 pair kernel of the mixed-precision path with FP64 energy and virial sums.
+//
+// The work split, the shared-memory table, the bucket lookup and the scheduling
+// are k_pair_m's.  Each pair's r2 comes from the exact integer differences of the
+// fixed-point coordinates (r2_from_fix), and the table rows carry z_low, c1 and c7
+// as FP32 (hi, lo) pairs (Row16), so the per-pair energy and virial carry no
+// systematic FP32 error; each lane sums them in FP64 and every particle's share
+// is rounded once to 64-bit fixed point.  Forces stay FP32 per pair.
+//
+// HALF = true: the list holds each unordered pair once (the row half_owner
+// names, k_nlist with half = 1), so every pair is evaluated once: half the list
+// to stream, half the pair arithmetic.  The row particle's force is summed over
+// its G lanes and stored to fsr; the partner's force (minus the same pair term)
+// is rounded to 64-bit fixed point (2^-32 kJ/(mol A)) per pair and added with
+// one integer atomic per component into fpart (x, y, z blocks of fstride
+// entries), which k_finalize adds to fsr and clears for the next step.  Integer
+// sums do not depend on their order, so results stay bitwise reproducible and
+// identical whether a system runs alone or batched.  Each pair's energy and
+// virial count once, in the row particle's lane.
+// HALF = false: the full list (each pair from both ends), no atomics; each end
+// keeps half of the pair's energy and virial.
+// ---------------------------------------------------------------------------
+// Register budget with two particle types: three blocks of 256 per SM with one or two
+// row entries in flight per lane, two blocks with four.
+template <int NT, int U, bool HALF>
+__global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_pair_h(
+    const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, const int2 *__restrict__ srange,
+    int nsys, int ntasks, int *__restrict__ sched,
+    const int4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
+    const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
+    const float *__restrict__ tc, const int2 *__restrict__ bkz, double4 *__restrict__ fsr,
+    unsigned long long *__restrict__ fpart, int fstride, long long *__restrict__ eacc, ErrWord *err)
+{
+    extern __shared__ __align__(16) unsigned char dyn[];
+    __shared__ PairTab sP[MSG_MAX_NATAT];
+    __shared__ float4 sT[MAXT * MAXT];        // (z_lo, 1/h, end row, bucket base), the last two as int bits
+    __shared__ int sMap[MAXT * MAXT];
+    __shared__ int sNpt, sDrained;
+    const int lane = threadIdx.x & 31;
+    constexpr int NQ = tpair<NT>(NT - 1, NT - 1) + 1;
+    long long ue[NQ];
+    long long vir = 0;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) ue[q] = 0;
+    int loaded = -1;
+    const float *Tc = nullptr;
+    const int2 *Tb = nullptr;
+    int kbase = 0;
+    int held = -1;
+    auto flush = [&](int sys) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ue[q] += __shfl_xor_sync(0xffffffffu, ue[q], o);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vir += __shfl_xor_sync(0xffffffffu, vir, o);
+        long long *ea = eacc + (size_t)sys * EA_N;
+        const int npt = sNpt;
+        if (lane < npt * npt) {
+            const int ta = lane / npt, tb = lane % npt;
+            if (ta <= tb) {
+                long long v = 0;
+#pragma unroll
+                for (int a = 0; a < NT; ++a)
+#pragma unroll
+                    for (int b = a; b < NT; ++b) v += (a == ta && b == tb) ? ue[tpair<NT>(a, b)] : 0;
+                if (v) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_UTWOB + sMap[lane]), (unsigned long long)v);
+            }
+        }
+        if (lane == 31 && vir) atomicAdd(reinterpret_cast<unsigned long long *>(ea + EA_VIRPAIR), (unsigned long long)vir);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) ue[q] = 0;
+        vir = 0;
+    };
+    unsigned long long *fpx = fpart, *fpy = fpart + fstride, *fpz = fpart + 2 * (size_t)fstride;
+    int s0 = 0;
+    {
+        const int p = (int)(((long long)blockIdx.x * ntasks) / gridDim.x);
+        while (s0 + 1 < nsys && srange[s0].y <= p) ++s0;
+    }
+    for (int visit = 0; visit < nsys; ++visit) {
+        const int sys = (s0 + visit) % nsys;
+        const int2 R = srange[sys];
+        if (R.y <= R.x) continue;
+        __syncthreads();
+        if (threadIdx.x == 0) sDrained = atomicAdd(&sched[sys], 0) >= R.y - R.x;
+        __syncthreads();
+        if (sDrained) continue;
+        if (held >= 0) flush(held);
+        held = sys;
+        if (sys != loaded) {
+            __syncthreads();
+            const PairTask W0 = tasks[R.x];
+            const SysDev &Sn = sysv[W0.sys];
+            if (threadIdx.x < Sn.natat) sP[threadIdx.x] = ptab[Sn.pt_off + threadIdx.x];
+            if (threadIdx.x < Sn.npt * Sn.npt) {
+                const int q = ptmap[Sn.ptmap_off + threadIdx.x] - Sn.pt_off;
+                sMap[threadIdx.x] = q;
+                const PairTab &P = ptab[Sn.pt_off + q];
+                const int a = threadIdx.x / Sn.npt, b = threadIdx.x % Sn.npt;
+                sT[a * MAXT + b] = make_float4(P.fz_lo, P.finv_h, __int_as_float(P.k0 - Sn.tab_k0 + P.nk),
+                                               __int_as_float(q * MSG_NBUCKET));
+            }
+            kbase = Sn.tab_k0;
+            if (Sn.tab_smem_h) {
+                float *sc = reinterpret_cast<float *>(dyn);
+                int2 *sb = reinterpret_cast<int2 *>(sc + (size_t)ROW16 * Sn.tab_nk);
+                const int nc = ROW16 * Sn.tab_nk, nb = Sn.natat * MSG_NBUCKET;
+                for (int k = threadIdx.x; k < nc; k += PAIR_BLOCK) sc[k] = tc[(size_t)ROW16 * Sn.tab_k0 + k];
+                for (int k = threadIdx.x; k < nb; k += PAIR_BLOCK) sb[k] = bkz[Sn.tab_b0 + k];
+                Tc = sc;
+                Tb = sb;
+            } else {
+                Tc = tc + (size_t)ROW16 * Sn.tab_k0;
+                Tb = bkz + Sn.tab_b0;
+            }
+            if (threadIdx.x == 0) sNpt = Sn.npt;
+            loaded = W0.sys;
+        }
+        __syncthreads();
+        const SysDev &S = sysv[sys];
+        const float rcut2 = (float)S.rcut2;
+        const float lowmax = (float)fmax(S.r2umin_max, S.r2atat_max);
+        const float sx = S.fxi[0], sy = S.fxi[1], sz = S.fxi[2];
+        int nxt = 0;
+        if (lane == 0) nxt = R.x + atomicAdd(&sched[sys], 1);
+        for (;;) {
+            const int task = __shfl_sync(0xffffffffu, nxt, 0);
+            if (task >= R.y) break;
+            if (lane == 0) nxt = R.x + atomicAdd(&sched[sys], 1);
+            const PairTask W = tasks[task];
+            const int G = W.g;
+            const int g = lane & (G - 1);
+            const int i = W.i0 + lane / G;
+            const bool act = i < W.i1;
+            // forces in FP32; energies and virial of the lane's pairs in FP64
+            float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+            double vi = 0.0;
+            double ut[NT];
+#pragma unroll
+            for (int t = 0; t < NT; ++t) ut[t] = 0.0;
+            int ti = 0, n = 0;
+            int4 xi = make_int4(0, 0, 0, 0);
+            const int *row = nbl;
+            if (act) {
+                xi = pos[i];
+                ti = typ[i];
+                n = nnb[i];
+                row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
+            }
+            const float4 *sTi = sT + ti * MAXT;
+            for (int kb = g; kb < n; kb += U * G) {
+                int ee[U];
+                int4 xj[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) ee[u] = (kb + u * G < n) ? __ldg(row + kb + u * G) : -1;
+#pragma unroll
+                for (int u = 0; u < U; ++u) xj[u] = pos[ee[u] >= 0 ? (ee[u] & NBL_JMASK) : i];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (ee[u] < 0) continue;
+                    const int e = ee[u];
+                    const int j = e & NBL_JMASK;
+                    const int tj = (unsigned)e >> 28;
+                    // exact integer differences, wrapped to the minimum image
+                    const int ax = (int)((unsigned)xi.x - (unsigned)xj[u].x);
+                    const int ay = (int)((unsigned)xi.y - (unsigned)xj[u].y);
+                    const int az = (int)((unsigned)xi.z - (unsigned)xj[u].z);
+                    const float r2 = r2_from_fix(ax, ay, az, S);
+                    if (r2 > rcut2) continue;
+                    const float dx = (float)ax * sx, dy = (float)ay * sy, dz = (float)az * sz;
+                    const float4 T = sTi[tj];
+                    int bk = __float2int_rz((r2 - T.x) * T.y);
+                    bk = min(max(bk, 0), MSG_NBUCKET - 1);
+                    const int2 B = Tb[__float_as_int(T.w) + bk];
+                    int kk = min(B.x + (r2 < __int_as_float(B.y) ? 1 : 0), __float_as_int(T.z) - 1);
+                    Row16 c;
+                    c.load(Tc + (size_t)kk * ROW16);
+                    bool ok = true;
+                    if (r2 < lowmax || r2 < c.c[0]) {
+                        const PairTab &Q = sP[sMap[ti * S.npt + tj]];
+                        const int kend = Q.k0 - kbase + Q.nk;
+                        if (r2 < (float)Q.r2atat) {
+                            // hard-core overlap: u = 1e10, f = 0 (the reference leaves fsum stale here)
+#pragma unroll
+                            for (int q = 0; q < ROW16; ++q) c.c[q] = 0.0f;
+                            c.c[0] = r2;
+                            c.c[2] = 1e10f;
+                        } else if (r2 < (float)Q.r2umin) {
+                            raise_error(err, 1, W.sys, i, j);
+                            ok = false;
+                        } else {
+                            while (r2 < c.c[0]) {
+                                if (++kk >= kend) {
+                                    raise_error(err, 2, W.sys, i, j);
+                                    kk = kend - 1;
+                                    c.load(Tc + (size_t)kk * ROW16);
+                                    break;
+                                }
+                                c.load(Tc + (size_t)kk * ROW16);
+                            }
+                        }
+                    }
+                    if (!ok) continue;
+                    // d = r2 - z_low with z_low's low part; the leading coefficients' low parts
+                    // join the FP32 polynomials, their high parts are added in FP64
+                    // d = r2 - z_low with z_low's low part; the leading coefficients' low parts
+                    // join the polynomials, so u and f round once each, without bias
+                    const float d = (r2 - c.c[0]) - c.c[1];
+                    const float ulo = c.c[3] + d * (c.c[4] + d * (c.c[5] + d * (c.c[6] + d * (c.c[7] + d * c.c[8]))));
+                    const float flo = c.c[10] + d * (c.c[11] + d * (c.c[12] + d * (c.c[13] + d * c.c[14])));
+                    const float f = c.c[9] + flo;
+                    const double uu = (double)(c.c[2] + ulo);
+                    const float px = f * dx, py = f * dy, pz = f * dz;
+                    fx += px;
+                    fy += py;
+                    fz += pz;
+                    if constexpr (HALF) {
+                        // the partner's share: -f d, rounded once to 2^-32 and added as an integer
+                        atomicAdd(fpx + j, (unsigned long long)__float2ll_rn(px * -4294967296.0f));
+                        atomicAdd(fpy + j, (unsigned long long)__float2ll_rn(py * -4294967296.0f));
+                        atomicAdd(fpz + j, (unsigned long long)__float2ll_rn(pz * -4294967296.0f));
+                    }
+#pragma unroll
+                    for (int t = 0; t < NT; ++t)
+                        if (tj == t) ut[t] += uu;
+                    vi -= (double)(f * r2);
+                }
+            }
+            // a full list sees each pair from both ends: each end keeps half of it
+            constexpr double ef = HALF ? kEFix : 0.5 * kEFix;
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                const long long v = __double2ll_rn(ut[t] * ef);
+#pragma unroll
+                for (int a = 0; a < NT; ++a) ue[tpair<NT>(min(a, t), max(a, t))] += (a == ti) ? v : 0;
+            }
+            vir += __double2ll_rn(vi * ef);
+            long long ax = __float2ll_rn(fx * 4294967296.0f), ay = __float2ll_rn(fy * 4294967296.0f),
+                      az = __float2ll_rn(fz * 4294967296.0f);
+            for (int o = G >> 1; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+                az += __shfl_xor_sync(0xffffffffu, az, o);
+            }
+            if (act && g == 0)
+                fsr[i] = make_double4((double)ax * kFixInv, (double)ay * kFixInv, (double)az * kFixInv, 0.0);
+        }
+    }
+    if (held >= 0) flush(held);
     __shared__ bool lastb;
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -22,6 +22,13 @@
 //   * Every call shares the one array and leaves its contents behind.  The
 //     call clears the counter and the error word before use; calls that
 //     overlap on the GPU (two streams, two host threads) race on it.
+//   * Every call waits for its stream to finish: it reads the status word
+//     back into host memory before it returns.
+//   * The minimum image is PBCr2's rectangular-box branch (lbcbox); MOLSIM's
+//     truncated-octahedron and rhombic-dodecahedron cells are not handled.
+//   * lmc = 0 takes a half list (SetVList's MD rows: every pair once);
+//     lmc = 1 takes a full list (every pair in both rows, as MOLSIM's Monte
+//     Carlo builds it) and skips jp < ip as UTwoBodyA does under lmc.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -35,12 +42,12 @@ constexpr int kNaMaxBlocks = 1024;
 constexpr int kNaMaxParticles = kNaThreads * kNaMaxBlocks;
 constexpr int kNaPart = 11;                             // 10 type-pair energies + virial
 constexpr size_t kNaPartBytes = sizeof(double) * kNaMaxBlocks * kNaPart;
-constexpr size_t kNaScratchBytes = kNaPartBytes + 16;   // + counter, error code, two indices
+constexpr size_t kNaScratchBytes = kNaPartBytes + 16;   // + counter, error code, the offending ip and jp
 
 static __device__ __align__(256) unsigned char g_na_scratch[kNaScratchBytes];
 
 struct NaArgs {
-    int np, npt, natat, maxnneigh, nbuf;
+    int np, npt, natat, maxnneigh, nbuf, lmc;
     double box[3], half[3];
     double rcut2;
     int iubuflow[10];
@@ -50,6 +57,15 @@ struct NaArgs {
 
 __device__ __forceinline__ unsigned *na_counter(unsigned char *s) { return (unsigned *)(s + kNaPartBytes); }
 __device__ __forceinline__ int *na_err(unsigned char *s) { return (int *)(s + kNaPartBytes + 4); }
+
+// The first status raised wins; it keeps the 1-based ip and jp of its pair (0 where none).
+__device__ __forceinline__ void na_raise(unsigned char *s, int code, int ip1, int jp1)
+{
+    if (atomicCAS(na_err(s), 0, code) == 0) {
+        na_err(s)[1] = ip1;
+        na_err(s)[2] = jp1;
+    }
+}
 
 __global__ void k_na_clear(double *__restrict__ force, int n3, unsigned char *scratch)
 {
@@ -85,19 +101,25 @@ __global__ void __launch_bounds__(kNaThreads) k_na_pair(NaArgs A, const double *
     if (ip < A.np) {
         ti = iptpn[ip] - 1;
         if (ti < 0 || ti >= A.npt) {
-            atomicCAS(na_err(scratch), 0, MSG_ERR_ARG);
+            na_raise(scratch, MSG_ERR_ARG, ip + 1, 0);
             ti = 0;
         }
         const double xi = ro[3 * ip], yi = ro[3 * ip + 1], zi = ro[3 * ip + 2];
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        const int n = min(nneighpn[ip], A.maxnneigh);
+        int n = nneighpn[ip];
+        if (n < 0 || n > A.maxnneigh) {
+            // a row longer than jpnlist holds: SetVListMD would have stopped (Src/nlist.F90:752)
+            na_raise(scratch, MSG_ERR_ARG, ip + 1, 0);
+            n = 0;
+        }
         const int *row = jpnlist + (size_t)ip * A.maxnneigh;
         for (int k = 0; k < n; ++k) {
             const int jp = row[k] - 1;
             if (jp < 0 || jp >= A.np) {
-                atomicCAS(na_err(scratch), 0, MSG_ERR_ARG);
+                na_raise(scratch, MSG_ERR_ARG, ip + 1, jp + 1);
                 continue;
             }
+            if (A.lmc && jp < ip) continue;     // full list: each pair once (Src/energy.F90:466-468)
             double dx = xi - ro[3 * jp], dy = yi - ro[3 * jp + 1], dz = zi - ro[3 * jp + 2];
             if (fabs(dx) > A.half[0]) dx = __dsub_rn(dx, copysign(A.box[0], dx));
             if (fabs(dy) > A.half[1]) dy = __dsub_rn(dy, copysign(A.box[1], dy));
@@ -106,7 +128,7 @@ __global__ void __launch_bounds__(kNaThreads) k_na_pair(NaArgs A, const double *
             if (r2 > A.rcut2) continue;
             const int tj = iptpn[jp] - 1;
             if (tj < 0 || tj >= A.npt) {
-                atomicCAS(na_err(scratch), 0, MSG_ERR_ARG);
+                na_raise(scratch, MSG_ERR_ARG, ip + 1, jp + 1);
                 continue;
             }
             const int p = A.pidx[ti * 4 + tj];
@@ -114,10 +136,7 @@ __global__ void __launch_bounds__(kNaThreads) k_na_pair(NaArgs A, const double *
             if (r2 < A.r2atat[p]) {
                 usum = 1e10;
             } else if (r2 < A.r2umin[p]) {
-                if (atomicCAS(na_err(scratch), 0, MSG_ERR_TABLE_MIN) == 0) {
-                    na_err(scratch)[1] = ip + 1;
-                    na_err(scratch)[2] = jp + 1;
-                }
+                na_raise(scratch, MSG_ERR_TABLE_MIN, ip + 1, jp + 1);     // StopUTwoBodyA
                 continue;
             } else {
                 int ib = A.iubuflow[p];
@@ -127,7 +146,7 @@ __global__ void __launch_bounds__(kNaThreads) k_na_pair(NaArgs A, const double *
                     if (ib + 11 > A.nbuf) { bad = true; break; }
                 }
                 if (bad) {
-                    atomicCAS(na_err(scratch), 0, MSG_ERR_TABLE_RANGE);
+                    na_raise(scratch, MSG_ERR_TABLE_RANGE, ip + 1, jp + 1);   // StopIbuf
                     continue;
                 }
                 const double *c = ubuf + ib - 1;
@@ -218,12 +237,15 @@ cudaError_t na_scratch(unsigned char **out)
 
 extern "C" int msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen[3], double rcut,
                                     const double *ro, const int32_t *iptpn, const int32_t *nneighpn,
-                                    const int32_t *jpnlist, int32_t maxnneigh, const double *ubuf, int32_t nbuf,
-                                    const int32_t *iubuflow, const double *r2umin, const double *r2atat,
-                                    double *force, double *utwob, double *virial, void *stream)
+                                    const int32_t *jpnlist, int32_t maxnneigh, int32_t lmc, const double *ubuf,
+                                    int32_t nbuf, const int32_t *iubuflow, const double *r2umin,
+                                    const double *r2atat, double *force, double *utwob, double *virial,
+                                    int32_t *stop_ipjp, void *stream)
 {
+    if (stop_ipjp) stop_ipjp[0] = stop_ipjp[1] = 0;
     if (np < 1 || np > kNaMaxParticles || npt < 1 || npt > 4 || maxnneigh < 1 || nbuf < 12 || !boxlen || !ro ||
-        !iptpn || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin || !force || !utwob || !virial)
+        !iptpn || !nneighpn || !jpnlist || !ubuf || !iubuflow || !r2umin || !force || !utwob || !virial ||
+        (lmc != 0 && lmc != 1))
         return MSG_ERR_ARG;
     NaArgs A = {};
     A.np = np;
@@ -231,6 +253,7 @@ extern "C" int msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen
     A.natat = npt * (npt + 1) / 2;
     A.maxnneigh = maxnneigh;
     A.nbuf = nbuf;
+    A.lmc = lmc;
     for (int d = 0; d < 3; ++d) {
         A.box[d] = boxlen[d];
         A.half[d] = boxlen[d] / 2.0;
@@ -259,5 +282,9 @@ extern "C" int msg_utwobody_noalloc(int32_t np, int32_t npt, const double boxlen
     if (cudaMemcpyAsync(err, scratch + kNaPartBytes + 4, sizeof(err), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return MSG_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return MSG_ERR_CUDA;
+    if (stop_ipjp && err[0]) {
+        stop_ipjp[0] = err[1];
+        stop_ipjp[1] = err[2];
+    }
     return err[0];
 }

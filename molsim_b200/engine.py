@@ -188,7 +188,8 @@ class Engine:
                          _p(k["fac2"], C.c_double) if "fac2" in k else null, int(maxnneigh),
                          int(t.get("ncut", s.get("ncut", 0)) or 0),
                          1 if s.get("ncutregion", "sphere") == "cube" else 0,
-                         int(bool(s.get("lewald2dlc", False))))
+                         int(bool(s.get("lewald2dlc", False))), int(s.get("inlist", 0)),
+                         int(bool(s.get("lvlistllist", False))))
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -252,6 +253,12 @@ class Engine:
     def tune_pair_lanes(self, shift):
         """Lanes per particle in the pair kernel scaled by 2**shift (results move by rounding only)."""
         self._check(_lib.lib().msg_tune(self.h, _lib.MSG_TUNE_PAIR_LANES, int(shift)))
+
+    def tune_pair_kernel(self, kind):
+        """Pair kernel of a mixed-precision handle: 2 the half-list kernel (default: each pair
+        stored and evaluated once, partner forces as fixed-point atomics), 1 the full-list lean
+        kernel, 0 the generic full-list kernel.  Switching list layouts rebuilds the lists."""
+        self._check(_lib.lib().msg_tune(self.h, _lib.MSG_TUNE_PAIR_KERNEL, int(kind)))
 
     def GetLinAcc(self):
         self._check(_lib.lib().msg_get_linacc(self.h))
@@ -336,6 +343,10 @@ class Engine:
         for k, a in zip(("ro", "rod", "rodd"), arrs):
             state[k] = a
         return [e[k].as_dict(self.natat[isys]) for k in range(nsteps)] if energies else None
+
+    def nlist_before_macrostep(self):
+        """NList(iBeforeMacrostep) for every system: drosum = 0, istep2 restarts."""
+        self._check(_lib.lib().msg_nlist_before_macrostep(self.h))
 
     def nrebuild(self, isys=0):
         return _lib.lib().msg_nrebuild(self.h, isys)

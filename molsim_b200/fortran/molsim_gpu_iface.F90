@@ -38,6 +38,8 @@ module MolsimGpu
       integer(c_int32_t) :: maxnneigh
       integer(c_int32_t) :: ncut, ncutregion
       integer(c_int32_t) :: lewald2dlc
+      integer(c_int32_t) :: inlist
+      integer(c_int32_t) :: lvlistllist
    end type msg_params
 
    ! struct msg_energy
@@ -95,6 +97,11 @@ module MolsimGpu
          import :: c_ptr
          type(c_ptr), value :: h
       end function msg_last_error
+
+      integer(c_int) function msg_nlist_before_macrostep(h) bind(c, name='msg_nlist_before_macrostep')
+         import :: c_int, c_ptr
+         type(c_ptr), value        :: h
+      end function msg_nlist_before_macrostep
 
       integer(c_int) function msg_set_state(h, isys, ro, rod, rodd) bind(c, name='msg_set_state')
          import :: c_int, c_int32_t, c_ptr
@@ -407,16 +414,19 @@ module MolsimGpu
       end function msg_pot_tab
 
       integer(c_int) function msg_utwobody_noalloc(np, npt, boxlen, rcut, ro, iptpn, nneighpn, jpnlist, maxnneigh, &
-            ubuf, nbuf, iubuflow, r2umin, r2atat, force, utwob, virial, stream) bind(c, name='msg_utwobody_noalloc')
+            lmc, ubuf, nbuf, iubuflow, r2umin, r2atat, force, utwob, virial, stop_ipjp, stream) &
+            bind(c, name='msg_utwobody_noalloc')
          import :: c_int, c_int32_t, c_double, c_ptr
          integer(c_int32_t), value  :: np, npt
          real(c_double), intent(in) :: boxlen(3)
          real(c_double), value      :: rcut
          type(c_ptr), value         :: ro, iptpn, nneighpn, jpnlist   ! device pointers
-         integer(c_int32_t), value  :: maxnneigh
+         integer(c_int32_t), value  :: maxnneigh, lmc
          type(c_ptr), value         :: ubuf
          integer(c_int32_t), value  :: nbuf
-         type(c_ptr), value         :: iubuflow, r2umin, r2atat, force, utwob, virial, stream
+         type(c_ptr), value         :: iubuflow, r2umin, r2atat, force, utwob, virial
+         integer(c_int32_t)         :: stop_ipjp(2)                 ! ip, jp of a nonzero status
+         type(c_ptr), value         :: stream
       end function msg_utwobody_noalloc
    end interface
 

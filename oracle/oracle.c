@@ -533,6 +533,8 @@ struct or_sys {
     int nbond; int32_t *bond_ij; double *bond_k, *bond_eq; int32_t *bond_p;
     double tstep;
     int lcellbuild;
+    int inlist, lvlistllist;
+    int istep2;              /* steps since NList(iBeforeMacrostep): MOLSIM's istep2 */
 };
 
 static void *dup(const void *p, size_t n)
@@ -670,6 +672,9 @@ or_sys *or_create(const or_params *p)
     s->bond_p = dup(p->bond_p, sizeof(int32_t) * p->nbond);
     s->tstep = p->tstep;
     s->lcellbuild = p->lcellbuild;
+    s->inlist = p->inlist;
+    s->lvlistllist = p->lvlistllist;
+    s->istep2 = 0;
     return s;
 }
 
@@ -829,7 +834,118 @@ static int set_vlist_cells(or_sys *s)
     return 0;
 }
 
-int or_set_vlist(or_sys *s) { return s->lcellbuild ? set_vlist_cells(s) : set_vlist_md(s); }
+/* Row rule of SetVListMDLList, Src/nlist.F90:790-792: the pair is skipped when
+ * (ip > jp, ip+jp even) or (ip < jp, ip+jp odd), the opposite rows from SetVListMD's. */
+static int owns_llist(int ip, int jp)
+{
+    int itemp = (ip + jp) % 2;
+    if (ip > jp && itemp == 0) return 0;
+    if (ip < jp && itemp != 0) return 0;
+    return ip != jp;
+}
+
+/* SetLList(distance), Src/nlist.F90:1168-1221: ndivllist = int(boxlen/distance), celli =
+ * real(ndivllist)*boxleni (real() is default real; exact for these integers), cells
+ * numbered 1 + ix + iy nx + iz nx ny from aint((ro+boxlen2)*celli); each cell's chain runs
+ * from its smallest ip upwards (particles inserted np..1).  The reference caps the cell
+ * arrays at 1000 and does not guard larger grids; this restatement refuses them (6). */
+static int llist_cell(const or_sys *s, const int nd[3], const double celli[3], const double *r)
+{
+    int c[3], d;
+    for (d = 0; d < 3; ++d) {
+        c[d] = (int)((r[d] + s->boxlen2[d]) * celli[d]);
+        if (c[d] >= nd[d]) c[d] = nd[d] - 1;     /* r = +boxlen2 exactly: outside the reference's grid */
+        if (c[d] < 0) c[d] = 0;
+    }
+    return c[0] + c[1] * nd[0] + c[2] * nd[0] * nd[1];
+}
+
+/* SetVListMDLList, Src/nlist.F90:769-811, over SetLList(rcut+drnlist) and, per particle,
+ * SetNCell(ro(ip), rcut) (:1231-1260): the cells of the 27 points ro(ip) + (i, j, k) rcut,
+ * i, j, k in {-1, 0, 1}, each put in the box by PBC, are scanned in ascending cell number,
+ * each cell's chain in ascending ip. */
+static int set_vlist_md_llist(or_sys *s)
+{
+    double dist = s->rcut + s->drnlist, rs2cut = dist * dist, celli[3];
+    int nd[3], d, np = s->np, ip, ncell;
+    for (d = 0; d < 3; ++d) {
+        nd[d] = (int)(s->boxlen[d] / dist);
+        celli[d] = (double)(float)nd[d] * s->boxleni[d];
+    }
+    ncell = nd[0] * nd[1] * nd[2];
+    if (ncell < 1 || ncell > 1000) return 6;
+    {
+        int32_t *head = malloc(sizeof(int32_t) * ncell), *next = malloc(sizeof(int32_t) * np);
+        unsigned char *mark = malloc((size_t)ncell);
+        int c;
+        for (c = 0; c < ncell; ++c) head[c] = -1;
+        for (ip = np - 1; ip >= 0; --ip) {
+            c = llist_cell(s, nd, celli, s->ro + 3 * ip);
+            next[ip] = head[c];
+            head[c] = ip;
+        }
+        for (ip = 0; ip < np; ++ip) {
+            int32_t *row = s->jpnlist + (size_t)ip * s->maxnneigh;
+            int nn = 0, a, b, e;
+            memset(mark, 0, (size_t)ncell);
+            for (a = -1; a <= 1; ++a)
+                for (b = -1; b <= 1; ++b)
+                    for (e = -1; e <= 1; ++e) {
+                        double q[3];
+                        q[0] = s->ro[3 * ip] + a * s->rcut;
+                        q[1] = s->ro[3 * ip + 1] + b * s->rcut;
+                        q[2] = s->ro[3 * ip + 2] + e * s->rcut;
+                        for (d = 0; d < 3; ++d) q[d] = pbc1(q[d], s->boxlen2[d], s->dpbc[d], s->boxleni[d]);
+                        mark[llist_cell(s, nd, celli, q)] = 1;
+                    }
+            for (c = 0; c < ncell; ++c) {
+                int32_t jp;
+                if (!mark[c]) continue;
+                for (jp = head[c]; jp >= 0; jp = next[jp]) {
+                    double dx, dy, dz, r2;
+                    if (!owns_llist(ip + 1, jp + 1)) continue;
+                    dx = s->ro[3 * ip] - s->ro[3 * jp];
+                    dy = s->ro[3 * ip + 1] - s->ro[3 * jp + 1];
+                    dz = s->ro[3 * ip + 2] - s->ro[3 * jp + 2];
+                    r2 = pbcr2(s, &dx, &dy, &dz);
+                    if (r2 < rs2cut) {
+                        if (nn >= s->maxnneigh) { free(head); free(next); free(mark); return 3; }
+                        row[nn++] = jp + 1;
+                    }
+                }
+            }
+            s->nneighpn[ip] = nn;
+        }
+        free(head); free(next); free(mark);
+    }
+    return 0;
+}
+
+int or_set_vlist(or_sys *s)
+{
+    if (s->lvlistllist) return set_vlist_md_llist(s);
+    return s->lcellbuild ? set_vlist_cells(s) : set_vlist_md(s);
+}
+
+void or_nlist_before_macrostep(or_sys *s)
+{
+    memset(s->drosum, 0, sizeof(double) * 3 * s->np);
+    s->istep2 = 0;
+}
+
+/* NList(iSimulationStep), Src/nlist.F90:597-621: the skin test when inlist == 0; with
+ * inlist > 0 a rebuild whenever mod(istep2, inlist) == 0, drosum untouched. */
+static int nlist_step(or_sys *s, int32_t *rebuilt)
+{
+    int due;
+    s->istep2 += 1;
+    if (s->inlist > 0)
+        due = (s->istep2 % s->inlist) == 0;
+    else
+        due = or_skin_test(s, s->drostep, NULL, NULL);
+    if (rebuilt) *rebuilt = due;
+    return due ? or_set_vlist(s) : 0;
+}
 
 void or_get_vlist(const or_sys *s, int32_t *nneighpn, int32_t *jpnlist)
 {
@@ -1321,12 +1437,7 @@ int or_velver_step(or_sys *s, double *ekin, int32_t *rebuilt)
         ek = ek * sclmas * (sclvel * sclvel) / sclene;
     }
     if (ekin) *ekin = ek;
-    if (or_skin_test(s, s->drostep, NULL, NULL)) {
-        if (rebuilt) *rebuilt = 1;
-        return or_set_vlist(s);
-    }
-    if (rebuilt) *rebuilt = 0;
-    return 0;
+    return nlist_step(s, rebuilt);
 }
 
 /* BDDriver iSimulationStep: BDStep then UTotal, then NList; Src/bd.F90:53-59, 120-155 */
@@ -1345,12 +1456,7 @@ int or_bd_step(or_sys *s, const double *xi, const double *fac1, const double *fa
     }
     rc = or_utotal(s, NULL, NULL, NULL, NULL);
     if (rc) return rc;
-    if (or_skin_test(s, s->drostep, NULL, NULL)) {
-        if (rebuilt) *rebuilt = 1;
-        return or_set_vlist(s);
-    }
-    if (rebuilt) *rebuilt = 0;
-    return 0;
+    return nlist_step(s, rebuilt);
 }
 
 /* GauRandom, Src/mollib.F90:2739-2766 (polar Box-Muller over a 31-bit LCG) */

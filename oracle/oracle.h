@@ -108,6 +108,8 @@ typedef struct or_params {
     int32_t ncut;            /* standard Ewald: largest |n| component of k = 2 pi n / L */
     int32_t ncutregion;      /* standard Ewald: 0 'sphere' (|n|^2 <= ncut^2), 1 'cube' */
     int32_t lewald2dlc;      /* 1: the 2D layer correction (UEwaldRecStd2dlc) and UEwaldSurf's 2D form */
+    int32_t inlist;          /* NList: 0 skin test; n > 0 rebuild when mod(istep2, n) == 0 */
+    int32_t lvlistllist;     /* 1: SetVList builds through linked lists (SetLList + SetVListMDLList) */
 } or_params;
 
 typedef struct or_sys or_sys;
@@ -118,7 +120,12 @@ void    or_set_state(or_sys *s, const double *ro, const double *rod, const doubl
 void    or_get_state(const or_sys *s, double *ro, double *rod, double *rodd, double *drosum);
 void    or_set_drosum(or_sys *s, const double *drosum);
 
-int  or_set_vlist(or_sys *s);                            /* SetVListMD, Src/nlist.F90:724-759 */
+/* SetVList for MD/BD, Src/nlist.F90:686-716: SetVListMD (:724-759), or with lvlistllist
+ * SetLList(rcut+drnlist) + SetVListMDLList (:1168-1221, :769-811).  Returns 3 on a row
+ * beyond maxnneigh; 6 when the linked-list grid has no cell or more than 1000 cells. */
+int  or_set_vlist(or_sys *s);
+/* NList(iBeforeMacrostep), Src/nlist.F90:594-596: drosum = 0; also restarts istep2. */
+void or_nlist_before_macrostep(or_sys *s);
 void or_get_vlist(const or_sys *s, int32_t *nneighpn, int32_t *jpnlist);
 int64_t or_npair(const or_sys *s);
 

@@ -33,7 +33,8 @@ class Params(C.Structure):
                 ("epsi_four_pi", C.c_double), ("nbond", C.c_int32), ("bond_ij", i32p),
                 ("bond_k", f64p), ("bond_eq", f64p), ("bond_p", i32p), ("tstep", C.c_double),
                 ("maxnneigh", C.c_int32), ("lcellbuild", C.c_int32), ("ncut", C.c_int32),
-                ("ncutregion", C.c_int32), ("lewald2dlc", C.c_int32)]
+                ("ncutregion", C.c_int32), ("lewald2dlc", C.c_int32), ("inlist", C.c_int32),
+                ("lvlistllist", C.c_int32)]
 
 
 def lib():
@@ -80,6 +81,7 @@ def lib():
         L.or_set_drosum.argtypes = [C.c_void_p, f64p]
         L.or_set_vlist.restype = C.c_int
         L.or_set_vlist.argtypes = [C.c_void_p]
+        L.or_nlist_before_macrostep.argtypes = [C.c_void_p]
         L.or_get_vlist.argtypes = [C.c_void_p, i32p, i32p]
         L.or_npair.restype = C.c_int64
         L.or_npair.argtypes = [C.c_void_p]
@@ -243,7 +245,8 @@ class System:
                    _p(k["bond_k"], C.c_double), _p(k["bond_eq"], C.c_double),
                    _p(k["bond_p"], C.c_int32), sysd["tstep"], self.maxnneigh, int(lcellbuild),
                    int(sysd.get("ncut", 0)), 1 if sysd.get("ncutregion", "sphere") == "cube" else 0,
-                   int(bool(sysd.get("lewald2dlc", False))))
+                   int(bool(sysd.get("lewald2dlc", False))), int(sysd.get("inlist", 0)),
+                   int(bool(sysd.get("lvlistllist", False))))
         self.h = L.or_create(C.byref(P))
 
     def __del__(self):
@@ -265,6 +268,10 @@ class System:
         rc = lib().or_set_vlist(self.h)
         if rc:
             raise RuntimeError("SetVListMD failed: %d" % rc)
+
+    def nlist_before_macrostep(self):
+        """NList(iBeforeMacrostep): drosum = 0, istep2 restarts."""
+        lib().or_nlist_before_macrostep(self.h)
 
     def get_vlist(self):
         nn = np.zeros(self.np, np.int32)

@@ -196,3 +196,119 @@ def test_batching_window_gathers_early_arrivals():
     at_once, windowed = run(0.0), run(0.01)
     assert windowed[0] > at_once[0] + 2
     assert len(windowed) < len(at_once)
+
+
+class RefillCohort:
+    """Simulated cohort with GpuCohort's protocol: jobs of different lengths, read out
+    at the chunk boundary where each finishes, drained and re-formed on request."""
+
+    refillable = True
+
+    def __init__(self, jobs, precision, chunk, ahead=2):
+        self.jobs = jobs
+        self.chunk = chunk
+        for j in jobs:
+            if j.left is None:
+                j.left = j.nsteps
+            j.carry = None
+        self.unsent = [j.left for j in jobs]
+        self.done = [False] * len(jobs)
+        self.drain = False
+        self.nbytes = sum(j.nbytes for j in jobs)
+        self.finished = []
+        self.chunks_sent = 0
+
+    def pump(self):
+        for k, j in enumerate(self.jobs):
+            if self.unsent[k] == 0 and not self.done[k]:
+                j.result = dict(n=j.n, steps=j.nsteps)
+                j.left = 0
+                self.done[k] = True
+                self.finished.append(j)
+        if not self.drain:
+            live = [u for u in self.unsent if u > 0]
+            if live:
+                step = min(self.chunk, min(live))
+                self.unsent = [max(0, u - step) for u in self.unsent]
+                self.chunks_sent += 1
+        return all(self.done)
+
+    def idle(self):
+        return True
+
+    def take_finished(self):
+        out, self.finished = self.finished, []
+        return out
+
+    def carry_out(self):
+        out = []
+        for k, j in enumerate(self.jobs):
+            if not self.done[k]:
+                j.left = self.unsent[k]
+                j.carry = dict(ro=None)
+                out.append(j)
+        return out
+
+    def harvest(self):
+        return [j.result for j in self.jobs]
+
+    def close(self):
+        pass
+
+
+def test_refill_lets_waiting_jobs_join_running_work():
+    """One cohort place only: without refill a job arriving just after a long job waits
+    for it to finish; with refill the long job's cohort is re-formed at the next chunk
+    boundary with the newcomer, every job runs exactly its step count, and the budget
+    holds throughout."""
+    def run(refill):
+        jobs = _jobs([(1000, 200, 0.0, 40)] + [(100, 20, 0.002 + 0.001 * k, 10) for k in range(4)])
+        srv = Server(100, backend=RefillCohort, clock=TickClock(), estimate=lambda j: j.nbytes,
+                     max_cohorts=1, max_jobs=8, chunk=10, refill=refill)
+        m = srv.run(jobs, poll_s=0)
+        assert m["jobs"] == 5 and m["failed"] == 0
+        assert all(j.result["steps"] == j.nsteps and j.left == 0 for j in jobs)
+        assert srv.peak_used <= 100 and srv.used == 0
+        return jobs, srv, m
+
+    jobs0, srv0, m0 = run(False)
+    jobs1, srv1, m1 = run(True)
+    big0, big1 = jobs0[0], jobs1[0]
+    assert all(j.admitted >= big0.done for j in jobs0[1:])          # without refill: wait for the big job
+    assert all(j.done < big1.done for j in jobs1[1:])               # with refill: done while it still runs
+    assert m1["reforms"] >= 1 and m1["joined_running"] == 4
+    assert m1["p99_s"] < m0["p99_s"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_job_joining_a_running_cohort_matches_alone(precision):
+    """Iteration-level admission on the GPU: with one cohort place, a job arriving while a
+    long job runs joins it at the next chunk boundary (the cohort is re-formed).  The
+    newcomer's result equals running it alone bit for bit (it starts fresh in the new
+    handle); the long job, carried across the re-form with a rebuilt list, agrees with
+    running alone to rounding: positions within 1e-6 A, energies within 1e-6 relative."""
+    from molsim_b200.engine import prepare
+    from molsim_b200.systems import scaled_job
+
+    rng = np.random.default_rng(21)
+    sa = scaled_job(rng, 1200, "electrolyte")
+    sb = scaled_job(rng, 600, "polyelectrolyte")
+    a = Job(0, sa, prepare(sa), 400, 0.0)
+    b = Job(1, sb, prepare(sb), 30, 0.005)
+    srv = Server(2 << 30, precision=precision, max_cohorts=1, max_jobs=4, chunk=10, refill=True)
+    m = srv.run([a, b])
+    assert m["failed"] == 0, (a.error, b.error)
+    assert m["joined_running"] == 1 and m["reforms"] >= 1
+    assert b.done < a.done
+    rb = _alone(b, precision)
+    for key in ("ro", "rod"):
+        assert np.array_equal(b.result[key], rb[key]), key
+    assert b.result["energy"]["utot"] == rb["energy"]["utot"]
+    ra = _alone(a, precision)
+    d = a.result["ro"] - ra["ro"]
+    box = sa["boxlen"][0]
+    d -= box * np.round(d / box)
+    assert np.abs(d).max() < 1e-6
+    for key in ("utot", "virial", "ekin"):
+        assert abs(a.result["energy"][key] - ra["energy"][key]) <= 1e-6 * abs(ra["energy"][key]), key
