@@ -56,8 +56,13 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=200,
                     help="jobs in the serving stream (Poisson arrivals at 200/s; 0: skip)")
     ap.add_argument("--serve-budget-gib", type=float, default=4.0)
+    ap.add_argument("--serve-refill", type=int, default=0,
+                    help="serving: iteration-level admission (re-form a running cohort with waiting jobs)")
     ap.add_argument("--serve-low-rate", type=float, default=50.0,
                     help="serving: the same stream again at this arrival rate (jobs/s; 0: skip)")
+    ap.add_argument("--profile", default=None, choices=["single", "batched", "bd"],
+                    help="profiling target for ncu: build that workload (mixed precision), run a "
+                         "UTotal and three steps, print one line of per-kernel times, no JSON line")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -827,7 +832,7 @@ def run_serving(a, rank=0, world=1):
         if world > 1:
             jobs = my_share(jobs, [j.n * j.nsteps for j in jobs], [1] * len(jobs), rank, world)
         srv = Server(int(a.serve_budget_gib * (1 << 30)), precision="mixed", max_cohorts=8, max_jobs=64, chunk=50,
-                     batch_wait_s=a.serve_wait, ahead=a.serve_ahead, refill=True)
+                     batch_wait_s=a.serve_wait, ahead=a.serve_ahead, refill=bool(a.serve_refill))
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
@@ -1102,8 +1107,44 @@ def run_gpu(a):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(a):
+    """A small fixed workload for ncu captures: the 16000-particle polyelectrolyte alone
+    or as 32 replicas in one handle, or the 200000-particle BD system; mixed precision with
+    the default pair kernel; one UTotal and three steps (launched directly when the
+    environment sets MSG_NO_GRAPHS=1, which ncu needs), then the library's per-kernel
+    timers over three more steps."""
+    import torch
+
+    from molsim_b200 import Engine
+    from molsim_b200 import systems as S
+
+    if a.profile == "bd":
+        s = S.colloid_bd(seed=0)
+        s["bd_fac"] = S.bd_factors(s)
+        e = Engine(s, precision="mixed")
+        step = lambda: e.BDStep(1, seed=7, energies=False)          # noqa: E731
+    else:
+        s = S.polyelectrolyte(seed=0)
+        e = Engine([dict(s) for _ in range(32 if a.profile == "batched" else 1)], precision="mixed")
+        step = lambda: e.VelVer(1, energies=False)                  # noqa: E731
+    e.UTotal(0)
+    if a.profile != "bd":
+        e.GetLinAcc()
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e.set_timing(True)
+    for _ in range(3):
+        step()
+    kt = e.kernel_times()
+    print(a.profile, {k: round(v[0] / v[1], 4) for k, v in kt.items() if v[1]})
+
+
 def main():
     a = parse()
+    if a.profile:
+        run_profile(a)
+        return
     if a.impl == "reference":
         run_reference(a)
     else:

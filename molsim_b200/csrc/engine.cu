@@ -180,6 +180,7 @@ struct msg_handle {
     Tile *t128 = nullptr;
     PairTask *ptask = nullptr;
     int2 *psrange = nullptr;          // lean pair kernel: each system's tasks [first, end)
+    int *pgsys = nullptr;             // lanes per particle of each system's tasks
     int *psched = nullptr;            // its per-system task counters and finished-block counter
     int nt128 = 0, nptask = 0, max_npt = 1;
     int4 *chunks = nullptr, *infl = nullptr;
@@ -430,7 +431,7 @@ static void free_all(msg_handle *h)
                     h->fo[0], h->fo[1], h->typ[0], h->typ[1], h->orig[0], h->orig[1], h->cellid, h->inv,
                     h->sysid, h->fsr, h->fpart, h->ftot, h->posfx, h->k0, h->v0, h->k1, h->v1, h->rhist, h->cstart,
                     h->cend, h->nbl, h->nnb, h->nmaxrow, h->r2o, h->skinout, h->sc, h->flag, h->nrebuild,
-                    h->t128, h->ptask, h->psrange, h->psched, h->chunks, h->infl, h->eacc, h->esys,
+                    h->t128, h->ptask, h->psrange, h->pgsys, h->psched, h->chunks, h->infl, h->eacc, h->esys,
                     h->hist, h->stepctr, h->sstep, h->rdone, h->fdone, h->errw, h->ptab, h->ptmap, h->tz, h->tc,
                     h->bst, h->bkz, h->tz32, h->tc32, h->massip, h->massp, h->fac1, h->fac2, h->bptr, h->bpart, h->bpw, h->bk, h->beq,
                     h->rgrid, h->mfac, h->emf, h->vmf, h->cgrid, h->rgrid32, h->cgrid32, h->igrid, h->stage, h->xin, h->dsys,
@@ -1172,14 +1173,21 @@ std::vector<PairTask> msg_handle::make_pair_tasks(int shift) const
 void msg_handle::set_pair_chunks(const std::vector<PairTask> &pt, bool replace)
 {
     std::vector<int2> r(nsys, make_int2(0, 0));
+    std::vector<int> gs(nsys, 32);
     for (size_t a = 0; a < pt.size();) {
         const int end = pt[a].send;
         r[pt[a].sys] = make_int2((int)a, end);
+        gs[pt[a].sys] = pt[a].g;
         a = (size_t)end;
     }
-    if (replace) dfree(psrange);
+    if (replace) {
+        dfree(psrange);
+        dfree(pgsys);
+    }
     psrange = dalloc<int2>(nsys);
     up(psrange, r.data(), r.size() * sizeof(int2));
+    pgsys = dalloc<int>(nsys);
+    up(pgsys, gs.data(), gs.size() * sizeof(int));
 }
 
 void msg_handle::set_pair_lanes(int shift, bool force)
@@ -1411,7 +1419,7 @@ static void launch_forces(msg_handle *h, int mode, bool record, bool skin)
         const int cap = per_sm > 0 ? std::min(h->pair_blocks_lean, h->nsm * per_sm) : h->pair_blocks_lean;
         const int grid = std::max(1, std::min(h->nptask, cap));
 #define MSG_HALF1(NTV, UV, HV)                                                                              \
-    k_pair_h<NTV, UV, HV><<<grid, PAIR_BLOCK, h->pair_smem_h, ps>>>(h->dsys, h->ptask, h->psrange, h->nsys,    \
+    k_pair_h<NTV, UV, HV><<<grid, PAIR_BLOCK, h->pair_smem_h, ps>>>(h->dsys, h->pgsys, h->psrange, h->nsys,    \
                                                                     h->nptask, h->psched, h->posfx, h->typ[0], \
                                                                     h->nbl, h->nnb, h->ptmap, h->ptab, h->tch, \
                                                                     h->bkz, h->fsr, h->fpart, h->ntot, h->eacc, \

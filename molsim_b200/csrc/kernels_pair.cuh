@@ -688,11 +688,12 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U == 1 ? 4 : (U == 2 ? 
 // HALF = false: the full list (each pair from both ends), no atomics; each end
 // keeps half of the pair's energy and virial.
 // ---------------------------------------------------------------------------
-// Register budget with two particle types: three blocks of 256 per SM with one or two
-// row entries in flight per lane, two blocks with four.
+// Register budget with two particle types: three blocks of 256 per SM with one or two row
+// entries in flight per lane (two entries spill a few values to L1, and still run faster
+// than at two blocks per SM), two blocks with four; two blocks with more types.
 template <int NT, int U, bool HALF>
-__global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_pair_h(
-    const SysDev *__restrict__ sysv, const PairTask *__restrict__ tasks, const int2 *__restrict__ srange,
+__global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? 3 : 2) k_pair_h(
+    const SysDev *__restrict__ sysv, const int *__restrict__ gsys, const int2 *__restrict__ srange,
     int nsys, int ntasks, int *__restrict__ sched,
     const int4 *__restrict__ pos, const int *__restrict__ typ, const int *__restrict__ nbl,
     const int *__restrict__ nnb, const int *__restrict__ ptmap, const PairTab *__restrict__ ptab,
@@ -758,8 +759,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_
         held = sys;
         if (sys != loaded) {
             __syncthreads();
-            const PairTask W0 = tasks[R.x];
-            const SysDev &Sn = sysv[W0.sys];
+            const SysDev &Sn = sysv[sys];
             if (threadIdx.x < Sn.natat) sP[threadIdx.x] = ptab[Sn.pt_off + threadIdx.x];
             if (threadIdx.x < Sn.npt * Sn.npt) {
                 const int q = ptmap[Sn.ptmap_off + threadIdx.x] - Sn.pt_off;
@@ -783,47 +783,56 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_
                 Tb = bkz + Sn.tab_b0;
             }
             if (threadIdx.x == 0) sNpt = Sn.npt;
-            loaded = W0.sys;
+            loaded = sys;
         }
         __syncthreads();
         const SysDev &S = sysv[sys];
         const float rcut2 = (float)S.rcut2;
         const float lowmax = (float)fmax(S.r2umin_max, S.r2atat_max);
         const float sx = S.fxi[0], sy = S.fxi[1], sz = S.fxi[2];
+        // a task is 32/G consecutive particles of the system, G lanes each (G per system)
+        const int G = gsys[sys];
+        const int per = 32 / G, g = lane & (G - 1);
         int nxt = 0;
         if (lane == 0) nxt = R.x + atomicAdd(&sched[sys], 1);
         for (;;) {
             const int task = __shfl_sync(0xffffffffu, nxt, 0);
             if (task >= R.y) break;
             if (lane == 0) nxt = R.x + atomicAdd(&sched[sys], 1);
-            const PairTask W = tasks[task];
-            const int G = W.g;
-            const int g = lane & (G - 1);
-            const int i = W.i0 + lane / G;
-            const bool act = i < W.i1;
+            const int li = (task - R.x) * per + lane / G;
+            const bool act = li < S.n;
+            const int i = S.off + (act ? li : 0);
             // forces in FP32; energies and virial of the lane's pairs in FP64
             float fx = 0.0f, fy = 0.0f, fz = 0.0f;
             double vi = 0.0;
             double ut[NT];
 #pragma unroll
             for (int t = 0; t < NT; ++t) ut[t] = 0.0;
-            int ti = 0, n = 0;
-            int4 xi = make_int4(0, 0, 0, 0);
-            const int *row = nbl;
-            if (act) {
-                xi = pos[i];
-                ti = typ[i];
-                n = nnb[i];
-                row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
-            }
+            // the particle's own data and its first row entries are loaded together: the
+            // entries' addresses need only i, and entries past the row's end are masked
+            // once its length has arrived
+            const int *row = nbl + S.nbl_off + (long long)(i - S.off) * S.cap;
+            int ee[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) ee[u] = (g + u * G < S.cap) ? __ldg(row + g + u * G) : -1;
+            const int4 xi = pos[i];
+            const int ti = typ[i];
+            const int n = act ? nnb[i] : 0;
             const float4 *sTi = sT + ti * MAXT;
             for (int kb = g; kb < n; kb += U * G) {
-                int ee[U];
                 int4 xj[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) ee[u] = (kb + u * G < n) ? __ldg(row + kb + u * G) : -1;
+                for (int u = 0; u < U; ++u)
+                    if (kb + u * G >= n) ee[u] = -1;
 #pragma unroll
                 for (int u = 0; u < U; ++u) xj[u] = pos[ee[u] >= 0 ? (ee[u] & NBL_JMASK) : i];
+                // the next batch's entries go out before this batch is evaluated
+                int en[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int kn = kb + U * G + u * G;
+                    en[u] = (kn < n) ? __ldg(row + kn) : -1;
+                }
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     if (ee[u] < 0) continue;
@@ -855,12 +864,12 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_
                             c.c[0] = r2;
                             c.c[2] = 1e10f;
                         } else if (r2 < (float)Q.r2umin) {
-                            raise_error(err, 1, W.sys, i, j);
+                            raise_error(err, 1, sys, i, j);
                             ok = false;
                         } else {
                             while (r2 < c.c[0]) {
                                 if (++kk >= kend) {
-                                    raise_error(err, 2, W.sys, i, j);
+                                    raise_error(err, 2, sys, i, j);
                                     kk = kend - 1;
                                     c.load(Tc + (size_t)kk * ROW16);
                                     break;
@@ -870,8 +879,6 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_
                         }
                     }
                     if (!ok) continue;
-                    // d = r2 - z_low with z_low's low part; the leading coefficients' low parts
-                    // join the FP32 polynomials, their high parts are added in FP64
                     // d = r2 - z_low with z_low's low part; the leading coefficients' low parts
                     // join the polynomials, so u and f round once each, without bias
                     const float d = (r2 - c.c[0]) - c.c[1];
@@ -894,6 +901,8 @@ __global__ void __launch_bounds__(PAIR_BLOCK, NT == 2 ? (U <= 2 ? 3 : 2) : 2) k_
                         if (tj == t) ut[t] += uu;
                     vi -= (double)(f * r2);
                 }
+#pragma unroll
+                for (int u = 0; u < U; ++u) ee[u] = en[u];
             }
             // a full list sees each pair from both ends: each end keeps half of it
             constexpr double ef = HALF ? kEFix : 0.5 * kEFix;
