@@ -95,15 +95,20 @@ def apply_grids(systems, edges, order=4):
     return out
 
 
-def _time_steps(engine, steps):
+def _time_steps(engine, steps, repeats=3):
+    """Milliseconds per MD step: the best of `repeats` runs of `steps` steps (a run that
+    happens to hold a list rebuild, or a busy moment of the host, does not decide)."""
     import torch
 
     engine.VelVer(2, energies=False)               # capture the graph for this layout
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    engine.VelVer(steps, energies=False)
-    torch.cuda.synchronize()
-    return 1000.0 * (time.perf_counter() - t0) / steps
+    best = float("inf")
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        engine.VelVer(steps, energies=False)
+        torch.cuda.synchronize()
+        best = min(best, 1000.0 * (time.perf_counter() - t0) / steps)
+    return best
 
 
 def tune_pair_lanes(engine, shifts=(-1, 0, 1), steps=10):

@@ -201,7 +201,7 @@ struct msg_handle {
     unsigned short *bst = nullptr;                    // bucket starts per type pair
     int2 *bkz = nullptr;                              // lean kernel buckets: (absolute row, its z_low)
     size_t pair_smem_m = 0, pair_smem_h = 0;
-    float *tch = nullptr;                             // k_pair_h rows (ROW16 floats: hi/lo z_low, c1, c7)
+    float *tch = nullptr;                             // k_pair_h rows (ROW16 floats used of ROWST: hi/lo z_low, c1, c7)
     // mixed path: k_pair_h over a half list (2) or a full list (3), k_pair_m (1) or k_pair (0)
     int pair_lean = 1;
     int pair_unroll = 2;                              // k_pair_m: row entries in flight per lane
@@ -876,7 +876,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             const size_t bm = lean_smem_bytes(S.tab_nk, S.natat * MSG_NBUCKET);
             S.tab_smem_m = bm <= 96 * 1024 ? 1 : 0;
             if (S.tab_smem_m) pair_smem_m = std::max(pair_smem_m, bm);
-            const size_t bh = lean_smem_bytes(S.tab_nk, S.natat * MSG_NBUCKET, ROW16);
+            const size_t bh = lean_smem_bytes(S.tab_nk, S.natat * MSG_NBUCKET, ROWST);
             S.tab_smem_h = bh <= 96 * 1024 ? 1 : 0;
             if (S.tab_smem_h) pair_smem_h = std::max(pair_smem_h, bh);
         }
@@ -940,10 +940,10 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         if (prec == MSG_PREC_MIXED) {
             // rows of k_pair_h: z_low, c1 and c7 as FP32 (hi, lo) pairs
             const size_t nk = vc.size() / 12;
-            std::vector<float> fh(nk * ROW16, 0.0f);
+            std::vector<float> fh(nk * ROWST, 0.0f);
             for (size_t k = 0; k < nk; ++k) {
                 const double *c = vc.data() + 12 * k;
-                float *o = fh.data() + ROW16 * k;
+                float *o = fh.data() + ROWST * k;
                 auto split = [](double v, float *hl) {
                     hl[0] = (float)v;
                     hl[1] = (float)(v - (double)hl[0]);

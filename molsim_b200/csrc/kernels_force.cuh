@@ -289,13 +289,42 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 aold = acc[i];
             }
         }
-        if (S.lewald && !S.recstd) {
-            const int s = S.s;
+    }
+    if (S.lewald && !S.recstd) {
+        // the y and z spline values of the block's particles, read by whichever lane takes a line
+        __shared__ R sTy[128][P], sDy[128][P], sTz[128][P], sDz[128][P];
+        const int pl = (int)threadIdx.x / FIN_LANES;
+        const int s = S.s;
+        R th0[P], dth0[P];
+        int km[3] = {0, 0, 0};
+        if (i < T.i1) {
             const double xc[3] = {x.x, x.y, x.z};
             R th[3][P], dth[3][P];
-            int km[3];
 #pragma unroll
             for (int m = 0; m < 3; ++m) km[m] = bspline_at<P, R>(S.dkdr[m] * xc[m], s, th[m], dth[m]);
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                th0[k] = th[0][k];
+                dth0[k] = dth[0][k];
+            }
+            if (g == 0) {
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    sTy[pl][k] = th[1][k];
+                    sDy[pl][k] = dth[1][k];
+                    sTz[pl][k] = th[2][k];
+                    sDz[pl][k] = dth[2][k];
+                }
+            }
+        }
+        __syncwarp();
+        if (i < T.i1) {
+            int nxs[P];
+#pragma unroll
+            for (int ix = 0; ix < P; ++ix) {
+                const int nx = km[0] - ix;
+                nxs[ix] = nx + ((nx < 0) ? s : 0);
+            }
             // the P*P (iy, iz) grid lines of the particle, dealt round the group's lanes
             for (int l = g; l < P * P; l += FIN_LANES) {
                 const int iy = l % P, iz = l / P;
@@ -303,23 +332,14 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 nz += (nz < 0) ? s : 0;
                 int ny = km[1] - iy;
                 ny += (ny < 0) ? s : 0;
-                R tz = th[2][0], dtz = dth[2][0], ty = th[1][0], dty = dth[1][0];
-#pragma unroll
-                for (int k = 1; k < P; ++k) {
-                    tz = (iz == k) ? th[2][k] : tz;
-                    dtz = (iz == k) ? dth[2][k] : dtz;
-                    ty = (iy == k) ? th[1][k] : ty;
-                    dty = (iy == k) ? dth[1][k] : dty;
-                }
+                const R ty = sTy[pl][iy], dty = sDy[pl][iy], tz = sTz[pl][iz], dtz = sDz[pl][iz];
                 const size_t rowo = S.grid_off + ((size_t)nz * s + ny) * s;
                 R a0 = 0, a1 = 0;
 #pragma unroll
                 for (int ix = 0; ix < P; ++ix) {
-                    int nx = km[0] - ix;
-                    nx += (nx < 0) ? s : 0;
-                    const R Q = PR::mixed ? (R)grid32[rowo + nx] : (R)grid[rowo + nx];
-                    a0 += dth[0][ix] * Q;
-                    a1 += th[0][ix] * Q;
+                    const R Q = PR::mixed ? (R)grid32[rowo + nxs[ix]] : (R)grid[rowo + nxs[ix]];
+                    a0 += dth0[ix] * Q;
+                    a1 += th0[ix] * Q;
                 }
                 e0 += a0 * ty * tz;
                 e1 += a1 * dty * tz;

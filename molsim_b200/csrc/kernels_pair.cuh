@@ -117,6 +117,10 @@ struct Row16 {
     }
 };
 constexpr int ROW16 = 16;
+// Rows are laid out 20 floats apart: with a 64-byte stride every row would start in one of
+// two 16-byte bank groups, and the 8 lanes of a 16-byte shared load phase, each reading its
+// own row, would collide 4 ways; a 80-byte stride spreads row starts over 8 bank groups.
+constexpr int ROWST = 20;
 
 // r2 of a pair from its exact fixed-point coordinate differences: in a cubic box
 // the exact 64-bit integer sum of squares (each square < 2^62) rounded to FP32 and
@@ -772,14 +776,14 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? 3 : 2) k_pai
             kbase = Sn.tab_k0;
             if (Sn.tab_smem_h) {
                 float *sc = reinterpret_cast<float *>(dyn);
-                int2 *sb = reinterpret_cast<int2 *>(sc + (size_t)ROW16 * Sn.tab_nk);
-                const int nc = ROW16 * Sn.tab_nk, nb = Sn.natat * MSG_NBUCKET;
-                for (int k = threadIdx.x; k < nc; k += PAIR_BLOCK) sc[k] = tc[(size_t)ROW16 * Sn.tab_k0 + k];
+                int2 *sb = reinterpret_cast<int2 *>(sc + (size_t)ROWST * Sn.tab_nk);
+                const int nc = ROWST * Sn.tab_nk, nb = Sn.natat * MSG_NBUCKET;
+                for (int k = threadIdx.x; k < nc; k += PAIR_BLOCK) sc[k] = tc[(size_t)ROWST * Sn.tab_k0 + k];
                 for (int k = threadIdx.x; k < nb; k += PAIR_BLOCK) sb[k] = bkz[Sn.tab_b0 + k];
                 Tc = sc;
                 Tb = sb;
             } else {
-                Tc = tc + (size_t)ROW16 * Sn.tab_k0;
+                Tc = tc + (size_t)ROWST * Sn.tab_k0;
                 Tb = bkz + Sn.tab_b0;
             }
             if (threadIdx.x == 0) sNpt = Sn.npt;
@@ -852,7 +856,7 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? 3 : 2) k_pai
                     const int2 B = Tb[__float_as_int(T.w) + bk];
                     int kk = min(B.x + (r2 < __int_as_float(B.y) ? 1 : 0), __float_as_int(T.z) - 1);
                     Row16 c;
-                    c.load(Tc + (size_t)kk * ROW16);
+                    c.load(Tc + (size_t)kk * ROWST);
                     bool ok = true;
                     if (r2 < lowmax || r2 < c.c[0]) {
                         const PairTab &Q = sP[sMap[ti * S.npt + tj]];
@@ -871,10 +875,10 @@ __global__ void __launch_bounds__(PAIR_BLOCK, (NT == 2 && U <= 2) ? 3 : 2) k_pai
                                 if (++kk >= kend) {
                                     raise_error(err, 2, sys, i, j);
                                     kk = kend - 1;
-                                    c.load(Tc + (size_t)kk * ROW16);
+                                    c.load(Tc + (size_t)kk * ROWST);
                                     break;
                                 }
-                                c.load(Tc + (size_t)kk * ROW16);
+                                c.load(Tc + (size_t)kk * ROWST);
                             }
                         }
                     }

@@ -141,18 +141,23 @@ class Engine:
         if rc:
             raise MolsimGpuError(rc, "msg_create failed")
         self.h = h
+        self.reset_states()
+
+    def reset_states(self):
+        """Every system back to the state its dict holds (ro, rod, rodd; the last two may be
+        absent): one call, one list rebuild, one device wait."""
+        systems = self.systems
         if self.nsys == 1:
             self.set_state(0, systems[0]["ro"], systems[0].get("rod"), systems[0].get("rodd"))
-        else:
-            # every system's state in one call: one list rebuild and one device wait
-            cat = []
-            for key in ("ro", "rod", "rodd"):
-                parts = [s.get(key) for s in systems]
-                cat.append(None if any(x is None for x in parts) else
-                           np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64).reshape(-1, 3)
-                                                                for x in parts]), np.float64))
-            ptrs = [None if a is None else _p(a, C.c_double) for a in cat]
-            self._check(L.msg_set_state_all(self.h, *ptrs))
+            return
+        cat = []
+        for key in ("ro", "rod", "rodd"):
+            parts = [s.get(key) for s in systems]
+            cat.append(None if any(x is None for x in parts) else
+                       np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64).reshape(-1, 3)
+                                                            for x in parts]), np.float64))
+        ptrs = [None if a is None else _p(a, C.c_double) for a in cat]
+        self._check(_lib.lib().msg_set_state_all(self.h, *ptrs))
 
     def _params(self, s, t, maxnneigh):
         return Engine._params_for(s, t, maxnneigh, self._keep)
