@@ -1361,9 +1361,10 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
     fo.alldone = h->rdone;
     h->tbeg(TM_FINAL);
     h->launches += 1;
-    k_finalize<P, PR><<<h->nt128, FIN_THREADS, 0, h->st>>>(
+    k_finalize<P, PR><<<h->nt128 * FIN_SPLIT, FIN_THREADS, 0, h->st>>>(
         h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->list_half ? h->fpart : nullptr,
-        h->ntot, h->ew_fks, h->eacc, h->massip, h->massp,
+        h->ntot, FinBonds{h->orig[0], h->inv, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bpw, h->bk, h->beq},
+        h->ew_fks, h->eacc, h->massip, h->massp,
         h->ftot, h->fo[0], h->vel[0], h->acc[0], mode, fo, h->errw);
     h->tend(TM_FINAL);
 }
@@ -1461,11 +1462,6 @@ static void launch_forces(msg_handle *h, int mode, bool record, bool skin)
         k_pair<PR, 4><<<h->pair_grid, PAIR_BLOCK, h->pair_smem, ps>>>(h->dsys, h->ptask, h->nptask, pp, h->typ[0], h->nbl,
                                                               h->nnb, h->ptmap, h->ptab, tzp, tcp, h->bst, h->fsr,
                                                               h->eacc, h->errw);
-    if (h->has_bonds) {
-        k_bonds<<<h->nt128, 128, 0, ps>>>(h->dsys, h->t128, h->pos[0], h->orig[0], h->inv, h->bptr, h->bpart, h->bk,
-                                          h->beq, h->bpw, h->fsr, h->eacc);
-        h->launches += 1;
-    }
     h->tend(TM_PAIR);
     h->launches += 1;
     if (h->any_std) launch_ewald_std(h);

@@ -162,75 +162,12 @@ __global__ void __launch_bounds__(INFL_THREADS) k_influence(const SysDev *__rest
 //   0 utot, 1 utwob(0), 2..11 utwob(1..10), 12 urec, 13 ubond, 14 virial, 15 ekin
 // mode 0: forces only; 1: + velocity Verlet update.
 // ---------------------------------------------------------------------------
-// ---------------------------------------------------------------------------
-// UBond (Src/energy.F90:5335-5387): u += k'(r - r0)^p, F = -p k'(r - r0)^(p-1)/r d.
-// Runs after the pair kernel on its stream, beside the SPME chain: each
-// particle adds the forces of its bonds (both ends of a bond compute it) to
-// its short-range force; a bond's energy and virial count once (o < po).
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_bonds(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
-                                              const double4 *__restrict__ pos, const int *__restrict__ orig,
-                                              const int *__restrict__ inv, const int *__restrict__ bptr,
-                                              const int *__restrict__ bpart, const double *__restrict__ bk,
-                                              const double *__restrict__ beq, const int *__restrict__ bpw,
-                                              double4 *__restrict__ fsr, long long *__restrict__ eacc)
-{
-    __shared__ double red[2][4];
-    const Tile T = tiles[blockIdx.x];
-    const SysDev &S = sysv[T.sys];
-    const int i = T.i0 + threadIdx.x;
-    double ub = 0.0, vb = 0.0;
-    if (i < T.i1) {
-        const int o = orig[i];
-        const int b0 = bptr[S.off + o], b1 = bptr[S.off + o + 1];
-        if (b1 > b0) {
-            const double4 x = pos[i];
-            double bx = 0.0, by = 0.0, bz = 0.0;
-            for (int b = b0; b < b1; ++b) {
-                const int po = bpart[b];
-                const double4 xj = pos[inv[S.off + po]];
-                double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
-                const double r2 = pbcr2_exact(dx, dy, dz, S), r1 = sqrt(r2);
-                const double term = r1 - beq[b];
-                const int pw = bpw[b];
-                double tp = 1.0;
-                for (int k = 0; k < pw - 1; ++k) tp *= term;
-                double fac = bk[b] * tp;
-                const double u = fac * term;
-                fac = -(pw * fac / r1);
-                bx += fac * dx;
-                by += fac * dy;
-                bz += fac * dz;
-                if (o < po) {
-                    ub += u;
-                    vb -= fac * r2;
-                }
-            }
-            double4 f = fsr[i];
-            f.x += bx;
-            f.y += by;
-            f.z += bz;
-            fsr[i] = f;
-        }
-    }
-    ub = warp_sum(ub);
-    vb = warp_sum(vb);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        red[0][w] = ub;
-        red[1][w] = vb;
-    }
-    __syncthreads();
-    if (threadIdx.x < 2) {
-        const double a = red[threadIdx.x][0] + red[threadIdx.x][1] + red[threadIdx.x][2] + red[threadIdx.x][3];
-        if (a != 0.0) acc_add(eacc + (size_t)T.sys * EA_N + EA_UBOND + threadIdx.x, a);
-    }
-}
-
 constexpr int NPART_FIN = 4;    // ubond, virbond, ekin, spare
 constexpr int ESZ = 16;
 constexpr int FIN_LANES = 4;                      // lanes per particle in the grid gather
-constexpr int FIN_THREADS = 128 * FIN_LANES;      // one 128-particle tile per block
+constexpr int FIN_PART = 64;                      // particles per block: half a 128-particle tile
+constexpr int FIN_SPLIT = 128 / FIN_PART;         // blocks per tile
+constexpr int FIN_THREADS = FIN_PART * FIN_LANES;
 
 struct FinOut {
     double *esys, *hist;
@@ -239,11 +176,47 @@ struct FinOut {
     unsigned *fdone, *alldone;
 };
 
+// Bonds of every system (CSR over MOLSIM indices; bptr null: no bonds in the handle).
+struct FinBonds {
+    const int *orig, *inv, *bptr, *bpart, *bpw;
+    const double *bk, *beq;
+};
+
+// UBond (Src/energy.F90:5335-5387) for particle i: the forces of its bonds (both ends of
+// a bond compute it) added to F; each bond's energy and virial counted once (o < po).
+__device__ __forceinline__ void bond_forces(const FinBonds &bd, const SysDev &S, const double4 *__restrict__ pos,
+                                            int i, const double4 &x, double &Fx, double &Fy, double &Fz,
+                                            double &ub, double &vb)
+{
+    const int o = bd.orig[i];
+    const int b0 = bd.bptr[S.off + o], b1 = bd.bptr[S.off + o + 1];
+    for (int b = b0; b < b1; ++b) {
+        const int po = bd.bpart[b];
+        const double4 xj = pos[bd.inv[S.off + po]];
+        double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
+        const double r2 = pbcr2_exact(dx, dy, dz, S), r1 = sqrt(r2);
+        const double term = r1 - bd.beq[b];
+        const int pw = bd.bpw[b];
+        double tp = 1.0;
+        for (int k = 0; k < pw - 1; ++k) tp *= term;
+        double fac = bd.bk[b] * tp;
+        const double u = fac * term;
+        fac = -(pw * fac / r1);
+        Fx += fac * dx;
+        Fy += fac * dy;
+        Fz += fac * dz;
+        if (o < po) {
+            ub += u;
+            vb -= fac * r2;
+        }
+    }
+}
+
 template <int P, class PR>
 __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles, const double4 *__restrict__ pos,
     const int *__restrict__ typ, const double *__restrict__ grid, const float *__restrict__ grid32,
-    const double4 *__restrict__ fsr, unsigned long long *__restrict__ fpart, int fstride,
+    const double4 *__restrict__ fsr, unsigned long long *__restrict__ fpart, int fstride, FinBonds bd,
     const double4 *__restrict__ fks, long long *__restrict__ eacc,
     const double *__restrict__ massip, const double *__restrict__ massp, double4 *__restrict__ ftot,
     double4 *__restrict__ forceo, double4 *__restrict__ vel, double4 *__restrict__ acc, int mode, FinOut out,
@@ -253,11 +226,11 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     __shared__ double sq[3];
     __shared__ double red[3][FIN_THREADS / 32];
     __shared__ bool last;
-    const Tile T = tiles[blockIdx.x];
+    const Tile T = tiles[blockIdx.x / FIN_SPLIT];
     const SysDev &S = sysv[T.sys];
     // FIN_LANES lanes per particle share the gather; the group's first lane does the rest
     const int g = threadIdx.x & (FIN_LANES - 1);
-    const int i = T.i0 + (int)threadIdx.x / FIN_LANES;
+    const int i = T.i0 + (int)(blockIdx.x % FIN_SPLIT) * FIN_PART + (int)threadIdx.x / FIN_LANES;
     long long *ea = eacc + (size_t)T.sys * EA_N;
     if (S.lsurf) {
         if (threadIdx.x < 3) sq[threadIdx.x] = acc_get(ea + EA_DIP + threadIdx.x);
@@ -283,16 +256,13 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 *py = 0ull;
                 *pz = 0ull;
             }
-            if (mode == 1) {
-                tyi = typ[i];
-                vold = vel[i];
-                aold = acc[i];
-            }
+            // the particle's bonds, before the gather, so that their registers are free again
+            if (bd.bptr) bond_forces(bd, S, pos, i, x, f0.x, f0.y, f0.z, ub, vb);
         }
     }
     if (S.lewald && !S.recstd) {
         // the y and z spline values of the block's particles, read by whichever lane takes a line
-        __shared__ R sTy[128][P], sDy[128][P], sTz[128][P], sDz[128][P];
+        __shared__ R sTy[FIN_PART][P], sDy[FIN_PART][P], sTz[FIN_PART][P], sDz[FIN_PART][P];
         const int pl = (int)threadIdx.x / FIN_LANES;
         const int s = S.s;
         R th0[P], dth0[P];
@@ -380,6 +350,12 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 Fz -= S.epsfp * (2.0 * fac) * x.w * sq[2];
             }
         }
+        if (mode == 1) {
+            // read after the gather: held across it they would cost the block its occupancy
+            tyi = typ[i];
+            vold = vel[i];
+            aold = acc[i];
+        }
         if (!isfinite(Fx) || !isfinite(Fy) || !isfinite(Fz)) raise_error(err, 7, T.sys, i, 0);
         ftot[i] = make_double4(Fx, Fy, Fz, 0.0);
         const double4 fo = make_double4(Fx * kForceFac, Fy * kForceFac, Fz * kForceFac, 0.0);
@@ -412,7 +388,7 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
     // ---- the last block of the system forms the system's totals ----
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(&out.fdone[T.sys], 1u) == (unsigned)(S.ntile128 - 1));
+    if (threadIdx.x == 0) last = (atomicAdd(&out.fdone[T.sys], 1u) == (unsigned)(FIN_SPLIT * S.ntile128 - 1));
     __syncthreads();
     if (!last) return;
     __threadfence();
