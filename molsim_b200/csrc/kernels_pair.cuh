@@ -1,7 +1,8 @@
-// kernels_pair.cuh -- UTwoBodyA (Src/energy.F90:445-544) over the full Verlet list.
+// kernels_pair.cuh -- UTwoBodyA (Src/energy.F90:445-544) over the Verlet list.
 //
-// k_pair (below) serves the FP64 path (and the mixed path on request); the
-// mixed path runs k_pair_m, further down, by default.
+// k_pair (below) serves the FP64 path over a full list; the mixed path runs
+// k_pair_h, at the end of this file, over a half list by default (or over a
+// full list), and keeps k_pair_m and k_pair<PrecM> as tuning alternatives.
 //
 // One particle per group of G lanes; the lanes stride over the particle's
 // row, so a row is read with coalesced 64-byte segments and every pair is
