@@ -85,6 +85,10 @@ struct SysDev {
     int fx_cubic, tab_smem_h;
     float fx2f, pad4;
     double fxd[3];
+    // SPME convolution kernel: radices of the grid edge's transform (pass count in
+    // the low 4 bits, radices in the 4-bit fields above; 0 when the edge goes
+    // through cuFFT) and the first entry of the edge's twiddle table
+    int fft_rad, fft_tw;
 };
 
 // One type pair's slice of the concatenated table.

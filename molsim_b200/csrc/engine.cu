@@ -22,6 +22,7 @@
 #include "../../include/molsim_gpu.h"
 #include "common.cuh"
 #include "kernels_force.cuh"
+#include "kernels_spme.cuh"
 #include "kernels_md.cuh"
 #include "kernels_ewald.cuh"
 #include "kernels_mc.cuh"
@@ -132,8 +133,26 @@ struct FftPart {
 struct FftClass {
     int s, count;
     long long grid_off, cgrid_off;
+    int rad = 0;                 // > 0: the edge goes through the convolution kernel, not cuFFT
     std::vector<FftPart> parts;
 };
+
+// Radices of the convolution kernel's transform of length s (pass count in the
+// low 4 bits, radices above), or 0 when the edge is left to cuFFT: odd, beyond
+// four passes of 8, 5, 4, 3 and 2, or with planes too large for shared memory.
+int conv_radices(int s)
+{
+    if (s < 8 || (s & 1) || s > CONV_MAX_EDGE || 32LL * s * (s / 2 + 1) > CONV_MAX_SMEM) return 0;
+    int rad = 0, np = 0, n = s;
+    for (int r : {8, 4, 5, 3, 2})
+        while (n % r == 0 && n > 1) {
+            if (np == 4) return 0;
+            rad |= r << (4 + 4 * np);
+            ++np;
+            n /= r;
+        }
+    return n == 1 ? (rad | np) : 0;
+}
 
 }  // namespace
 
@@ -258,6 +277,12 @@ struct msg_handle {
     unsigned long long *igrid = nullptr;
     long long grid_tot = 0, cgrid_tot = 0;
     std::vector<FftClass> fft;
+    // convolution kernel: tasks, counters, twiddle tables, buffer size, grid
+    int4 *conv_tasks = nullptr;
+    unsigned *conv_ctr = nullptr;
+    double2 *conv_tw = nullptr;
+    float2 *conv_tw32 = nullptr;
+    int conv_ntasks = 0, conv_nctr = 0, conv_cap = 0, conv_grid = 0;
     // staging
     double *stage = nullptr;
     size_t stage_n = 0;
@@ -439,7 +464,8 @@ static void free_all(msg_handle *h)
                     h->ew_sk, h->ew_fks, h->mc_rng, h->mc_u, h->mc_dtr, h->mc_cnt, h->mc_par, h->ew_sktm,
                     h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig,
                     h->mc_jumpt, h->mca_psave, h->mca_esave, h->mca_beta, h->mca_acc, h->mca_step,
-                    h->mca_flag, h->llinfo, h->istep2, h->tch};
+                    h->mca_flag, h->llinfo, h->istep2, h->tch, h->conv_tasks, h->conv_ctr, h->conv_tw,
+                    h->conv_tw32};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -651,6 +677,13 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         for (int s = 0; s < n; ++s)
             if (hs[s].lewald && !hs[s].recstd) bys[hs[s].s].push_back(s);
         long long go = 0, co = 0, fo_acc = 0;
+        // MSG_SPME_CONV=1 at handle creation: the convolution kernel takes every edge it
+        // supports (the rest stays on cuFFT); the choice depends on the edge alone, so a
+        // system's result does not depend on the systems batched with it.  Off by default:
+        // on the bench's workloads it runs no faster than the cuFFT chain.
+        const char *ev_conv = std::getenv("MSG_SPME_CONV");
+        const bool conv_on = ev_conv && std::atoi(ev_conv) != 0;
+        std::vector<double2> tw;
         for (auto &kv : bys) {
             const int e = kv.first;
             FftClass fc;
@@ -658,13 +691,44 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             fc.count = (int)kv.second.size();
             fc.grid_off = go;
             fc.cgrid_off = co;
+            fc.rad = conv_on ? conv_radices(e) : 0;
+            const int tw_off = (int)tw.size();
+            if (fc.rad) {
+                // exp(-2 pi i m / e), m = 0..e-1
+                for (int m = 0; m < e; ++m) {
+                    const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)e;
+                    tw.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+                }
+                conv_cap = std::max(conv_cap, e * (e / 2 + 1));
+            }
             for (int s : kv.second) {
                 hs[s].grid_off = go;
                 hs[s].cgrid_off = co;
+                hs[s].fft_rad = fc.rad;
+                hs[s].fft_tw = fc.rad ? tw_off : 0;
                 go += (long long)e * e * e;
                 co += (long long)e * e * (e / 2 + 1);
             }
             fft.push_back(fc);
+        }
+        if (!tw.empty()) {
+            // tasks in stage order: every FWD plane, then every ZSLAB, then every BWD plane
+            std::vector<int4> ct;
+            for (int kind = CONV_FWD; kind <= CONV_BWD; ++kind)
+                for (int s = 0; s < n; ++s)
+                    if (hs[s].lewald && !hs[s].recstd && hs[s].fft_rad)
+                        for (int z = 0; z < hs[s].s; ++z) ct.push_back(make_int4(s, kind, z, 0));
+            conv_ntasks = (int)ct.size();
+            conv_tasks = dalloc<int4>(ct.size());
+            up(conv_tasks, ct.data(), ct.size() * sizeof(int4));
+            conv_nctr = CONV_HDR + 2 * n;
+            conv_ctr = dalloc<unsigned>(conv_nctr);
+            std::vector<float2> tw32(tw.size());
+            for (size_t k = 0; k < tw.size(); ++k) tw32[k] = make_float2((float)tw[k].x, (float)tw[k].y);
+            conv_tw = dalloc<double2>(tw.size());
+            conv_tw32 = dalloc<float2>(tw.size());
+            up(conv_tw, tw.data(), tw.size() * sizeof(double2));
+            up(conv_tw32, tw32.data(), tw32.size() * sizeof(float2));
         }
         for (int s = 0; s < n; ++s)
             if (hs[s].lewald && !hs[s].recstd) {
@@ -698,7 +762,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         // influence work items
         std::vector<int4> it;
         for (int s = 0; s < n; ++s) {
-            if (!hs[s].lewald || hs[s].recstd) continue;
+            if (!hs[s].lewald || hs[s].recstd || hs[s].fft_rad) continue;
             const int e = hs[s].s;
             const int nc = e * e * (e / 2 + 1);
             hs[s].infl_off = (int)it.size();
@@ -1116,6 +1180,21 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         pair_blocks_max = nsm * std::max(1, per);
         if (prec != MSG_PREC_MIXED) pair_blocks_lean = pair_blocks_max;
         pair_grid = std::max(1, std::min(nptask, pair_blocks_max));
+        if (conv_ntasks) {
+            // convolution kernel: one block per SM (a block waiting for its system's
+            // previous stage holds its SM's registers and shared memory, which the pair
+            // kernel beside it needs), at most as many as the widest stage has tasks.  The shared-memory limit is
+            // the kernel's largest (a process-wide attribute, shared by every handle).
+            const int smax = (int)conv_smem_bytes(CONV_MAX_SMEM / (2 * (int)sizeof(double2)));
+            if (prec == MSG_PREC_MIXED)
+                CK(cudaFuncSetAttribute(k_spme_conv<PrecM>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            else
+                CK(cudaFuncSetAttribute(k_spme_conv<PrecD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+            int widest = 0;   // tasks of the widest stage (one per plane or slab of every system)
+            for (int s = 0; s < n; ++s)
+                if (hs[s].lewald && !hs[s].recstd && hs[s].fft_rad) widest += hs[s].s;
+            conv_grid = std::max(1, std::min(widest, nsm));
+        }
     }
     if (!dry) CK(cudaStreamSynchronize(st));
 }
@@ -1214,6 +1293,7 @@ void msg_handle::plan_fft()
     const int f32 = prec == MSG_PREC_MIXED ? 1 : 0;
     size_t need = 0;
     for (auto &fc : fft) {
+        if (fc.rad) continue;   // the convolution kernel's edge
         long long go = fc.grid_off, co = fc.cgrid_off;
         const long long rs = (long long)fc.s * fc.s * fc.s, cs = (long long)fc.s * fc.s * (fc.s / 2 + 1);
         for (int bit = 30; bit >= 0; --bit) {
@@ -1321,9 +1401,26 @@ static void launch_spme(msg_handle *h)
     k_spread<P, PR><<<h->nt128 * (128 / SPREAD_PART), SPREAD_THREADS, 0, h->st>>>(h->dsys, h->t128, h->pos[0], h->rgrid, h->igrid,
                                                   h->eacc);
     h->launches += 1;
-    k_grid_to_f64<<<(unsigned)((h->grid_tot + 255) / 256), 256, 0, h->st>>>(h->igrid, h->rgrid, h->grid_tot);
-    h->launches += 1;
+    bool cufft = false;
+    for (auto &fc : h->fft) {
+        if (fc.rad) continue;
+        // cuFFT edges: the fixed-point grid to the FP64 input of the forward transform
+        const long long ng = (long long)fc.count * fc.s * fc.s * fc.s;
+        k_grid_to_f64<<<(unsigned)((ng + 255) / 256), 256, 0, h->st>>>(h->igrid + fc.grid_off, h->rgrid + fc.grid_off, ng);
+        h->launches += 1;
+        cufft = true;
+    }
     h->tend(TM_SPREAD);
+    if (h->conv_ntasks) {
+        h->tbeg(TM_FFT);
+        k_spme_conv<PR><<<h->conv_grid, CONV_THREADS, conv_smem_bytes(h->conv_cap), h->st>>>(
+            h->dsys, h->conv_tasks, h->conv_ntasks, h->conv_cap, h->igrid, h->cgrid, h->cgrid32, h->rgrid,
+            h->rgrid32, h->conv_tw, h->conv_tw32, h->mfac, h->emf, h->vmf, h->eacc, h->conv_ctr, h->conv_nctr,
+            h->errw);
+        h->launches += 1;
+        h->tend(TM_FFT);
+    }
+    if (!cufft) return;
     h->tbeg(TM_FFT);
     for (auto &fc : h->fft)
         for (auto &f : fc.parts)
