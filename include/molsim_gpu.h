@@ -183,6 +183,11 @@ int  msg_get_forces(msg_handle *h, int32_t isys, double *force, double *forceo);
  * changes results. */
 #define MSG_TUNE_OVERLAP 4
 #define MSG_TUNE_PAIR_BLOCKS 5
+/* MSG_TUNE_CONV_BLOCKS: blocks per SM of the persistent SPME convolution kernel
+ * of a handle created with MSG_SPME_CONV=1 in the environment (0, the default:
+ * one per SM, at most one per plane of the handle's grids).  No effect on other
+ * handles; results do not depend on it. */
+#define MSG_TUNE_CONV_BLOCKS 6
 int  msg_tune(msg_handle *h, int32_t key, int32_t value);
 
 /* rodd = massip * forceo (GetLinAcc) from the last msg_utotal. */

@@ -17,6 +17,7 @@ MSG_TUNE_PAIR_KERNEL = 2
 MSG_TUNE_PAIR_UNROLL = 3
 MSG_TUNE_OVERLAP = 4
 MSG_TUNE_PAIR_BLOCKS = 5
+MSG_TUNE_CONV_BLOCKS = 6
 STATUS = {0: "ok", 1: "r2 < r2umin", 2: "table interval overrun", 3: "neighbour capacity exceeded",
           4: "CUDA error", 5: "device timeout", 6: "invalid argument", 7: "non-finite force",
           8: "hard-core overlap"}

@@ -283,6 +283,8 @@ struct msg_handle {
     double2 *conv_tw = nullptr;
     float2 *conv_tw32 = nullptr;
     int conv_ntasks = 0, conv_nctr = 0, conv_cap = 0, conv_grid = 0;
+    int conv_widest = 0, conv_occ = 1;   // tasks of the widest stage; blocks per SM that fit
+    void set_conv_grid(int per_sm);
     // staging
     double *stage = nullptr;
     size_t stage_n = 0;
@@ -1186,17 +1188,31 @@ void msg_handle::build(const msg_params *P, int n, int precision)
             // kernel beside it needs), at most as many as the widest stage has tasks.  The shared-memory limit is
             // the kernel's largest (a process-wide attribute, shared by every handle).
             const int smax = (int)conv_smem_bytes(CONV_MAX_SMEM / (2 * (int)sizeof(double2)));
-            if (prec == MSG_PREC_MIXED)
+            const int smem = (int)conv_smem_bytes(conv_cap);
+            if (prec == MSG_PREC_MIXED) {
                 CK(cudaFuncSetAttribute(k_spme_conv<PrecM>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            else
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&conv_occ, k_spme_conv<PrecM>, CONV_THREADS, smem));
+            } else {
                 CK(cudaFuncSetAttribute(k_spme_conv<PrecD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
-            int widest = 0;   // tasks of the widest stage (one per plane or slab of every system)
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&conv_occ, k_spme_conv<PrecD>, CONV_THREADS, smem));
+            }
+            conv_occ = std::max(1, conv_occ);
+            conv_widest = 0;   // tasks of the widest stage (one per plane or slab of every system)
             for (int s = 0; s < n; ++s)
-                if (hs[s].lewald && !hs[s].recstd && hs[s].fft_rad) widest += hs[s].s;
-            conv_grid = std::max(1, std::min(widest, nsm));
+                if (hs[s].lewald && !hs[s].recstd && hs[s].fft_rad) conv_widest += hs[s].s;
+            set_conv_grid(0);
         }
     }
     if (!dry) CK(cudaStreamSynchronize(st));
+}
+
+// Grid of the convolution kernel: per_sm blocks on every SM (at most as many as
+// fit), or with per_sm = 0 one per SM and at most one per task of the widest stage.
+void msg_handle::set_conv_grid(int per_sm)
+{
+    if (!conv_ntasks) return;
+    conv_grid = per_sm > 0 ? std::min(conv_ntasks, nsm * std::min(per_sm, conv_occ)) : std::min(conv_widest, nsm);
+    conv_grid = std::max(1, conv_grid);
 }
 
 // Persistent grid of the lean pair kernel for its current unroll: as many
@@ -2213,6 +2229,12 @@ extern "C" int msg_tune(msg_handle *h, int32_t key, int32_t value)
             h->drop_graph();
             h->pair_per_sm = value;
         }
+        return MSG_OK;
+    }
+    if (key == MSG_TUNE_CONV_BLOCKS) {
+        if (value < 0 || value > 32) return MSG_ERR_ARG;
+        h->drop_graph();
+        h->set_conv_grid(value);
         return MSG_OK;
     }
     if (key == MSG_TUNE_PAIR_KERNEL) {
