@@ -105,3 +105,22 @@ def test_conv_trajectory_matches_cufft(precision, monkeypatch):
     for x, y in zip(eg, ec):
         assert Hp.rel(x["utot"], y["utot"]) < tol
     assert np.abs(g.get_state()["ro"] - c.get_state()["ro"]).max() < (1e-8 if precision == "fp64" else 1e-4)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_conv_blocks_do_not_change_results(precision, monkeypatch):
+    """Blocks per SM of the convolution kernel (MSG_TUNE_CONV_BLOCKS) move work between
+    blocks only: forces and energies stay bit for bit the same."""
+    from molsim_b200 import _lib
+
+    sys_list = [_system(64, seed=7), _system(24, seed=8)]
+    tabs = [Hp.oracle_table(s) for s in sys_list]
+    g = _conv_engine(monkeypatch, sys_list, tabs, precision=precision)
+    ref = [g.UTotal(k) for k in range(2)]
+    for blocks in (1, 3, 0):
+        assert _lib.lib().msg_tune(g.h, _lib.MSG_TUNE_CONV_BLOCKS, blocks) == 0
+        for k in range(2):
+            r = g.UTotal(k)
+            assert np.array_equal(r["force"], ref[k]["force"])
+            assert r["urec"] == ref[k]["urec"] and r["virial"] == ref[k]["virial"]
+    assert _lib.lib().msg_tune(g.h, _lib.MSG_TUNE_CONV_BLOCKS, -1) != 0
