@@ -295,8 +295,12 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
                 const int nx = km[0] - ix;
                 nxs[ix] = nx + ((nx < 0) ? s : 0);
             }
-            // the P*P (iy, iz) grid lines of the particle, dealt round the group's lanes
-            for (int l = g; l < P * P; l += FIN_LANES) {
+            // the P*P (iy, iz) grid lines of the particle, dealt round the group's lanes;
+            // unrolled so that the lane's grid loads go out together
+#pragma unroll
+            for (int t = 0; t < (P * P + FIN_LANES - 1) / FIN_LANES; ++t) {
+                const int l = g + t * FIN_LANES;
+                if (l >= P * P) break;
                 const int iy = l % P, iz = l / P;
                 int nz = km[2] - iz;
                 nz += (nz < 0) ? s : 0;
