@@ -1141,7 +1141,7 @@ void msg_handle::build(const msg_params *P, int n, int precision)
     v0 = dalloc<uint32_t>(ntot);
     k1 = dalloc<uint32_t>(ntot);
     v1 = dalloc<uint32_t>(ntot);
-    rhist = dalloc<uint32_t>((size_t)RS_BINS * ((ntot + RS_TILE - 1) / RS_TILE));
+    rhist = dalloc<uint32_t>((size_t)RS_BINS * ((ntot + RS_TILE - 1) / RS_TILE) + RS_BINS);
     cstart = dalloc<int>(ncell_tot);
     cend = dalloc<int>(ncell_tot);
     nbl = dalloc<int>(nbl_tot);

@@ -3,8 +3,8 @@
 // Used by the Verlet-cell rebuild so that the new particle order is a pure
 // function of the positions: (cell, previous order), which for rebuilt
 // systems is (cell, MOLSIM index).  8-bit digits; each pass is a histogram
-// kernel, one exclusive scan over the (digit, block) table and a stable
-// scatter.  1024 items per block (256 threads x 4 rounds); within a round
+// kernel, an exclusive scan of each digit's per-block counts (one block per
+// digit) and a stable scatter that adds the digits' bases.  1024 items per block (256 threads x 4 rounds); within a round
 // the item order is the thread order, so ranks come from __match_any_sync
 // plus per-warp digit counts in shared memory.
 #pragma once
@@ -37,52 +37,39 @@ __global__ void __launch_bounds__(RS_THREADS) rs_hist(const uint32_t *__restrict
     for (int b = threadIdx.x; b < NB; b += RS_THREADS) hist[b * gridDim.x + blockIdx.x] = cnt[b];
 }
 
-// Exclusive scan of len entries in place, one block of 1024 threads.
-__global__ void __launch_bounds__(1024) rs_scan(uint32_t *__restrict__ a, int len)
+// Exclusive scan of each digit's row of per-tile counts in place (row d holds
+// hist[d * ntile + tile]), one block per digit, 256 consecutive entries at a
+// time; the row total goes to tot[d].  The scatter adds the exclusive scan of
+// the totals (the digit's base), so the two together give the exclusive scan
+// of the whole (digit, tile) table.
+__global__ void __launch_bounds__(RS_THREADS) rs_scan(uint32_t *__restrict__ hist, int ntile,
+                                                      uint32_t *__restrict__ tot)
 {
-    __shared__ uint32_t wsum[32];
-    const int t = threadIdx.x, per = (len + 1023) / 1024;
-    const int b = t * per, e = min(len, b + per);
-    uint32_t s = 0;
-    // eight independent loads in flight per thread
-    for (int i0 = b; i0 < e; i0 += 8) {
-        uint32_t x[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) x[k] = (i0 + k < e) ? a[i0 + k] : 0u;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) s += x[k];
-    }
-    // inclusive warp scan of the per-thread sums
-    uint32_t v = s;
-    const int lane = t & 31, w = t >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += y;
-    }
-    if (lane == 31) wsum[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        uint32_t x = wsum[lane];
+    __shared__ uint32_t wsum[RS_WARPS];
+    uint32_t *row = hist + (size_t)blockIdx.x * ntile;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < ntile; b0 += RS_THREADS) {
+        const int i = b0 + t;
+        const uint32_t x = i < ntile ? row[i] : 0u;
+        uint32_t v = x;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
         }
-        wsum[lane] = x;
-    }
-    __syncthreads();
-    uint32_t run = v - s + (w > 0 ? wsum[w - 1] : 0u);
-    for (int i0 = b; i0 < e; i0 += 8) {
-        uint32_t x[8];
+        if (lane == 31) wsum[w] = v;
+        __syncthreads();
+        uint32_t before = carry;
+        for (int k = 0; k < w; ++k) before += wsum[k];
+        uint32_t all = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) x[k] = (i0 + k < e) ? a[i0 + k] : 0u;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (i0 + k < e) a[i0 + k] = run;
-            run += x[k];
-        }
+        for (int k = 0; k < RS_WARPS; ++k) all += wsum[k];
+        if (i < ntile) row[i] = before + v - x;
+        carry += all;
+        __syncthreads();
     }
+    if (t == 0) tot[blockIdx.x] = carry;
 }
 
 template <int NB>
@@ -90,15 +77,30 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t *__restr
                                                          const uint32_t *__restrict__ vin,
                                                          uint32_t *__restrict__ kout,
                                                          uint32_t *__restrict__ vout, int n, int shift,
-                                                         const uint32_t *__restrict__ offs)
+                                                         const uint32_t *__restrict__ offs,
+                                                         const uint32_t *__restrict__ tot)
 {
+    static_assert(NB == RS_THREADS, "one digit per thread");
     __shared__ uint32_t base[NB];
     __shared__ uint32_t wcnt[RS_WARPS][NB];
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-    for (int b = t; b < NB; b += RS_THREADS) {
-        base[b] = offs[b * gridDim.x + blockIdx.x];
+    // the digit's base: exclusive scan of the digit totals
+    {
+        const uint32_t x = tot[t];
+        uint32_t v = x;
 #pragma unroll
-        for (int ww = 0; ww < RS_WARPS; ++ww) wcnt[ww][b] = 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane == 31) wcnt[0][w] = v;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int k = 0; k < w; ++k) before += wcnt[0][k];
+        __syncthreads();
+        base[t] = before + v - x + offs[t * gridDim.x + blockIdx.x];
+#pragma unroll
+        for (int ww = 0; ww < RS_WARPS; ++ww) wcnt[ww][t] = 0;
     }
     __syncthreads();
     const int blockbase = blockIdx.x * RS_TILE;
@@ -137,7 +139,7 @@ __global__ void __launch_bounds__(RS_THREADS) rs_scatter(const uint32_t *__restr
 
 // Sort n pairs by the low `bits` bits of the key in 8-bit passes.  k0/v0 hold
 // the input; k1/v1 are scratch of the same size; hist needs 256*ceil(n/1024)
-// entries.  Returns true when the sorted data ended in (k1, v1), false when in
+// + 256 entries (the per-tile counts, then the digit totals).  Returns true when the sorted data ended in (k1, v1), false when in
 // (k0, v0).  Sets *launches.
 inline bool radix_sort_pairs(uint32_t *k0, uint32_t *v0, uint32_t *k1, uint32_t *v1, uint32_t *hist,
                              int n, int bits, cudaStream_t st, int *launches = nullptr)
@@ -149,9 +151,10 @@ inline bool radix_sort_pairs(uint32_t *k0, uint32_t *v0, uint32_t *k1, uint32_t 
     for (int shift = 0; shift < bits; shift += 8) {
         uint32_t *ki = flip ? k1 : k0, *vi = flip ? v1 : v0;
         uint32_t *ko = flip ? k0 : k1, *vo = flip ? v0 : v1;
+        uint32_t *tot = hist + (size_t)RS_BINS * nb;
         rs_hist<RS_BINS><<<nb, RS_THREADS, 0, st>>>(ki, n, shift, hist);
-        rs_scan<<<1, 1024, 0, st>>>(hist, RS_BINS * nb);
-        rs_scatter<RS_BINS><<<nb, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n, shift, hist);
+        rs_scan<<<RS_BINS, RS_THREADS, 0, st>>>(hist, nb, tot);
+        rs_scatter<RS_BINS><<<nb, RS_THREADS, 0, st>>>(ki, vi, ko, vo, n, shift, hist, tot);
         if (launches) *launches += 3;
         flip = !flip;
     }
