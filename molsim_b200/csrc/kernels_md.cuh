@@ -549,7 +549,8 @@ __device__ __forceinline__ bool llist_owner(int ip, int jp)
 // r2 < (rcut+drnlist)^2 (SetVListMD's test, Src/nlist.F90:746-751), compacted
 // with a warp ballot.  Rows are ordered by stencil cell, then by MOLSIM index.
 // half = 0: full list (each pair in both rows); half = 1: each pair once, in the
-// row half_owner names.  With lvlistllist a pair also needs its MOLSIM row owner
+// row half_owner names (only those candidates are read: every other index on
+// either side of i).  With lvlistllist a pair also needs its MOLSIM row owner
 // (SetVListMDLList's rule) to reach the partner's cell with SetNCell's probes, so
 // the list holds SetVListMDLList's pair set (which can leave out skin pairs).
 __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, const int *__restrict__ sys,
@@ -582,30 +583,43 @@ __global__ void __launch_bounds__(256) k_nlist(const SysDev *__restrict__ sysv, 
         li = llinfo[i];
         ip = orig[i] + 1;
     }
+    // the pair test of candidates a, a+step, ... below b, 32 at a time, compacted into the row
+    auto scan = [&](int a, int b, int step) {
+        for (int jb = a; jb < b; jb += 32 * step) {
+            const int j = jb + lane * step;
+            bool ok = false;
+            if (j < b && j != i) {
+                const double4 xj = pos[j];
+                double dx = __dsub_rn(xi.x, xj.x), dy = __dsub_rn(xi.y, xj.y), dz = __dsub_rn(xi.z, xj.z);
+                ok = pbcr2_exact(dx, dy, dz, S) < S.rs2cut;
+                if (ok && ll) {
+                    const int4 lj = llinfo[j];
+                    ok = llist_owner(ip, orig[j] + 1) ? llist_marked(li, lj.x) : llist_marked(lj, li.x);
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int slot = count + __popc(bal & lt);
+                // entry: partner index, partner type in bits 28-29
+                if (slot < S.cap) row[slot] = j | (typ[j] << 28);
+            }
+            count += __popc(bal);
+        }
+    };
     for (int a = 0; a < nz; ++a)
         for (int b = 0; b < ny; ++b)
             for (int e = 0; e < nx; ++e) {
                 const int cc = S.cell_off + (sz[a] * S.ncell[1] + sy[b]) * S.ncell[0] + sx[e];
                 const int j0 = cstart[cc], j1 = cend[cc];
-                for (int jb = j0; jb < j1; jb += 32) {
-                    const int j = jb + lane;
-                    bool ok = false;
-                    if (j < j1 && j != i && (!half || half_owner(i, j))) {
-                        const double4 xj = pos[j];
-                        double dx = __dsub_rn(xi.x, xj.x), dy = __dsub_rn(xi.y, xj.y), dz = __dsub_rn(xi.z, xj.z);
-                        ok = pbcr2_exact(dx, dy, dz, S) < S.rs2cut;
-                        if (ok && ll) {
-                            const int4 lj = llinfo[j];
-                            ok = llist_owner(ip, orig[j] + 1) ? llist_marked(li, lj.x) : llist_marked(lj, li.x);
-                        }
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                    if (ok) {
-                        const int slot = count + __popc(bal & lt);
-                        // entry: partner index, partner type in bits 28-29
-                        if (slot < S.cap) row[slot] = j | (typ[j] << 28);
-                    }
-                    count += __popc(bal);
+                if (half) {
+                    // the partners half_owner gives row i: below i those of i's parity,
+                    // above i those of the other parity (every other index, in order)
+                    scan(j0 + ((j0 ^ i) & 1), min(j1, i), 2);
+                    int jb = max(j0, i + 1);
+                    jb += ((jb + i) & 1) ^ 1;
+                    scan(jb, j1, 2);
+                } else {
+                    scan(j0, j1, 1);
                 }
             }
     if (lane == 0) {
