@@ -262,6 +262,32 @@ def _check_nlist_fast(o, g, n):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_past_one_scan_round_equals_alone(precision):
+    """Two copies of the 200,000-particle BD config in one handle: 400,000 keys make the
+    list rebuild's radix sort scan each digit's tile counts in more than one round of 256
+    tiles (a copy alone needs one).  Each copy's list and forces equal the copy alone, bit
+    for bit."""
+    s = Hp.config2()
+    t = Hp.oracle_table(s)
+    sb = [dict(s), dict(s)]
+    sb[1]["ro"] = np.array(s["ro"])[::-1].copy()      # the second copy in another MOLSIM order
+    sb[1]["iptpn"] = np.array(s["iptpn"])[::-1].copy()
+    sb[1]["az"] = np.array(s["az"])[::-1].copy()
+    if "rod" in s:
+        sb[1]["rod"] = np.array(s["rod"])[::-1].copy()
+    gb = Engine(sb, [t, t], precision=precision, maxnneigh=256)
+    for k in range(2):
+        ga = Engine(sb[k], t, precision=precision, maxnneigh=256)
+        ra, rb = ga.UTotal(), gb.UTotal(k)
+        assert np.array_equal(rb["force"], ra["force"]), k
+        assert rb["utot"] == ra["utot"] and rb["virial"] == ra["virial"], k
+        nn_a, jp_a, _ = ga.SetVList(0, export=True, maxnneigh=256)
+        nn_b, jp_b, _ = gb.SetVList(k, export=True, maxnneigh=256)
+        assert np.array_equal(nn_a, nn_b) and np.array_equal(jp_a, jp_b), k
+        del ga
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_config2_colloid_bd_full_size(precision):
     """The 200,000-particle Brownian-dynamics config at full size against the oracle with
     its cell-list build: pair set bit-exact, UTotal, and two BD steps with injected noise."""
