@@ -390,9 +390,13 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(
         acc_add(ea + EA_UBOND + threadIdx.x, a);
     }
     // ---- the last block of the system forms the system's totals ----
-    __threadfence();
+    // (the block's energy atomics above are ordered before its count by the barrier
+    // and one thread's fence)
     __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(&out.fdone[T.sys], 1u) == (unsigned)(FIN_SPLIT * S.ntile128 - 1));
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = (atomicAdd(&out.fdone[T.sys], 1u) == (unsigned)(FIN_SPLIT * S.ntile128 - 1));
+    }
     __syncthreads();
     if (!last) return;
     __threadfence();
