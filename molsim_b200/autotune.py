@@ -123,10 +123,12 @@ def tune_pair_lanes(engine, shifts=(-1, 0, 1), steps=10):
     return best, times
 
 
-def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2), kinds=(2, 3)):
+def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2), kinds=(2, 3),
+                     overlaps=(1, 0)):
     """Shape of the pair kernel for this handle, by timing MD steps: the list layout
     (kind 2: half list with partner atomics, 3: full list), lanes per particle
-    (2^shift times the default), row entries in flight per lane (unroll), and pair blocks
+    (2^shift times the default), row entries in flight per lane (unroll), whether the
+    pair kernel runs beside the SPME chain or after it (overlap 1 or 0), and pair blocks
     per SM (0: as many as fit; 2: room for the SPME chain beside it), one knob at a time
     from the defaults.  Leaves the engine on the best; returns ({knob: value}, {setting:
     ms per step}).  Mixed precision only (the knobs belong to its pair kernel).  Every
@@ -139,10 +141,11 @@ def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blo
         if L.msg_tune(engine.h, key, int(val)):
             raise RuntimeError("msg_tune(%d, %d) failed" % (key, val))
 
-    best = {"kind": 2, "shift": 0, "unroll": 2, "blocks": 0}
+    best = {"kind": 2, "shift": 0, "unroll": 2, "overlap": 1, "blocks": 0}
     log = {}
     for name, vals, key in (("kind", kinds, _lib.MSG_TUNE_PAIR_KERNEL), ("shift", shifts, None),
                             ("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
+                            ("overlap", overlaps, _lib.MSG_TUNE_OVERLAP),
                             ("blocks", blocks, _lib.MSG_TUNE_PAIR_BLOCKS)):
         res = {}
         for v in vals:
