@@ -229,6 +229,7 @@ struct msg_handle {
     int has_bd = 0, has_bonds = 0;
     // bonds
     int *bptr = nullptr, *bpart = nullptr, *bpw = nullptr;
+    int4 *btab = nullptr;       // per-particle bond table (every particle with at most two bonds)
     double *bk = nullptr, *beq = nullptr;
     // Ewald sums: any_ewald = any system with one (SPME or standard), any_spme / any_std by method
     int any_ewald = 0, any_spme = 0, any_std = 0;
@@ -467,7 +468,7 @@ static void free_all(msg_handle *h)
                     h->elc_kv, h->elc_kfac, h->elc_st, h->elc_sttm, h->mc_F, h->mc_rg, h->mc_ig,
                     h->mc_jumpt, h->mca_psave, h->mca_esave, h->mca_beta, h->mca_acc, h->mca_step,
                     h->mca_flag, h->llinfo, h->istep2, h->tch, h->conv_tasks, h->conv_ctr, h->conv_tw,
-                    h->conv_tw32};
+                    h->conv_tw32, h->btab};
     if (!h->dry && h->st) {
         for (void *p : ptrs) h->dfree(p);
         h->dfree(h->fftwork);
@@ -1069,6 +1070,22 @@ void msg_handle::build(const msg_params *P, int n, int precision)
         up(bpw, pw.data(), pw.size() * sizeof(int));
         up(bk, kk.data(), kk.size() * sizeof(double));
         up(beq, eq.data(), eq.size() * sizeof(double));
+        // the bond table, in the initial internal order (MOLSIM order within each system),
+        // when no particle has more than two bonds; list rebuilds rewrite it
+        int maxdeg = 0;
+        for (int i = 0; i < ntot; ++i) maxdeg = std::max(maxdeg, deg[i + 1] - deg[i]);
+        if (deg[ntot] > 0 && maxdeg <= 2) {
+            std::vector<int4> bt(ntot, make_int4(-1, 0, -1, 0));
+            for (int s = 0; s < n; ++s)
+                for (int i = 0; i < P[s].np; ++i) {
+                    const int g = hs[s].off + i, b0 = deg[g], b1 = deg[g + 1];
+                    if (b0 < b1) bt[g].x = hs[s].off + part[b0], bt[g].y = b0 | (i < part[b0] ? BT_COUNT : 0);
+                    if (b0 + 1 < b1)
+                        bt[g].z = hs[s].off + part[b0 + 1], bt[g].w = (b0 + 1) | (i < part[b0 + 1] ? BT_COUNT : 0);
+                }
+            btab = dalloc<int4>(ntot);
+            up(btab, bt.data(), ntot * sizeof(int4));
+        }
     }
 
     // --- work lists ---
@@ -1400,6 +1417,10 @@ void msg_handle::enqueue_rebuild()
                                       ntot);
     k_copyback<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], pos[1], vel[0], vel[1], acc[0], acc[1], fo[0],
                                        fo[1], typ[0], typ[1], orig[0], orig[1], dsum[0], posfx);
+    if (btab) {
+        k_bond_table<<<nt128, 128, 0, st>>>(dsys, t128, flag, orig[0], inv, bptr, bpart, btab);
+        launches += 1;
+    }
     if (any_llist) {
         k_llist_info<<<nt128, 128, 0, st>>>(dsys, t128, flag, pos[0], llinfo);
         launches += 1;
@@ -1476,7 +1497,8 @@ static void launch_finalize(msg_handle *h, int mode, bool record)
     h->launches += 1;
     k_finalize<P, PR><<<h->nt128 * FIN_SPLIT, FIN_THREADS, 0, h->st>>>(
         h->dsys, h->t128, h->pos[0], h->typ[0], h->rgrid, h->rgrid32, h->fsr, h->list_half ? h->fpart : nullptr,
-        h->ntot, FinBonds{h->orig[0], h->inv, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bpw, h->bk, h->beq},
+        h->ntot, FinBonds{h->orig[0], h->inv, h->has_bonds ? h->bptr : nullptr, h->bpart, h->bpw, h->bk, h->beq,
+                          h->has_bonds ? h->btab : nullptr},
         h->ew_fks, h->eacc, h->massip, h->massp,
         h->ftot, h->fo[0], h->vel[0], h->acc[0], mode, fo, h->errw);
     h->tend(TM_FINAL);

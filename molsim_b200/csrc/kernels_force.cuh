@@ -180,35 +180,85 @@ struct FinOut {
 struct FinBonds {
     const int *orig, *inv, *bptr, *bpart, *bpw;
     const double *bk, *beq;
+    const int4 *tab;   // per-particle bond table in internal order, or null (CSR walk)
 };
+
+// Bond table entry flag: this end counts the bond's energy and virial (UBond's o < po).
+constexpr int BT_COUNT = 1 << 30;
+
+// Per-particle bond table for systems whose particles have at most two bonds: entry
+// k of particle i = (internal index of its k-th partner, CSR slot of the bond |
+// BT_COUNT when this end counts its energy), partner -1 when absent.  Written for
+// the rebuilt systems after their particles are re-ordered, so that the finalize
+// reads a particle's bonds with one load and its partners' positions with one more.
+__global__ void __launch_bounds__(128) k_bond_table(const SysDev *__restrict__ sysv, const Tile *__restrict__ tiles,
+                                                   const int *__restrict__ flag, const int *__restrict__ orig,
+                                                   const int *__restrict__ inv, const int *__restrict__ bptr,
+                                                   const int *__restrict__ bpart, int4 *__restrict__ tab)
+{
+    const Tile T = tiles[blockIdx.x];
+    if (!flag[T.sys]) return;
+    const int i = T.i0 + threadIdx.x;
+    if (i >= T.i1) return;
+    const SysDev &S = sysv[T.sys];
+    const int o = orig[i];
+    const int b0 = bptr[S.off + o], b1 = bptr[S.off + o + 1];
+    int4 e = make_int4(-1, 0, -1, 0);
+    if (b0 < b1) {
+        const int po = bpart[b0];
+        e.x = inv[S.off + po];
+        e.y = b0 | (o < po ? BT_COUNT : 0);
+    }
+    if (b0 + 1 < b1) {
+        const int po = bpart[b0 + 1];
+        e.z = inv[S.off + po];
+        e.w = (b0 + 1) | (o < po ? BT_COUNT : 0);
+    }
+    tab[i] = e;
+}
+
+// One bond of particle i (position x) with its partner at xj: its force added to F;
+// its energy and virial counted when this end counts them.
+__device__ __forceinline__ void bond_term(const FinBonds &bd, const SysDev &S, const double4 &x, const double4 &xj,
+                                          int b, bool count, double &Fx, double &Fy, double &Fz, double &ub,
+                                          double &vb)
+{
+    double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
+    const double r2 = pbcr2_exact(dx, dy, dz, S), r1 = sqrt(r2);
+    const double term = r1 - bd.beq[b];
+    const int pw = bd.bpw[b];
+    double tp = 1.0;
+    for (int k = 0; k < pw - 1; ++k) tp *= term;
+    double fac = bd.bk[b] * tp;
+    const double u = fac * term;
+    fac = -(pw * fac / r1);
+    Fx += fac * dx;
+    Fy += fac * dy;
+    Fz += fac * dz;
+    if (count) {
+        ub += u;
+        vb -= fac * r2;
+    }
+}
 
 // UBond (Src/energy.F90:5335-5387) for particle i: the forces of its bonds (both ends of
 // a bond compute it) added to F; each bond's energy and virial counted once (o < po).
+// Bonds in CSR order, from the bond table when there is one.
 __device__ __forceinline__ void bond_forces(const FinBonds &bd, const SysDev &S, const double4 *__restrict__ pos,
                                             int i, const double4 &x, double &Fx, double &Fy, double &Fz,
                                             double &ub, double &vb)
 {
+    if (bd.tab) {
+        const int4 e = bd.tab[i];
+        if (e.x >= 0) bond_term(bd, S, x, pos[e.x], e.y & (BT_COUNT - 1), (e.y & BT_COUNT) != 0, Fx, Fy, Fz, ub, vb);
+        if (e.z >= 0) bond_term(bd, S, x, pos[e.z], e.w & (BT_COUNT - 1), (e.w & BT_COUNT) != 0, Fx, Fy, Fz, ub, vb);
+        return;
+    }
     const int o = bd.orig[i];
     const int b0 = bd.bptr[S.off + o], b1 = bd.bptr[S.off + o + 1];
     for (int b = b0; b < b1; ++b) {
         const int po = bd.bpart[b];
-        const double4 xj = pos[bd.inv[S.off + po]];
-        double dx = x.x - xj.x, dy = x.y - xj.y, dz = x.z - xj.z;
-        const double r2 = pbcr2_exact(dx, dy, dz, S), r1 = sqrt(r2);
-        const double term = r1 - bd.beq[b];
-        const int pw = bd.bpw[b];
-        double tp = 1.0;
-        for (int k = 0; k < pw - 1; ++k) tp *= term;
-        double fac = bd.bk[b] * tp;
-        const double u = fac * term;
-        fac = -(pw * fac / r1);
-        Fx += fac * dx;
-        Fy += fac * dy;
-        Fz += fac * dz;
-        if (o < po) {
-            ub += u;
-            vb -= fac * r2;
-        }
+        bond_term(bd, S, x, pos[bd.inv[S.off + po]], b, o < po, Fx, Fy, Fz, ub, vb);
     }
 }
 
