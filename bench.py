@@ -221,6 +221,12 @@ class L2Flush:
         self.r.sum()
 
 
+def tuner_run(flush):
+    """Step timer for the pair-kernel tuner: ms per step of `steps` device-timed MD steps
+    with the L2 flushed before each, as the timed legs run them."""
+    return lambda e, steps: timed_md_steps(e, steps, flush, 0) / steps
+
+
 def timed_md_steps(e, K, flush, warmup):
     """K MD steps of every system of engine e, L2 flushed before each; device time
     summed over the steps (ms), CUDA events on the engine's stream."""
@@ -331,7 +337,7 @@ def run_ensemble(a, flush, rank=0, world=1):
     eng = Engine(sy, tables, precision="mixed")
     eng.UTotal(0)
     eng.GetLinAcc()
-    best, lane_ms = tune_pair_kernel(eng)
+    best, lane_ms = tune_pair_kernel(eng, run=tuner_run(flush))
     eng.reset_states()
     eng.UTotal(0)
     eng.GetLinAcc()
@@ -893,17 +899,18 @@ def run_gpu(a):
     eng = Engine(s, precision=a.precision)
     eng.UTotal()
     eng.GetLinAcc()
+    flush = L2Flush()
     tuned = None
     if a.precision == "mixed":
         from molsim_b200.autotune import tune_pair_kernel
-        tuned, _ = tune_pair_kernel(eng, steps=20)
+        # the tuner times steps as this bench does: on the device, L2 flushed before each
+        tuned, _ = tune_pair_kernel(eng, steps=40, run=tuner_run(flush))
         # the timed steps start from the seeded initial state, however long the tuning ran
         eng.reset_states()
         eng.UTotal()
         eng.GetLinAcc()
     _, _, npair = eng.SetVList(0, export=False)
     ext = torch.cuda.ExternalStream(eng.stream())
-    flush = L2Flush()
     L = _lib.lib()
 
     def step_async(k):
@@ -978,7 +985,7 @@ def run_gpu(a):
         tuned_b = None
         if a.precision == "mixed":
             from molsim_b200.autotune import tune_pair_kernel
-            tuned_b, _ = tune_pair_kernel(eb, steps=5)
+            tuned_b, _ = tune_pair_kernel(eb, steps=5, run=tuner_run(flush))
             eb.reset_states()
             eb.UTotal(0)
             eb.GetLinAcc()

@@ -95,15 +95,27 @@ def apply_grids(systems, edges, order=4):
     return out
 
 
-def _time_steps(engine, steps, repeats=3):
-    """Milliseconds per MD step: the best of `repeats` runs of `steps` steps (a run that
-    happens to hold a list rebuild, or a busy moment of the host, does not decide)."""
+def _time_steps(engine, steps, repeats=3, run=None):
+    """Milliseconds per MD step: the best of `repeats` runs of `steps` steps, each from the
+    systems' initial state, so that every setting is timed over the same stretch of the
+    same trajectory (the systems relax from their start and rebuild their lists more or
+    less often as they go, which would otherwise favour whichever setting is timed
+    first); a run that happens to meet a busy moment of the host does not decide.  `run`,
+    when given, times the steps instead: run(engine, steps) -> ms per step (for instance
+    device-timed steps with the caller's cache conditions); by default the wall clock
+    times them."""
     import torch
 
-    engine.VelVer(2, energies=False)               # capture the graph for this layout
-    torch.cuda.synchronize()
     best = float("inf")
     for _ in range(repeats):
+        engine.reset_states()
+        engine.UTotal(0)
+        engine.GetLinAcc()
+        if run is not None:
+            best = min(best, run(engine, steps))
+            continue
+        engine.VelVer(2, energies=False)           # (re)capture the graph for this layout
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         engine.VelVer(steps, energies=False)
         torch.cuda.synchronize()
@@ -123,15 +135,17 @@ def tune_pair_lanes(engine, shifts=(-1, 0, 1), steps=10):
     return best, times
 
 
-def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2), kinds=(2, 3),
-                     overlaps=(1, 0)):
+def tune_pair_kernel(engine, steps=10, shifts=(-3, -2, -1, 0, 1), unrolls=(1, 2, 4), blocks=(0, 2), kinds=(2, 3),
+                     overlaps=(1, 0), run=None):
     """Shape of the pair kernel for this handle, by timing MD steps: the list layout
     (kind 2: half list with partner atomics, 3: full list), lanes per particle
     (2^shift times the default), row entries in flight per lane (unroll), whether the
     pair kernel runs beside the SPME chain or after it (overlap 1 or 0), and pair blocks
-    per SM (0: as many as fit; 2: room for the SPME chain beside it), one knob at a time
-    from the defaults.  Leaves the engine on the best; returns ({knob: value}, {setting:
-    ms per step}).  Mixed precision only (the knobs belong to its pair kernel).  Every
+    per SM (0: as many as fit; 2: room for the SPME chain beside it).  Layout and lanes
+    are searched together (which lane count suits a system depends on the layout), the
+    other knobs one at a time from there; each setting is timed from the systems'
+    initial state (by `run` when given, see _time_steps).  Leaves the engine on the best; returns ({knob: value},
+    {setting: ms per step}).  Mixed precision only (the knobs belong to its pair kernel).  Every
     setting gives the same results to FP32 rounding of the forces."""
     from . import _lib
 
@@ -143,21 +157,24 @@ def tune_pair_kernel(engine, steps=10, shifts=(-1, 0, 1), unrolls=(1, 2, 4), blo
 
     best = {"kind": 2, "shift": 0, "unroll": 2, "overlap": 1, "blocks": 0}
     log = {}
-    for name, vals, key in (("kind", kinds, _lib.MSG_TUNE_PAIR_KERNEL), ("shift", shifts, None),
-                            ("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
+    res = {}
+    for kd in kinds:
+        setk(_lib.MSG_TUNE_PAIR_KERNEL, kd)
+        for sh in shifts:
+            engine.tune_pair_lanes(sh)
+            res[(kd, sh)] = _time_steps(engine, steps, run=run)
+            log["kind=%s,shift=%s" % (kd, sh)] = res[(kd, sh)]
+    best["kind"], best["shift"] = min(res, key=res.get)
+    setk(_lib.MSG_TUNE_PAIR_KERNEL, best["kind"])
+    engine.tune_pair_lanes(best["shift"])
+    for name, vals, key in (("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
                             ("overlap", overlaps, _lib.MSG_TUNE_OVERLAP),
                             ("blocks", blocks, _lib.MSG_TUNE_PAIR_BLOCKS)):
         res = {}
         for v in vals:
-            if key is None:
-                engine.tune_pair_lanes(v)
-            else:
-                setk(key, v)
-            res[v] = _time_steps(engine, steps)
+            setk(key, v)
+            res[v] = _time_steps(engine, steps, run=run)
             log["%s=%s" % (name, v)] = res[v]
         best[name] = min(res, key=res.get)
-        if key is None:
-            engine.tune_pair_lanes(best[name])
-        else:
-            setk(key, best[name])
+        setk(key, best[name])
     return best, log
