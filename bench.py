@@ -337,7 +337,7 @@ def run_ensemble(a, flush, rank=0, world=1):
     eng = Engine(sy, tables, precision="mixed")
     eng.UTotal(0)
     eng.GetLinAcc()
-    best, lane_ms = tune_pair_kernel(eng, run=tuner_run(flush))
+    best, lane_ms = tune_pair_kernel(eng, steps=25, run=tuner_run(flush))
     eng.reset_states()
     eng.UTotal(0)
     eng.GetLinAcc()

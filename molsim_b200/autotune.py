@@ -142,9 +142,11 @@ def tune_pair_kernel(engine, steps=10, shifts=(-3, -2, -1, 0, 1), unrolls=(1, 2,
     (2^shift times the default), row entries in flight per lane (unroll), whether the
     pair kernel runs beside the SPME chain or after it (overlap 1 or 0), and pair blocks
     per SM (0: as many as fit; 2: room for the SPME chain beside it).  Layout and lanes
-    are searched together (which lane count suits a system depends on the layout), the
-    other knobs one at a time from there; each setting is timed from the systems'
-    initial state (by `run` when given, see _time_steps).  Leaves the engine on the best; returns ({knob: value},
+    are searched together (which lane count suits a system depends on the layout), then
+    entries in flight and the overlap together (more entries in flight hold more of an
+    SM's registers, which the SPME chain beside the kernel also needs), then the blocks;
+    each setting is timed from the systems' initial state (by `run` when given, see
+    _time_steps).  Leaves the engine on the best; returns ({knob: value},
     {setting: ms per step}).  Mixed precision only (the knobs belong to its pair kernel).  Every
     setting gives the same results to FP32 rounding of the forces."""
     from . import _lib
@@ -167,9 +169,17 @@ def tune_pair_kernel(engine, steps=10, shifts=(-3, -2, -1, 0, 1), unrolls=(1, 2,
     best["kind"], best["shift"] = min(res, key=res.get)
     setk(_lib.MSG_TUNE_PAIR_KERNEL, best["kind"])
     engine.tune_pair_lanes(best["shift"])
-    for name, vals, key in (("unroll", unrolls, _lib.MSG_TUNE_PAIR_UNROLL),
-                            ("overlap", overlaps, _lib.MSG_TUNE_OVERLAP),
-                            ("blocks", blocks, _lib.MSG_TUNE_PAIR_BLOCKS)):
+    res = {}
+    for un in unrolls:
+        setk(_lib.MSG_TUNE_PAIR_UNROLL, un)
+        for ov in overlaps:
+            setk(_lib.MSG_TUNE_OVERLAP, ov)
+            res[(un, ov)] = _time_steps(engine, steps, run=run)
+            log["unroll=%s,overlap=%s" % (un, ov)] = res[(un, ov)]
+    best["unroll"], best["overlap"] = min(res, key=res.get)
+    setk(_lib.MSG_TUNE_PAIR_UNROLL, best["unroll"])
+    setk(_lib.MSG_TUNE_OVERLAP, best["overlap"])
+    for name, vals, key in (("blocks", blocks, _lib.MSG_TUNE_PAIR_BLOCKS),):
         res = {}
         for v in vals:
             setk(key, v)
