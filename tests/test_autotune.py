@@ -100,3 +100,30 @@ def test_scheduling_knobs_keep_mixed_results_bitwise():
             assert np.array_equal(a, b), knobs
         for a, b in zip(got[1], ref[1]):
             assert a == b, knobs
+
+
+@pytest.mark.gpu
+def test_pair_kernel_search_end_to_end():
+    """The pair-kernel search on a small batch (a reduced grid of settings, each timed from
+    the initial state): every knob comes back, the log holds one time per setting, and the
+    tuned handle, put back at the initial state, agrees with an untuned one to the
+    mixed-precision bars (forces 1e-5 relative RMS, energies 1e-7 relative)."""
+    from molsim_b200 import Engine
+
+    sy, tb = _ensemble(n=3, seed=9)
+    e = Engine(sy, tb, precision="mixed")
+    e.UTotal(0)
+    e.GetLinAcc()
+    best, log = A.tune_pair_kernel(e, steps=2, shifts=(-1, 0), unrolls=(1, 2), blocks=(0, 2), kinds=(2, 3),
+                                   overlaps=(1, 0))
+    assert set(best) == {"kind", "shift", "unroll", "overlap", "blocks"}
+    assert len(log) == 2 * 2 + 2 * 2 + 2 and all(v > 0 for v in log.values())
+    assert (best["kind"], best["shift"]) in {(2, -1), (2, 0), (3, -1), (3, 0)}
+    e.reset_states()
+    ref = Engine(sy, tb, precision="mixed")
+    for k in range(len(sy)):
+        a, b = e.UTotal(k), ref.UTotal(k)
+        f0, f1 = np.asarray(a["force"]), np.asarray(b["force"])
+        assert np.sqrt(((f0 - f1) ** 2).sum() / (f1 ** 2).sum()) < 1e-5
+        for key in ("utot", "urec", "virial"):
+            assert abs(a[key] - b[key]) <= 1e-7 * abs(b[key]), (k, key)
