@@ -35,7 +35,8 @@ __device__ __forceinline__ void block_dipole(double qx, double qy, double qz, lo
 // bit, alone or batched).  The splines are FP64 in both precisions: the charge
 // grid feeds the reciprocal energy and virial, which stay FP64.  A conversion
 // kernel then turns the integer grid into the FP64 input of the forward FFT and
-// clears it.
+// clears it (the convolution kernel of kernels_spme.cuh, where a handle uses it,
+// reads and clears the integer grid itself).
 // A block takes SPREAD_PART particles: one thread per particle forms the
 // splines into shared memory, then the block walks the particles' P^3
 // contributions x-fastest, so the lanes of a warp add into runs of P
