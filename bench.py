@@ -354,10 +354,43 @@ def run_ensemble(a, flush, rank=0, world=1):
     ms64 = timed_md_steps(e64, K, flush, a.warmup)
     del e64
     torch.cuda.synchronize()
+    # the same systems with the SPME reciprocal-space chain as one persistent kernel
+    # (MSG_SPME_CONV=1) and the pair kernel shaped as tuned above; a failure is recorded,
+    # not raised, so that it cannot cost the legs that follow
+    ms_conv, conv_err = None, None
+    try:
+        from molsim_b200 import _lib
+
+        os.environ["MSG_SPME_CONV"] = "1"
+        try:
+            ec = Engine(sy, tables, precision="mixed")
+        finally:
+            os.environ.pop("MSG_SPME_CONV", None)
+        Lc = _lib.lib()
+        for key, val in ((_lib.MSG_TUNE_PAIR_KERNEL, best["kind"]), (_lib.MSG_TUNE_PAIR_UNROLL, best["unroll"]),
+                         (_lib.MSG_TUNE_OVERLAP, best["overlap"]), (_lib.MSG_TUNE_PAIR_BLOCKS, best["blocks"])):
+            if Lc.msg_tune(ec.h, key, int(val)):
+                raise RuntimeError(Lc.msg_last_error(ec.h).decode())
+        ec.tune_pair_lanes(best["shift"])
+        ec.UTotal(0)
+        ec.GetLinAcc()
+        ms_conv = timed_md_steps(ec, K, flush, a.warmup)
+        del ec
+        torch.cuda.synchronize()
+    except Exception as ex:                                  # noqa: BLE001
+        conv_err = str(ex)[:200]
     per = gather_metrics({"systems": len(sy), "particles": ntot, "steps": K, "device_ms": ms,
-                          "device_ms_fp64": ms64, "edges": list(edges), "met": int(sum(r["met"] for r in rep))})
+                          "device_ms_fp64": ms64, "device_ms_conv": ms_conv, "conv_error": conv_err,
+                          "edges": list(edges), "met": int(sum(r["met"] for r in rep))})
     comb = combine_ensemble(per)
     comb64 = combine_ensemble([dict(m, device_ms=m["device_ms_fp64"]) for m in per])
+    conv = None
+    if all(m["device_ms_conv"] is not None for m in per):
+        cc = combine_ensemble([dict(m, device_ms=m["device_ms_conv"]) for m in per])
+        conv = {"value": cc["value"], "ms_per_step": cc["device_ms_max"] / K,
+                "vs_graph_cufft": cc["value"] / comb["value"]}
+    else:
+        conv = {"error": next((m["conv_error"] for m in per if m["conv_error"]), "not measured")}
     all_edges = [e_ for m in per for e_ in m["edges"]]
     hist = {g: all_edges.count(g) for g in sorted(set(all_edges))}
     return {"systems": comb["systems"], "particles": comb["particles"], "value": comb["value"], "unit": METRIC,
@@ -368,7 +401,7 @@ def run_ensemble(a, flush, rank=0, world=1):
                          "rule": "cheapest edge with measured reciprocal RMS force error <= Kolafa-Perram "
                                  "real-space estimate (reference 96^3 order 6)",
                          "pair_kernel": best, "pair_kernel_ms_per_step": lane_ms, "tune_s": t_tune},
-            "generate_s": t_gen}
+            "spme_conv_kernel": conv, "generate_s": t_gen}
 
 
 def run_bd(a, flush):
@@ -1115,6 +1148,7 @@ def run_gpu(a):
         "batched_roofline_frac": g(batched, "roofline", "frac"),
         "ensemble_value": g(ensemble, "value"), "ensemble_fp64_value": g(ensemble, "fp64_batched_value"),
         "vs_fp64_ensemble": g(ensemble, "vs_fp64_batched"),
+        "ensemble_spme_conv_value": g(ensemble, "spme_conv_kernel", "value"),
         "bd_200k_value": g(bd, "value"), "bd_200k_fp64_value": g(bd, "fp64_value"),
         "vs_fp64_bd_200k": g(bd, "vs_fp64"), "bd_200k_roofline_frac": g(bd, "roofline", "frac"),
         "serving_value": g(serving, "value"), "serving_p50_s": g(serving, "p50_s"),
