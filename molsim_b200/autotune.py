@@ -151,12 +151,7 @@ def tune_pair_kernel(engine, steps=10, shifts=(-3, -2, -1, 0, 1), unrolls=(1, 2,
     setting gives the same results to FP32 rounding of the forces."""
     from . import _lib
 
-    L = _lib.lib()
-
-    def setk(key, val):
-        if L.msg_tune(engine.h, key, int(val)):
-            raise RuntimeError("msg_tune(%d, %d) failed" % (key, val))
-
+    setk = engine.tune
     best = {"kind": 2, "shift": 0, "unroll": 2, "overlap": 1, "blocks": 0}
     log = {}
     res = {}

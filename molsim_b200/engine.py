@@ -255,6 +255,10 @@ class Engine:
         self._check(_lib.lib().msg_get_forces(self.h, isys, _p(f, C.c_double), _p(fo, C.c_double)))
         return f, fo
 
+    def tune(self, key, value):
+        """msg_tune: one scheduling knob (MSG_TUNE_*) of this handle."""
+        self._check(_lib.lib().msg_tune(self.h, int(key), int(value)))
+
     def tune_pair_lanes(self, shift):
         """Lanes per particle in the pair kernel scaled by 2**shift (results move by rounding only)."""
         self._check(_lib.lib().msg_tune(self.h, _lib.MSG_TUNE_PAIR_LANES, int(shift)))

@@ -127,3 +127,57 @@ def test_pair_kernel_search_end_to_end():
         assert np.sqrt(((f0 - f1) ** 2).sum() / (f1 ** 2).sum()) < 1e-5
         for key in ("utot", "urec", "virial"):
             assert abs(a[key] - b[key]) <= 1e-7 * abs(b[key]), (k, key)
+
+
+class _FakeHandle:
+    """Stands in for an engine in the pair-kernel search: records the knobs it is set to
+    and how often it is put back at its initial state; no device."""
+
+    def __init__(self):
+        from molsim_b200 import _lib
+
+        self.knobs = {_lib.MSG_TUNE_PAIR_KERNEL: 2, _lib.MSG_TUNE_PAIR_UNROLL: 2, _lib.MSG_TUNE_OVERLAP: 1,
+                      _lib.MSG_TUNE_PAIR_BLOCKS: 0}
+        self.shift = 0
+        self.resets = 0
+
+    def tune(self, key, value):
+        self.knobs[key] = int(value)
+
+    def tune_pair_lanes(self, shift):
+        self.shift = int(shift)
+
+    def reset_states(self):
+        self.resets += 1
+
+    def UTotal(self, isys=0):
+        return {}
+
+    def GetLinAcc(self):
+        pass
+
+
+def test_pair_kernel_search_finds_interacting_settings():
+    """The search on a handle whose step time has the interactions the measured workloads
+    showed: the full list wins only with a quarter of the lanes, four entries in flight win
+    only with the pair kernel beside the SPME chain.  Knob by knob from the defaults the
+    search would stop at (half list, 2^-2 lanes) and (4 entries, beside); searching layout
+    with lanes and entries with overlap together it lands on the best of each pair, and every
+    setting is timed from a fresh start."""
+    from molsim_b200 import _lib as K
+
+    e = _FakeHandle()
+
+    def step_ms(h, steps):
+        kind, un = h.knobs[K.MSG_TUNE_PAIR_KERNEL], h.knobs[K.MSG_TUNE_PAIR_UNROLL]
+        ov, bl = h.knobs[K.MSG_TUNE_OVERLAP], h.knobs[K.MSG_TUNE_PAIR_BLOCKS]
+        t = 5.0 + {(2, 0): 0.0, (3, 0): 0.1, (2, -2): -0.2, (3, -2): -0.5}.get((kind, h.shift), 0.3)
+        t += {(2, 1): 0.0, (4, 1): -0.02, (2, 0): -0.2, (4, 0): 0.25}.get((un, ov), 0.4)
+        return t + (0.0 if bl == 0 else 0.05)
+
+    best, log = A.tune_pair_kernel(e, steps=3, run=step_ms)
+    assert best == {"kind": 3, "shift": -2, "unroll": 2, "overlap": 0, "blocks": 0}
+    assert len(log) == 2 * 5 + 3 * 2 + 2
+    assert e.resets == 3 * len(log)
+    assert (e.knobs[K.MSG_TUNE_PAIR_KERNEL], e.shift, e.knobs[K.MSG_TUNE_PAIR_UNROLL],
+            e.knobs[K.MSG_TUNE_OVERLAP], e.knobs[K.MSG_TUNE_PAIR_BLOCKS]) == (3, -2, 2, 0, 0)
